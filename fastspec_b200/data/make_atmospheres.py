@@ -1,0 +1,396 @@
+#!/usr/bin/env python3
+"""Derive the host-side atmosphere states of the benchmark configurations from the reference.
+
+The hot path consumes, per atmosphere, what the reference's host code (EOS, continuum) hands
+it: T, Rhox, Xne, Rho, the species populations FractionPF (FP32), species masses, the
+perturber density of van der Waals broadening, and the continuum opacity.  The EOS and the
+continuum stay on the host and out of scope, and the reference is Fortran with no compiler on
+either machine, so this script runs the reference's shipped program as a black box, here,
+once, and stores what it computed:
+
+  * model atmospheres: synthetic Eddington-grey hydrostatic models (workloads.eddington_model)
+    for the solar-type (Teff 5777, log g 4.44, 56 depths), cool-dwarf (3500, 5.0, 72) and
+    magnetic (5000, 4.5, 56) configurations;
+  * T, Rhox, Xne, Xna, Rho after the EOS: read from fs_lineop.bin;
+  * FractionPF per species: one probe line per species placed on a grid point, with only
+    radiative damping, E_low = 0: LineOpac at the centre is H(a, 0) * LinCop, every factor of
+    LinCop except FractionPF is known (opacity.f90:239-293), so FractionPF is the ratio.
+    The recovered value must sit on an FP32 number (FractionPF is REAL(4)); that check
+    confirms the species mass used for the Doppler width too;
+  * the van der Waals perturber density Nprtb: one probe with a large G6: H(a, 0) is
+    inverted on the table's bilinear lerp for a, a -> Gamma_6 -> Nprtb;
+  * the continuum opacity on coarse knots spanning each configuration's range.
+
+Also writes parity fixtures (tests/golden/pin_*.npz): line lists run through the reference
+with the reference's line opacity, windows and spectra, for the oracle/GPU parity tests.
+
+Needs the reference at /root/reference (this container only); the outputs are committed.
+"""
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+
+import oracle  # noqa: E402  (fixture generation: the oracle is the inversion model)
+from fastspec_b200 import fsio, workloads as W  # noqa: E402
+
+BIN = "/root/reference/src/fastspec_Linux_x86_64"
+
+AMASS = {"H": 1.00794, "He": 4.002602, "C": 12.0107, "N": 14.0067, "O": 15.9994,
+         "Ca": 40.078, "Ti": 47.867, "Cr": 51.9961, "Fe": 55.845, "Ni": 58.6934}
+POTION = {("Fe", 1): 7.9024, ("Fe", 2): 16.1878, ("Ti", 1): 6.8281, ("Cr", 1): 6.7665,
+          ("Ni", 1): 7.6399, ("Ca", 1): 6.1132, ("TiO", 1): 6.4, ("H2O", 1): 12.621,
+          ("CO", 1): 14.014, ("OH", 1): 13.017}
+COMPOSITION = {"TiO": [("Ti", 1), ("O", 1)], "H2O": [("H", 2), ("O", 1)],
+               "CO": [("C", 1), ("O", 1)], "OH": [("O", 1), ("H", 1)]}
+
+
+def mass_candidates(name):
+    """FP32 species mass as the EOS forms it: atoms REAL(4) Amass, molecules the REAL(4) sum of
+    constituent masses (eos.f:1817, 1865); both summation orders are tried."""
+    if name not in COMPOSITION:
+        return [np.float32(AMASS[name])]
+    comp = COMPOSITION[name]
+    out = []
+    for order in (comp, comp[::-1]):
+        s = np.float32(0.0)
+        for el, k in order:
+            s = np.float32(s + np.float32(k) * np.float32(AMASS[el]))
+        out.append(s)
+    return out
+
+
+def run_ref(workdir, deck):
+    with open(os.path.join(workdir, "in.dat"), "w") as f:
+        f.write(deck)
+    r = subprocess.run([BIN, "in.dat"], cwd=workdir, capture_output=True, text=True)
+    if r.returncode != 0 or "Total time" not in r.stdout:
+        raise RuntimeError("reference run failed:\n" + r.stdout + r.stderr)
+    return r.stdout
+
+
+def probe_list(species, wl0, spacing, vdw_species=0, ismol=False, loggf=None):
+    """One probe per species (G_rad only, E_low = 0) plus one van der Waals probe."""
+    n = len(species)
+    wl = wl0 + spacing * (1 + np.arange(n + 1))
+    spc = np.concatenate([np.arange(n), [vdw_species]])
+    loggf = np.full(n + 1, -1.0) if loggf is None else np.asarray(loggf, np.float64)
+    elo = np.zeros(n + 1)
+    lgrad = np.concatenate([np.full(n, 8.0), [5.0]])
+    lgqst = np.full(n + 1, -30.0)
+    lgvdw = np.concatenate([np.full(n, -30.0), [-6.5]])
+    return W.LineList(species, wl, loggf, elo, lgrad, lgqst, lgvdw, spc,
+                      np.full(n + 1, int(ismol), np.int32))
+
+
+def calibrate_probes(species, ismol, wl0, dstep, vmic, molbrd, workdir, target=(0.3, 0.1)):
+    """log gf of each probe so that its peak line/continuum ratio is about `target`
+    (species probes, vdW probe): weak enough that the windows stay isolated."""
+    nsp = len(species)
+    probes = probe_list(species, wl0, 2.0, ismol=ismol)
+    wend = wl0 + 2.0 * (nsp + 2)
+    probes.write_z(os.path.join(workdir, "lines.z"), wl0, wend)
+    deck = ("wave=%.4f, %.4f, %.6f, 0\nsave=0, 1, 1, 0, 0\nvmic=%.3f\nmolbrd=%d\n"
+            "lines=\n-1  lines.z\n\nmodel=model.krz\nmus=0\n" % (wl0, wend, dstep, vmic, molbrd))
+    run_ref(workdir, deck)
+    lo = fsio.read_opac(os.path.join(workdir, "fs_lineop.bin"))
+    co = fsio.read_opac(os.path.join(workdir, "fs_contop.bin"))
+    out = []
+    for k in range(nsp + 1):
+        ic = int(np.argmin(np.abs(lo["wave"] - probes.wl[k])))
+        ratio = np.max(lo["opac"][ic] / co["opac"][ic])
+        tgt = target[0] if k < nsp else target[1]
+        out.append(round(-1.0 + np.log10(tgt / ratio), 3))
+    return np.array(out)
+
+
+def make_state(atm, species, masses, fpf, nprtb=None, contopac=None):
+    nt = len(atm["T"])
+    if nprtb is None:
+        h1 = np.zeros(nt, np.float32); he1 = np.zeros(nt, np.float32)
+    else:
+        h1, he1 = encode_nprtb(nprtb)
+    st = dict(rhox=atm["rhox"], T=atm["T"], xne=atm["xne"], xna=atm["xna"], rho=atm["rho"],
+              fractionpf=fpf, xamass=np.asarray(masses, np.float32),
+              potion=np.array([POTION.get(s, 7.0) for s in species], np.float32),
+              ion=np.array([s[1] for s in species], np.int32), frac_h1=h1, frac_he1=he1,
+              frac_h2=np.zeros(nt, np.float32))
+    return st
+
+
+def encode_nprtb(nprtb):
+    """FP32 (H I, He I) pair with Fraction(H1) + 0.412265 Fraction(He1) == nprtb to ~1e-15."""
+    h1 = nprtb.astype(np.float32)
+    he1 = ((nprtb - h1.astype(np.float64)) / 0.412265).astype(np.float32)
+    return h1, he1
+
+
+def invert_h0(h, a_guess):
+    """a with HVoigt(a, 0) == h (voigt.f90:76-110), by bisection on the oracle's HVoigt,
+    which decreases monotonically in a at v = 0 (table lerp and asymptotic branches)."""
+    out = np.empty_like(h)
+    for i, hv in enumerate(h):
+        lo, hi = 0.0, max(16.0, 4.0 * a_guess[i])
+        while oracle.hvoigt(hi, 0.0) > hv:
+            hi *= 2.0
+        for _ in range(200):
+            mid = 0.5 * (lo + hi)
+            if mid == lo or mid == hi:
+                break
+            if oracle.hvoigt(mid, 0.0) > hv:
+                lo = mid
+            else:
+                hi = mid
+        out[i] = 0.5 * (lo + hi)
+    return out
+
+
+def recover(model, species, ismol, wl0, dstep, vmic, molbrd, workdir, extra_lines=None,
+            extra_region=None, mus=0, save_spec=False, bfield=None):
+    """Run the probes (+ optional extra lines in a separate region); recover the state."""
+    nsp = len(species)
+    W.write_krz(os.path.join(workdir, "model.krz"), model)
+    pgf = calibrate_probes(species, ismol, wl0, dstep, vmic, molbrd, workdir)
+    probes = probe_list(species, wl0, 2.0, vdw_species=0, ismol=ismol, loggf=pgf)
+    wend = wl0 + 2.0 * (nsp + 2)
+    if extra_region is not None:
+        wend = extra_region[1]
+    allw = [probes]
+    if extra_lines is not None:
+        allw.append(extra_lines)
+    merged = merge(allw)
+    W.write_krz(os.path.join(workdir, "model.krz"), model)
+    pats = None
+    if bfield is not None:
+        pats = zeeman_blocks(merged)
+    merged.write_z(os.path.join(workdir, "lines.z"), wl0, wend, patterns=pats)
+    deck = ("wave=%.4f, %.4f, %.6f, 0\nsave=0, %d, 1, %d, %d\nvmic=%.3f\nmolbrd=%d\n"
+            "lines=\n-1  lines.z\n\nmodel=model.krz\nmus=%d\n"
+            % (wl0, wend, dstep, 0 if bfield is not None else 1, int(save_spec), int(save_spec and mus > 1),
+               vmic, molbrd, mus))
+    if bfield is not None:
+        deck += "bframe=1\nbfield=%g, %g, %g\n" % tuple(bfield)
+    log = run_ref(workdir, deck)
+    co = fsio.read_opac(os.path.join(workdir, "fs_contop.bin"))
+    if bfield is None:
+        lo = fsio.read_opac(os.path.join(workdir, "fs_lineop.bin"))
+        atm = lo
+    else:
+        # the magnetic run saves no line opacity: recover from a companion field-free run
+        raise RuntimeError("use recover() without bfield for the state")
+    grid = dict(wmode=0, wstart=wl0, wend=wend, dstep=dstep)
+    nt = len(atm["T"])
+    # FractionPF per species, with the FP32 species mass that makes it land on FP32 values
+    fpf = np.zeros((nt, nsp), np.float32)
+    masses = []
+    one = np.ones((nt, nsp), np.float32)
+    wave = None
+    for k, sp in enumerate(species):
+        best = None
+        for m in mass_candidates(sp[0]):
+            ms = [np.float32(1.0)] * nsp
+            ms[k] = m
+            st = oracle.State(grid, make_state(atm, species, ms, one), contopac=co["opac"],
+                              vmicro=vmic, molbrd=molbrd)
+            if wave is None:
+                wave = st.wave + st.wfirst
+            L = oracle.Lines(**lines_args(probes), kind=2)
+            cop, vv, av = oracle.xline(st, L, k)
+            ic = int(np.argmin(np.abs(wave - probes.wl[k])))
+            assert abs(wave[ic] - probes.wl[k]) < 1e-9, "probe not on a grid point"
+            h0 = np.array([oracle.hvoigt(a, 0.0) for a in av])
+            rec = atm["opac"][ic] / (h0 * cop)
+            f32 = rec.astype(np.float32)
+            dev = np.max(np.abs(rec / f32.astype(np.float64) - 1.0))
+            if best is None or dev < best[0]:
+                best = (dev, m, f32)
+        if best[0] > 1e-10:
+            print("  warning: %s %d FractionPF off FP32 by %.2e" % (sp[0], sp[1], best[0]))
+        fpf[:, k] = best[2]
+        masses.append(best[1])
+        print("  %-4s %d  mass %.6f  FractionPF fp32 dev %.1e" % (sp[0], sp[1], best[1], best[0]))
+    # Nprtb from the vdW probe (species 0)
+    st = oracle.State(grid, make_state(atm, species, masses, fpf), contopac=co["opac"],
+                      vmicro=vmic, molbrd=molbrd)
+    L = oracle.Lines(**lines_args(probes), kind=2)
+    kv = nsp
+    cop, vv, av0 = oracle.xline(st, L, kv)
+    ic = int(np.argmin(np.abs(wave - probes.wl[kv])))
+    h = atm["opac"][ic] / cop
+    a = invert_h0(h, av0)
+    WaveL = probes.wl[kv]
+    dopl = 1.0 / (vv * WaveL)
+    dndopl = dopl / WaveL
+    c4pi = 4.0 * 299792.458e13 * np.pi
+    gam = a * (dndopl * c4pi)
+    g6 = gam - float(probes.grad[kv])
+    temp3 = (atm["T"] / 1e4) ** 0.3
+    nprtb = g6 / (float(probes.gvdw[kv]) * temp3)
+    state = make_state(atm, species, masses, fpf, nprtb=nprtb)
+    # verify: the oracle reproduces the whole probe run
+    st = oracle.State(grid, state, contopac=co["opac"], vmicro=vmic, molbrd=molbrd)
+    Lall = oracle.Lines(**lines_args(merged), kind=2)
+    res = oracle.lineop_calc(st, Lall, list_type=2)
+    ref = atm["opac"]
+    m = ref > 1e-30 * ref.max()
+    rel = np.max(np.abs(res["lineopac"][m] / ref[m] - 1.0)) if m.any() else 0.0
+    zero_match = np.array_equal(res["lineopac"] > 0, ref > 0)
+    print("  probe run reproduced: max rel %.2e, nonzero pattern equal %s" % (rel, zero_match))
+    return dict(state=state, nprtb=nprtb, masses=masses, atm=atm, contopac=co["opac"], probe_loggf=pgf,
+                wave=wave, grid=grid, merged=merged, oracle_lineopac=res["lineopac"],
+                ref_lineopac=ref, log=log, rel=rel, zero_match=zero_match, res=res)
+
+
+def lines_args(L):
+    a = L.arrays()
+    return dict(wl=a["wl"], elo=a["elo"], gf=a["gf"], grad=a["grad"], gqst=a["gqst"],
+                gvdw=a["gvdw"], spc=a["spc"], ismol=a["ismol"])
+
+
+def merge(lists):
+    sp = lists[0].species
+    cat = lambda f: np.concatenate([getattr(l, f) for l in lists])
+    txt = lambda f: np.concatenate([l._txt[f] for l in lists])
+    out = W.LineList(sp, cat("wl"), txt("loggf"), txt("elo"), txt("lgrad"), txt("lgqst"),
+                     txt("lgvdw"), cat("spc"), cat("ismol"))
+    if any(l.zeeman is not None for l in lists):
+        zz = []
+        for l in lists:
+            if l.zeeman is None:
+                z = (np.full(l.n, 1.0, np.float32), np.full(l.n, 1.0, np.float32),
+                     np.full(l.n, 1.0, np.float32), np.full(l.n, 1.0, np.float32))
+            else:
+                z = l.zeeman
+            zz.append(z)
+        z4 = [np.concatenate([z[q] for z in zz]) for q in range(4)]
+        order = np.argsort(cat("wl"), kind="stable")
+        out.zeeman = tuple(a[order] for a in z4)
+    return out
+
+
+def zeeman_blocks(L):
+    pats = []
+    jlo, jup, glo, gup = L.zeeman
+    for i in range(L.n):
+        spi, rpi, ss, rs = oracle.zeeman_pattern(jlo[i], jup[i], glo[i], gup[i])
+        pats.append((spi, rpi, ss, rs))
+    return pats
+
+
+def coarse_contopac(model, wmin, wmax, step, species, vmic, molbrd, workdir, nknots):
+    """Continuum opacity of the model on `nknots` knots spanning [wmin, wmax]."""
+    probes = probe_list(species, wmin, 1.0)
+    W.write_krz(os.path.join(workdir, "model.krz"), model)
+    probes.write_z(os.path.join(workdir, "lines.z"), wmin, wmax)
+    deck = ("wave=%.4f, %.4f, %.6f, 0\nsave=0, 0, 1, 0, 0\nvmic=%.3f\nmolbrd=%d\n"
+            "lines=\n-1  lines.z\n\nmodel=model.krz\nmus=0\n" % (wmin, wmax, step, vmic, molbrd))
+    run_ref(workdir, deck)
+    co = fsio.read_opac(os.path.join(workdir, "fs_contop.bin"))
+    idx = np.unique(np.linspace(0, len(co["wave"]) - 1, nknots).round().astype(int))
+    return co["wave"][idx], co["opac"][idx]
+
+
+CONFIGS = {
+    # name: (teff, logg, ntau, species, ismol, probe wl0, dstep, vmic, molbrd, range, nknots)
+    "solar": (5777.0, 4.44, 56, W.ATOMIC_C0, 0, 5000.0, 0.005, 1.0, 0, (3000.0, 9000.0), 1201),
+    "cooldwarf": (3500.0, 5.0, 72, W.MOLECULES_C1, 1, 9000.0, 0.01, 1.0, 1, (5000.0, 25000.0), 2001),
+    "magnetic": (5000.0, 4.5, 56, W.ATOMIC_C0, 0, 6000.0, 0.002, 1.0, 0, (5900.0, 6200.0), 301),
+}
+
+
+def main():
+    outdir = HERE
+    gold = os.path.join(REPO, "tests", "golden")
+    os.makedirs(gold, exist_ok=True)
+    oracle.build()
+    for name, (teff, logg, ntau, species, ismol, wl0, dstep, vmic, molbrd, rng_, nk) in CONFIGS.items():
+        print(name)
+        model = W.eddington_model(teff, logg, ntau)
+        with tempfile.TemporaryDirectory() as wd:
+            r = recover(model, species, ismol, wl0, dstep, vmic, molbrd, wd)
+            kw, kc = coarse_contopac(model, rng_[0], rng_[1], 0.5 if name != "cooldwarf" else 1.0,
+                                     species, vmic, molbrd, wd, nk)
+        st = r["state"]
+        np.savez_compressed(
+            os.path.join(outdir, "atm_%s.npz" % name), teff=teff, logg=logg,
+            species=np.array(["%s %d" % s for s in species]), ismol=ismol, vmicro=vmic,
+            molbrd=molbrd, rhox=st["rhox"], T=st["T"], xne=st["xne"], xna=st["xna"],
+            rho=st["rho"], fractionpf=st["fractionpf"], xamass=st["xamass"],
+            potion=st["potion"], ion=st["ion"], frac_h1=st["frac_h1"], frac_he1=st["frac_he1"],
+            nprtb=r["nprtb"], cont_wave=kw, cont_opac=kc.astype(np.float64),
+            probe_rel=r["rel"], probe_loggf=r["probe_loggf"], model_rhox=model["rhox"],
+            model_T=model["T"])
+    make_pins(gold)
+
+
+def load_state(name):
+    d = np.load(os.path.join(HERE, "atm_%s.npz" % name))
+    keys = ("rhox", "T", "xne", "xna", "rho", "fractionpf", "xamass", "potion", "ion",
+            "frac_h1", "frac_he1")
+    st = {k: d[k] for k in keys}
+    st["frac_h2"] = np.zeros(len(d["T"]), np.float32)
+    return st
+
+
+def make_pins(gold):
+    """Parity fixtures: reference line opacity and spectra of seeded lists on small grids.
+
+    Each run holds the probe lines first (they fix the species inventory order of the EOS,
+    hence the identical state) and the seeded list in a separate region; the region's line
+    opacity, continuum opacity and spectra are stored with the list."""
+    specs = [
+        # name, atmosphere, list maker, (wstart, wend, step, wmode), pin region
+        ("pin_solar", "solar", lambda: W.atomic_lines(160, 5040.5, 5044.5, W.SEED0 + 0),
+         (5000.0, 5045.0, 0.005, 0), (5040.0, 5045.0)),
+        ("pin_cooldwarf", "cooldwarf", lambda: W.molecular_lines(400, 9040.5, 9046.5, W.SEED0 + 1),
+         (9000.0, 9047.0, 0.3, 1), (9040.0, 9047.0)),
+    ]
+    for name, atmname, mk, grid, region in specs:
+        teff, logg, ntau, species, ismol, _, _, vmic, molbrd, _, _ = CONFIGS[atmname]
+        model = W.eddington_model(teff, logg, ntau)
+        state = load_state(atmname)
+        extra = mk()
+        pgf = np.load(os.path.join(HERE, "atm_%s.npz" % atmname))["probe_loggf"]
+        probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
+        merged = merge([probes, extra])
+        with tempfile.TemporaryDirectory() as wd:
+            W.write_krz(os.path.join(wd, "model.krz"), model)
+            merged.write_z(os.path.join(wd, "lines.z"), grid[0], grid[1])
+            deck = ("wave=%.4f, %.4f, %.6f, %d\nsave=0, 1, 1, 1, 1\nvmic=%.3f\nmolbrd=%d\n"
+                    "lines=\n-1  lines.z\n\nmodel=model.krz\nmus=7\n"
+                    % (grid[0], grid[1], grid[2], grid[3], vmic, molbrd))
+            run_ref(wd, deck)
+            lo = fsio.read_opac(os.path.join(wd, "fs_lineop.bin"))
+            co = fsio.read_opac(os.path.join(wd, "fs_contop.bin"))
+            sp = fsio.read_spec(os.path.join(wd, "fs_spec.bin"))
+            fl = fsio.read_flux(os.path.join(wd, "fs_flux.bin"))
+        for k in ("rhox", "T", "xne", "xna", "rho"):
+            assert np.array_equal(lo[k], state[k]), "EOS state differs from the recovered one: " + k
+        wave = lo["wave"]
+        sel = (wave >= region[0] - 1e-9) & (wave <= region[1] + 1e-9)
+        i0, i1 = (int(x) for x in np.nonzero(sel)[0][[0, -1]])
+        # the probes' windows must end before the region: check with the oracle
+        g = dict(wmode=grid[3], wstart=grid[0], wend=grid[1], dstep=grid[2])
+        st = oracle.State(g, state, contopac=co["opac"], vmicro=vmic, molbrd=molbrd)
+        rp = oracle.lineop_calc(st, oracle.Lines(**lines_args(probes), kind=2), list_type=2)
+        assert rp["iright"].max() < i0 + 1, "probe windows reach the pin region"
+        a = extra.arrays()
+        np.savez_compressed(
+            os.path.join(gold, name + ".npz"),
+            grid=np.array(grid, np.float64), i0=i0, i1=i1, atm=atmname,
+            species=np.array(["%s %d" % s for s in species]), vmicro=vmic, molbrd=molbrd,
+            contopac=co["opac"][i0:i1 + 1], lineopac=lo["opac"][i0:i1 + 1],
+            wave=wave[i0:i1 + 1], xmu=sp["xmu"], spl=sp["spl"][i0:i1 + 1],
+            spc=sp["spc"][i0:i1 + 1], sfl=fl["sfl"][i0:i1 + 1], sfc=fl["sfc"][i0:i1 + 1],
+            **{"line_" + k: v for k, v in a.items()})
+        print(name, "lines", extra.n, "region pixels", i1 - i0 + 1)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,250 @@
+"""Seeded synthetic workloads: model atmospheres and line lists.
+
+No public benchmark is involved: every line below is generated from numpy's PCG64 with seed
+20261203 + config, using the distributions of the five benchmark configurations (solar-type
+atomic synthesis, cool-dwarf molecular synthesis, polarised Zeeman synthesis, a batched grid
+and a differentiable fit).
+
+Line records carry exactly the FP32 values the reference's ASCII reader stores
+(ioutils.f90:1436-1466): gf = 10.0**loggf, Grad = 10.0**x for 0 < x < 20, Gqst/Gvdw =
+10.0**x for x < 0, all in single precision through the C library's powf, applied to the FP32
+parse of the printed decimal.  The same records can therefore be written as a `.z` file for
+the reference program and uploaded to the GPU path bit-identically.
+"""
+import ctypes
+import ctypes.util
+import math
+
+import numpy as np
+
+KBOLT = 1.380649e-16
+AMU = 1.66053906660e-24
+SEED0 = 20261203
+
+_libm = ctypes.CDLL(ctypes.util.find_library("m") or "libm.so.6")
+_libm.powf.restype = ctypes.c_float
+_libm.powf.argtypes = [ctypes.c_float, ctypes.c_float]
+
+
+def pow10f(x):
+    """Single-precision 10.0**x as the reference's REAL(4) exponentiation (libm powf)."""
+    x = np.asarray(x, dtype=np.float32)
+    out = np.empty(x.shape, np.float32)
+    flat = x.ravel(); o = out.ravel()
+    pw = _libm.powf
+    for i in range(flat.size):
+        o[i] = pw(10.0, float(flat[i]))
+    return out
+
+
+def f32_of_text(values, fmt):
+    """FP32 value the reference parses from each number printed with `fmt`."""
+    return np.array([np.float32(fmt % v) for v in np.asarray(values, dtype=np.float64)], np.float32)
+
+
+# ---- model atmospheres ------------------------------------------------------------------------
+
+# Asplund et al. (2021) log(N_el/N_tot) pattern of the reference (shared.f90:72-90), first 30
+SOLAR30 = [0.923, -1.121, -11.07, -10.65, -9.33, -3.57, -4.20, -3.34, -7.63, -3.97, -5.81,
+           -4.48, -5.60, -4.52, -6.62, -4.91, -6.72, -5.65, -6.96, -5.73, -8.89, -7.06, -8.13,
+           -6.41, -6.61, -4.57, -7.09, -5.83, -7.85, -7.47]
+
+
+def eddington_model(teff, logg, ntau, logtau_min=-5.0, logtau_max=2.0, metal=1e-4):
+    """Eddington-grey plane-parallel model in hydrostatic equilibrium.
+
+    T^4 = 3/4 Teff^4 (tau + 2/3) on a log tau grid.  dP/dtau = g / kappa with an H-minus
+    bound-free opacity fit, kappa = 2.5e-31 (rho^0.5) T^9 cm^2/g for T <= 6000 K continued
+    as T^3 above it, plus electron scattering; the fit only shapes P(tau) for this synthetic
+    model (the reference re-solves the equation of state from Pgas = (Xna + Xne) k T).
+    The electron density is a Saha estimate for hydrogen plus a metal donor of ionisation
+    potential 7.9 eV at relative abundance `metal`.
+    """
+    g = 10.0 ** logg
+    lt = np.linspace(logtau_min, logtau_max, ntau)
+    tau = 10.0 ** lt
+    T = (0.75 * teff ** 4 * (tau + 2.0 / 3.0)) ** 0.25
+    mu = 1.3
+
+    def kappa(P, T):
+        rho = P * mu * AMU / (KBOLT * T)
+        Tt = min(T, 6000.0)
+        k = 2.5e-31 * math.sqrt(max(rho, 1e-30)) * Tt ** 9
+        if T > 6000.0:
+            k *= (T / 6000.0) ** 3
+        return k + 0.03 + 1e-4
+
+    # integrate d ln P / d ln tau = g tau / (kappa P) from a self-consistent top boundary
+    P = g * tau[0] / 1.0
+    for _ in range(50):
+        P = g * tau[0] / kappa(P, T[0])
+    Ps = [P]
+    for i in range(1, ntau):
+        x0, x1 = math.log(tau[i - 1]), math.log(tau[i])
+        h = (x1 - x0) / 8.0
+        y = math.log(Ps[-1])
+        Tl = lambda x: (0.75 * teff ** 4 * (math.exp(x) + 2.0 / 3.0)) ** 0.25
+        f = lambda x, y: g * math.exp(x) / (kappa(math.exp(y), Tl(x)) * math.exp(y))
+        x = x0
+        for _ in range(8):
+            k1 = f(x, y); k2 = f(x + h / 2, y + h * k1 / 2); k3 = f(x + h / 2, y + h * k2 / 2)
+            k4 = f(x + h, y + h * k3)
+            y += h * (k1 + 2 * k2 + 2 * k3 + k4) / 6.0
+            x += h
+        Ps.append(math.exp(y))
+    Pg = np.array(Ps)
+    ntot = Pg / (KBOLT * T)
+    # Saha electron density: hydrogen (13.6 eV) + metal donor (7.9 eV)
+    xne = np.empty(ntau)
+    for i in range(ntau):
+        ne = 1e10
+        for _ in range(200):
+            def phi(chi, u):
+                return 2.4148e15 * T[i] ** 1.5 * math.exp(-chi * 11604.518 / T[i]) * u
+            fH = phi(13.598, 1.0) / (phi(13.598, 1.0) + ne)
+            fM = phi(7.9, 1.0) / (phi(7.9, 1.0) + ne)
+            nh = 0.92 * ntot[i]
+            new = nh * fH + metal * ntot[i] * fM
+            if abs(new - ne) <= 1e-10 * ne:
+                ne = new
+                break
+            ne = math.sqrt(ne * max(new, 1.0))
+        xne[i] = ne
+    xna = ntot - xne
+    rho = xna * mu * AMU
+    rhox = Pg / g
+    return dict(teff=float(teff), logg=float(logg), ntau=ntau, logtau=lt, rhox=rhox, T=T,
+                xne=xne, xna=xna, rho=rho)
+
+
+def write_krz(path, model, abund=None, title="synthetic Eddington-grey model"):
+    """Write a plane-parallel `.krz` model (the format ReadModel parses, ioutils.f90:1614-1748)."""
+    ab = list(abund if abund is not None else SOLAR30) + [-20.0] * (99 - len(SOLAR30))
+    with open(path, "w") as f:
+        f.write("TITLE %s\n" % title)
+        f.write("T EFF= %.0f. GRAV= %.2f  MODEL TYPE= 0 WLSTD= 5000 PLANE-PARALLEL.\n"
+                % (model["teff"], model["logg"]))
+        f.write(" 1 1 1 1 1 1 1 1 1 1 1 1 1 0 1 0 0 0 0 0 - OPACITY SWITCHES\n")
+        for i in range(0, 99, 10):
+            f.write(" ".join("%7.3f" % a for a in ab[i:i + 10]))
+            f.write(" %d\n" % model["ntau"] if i + 10 >= 99 else "\n")
+        for i in range(model["ntau"]):
+            f.write(" %.9E, %8.1f, %.6E, %.6E, %.6E,\n" % (
+                model["rhox"][i], model["T"][i], model["xne"][i], model["xna"][i], model["rho"][i]))
+
+
+# ---- line lists ------------------------------------------------------------------------------
+
+# species tables: (name, ion, atomic/molecular mass) in the order their indices are used
+ATOMIC_C0 = [("Fe", 1), ("Fe", 2), ("Ti", 1), ("Cr", 1), ("Ni", 1), ("Ca", 1)]
+ATOMIC_C0_P = [0.5, 0.1, 0.1, 0.1, 0.1, 0.1]
+MOLECULES_C1 = [("TiO", 1), ("H2O", 1), ("CO", 1), ("OH", 1)]
+
+
+class LineList:
+    """SoA line list with the reference's stored FP32 fields.
+
+    wl (f8), elo/gf/grad/gqst/gvdw (f4, linear as stored), spc (species index into
+    `species`), ismol, and the printed log values used to write the ASCII file.
+    Zeeman components (optional): npi, nsi (int), comp arrays CSR by line.
+    """
+
+    def __init__(self, species, wl, loggf, elo, lgrad, lgqst, lgvdw, spc, ismol, zeeman=None):
+        self.species = species
+        order = np.argsort(wl, kind="stable")
+        self.wl = np.asarray(wl, np.float64)[order]
+        self._txt = dict(loggf=np.asarray(loggf)[order], elo=np.asarray(elo)[order],
+                         lgrad=np.asarray(lgrad)[order], lgqst=np.asarray(lgqst)[order],
+                         lgvdw=np.asarray(lgvdw)[order])
+        self.spc = np.asarray(spc, np.int32)[order]
+        self.ismol = np.asarray(ismol, np.int32)[order]
+        t = self._txt
+        self.elo = f32_of_text(t["elo"], "%.4f")
+        self.gf = pow10f(f32_of_text(t["loggf"], "%.3f"))
+        lg = f32_of_text(t["lgrad"], "%.3f")
+        self.grad = np.where((lg < 20.0) & (lg > 0.0), pow10f(lg), lg).astype(np.float32)
+        lq = f32_of_text(t["lgqst"], "%.3f")
+        self.gqst = np.where(lq < 0.0, pow10f(lq), lq).astype(np.float32)
+        lv = f32_of_text(t["lgvdw"], "%.3f")
+        self.gvdw = np.where(lv < 0.0, pow10f(lv), lv).astype(np.float32)
+        self.zeeman = None
+        if zeeman is not None:
+            jlo, jup, glo, gup = (np.asarray(a)[order] for a in zeeman)
+            self.zeeman = (jlo, jup, glo, gup)
+        self.n = len(self.wl)
+
+    def write_z(self, path, wstart, wend, patterns=None):
+        """ASCII list in the VALD-short / .z layout parsed by ReadAscMag (ioutils.f90:1194-1571).
+
+        patterns: per-line (spi, rpi, ssig_half, rsig_half) Zeeman blocks written after a
+        Lande factor below -10, with the sigma block holding the red half (ioutils.f90:1324-1410).
+        """
+        t = self._txt
+        with open(path, "w") as f:
+            f.write(" %.5f, %.5f, %d, %d, 1.0, Wavelength region, lines selected, lines processed, Vmicro\n"
+                    % (wstart, wend, self.n, self.n))
+            f.write("                                                   Damping parameters    Lande  Central\n")
+            f.write(" Spec Ion       WL(A)   Excit(eV) Vmic  log gf*   Rad.   Stark  Waals  factor  depth  Reference\n")
+            for i in range(self.n):
+                nm, ion = self.species[self.spc[i]]
+                lande = -99.0 if patterns is not None else 99.0
+                f.write("'%s %d',%18.10f,%9.4f, 1.0,%8.3f,%8.3f,%8.3f,%8.3f,%8.3f, 0.500, 'syn'\n"
+                        % (nm, ion, self.wl[i], t["elo"][i], t["loggf"][i], t["lgrad"][i],
+                           t["lgqst"][i], t["lgvdw"][i], lande))
+                if patterns is not None:
+                    spi, rpi, ssh, rsh = patterns[i]
+                    f.write("%d %s\n" % (len(spi), " ".join("%.9g" % x for x in spi)))
+                    f.write("%s\n" % " ".join("%.9g" % x for x in rpi))
+                    f.write("%d %s\n" % (len(ssh), " ".join("%.9g" % x for x in ssh)))
+                    f.write("%s\n" % " ".join("%.9g" % x for x in rsh))
+            f.write("'References:'\n")
+
+    def arrays(self):
+        return dict(wl=self.wl, elo=self.elo, gf=self.gf, grad=self.grad, gqst=self.gqst,
+                    gvdw=self.gvdw, spc=self.spc, ismol=self.ismol)
+
+
+def atomic_lines(n, wmin, wmax, seed, species=ATOMIC_C0, probs=ATOMIC_C0_P):
+    """Config-0 distributions: lambda0 ~ U, species mix, log gf ~ N(-2, 1.2) clipped [-6, 1],
+    E_low ~ U(0, 6) eV, log Grad ~ U(7, 9), log G4/Ne ~ U(-7, -4), log G6/NH ~ U(-8, -7)."""
+    rng = np.random.default_rng(seed)
+    wl = rng.uniform(wmin, wmax, n)
+    spc = rng.choice(len(species), size=n, p=probs)
+    loggf = np.clip(rng.normal(-2.0, 1.2, n), -6.0, 1.0)
+    elo = rng.uniform(0.0, 6.0, n)
+    lgrad = rng.uniform(7.0, 9.0, n)
+    lgqst = rng.uniform(-7.0, -4.0, n)
+    lgvdw = rng.uniform(-8.0, -7.0, n)
+    return LineList(species, wl, loggf, elo, lgrad, lgqst, lgvdw, spc, np.zeros(n, np.int32))
+
+
+def molecular_lines(n, wmin, wmax, seed, species=MOLECULES_C1):
+    """Config-1 distributions: wavenumber uniform over [1e8/wmax, 1e8/wmin] cm^-1 (lambda in A),
+    four species at 25 % each, log gf ~ N(-5, 1.5), E_low ~ Exp(1 eV) capped at 5 eV,
+    log G6/NH ~ U(-8, -7), radiative damping from the classical fallback (Grad = 0)."""
+    rng = np.random.default_rng(seed)
+    sigma = rng.uniform(1e8 / wmax, 1e8 / wmin, n)
+    wl = 1e8 / sigma
+    spc = rng.integers(0, len(species), n)
+    loggf = rng.normal(-5.0, 1.5, n)
+    elo = np.minimum(rng.exponential(1.0, n), 5.0)
+    lgvdw = rng.uniform(-8.0, -7.0, n)
+    z = np.zeros(n)
+    return LineList(species, wl, loggf, elo, z, z, lgvdw, spc, np.ones(n, np.int32))
+
+
+def zeeman_lines(n, wmin, wmax, seed):
+    """Config-2: config-0 parameters plus Lande g_up, g_lo ~ U(0, 2.5) and J in {0..4} with
+    Delta J in {-1, 0, 1}, excluding 0 -> 0."""
+    L = atomic_lines(n, wmin, wmax, seed)
+    rng = np.random.default_rng(seed + 1000)
+    jlo = rng.integers(0, 5, n).astype(np.float64)
+    dj = rng.integers(-1, 2, n)
+    jup = np.clip(jlo + dj, 0, 4)
+    bad = (jlo == 0) & (jup == 0)
+    jup[bad] = 1.0
+    glo = rng.uniform(0.0, 2.5, n)
+    gup = rng.uniform(0.0, 2.5, n)
+    L.zeeman = (f32_of_text(jlo, "%.1f"), f32_of_text(jup, "%.1f"),
+                f32_of_text(glo, "%.3f"), f32_of_text(gup, "%.3f"))
+    return L

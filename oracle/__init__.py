@@ -1,0 +1,365 @@
+"""ctypes binding of the CPU FP64 oracle (oracle/fs_oracle.c).
+
+TEST INFRASTRUCTURE ONLY.  The oracle restates the reference's Fortran algorithms
+(voigt.f90, opacity.f90, solver.f90, synth.f90 drivers, convol.f90, utils.f90 quadrature)
+operation by operation.  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline /
+reference arm may import this module, and only to check or to time a CPU baseline -- the
+product (fastspec_b200) never calls it.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libfsoracle.so")
+_lib = None
+
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int)
+_lp = C.POINTER(C.c_long)
+
+
+class _State(C.Structure):
+    _fields_ = [
+        ("wmode", C.c_int), ("wstart", C.c_double), ("wend", C.c_double), ("dstep", C.c_double),
+        ("nwl", C.c_int), ("wave", _dp), ("wfirst", C.c_double), ("wlast", C.c_double),
+        ("rstep", C.c_double),
+        ("ntau", C.c_int), ("rhox", _dp), ("T", _dp), ("xne", _dp), ("xna", _dp), ("rho", _dp),
+        ("height", _dp),
+        ("nspc", C.c_int), ("fractionpf", _fp), ("xamass", _fp), ("potion", _fp), ("ion", _ip),
+        ("frac_h1", _fp), ("frac_he1", _fp), ("frac_h2", _fp), ("spc_he1", C.c_int),
+        ("contopac", _dp), ("contopac_std", _dp), ("motype", C.c_int),
+        ("nhe", C.c_int), ("hegam", _dp), ("heshf", _dp),
+        ("vmicro", C.c_double), ("epsopac", C.c_double), ("vwfudge", C.c_double),
+        ("h2brd", C.c_double), ("vwmol", C.c_double), ("molbrd", C.c_int),
+        ("x_nprtb", _dp), ("x_gvwprt", _dp), ("x_temp6", _dp), ("x_temp3", _dp), ("x_kbt", _dp),
+        ("x_kbet", _dp), ("x_vturb2", C.c_double),
+    ]
+
+
+class _Lines(C.Structure):
+    _fields_ = [
+        ("n", C.c_long), ("wl", _dp), ("elo", _fp), ("gf", _fp), ("grad", _fp), ("gqst", _fp),
+        ("gvdw", _fp), ("spc", _ip), ("kind", _ip), ("ismol", _ip), ("ihe", _ip),
+        ("npi", _ip), ("nsi", _ip), ("pi_off", _lp), ("si_off", _lp),
+        ("spl_pi", _fp), ("str_pi", _fp), ("spl_si", _fp), ("str_si", _fp),
+    ]
+
+
+class _Stats(C.Structure):
+    _fields_ = [("nlines_in", C.c_long), ("nlines_used", C.c_long), ("nwide", C.c_long),
+                ("nweak", C.c_long), ("nsegments", C.c_long), ("nrefills", C.c_long),
+                ("line_evals", C.c_double), ("wide_evals", C.c_double)]
+
+
+def build():
+    """Compile oracle/libfsoracle.so with its Makefile (gcc, OpenMP, -ffp-contract=off)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        L.or_hvoigt_exact.restype = C.c_double
+        L.or_hvoigt_exact.argtypes = [C.c_double, C.c_double]
+        L.or_wvoigt_exact.argtypes = [C.c_double, C.c_double, _dp, _dp]
+        L.or_hvoigt.restype = C.c_double
+        L.or_hvoigt.argtypes = [C.c_double, C.c_double]
+        L.or_fvoigt.argtypes = [C.c_double, C.c_double, _dp, _dp]
+        L.or_voigt_table.restype = _fp
+        L.or_fvoigt_table.restype = _fp
+        L.or_grid_init.argtypes = [C.POINTER(_State)]
+        L.or_xline_init.argtypes = [C.POINTER(_State)]
+        L.or_state_free.argtypes = [C.POINTER(_State)]
+        L.or_waveidx.argtypes = [C.POINTER(_State), C.c_double]
+        L.or_air2vac.restype = C.c_double
+        L.or_air2vac.argtypes = [C.c_double]
+        L.or_xline.argtypes = [C.POINTER(_State), C.POINTER(_Lines), C.c_long, _dp, _dp, _dp]
+        L.or_lineop_calc.argtypes = [C.POINTER(_State), C.POINTER(_Lines), C.c_int, C.c_long, _dp,
+                                     _ip, _ip, _ip, _fp, C.c_int, _dp, _dp, C.POINTER(_Stats)]
+        L.or_mag_lineop_calc.argtypes = [C.POINTER(_State), C.POINTER(_Lines), C.c_int, _dp,
+                                         C.c_long, _dp, _ip, _ip, _ip, _fp, C.c_int, _dp, _dp,
+                                         C.POINTER(_Stats)]
+        L.or_locprf_pp.argtypes = [_dp, _dp, C.c_int, _dp, _dp, _dp, C.c_int]
+        L.or_solve4x4.argtypes = [_dp, _dp, _dp]
+        L.or_radtran.argtypes = [C.POINTER(_State), C.c_int, _dp, _dp, _dp, _dp]
+        L.or_mag_radtran.argtypes = [C.POINTER(_State), C.c_int, _dp, C.c_int, _dp, _dp, _dp, _dp, _dp]
+        L.or_mu_quadrature.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, C.c_int]
+        L.or_gauss_mu.argtypes = [C.c_int, C.c_int, _dp, _dp]
+        L.or_disk_integ.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp]
+        L.or_zeeman_pattern.argtypes = [C.c_float, C.c_float, C.c_float, C.c_float, _ip, _fp, _fp,
+                                        _ip, _fp, _fp]
+        _lib = L
+    return _lib
+
+
+def _p(a, ct):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(ct))
+
+
+def _f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _f32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _i32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.int32)
+
+
+# ---- Voigt ------------------------------------------------------------------------------
+
+def hvoigt_exact(a, v):
+    return lib().or_hvoigt_exact(float(a), float(v))
+
+
+def wvoigt_exact(a, v):
+    re, im = C.c_double(), C.c_double()
+    lib().or_wvoigt_exact(float(a), float(v), C.byref(re), C.byref(im))
+    return re.value + 1j * im.value
+
+
+def hvoigt(a, v):
+    return lib().or_hvoigt(float(a), float(v))
+
+
+def fvoigt(a, v):
+    h, l = C.c_double(), C.c_double()
+    lib().or_fvoigt(float(a), float(v), C.byref(h), C.byref(l))
+    return h.value, l.value
+
+
+def voigt_table():
+    """VgtTab as float32 [402][1002] (row = a node, column = v node)."""
+    p = lib().or_voigt_table()
+    return np.ctypeslib.as_array(p, shape=(402 * 1002,)).reshape(402, 1002).copy()
+
+
+def fvoigt_table():
+    """FvTab as float32 [402][1002][2] (H, L)."""
+    p = lib().or_fvoigt_table()
+    return np.ctypeslib.as_array(p, shape=(402 * 1002 * 2,)).reshape(402, 1002, 2).copy()
+
+
+# ---- state --------------------------------------------------------------------------------
+
+class State:
+    """One atmosphere + grid + configuration, as consumed by the hot path.
+
+    atm: dict with rhox, T, xne, xna, rho (FP64 [ntau]); species: fractionpf (FP32 [ntau][nspc]),
+    xamass, potion (FP32 [nspc]), ion (int [nspc]); frac_h1/frac_he1/frac_h2 (FP32 [ntau]);
+    contopac (FP64 [nwl][ntau]); grid: wmode, wstart, wend, dstep.
+    """
+
+    def __init__(self, grid, atm, contopac=None, contopac_std=None, motype=0, vmicro=0.0,
+                 epsopac=1e-4, vwfudge=1.0, h2brd=0.0, vwmol=0.0, molbrd=0, hegam=None,
+                 heshf=None, spc_he1=-1):
+        L = lib()
+        s = _State()
+        s.wmode = int(grid["wmode"]); s.wstart = float(grid["wstart"])
+        s.wend = float(grid["wend"]); s.dstep = float(grid["dstep"])
+        nwl = L.or_grid_init(C.byref(s))
+        if nwl < 2:
+            raise ValueError("grid has fewer than two points")
+        self._keep = {}
+        k = self._keep
+        for name in ("rhox", "T", "xne", "xna", "rho"):
+            k[name] = _f64(atm[name])
+            setattr(s, name, _p(k[name], C.c_double))
+        s.ntau = len(k["T"])
+        k["fractionpf"] = _f32(atm["fractionpf"])
+        s.nspc = k["fractionpf"].shape[1]
+        s.fractionpf = _p(k["fractionpf"], C.c_float)
+        for name in ("xamass", "potion", "frac_h1", "frac_he1", "frac_h2"):
+            k[name] = _f32(atm[name])
+            setattr(s, name, _p(k[name], C.c_float))
+        k["ion"] = _i32(atm["ion"]); s.ion = _p(k["ion"], C.c_int)
+        s.spc_he1 = int(spc_he1)
+        if contopac is not None:
+            k["contopac"] = _f64(contopac)
+            if k["contopac"].shape != (nwl, s.ntau):
+                raise ValueError("contopac shape %s != (%d, %d)" % (k["contopac"].shape, nwl, s.ntau))
+            s.contopac = _p(k["contopac"], C.c_double)
+        if contopac_std is not None:
+            k["contopac_std"] = _f64(contopac_std); s.contopac_std = _p(k["contopac_std"], C.c_double)
+        s.motype = int(motype)
+        if hegam is not None:
+            k["hegam"] = _f64(hegam); k["heshf"] = _f64(heshf)
+            s.nhe = k["hegam"].shape[0]
+            s.hegam = _p(k["hegam"], C.c_double); s.heshf = _p(k["heshf"], C.c_double)
+        s.vmicro = vmicro; s.epsopac = epsopac; s.vwfudge = vwfudge; s.h2brd = h2brd
+        s.vwmol = vwmol; s.molbrd = int(molbrd)
+        L.or_xline_init(C.byref(s))
+        self.s = s
+        self.nwl = nwl
+        self.ntau = s.ntau
+
+    @property
+    def wave(self):
+        return np.ctypeslib.as_array(self.s.wave, shape=(self.nwl,)).copy()
+
+    @property
+    def wfirst(self):
+        return self.s.wfirst
+
+    def waveidx(self, w):
+        return lib().or_waveidx(C.byref(self.s), float(w))
+
+    def xline_init_arrays(self):
+        n = self.ntau
+        g = lambda p: np.ctypeslib.as_array(p, shape=(n,)).copy()
+        return dict(nprtb=g(self.s.x_nprtb), gvwprt=g(self.s.x_gvwprt), temp6=g(self.s.x_temp6),
+                    temp3=g(self.s.x_temp3), kbt=g(self.s.x_kbt), kbet=g(self.s.x_kbet),
+                    vturb2=self.s.x_vturb2)
+
+    def __del__(self):
+        try:
+            lib().or_state_free(C.byref(self.s))
+        except Exception:
+            pass
+
+
+class Lines:
+    """SoA line list.  kind: 0 atomic, 1 molecular, 2 magnetic/ASCII record."""
+
+    def __init__(self, wl, elo, gf, grad, gqst, gvdw, spc, kind=2, ismol=None, ihe=None,
+                 zeeman=None):
+        n = len(wl)
+        k = self._keep = {}
+        L = _Lines()
+        L.n = n
+        k["wl"] = _f64(wl); L.wl = _p(k["wl"], C.c_double)
+        for name, arr in (("elo", elo), ("gf", gf), ("grad", grad), ("gqst", gqst), ("gvdw", gvdw)):
+            k[name] = _f32(arr); setattr(L, name, _p(k[name], C.c_float))
+        k["spc"] = _i32(spc); L.spc = _p(k["spc"], C.c_int)
+        k["kind"] = _i32(np.broadcast_to(np.asarray(kind, dtype=np.int32), (n,)))
+        L.kind = _p(k["kind"], C.c_int)
+        if ismol is not None:
+            k["ismol"] = _i32(ismol); L.ismol = _p(k["ismol"], C.c_int)
+        if ihe is not None:
+            k["ihe"] = _i32(ihe); L.ihe = _p(k["ihe"], C.c_int)
+        if zeeman is not None:
+            npi, nsi, spl_pi, str_pi, spl_si, str_si = zeeman
+            k["npi"] = _i32(npi); k["nsi"] = _i32(nsi)
+            k["pi_off"] = np.ascontiguousarray(np.concatenate([[0], np.cumsum(k["npi"])[:-1]]), dtype=np.int64)
+            k["si_off"] = np.ascontiguousarray(np.concatenate([[0], np.cumsum(k["nsi"])[:-1]]), dtype=np.int64)
+            for name, arr in (("spl_pi", spl_pi), ("str_pi", str_pi), ("spl_si", spl_si), ("str_si", str_si)):
+                k[name] = _f32(arr if len(arr) else np.zeros(1, np.float32))
+                setattr(L, name, _p(k[name], C.c_float))
+            L.npi = _p(k["npi"], C.c_int); L.nsi = _p(k["nsi"], C.c_int)
+            L.pi_off = _p(k["pi_off"], C.c_long); L.si_off = _p(k["si_off"], C.c_long)
+        self.L = L
+        self.n = n
+
+
+def xline(state, lines, i):
+    n = state.ntau
+    cop, vv, av = (np.zeros(n) for _ in range(3))
+    lib().or_xline(C.byref(state.s), C.byref(lines.L), int(i), _p(cop, C.c_double),
+                   _p(vv, C.c_double), _p(av, C.c_double))
+    return cop, vv, av
+
+
+def lineop_calc(state, lines, list_type=2, nlines_lim=0, lineopac=None, nmu=0, xmu=None, wmu=None,
+                want_linstr=False):
+    """LineopCalc.  Returns dict(lineopac [nwl][ntau], flags, ileft, iright, stats, linstr)."""
+    n = lines.n
+    lo = np.zeros((state.nwl, state.ntau)) if lineopac is None else lineopac
+    flags = np.zeros(max(n, 1), np.int32); il = np.zeros(max(n, 1), np.int32)
+    ir = np.zeros(max(n, 1), np.int32)
+    ls = np.zeros(max(n, 1), np.float32) if want_linstr else None
+    st = _Stats()
+    xmu = _f64(xmu); wmu = _f64(wmu)
+    rc = lib().or_lineop_calc(C.byref(state.s), C.byref(lines.L), int(list_type), int(nlines_lim),
+                              _p(lo, C.c_double), _p(flags, C.c_int), _p(il, C.c_int), _p(ir, C.c_int),
+                              _p(ls, C.c_float), int(nmu), _p(xmu, C.c_double), _p(wmu, C.c_double),
+                              C.byref(st))
+    if rc != 0:
+        raise RuntimeError("or_lineop_calc failed: %d" % rc)
+    return dict(lineopac=lo, flags=flags[:n], ileft=il[:n], iright=ir[:n], linstr=None if ls is None else ls[:n],
+                stats={f: getattr(st, f) for f, _ in _Stats._fields_})
+
+
+def mag_lineop_calc(state, lines, bframe, bfield, nlines_lim=0, nmu=0, xmu=None, wmu=None,
+                    want_linstr=False):
+    n = lines.n
+    mlo = np.zeros((state.nwl, state.ntau, 6))
+    flags = np.zeros(max(n, 1), np.int32); il = np.zeros(max(n, 1), np.int32)
+    ir = np.zeros(max(n, 1), np.int32)
+    ls = np.zeros(max(n, 1), np.float32) if want_linstr else None
+    st = _Stats()
+    bf = _f64(bfield); xmu = _f64(xmu); wmu = _f64(wmu)
+    rc = lib().or_mag_lineop_calc(C.byref(state.s), C.byref(lines.L), int(bframe), _p(bf, C.c_double),
+                                  int(nlines_lim), _p(mlo, C.c_double), _p(flags, C.c_int),
+                                  _p(il, C.c_int), _p(ir, C.c_int), _p(ls, C.c_float), int(nmu),
+                                  _p(xmu, C.c_double), _p(wmu, C.c_double), C.byref(st))
+    if rc != 0:
+        raise RuntimeError("or_mag_lineop_calc failed: %d" % rc)
+    return dict(maglineopac=mlo, flags=flags[:n], ileft=il[:n], iright=ir[:n],
+                linstr=None if ls is None else ls[:n],
+                stats={f: getattr(st, f) for f, _ in _Stats._fields_})
+
+
+def radtran(state, xmu, lineopac, want_spc=True):
+    xmu = _f64(xmu); nmu = len(xmu)
+    lo = _f64(lineopac)
+    spl = np.zeros((state.nwl, nmu)); spc = np.zeros((state.nwl, nmu)) if want_spc else None
+    lib().or_radtran(C.byref(state.s), nmu, _p(xmu, C.c_double), _p(lo, C.c_double),
+                     _p(spl, C.c_double), _p(spc, C.c_double))
+    return spl, spc
+
+
+def mag_radtran(state, xmu, bframe, bfield, lineopac, maglineopac):
+    xmu = _f64(xmu); nmu = len(xmu)
+    bf = _f64(bfield); lo = _f64(lineopac); mlo = _f64(maglineopac)
+    spz = np.zeros((state.nwl, 4, nmu)); spc = np.zeros((state.nwl, nmu))
+    lib().or_mag_radtran(C.byref(state.s), nmu, _p(xmu, C.c_double), int(bframe), _p(bf, C.c_double),
+                         _p(lo, C.c_double), _p(mlo, C.c_double), _p(spz, C.c_double), _p(spc, C.c_double))
+    return spz, spc
+
+
+def locprf_pp(xmu, xki, src, rhox):
+    xmu = _f64(xmu); xki = _f64(xki); src = _f64(src); rhox = _f64(rhox)
+    out = np.zeros(len(xmu))
+    lib().or_locprf_pp(_p(out, C.c_double), _p(xmu, C.c_double), len(xmu), _p(xki, C.c_double),
+                       _p(src, C.c_double), _p(rhox, C.c_double), len(xki))
+    return out
+
+
+def mu_quadrature(quad, n, x=None):
+    setnodes = x is None
+    x = np.zeros(n) if x is None else _f64(x).copy()
+    w = np.zeros(n); r = np.zeros(n + 1)
+    rc = lib().or_mu_quadrature(int(quad), int(n), _p(x, C.c_double), _p(w, C.c_double),
+                                _p(r, C.c_double), int(setnodes))
+    if rc != 0:
+        raise ValueError("unknown quadrature %d" % quad)
+    return x, w, r
+
+
+def disk_integ(wmu, spl, spc):
+    wmu = _f64(wmu); spl = _f64(spl); spc = _f64(spc)
+    nwl, nmu = spl.shape
+    sfl = np.zeros(nwl); sfc = np.zeros(nwl)
+    lib().or_disk_integ(nmu, nwl, _p(wmu, C.c_double), _p(spl, C.c_double), _p(spc, C.c_double),
+                        _p(sfl, C.c_double), _p(sfc, C.c_double))
+    return sfl, sfc
+
+
+def zeeman_pattern(jlo, jup, glo, gup):
+    m = int(round(2 * jup)) + 1
+    npi, nsi = C.c_int(), C.c_int()
+    spi, rpi, ssi, rsi = (np.zeros(max(m, 1), np.float32) for _ in range(4))
+    lib().or_zeeman_pattern(jlo, jup, glo, gup, C.byref(npi), _p(spi, C.c_float), _p(rpi, C.c_float),
+                            C.byref(nsi), _p(ssi, C.c_float), _p(rsi, C.c_float))
+    return spi[:npi.value], rpi[:npi.value], ssi[:nsi.value], rsi[:nsi.value]

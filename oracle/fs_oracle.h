@@ -1,0 +1,152 @@
+/*
+ * fs_oracle.h -- CPU FP64 restatement of FastSpec's line-opacity -> formal-solver path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the parity checker for the CUDA product in
+ * fastspec_b200/.  Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline /
+ * reference arm may load it, and only as the checker or as the timed CPU baseline, never
+ * as a code path of the product.
+ *
+ * Every routine restates the reference algorithm operation by operation (same operand order,
+ * FP64, no FMA contraction: build with -ffp-contract=off) and cites the reference file:line
+ * it follows.  Arrays use the reference's Fortran column-major layouts seen from C:
+ *   LineOpac(Ntau,Nwl)        -> double[nwl][ntau]
+ *   MagLineOpac(6,Ntau,Nwl)   -> double[nwl][ntau][6]
+ *   SpL/SpC(Nmu,Nwl)          -> double[nwl][nmu]
+ *   SpZ(Nmu,4,Nwl)            -> double[nwl][4][nmu]
+ *   FractionPF(Maxspl,Ntau)   -> float[ntau][nspc]     (species fastest, FP32 as the EOS)
+ * Line and wavelength indices on this interface are 1-based, as in the reference.
+ */
+#ifndef FS_ORACLE_H
+#define FS_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- Voigt / Faraday-Voigt (voigt.f90) ------------------------------------------------ */
+void   or_voigt_init(void);                                   /* VoigtInit  voigt.f90:42-72   */
+void   or_fvoigt_init(void);                                  /* FVoigtInit voigt.f90:219-251 */
+double or_hvoigt_exact(double a, double v);                   /* voigt.f90:158-187 */
+void   or_wvoigt_exact(double a, double v, double *re, double *im); /* voigt.f90:356-393 */
+double or_hvoigt(double a, double v);                         /* voigt.f90:76-110 */
+void   or_fvoigt(double a, double v, double *vgt, double *fvgt);    /* voigt.f90:256-299 */
+const float *or_voigt_table(void);    /* VgtTab(NVv+1,NVa+1), v fastest: 1002 x 402 */
+const float *or_fvoigt_table(void);   /* FvTab(2,NVv+1,NVa+1): 2 x 1002 x 402 */
+
+/* ---- Physical state of one atmosphere (host inputs of the hot path) ------------------- */
+typedef struct {
+    /* wavelength grid (synth.f90:56-74) */
+    int     wmode;          /* 0: uniform in lambda, 1: uniform in ln lambda */
+    double  wstart, wend, dstep;
+    int     nwl;
+    double *wave;           /* [nwl] offsets from wfirst (filled by or_grid_init) */
+    double  wfirst, wlast, rstep;
+
+    /* model atmosphere after the EOS (shared.f90:514-534) */
+    int     ntau;
+    const double *rhox, *T, *xne, *xna, *rho, *height;
+    int     nspc;
+    const float *fractionpf;   /* [ntau][nspc] */
+    const float *xamass;       /* [nspc] */
+    const float *potion;       /* [nspc] */
+    const int   *ion;          /* [nspc] ionization stage (1 = neutral) */
+    const float *frac_h1, *frac_he1, *frac_h2;   /* [ntau] number densities (Fraction) */
+    int     spc_he1;           /* species index (0-based) of He I for Stark tables, -1 none */
+
+    /* continuum opacity (ContopCalc output) */
+    const double *contopac;    /* [nwl][ntau] */
+    const double *contopac_std;/* [ntau] (Motype 1 only) */
+    int     motype;
+
+    /* He I Stark tables (hestark.f90), optional */
+    int     nhe;
+    const double *hegam, *heshf;   /* [nhe][ntau] */
+
+    /* configuration (shared.f90:416-443) */
+    double  vmicro, epsopac, vwfudge, h2brd, vwmol;
+    int     molbrd;
+
+    /* XlineInit state (opacity.f90:65-93) */
+    double *x_nprtb, *x_gvwprt, *x_temp6, *x_temp3, *x_kbt, *x_kbet;
+    double  x_vturb2;
+} or_state;
+
+/* ---- Line list (SoA; LineData records shared.f90:451-482) ----------------------------- */
+typedef struct {
+    long    n;
+    const double *wl;                     /* air wavelength [A], FP64 */
+    const float  *elo, *gf, *grad, *gqst, *gvdw;   /* FP32 as stored by the readers */
+    const int    *spc;                    /* species index 0-based */
+    const int    *kind;                   /* 0 LineTypeAtm, 1 LineTypeMol, 2 LineTypeMag */
+    const int    *ismol;                  /* molecule flag (LineTypeMag: bit 1) */
+    const int    *ihe;                    /* He I Stark table entry 1..nhe, 0 none */
+    /* Zeeman components (LineTypeMag), CSR: line i has npi[i] pi and nsi[i] sigma comps */
+    const int    *npi, *nsi;
+    const long   *pi_off, *si_off;
+    const float  *spl_pi, *str_pi, *spl_si, *str_si;
+} or_lines;
+
+typedef struct {
+    long nlines_in, nlines_used, nwide, nweak, nsegments, nrefills;
+    double line_evals;          /* Ntau * sum over retained non-wide lines of window length */
+    double wide_evals;
+} or_stats;
+
+int  or_grid_init(or_state *s);          /* allocates s->wave; returns nwl or <0 */
+void or_xline_init(or_state *s);         /* allocates x_* */
+void or_state_free(or_state *s);
+int  or_waveidx(const or_state *s, double wavein);   /* opacity.f90:594-608 */
+double or_air2vac(double lambda_air);                /* utils.f90:1020-1032 */
+
+/* per-line prefactors, all depths: XlineSetup + XlineDepth (opacity.f90:96-293) */
+void or_xline(const or_state *s, const or_lines *L, long iline0, double *lincop,
+              double *linvvgt, double *linavgt);
+
+/* LineopCalc (synth.f90:747-1095).  lineopac [nwl][ntau] is ACCUMULATED into.
+ * list_type 0 atomic HDF, 1 molecular HDF, 2 ASCII/.z (LineTypeMag).
+ * Per-line outputs (original order, may be NULL): flags, ileft, iright (1-based).
+ * linstr (may be NULL): central depths of retained lines (LinStrCalc), needs nmu/xmu/wmu. */
+int or_lineop_calc(const or_state *s, const or_lines *L, int list_type, long nlines_lim,
+                   double *lineopac, int *flags_out, int *ileft_out, int *iright_out,
+                   float *linstr_out, int nmu, const double *xmu, const double *wmu,
+                   or_stats *st);
+
+/* MagLineopCalc (synth.f90:1098-1455); maglineopac [nwl][ntau][6] accumulated. */
+int or_mag_lineop_calc(const or_state *s, const or_lines *L, int bframe, const double *bfield,
+                       long nlines_lim, double *maglineopac, int *flags_out, int *ileft_out,
+                       int *iright_out, float *linstr_out, int nmu, const double *xmu,
+                       const double *wmu, or_stats *st);
+
+/* Solver (solver.f90) */
+void or_taustep(const double *rhox, const double *xki, double xmu, int n, double *dtau);
+void or_centder(const double *dxx, const double *y, int m, int n, double *yp);
+void or_locprf_pp(double *ploc, const double *xmu, int nmu, const double *xki,
+                  const double *src, const double *rhox, int ntau);
+void or_solve4x4(const double *a /*[4][4] col-major*/, const double *b, double *x);
+
+/* RadTranCalc (synth.f90:1825-1901): spl/spc [nwl][nmu] */
+void or_radtran(const or_state *s, int nmu, const double *xmu, const double *lineopac,
+                double *spl, double *spc);
+/* MagRadTranCalc (synth.f90:1904-2012), plane-parallel: spz [nwl][4][nmu], spc [nwl][nmu] */
+void or_mag_radtran(const or_state *s, int nmu, const double *xmu, int bframe,
+                    const double *bfield, const double *lineopac, const double *maglineopac,
+                    double *spz, double *spc);
+
+/* Quadrature (utils.f90:1273-1431) and disk integration (convol.f90:67-246, no broadening) */
+int  or_mu_quadrature(int quad, int n, double *x, double *w, double *r, int setnodes);
+void or_gauss_mu(int quad, int n, double *x, double *w);
+void or_disk_integ(int nmu, int nwl, const double *wmu, const double *spl, const double *spc,
+                   double *sfl, double *sfc);
+
+/* ZeemanPattern (utils.f90:901-1004).  Outputs must hold 2*Jup+1 entries each. */
+void or_zeeman_pattern(float jlo, float jup, float glo, float gup, int *npi, float *spi,
+                       float *rpi, int *nsig, float *ssig, float *rsig);
+
+/* ZeemanPattern sigma mirroring of the .z reader (ioutils.f90:1393-1410) is done by callers. */
+
+#ifdef __cplusplus
+}
+#endif
+#endif
