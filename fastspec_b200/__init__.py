@@ -1,0 +1,370 @@
+"""fastspec_b200 -- B200-native line-opacity -> formal-solver path of FastSpec.
+
+The product is the sm_100a CUDA library libfastspec_b200.so behind the C-ABI in
+include/fastspec_gpu.h.  This module binds that ABI with ctypes and mirrors the reference's
+driver sequence (Init grid -> EOS state -> ContopCalc -> LineopCalc per list -> RadTranCalc ->
+DiskInteg, fastspec.f90:192-461).  There is no CPU fallback: every call fails loudly when the
+library is missing or no CUDA device is present.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfastspec_b200.so")
+
+PREC_MIXED = 0
+PREC_FP64 = 1
+F_WEAK, F_MOL, F_ABO, F_WIDE = 1, 2, 4, 8
+
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int32)
+_lp = C.POINTER(C.c_int64)
+
+
+class FsgError(RuntimeError):
+    pass
+
+
+class Config(C.Structure):
+    _fields_ = [("device", C.c_int), ("precision", C.c_int), ("vmicro", C.c_double),
+                ("epsopac", C.c_double), ("vwfudge", C.c_double), ("h2brd", C.c_double),
+                ("vwmol", C.c_double), ("molbrd", C.c_int), ("limitram_gb", C.c_double)]
+
+
+class CLines(C.Structure):
+    _fields_ = [("n", C.c_int64), ("wl", _dp), ("elo", _fp), ("gf", _fp), ("grad", _fp),
+                ("gqst", _fp), ("gvdw", _fp), ("spc", _ip), ("kind", C.c_int32), ("ismol", _ip),
+                ("ihe", _ip), ("npi", _ip), ("nsi", _ip), ("pi_off", _lp), ("si_off", _lp),
+                ("spl_pi", _fp), ("str_pi", _fp), ("spl_si", _fp), ("str_si", _fp)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("nlines_in", C.c_int64), ("nlines_used", C.c_int64), ("nwide", C.c_int64),
+                ("nweak", C.c_int64), ("nblocks", C.c_int64), ("line_evals", C.c_double),
+                ("ms_center", C.c_double), ("ms_params", C.c_double), ("ms_accum", C.c_double),
+                ("ms_total", C.c_double)]
+
+    def asdict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+# every symbol the header declares (checked by the CPU test suite)
+EXPORTS = [
+    "fsg_create", "fsg_destroy", "fsg_last_error", "fsg_version", "fsg_make_grid", "fsg_set_grid",
+    "fsg_set_atmosphere", "fsg_set_contopac", "fsg_set_contopac_dev", "fsg_set_hestark",
+    "fsg_lineop_calc", "fsg_lineop_calc_dev", "fsg_lineop_reset", "fsg_lineop_get", "fsg_lineop_set",
+    "fsg_lineop_device_ptr", "fsg_set_mu", "fsg_radtran", "fsg_radtran_dev", "fsg_mag_lineop_calc",
+    "fsg_mag_lineop_reset", "fsg_mag_radtran", "fsg_hvoigt", "fsg_fvoigt", "fsg_voigt_tables",
+    "fsg_locprf_pp", "fsg_mu_quadrature", "fsg_zeeman_pattern",
+]
+
+_lib = None
+
+
+def build_library(force=False):
+    """Compile libfastspec_b200.so for sm_100a (nvcc; see fastspec_b200/build.py)."""
+    import importlib
+    return importlib.import_module(__name__ + ".build").build(force=force)
+
+
+def lib():
+    """Load libfastspec_b200.so (raises FsgError when it is absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FsgError("libfastspec_b200.so not built: run python -m fastspec_b200.build")
+    L = C.CDLL(LIB_PATH)
+    L.fsg_create.argtypes = [C.POINTER(Config), C.POINTER(C.c_void_p)]
+    L.fsg_destroy.argtypes = [C.c_void_p]
+    L.fsg_destroy.restype = None
+    L.fsg_last_error.argtypes = [C.c_void_p]
+    L.fsg_last_error.restype = C.c_char_p
+    L.fsg_make_grid.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, _dp, C.POINTER(C.c_int)]
+    L.fsg_set_grid.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, _dp]
+    L.fsg_set_atmosphere.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_int, _fp, _fp, _fp,
+                                     _ip, _fp, _fp, _fp]
+    L.fsg_set_contopac.argtypes = [C.c_void_p, _dp, _dp, C.c_int]
+    L.fsg_set_contopac_dev.argtypes = [C.c_void_p, C.c_void_p]
+    L.fsg_set_hestark.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.c_int]
+    L.fsg_lineop_calc.argtypes = [C.c_void_p, C.POINTER(CLines), _dp, _ip, _ip, _ip, _fp, C.POINTER(Stats)]
+    L.fsg_lineop_calc_dev.argtypes = [C.c_void_p, C.POINTER(CLines), C.POINTER(Stats)]
+    L.fsg_lineop_reset.argtypes = [C.c_void_p]
+    L.fsg_lineop_get.argtypes = [C.c_void_p, _dp]
+    L.fsg_lineop_set.argtypes = [C.c_void_p, _dp]
+    L.fsg_lineop_device_ptr.argtypes = [C.c_void_p]
+    L.fsg_lineop_device_ptr.restype = C.c_void_p
+    L.fsg_set_mu.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
+    L.fsg_radtran.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
+    L.fsg_radtran_dev.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.fsg_mag_lineop_calc.argtypes = [C.c_void_p, C.POINTER(CLines), C.c_int, _dp, C.c_int, _dp, _ip, _ip,
+                                      _ip, _fp, C.POINTER(Stats)]
+    L.fsg_mag_lineop_reset.argtypes = [C.c_void_p]
+    L.fsg_mag_radtran.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int, _dp, _dp, _dp, _dp]
+    L.fsg_hvoigt.argtypes = [C.c_void_p, C.c_int64, _dp, _dp, _dp]
+    L.fsg_fvoigt.argtypes = [C.c_void_p, C.c_int64, _dp, _dp, _dp, _dp]
+    L.fsg_voigt_tables.argtypes = [C.c_void_p, _fp, _fp]
+    L.fsg_locprf_pp.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, C.c_int, _dp, _dp, _dp, _dp]
+    L.fsg_mu_quadrature.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, C.c_int]
+    L.fsg_zeeman_pattern.argtypes = [C.c_float, C.c_float, C.c_float, C.c_float, _ip, _fp, _fp, _ip, _fp, _fp]
+    _lib = L
+    return L
+
+
+def _p(a, ct):
+    return None if a is None else a.ctypes.data_as(C.POINTER(ct))
+
+
+def _f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _f32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _i32(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.int32)
+
+
+# ---- host set-up routines ------------------------------------------------------------------
+
+def make_grid(wmode, wstart, wend, dstep):
+    """Wavelength grid of Init (synth.f90:56-74): offsets from wstart."""
+    n = C.c_int()
+    rc = lib().fsg_make_grid(int(wmode), float(wstart), float(wend), float(dstep), None, C.byref(n))
+    if rc != 0:
+        raise FsgError("fsg_make_grid: bad grid (%d)" % rc)
+    w = np.zeros(n.value)
+    lib().fsg_make_grid(int(wmode), float(wstart), float(wend), float(dstep), _p(w, C.c_double), C.byref(n))
+    return w
+
+
+def mu_quadrature(quad, n, x=None):
+    setnodes = x is None
+    x = np.zeros(n) if x is None else _f64(x).copy()
+    w = np.zeros(n); r = np.zeros(n + 1)
+    rc = lib().fsg_mu_quadrature(int(quad), int(n), _p(x, C.c_double), _p(w, C.c_double), _p(r, C.c_double),
+                                 int(setnodes))
+    if rc != 0:
+        raise FsgError("fsg_mu_quadrature failed (%d)" % rc)
+    return x, w, r
+
+
+def zeeman_pattern(jlo, jup, glo, gup):
+    m = int(round(2 * jup)) + 1
+    npi, nsi = C.c_int32(), C.c_int32()
+    spi, rpi, ssi, rsi = (np.zeros(max(m, 1), np.float32) for _ in range(4))
+    rc = lib().fsg_zeeman_pattern(jlo, jup, glo, gup, C.byref(npi), _p(spi, C.c_float), _p(rpi, C.c_float),
+                                  C.byref(nsi), _p(ssi, C.c_float), _p(rsi, C.c_float))
+    if rc != 0:
+        raise FsgError("fsg_zeeman_pattern failed (%d)" % rc)
+    return spi[:npi.value], rpi[:npi.value], ssi[:nsi.value], rsi[:nsi.value]
+
+
+class LineList:
+    """Host SoA line list in the reference's stored precision (wl FP64, the rest FP32).
+
+    kind: 0 atomic HDF records, 1 single-species molecular, 2 ASCII / magnetic records.
+    zeeman: (npi, nsi, spl_pi, str_pi, spl_si, str_si) with the sigma components mirrored as
+    the .z reader stores them (blue half first)."""
+
+    def __init__(self, wl, elo, gf, grad, gqst, gvdw, spc, kind=2, ismol=None, ihe=None, zeeman=None):
+        k = self._keep = {}
+        s = CLines()
+        n = len(wl)
+        s.n = n
+        k["wl"] = _f64(wl); s.wl = _p(k["wl"], C.c_double)
+        for name, arr in (("elo", elo), ("gf", gf), ("grad", grad), ("gqst", gqst), ("gvdw", gvdw)):
+            k[name] = _f32(arr); setattr(s, name, _p(k[name], C.c_float))
+        k["spc"] = _i32(spc); s.spc = _p(k["spc"], C.c_int32)
+        s.kind = int(kind)
+        if ismol is not None:
+            k["ismol"] = _i32(ismol); s.ismol = _p(k["ismol"], C.c_int32)
+        if ihe is not None:
+            k["ihe"] = _i32(ihe); s.ihe = _p(k["ihe"], C.c_int32)
+        if zeeman is not None:
+            npi, nsi, spl_pi, str_pi, spl_si, str_si = zeeman
+            k["npi"] = _i32(npi); k["nsi"] = _i32(nsi)
+            k["pi_off"] = np.ascontiguousarray(np.concatenate([[0], np.cumsum(k["npi"])[:-1]]), np.int64)
+            k["si_off"] = np.ascontiguousarray(np.concatenate([[0], np.cumsum(k["nsi"])[:-1]]), np.int64)
+            for name, arr in (("spl_pi", spl_pi), ("str_pi", str_pi), ("spl_si", spl_si), ("str_si", str_si)):
+                k[name] = _f32(arr if len(arr) else np.zeros(1, np.float32))
+                setattr(s, name, _p(k[name], C.c_float))
+            s.npi = _p(k["npi"], C.c_int32); s.nsi = _p(k["nsi"], C.c_int32)
+            s.pi_off = _p(k["pi_off"], C.c_int64); s.si_off = _p(k["si_off"], C.c_int64)
+        self.c = s
+        self.n = n
+
+    @classmethod
+    def from_arrays(cls, a, kind=2, zeeman=None):
+        return cls(a["wl"], a["elo"], a["gf"], a["grad"], a["gqst"], a["gvdw"], a["spc"], kind=kind,
+                   ismol=a.get("ismol"), zeeman=zeeman)
+
+
+class Context:
+    """One device context: grid + atmosphere + continuum + accumulators (fsg_ctx)."""
+
+    def __init__(self, device=0, precision=PREC_MIXED, vmicro=0.0, epsopac=1e-4, vwfudge=1.0, h2brd=0.0,
+                 vwmol=0.0, molbrd=0, limitram_gb=16.0):
+        self._lib = lib()
+        cfg = Config(device, precision, vmicro, epsopac, vwfudge, h2brd, vwmol, int(molbrd), limitram_gb)
+        h = C.c_void_p()
+        rc = self._lib.fsg_create(C.byref(cfg), C.byref(h))
+        if rc != 0:
+            raise FsgError("fsg_create failed (%d): no usable CUDA device or bad configuration" % rc)
+        self.h = h
+        self.nwl = self.ntau = self.nmu = 0
+        self._keep = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.fsg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc, what):
+        if rc != 0:
+            msg = self._lib.fsg_last_error(self.h)
+            raise FsgError("%s failed (%d): %s" % (what, rc, msg.decode() if msg else ""))
+
+    def set_grid(self, wmode, wstart, wend, dstep, wave=None):
+        w = make_grid(wmode, wstart, wend, dstep) if wave is None else _f64(wave)
+        self._ck(self._lib.fsg_set_grid(self.h, int(wmode), float(wstart), float(wend), float(dstep), len(w),
+                                        _p(w, C.c_double)), "fsg_set_grid")
+        self.nwl = len(w)
+        self.wave = w
+        self.wfirst = float(wstart)
+        return w
+
+    def set_atmosphere(self, st):
+        """st: dict rhox, T, xne, xna, rho (FP64 [ntau]); fractionpf (FP32 [ntau][nspc]); xamass,
+        potion (FP32 [nspc]); ion (int [nspc]); frac_h1, frac_he1[, frac_h2] (FP32 [ntau])."""
+        a = {k: _f64(st[k]) for k in ("rhox", "T", "xne", "xna", "rho")}
+        fpf = _f32(st["fractionpf"])
+        ntau, nspc = fpf.shape
+        x = dict(xamass=_f32(st["xamass"]), potion=_f32(st["potion"]), ion=_i32(st["ion"]),
+                 h1=_f32(st["frac_h1"]), he1=_f32(st["frac_he1"]),
+                 h2=_f32(st.get("frac_h2", np.zeros(ntau, np.float32))))
+        self._ck(self._lib.fsg_set_atmosphere(
+            self.h, ntau, _p(a["rhox"], C.c_double), _p(a["T"], C.c_double), _p(a["xne"], C.c_double),
+            _p(a["xna"], C.c_double), _p(a["rho"], C.c_double), nspc, _p(fpf, C.c_float),
+            _p(x["xamass"], C.c_float), _p(x["potion"], C.c_float), _p(x["ion"], C.c_int32),
+            _p(x["h1"], C.c_float), _p(x["he1"], C.c_float), _p(x["h2"], C.c_float)), "fsg_set_atmosphere")
+        self.ntau = ntau
+        self.rhox = a["rhox"]; self.T = a["T"]
+
+    def set_contopac(self, contopac, contopac_std=None, motype=0):
+        co = _f64(contopac)
+        if co.shape != (self.nwl, self.ntau):
+            raise FsgError("contopac shape %s != (%d, %d)" % (co.shape, self.nwl, self.ntau))
+        cs = _f64(contopac_std)
+        self._ck(self._lib.fsg_set_contopac(self.h, _p(co, C.c_double), _p(cs, C.c_double), int(motype)),
+                 "fsg_set_contopac")
+
+    def set_contopac_dev(self, ptr):
+        self._ck(self._lib.fsg_set_contopac_dev(self.h, C.c_void_p(ptr)), "fsg_set_contopac_dev")
+
+    def set_mu(self, xmu, wmu):
+        xmu = _f64(xmu); wmu = _f64(wmu)
+        self._ck(self._lib.fsg_set_mu(self.h, len(xmu), _p(xmu, C.c_double), _p(wmu, C.c_double)), "fsg_set_mu")
+        self.nmu = len(xmu)
+
+    def lineop_reset(self):
+        self._ck(self._lib.fsg_lineop_reset(self.h), "fsg_lineop_reset")
+
+    def lineop_calc(self, lines, want_lineopac=True, want_lines=True):
+        """LineopCalc for one list; returns dict(lineopac, flags, ileft, iright, stats)."""
+        n = lines.n
+        lo = np.zeros((self.nwl, self.ntau)) if want_lineopac else None
+        fl = np.zeros(max(n, 1), np.int32) if want_lines else None
+        il = np.zeros(max(n, 1), np.int32) if want_lines else None
+        ir = np.zeros(max(n, 1), np.int32) if want_lines else None
+        st = Stats()
+        self._ck(self._lib.fsg_lineop_calc(self.h, C.byref(lines.c), _p(lo, C.c_double), _p(fl, C.c_int32),
+                                           _p(il, C.c_int32), _p(ir, C.c_int32), None, C.byref(st)),
+                 "fsg_lineop_calc")
+        out = dict(lineopac=lo, stats=st.asdict())
+        if want_lines:
+            out.update(flags=fl[:n], ileft=il[:n], iright=ir[:n])
+        return out
+
+    def lineop_calc_dev(self, dlines):
+        st = Stats()
+        self._ck(self._lib.fsg_lineop_calc_dev(self.h, C.byref(dlines), C.byref(st)), "fsg_lineop_calc_dev")
+        return st.asdict()
+
+    def lineop_get(self):
+        lo = np.zeros((self.nwl, self.ntau))
+        self._ck(self._lib.fsg_lineop_get(self.h, _p(lo, C.c_double)), "fsg_lineop_get")
+        return lo
+
+    def lineop_set(self, lineopac):
+        lo = _f64(lineopac)
+        self._ck(self._lib.fsg_lineop_set(self.h, _p(lo, C.c_double)), "fsg_lineop_set")
+
+    def radtran(self):
+        """RadTranCalc + disk integration: (spl [nwl][nmu], spc, sfl [nwl], sfc)."""
+        spl = np.zeros((self.nwl, self.nmu)); spc = np.zeros((self.nwl, self.nmu))
+        sfl = np.zeros(self.nwl); sfc = np.zeros(self.nwl)
+        self._ck(self._lib.fsg_radtran(self.h, _p(spl, C.c_double), _p(spc, C.c_double), _p(sfl, C.c_double),
+                                       _p(sfc, C.c_double)), "fsg_radtran")
+        return spl, spc, sfl, sfc
+
+    def radtran_dev(self, d_spl, d_spc, d_sfl, d_sfc):
+        v = lambda p: C.c_void_p(p) if p else None
+        self._ck(self._lib.fsg_radtran_dev(self.h, v(d_spl), v(d_spc), v(d_sfl), v(d_sfc)), "fsg_radtran_dev")
+
+    def mag_lineop_calc(self, lines, bframe, bfield, want=True):
+        n = lines.n
+        bf = _f64(bfield)
+        mlo = np.zeros((self.nwl, self.ntau, 6)) if want else None
+        fl = np.zeros(max(n, 1), np.int32); il = np.zeros(max(n, 1), np.int32); ir = np.zeros(max(n, 1), np.int32)
+        st = Stats()
+        self._ck(self._lib.fsg_mag_lineop_calc(self.h, C.byref(lines.c), int(bframe), _p(bf, C.c_double), len(bf),
+                                               _p(mlo, C.c_double), _p(fl, C.c_int32), _p(il, C.c_int32),
+                                               _p(ir, C.c_int32), None, C.byref(st)), "fsg_mag_lineop_calc")
+        return dict(maglineopac=mlo, flags=fl[:n], ileft=il[:n], iright=ir[:n], stats=st.asdict())
+
+    def mag_radtran(self, bframe, bfield):
+        bf = _f64(bfield)
+        spz = np.zeros((self.nwl, 4, self.nmu)); spc = np.zeros((self.nwl, self.nmu))
+        sfl = np.zeros(self.nwl); sfc = np.zeros(self.nwl)
+        self._ck(self._lib.fsg_mag_radtran(self.h, int(bframe), _p(bf, C.c_double), len(bf), _p(spz, C.c_double),
+                                           _p(spc, C.c_double), _p(sfl, C.c_double), _p(sfc, C.c_double)),
+                 "fsg_mag_radtran")
+        return spz, spc, sfl, sfc
+
+    def hvoigt(self, a, v):
+        a = _f64(a); v = _f64(v); h = np.zeros_like(a)
+        self._ck(self._lib.fsg_hvoigt(self.h, len(a), _p(a, C.c_double), _p(v, C.c_double), _p(h, C.c_double)),
+                 "fsg_hvoigt")
+        return h
+
+    def fvoigt(self, a, v):
+        a = _f64(a); v = _f64(v); h = np.zeros_like(a); l = np.zeros_like(a)
+        self._ck(self._lib.fsg_fvoigt(self.h, len(a), _p(a, C.c_double), _p(v, C.c_double), _p(h, C.c_double),
+                                      _p(l, C.c_double)), "fsg_fvoigt")
+        return h, l
+
+    def voigt_tables(self):
+        v = np.zeros((402, 1002), np.float32); f = np.zeros((402, 1002, 2), np.float32)
+        self._ck(self._lib.fsg_voigt_tables(self.h, _p(v, C.c_float), _p(f, C.c_float)), "fsg_voigt_tables")
+        return v, f
+
+    def locprf_pp(self, xmu, xki, src, rhox):
+        xmu = _f64(xmu); xki = np.atleast_2d(_f64(xki)); src = np.atleast_2d(_f64(src)); rhox = _f64(rhox)
+        nprof, ntau = xki.shape
+        out = np.zeros((nprof, len(xmu)))
+        self._ck(self._lib.fsg_locprf_pp(self.h, nprof, len(xmu), _p(xmu, C.c_double), ntau, _p(xki, C.c_double),
+                                         _p(src, C.c_double), _p(rhox, C.c_double), _p(out, C.c_double)),
+                 "fsg_locprf_pp")
+        return out

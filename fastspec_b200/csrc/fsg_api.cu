@@ -1,0 +1,898 @@
+// fsg_api.cu -- C-ABI entry points: context, uploads, and the LineopCalc / RadTranCalc drivers.
+#include "fsg_internal.cuh"
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+// ---- kernels defined in fsg_kernels64.cu / fsg_fast.cu / fsg_mag.cu ------------------------------
+void fsg_launch_xline_init(cudaStream_t, int, const double *, const double *, const double *, const float *,
+                           const float *, const float *, double, double *);
+void fsg_launch_center(cudaStream_t, const AtmView &, const LineView &, const VoigtTables &, int32_t *,
+                       int32_t *, int32_t *, unsigned long long *);
+void fsg_launch_params_fast(cudaStream_t, const AtmView &, const LineView &, const int64_t *, int64_t, int64_t,
+                            const int32_t *, const int32_t *, const int32_t *, WingRec *, CoreRec *, LineHdr *);
+void fsg_launch_params_fp64(cudaStream_t, const AtmView &, const LineView &, int64_t, int64_t, const int32_t *,
+                            double3 *);
+void fsg_launch_span(cudaStream_t, int64_t, const int32_t *, const int32_t *, const int32_t *, int *, int *);
+void fsg_launch_accum_fp64(cudaStream_t, const AtmView &, const double *, int, int, const int *, const int *,
+                           const int32_t *, const int32_t *, const int32_t *, int64_t, const double3 *,
+                           const VoigtTables &, double *, double *);
+void fsg_launch_wide_fp64(cudaStream_t, const AtmView &, const LineView &, int, const int64_t *, const int32_t *,
+                          const int32_t *, const int32_t *, double3 *, const VoigtTables &, int, int, double *,
+                          double *);
+int fsg_launch_radtran(cudaStream_t, const AtmView &, const double *, const double *, int, const double *,
+                       const double *, double *, double *, double *, double *);
+void fsg_launch_hvoigt(cudaStream_t, int64_t, const double *, const double *, double *, const VoigtTables &);
+void fsg_launch_fvoigt(cudaStream_t, int64_t, const double *, const double *, double *, double *,
+                       const VoigtTables &);
+void fsg_launch_locprf(cudaStream_t, int, int, const double *, int, const double *, const double *, const double *,
+                       double *, double *);
+int fsg_fast_set_constants(const double *, const double *);
+int fsg_launch_accum_fast(cudaStream_t, int, int, const double *, const LineHdr *, const WingRec *,
+                          const CoreRec *, const int *, const int *, const float *, double *);
+int fsg_fast_tiles(int);
+void fsg_launch_tile_span(cudaStream_t, int, int64_t, const LineHdr *, int *, int *);
+int fsg_select(cudaStream_t, int64_t, const int32_t *, const int32_t *, const int32_t *, int, int *, int64_t *,
+               int64_t *, int64_t *);
+void fsg_launch_class_hist(cudaStream_t, int64_t, const int32_t *, const int32_t *, const int32_t *,
+                           unsigned long long *);
+void fsg_launch_mark_wide(cudaStream_t, const AtmView &, int64_t, const double *, int64_t, int32_t *,
+                          const int32_t *, const int32_t *, unsigned long long *);
+
+void fsg_launch_gather_lines(cudaStream_t, const LineView &, const int64_t *, int64_t, char *, const int32_t *,
+                             const int32_t *, const int32_t *, LineView *, int32_t **, int32_t **, int32_t **);
+int fsg_select_wide(cudaStream_t, int64_t, const int32_t *, int *, int64_t *, int64_t *, int64_t *);
+void fsg_launch_scatter_flags(cudaStream_t, int64_t, const int64_t *, const int32_t *, int32_t *);
+double fsg_count_evals(fsg_ctx *, int64_t);
+
+std::string fsg_cuda_msg(cudaError_t e, const char *what) {
+    char b[512];
+    snprintf(b, sizeof b, "%s: CUDA error %d (%s)", what, (int)e, cudaGetErrorString(e));
+    return b;
+}
+
+// ---- device buffer that only grows ---------------------------------------------------------------
+struct DBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t bytes) {
+        if (bytes <= cap) return FSG_OK;
+        if (p) cudaFree(p);
+        p = nullptr; cap = 0;
+        if (bytes == 0) return FSG_OK;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) { cudaGetLastError(); return FSG_E_NOMEM; }
+        cap = bytes;
+        return FSG_OK;
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+    template <class T> T *as() const { return (T *)p; }
+};
+
+struct fsg_ctx {
+    fsg_config cfg;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    VoigtTables tab{};
+    double h_anode[FSG_NA1], h_aida[FSG_NA1];
+    // grid
+    int have_grid = 0, wmode = 0, nwl = 0;
+    double wstart = 0, wend = 0, dstep = 0, rstep = 0, wfirst = 0;
+    DBuf d_wave;
+    // atmosphere
+    int have_atm = 0, ntau = 0, nspc = 0;
+    DBuf d_xi, d_fpf, d_xamass, d_potion, d_ion, d_rhox, d_tmp;
+    int have_cont = 0, motype = 0;
+    DBuf d_cont, d_contstd;
+    int nhe = 0, spc_he1 = -1;
+    DBuf d_hegam, d_heshf;
+    // mu
+    int nmu = 0;
+    DBuf d_xmu, d_wmu;
+    // accumulators
+    DBuf d_lineopac, d_maglineopac;
+    // line list staging + per-line outputs
+    DBuf l_wl, l_elo, l_gf, l_grad, l_gqst, l_gvdw, l_spc, l_ismol, l_ihe;
+    DBuf d_flags, d_ileft, d_iright, d_idx, d_counts, d_offs, d_total, d_hist, d_nkeep;
+    // block buffers
+    DBuf d_wing, d_core, d_hdr, d_tlo, d_thi, d_p64, d_lstart, d_lstop, d_widx, d_pw, d_evals;
+    // spectra
+    DBuf d_spl, d_spc, d_sfl, d_sfc, d_work, d_a, d_v, d_h, d_l;
+    // magnetic
+    DBuf z_npi, z_nsi, z_pioff, z_sioff, z_splpi, z_strpi, z_splsi, z_strsi, d_zsc;
+    cudaEvent_t ev[8];
+};
+
+static int fail(fsg_ctx *c, int code, const char *msg) { if (c) c->err = msg; return code; }
+static int cuda_fail(fsg_ctx *c, cudaError_t e, const char *what) {
+    if (c) c->err = fsg_cuda_msg(e, what);
+    return FSG_E_CUDA;
+}
+#define CK(call, what) do { cudaError_t _e = (call); if (_e != cudaSuccess) return cuda_fail(ctx, _e, what); } while (0)
+#define ALLOC(buf, bytes) do { if ((buf).ensure(bytes) != FSG_OK) return fail(ctx, FSG_E_NOMEM, "device allocation failed: " #buf); } while (0)
+
+AtmView fsg_view(const fsg_ctx *ctx) {
+    AtmView A;
+    memset(&A, 0, sizeof A);
+    A.ntau = ctx->ntau; A.nspc = ctx->nspc; A.nwl = ctx->nwl; A.wmode = ctx->wmode; A.motype = ctx->motype;
+    A.nhe = ctx->nhe; A.spc_he1 = ctx->spc_he1; A.molbrd = ctx->cfg.molbrd;
+    A.wfirst = ctx->wfirst; A.wstart = ctx->wstart; A.dstep = ctx->dstep; A.rstep = ctx->rstep;
+    double c = FSG_VC * 1e13;
+    A.vturb2 = 1e26 / c / c * (ctx->cfg.vmicro * ctx->cfg.vmicro);
+    A.epsopac = ctx->cfg.epsopac; A.vwfudge = ctx->cfg.vwfudge; A.vwmol = ctx->cfg.vwmol;
+    A.xi = ctx->d_xi.as<double>(); A.fpf = ctx->d_fpf.as<float>(); A.xamass = ctx->d_xamass.as<float>();
+    A.potion = ctx->d_potion.as<float>(); A.ion = ctx->d_ion.as<int>(); A.wave = ctx->d_wave.as<double>();
+    A.contopac = ctx->d_cont.as<double>(); A.contstd = ctx->d_contstd.as<double>();
+    A.hegam = ctx->d_hegam.as<double>(); A.heshf = ctx->d_heshf.as<double>();
+    return A;
+}
+
+extern "C" {
+
+int fsg_version(void) { return 10000; }
+
+const char *fsg_last_error(const fsg_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int fsg_create(const fsg_config *cfg, fsg_ctx **out) {
+    if (!cfg || !out) return FSG_E_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) { cudaGetLastError(); return FSG_E_CUDA; }
+    if (cfg->device < 0 || cfg->device >= ndev) return FSG_E_ARG;
+    if (cfg->precision != FSG_PREC_MIXED && cfg->precision != FSG_PREC_FP64) return FSG_E_ARG;
+    fsg_ctx *ctx = new fsg_ctx();
+    ctx->cfg = *cfg;
+    if (ctx->cfg.epsopac <= 0) ctx->cfg.epsopac = 1e-4;
+    if (ctx->cfg.limitram_gb <= 0) ctx->cfg.limitram_gb = 16.0;
+    ctx->device = cfg->device;
+    if (cudaSetDevice(ctx->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError(); delete ctx; return FSG_E_CUDA;
+    }
+    for (int i = 0; i < 8; i++) cudaEventCreate(&ctx->ev[i]);
+    std::string e;
+    int rc = fsg_build_tables(&ctx->tab, ctx->stream, &e);
+    if (rc == FSG_OK) {
+        if (cudaMemcpyAsync(ctx->h_anode, ctx->tab.anode, sizeof ctx->h_anode, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+            cudaMemcpyAsync(ctx->h_aida, ctx->tab.aida, sizeof ctx->h_aida, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+            cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = FSG_E_CUDA;
+        else rc = fsg_fast_set_constants(ctx->h_anode, ctx->h_aida);
+    }
+    if (rc != FSG_OK) { fsg_destroy(ctx); return rc; }
+    *out = ctx;
+    return FSG_OK;
+}
+
+void fsg_destroy(fsg_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    fsg_free_tables(&ctx->tab);
+    DBuf *bufs[] = { &ctx->d_wave, &ctx->d_xi, &ctx->d_fpf, &ctx->d_xamass, &ctx->d_potion, &ctx->d_ion, &ctx->d_rhox,
+                     &ctx->d_tmp, &ctx->d_cont, &ctx->d_contstd, &ctx->d_hegam, &ctx->d_heshf, &ctx->d_xmu,
+                     &ctx->d_wmu, &ctx->d_lineopac, &ctx->d_maglineopac, &ctx->l_wl, &ctx->l_elo, &ctx->l_gf,
+                     &ctx->l_grad, &ctx->l_gqst, &ctx->l_gvdw, &ctx->l_spc, &ctx->l_ismol, &ctx->l_ihe,
+                     &ctx->d_flags, &ctx->d_ileft, &ctx->d_iright, &ctx->d_idx, &ctx->d_counts, &ctx->d_offs,
+                     &ctx->d_total, &ctx->d_hist, &ctx->d_nkeep, &ctx->d_wing, &ctx->d_core, &ctx->d_hdr,
+                     &ctx->d_tlo, &ctx->d_thi, &ctx->d_p64, &ctx->d_lstart, &ctx->d_lstop, &ctx->d_widx,
+                     &ctx->d_pw, &ctx->d_evals, &ctx->d_spl, &ctx->d_spc, &ctx->d_sfl, &ctx->d_sfc,
+                     &ctx->d_work, &ctx->d_a, &ctx->d_v, &ctx->d_h, &ctx->d_l, &ctx->z_npi, &ctx->z_nsi,
+                     &ctx->z_pioff, &ctx->z_sioff, &ctx->z_splpi, &ctx->z_strpi, &ctx->z_splsi, &ctx->z_strsi,
+                     &ctx->d_zsc };
+    for (DBuf *b : bufs) b->release();
+    for (int i = 0; i < 8; i++) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+// ---- grid (synth.f90:56-74) ---------------------------------------------------------------------
+int fsg_make_grid(int wmode, double wstart, double wend, double dstep, double *wave, int *nwl) {
+    if (!nwl || dstep <= 0 || wend <= wstart || (wmode != 0 && wmode != 1)) return FSG_E_ARG;
+    const double EpsWl = 1e-12;
+    int n;
+    if (wmode == 0) {
+        n = (int)floor((wend - wstart) / dstep + EpsWl) + 1;
+        if (n < 2) return FSG_E_ARG;
+        if (wave) for (int i = 1; i <= n; i++) wave[i - 1] = (double)(i - 1) * dstep;
+    } else {
+        double rstep = dstep / FSG_VC;
+        n = (int)floor(log(wend / wstart) / rstep + EpsWl) + 1;
+        if (n < 2) return FSG_E_ARG;
+        if (wave) for (int i = 1; i <= n; i++) wave[i - 1] = wstart * exp((double)(i - 1) * rstep) - wstart;
+    }
+    *nwl = n;
+    return FSG_OK;
+}
+
+int fsg_set_grid(fsg_ctx *ctx, int wmode, double wstart, double wend, double dstep, int nwl, const double *wave) {
+    if (!ctx || !wave || nwl < 2 || (wmode != 0 && wmode != 1) || dstep <= 0) return fail(ctx, FSG_E_ARG, "fsg_set_grid: bad arguments");
+    cudaSetDevice(ctx->device);
+    ctx->wmode = wmode; ctx->wstart = wstart; ctx->wend = wend; ctx->dstep = dstep; ctx->nwl = nwl;
+    ctx->rstep = dstep / FSG_VC; ctx->wfirst = wstart;
+    ALLOC(ctx->d_wave, sizeof(double) * nwl);
+    CK(cudaMemcpyAsync(ctx->d_wave.p, wave, sizeof(double) * nwl, cudaMemcpyHostToDevice, ctx->stream), "grid upload");
+    CK(cudaStreamSynchronize(ctx->stream), "grid upload");
+    ctx->have_grid = 1; ctx->have_cont = 0;
+    return FSG_OK;
+}
+
+int fsg_set_atmosphere(fsg_ctx *ctx, int ntau, const double *rhox, const double *T, const double *xne,
+                       const double *xna, const double *rho, int nspc, const float *fractionpf, const float *xamass,
+                       const float *potion, const int32_t *ion, const float *frac_h1, const float *frac_he1,
+                       const float *frac_h2) {
+    (void)xna;
+    if (!ctx || ntau < 3 || ntau > 128 || nspc < 1 || !rhox || !T || !xne || !rho || !fractionpf || !xamass ||
+        !potion || !ion || !frac_h1 || !frac_he1)
+        return fail(ctx, FSG_E_ARG, "fsg_set_atmosphere: bad arguments (3 <= ntau <= 128, nspc >= 1)");
+    cudaSetDevice(ctx->device);
+    ctx->ntau = ntau; ctx->nspc = nspc;
+    ALLOC(ctx->d_xi, sizeof(double) * XI_NROWS * ntau);
+    ALLOC(ctx->d_fpf, sizeof(float) * (size_t)nspc * ntau);
+    ALLOC(ctx->d_xamass, sizeof(float) * nspc);
+    ALLOC(ctx->d_potion, sizeof(float) * nspc);
+    ALLOC(ctx->d_ion, sizeof(int) * nspc);
+    ALLOC(ctx->d_rhox, sizeof(double) * ntau);
+    ALLOC(ctx->d_tmp, sizeof(double) * 3 * ntau + sizeof(float) * 3 * ntau);
+    // FractionPF arrives as [ntau][nspc] (species fastest); stored species-major [nspc][ntau]
+    std::vector<float> fpf((size_t)nspc * ntau);
+    for (int t = 0; t < ntau; t++) for (int s = 0; s < nspc; s++) fpf[(size_t)s * ntau + t] = fractionpf[(size_t)t * nspc + s];
+    std::vector<float> h2(ntau, 0.0f);
+    if (frac_h2) for (int t = 0; t < ntau; t++) h2[t] = frac_h2[t];
+    double *dT = ctx->d_tmp.as<double>(), *dxne = dT + ntau, *drho = dxne + ntau;
+    float *dh1 = (float *)(drho + ntau), *dhe1 = dh1 + ntau, *dh2 = dhe1 + ntau;
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemcpyAsync(ctx->d_fpf.p, fpf.data(), sizeof(float) * fpf.size(), cudaMemcpyHostToDevice, s), "atm upload");
+    CK(cudaMemcpyAsync(ctx->d_xamass.p, xamass, sizeof(float) * nspc, cudaMemcpyHostToDevice, s), "atm upload");
+    CK(cudaMemcpyAsync(ctx->d_potion.p, potion, sizeof(float) * nspc, cudaMemcpyHostToDevice, s), "atm upload");
+    CK(cudaMemcpyAsync(ctx->d_ion.p, ion, sizeof(int) * nspc, cudaMemcpyHostToDevice, s), "atm upload");
+    CK(cudaMemcpyAsync(ctx->d_rhox.p, rhox, sizeof(double) * ntau, cudaMemcpyHostToDevice, s), "atm upload");
+    CK(cudaMemcpyAsync(dT, T, sizeof(double) * ntau, cudaMemcpyHostToDevice, s), "atm upload");
+    CK(cudaMemcpyAsync(dxne, xne, sizeof(double) * ntau, cudaMemcpyHostToDevice, s), "atm upload");
+    CK(cudaMemcpyAsync(drho, rho, sizeof(double) * ntau, cudaMemcpyHostToDevice, s), "atm upload");
+    CK(cudaMemcpyAsync(dh1, frac_h1, sizeof(float) * ntau, cudaMemcpyHostToDevice, s), "atm upload");
+    CK(cudaMemcpyAsync(dhe1, frac_he1, sizeof(float) * ntau, cudaMemcpyHostToDevice, s), "atm upload");
+    CK(cudaMemcpyAsync(dh2, h2.data(), sizeof(float) * ntau, cudaMemcpyHostToDevice, s), "atm upload");
+    fsg_launch_xline_init(s, ntau, dT, dxne, drho, dh1, dhe1, dh2, ctx->cfg.h2brd, ctx->d_xi.as<double>());
+    CK(cudaGetLastError(), "k_xline_init");
+    CK(cudaStreamSynchronize(s), "atm upload");
+    ctx->have_atm = 1; ctx->have_cont = 0;
+    return FSG_OK;
+}
+
+int fsg_set_contopac(fsg_ctx *ctx, const double *contopac, const double *contopac_std, int motype) {
+    if (!ctx) return FSG_E_ARG;
+    if (!ctx->have_grid || !ctx->have_atm) return fail(ctx, FSG_E_STATE, "fsg_set_contopac: set grid and atmosphere first");
+    if (!contopac || (motype == 1 && !contopac_std) || (motype != 0 && motype != 1))
+        return fail(ctx, FSG_E_ARG, "fsg_set_contopac: bad arguments");
+    cudaSetDevice(ctx->device);
+    size_t nb = sizeof(double) * (size_t)ctx->nwl * ctx->ntau;
+    ALLOC(ctx->d_cont, nb);
+    CK(cudaMemcpyAsync(ctx->d_cont.p, contopac, nb, cudaMemcpyHostToDevice, ctx->stream), "contopac upload");
+    ctx->motype = motype;
+    if (motype == 1) {
+        ALLOC(ctx->d_contstd, sizeof(double) * ctx->ntau);
+        CK(cudaMemcpyAsync(ctx->d_contstd.p, contopac_std, sizeof(double) * ctx->ntau, cudaMemcpyHostToDevice, ctx->stream), "contstd upload");
+    }
+    CK(cudaStreamSynchronize(ctx->stream), "contopac upload");
+    ctx->have_cont = 1;
+    return FSG_OK;
+}
+
+int fsg_set_contopac_dev(fsg_ctx *ctx, const double *d_contopac) {
+    if (!ctx || !d_contopac) return FSG_E_ARG;
+    if (!ctx->have_grid || !ctx->have_atm) return fail(ctx, FSG_E_STATE, "fsg_set_contopac_dev: set grid and atmosphere first");
+    cudaSetDevice(ctx->device);
+    size_t nb = sizeof(double) * (size_t)ctx->nwl * ctx->ntau;
+    ALLOC(ctx->d_cont, nb);
+    CK(cudaMemcpyAsync(ctx->d_cont.p, d_contopac, nb, cudaMemcpyDeviceToDevice, ctx->stream), "contopac copy");
+    CK(cudaStreamSynchronize(ctx->stream), "contopac copy");
+    ctx->motype = 0; ctx->have_cont = 1;
+    return FSG_OK;
+}
+
+int fsg_set_hestark(fsg_ctx *ctx, int nhe, const double *hegam, const double *heshf, int spc_he1) {
+    if (!ctx || nhe < 0 || nhe > 255 || (nhe > 0 && (!hegam || !heshf)) || !ctx->have_atm)
+        return fail(ctx, FSG_E_ARG, "fsg_set_hestark: bad arguments");
+    cudaSetDevice(ctx->device);
+    ctx->nhe = nhe; ctx->spc_he1 = spc_he1;
+    if (nhe > 0) {
+        size_t nb = sizeof(double) * (size_t)nhe * ctx->ntau;
+        ALLOC(ctx->d_hegam, nb); ALLOC(ctx->d_heshf, nb);
+        CK(cudaMemcpyAsync(ctx->d_hegam.p, hegam, nb, cudaMemcpyHostToDevice, ctx->stream), "hestark upload");
+        CK(cudaMemcpyAsync(ctx->d_heshf.p, heshf, nb, cudaMemcpyHostToDevice, ctx->stream), "hestark upload");
+        CK(cudaStreamSynchronize(ctx->stream), "hestark upload");
+    }
+    return FSG_OK;
+}
+
+int fsg_set_mu(fsg_ctx *ctx, int nmu, const double *xmu, const double *wmu) {
+    if (!ctx || nmu < 1 || nmu > 16 || !xmu || !wmu) return fail(ctx, FSG_E_ARG, "fsg_set_mu: 1 <= nmu <= 16");
+    for (int i = 0; i < nmu; i++) if (!(xmu[i] > 0.0 && xmu[i] <= 1.0)) return fail(ctx, FSG_E_ARG, "fsg_set_mu: mu outside (0, 1]");
+    cudaSetDevice(ctx->device);
+    ALLOC(ctx->d_xmu, sizeof(double) * nmu); ALLOC(ctx->d_wmu, sizeof(double) * nmu);
+    CK(cudaMemcpyAsync(ctx->d_xmu.p, xmu, sizeof(double) * nmu, cudaMemcpyHostToDevice, ctx->stream), "mu upload");
+    CK(cudaMemcpyAsync(ctx->d_wmu.p, wmu, sizeof(double) * nmu, cudaMemcpyHostToDevice, ctx->stream), "mu upload");
+    CK(cudaStreamSynchronize(ctx->stream), "mu upload");
+    ctx->nmu = nmu;
+    return FSG_OK;
+}
+
+// ---- line opacity accumulator -----------------------------------------------------------------------
+static int ensure_lineopac(fsg_ctx *ctx) {
+    size_t nb = sizeof(double) * (size_t)ctx->nwl * ctx->ntau;
+    if (ctx->d_lineopac.cap < nb) {
+        ALLOC(ctx->d_lineopac, nb);
+        CK(cudaMemsetAsync(ctx->d_lineopac.p, 0, nb, ctx->stream), "lineopac reset");
+    }
+    return FSG_OK;
+}
+
+int fsg_lineop_reset(fsg_ctx *ctx) {
+    if (!ctx) return FSG_E_ARG;
+    if (!ctx->have_grid || !ctx->have_atm) return fail(ctx, FSG_E_STATE, "fsg_lineop_reset: set grid and atmosphere first");
+    cudaSetDevice(ctx->device);
+    int rc = ensure_lineopac(ctx); if (rc) return rc;
+    CK(cudaMemsetAsync(ctx->d_lineopac.p, 0, sizeof(double) * (size_t)ctx->nwl * ctx->ntau, ctx->stream), "lineopac reset");
+    CK(cudaStreamSynchronize(ctx->stream), "lineopac reset");
+    return FSG_OK;
+}
+
+int fsg_lineop_get(fsg_ctx *ctx, double *lineopac) {
+    if (!ctx || !lineopac) return FSG_E_ARG;
+    if (!ctx->d_lineopac.p) return fail(ctx, FSG_E_STATE, "fsg_lineop_get: no line opacity");
+    cudaSetDevice(ctx->device);
+    CK(cudaMemcpyAsync(lineopac, ctx->d_lineopac.p, sizeof(double) * (size_t)ctx->nwl * ctx->ntau, cudaMemcpyDeviceToHost, ctx->stream), "lineopac get");
+    CK(cudaStreamSynchronize(ctx->stream), "lineopac get");
+    return FSG_OK;
+}
+
+int fsg_lineop_set(fsg_ctx *ctx, const double *lineopac) {
+    if (!ctx || !lineopac) return FSG_E_ARG;
+    if (!ctx->have_grid || !ctx->have_atm) return fail(ctx, FSG_E_STATE, "fsg_lineop_set: set grid and atmosphere first");
+    cudaSetDevice(ctx->device);
+    int rc = ensure_lineopac(ctx); if (rc) return rc;
+    CK(cudaMemcpyAsync(ctx->d_lineopac.p, lineopac, sizeof(double) * (size_t)ctx->nwl * ctx->ntau, cudaMemcpyHostToDevice, ctx->stream), "lineopac set");
+    CK(cudaStreamSynchronize(ctx->stream), "lineopac set");
+    return FSG_OK;
+}
+
+const double *fsg_lineop_device_ptr(fsg_ctx *ctx) { return ctx ? ctx->d_lineopac.as<double>() : nullptr; }
+
+// ---- LineopCalc -----------------------------------------------------------------------------------
+static LineView make_view(const fsg_lines *L) {
+    LineView v;
+    v.n = L->n; v.kind = L->kind; v.wl = L->wl; v.elo = L->elo; v.gf = L->gf; v.grad = L->grad;
+    v.gqst = L->gqst; v.gvdw = L->gvdw; v.spc = L->spc; v.ismol = L->ismol; v.ihe = L->ihe;
+    return v;
+}
+
+static int upload_lines(fsg_ctx *ctx, const fsg_lines *L, fsg_lines *D) {
+    int64_t n = L->n;
+    size_t n8 = sizeof(double) * n, n4 = sizeof(float) * n;
+    ALLOC(ctx->l_wl, n8); ALLOC(ctx->l_elo, n4); ALLOC(ctx->l_gf, n4); ALLOC(ctx->l_grad, n4);
+    ALLOC(ctx->l_gqst, n4); ALLOC(ctx->l_gvdw, n4); ALLOC(ctx->l_spc, n4);
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemcpyAsync(ctx->l_wl.p, L->wl, n8, cudaMemcpyHostToDevice, s), "line upload");
+    CK(cudaMemcpyAsync(ctx->l_elo.p, L->elo, n4, cudaMemcpyHostToDevice, s), "line upload");
+    CK(cudaMemcpyAsync(ctx->l_gf.p, L->gf, n4, cudaMemcpyHostToDevice, s), "line upload");
+    CK(cudaMemcpyAsync(ctx->l_grad.p, L->grad, n4, cudaMemcpyHostToDevice, s), "line upload");
+    CK(cudaMemcpyAsync(ctx->l_gqst.p, L->gqst, n4, cudaMemcpyHostToDevice, s), "line upload");
+    CK(cudaMemcpyAsync(ctx->l_gvdw.p, L->gvdw, n4, cudaMemcpyHostToDevice, s), "line upload");
+    CK(cudaMemcpyAsync(ctx->l_spc.p, L->spc, n4, cudaMemcpyHostToDevice, s), "line upload");
+    *D = *L;
+    D->wl = ctx->l_wl.as<double>(); D->elo = ctx->l_elo.as<float>(); D->gf = ctx->l_gf.as<float>();
+    D->grad = ctx->l_grad.as<float>(); D->gqst = ctx->l_gqst.as<float>(); D->gvdw = ctx->l_gvdw.as<float>();
+    D->spc = ctx->l_spc.as<int32_t>();
+    D->ismol = nullptr; D->ihe = nullptr;
+    if (L->ismol) {
+        ALLOC(ctx->l_ismol, n4);
+        CK(cudaMemcpyAsync(ctx->l_ismol.p, L->ismol, n4, cudaMemcpyHostToDevice, s), "line upload");
+        D->ismol = ctx->l_ismol.as<int32_t>();
+    }
+    if (L->ihe) {
+        ALLOC(ctx->l_ihe, n4);
+        CK(cudaMemcpyAsync(ctx->l_ihe.p, L->ihe, n4, cudaMemcpyHostToDevice, s), "line upload");
+        D->ihe = ctx->l_ihe.as<int32_t>();
+    }
+    return FSG_OK;
+}
+
+static int check_lines(fsg_ctx *ctx, const fsg_lines *L) {
+    if (!ctx) return FSG_E_ARG;
+    if (!ctx->have_grid || !ctx->have_atm || !ctx->have_cont)
+        return fail(ctx, FSG_E_STATE, "lineop: set grid, atmosphere and continuum opacity first");
+    if (!L || L->n < 0 || (L->n > 0 && (!L->wl || !L->elo || !L->gf || !L->grad || !L->gqst || !L->gvdw || !L->spc)))
+        return fail(ctx, FSG_E_ARG, "lineop: bad line list");
+    if (L->kind < 0 || L->kind > 2) return fail(ctx, FSG_E_ARG, "lineop: kind must be 0, 1 or 2");
+    if (L->n > 2000000000LL) return fail(ctx, FSG_E_ARG, "lineop: more than 2e9 lines");
+    return FSG_OK;
+}
+
+static int64_t block_capacity(const fsg_ctx *ctx, size_t per_line) {
+    double cap = ctx->cfg.limitram_gb * 1e9 / (double)per_line;
+    int64_t c = (int64_t)cap;
+    if (c < 8) c = 8;
+    return c;
+}
+
+// central pass common to both precisions; leaves flags/ileft/iright on the device
+static int central_pass(fsg_ctx *ctx, const LineView &LV, int64_t *nkeep) {
+    int64_t n = LV.n;
+    ALLOC(ctx->d_flags, sizeof(int32_t) * std::max<int64_t>(n, 1));
+    ALLOC(ctx->d_ileft, sizeof(int32_t) * std::max<int64_t>(n, 1));
+    ALLOC(ctx->d_iright, sizeof(int32_t) * std::max<int64_t>(n, 1));
+    ALLOC(ctx->d_nkeep, sizeof(unsigned long long));
+    CK(cudaMemsetAsync(ctx->d_nkeep.p, 0, sizeof(unsigned long long), ctx->stream), "center");
+    AtmView A = fsg_view(ctx);
+    fsg_launch_center(ctx->stream, A, LV, ctx->tab, ctx->d_flags.as<int32_t>(), ctx->d_ileft.as<int32_t>(),
+                      ctx->d_iright.as<int32_t>(), ctx->d_nkeep.as<unsigned long long>());
+    CK(cudaGetLastError(), "k_center");
+    unsigned long long nk = 0;
+    CK(cudaMemcpyAsync(&nk, ctx->d_nkeep.p, sizeof nk, cudaMemcpyDeviceToHost, ctx->stream), "center");
+    CK(cudaStreamSynchronize(ctx->stream), "center");
+    *nkeep = (int64_t)nk;
+    return FSG_OK;
+}
+
+// mixed-precision accumulation: classes by window width, blocks within a class
+static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st) {
+    int64_t n = LV.n;
+    const int nt = ctx->ntau;
+    AtmView A = fsg_view(ctx);
+    cudaStream_t s = ctx->stream;
+    ALLOC(ctx->d_hist, sizeof(unsigned long long) * 32);
+    CK(cudaMemsetAsync(ctx->d_hist.p, 0, sizeof(unsigned long long) * 32, s), "hist");
+    fsg_launch_class_hist(s, n, ctx->d_flags.as<int32_t>(), ctx->d_ileft.as<int32_t>(), ctx->d_iright.as<int32_t>(),
+                          ctx->d_hist.as<unsigned long long>());
+    unsigned long long hist[32];
+    CK(cudaMemcpyAsync(hist, ctx->d_hist.p, sizeof hist, cudaMemcpyDeviceToHost, s), "hist");
+    CK(cudaStreamSynchronize(s), "hist");
+    int64_t nblkscan = (n + 1023) / 1024;
+    ALLOC(ctx->d_counts, sizeof(int) * std::max<int64_t>(nblkscan, 1));
+    ALLOC(ctx->d_offs, sizeof(int64_t) * std::max<int64_t>(nblkscan, 1));
+    ALLOC(ctx->d_total, sizeof(int64_t));
+    ALLOC(ctx->d_idx, sizeof(int64_t) * std::max<int64_t>(n, 1));
+    int ntiles = fsg_fast_tiles(ctx->nwl);
+    ALLOC(ctx->d_tlo, sizeof(int) * ntiles); ALLOC(ctx->d_thi, sizeof(int) * ntiles);
+    size_t per_line = (size_t)nt * (sizeof(WingRec) + sizeof(CoreRec)) + sizeof(LineHdr);
+    int64_t cap = block_capacity(ctx, per_line);
+    int64_t nblocks = 0;
+    for (int c = 0; c < 32; c++) {
+        if (!hist[c]) continue;
+        int rc = fsg_select(s, n, ctx->d_flags.as<int32_t>(), ctx->d_ileft.as<int32_t>(), ctx->d_iright.as<int32_t>(), c,
+                            ctx->d_counts.as<int>(), ctx->d_offs.as<int64_t>(), ctx->d_idx.as<int64_t>(),
+                            ctx->d_total.as<int64_t>());
+        if (rc) return cuda_fail(ctx, cudaGetLastError(), "select");
+        int64_t nc = (int64_t)hist[c];
+        int64_t bcap = std::min(cap, nc);
+        ALLOC(ctx->d_wing, sizeof(WingRec) * (size_t)bcap * nt);
+        ALLOC(ctx->d_core, sizeof(CoreRec) * (size_t)bcap * nt);
+        ALLOC(ctx->d_hdr, sizeof(LineHdr) * (size_t)bcap);
+        for (int64_t j0 = 0; j0 < nc; j0 += bcap) {
+            int64_t nb = std::min(bcap, nc - j0);
+            fsg_launch_params_fast(s, A, LV, ctx->d_idx.as<int64_t>(), j0, nb, ctx->d_flags.as<int32_t>(),
+                                   ctx->d_ileft.as<int32_t>(), ctx->d_iright.as<int32_t>(), ctx->d_wing.as<WingRec>(),
+                                   ctx->d_core.as<CoreRec>(), ctx->d_hdr.as<LineHdr>());
+            fsg_launch_tile_span(s, ctx->nwl, nb, ctx->d_hdr.as<LineHdr>(), ctx->d_tlo.as<int>(), ctx->d_thi.as<int>());
+            int rc2 = fsg_launch_accum_fast(s, nt, ctx->nwl, ctx->d_wave.as<double>(), ctx->d_hdr.as<LineHdr>(),
+                                            ctx->d_wing.as<WingRec>(), ctx->d_core.as<CoreRec>(), ctx->d_tlo.as<int>(),
+                                            ctx->d_thi.as<int>(), ctx->tab.vtab, ctx->d_lineopac.as<double>());
+            if (rc2) return cuda_fail(ctx, cudaGetLastError(), "k_accum_fast");
+            nblocks++;
+        }
+    }
+    CK(cudaGetLastError(), "fast accumulation");
+    if (st) st->nblocks = nblocks;
+    return FSG_OK;
+}
+
+// plain FP64 path mirroring LineopCalc's PACK / MarkWideLines / Lstart-Lstop / segment loop
+static int accumulate_fp64(fsg_ctx *ctx, const LineView &LV, int64_t nkeep, fsg_stats *st) {
+    int64_t n = LV.n;
+    const int nt = ctx->ntau, nwl = ctx->nwl;
+    cudaStream_t s = ctx->stream;
+    AtmView A = fsg_view(ctx);
+    // NlinesStep (synth.f90:767): lines per FP64 block within LIMITRAM
+    int64_t cap = block_capacity(ctx, sizeof(double3) * nt);
+    int64_t nstep = std::min<int64_t>(n, cap);
+    // PACK for atomic and .z lists in a single block (synth.f90:915-933)
+    bool pack = (LV.kind == 0 || LV.kind == 2) && nstep == n;
+    int64_t nblkscan = (n + 1023) / 1024;
+    ALLOC(ctx->d_counts, sizeof(int) * std::max<int64_t>(nblkscan, 1));
+    ALLOC(ctx->d_offs, sizeof(int64_t) * std::max<int64_t>(nblkscan, 1));
+    ALLOC(ctx->d_total, sizeof(int64_t));
+    ALLOC(ctx->d_idx, sizeof(int64_t) * std::max<int64_t>(n, 1));
+    // working arrays in packed order: wl, flags, ileft, iright (gathered)
+    LineView W = LV;
+    int32_t *pf = ctx->d_flags.as<int32_t>(), *pl = ctx->d_ileft.as<int32_t>(), *pr = ctx->d_iright.as<int32_t>();
+    int64_t nw = n;
+    DBuf &gbuf = ctx->d_work;
+    if (pack) {
+        fsg_select(s, n, pf, pl, pr, -1, ctx->d_counts.as<int>(), ctx->d_offs.as<int64_t>(), ctx->d_idx.as<int64_t>(),
+                   ctx->d_total.as<int64_t>());
+        nw = nkeep;
+        // gather the per-line arrays of the retained lines (host-side gather is avoided: device gather)
+        size_t need = 64 * (size_t)std::max<int64_t>(nw, 1);
+        ALLOC(gbuf, need);
+        int32_t *gf, *gl, *gr;
+        fsg_launch_gather_lines(s, LV, ctx->d_idx.as<int64_t>(), nw, gbuf.as<char>(), pf, pl, pr, &W, &gf, &gl, &gr);
+        pf = gf; pl = gl; pr = gr;
+        W.n = nw;
+    }
+    if (nw == 0) { if (st) st->nlines_used = 0; return FSG_OK; }
+    // MarkWideLines (synth.f90:709-744)
+    unsigned long long *d_nw = ctx->d_nkeep.as<unsigned long long>();
+    CK(cudaMemsetAsync(d_nw, 0, sizeof(unsigned long long), s), "wide");
+    fsg_launch_mark_wide(s, A, nw, W.wl, nstep, pf, pl, pr, d_nw);
+    unsigned long long nwide = 0;
+    CK(cudaMemcpyAsync(&nwide, d_nw, sizeof nwide, cudaMemcpyDeviceToHost, s), "wide");
+    // Lstart/Lstop (synth.f90:955-978)
+    ALLOC(ctx->d_lstart, sizeof(int) * nwl); ALLOC(ctx->d_lstop, sizeof(int) * nwl);
+    {
+        std::vector<int> ls(nwl, (int)nw), le(nwl, 1);
+        CK(cudaMemcpyAsync(ctx->d_lstart.p, ls.data(), sizeof(int) * nwl, cudaMemcpyHostToDevice, s), "lstart");
+        CK(cudaMemcpyAsync(ctx->d_lstop.p, le.data(), sizeof(int) * nwl, cudaMemcpyHostToDevice, s), "lstop");
+        CK(cudaStreamSynchronize(s), "lstart");
+    }
+    fsg_launch_span(s, nw, pf, pl, pr, ctx->d_lstart.as<int>(), ctx->d_lstop.as<int>());
+    ALLOC(ctx->d_evals, sizeof(double));
+    CK(cudaMemsetAsync(ctx->d_evals.p, 0, sizeof(double), s), "evals");
+    // wide lines: list, parameters, per-wavelength ordered accumulation
+    if (nwide > 0) {
+        ALLOC(ctx->d_widx, sizeof(int64_t) * nwide);
+        fsg_select_wide(s, nw, pf, ctx->d_counts.as<int>(), ctx->d_offs.as<int64_t>(), ctx->d_widx.as<int64_t>(),
+                        ctx->d_total.as<int64_t>());
+        ALLOC(ctx->d_pw, sizeof(double3) * nwide * nt);
+        fsg_launch_wide_fp64(s, A, W, (int)nwide, ctx->d_widx.as<int64_t>(), pf, pl, pr, ctx->d_pw.as<double3>(),
+                             ctx->tab, 1, nwl, ctx->d_lineopac.as<double>(), ctx->d_evals.as<double>());
+    }
+    // segment loop (synth.f90:1006-1088): choose segments on the host from Lstart/Lstop
+    std::vector<int> ls(nwl), le(nwl);
+    CK(cudaMemcpyAsync(ls.data(), ctx->d_lstart.p, sizeof(int) * nwl, cudaMemcpyDeviceToHost, s), "lstart");
+    CK(cudaMemcpyAsync(le.data(), ctx->d_lstop.p, sizeof(int) * nwl, cudaMemcpyDeviceToHost, s), "lstop");
+    CK(cudaStreamSynchronize(s), "lstart");
+    ALLOC(ctx->d_p64, sizeof(double3) * (size_t)std::min<int64_t>(nstep, nw) * nt);
+    int64_t iline1 = 1, ilineb = 0;
+    int iwl1 = 1;
+    int64_t nblocks = 0;
+    for (;;) {
+        int iwl2;
+        if (nstep >= nw) iwl2 = nwl;
+        else {
+            int64_t ilo = nw + 1, ihi = 0;
+            iwl2 = iwl1 - 1;
+            for (int iwl = iwl1; iwl <= nwl; iwl++) {
+                int64_t ilot = std::min<int64_t>(ilo, ls[iwl - 1]), ihit = std::max<int64_t>(ihi, le[iwl - 1]);
+                if (ihit - ilot + 1 > nstep) break;
+                ilo = ilot; ihi = ihit; iwl2 = iwl;
+            }
+            if (iwl2 < iwl1) {
+                char m[256];
+                snprintf(m, sizeof m, "line opacity segmentation: lines contributing to wavelength point #%d span more "
+                         "than %lld line records; increase limitram", iwl1, (long long)nstep);
+                return fail(ctx, FSG_E_SEGMENT, m);
+            }
+            iline1 = std::min<int64_t>(std::max<int64_t>(ilo, 1), nw);
+        }
+        int64_t iline2 = std::min<int64_t>(iline1 + nstep - 1, nw);
+        int64_t loff = iline1 - 1;
+        if (iline1 != ilineb) {
+            ilineb = iline1;
+            fsg_launch_params_fp64(s, A, W, loff, iline2 - loff, pf, ctx->d_p64.as<double3>());
+            nblocks++;
+        }
+        fsg_launch_accum_fp64(s, A, W.wl, iwl1, iwl2, ctx->d_lstart.as<int>(), ctx->d_lstop.as<int>(), pf, pl, pr,
+                              loff, ctx->d_p64.as<double3>(), ctx->tab, ctx->d_lineopac.as<double>(),
+                              ctx->d_evals.as<double>());
+        CK(cudaGetLastError(), "fp64 accumulation");
+        if (iwl2 == nwl) break;
+        iwl1 = iwl2 + 1;
+    }
+    double ev = 0;
+    CK(cudaMemcpyAsync(&ev, ctx->d_evals.p, sizeof ev, cudaMemcpyDeviceToHost, s), "evals");
+    CK(cudaStreamSynchronize(s), "fp64 accumulation");
+    if (st) { st->nwide = (int64_t)nwide; st->nblocks = nblocks; st->line_evals = ev; }
+    // per-line outputs in original order: scatter the packed wide flags back
+    if (pack) {
+        fsg_launch_scatter_flags(s, nw, ctx->d_idx.as<int64_t>(), pf, ctx->d_flags.as<int32_t>());
+    }
+    return FSG_OK;
+}
+
+static int lineop_dev(fsg_ctx *ctx, const fsg_lines *D, fsg_stats *st) {
+    LineView LV = make_view(D);
+    int rc = ensure_lineopac(ctx); if (rc) return rc;
+    if (st) { memset(st, 0, sizeof *st); st->nlines_in = D->n; }
+    if (D->n == 0) return FSG_OK;
+    cudaStream_t s = ctx->stream;
+    CK(cudaEventRecord(ctx->ev[0], s), "event");
+    int64_t nkeep = 0;
+    rc = central_pass(ctx, LV, &nkeep); if (rc) return rc;
+    CK(cudaEventRecord(ctx->ev[1], s), "event");
+    if (st) { st->nlines_used = nkeep; st->nweak = D->n - nkeep; }
+    if (ctx->cfg.precision == FSG_PREC_FP64) rc = accumulate_fp64(ctx, LV, nkeep, st);
+    else rc = accumulate_fast(ctx, LV, st);
+    if (rc) return rc;
+    CK(cudaEventRecord(ctx->ev[2], s), "event");
+    CK(cudaStreamSynchronize(s), "lineop");
+    if (st) {
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
+        cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
+        st->ms_center = a; st->ms_accum = b; st->ms_total = a + b;
+        if (ctx->cfg.precision != FSG_PREC_FP64) {
+            st->line_evals = fsg_count_evals(ctx, D->n);
+        }
+    }
+    return FSG_OK;
+}
+
+int fsg_lineop_calc_dev(fsg_ctx *ctx, const fsg_lines *d_lines, fsg_stats *st) {
+    int rc = check_lines(ctx, d_lines); if (rc) return rc;
+    cudaSetDevice(ctx->device);
+    return lineop_dev(ctx, d_lines, st);
+}
+
+int fsg_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, double *lineopac, int32_t *flags, int32_t *ileft,
+                    int32_t *iright, float *linstr, fsg_stats *st) {
+    int rc = check_lines(ctx, lines); if (rc) return rc;
+    (void)linstr;
+    cudaSetDevice(ctx->device);
+    fsg_lines D;
+    if (lines->n > 0) { rc = upload_lines(ctx, lines, &D); if (rc) return rc; }
+    else D = *lines;
+    rc = lineop_dev(ctx, &D, st); if (rc) return rc;
+    cudaStream_t s = ctx->stream;
+    size_t n4 = sizeof(int32_t) * lines->n;
+    if (lines->n > 0) {
+        if (flags) CK(cudaMemcpyAsync(flags, ctx->d_flags.p, n4, cudaMemcpyDeviceToHost, s), "flags");
+        if (ileft) CK(cudaMemcpyAsync(ileft, ctx->d_ileft.p, n4, cudaMemcpyDeviceToHost, s), "ileft");
+        if (iright) CK(cudaMemcpyAsync(iright, ctx->d_iright.p, n4, cudaMemcpyDeviceToHost, s), "iright");
+    }
+    if (lineopac) CK(cudaMemcpyAsync(lineopac, ctx->d_lineopac.p, sizeof(double) * (size_t)ctx->nwl * ctx->ntau, cudaMemcpyDeviceToHost, s), "lineopac");
+    CK(cudaStreamSynchronize(s), "lineop outputs");
+    return FSG_OK;
+}
+
+// ---- RadTranCalc ------------------------------------------------------------------------------------
+static int radtran_dev(fsg_ctx *ctx, double *spl, double *spc, double *sfl, double *sfc) {
+    if (!ctx->have_grid || !ctx->have_atm || !ctx->have_cont || ctx->nmu < 1)
+        return fail(ctx, FSG_E_STATE, "radtran: set grid, atmosphere, continuum and mu first");
+    int rc = ensure_lineopac(ctx); if (rc) return rc;
+    AtmView A = fsg_view(ctx);
+    rc = fsg_launch_radtran(ctx->stream, A, ctx->d_lineopac.as<double>(), ctx->d_rhox.as<double>(), ctx->nmu,
+                            ctx->d_xmu.as<double>(), ctx->d_wmu.as<double>(), spl, spc, sfl, sfc);
+    if (rc) return cuda_fail(ctx, cudaGetLastError(), "k_radtran");
+    return FSG_OK;
+}
+
+int fsg_radtran_dev(fsg_ctx *ctx, double *d_spl, double *d_spc, double *d_sfl, double *d_sfc) {
+    if (!ctx) return FSG_E_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = radtran_dev(ctx, d_spl, d_spc, d_sfl, d_sfc); if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->stream), "radtran");
+    return FSG_OK;
+}
+
+int fsg_radtran(fsg_ctx *ctx, double *spl, double *spc, double *sfl, double *sfc) {
+    if (!ctx) return FSG_E_ARG;
+    cudaSetDevice(ctx->device);
+    size_t nsp = sizeof(double) * (size_t)ctx->nwl * ctx->nmu, nf = sizeof(double) * ctx->nwl;
+    ALLOC(ctx->d_spl, nsp); ALLOC(ctx->d_spc, nsp); ALLOC(ctx->d_sfl, nf); ALLOC(ctx->d_sfc, nf);
+    int rc = radtran_dev(ctx, ctx->d_spl.as<double>(), ctx->d_spc.as<double>(), ctx->d_sfl.as<double>(),
+                         ctx->d_sfc.as<double>());
+    if (rc) return rc;
+    cudaStream_t s = ctx->stream;
+    if (spl) CK(cudaMemcpyAsync(spl, ctx->d_spl.p, nsp, cudaMemcpyDeviceToHost, s), "spl");
+    if (spc) CK(cudaMemcpyAsync(spc, ctx->d_spc.p, nsp, cudaMemcpyDeviceToHost, s), "spc");
+    if (sfl) CK(cudaMemcpyAsync(sfl, ctx->d_sfl.p, nf, cudaMemcpyDeviceToHost, s), "sfl");
+    if (sfc) CK(cudaMemcpyAsync(sfc, ctx->d_sfc.p, nf, cudaMemcpyDeviceToHost, s), "sfc");
+    CK(cudaStreamSynchronize(s), "radtran");
+    return FSG_OK;
+}
+
+// ---- elemental entry points --------------------------------------------------------------------------
+int fsg_hvoigt(fsg_ctx *ctx, int64_t n, const double *a, const double *v, double *h) {
+    if (!ctx || n < 0 || (n > 0 && (!a || !v || !h))) return fail(ctx, FSG_E_ARG, "fsg_hvoigt: bad arguments");
+    if (n == 0) return FSG_OK;
+    cudaSetDevice(ctx->device);
+    size_t nb = sizeof(double) * n;
+    ALLOC(ctx->d_a, nb); ALLOC(ctx->d_v, nb); ALLOC(ctx->d_h, nb);
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemcpyAsync(ctx->d_a.p, a, nb, cudaMemcpyHostToDevice, s), "hvoigt");
+    CK(cudaMemcpyAsync(ctx->d_v.p, v, nb, cudaMemcpyHostToDevice, s), "hvoigt");
+    fsg_launch_hvoigt(s, n, ctx->d_a.as<double>(), ctx->d_v.as<double>(), ctx->d_h.as<double>(), ctx->tab);
+    CK(cudaGetLastError(), "k_hvoigt");
+    CK(cudaMemcpyAsync(h, ctx->d_h.p, nb, cudaMemcpyDeviceToHost, s), "hvoigt");
+    CK(cudaStreamSynchronize(s), "hvoigt");
+    return FSG_OK;
+}
+
+int fsg_fvoigt(fsg_ctx *ctx, int64_t n, const double *a, const double *v, double *h, double *l) {
+    if (!ctx || n < 0 || (n > 0 && (!a || !v || !h || !l))) return fail(ctx, FSG_E_ARG, "fsg_fvoigt: bad arguments");
+    if (n == 0) return FSG_OK;
+    cudaSetDevice(ctx->device);
+    size_t nb = sizeof(double) * n;
+    ALLOC(ctx->d_a, nb); ALLOC(ctx->d_v, nb); ALLOC(ctx->d_h, nb); ALLOC(ctx->d_l, nb);
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemcpyAsync(ctx->d_a.p, a, nb, cudaMemcpyHostToDevice, s), "fvoigt");
+    CK(cudaMemcpyAsync(ctx->d_v.p, v, nb, cudaMemcpyHostToDevice, s), "fvoigt");
+    fsg_launch_fvoigt(s, n, ctx->d_a.as<double>(), ctx->d_v.as<double>(), ctx->d_h.as<double>(), ctx->d_l.as<double>(), ctx->tab);
+    CK(cudaGetLastError(), "k_fvoigt");
+    CK(cudaMemcpyAsync(h, ctx->d_h.p, nb, cudaMemcpyDeviceToHost, s), "fvoigt");
+    CK(cudaMemcpyAsync(l, ctx->d_l.p, nb, cudaMemcpyDeviceToHost, s), "fvoigt");
+    CK(cudaStreamSynchronize(s), "fvoigt");
+    return FSG_OK;
+}
+
+int fsg_voigt_tables(fsg_ctx *ctx, float *vgt, float *fvt) {
+    if (!ctx) return FSG_E_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    if (vgt) CK(cudaMemcpyAsync(vgt, ctx->tab.vtab, sizeof(float) * FSG_NA1 * FSG_NV1, cudaMemcpyDeviceToHost, s), "tables");
+    if (fvt) CK(cudaMemcpyAsync(fvt, ctx->tab.fvtab, sizeof(float2) * FSG_NA1 * FSG_NV1, cudaMemcpyDeviceToHost, s), "tables");
+    CK(cudaStreamSynchronize(s), "tables");
+    return FSG_OK;
+}
+
+int fsg_locprf_pp(fsg_ctx *ctx, int nprof, int nmu, const double *xmu, int ntau, const double *xki,
+                  const double *src, const double *rhox, double *ploc) {
+    if (!ctx || nprof < 0 || nmu < 1 || ntau < 3 || !xmu || !xki || !src || !rhox || !ploc)
+        return fail(ctx, FSG_E_ARG, "fsg_locprf_pp: bad arguments");
+    if (nprof == 0) return FSG_OK;
+    cudaSetDevice(ctx->device);
+    size_t np = (size_t)nprof * ntau * sizeof(double);
+    DBuf bx, bs, br, bm, bp, bw;
+    int ok = bx.ensure(np) | bs.ensure(np) | br.ensure(sizeof(double) * ntau) | bm.ensure(sizeof(double) * nmu) |
+             bp.ensure(sizeof(double) * (size_t)nprof * nmu) | bw.ensure(3 * np);
+    int rc = FSG_OK;
+    cudaStream_t s = ctx->stream;
+    if (ok != FSG_OK) rc = fail(ctx, FSG_E_NOMEM, "fsg_locprf_pp: allocation failed");
+    else if (cudaMemcpyAsync(bx.p, xki, np, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+             cudaMemcpyAsync(bs.p, src, np, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+             cudaMemcpyAsync(br.p, rhox, sizeof(double) * ntau, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+             cudaMemcpyAsync(bm.p, xmu, sizeof(double) * nmu, cudaMemcpyHostToDevice, s) != cudaSuccess) rc = FSG_E_CUDA;
+    if (rc == FSG_OK) {
+        fsg_launch_locprf(s, nprof, nmu, bm.as<double>(), ntau, bx.as<double>(), bs.as<double>(), br.as<double>(),
+                          bp.as<double>(), bw.as<double>());
+        if (cudaMemcpyAsync(ploc, bp.p, sizeof(double) * (size_t)nprof * nmu, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) rc = cuda_fail(ctx, cudaGetLastError(), "locprf");
+    }
+    bx.release(); bs.release(); br.release(); bm.release(); bp.release(); bw.release();
+    return rc;
+}
+
+// ---- quadrature and Zeeman patterns (host set-up routines) -------------------------------------------
+static void legendre_p(int N, double Z, double *Pn, double *Pn1, double *Pn2) {
+    *Pn1 = 0.0; *Pn = 1.0; *Pn2 = 0.0;
+    for (int j = 1; j <= N; j++) { *Pn2 = *Pn1; *Pn1 = *Pn; *Pn = ((2.0 * j - 1.0) * Z * *Pn1 - (j - 1.0) * *Pn2) / j; }
+}
+
+static void gauss_mu(int quad, int N, double *X, double *W) {
+    double Z, Dz, Pn, Pn1, Pn2, F, Df;
+    if (quad == 1) {
+        for (int i = 1; i <= (N + 1) / 2; i++) {
+            Z = cos(FSG_PI * (i - 0.25) / (N + 0.5));
+            for (int it = 1; it <= 100; it++) {
+                legendre_p(N, Z, &Pn, &Pn1, &Pn2);
+                Df = N * (Z * Pn - Pn1) / (Z * Z - 1.0);
+                Dz = Pn / Df; Z = Z - Dz;
+                if (fabs(Dz) < 1e-15) break;
+            }
+            legendre_p(N, Z, &Pn, &Pn1, &Pn2);
+            Df = N * (Z * Pn - Pn1) / (Z * Z - 1.0);
+            X[i - 1] = 0.5 * (1.0 + Z); X[N - i] = 0.5 * (1.0 - Z);
+            W[i - 1] = 1.0 / ((1.0 - Z * Z) * Df * Df); W[N - i] = W[i - 1];
+        }
+    } else {
+        X[0] = 1.0; W[0] = 1.0 / (double)(N * N);
+        for (int i = 1; i <= N - 1; i++) {
+            Z = cos(2.0 * FSG_PI * i / (2.0 * N - 1.0));
+            for (int it = 1; it <= 100; it++) {
+                legendre_p(N, Z, &Pn, &Pn1, &Pn2);
+                F = Pn1 - Pn;
+                Df = ((N - 1) * (Z * Pn1 - Pn2) - N * (Z * Pn - Pn1)) / (Z * Z - 1.0);
+                Dz = F / Df; Z = Z - Dz;
+                if (fabs(Dz) < 1e-15) break;
+            }
+            legendre_p(N, Z, &Pn, &Pn1, &Pn2);
+            X[i] = 0.5 * (1.0 + Z);
+            W[i] = 0.5 * (1.0 + Z) / ((double)(N * N) * Pn1 * Pn1);
+        }
+    }
+}
+
+int fsg_mu_quadrature(int quad, int N, double *X, double *W, double *R, int setnodes) {
+    if (N < 1 || N > 64 || !X || !W || !R) return FSG_E_ARG;
+    if (N == 1) { if (setnodes) X[0] = 1.0; W[0] = 1.0; R[0] = 0.0; R[1] = 1.0; return FSG_OK; }
+    if (quad == 0) {
+        double Rmu[64];
+        if (setnodes) for (int i = 1; i <= N; i++) X[i - 1] = sqrt(fmax(0.0, 1.0 - ((double)i - 0.5) / (double)N));
+        for (int i = 0; i < N; i++) Rmu[i] = sqrt(1.0 - X[i] * X[i]);
+        R[0] = 0.0;
+        for (int i = 2; i <= N; i++) R[i - 1] = sqrt(0.5 * (Rmu[i - 2] * Rmu[i - 2] + Rmu[i - 1] * Rmu[i - 1]));
+        R[N] = 1.0;
+        for (int i = 1; i <= N; i++) W[i - 1] = R[i] * R[i] - R[i - 1] * R[i - 1];
+        return FSG_OK;
+    }
+    if (quad != 1 && quad != 2) return FSG_E_ARG;
+    double Xg[64], Wg[64];
+    gauss_mu(quad, N, Xg, Wg);
+    if (setnodes) for (int i = 0; i < N; i++) X[i] = Xg[i];
+    for (int i = 0; i < N; i++) W[i] = 2.0 * Wg[i] * Xg[i];
+    R[0] = 0.0;
+    for (int i = 1; i <= N - 1; i++) R[i] = sqrt(R[i - 1] * R[i - 1] + W[i - 1]);
+    R[N] = 1.0;
+    return FSG_OK;
+}
+
+static void merge_shifts(double *G, double *R, int *N, double Tol) {
+    double Gm[64], Rm[64]; int Nm = 0;
+    for (int i = 0; i < *N; i++) {
+        int found = 0;
+        for (int k = 0; k < Nm; k++) if (fabs(G[i] - Gm[k]) < Tol) { Rm[k] = Rm[k] + R[i]; found = 1; break; }
+        if (!found) { Gm[Nm] = G[i]; Rm[Nm] = R[i]; Nm++; }
+    }
+    for (int i = 0; i < Nm; i++) { G[i] = Gm[i]; R[i] = Rm[i]; }
+    *N = Nm;
+}
+
+int fsg_zeeman_pattern(float jlo, float jup, float glo, float gup, int32_t *npi, float *spi, float *rpi,
+                       int32_t *nsig, float *ssig, float *rsig) {
+    if (!npi || !spi || !rpi || !nsig || !ssig || !rsig || jup < 0 || jlo < 0 || jup > 30 || fabsf(jup - jlo) > 1.0f)
+        return FSG_E_ARG;
+    const double TolZ = 1e-5;
+    double Jl = jlo, Ju = jup, Gl = glo, Gu = gup;
+    int Nm = (int)lround(2.0 * Ju) + 1;
+    double gp[64], rp[64], gs[64], rs[64];
+    for (int i = 1; i <= Nm; i++) {
+        double m = Ju - (double)(i - 1);
+        gp[i - 1] = m * (Gu - Gl);
+        gs[i - 1] = m * Gu - (m + 1.0) * Gl;
+        if (Jl == Ju) { rp[i - 1] = m * m; rs[i - 1] = 0.25 * (Ju - m) * (Ju + m + 1.0); }
+        else if (Jl > Ju) { rp[i - 1] = (Ju + 1.0) * (Ju + 1.0) - m * m; rs[i - 1] = 0.25 * (Ju + m + 1.0) * (Ju + m + 2.0); }
+        else { rp[i - 1] = Ju * Ju - m * m; rs[i - 1] = 0.25 * (Ju - m) * (Ju - m - 1.0); }
+    }
+    for (int i = 0; i < Nm; i++) { if (fabs(gp[i]) < TolZ) gp[i] = 0.0; if (fabs(gs[i]) < TolZ) gs[i] = 0.0; }
+    int Np = 0, Ns = 0;
+    for (int i = 0; i < Nm; i++) if (fabs(rp[i]) > TolZ) { gp[Np] = gp[i]; rp[Np] = rp[i]; Np++; }
+    for (int i = 0; i < Nm; i++) if (fabs(rs[i]) > TolZ) { gs[Ns] = -gs[i]; rs[Ns] = rs[i]; Ns++; }
+    merge_shifts(gp, rp, &Np, TolZ);
+    merge_shifts(gs, rs, &Ns, TolZ);
+    double sm = 0.0; for (int i = 0; i < Np; i++) sm = sm + rp[i];
+    if (sm > 0.0) for (int i = 0; i < Np; i++) rp[i] = rp[i] / sm;
+    sm = 0.0; for (int i = 0; i < Ns; i++) sm = sm + rs[i];
+    if (sm > 0.0) for (int i = 0; i < Ns; i++) rs[i] = rs[i] / sm;
+    *npi = Np; *nsig = Ns;
+    for (int i = 0; i < Np; i++) { spi[i] = (float)gp[i]; rpi[i] = (float)rp[i]; }
+    for (int i = 0; i < Ns; i++) { ssig[i] = (float)gs[i]; rsig[i] = (float)rs[i]; }
+    return FSG_OK;
+}
+
+}  // extern "C"
+
+// ---- eval counting for the stats (sum over retained lines of Ntau x window) -------------------------
+__global__ void k_count_evals(int64_t n, const int32_t *flags, const int32_t *il, const int32_t *ir,
+                              unsigned long long *acc) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long v = 0;
+    if (i < n && !(flags[i] & FSG_F_WEAK)) v = (unsigned long long)(ir[i] - il[i] + 1);
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(acc, v);
+}
+
+double fsg_count_evals(fsg_ctx *ctx, int64_t n) {
+    unsigned long long *d = ctx->d_nkeep.as<unsigned long long>();
+    cudaMemsetAsync(d, 0, sizeof(unsigned long long), ctx->stream);
+    k_count_evals<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(n, ctx->d_flags.as<int32_t>(),
+        ctx->d_ileft.as<int32_t>(), ctx->d_iright.as<int32_t>(), d);
+    unsigned long long h = 0;
+    cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaStreamSynchronize(ctx->stream);
+    return (double)h * ctx->ntau;
+}

@@ -1,0 +1,92 @@
+// fsg_internal.cuh -- shared definitions of the B200 line-opacity / formal-solver library.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "../../include/fastspec_gpu.h"
+
+// ---- physical constants (shared.f90:20-33) --------------------------------------------------
+#define FSG_PI        3.141592653589793115997963468544185161590576171875
+#define FSG_VC        299792.458
+#define FSG_HC        6.62607015e-27
+#define FSG_KBOLT     1.380649e-16
+#define FSG_EV2ANG    8065.544005e-8
+#define FSG_A0        5.29177210903e-11
+#define FSG_M0        1.66053906660e-27
+#define FSG_CE        4.803204712e-10
+#define FSG_ME        9.1093837139e-28
+#define FSG_MH        1.673532499e-24
+#define FSG_HIE       13.598434005
+#define FSG_KZ        4.668644778e-13
+#define FSG_SQRTPIINV 0.56418958354775628695
+
+// ---- Voigt table geometry (voigt.f90:19-26) ------------------------------------------------
+#define FSG_NVV 1001
+#define FSG_NVA 401
+#define FSG_NV1 (FSG_NVV + 1)    // 1002 v nodes, v in [0, 8], dv = 0.008
+#define FSG_NA1 (FSG_NVA + 1)    // 402 a nodes, sqrt(a) uniform in [0, sqrt(8)]
+
+// Per-line flag bits (synth.f90:850 and opacity.f90:314): 0 weak, 1 molecule, 2 ABO,
+// 3 wide, 8..15 He I Stark table entry.
+#define FSG_F_WEAK 1
+#define FSG_F_MOL  2
+#define FSG_F_ABO  4
+#define FSG_F_WIDE 8
+
+// Per-depth precomputation of XlineInit (opacity.f90:65-93), FP64, one row each.
+enum { XI_NPRTB = 0, XI_GVWPRT, XI_TEMP6, XI_TEMP3, XI_KBT, XI_KBET, XI_T, XI_XNE, XI_RHO, XI_NROWS };
+
+// Device view of one atmosphere + grid + configuration (passed by value to kernels).
+struct AtmView {
+    int     ntau, nspc, nwl, wmode, motype, nhe, spc_he1, molbrd;
+    double  wfirst, wstart, dstep, rstep;
+    double  vturb2, epsopac, vwfudge, vwmol;
+    const double *xi;          // [XI_NROWS][ntau]
+    const float  *fpf;         // [nspc][ntau]   species-major (transposed on upload)
+    const float  *xamass, *potion;
+    const int    *ion;
+    const double *wave;        // [nwl] offsets from wfirst
+    const double *contopac;    // [nwl][ntau]
+    const double *contstd;     // [ntau] or null
+    const double *hegam, *heshf;   // [nhe][ntau] or null
+};
+
+// Device view of a line list (SoA, device pointers).
+struct LineView {
+    int64_t n;
+    int     kind;
+    const double  *wl;
+    const float   *elo, *gf, *grad, *gqst, *gvdw;
+    const int32_t *spc, *ismol, *ihe;
+};
+
+// XlineCoef (opacity.f90:43-58)
+struct XCoef {
+    double WaveL, Hnux, Elo, Gf, Grad, Xmass, Cqst, Qdiv, Cvdw, AboPre, AboVbc, AboExp;
+    int    IxPF, MdQst, MdVdw, IxHe;
+};
+
+// Fast-path record of one (line, depth): FP32 wing coefficients of HVoigt * LinCop.
+// For s = v^2 + a^2 >= 196 the reference evaluates (voigt.f90:100-101)
+//   H = a (s + 1/2) / (sqrt(pi) (s^2 - v^2 + a^2 + 1/4)),
+// which with x = v^2 and A = a^2 reads c1 (x + c2) / (x^2 + d1 x + d0), with
+//   c1 = LinCop a / sqrt(pi), c2 = A + 1/2, d1 = 2A - 1, d0 = A^2 + A + 1/4.
+struct __align__(16) WingRec { float vv2, c1, c2, d1; };
+struct __align__(16) CoreRec { float d0, vv, cop, a; };
+
+// Line header of a retained line inside a block (fast path).
+struct __align__(16) LineHdr { double wlc; int ileft, iright; };   // wlc = Wlcent (offset)
+
+// Error reporting
+std::string fsg_cuda_msg(cudaError_t e, const char *what);
+
+// Tables in device memory (built by fsg_tables.cu).
+struct VoigtTables {
+    float  *vtab;      // [402][1002]
+    float2 *fvtab;     // [402][1002] (H, L)
+    double *anode, *aida;   // [402] each
+};
+int fsg_build_tables(VoigtTables *t, cudaStream_t s, std::string *err);
+void fsg_free_tables(VoigtTables *t);

@@ -1,0 +1,665 @@
+// fsg_kernels64.cu -- FP64 kernels of the line-opacity / formal-solver path (built -fmad=false).
+//
+//   k_tables        VoigtInit / FVoigtInit (voigt.f90:42-72, 219-251) on the device
+//   k_xline_init    XlineInit (opacity.f90:65-93)
+//   k_center        LineopCalc central pass (synth.f90:833-907): XlineSetup + XlineDepth,
+//                   weak-line bound and centre tests, AnalyticWindow + WaveIdx windows
+//   k_params_fast   block refill (synth.f90:1049-1070) into FP32 wing/core records
+//   k_params_fp64   block refill into FP64 (LinCop, LinVvgt, LinAvgt) for the plain path
+//   k_span, k_accum_fp64, k_wide_fp64   plain FP64 LineOpacity1 gather (opacity.f90:297-346)
+//                   and the wide-line accumulation (synth.f90:981-1001)
+//   k_radtran       RadTranCalc (synth.f90:1825-1866) + DiskInteg quadrature (convol.f90:233-234)
+#include "fsg_fp64.cuh"
+
+#include <stdio.h>
+
+// ================================================================================================
+// Voigt tables: Chiarella-Reichel (1968) trapezoid sum with pole correction (voigt.f90:158-187,
+// 356-393).  Complex arithmetic as gfortran expands it: naive products, Smith's division.
+// ================================================================================================
+struct cd { double re, im; };
+__device__ __forceinline__ cd c_mul(cd a, cd b) {
+    double t1 = a.re * b.re, t2 = a.im * b.im, t3 = a.re * b.im, t4 = a.im * b.re;
+    return cd{ t1 - t2, t3 + t4 };
+}
+__device__ __forceinline__ cd c_div(cd a, cd b) {
+    double ratio, div, tr, ti;
+    if (fabs(b.re) < fabs(b.im)) {
+        ratio = b.re / b.im; div = (b.re * ratio) + b.im;
+        tr = (a.re * ratio) + a.im; ti = (a.im * ratio) - a.re;
+    } else {
+        ratio = b.im / b.re; div = (b.im * ratio) + b.re;
+        tr = (a.im * ratio) + a.re; ti = a.im - (a.re * ratio);
+    }
+    return cd{ tr / div, ti / div };
+}
+
+__device__ cd cr_sum(double a, double av) {
+    const double HH = 0.5;
+    cd z{ av, a }, z2 = c_mul(z, z);
+    cd s = c_div(cd{ 1.0, 0.0 }, z);
+    for (int n = 1; n <= 16; n++) {
+        double nh = (double)n * HH;
+        double e = exp(-nh * nh);
+        cd num{ (2.0 * z.re) * e, (2.0 * z.im) * e };
+        cd q = c_div(num, cd{ z2.re - nh * nh, z2.im });
+        s.re = s.re + q.re; s.im = s.im + q.im;
+    }
+    double c = HH / FSG_PI;
+    s = cd{ -(c * s.im), c * s.re };
+    if (a < 6.0) {
+        double p = 2.0 * FSG_PI * a / HH;
+        double th = 2.0 * FSG_PI * (2.0 * av - round(2.0 * av));
+        double sn = sin(0.5 * th);
+        double redd = -(2.0 * exp(0.5 * p) * sinh(0.5 * p)) + exp(p) * 2.0 * (sn * sn);
+        double imdd = exp(p) * sin(th);
+        double ex = exp(a * a - av * av), ang = -2.0 * a * av;
+        cd num{ 2.0 * (ex * cos(ang)), 2.0 * (ex * sin(ang)) };
+        cd q = c_div(num, cd{ redd, imdd });
+        s.re = s.re + q.re; s.im = s.im + q.im;
+    }
+    return s;
+}
+
+__global__ void k_tables(float *vtab, float2 *fvtab, double *anode, double *aida) {
+    const double dv = 8.0 / 1000.0, dt = 2.8284271247461903 / 400.0;
+    int iv = blockIdx.x * blockDim.x + threadIdx.x;   // 0..1001
+    int ia = blockIdx.y;                              // 0..401
+    double aa = ((double)ia * dt) * ((double)ia * dt);
+    if (iv == 0) {
+        anode[ia] = aa;
+        if (ia < FSG_NVA) {
+            double an1 = ((double)(ia + 1) * dt) * ((double)(ia + 1) * dt);
+            aida[ia] = 1.0 / (an1 - aa);
+        } else aida[ia] = 0.0;
+    }
+    if (iv >= FSG_NV1) return;
+    double vv = (double)iv * dv;
+    double h, l;
+    if (aa <= 0.0) {
+        h = exp(-fmin(vv * vv, 700.0));
+        int m = 2 * (int)llround(2.0 * vv);
+        double x0 = vv - 0.25 * (double)m, p = 0.0;
+        for (int n = -31; n <= 31; n += 2) {
+            double t = x0 - 0.25 * (double)n;
+            p = p + exp(-(t * t)) / (double)(m + n);
+        }
+        l = (2.0 / FSG_PI) * p;
+    } else {
+        cd s = cr_sum(aa, vv);
+        h = s.re; l = s.im;
+    }
+    vtab[ia * FSG_NV1 + iv] = (float)h;
+    fvtab[ia * FSG_NV1 + iv] = make_float2((float)h, (float)l);
+}
+
+int fsg_build_tables(VoigtTables *t, cudaStream_t s, std::string *err) {
+    cudaError_t e;
+    if ((e = cudaMalloc(&t->vtab, sizeof(float) * FSG_NA1 * FSG_NV1)) != cudaSuccess ||
+        (e = cudaMalloc(&t->fvtab, sizeof(float2) * FSG_NA1 * FSG_NV1)) != cudaSuccess ||
+        (e = cudaMalloc(&t->anode, sizeof(double) * FSG_NA1)) != cudaSuccess ||
+        (e = cudaMalloc(&t->aida, sizeof(double) * FSG_NA1)) != cudaSuccess) {
+        *err = fsg_cuda_msg(e, "table allocation");
+        return FSG_E_NOMEM;
+    }
+    dim3 grid((FSG_NV1 + 127) / 128, FSG_NA1);
+    k_tables<<<grid, 128, 0, s>>>(t->vtab, t->fvtab, t->anode, t->aida);
+    if ((e = cudaGetLastError()) != cudaSuccess) { *err = fsg_cuda_msg(e, "k_tables"); return FSG_E_CUDA; }
+    return FSG_OK;
+}
+
+void fsg_free_tables(VoigtTables *t) {
+    cudaFree(t->vtab); cudaFree(t->fvtab); cudaFree(t->anode); cudaFree(t->aida);
+    t->vtab = nullptr; t->fvtab = nullptr; t->anode = nullptr; t->aida = nullptr;
+}
+
+// ================================================================================================
+// XlineInit (opacity.f90:65-93): rows of A.xi
+// ================================================================================================
+__global__ void k_xline_init(int nt, const double *T, const double *xne, const double *rho,
+                             const float *h1, const float *he1, const float *h2, double h2brd,
+                             double *xi) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nt) return;
+    double Temp = T[t], Xne = xne[t];
+    double Vh = sqrt(2.0 * FSG_KBOLT * Temp / FSG_MH);
+    double np = (double)h1[t] + 0.412265 * (double)he1[t];
+    if (h2brd > 0.0) np = np + h2brd * 0.874307 * (double)h2[t];
+    const double erg2ev = 1e-7 / 1.602176634e-19;
+    xi[XI_NPRTB * nt + t] = np;
+    xi[XI_GVWPRT * nt + t] = 17.0 * pow(Vh, 0.6) * np;
+    xi[XI_TEMP6 * nt + t] = pow(Temp / 1e4, 1.0 / 6.0) * Xne;
+    xi[XI_TEMP3 * nt + t] = pow(Temp / 1e4, 0.3) * np;
+    xi[XI_KBT * nt + t] = FSG_KBOLT * Temp;
+    xi[XI_KBET * nt + t] = FSG_KBOLT * erg2ev * Temp;
+    xi[XI_T * nt + t] = Temp;
+    xi[XI_XNE * nt + t] = Xne;
+    xi[XI_RHO * nt + t] = rho[t];
+}
+
+void fsg_launch_xline_init(cudaStream_t s, int nt, const double *T, const double *xne, const double *rho,
+                           const float *h1, const float *he1, const float *h2, double h2brd, double *xi) {
+    k_xline_init<<<(nt + 127) / 128, 128, 0, s>>>(nt, T, xne, rho, h1, he1, h2, h2brd, xi);
+}
+
+// ================================================================================================
+// Central pass (synth.f90:833-907).  One thread per line, three sweeps over depth that recompute
+// XlineDepth instead of holding Ntau-long arrays: (1) LinCop bound test against the continuum,
+// (2) single-line opacity at the line centre (LineOpacity2), (3) AnalyticWindow.
+// ================================================================================================
+__device__ __forceinline__ double center_shift(const AtmView &A, int ihe, int t) {
+    return (ihe > 0) ? A.heshf[(ihe - 1) * A.ntau + t] : 0.0;
+}
+
+__global__ void k_center(AtmView A, LineView L, const float *__restrict__ vtab,
+                         const double *__restrict__ anode, const double *__restrict__ aida,
+                         int32_t *flags, int32_t *ileft, int32_t *iright, unsigned long long *nkeep) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L.n) return;
+    const int nt = A.ntau;
+    int f = line_input_flags(L, i, 0);
+    double wlc = L.wl[i] - A.wfirst;
+    XCoef XC;
+    xline_setup(A, L, i, wlc, f, &XC);
+    if (XC.IxHe > 0) f |= (XC.IxHe << 8);
+    int ihe = XC.IxHe;
+    int iwl = waveidx(A, wlc);
+    double dW = (wlc - A.wave[iwl - 1]) / (A.wave[iwl] - A.wave[iwl - 1]);
+    // (1) upper bound: H(a, v) <= 1 (synth.f90:876-887)
+    double mx = -1.0e308;
+    for (int t = 0; t < nt; t++) {
+        double dopl;
+        double cop = xline_cop(A, t, XC, &dopl);
+        double co = cont_center(A, iwl, dW, t);
+        double r = (A.motype == 1) ? cop / (co * A.contstd[t]) : cop / co;
+        mx = fmax(mx, r);
+    }
+    int il = 1, ir = A.nwl;
+    if (mx < A.epsopac) { f |= FSG_F_WEAK; }
+    else {
+        // (2) centre opacity (synth.f90:890-898; LineOpacity2 at Wl = Wlcent)
+        mx = -1.0e308;
+        for (int t = 0; t < nt; t++) {
+            double cop, vv, av;
+            xline_depth(A, t, XC, &cop, &vv, &av);
+            double dWl = 0.0;
+            if (ihe > 0) dWl = 0.0 - center_shift(A, ihe, t);
+            double lo = hvoigt64(vtab, anode, aida, av, dWl * vv) * cop;
+            if (A.motype == 1) lo = lo / A.contstd[t];
+            mx = fmax(mx, lo / cont_center(A, iwl, dW, t));
+        }
+        if (mx < A.epsopac) { f |= FSG_F_WEAK; }
+        else {
+            // (3) AnalyticWindow (opacity.f90:678-710) + WaveIdx (synth.f90:904-906)
+            const double iSqrtPi = 0.5641895835477563;
+            double dWwin = 0.0;
+            for (int t = 0; t < nt; t++) {
+                double cop, vv, av;
+                xline_depth(A, t, XC, &cop, &vv, &av);
+                double r = cop / (A.epsopac * cont_center(A, iwl, dW, t));
+                if (A.motype == 1) r = r / A.contstd[t];
+                if (r <= 1.0) continue;
+                double w = sqrt(log(r) + fmax(0.0, av * (r * iSqrtPi - av))) / vv;
+                if (ihe > 0) w = w + fabs(center_shift(A, ihe, t));
+                dWwin = fmax(dWwin, w);
+            }
+            il = waveidx(A, wlc - dWwin);
+            ir = waveidx(A, wlc + dWwin) + 1;
+            if (ir > A.nwl) ir = A.nwl;
+        }
+    }
+    flags[i] = f; ileft[i] = il; iright[i] = ir;
+    // warp-aggregated count of retained lines
+    unsigned m = __ballot_sync(__activemask(), !(f & FSG_F_WEAK));
+    if ((threadIdx.x & 31) == (__ffs(__activemask()) - 1) && m) atomicAdd(nkeep, (unsigned long long)__popc(m));
+}
+
+void fsg_launch_center(cudaStream_t s, const AtmView &A, const LineView &L, const VoigtTables &T,
+                       int32_t *flags, int32_t *ileft, int32_t *iright, unsigned long long *nkeep) {
+    if (L.n <= 0) return;
+    unsigned nb = (unsigned)((L.n + 127) / 128);
+    k_center<<<nb, 128, 0, s>>>(A, L, T.vtab, T.anode, T.aida, flags, ileft, iright, nkeep);
+}
+
+// ================================================================================================
+// Block refill: per retained line of the block, XlineSetup once then XlineDepth over depths.
+// ================================================================================================
+__global__ void k_params_fast(AtmView A, LineView L, const int64_t *__restrict__ idx, int64_t j0,
+                              int64_t nb, const int32_t *__restrict__ flags,
+                              const int32_t *__restrict__ ileft, const int32_t *__restrict__ iright,
+                              WingRec *wing, CoreRec *core, LineHdr *hdr) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nb) return;
+    int64_t i = idx[j0 + j];
+    const int nt = A.ntau;
+    int f = flags[i];
+    double wlc = L.wl[i] - A.wfirst;
+    XCoef XC;
+    xline_setup(A, L, i, wlc, f, &XC);
+    LineHdr h; h.wlc = wlc; h.ileft = ileft[i]; h.iright = iright[i];
+    hdr[j] = h;
+    for (int t = 0; t < nt; t++) {
+        double cop, vv, av;
+        xline_depth(A, t, XC, &cop, &vv, &av);
+        if (A.motype == 1) cop = cop / A.contstd[t];     // LineOpacity1 divides the sum by ContOpacStd
+        double a2 = av * av;
+        WingRec w;
+        w.vv2 = (float)(vv * vv);
+        w.c1 = (float)(cop * av * FSG_SQRTPIINV);
+        w.c2 = (float)(a2 + 0.5);
+        w.d1 = (float)(2.0 * a2 - 1.0);
+        CoreRec c;
+        c.d0 = (float)(a2 * a2 + a2 + 0.25);
+        c.vv = (float)vv; c.cop = (float)cop; c.a = (float)av;
+        wing[(size_t)j * nt + t] = w;
+        core[(size_t)j * nt + t] = c;
+    }
+}
+
+void fsg_launch_params_fast(cudaStream_t s, const AtmView &A, const LineView &L, const int64_t *idx,
+                            int64_t j0, int64_t nb, const int32_t *flags, const int32_t *ileft,
+                            const int32_t *iright, WingRec *wing, CoreRec *core, LineHdr *hdr) {
+    if (nb <= 0) return;
+    k_params_fast<<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(A, L, idx, j0, nb, flags, ileft, iright,
+                                                               wing, core, hdr);
+}
+
+// FP64 parameters for the plain path: p64[j][t] = (LinCop, LinVvgt, LinAvgt)
+__global__ void k_params_fp64(AtmView A, LineView L, int64_t i0, int64_t nb,
+                              const int32_t *__restrict__ flags, double3 *p64) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nb) return;
+    int64_t i = i0 + j;
+    int f = flags[i];
+    if (f & FSG_F_WEAK) return;
+    double wlc = L.wl[i] - A.wfirst;
+    XCoef XC;
+    xline_setup(A, L, i, wlc, f, &XC);
+    for (int t = 0; t < A.ntau; t++) {
+        double cop, vv, av;
+        xline_depth(A, t, XC, &cop, &vv, &av);
+        p64[(size_t)j * A.ntau + t] = make_double3(cop, vv, av);
+    }
+}
+
+void fsg_launch_params_fp64(cudaStream_t s, const AtmView &A, const LineView &L, int64_t i0, int64_t nb,
+                            const int32_t *flags, double3 *p64) {
+    if (nb <= 0) return;
+    k_params_fp64<<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(A, L, i0, nb, flags, p64);
+}
+
+// ================================================================================================
+// Plain FP64 path: Lstart/Lstop pointers (synth.f90:955-978), wide lines (synth.f90:981-1001)
+// and the per-wavelength gather LineOpacity1 (opacity.f90:297-346).
+// ================================================================================================
+__global__ void k_span(int64_t n, const int32_t *flags, const int32_t *ileft, const int32_t *iright,
+                       int *lstart, int *lstop) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int f = flags[i];
+    if ((f & FSG_F_WEAK) || (f & FSG_F_WIDE)) return;
+    for (int w = ileft[i]; w <= iright[i]; w++) {
+        atomicMin(&lstart[w - 1], (int)(i + 1));
+        atomicMax(&lstop[w - 1], (int)(i + 1));
+    }
+}
+
+void fsg_launch_span(cudaStream_t s, int64_t n, const int32_t *flags, const int32_t *ileft,
+                     const int32_t *iright, int *lstart, int *lstop) {
+    if (n <= 0) return;
+    k_span<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(n, flags, ileft, iright, lstart, lstop);
+}
+
+// One warp per wavelength; lanes stride the depths.  Lines l1..l2 (1-based), block offset loff.
+#define FP64_MAXD 4   // up to 128 depths
+__global__ void k_accum_fp64(AtmView A, const double *__restrict__ wl, int iwl1, int iwl2,
+                             const int *__restrict__ lstart, const int *__restrict__ lstop,
+                             const int32_t *__restrict__ flags, const int32_t *__restrict__ ileft,
+                             const int32_t *__restrict__ iright, int64_t loff, const double3 *__restrict__ p64,
+                             const float *__restrict__ vtab, const double *__restrict__ anode,
+                             const double *__restrict__ aida, double *lineopac, double *evals) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    int iwl = iwl1 + warp;
+    if (iwl > iwl2) return;
+    const int nt = A.ntau;
+    double acc[FP64_MAXD];
+#pragma unroll
+    for (int k = 0; k < FP64_MAXD; k++) acc[k] = 0.0;
+    double Wl = A.wave[iwl - 1];
+    int l1 = lstart[iwl - 1], l2 = lstop[iwl - 1];
+    double cnt = 0.0;
+    for (int il = l1; il <= l2; il++) {
+        int f = flags[il - 1];
+        if ((f & FSG_F_WEAK) || (f & FSG_F_WIDE) || iwl < ileft[il - 1] || iwl > iright[il - 1]) continue;
+        int ihe = (f >> 8) & 255;
+        double dWl0 = Wl - (wl[il - 1] - A.wfirst);
+        const double3 *p = p64 + (size_t)(il - 1 - loff) * nt;
+#pragma unroll
+        for (int k = 0; k < FP64_MAXD; k++) {
+            int t = lane + 32 * k;
+            if (t < nt) {
+                double dWl = dWl0;
+                if (ihe > 0) dWl = dWl0 - A.heshf[(ihe - 1) * nt + t];
+                double3 q = p[t];
+                double V = dWl * q.y;
+                acc[k] = acc[k] + hvoigt64(vtab, anode, aida, q.z, V) * q.x;
+            }
+        }
+        cnt += 1.0;
+    }
+    double *dst = lineopac + (size_t)(iwl - 1) * nt;
+#pragma unroll
+    for (int k = 0; k < FP64_MAXD; k++) {
+        int t = lane + 32 * k;
+        if (t < nt) {
+            double v = acc[k];
+            if (A.motype == 1) v = v / A.contstd[t];
+            dst[t] = dst[t] + v;
+        }
+    }
+    if (lane == 0 && cnt > 0.0) atomicAdd(evals, cnt * nt);
+}
+
+void fsg_launch_accum_fp64(cudaStream_t s, const AtmView &A, const double *wl, int iwl1, int iwl2,
+                           const int *lstart, const int *lstop, const int32_t *flags, const int32_t *ileft,
+                           const int32_t *iright, int64_t loff, const double3 *p64, const VoigtTables &T,
+                           double *lineopac, double *evals) {
+    int nw = iwl2 - iwl1 + 1;
+    if (nw <= 0) return;
+    k_accum_fp64<<<(nw + 7) / 8, 256, 0, s>>>(A, wl, iwl1, iwl2, lstart, lstop, flags, ileft, iright, loff,
+                                              p64, T.vtab, T.anode, T.aida, lineopac, evals);
+}
+
+// Wide lines, in line order, each over its own window (LineOpacity2): one warp per wavelength,
+// looping over the wide-line list so the per-wavelength additions keep the reference's order.
+__global__ void k_wide_fp64(AtmView A, LineView L, int nwide, const int64_t *__restrict__ widx,
+                            const int32_t *__restrict__ flags, const int32_t *__restrict__ ileft,
+                            const int32_t *__restrict__ iright, const double3 *__restrict__ pw,
+                            const float *__restrict__ vtab, const double *__restrict__ anode,
+                            const double *__restrict__ aida, int wlo, int whi, double *lineopac,
+                            double *evals) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    int iwl = wlo + warp;
+    if (iwl > whi) return;
+    const int nt = A.ntau;
+    double Wl = A.wave[iwl - 1];
+    double *dst = lineopac + (size_t)(iwl - 1) * nt;
+    double cnt = 0.0;
+    for (int q = 0; q < nwide; q++) {
+        int64_t i = widx[q];
+        if (iwl < ileft[i] || iwl > iright[i]) continue;
+        int f = flags[i], ihe = (f >> 8) & 255;
+        double dWl0 = Wl - (L.wl[i] - A.wfirst);
+        for (int t = lane; t < nt; t += 32) {
+            double dWl = dWl0;
+            if (ihe > 0) dWl = dWl0 - A.heshf[(ihe - 1) * nt + t];
+            double3 p = pw[(size_t)q * nt + t];
+            double v = hvoigt64(vtab, anode, aida, p.z, dWl * p.y) * p.x;
+            if (A.motype == 1) v = v / A.contstd[t];
+            dst[t] = dst[t] + v;
+        }
+        cnt += 1.0;
+    }
+    if (lane == 0 && cnt > 0.0) atomicAdd(evals, cnt * nt);
+}
+
+__global__ void k_params_wide(AtmView A, LineView L, int nwide, const int64_t *widx,
+                              const int32_t *flags, double3 *pw) {
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nwide) return;
+    int64_t i = widx[q];
+    double wlc = L.wl[i] - A.wfirst;
+    XCoef XC;
+    xline_setup(A, L, i, wlc, flags[i], &XC);
+    for (int t = 0; t < A.ntau; t++) {
+        double cop, vv, av;
+        xline_depth(A, t, XC, &cop, &vv, &av);
+        pw[(size_t)q * A.ntau + t] = make_double3(cop, vv, av);
+    }
+}
+
+void fsg_launch_wide_fp64(cudaStream_t s, const AtmView &A, const LineView &L, int nwide, const int64_t *widx,
+                          const int32_t *flags, const int32_t *ileft, const int32_t *iright, double3 *pw,
+                          const VoigtTables &T, int wlo, int whi, double *lineopac, double *evals) {
+    if (nwide <= 0 || whi < wlo) return;
+    k_params_wide<<<(nwide + 63) / 64, 64, 0, s>>>(A, L, nwide, widx, flags, pw);
+    int nw = whi - wlo + 1;
+    k_wide_fp64<<<(nw + 7) / 8, 256, 0, s>>>(A, L, nwide, widx, flags, ileft, iright, pw, T.vtab, T.anode,
+                                             T.aida, wlo, whi, lineopac, evals);
+}
+
+// ================================================================================================
+// RadTranCalc + disk integration.  A CTA takes RT_LW wavelengths; the two opacity columns
+// (continuum, continuum + line) of each wavelength are staged in shared memory with coalesced
+// loads, TauStep / CentDer / U run over depths in parallel, then one thread per
+// (wavelength, kind, mu) sweeps the depths (LocPrfPP, solver.f90:123-179).
+// ================================================================================================
+#define RT_LW 8
+#define RT_MAXT 128
+#define RT_MAXMU 16
+
+__global__ void k_radtran(AtmView A, const double *__restrict__ lineopac, const double *__restrict__ rhox,
+                          int nmu, const double *__restrict__ xmu, const double *__restrict__ wmu,
+                          double *spl, double *spc, double *sfl, double *sfc) {
+    extern __shared__ double sm[];
+    const int nt = A.ntau;
+    const int w0 = blockIdx.x * RT_LW;
+    const int nw = min(RT_LW, A.nwl - w0);
+    // layout: X[kind][w][t], S[w][t], D[kind][w][t], R[kind][w][t] (derivative), U[kind][w][t]
+    double *X = sm, *S = X + 2 * RT_LW * nt, *D = S + RT_LW * nt, *R = D + 2 * RT_LW * nt,
+           *U = R + 2 * RT_LW * nt, *I = U + 2 * RT_LW * nt;      // I[kind][w][mu]
+    const double PlkC1 = FSG_HC * FSG_VC * 1e13 / FSG_KBOLT;
+    for (int e = threadIdx.x; e < nw * nt; e += blockDim.x) {
+        int w = e / nt, t = e - w * nt;
+        size_t g = (size_t)(w0 + w) * nt + t;
+        double c = A.contopac[g];
+        X[(0 * RT_LW + w) * nt + t] = c;
+        X[(1 * RT_LW + w) * nt + t] = c + lineopac[g];
+        double wl = A.wave[w0 + w] + A.wfirst;
+        double C1 = PlkC1 / wl, C2 = exp(50.7649141 - 5.0 * log(wl));
+        S[w * nt + t] = C2 / (exp(C1 / A.xi[XI_T * nt + t]) - 1.0);
+    }
+    __syncthreads();
+    // TauStep at mu = 1 (solver.f90:591-615)
+    for (int e = threadIdx.x; e < 2 * nw * nt; e += blockDim.x) {
+        int kw = e / nt, t = e - kw * nt;            // kw = kind * nw + w
+        int kind = kw / nw, w = kw - kind * nw;
+        const double *x = X + (kind * RT_LW + w) * nt;
+        double *d = D + (kind * RT_LW + w) * nt;
+        if (t == 0) {
+            double Dx1 = (rhox[1] - rhox[0]) / 1.0;
+            double Yp = (x[1] - x[0]) / Dx1;
+            d[0] = Dx1 * (x[1] + 2.0 * x[0] + Dx1 / 2.0 * Yp) / 3.0;
+        } else if (t < nt - 1) {
+            int k = t + 1;
+            double Dx = (rhox[k - 1] - rhox[k - 2]) / 1.0, Dx1 = (rhox[k] - rhox[k - 1]) / 1.0;
+            double Der = (x[k - 1] - x[k - 2]) / Dx, Der1 = (x[k] - x[k - 1]) / Dx1, Yp;
+            if (Der * Der1 > 0.0) {
+                double Lambda = (1.0 + Dx1 / (Dx + Dx1)) / 3.0;
+                Yp = (Der / (Lambda * Der1 + (1.0 - Lambda) * Der)) * Der1;
+            } else Yp = 0.0;
+            d[k - 1] = Dx1 * (x[k] + 2.0 * x[k - 1] + Dx1 / 2.0 * Yp) / 3.0;
+        } else d[nt - 1] = 0.0;
+    }
+    __syncthreads();
+    // CentDer of the source function on each Deltau scale (solver.f90:618-647)
+    for (int e = threadIdx.x; e < 2 * nw * nt; e += blockDim.x) {
+        int kw = e / nt, t = e - kw * nt;
+        int kind = kw / nw, w = kw - kind * nw;
+        const double *d = D + (kind * RT_LW + w) * nt, *y = S + w * nt;
+        double *r = R + (kind * RT_LW + w) * nt;
+        if (t == 0) r[0] = (y[1] - y[0]) / d[0];
+        else if (t == nt - 1) r[nt - 1] = (y[nt - 1] - y[nt - 2]) / d[nt - 2];
+        else {
+            int k = t + 1;
+            double Dx = d[k - 2], Dx1 = d[k - 1];
+            double InvDx = 1.0 / Dx, InvDx1 = 1.0 / Dx1;
+            double Lambda = (1.0 + Dx1 / (Dx + Dx1)) / 3.0, Lambda1 = 1.0 - Lambda;
+            double Der = (y[k - 1] - y[k - 2]) * InvDx, Der1 = (y[k] - y[k - 1]) * InvDx1;
+            r[k - 1] = (Der * Der1 > 0.0) ? (Der / (Lambda * Der1 + Lambda1 * Der)) * Der1 : 0.0;
+        }
+    }
+    __syncthreads();
+    // Bezier control term U (solver.f90:136-138)
+    for (int e = threadIdx.x; e < 2 * nw * nt; e += blockDim.x) {
+        int kw = e / nt, t = e - kw * nt;
+        int kind = kw / nw, w = kw - kind * nw;
+        if (t >= nt - 1) continue;
+        const double *d = D + (kind * RT_LW + w) * nt, *r = R + (kind * RT_LW + w) * nt, *y = S + w * nt;
+        U[(kind * RT_LW + w) * nt + t] = 0.5 * (y[t] + 0.5 * d[t] * r[t] + y[t + 1] - 0.5 * d[t] * r[t + 1]);
+    }
+    __syncthreads();
+    // sweeps: one thread per (kind, w, mu)
+    for (int e = threadIdx.x; e < 2 * nw * nmu; e += blockDim.x) {
+        int kw = e / nmu, im = e - kw * nmu;
+        int kind = kw / nw, w = kw - kind * nw;
+        const double *d = D + (kind * RT_LW + w) * nt, *u = U + (kind * RT_LW + w) * nt, *y = S + w * nt;
+        double Imu = 1.0 / xmu[im], Y = y[nt - 1];
+        for (int k = nt - 2; k >= 0; k--) {
+            double Eps, Alpha, Beta, Gamma;
+            delo_coef(d[k] * Imu, Eps, Alpha, Beta, Gamma);
+            Y = Y * Eps + Alpha * y[k] + Beta * y[k + 1] + Gamma * u[k];
+        }
+        I[(kind * RT_LW + w) * nmu + im] = Y;
+        double *out = (kind == 0) ? spc : spl;
+        if (out) out[(size_t)(w0 + w) * nmu + im] = Y;
+    }
+    __syncthreads();
+    // disk integration without broadening: Sf = sum over mu of Sp * Wmu (convol.f90:233-234)
+    for (int e = threadIdx.x; e < 2 * nw; e += blockDim.x) {
+        int kind = e / nw, w = e - kind * nw;
+        double a = 0.0;
+        for (int im = 0; im < nmu; im++) a = a + I[(kind * RT_LW + w) * nmu + im] * wmu[im];
+        double *out = (kind == 0) ? sfc : sfl;
+        if (out) out[w0 + w] = a;
+    }
+}
+
+size_t fsg_radtran_smem(int nt, int nmu) {
+    return sizeof(double) * ((size_t)(2 + 1 + 2 + 2 + 2) * RT_LW * nt + 2 * RT_LW * nmu);
+}
+
+int fsg_launch_radtran(cudaStream_t s, const AtmView &A, const double *lineopac, const double *rhox,
+                       int nmu, const double *xmu, const double *wmu, double *spl, double *spc,
+                       double *sfl, double *sfc) {
+    size_t sm = fsg_radtran_smem(A.ntau, nmu);
+    static int attr_set = 0;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_radtran, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        attr_set = 1;
+    }
+    int nb = (A.nwl + RT_LW - 1) / RT_LW;
+    k_radtran<<<nb, 128, sm, s>>>(A, lineopac, rhox, nmu, xmu, wmu, spl, spc, sfl, sfc);
+    return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
+}
+
+// ================================================================================================
+// Elemental HVoigt / FVoigt over arrays (kernel-level entry points)
+// ================================================================================================
+__global__ void k_hvoigt(int64_t n, const double *a, const double *v, double *h, const float *vtab,
+                         const double *anode, const double *aida) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) h[i] = hvoigt64(vtab, anode, aida, a[i], v[i]);
+}
+
+__global__ void k_fvoigt(int64_t n, const double *a, const double *v, double *h, double *l,
+                         const float2 *fvtab, const double *anode, const double *aida) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    // FVoigt (voigt.f90:256-299): same a-state rule as HVoigt
+    double A = a[i], V = v[i], av = fabs(V), vg, fv;
+    if (A < 8.0 && av < 8.0) {
+        VLine64 L;
+        L.A = A;
+        if (A < anode[1]) { L.IA = 1; L.UA = A * aida[0]; }
+        else { L = vline64(anode, aida, A); }
+        fvoigt_line64(fvtab, L, V, &vg, &fv);
+    } else { fv_asym64(A, av, &vg, &fv); fv = copysign(fabs(fv), V); }
+    h[i] = vg; l[i] = fv;
+}
+
+void fsg_launch_hvoigt(cudaStream_t s, int64_t n, const double *a, const double *v, double *h,
+                       const VoigtTables &T) {
+    if (n > 0) k_hvoigt<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, a, v, h, T.vtab, T.anode, T.aida);
+}
+void fsg_launch_fvoigt(cudaStream_t s, int64_t n, const double *a, const double *v, double *h, double *l,
+                       const VoigtTables &T) {
+    if (n > 0) k_fvoigt<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, a, v, h, l, T.fvtab, T.anode, T.aida);
+}
+
+// LocPrfPP over independent profiles: one thread per profile (kernel-level entry point)
+__global__ void k_locprf(int nprof, int nmu, const double *xmu, int nt, const double *xki,
+                         const double *src, const double *rhox, double *ploc, double *work) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nprof) return;
+    const double *x = xki + (size_t)p * nt, *y = src + (size_t)p * nt;
+    double *d = work + (size_t)p * 3 * nt, *r = d + nt, *u = r + nt;
+    // TauStep
+    {
+        double Dx1 = (rhox[1] - rhox[0]) / 1.0, Yp = (x[1] - x[0]) / Dx1;
+        d[0] = Dx1 * (x[1] + 2.0 * x[0] + Dx1 / 2.0 * Yp) / 3.0;
+        for (int k = 2; k <= nt - 1; k++) {
+            double Dx = (rhox[k - 1] - rhox[k - 2]) / 1.0; Dx1 = (rhox[k] - rhox[k - 1]) / 1.0;
+            double Der = (x[k - 1] - x[k - 2]) / Dx, Der1 = (x[k] - x[k - 1]) / Dx1;
+            if (Der * Der1 > 0.0) {
+                double Lambda = (1.0 + Dx1 / (Dx + Dx1)) / 3.0;
+                Yp = (Der / (Lambda * Der1 + (1.0 - Lambda) * Der)) * Der1;
+            } else Yp = 0.0;
+            d[k - 1] = Dx1 * (x[k] + 2.0 * x[k - 1] + Dx1 / 2.0 * Yp) / 3.0;
+        }
+    }
+    for (int k = 2; k <= nt - 1; k++) {
+        double Dx = d[k - 2], Dx1 = d[k - 1];
+        double InvDx = 1.0 / Dx, InvDx1 = 1.0 / Dx1;
+        double Lambda = (1.0 + Dx1 / (Dx + Dx1)) / 3.0, Lambda1 = 1.0 - Lambda;
+        double Der = (y[k - 1] - y[k - 2]) * InvDx, Der1 = (y[k] - y[k - 1]) * InvDx1;
+        r[k - 1] = (Der * Der1 > 0.0) ? (Der / (Lambda * Der1 + Lambda1 * Der)) * Der1 : 0.0;
+    }
+    r[0] = (y[1] - y[0]) / d[0];
+    r[nt - 1] = (y[nt - 1] - y[nt - 2]) / d[nt - 2];
+    for (int k = 0; k < nt - 1; k++) u[k] = 0.5 * (y[k] + 0.5 * d[k] * r[k] + y[k + 1] - 0.5 * d[k] * r[k + 1]);
+    for (int im = 0; im < nmu; im++) {
+        double Imu = 1.0 / xmu[im], Y = y[nt - 1];
+        for (int k = nt - 2; k >= 0; k--) {
+            double Eps, Alpha, Beta, Gamma;
+            delo_coef(d[k] * Imu, Eps, Alpha, Beta, Gamma);
+            Y = Y * Eps + Alpha * y[k] + Beta * y[k + 1] + Gamma * u[k];
+        }
+        ploc[(size_t)p * nmu + im] = Y;
+    }
+}
+
+void fsg_launch_locprf(cudaStream_t s, int nprof, int nmu, const double *xmu, int nt, const double *xki,
+                       const double *src, const double *rhox, double *ploc, double *work) {
+    if (nprof > 0) k_locprf<<<(nprof + 127) / 128, 128, 0, s>>>(nprof, nmu, xmu, nt, xki, src, rhox, ploc, work);
+}
+
+// ================================================================================================
+// MarkWideLines (synth.f90:709-744) over the (packed) line arrays; WlcIdx (synth.f90:677-706)
+// ================================================================================================
+__device__ __forceinline__ int64_t wlc_idx(const double *wl, double wfirst, int64_t n, double w) {
+    if (n == 0 || w < wl[0] - wfirst) return 0;
+    int64_t ia = 1, ib = n;
+    while (ib - ia > 1) {
+        int64_t im = (ia + ib) / 2;
+        if (wl[im - 1] - wfirst <= w) ia = im; else ib = im;
+    }
+    return (wl[ib - 1] - wfirst <= w) ? ib : ia;
+}
+
+__global__ void k_mark_wide(AtmView A, int64_t n, const double *wl, int64_t nstep, int32_t *flags,
+                            const int32_t *ileft, const int32_t *iright, unsigned long long *nwide) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int f = flags[i];
+    if (f & FSG_F_WEAK) return;
+    double wr = A.wave[iright[i] - 1], wlft = A.wave[ileft[i] - 1];
+    int64_t nrec = wlc_idx(wl, A.wfirst, n, wr) - wlc_idx(wl, A.wfirst, n, wlft) + 1;
+    double dv = FSG_VC * (wr - wlft) / ((wl[i] - A.wfirst) + A.wfirst);
+    if (nrec > nstep / 2 || dv > 5e3) { flags[i] = f | FSG_F_WIDE; atomicAdd(nwide, 1ull); }
+}
+
+void fsg_launch_mark_wide(cudaStream_t s, const AtmView &A, int64_t n, const double *wl, int64_t nstep,
+                          int32_t *flags, const int32_t *ileft, const int32_t *iright, unsigned long long *nwide) {
+    if (n > 0) k_mark_wide<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(A, n, wl, nstep, flags, ileft, iright, nwide);
+}

@@ -1,0 +1,164 @@
+/*
+ * fastspec_gpu.h -- C-ABI of the B200 line-opacity -> formal-solver path of FastSpec.
+ *
+ * The reference is a Fortran 90 program whose drivers exchange data through module globals
+ * (shared.f90:447-548).  This ABI is what its ISO_C_BINDING shim would bind in their place:
+ * plain pointers and sizes, no CUDA or torch types.  Every entry point returns 0 on success
+ * or a negative FSG_E* code; fsg_last_error() gives the message.  The Fortran shim maps a
+ * nonzero status to ErrStop (utils.f90:201), the reference's fatal-error path.
+ *
+ * Conventions (the reference's, seen from C):
+ *   - arrays are Fortran column-major: LineOpac(Ntau,Nwl) -> double[nwl][ntau],
+ *     MagLineOpac(6,Ntau,Nwl) -> double[nwl][ntau][6], SpL/SpC(Nmu,Nwl) -> double[nwl][nmu],
+ *     SpZ(Nmu,4,Nwl) -> double[nwl][4][nmu], FractionPF(Maxspl,Ntau) -> float[ntau][nspc];
+ *   - line and wavelength indices on output are 1-based (Ileft, Iright as the reference);
+ *   - the caller owns every host array; the context owns device buffers;
+ *   - a context is not thread-safe; use one per host thread (each has its own stream).
+ * Functions with a _dev suffix take DEVICE pointers (inputs already resident in HBM).
+ */
+#ifndef FASTSPEC_GPU_H
+#define FASTSPEC_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FSG_OK            0
+#define FSG_E_ARG        -1   /* invalid argument (sizes, null pointers, ranges) */
+#define FSG_E_CUDA       -2   /* CUDA runtime error */
+#define FSG_E_NOMEM      -3   /* device or host allocation failed */
+#define FSG_E_STATE      -4   /* call order: grid / atmosphere / continuum not set */
+#define FSG_E_SEGMENT    -5   /* lines at one wavelength exceed the block capacity */
+#define FSG_E_TIMEOUT    -6   /* a bounded device wait gave up (error word set) */
+
+#define FSG_PREC_MIXED    0   /* FP32 Voigt + compensated on-chip sums, FP64 prefactors */
+#define FSG_PREC_FP64     1   /* plain FP64-faithful path: per-wavelength gather as LineOpacity1 */
+
+typedef struct fsg_ctx fsg_ctx;
+
+/* Configuration: the Config-module fields the hot path reads (shared.f90:416-443). */
+typedef struct {
+    int    device;        /* CUDA device ordinal */
+    int    precision;     /* FSG_PREC_MIXED or FSG_PREC_FP64 */
+    double vmicro;        /* VMIC [km/s] */
+    double epsopac;       /* EPSOPAC, line inclusion threshold (default 1e-4) */
+    double vwfudge;       /* VWFUDGE (default 1) */
+    double h2brd;         /* H2BRD (default 0) */
+    double vwmol;         /* VWMOL (default 0) */
+    int    molbrd;        /* MOLBRD 0/1 */
+    double limitram_gb;   /* LIMITRAM: cap of the per-block line parameter buffers [GB] */
+} fsg_config;
+
+/* Line list, structure of arrays (LineData records, shared.f90:451-482).
+ * kind: 0 LineTypeAtm (HDF atomic), 1 LineTypeMol (single-species molecular), 2 LineTypeMag
+ * (ASCII .z / magnetic).  ismol: molecule flag of LineTypeMag records (IsMolecule).
+ * ihe: He I Stark table entry (HeMatchIdx, 1-based) or 0; may be NULL.
+ * Zeeman components (magnetic lists only; NULL otherwise): line i owns npi[i] pi components at
+ * spl_pi[pi_off[i] ...] / str_pi[...] and nsi[i] sigma components (blue half first, then red,
+ * as ReadAscMag stores them, ioutils.f90:1393-1410).  Shifts are in the reader's units
+ * (Lande-type factors), scaled by Kz |B| lambda^2 inside fsg_mag_lineop_calc. */
+typedef struct {
+    int64_t       n;
+    const double *wl;                 /* air wavelength [A], sorted ascending */
+    const float  *elo, *gf, *grad, *gqst, *gvdw;
+    const int32_t *spc;               /* species index 0..nspc-1 */
+    int32_t       kind;               /* one kind for the whole list */
+    const int32_t *ismol;             /* may be NULL (all 0) */
+    const int32_t *ihe;               /* may be NULL */
+    const int32_t *npi, *nsi;
+    const int64_t *pi_off, *si_off;
+    const float   *spl_pi, *str_pi, *spl_si, *str_si;
+} fsg_lines;
+
+typedef struct {
+    int64_t nlines_in, nlines_used, nwide, nweak, nblocks;
+    double  line_evals;     /* profile evaluations inside windows (x components if magnetic) */
+    double  ms_center, ms_params, ms_accum, ms_total;   /* device time per stage [ms] */
+} fsg_stats;
+
+/* ---- context ------------------------------------------------------------------------- */
+int         fsg_create(const fsg_config *cfg, fsg_ctx **out);
+void        fsg_destroy(fsg_ctx *ctx);
+const char *fsg_last_error(const fsg_ctx *ctx);
+int         fsg_version(void);
+
+/* ---- set-up (the reference's Init, synth.f90:22-331) ------------------------------------ */
+/* Wavelength grid of Init (synth.f90:56-74): wave[] = offsets from wstart.  Returns Nwl in
+ * *nwl; wave may be NULL to query the size.  Host computation: set-up, not hot path. */
+int fsg_make_grid(int wmode, double wstart, double wend, double dstep, double *wave, int *nwl);
+/* Upload the grid (wave = offsets from wfirst = wstart, as Wave in SpecData). */
+int fsg_set_grid(fsg_ctx *ctx, int wmode, double wstart, double wend, double dstep, int nwl,
+                 const double *wave);
+/* Model atmosphere after the EOS (AtmosData) and the species data the opacity kernel reads:
+ * FractionPF [ntau][nspc] (FP32), Xamass, PotIon (FP32), ion stage per species, and the
+ * H I / He I / H2 number densities of the perturber sum (Fraction, FP32).  Runs XlineInit
+ * (opacity.f90:65-93) on the device.  Replaces (opacity.f90:65-93) + module state. */
+int fsg_set_atmosphere(fsg_ctx *ctx, int ntau, const double *rhox, const double *T,
+                       const double *xne, const double *xna, const double *rho, int nspc,
+                       const float *fractionpf, const float *xamass, const float *potion,
+                       const int32_t *ion, const float *frac_h1, const float *frac_he1,
+                       const float *frac_h2);
+/* Continuum opacity ContOpac [nwl][ntau] (ContopCalc output, synth.f90:642-674), ContOpacStd
+ * [ntau] (may be NULL when motype == 0) and the model type (Motype). */
+int fsg_set_contopac(fsg_ctx *ctx, const double *contopac, const double *contopac_std, int motype);
+int fsg_set_contopac_dev(fsg_ctx *ctx, const double *d_contopac);
+/* He I Stark widths/shifts HeGam/HeShf [nhe][ntau] (hestark.f90:332-370), optional. */
+int fsg_set_hestark(fsg_ctx *ctx, int nhe, const double *hegam, const double *heshf, int spc_he1);
+
+/* ---- hot path ------------------------------------------------------------------------- */
+/* LineopCalc (synth.f90:747-1095): central pass (XlineSetup/XlineDepth, weak-line rejection,
+ * AnalyticWindow + WaveIdx), then the line opacity accumulated onto the device LineOpac.
+ * lineopac (host, [nwl][ntau], may be NULL) receives the accumulated total when non-NULL.
+ * Per-line outputs (host, length n, may be NULL): LinFlag bits, Ileft, Iright, LinStr
+ * (central depths via LinStrCalc when nmu > 0 was given with fsg_set_mu). */
+int fsg_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, double *lineopac, int32_t *flags,
+                    int32_t *ileft, int32_t *iright, float *linstr, fsg_stats *stats);
+int fsg_lineop_calc_dev(fsg_ctx *ctx, const fsg_lines *d_lines, fsg_stats *stats);
+/* Zero / read / write the device LineOpac accumulator ([nwl][ntau]; OPACITY= re-entry). */
+int fsg_lineop_reset(fsg_ctx *ctx);
+int fsg_lineop_get(fsg_ctx *ctx, double *lineopac);
+int fsg_lineop_set(fsg_ctx *ctx, const double *lineopac);
+const double *fsg_lineop_device_ptr(fsg_ctx *ctx);
+
+/* Limb angles and flux weights used by RadTranCalc, LinStrCalc and the disk integration. */
+int fsg_set_mu(fsg_ctx *ctx, int nmu, const double *xmu, const double *wmu);
+/* RadTranCalc (synth.f90:1825-1901) + DiskInteg without broadening (convol.f90:111-235):
+ * spl/spc [nwl][nmu], sfl/sfc [nwl]; any output may be NULL.  Uses the device LineOpac. */
+int fsg_radtran(fsg_ctx *ctx, double *spl, double *spc, double *sfl, double *sfc);
+int fsg_radtran_dev(fsg_ctx *ctx, double *d_spl, double *d_spc, double *d_sfl, double *d_sfc);
+
+/* ---- magnetic path ---------------------------------------------------------------------- */
+/* MagLineopCalc (synth.f90:1098-1455): bframe/bfield as BFRAME/BFIELD (3 values for frames
+ * 0/1, 2*nmu+1 for frame 2).  Accumulates the device MagLineOpac [nwl][ntau][6]. */
+int fsg_mag_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, int bframe, const double *bfield,
+                        int nbfield, double *maglineopac, int32_t *flags, int32_t *ileft,
+                        int32_t *iright, float *linstr, fsg_stats *stats);
+int fsg_mag_lineop_reset(fsg_ctx *ctx);
+/* MagRadTranCalc plane-parallel (synth.f90:1904-2012): spz [nwl][4][nmu], spc [nwl][nmu],
+ * and the Stokes-I flux sfl / continuum flux sfc [nwl] (may be NULL). */
+int fsg_mag_radtran(fsg_ctx *ctx, int bframe, const double *bfield, int nbfield, double *spz,
+                    double *spc, double *sfl, double *sfc);
+
+/* ---- kernel-level entry points (elemental reference functions, batched on the GPU) ------- */
+/* HVoigt (voigt.f90:76-110) and FVoigt (voigt.f90:256-299) over host arrays of length n. */
+int fsg_hvoigt(fsg_ctx *ctx, int64_t n, const double *a, const double *v, double *h);
+int fsg_fvoigt(fsg_ctx *ctx, int64_t n, const double *a, const double *v, double *h, double *l);
+/* The device-built FP32 tables VgtTab [402][1002] and FvTab [402][1002][2]. */
+int fsg_voigt_tables(fsg_ctx *ctx, float *vgt, float *fvt);
+/* LocPrfPP (solver.f90:123-179) for nprof independent profiles: xki/src [nprof][ntau],
+ * ploc [nprof][nmu]. */
+int fsg_locprf_pp(fsg_ctx *ctx, int nprof, int nmu, const double *xmu, int ntau,
+                  const double *xki, const double *src, const double *rhox, double *ploc);
+/* MuQuadrature (utils.f90:1273-1330): x (in/out when setnodes == 0), w, r [n+1]. */
+int fsg_mu_quadrature(int quad, int n, double *x, double *w, double *r, int setnodes);
+/* ZeemanPattern (utils.f90:901-1004): outputs hold up to 2*jup+1 entries each. */
+int fsg_zeeman_pattern(float jlo, float jup, float glo, float gup, int32_t *npi, float *spi,
+                       float *rpi, int32_t *nsig, float *ssig, float *rsig);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,54 @@
+"""Shared test helpers: atmosphere states, continuum on a grid, seeded line lists."""
+import os
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DATA = os.path.join(REPO, "fastspec_b200", "data")
+GOLD = os.path.join(REPO, "tests", "golden")
+
+STATE_KEYS = ("rhox", "T", "xne", "xna", "rho", "fractionpf", "xamass", "potion", "ion", "frac_h1", "frac_he1")
+
+
+def load_atm(name):
+    d = np.load(os.path.join(DATA, "atm_%s.npz" % name))
+    st = {k: d[k] for k in STATE_KEYS}
+    st["frac_h2"] = np.zeros(len(d["T"]), np.float32)
+    meta = dict(vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]), cont_wave=d["cont_wave"],
+                cont_opac=d["cont_opac"], species=[str(s) for s in d["species"]])
+    return st, meta
+
+
+def contopac_on(meta, wave_abs):
+    """Continuum opacity on absolute wavelengths by log-linear interpolation of the knots."""
+    lk = np.log(meta["cont_opac"])
+    out = np.empty((len(wave_abs), lk.shape[1]))
+    for t in range(lk.shape[1]):
+        out[:, t] = np.exp(np.interp(wave_abs, meta["cont_wave"], lk[:, t]))
+    return out
+
+
+def load_pin(name):
+    d = np.load(os.path.join(GOLD, name + ".npz"))
+    return {k: d[k] for k in d.files}
+
+
+def pin_lines(d):
+    return dict(wl=d["line_wl"], elo=d["line_elo"], gf=d["line_gf"], grad=d["line_grad"], gqst=d["line_gqst"],
+                gvdw=d["line_gvdw"], spc=d["line_spc"], ismol=d["line_ismol"])
+
+
+def pin_setup(d):
+    """(grid dict, state, contopac on the full grid) of a pin fixture."""
+    g = d["grid"]
+    grid = dict(wmode=int(g[3]), wstart=float(g[0]), wend=float(g[1]), dstep=float(g[2]))
+    st, meta = load_atm(str(d["atm"]))
+    from fastspec_b200 import workloads  # noqa: F401
+    import oracle
+    nwl = oracle.State(grid, st).nwl
+    i0, i1 = int(d["i0"]), int(d["i1"])
+    co = np.empty((nwl, len(st["T"])))
+    co[i0:i1 + 1] = d["contopac"]
+    co[:i0] = d["contopac"][0]
+    co[i1 + 1:] = d["contopac"][-1]
+    return grid, st, meta, co

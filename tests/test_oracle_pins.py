@@ -1,0 +1,81 @@
+"""The CPU oracle against the reference program's own outputs (fixtures in tests/golden and
+fastspec_b200/data, generated by fastspec_b200/data/make_atmospheres.py).
+
+Tolerances: window indices are integers and must be identical; FP64 values differ only through
+libm ulps (the reference's gfortran build uses glibc's vectorised exp/log in some loops), which
+the DELO coefficients amplify near their Taylor branch (solver.f90:155-169), hence 1e-8."""
+import numpy as np
+import pytest
+
+import helpers as H
+
+
+def test_voigt_exact_vs_faddeeva(oracle_mod):
+    scipy = pytest.importorskip("scipy.special")
+    for a in (1e-5, 1e-3, 0.05, 0.5, 2.0, 5.9, 7.5):
+        for v in (0.0, 0.2, 1.0, 2.7, 5.0, 7.9):
+            z = scipy.wofz(v + 1j * a)
+            assert abs(oracle_mod.hvoigt_exact(a, v) - z.real) <= 1e-9 * abs(z.real)
+            w = oracle_mod.wvoigt_exact(a, v)
+            assert abs(w.imag - z.imag) <= 1e-8 * abs(z.imag) + 1e-15   # method accuracy (h = 0.5, N = 16)
+
+
+def test_voigt_table_lerp_accuracy(oracle_mod):
+    scipy = pytest.importorskip("scipy.special")
+    rng = np.random.default_rng(5)
+    a = rng.uniform(0, 7.9, 2000); v = rng.uniform(-7.9, 7.9, 2000)
+    h = np.array([oracle_mod.hvoigt(x, y) for x, y in zip(a, v)])
+    ref = scipy.wofz(np.abs(v) + 1j * a).real
+    # the table's own interpolation error (the reference's, by design) is below 1e-4 of H(a, 0)
+    assert np.max(np.abs(h - ref)) < 2e-4
+
+
+@pytest.mark.parametrize("name", ["pin_solar", "pin_cooldwarf"])
+def test_oracle_lineop_pins_reference(oracle_mod, name):
+    d = H.load_pin(name)
+    grid, st, meta, co = H.pin_setup(d)
+    S = oracle_mod.State(grid, st, contopac=co, vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]))
+    i0, i1 = int(d["i0"]), int(d["i1"])
+    assert np.abs(S.wave[i0:i1 + 1] + S.wfirst - d["wave"]).max() < 1e-9
+    L = oracle_mod.Lines(**H.pin_lines(d), kind=2)
+    r = oracle_mod.lineop_calc(S, L, list_type=2)
+    lo, ref = r["lineopac"][i0:i1 + 1], d["lineopac"]
+    # window pin: identical nonzero pattern (LineOpac is exactly 0 outside every window)
+    assert np.array_equal(lo > 0, ref > 0)
+    m = ref > 0
+    assert np.max(np.abs(lo[m] / ref[m] - 1)) < 1e-8
+    spl, spc = oracle_mod.radtran(S, d["xmu"], r["lineopac"])
+    assert np.max(np.abs(spl[i0:i1 + 1] / d["spl"] - 1)) < 1e-8
+    assert np.max(np.abs(spc[i0:i1 + 1] / d["spc"] - 1)) < 1e-8
+    x, w, _ = oracle_mod.mu_quadrature(1, len(d["xmu"]))
+    assert np.max(np.abs(x - d["xmu"])) == 0.0
+    sfl, sfc = oracle_mod.disk_integ(w, spl[i0:i1 + 1], spc[i0:i1 + 1])
+    assert np.max(np.abs(sfl / d["sfl"] - 1)) < 1e-8
+    assert np.max(np.abs(sfc / d["sfc"] - 1)) < 1e-8
+
+
+def test_oracle_blocks_equal_single_block(oracle_mod):
+    """Segmented blocks (NlinesStep < Nlines) give the single-block result (synth.f90:1012-1088)."""
+    d = H.load_pin("pin_solar")
+    grid, st, meta, co = H.pin_setup(d)
+    S = oracle_mod.State(grid, st, contopac=co, vmicro=1.0)
+    L = oracle_mod.Lines(**H.pin_lines(d), kind=2)
+    r1 = oracle_mod.lineop_calc(S, L, list_type=2)
+    r2 = oracle_mod.lineop_calc(S, L, list_type=2, nlines_lim=40)
+    assert r2["stats"]["nsegments"] > 1
+    np.testing.assert_allclose(r2["lineopac"], r1["lineopac"], rtol=1e-13, atol=0)
+    assert np.array_equal(r1["ileft"], r2["ileft"]) and np.array_equal(r1["iright"], r2["iright"])
+
+
+def test_mu_quadratures(oracle_mod):
+    for q in (0, 1, 2):
+        for n in (1, 2, 7, 9):
+            x, w, r = oracle_mod.mu_quadrature(q, n)
+            assert abs(w.sum() - 1.0) < 1e-12
+            assert np.all(np.diff(x) <= 0)
+
+
+def test_zeeman_pattern_normal_triplet(oracle_mod):
+    spi, rpi, ssi, rsi = oracle_mod.zeeman_pattern(1.0, 0.0, 1.5, 1.5)
+    assert len(spi) == 1 and spi[0] == 0 and rpi[0] == 1
+    assert len(ssi) == 1 and abs(abs(ssi[0]) - 1.5) < 1e-6
