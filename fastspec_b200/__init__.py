@@ -45,7 +45,7 @@ class Stats(C.Structure):
     _fields_ = [("nlines_in", C.c_int64), ("nlines_used", C.c_int64), ("nwide", C.c_int64),
                 ("nweak", C.c_int64), ("nblocks", C.c_int64), ("line_evals", C.c_double),
                 ("ms_center", C.c_double), ("ms_params", C.c_double), ("ms_accum", C.c_double),
-                ("ms_total", C.c_double)]
+                ("ms_total", C.c_double), ("accum_launches", C.c_int64), ("ms_accum_kernels", C.c_double)]
 
     def asdict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -53,7 +53,7 @@ class Stats(C.Structure):
 
 # every symbol the header declares (checked by the CPU test suite)
 EXPORTS = [
-    "fsg_create", "fsg_destroy", "fsg_last_error", "fsg_version", "fsg_make_grid", "fsg_set_grid",
+    "fsg_create", "fsg_destroy", "fsg_last_error", "fsg_version", "fsg_kernel_launches", "fsg_cuda_stream", "fsg_make_grid", "fsg_set_grid",
     "fsg_set_atmosphere", "fsg_set_contopac", "fsg_set_contopac_dev", "fsg_set_hestark",
     "fsg_lineop_calc", "fsg_lineop_calc_dev", "fsg_lineop_reset", "fsg_lineop_get", "fsg_lineop_set",
     "fsg_lineop_device_ptr", "fsg_set_mu", "fsg_radtran", "fsg_radtran_dev", "fsg_mag_lineop_calc",
@@ -83,6 +83,10 @@ def lib():
     L.fsg_destroy.restype = None
     L.fsg_last_error.argtypes = [C.c_void_p]
     L.fsg_last_error.restype = C.c_char_p
+    L.fsg_kernel_launches.argtypes = [C.c_void_p]
+    L.fsg_kernel_launches.restype = C.c_int64
+    L.fsg_cuda_stream.argtypes = [C.c_void_p]
+    L.fsg_cuda_stream.restype = C.c_void_p
     L.fsg_make_grid.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, _dp, C.POINTER(C.c_int)]
     L.fsg_set_grid.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int, _dp]
     L.fsg_set_atmosphere.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_int, _fp, _fp, _fp,
@@ -230,6 +234,14 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    def stream_ptr(self):
+        """The context's cudaStream_t as an integer (torch.cuda.ExternalStream can wrap it)."""
+        return int(self._lib.fsg_cuda_stream(self.h))
+
+    def launches(self):
+        """Kernels launched by this context so far."""
+        return int(self._lib.fsg_kernel_launches(self.h))
 
     def _ck(self, rc, what):
         if rc != 0:

@@ -33,10 +33,10 @@ void fsg_launch_fvoigt(cudaStream_t, int64_t, const double *, const double *, do
 void fsg_launch_locprf(cudaStream_t, int, int, const double *, int, const double *, const double *, const double *,
                        double *, double *);
 int fsg_fast_set_constants(const double *, const double *);
-int fsg_launch_accum_fast(cudaStream_t, int, int, const double *, const LineHdr *, const WingRec *,
+int fsg_launch_accum_fast(cudaStream_t, int, int, int, const double *, const LineHdr *, const WingRec *,
                           const CoreRec *, const int *, const int *, const float *, double *);
 int fsg_fast_tiles(int);
-void fsg_launch_tile_span(cudaStream_t, int, int64_t, const LineHdr *, int *, int *);
+void fsg_launch_tile_span(cudaStream_t, int, int, int64_t, const LineHdr *, int *, int *);
 int fsg_select(cudaStream_t, int64_t, const int32_t *, const int32_t *, const int32_t *, int, int *, int64_t *,
                int64_t *, int64_t *);
 void fsg_launch_class_hist(cudaStream_t, int64_t, const int32_t *, const int32_t *, const int32_t *,
@@ -49,6 +49,19 @@ void fsg_launch_gather_lines(cudaStream_t, const LineView &, const int64_t *, in
 int fsg_select_wide(cudaStream_t, int64_t, const int32_t *, int *, int64_t *, int64_t *, int64_t *);
 void fsg_launch_scatter_flags(cudaStream_t, int64_t, const int64_t *, const int32_t *, int32_t *);
 double fsg_count_evals(fsg_ctx *, int64_t);
+size_t fsg_stokes_smem(int, int);
+int fsg_launch_stokes(cudaStream_t, const AtmView &, const double *, const double *, const double *, int,
+                      const double *, const double *, const double *, double *, double *);
+void fsg_launch_mag_center(cudaStream_t, const AtmView &, const LineView &, const ZView &, double, const VoigtTables &,
+                           int32_t *, int32_t *, int32_t *, unsigned long long *);
+void fsg_launch_mag_params(cudaStream_t, const AtmView &, const LineView &, int64_t, const int64_t *, int64_t,
+                           const int32_t *, double3 *);
+void fsg_launch_mag_accum(cudaStream_t, const AtmView &, const double *, const ZView &, const int64_t *, int, int,
+                          const int *, const int *, const int32_t *, const int32_t *, const int32_t *, int64_t,
+                          const double3 *, const VoigtTables &, double *, double *);
+void fsg_launch_mag_wide(cudaStream_t, const AtmView &, const double *, const ZView &, const int64_t *, int,
+                         const int64_t *, const int32_t *, const int32_t *, const int32_t *, const double3 *,
+                         const VoigtTables &, double *);
 
 std::string fsg_cuda_msg(cudaError_t e, const char *what) {
     char b[512];
@@ -104,8 +117,10 @@ struct fsg_ctx {
     // spectra
     DBuf d_spl, d_spc, d_sfl, d_sfc, d_work, d_a, d_v, d_h, d_l;
     // magnetic
-    DBuf z_npi, z_nsi, z_pioff, z_sioff, z_splpi, z_strpi, z_splsi, z_strsi, d_zsc;
+    DBuf z_npi, z_nsi, z_pioff, z_sioff, z_splpi, z_strpi, z_splsi, z_strsi, d_zsc, z_rawpi, z_rawsi, d_zmap, d_geo;
     cudaEvent_t ev[8];
+    int64_t launches = 0;
+    std::vector<cudaEvent_t> kev;
 };
 
 static int fail(fsg_ctx *c, int code, const char *msg) { if (c) c->err = msg; return code; }
@@ -135,6 +150,10 @@ AtmView fsg_view(const fsg_ctx *ctx) {
 extern "C" {
 
 int fsg_version(void) { return 10000; }
+
+int64_t fsg_kernel_launches(const fsg_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+void *fsg_cuda_stream(fsg_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
 const char *fsg_last_error(const fsg_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
@@ -183,9 +202,10 @@ void fsg_destroy(fsg_ctx *ctx) {
                      &ctx->d_pw, &ctx->d_evals, &ctx->d_spl, &ctx->d_spc, &ctx->d_sfl, &ctx->d_sfc,
                      &ctx->d_work, &ctx->d_a, &ctx->d_v, &ctx->d_h, &ctx->d_l, &ctx->z_npi, &ctx->z_nsi,
                      &ctx->z_pioff, &ctx->z_sioff, &ctx->z_splpi, &ctx->z_strpi, &ctx->z_splsi, &ctx->z_strsi,
-                     &ctx->d_zsc };
+                     &ctx->d_zsc, &ctx->z_rawpi, &ctx->z_rawsi, &ctx->d_zmap, &ctx->d_geo };
     for (DBuf *b : bufs) b->release();
     for (int i = 0; i < 8; i++) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+    for (cudaEvent_t e : ctx->kev) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -431,6 +451,7 @@ static int central_pass(fsg_ctx *ctx, const LineView &LV, int64_t *nkeep) {
     AtmView A = fsg_view(ctx);
     fsg_launch_center(ctx->stream, A, LV, ctx->tab, ctx->d_flags.as<int32_t>(), ctx->d_ileft.as<int32_t>(),
                       ctx->d_iright.as<int32_t>(), ctx->d_nkeep.as<unsigned long long>());
+    ctx->launches += 1;
     CK(cudaGetLastError(), "k_center");
     unsigned long long nk = 0;
     CK(cudaMemcpyAsync(&nk, ctx->d_nkeep.p, sizeof nk, cudaMemcpyDeviceToHost, ctx->stream), "center");
@@ -449,6 +470,13 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st) {
     CK(cudaMemsetAsync(ctx->d_hist.p, 0, sizeof(unsigned long long) * 32, s), "hist");
     fsg_launch_class_hist(s, n, ctx->d_flags.as<int32_t>(), ctx->d_ileft.as<int32_t>(), ctx->d_iright.as<int32_t>(),
                           ctx->d_hist.as<unsigned long long>());
+    ctx->launches += 1;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kt;
+    size_t kev_used = 0;
+    auto kevent = [&]() -> cudaEvent_t {
+        if (kev_used == ctx->kev.size()) { cudaEvent_t e; cudaEventCreate(&e); ctx->kev.push_back(e); }
+        return ctx->kev[kev_used++];
+    };
     unsigned long long hist[32];
     CK(cudaMemcpyAsync(hist, ctx->d_hist.p, sizeof hist, cudaMemcpyDeviceToHost, s), "hist");
     CK(cudaStreamSynchronize(s), "hist");
@@ -468,6 +496,7 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st) {
                             ctx->d_counts.as<int>(), ctx->d_offs.as<int64_t>(), ctx->d_idx.as<int64_t>(),
                             ctx->d_total.as<int64_t>());
         if (rc) return cuda_fail(ctx, cudaGetLastError(), "select");
+        ctx->launches += 3;
         int64_t nc = (int64_t)hist[c];
         int64_t bcap = std::min(cap, nc);
         ALLOC(ctx->d_wing, sizeof(WingRec) * (size_t)bcap * nt);
@@ -478,16 +507,24 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st) {
             fsg_launch_params_fast(s, A, LV, ctx->d_idx.as<int64_t>(), j0, nb, ctx->d_flags.as<int32_t>(),
                                    ctx->d_ileft.as<int32_t>(), ctx->d_iright.as<int32_t>(), ctx->d_wing.as<WingRec>(),
                                    ctx->d_core.as<CoreRec>(), ctx->d_hdr.as<LineHdr>());
-            fsg_launch_tile_span(s, ctx->nwl, nb, ctx->d_hdr.as<LineHdr>(), ctx->d_tlo.as<int>(), ctx->d_thi.as<int>());
-            int rc2 = fsg_launch_accum_fast(s, nt, ctx->nwl, ctx->d_wave.as<double>(), ctx->d_hdr.as<LineHdr>(),
+            fsg_launch_tile_span(s, c, ctx->nwl, nb, ctx->d_hdr.as<LineHdr>(), ctx->d_tlo.as<int>(), ctx->d_thi.as<int>());
+            cudaEvent_t ea = kevent(), eb = kevent();
+            cudaEventRecord(ea, s);
+            int rc2 = fsg_launch_accum_fast(s, c, nt, ctx->nwl, ctx->d_wave.as<double>(), ctx->d_hdr.as<LineHdr>(),
                                             ctx->d_wing.as<WingRec>(), ctx->d_core.as<CoreRec>(), ctx->d_tlo.as<int>(),
                                             ctx->d_thi.as<int>(), ctx->tab.vtab, ctx->d_lineopac.as<double>());
             if (rc2) return cuda_fail(ctx, cudaGetLastError(), "k_accum_fast");
+            cudaEventRecord(eb, s);
+            kt.push_back({ ea, eb });
+            ctx->launches += 4;
             nblocks++;
         }
     }
     CK(cudaGetLastError(), "fast accumulation");
-    if (st) st->nblocks = nblocks;
+    CK(cudaStreamSynchronize(s), "fast accumulation");
+    double ms = 0.0;
+    for (auto &p : kt) { float x = 0; cudaEventElapsedTime(&x, p.first, p.second); ms += x; }
+    if (st) { st->nblocks = nblocks; st->accum_launches = (int64_t)kt.size(); st->ms_accum_kernels = ms; }
     return FSG_OK;
 }
 
@@ -529,6 +566,7 @@ static int accumulate_fp64(fsg_ctx *ctx, const LineView &LV, int64_t nkeep, fsg_
     unsigned long long *d_nw = ctx->d_nkeep.as<unsigned long long>();
     CK(cudaMemsetAsync(d_nw, 0, sizeof(unsigned long long), s), "wide");
     fsg_launch_mark_wide(s, A, nw, W.wl, nstep, pf, pl, pr, d_nw);
+    ctx->launches += pack ? 5 : 1;
     unsigned long long nwide = 0;
     CK(cudaMemcpyAsync(&nwide, d_nw, sizeof nwide, cudaMemcpyDeviceToHost, s), "wide");
     // Lstart/Lstop (synth.f90:955-978)
@@ -540,6 +578,7 @@ static int accumulate_fp64(fsg_ctx *ctx, const LineView &LV, int64_t nkeep, fsg_
         CK(cudaStreamSynchronize(s), "lstart");
     }
     fsg_launch_span(s, nw, pf, pl, pr, ctx->d_lstart.as<int>(), ctx->d_lstop.as<int>());
+    ctx->launches += 1;
     ALLOC(ctx->d_evals, sizeof(double));
     CK(cudaMemsetAsync(ctx->d_evals.p, 0, sizeof(double), s), "evals");
     // wide lines: list, parameters, per-wavelength ordered accumulation
@@ -550,6 +589,7 @@ static int accumulate_fp64(fsg_ctx *ctx, const LineView &LV, int64_t nkeep, fsg_
         ALLOC(ctx->d_pw, sizeof(double3) * nwide * nt);
         fsg_launch_wide_fp64(s, A, W, (int)nwide, ctx->d_widx.as<int64_t>(), pf, pl, pr, ctx->d_pw.as<double3>(),
                              ctx->tab, 1, nwl, ctx->d_lineopac.as<double>(), ctx->d_evals.as<double>());
+        ctx->launches += 5;
     }
     // segment loop (synth.f90:1006-1088): choose segments on the host from Lstart/Lstop
     std::vector<int> ls(nwl), le(nwl);
@@ -584,12 +624,19 @@ static int accumulate_fp64(fsg_ctx *ctx, const LineView &LV, int64_t nkeep, fsg_
         if (iline1 != ilineb) {
             ilineb = iline1;
             fsg_launch_params_fp64(s, A, W, loff, iline2 - loff, pf, ctx->d_p64.as<double3>());
+            ctx->launches += 1;
             nblocks++;
         }
+        cudaEvent_t ea = ctx->ev[4], eb = ctx->ev[5];
+        cudaEventRecord(ea, s);
         fsg_launch_accum_fp64(s, A, W.wl, iwl1, iwl2, ctx->d_lstart.as<int>(), ctx->d_lstop.as<int>(), pf, pl, pr,
                               loff, ctx->d_p64.as<double3>(), ctx->tab, ctx->d_lineopac.as<double>(),
                               ctx->d_evals.as<double>());
         CK(cudaGetLastError(), "fp64 accumulation");
+        cudaEventRecord(eb, s);
+        CK(cudaEventSynchronize(eb), "fp64 accumulation");
+        { float x = 0; cudaEventElapsedTime(&x, ea, eb); if (st) { st->ms_accum_kernels += x; st->accum_launches++; } }
+        ctx->launches += 1;
         if (iwl2 == nwl) break;
         iwl1 = iwl2 + 1;
     }
@@ -600,6 +647,7 @@ static int accumulate_fp64(fsg_ctx *ctx, const LineView &LV, int64_t nkeep, fsg_
     // per-line outputs in original order: scatter the packed wide flags back
     if (pack) {
         fsg_launch_scatter_flags(s, nw, ctx->d_idx.as<int64_t>(), pf, ctx->d_flags.as<int32_t>());
+        ctx->launches += 1;
     }
     return FSG_OK;
 }
@@ -667,6 +715,7 @@ static int radtran_dev(fsg_ctx *ctx, double *spl, double *spc, double *sfl, doub
     AtmView A = fsg_view(ctx);
     rc = fsg_launch_radtran(ctx->stream, A, ctx->d_lineopac.as<double>(), ctx->d_rhox.as<double>(), ctx->nmu,
                             ctx->d_xmu.as<double>(), ctx->d_wmu.as<double>(), spl, spc, sfl, sfc);
+    ctx->launches += 1;
     if (rc) return cuda_fail(ctx, cudaGetLastError(), "k_radtran");
     return FSG_OK;
 }
@@ -693,6 +742,270 @@ int fsg_radtran(fsg_ctx *ctx, double *spl, double *spc, double *sfl, double *sfc
     if (sfl) CK(cudaMemcpyAsync(sfl, ctx->d_sfl.p, nf, cudaMemcpyDeviceToHost, s), "sfl");
     if (sfc) CK(cudaMemcpyAsync(sfc, ctx->d_sfc.p, nf, cudaMemcpyDeviceToHost, s), "sfc");
     CK(cudaStreamSynchronize(s), "radtran");
+    return FSG_OK;
+}
+
+
+// ---- MagLineopCalc (synth.f90:1098-1455) ---------------------------------------------------------
+static int ensure_maglineopac(fsg_ctx *ctx) {
+    size_t nb = sizeof(double) * 6 * (size_t)ctx->nwl * ctx->ntau;
+    if (ctx->d_maglineopac.cap < nb) {
+        ALLOC(ctx->d_maglineopac, nb);
+        CK(cudaMemsetAsync(ctx->d_maglineopac.p, 0, nb, ctx->stream), "maglineopac reset");
+    }
+    return FSG_OK;
+}
+
+int fsg_mag_lineop_reset(fsg_ctx *ctx) {
+    if (!ctx) return FSG_E_ARG;
+    if (!ctx->have_grid || !ctx->have_atm) return fail(ctx, FSG_E_STATE, "fsg_mag_lineop_reset: set grid and atmosphere first");
+    cudaSetDevice(ctx->device);
+    int rc = ensure_maglineopac(ctx); if (rc) return rc;
+    CK(cudaMemsetAsync(ctx->d_maglineopac.p, 0, sizeof(double) * 6 * (size_t)ctx->nwl * ctx->ntau, ctx->stream), "reset");
+    CK(cudaStreamSynchronize(ctx->stream), "reset");
+    return FSG_OK;
+}
+
+int fsg_mag_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, int bframe, const double *bfield, int nbfield,
+                        double *maglineopac, int32_t *flags, int32_t *ileft, int32_t *iright, float *linstr,
+                        fsg_stats *st) {
+    (void)linstr;
+    int rc = check_lines(ctx, lines); if (rc) return rc;
+    if (lines->kind != 2) return fail(ctx, FSG_E_ARG, "fsg_mag_lineop_calc: magnetic lists have kind 2");
+    if (!bfield || (bframe < 0 || bframe > 2) || nbfield < 3 || (bframe == 2 && nbfield != 2 * ctx->nmu + 1))
+        return fail(ctx, FSG_E_ARG, "fsg_mag_lineop_calc: BFIELD needs 3 values (frames 0, 1) or 2*nmu+1 (frame 2)");
+    int64_t n = lines->n;
+    if (n > 0 && (!lines->npi || !lines->nsi || !lines->pi_off || !lines->si_off || !lines->spl_pi || !lines->str_pi ||
+                  !lines->spl_si || !lines->str_si))
+        return fail(ctx, FSG_E_ARG, "fsg_mag_lineop_calc: Zeeman component arrays missing");
+    cudaSetDevice(ctx->device);
+    rc = ensure_maglineopac(ctx); if (rc) return rc;
+    if (st) { memset(st, 0, sizeof *st); st->nlines_in = n; }
+    if (n == 0) return FSG_OK;
+    cudaStream_t s = ctx->stream;
+    const int nt = ctx->ntau, nwl = ctx->nwl;
+    CK(cudaEventRecord(ctx->ev[0], s), "event");
+    fsg_lines D;
+    rc = upload_lines(ctx, lines, &D); if (rc) return rc;
+    int64_t npi_tot = lines->pi_off[n - 1] + lines->npi[n - 1], nsi_tot = lines->si_off[n - 1] + lines->nsi[n - 1];
+    ALLOC(ctx->z_npi, sizeof(int32_t) * n); ALLOC(ctx->z_nsi, sizeof(int32_t) * n);
+    ALLOC(ctx->z_pioff, sizeof(int64_t) * n); ALLOC(ctx->z_sioff, sizeof(int64_t) * n);
+    ALLOC(ctx->z_rawpi, sizeof(float) * (npi_tot + 1)); ALLOC(ctx->z_strpi, sizeof(float) * (npi_tot + 1));
+    ALLOC(ctx->z_rawsi, sizeof(float) * (nsi_tot + 1)); ALLOC(ctx->z_strsi, sizeof(float) * (nsi_tot + 1));
+    ALLOC(ctx->z_splpi, sizeof(float) * (npi_tot + 1)); ALLOC(ctx->z_splsi, sizeof(float) * (nsi_tot + 1));
+    CK(cudaMemcpyAsync(ctx->z_npi.p, lines->npi, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s), "zeeman upload");
+    CK(cudaMemcpyAsync(ctx->z_nsi.p, lines->nsi, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s), "zeeman upload");
+    CK(cudaMemcpyAsync(ctx->z_pioff.p, lines->pi_off, sizeof(int64_t) * n, cudaMemcpyHostToDevice, s), "zeeman upload");
+    CK(cudaMemcpyAsync(ctx->z_sioff.p, lines->si_off, sizeof(int64_t) * n, cudaMemcpyHostToDevice, s), "zeeman upload");
+    if (npi_tot > 0) {
+        CK(cudaMemcpyAsync(ctx->z_rawpi.p, lines->spl_pi, sizeof(float) * npi_tot, cudaMemcpyHostToDevice, s), "zeeman upload");
+        CK(cudaMemcpyAsync(ctx->z_strpi.p, lines->str_pi, sizeof(float) * npi_tot, cudaMemcpyHostToDevice, s), "zeeman upload");
+    }
+    if (nsi_tot > 0) {
+        CK(cudaMemcpyAsync(ctx->z_rawsi.p, lines->spl_si, sizeof(float) * nsi_tot, cudaMemcpyHostToDevice, s), "zeeman upload");
+        CK(cudaMemcpyAsync(ctx->z_strsi.p, lines->str_si, sizeof(float) * nsi_tot, cudaMemcpyHostToDevice, s), "zeeman upload");
+    }
+    ZView Z;
+    Z.npi = ctx->z_npi.as<int32_t>(); Z.nsi = ctx->z_nsi.as<int32_t>();
+    Z.pi_off = ctx->z_pioff.as<int64_t>(); Z.si_off = ctx->z_sioff.as<int64_t>();
+    Z.strpi = ctx->z_strpi.as<float>(); Z.strsi = ctx->z_strsi.as<float>();
+    Z.splpi = ctx->z_splpi.as<float>(); Z.splsi = ctx->z_splsi.as<float>();
+    Z.rawpi = ctx->z_rawpi.as<float>(); Z.rawsi = ctx->z_rawsi.as<float>();
+    double Bsplit = (bframe == 0) ? FSG_KZ * sqrt(bfield[0] * bfield[0] + bfield[1] * bfield[1] + bfield[2] * bfield[2])
+                                  : FSG_KZ * fabs(bfield[0]);
+    LineView LV = make_view(&D);
+    AtmView A = fsg_view(ctx);
+    ALLOC(ctx->d_flags, sizeof(int32_t) * n); ALLOC(ctx->d_ileft, sizeof(int32_t) * n);
+    ALLOC(ctx->d_iright, sizeof(int32_t) * n); ALLOC(ctx->d_nkeep, sizeof(unsigned long long));
+    CK(cudaMemsetAsync(ctx->d_nkeep.p, 0, sizeof(unsigned long long), s), "mag center");
+    int32_t *pf = ctx->d_flags.as<int32_t>(), *pl = ctx->d_ileft.as<int32_t>(), *pr = ctx->d_iright.as<int32_t>();
+    fsg_launch_mag_center(s, A, LV, Z, Bsplit, ctx->tab, pf, pl, pr, ctx->d_nkeep.as<unsigned long long>());
+    ctx->launches += 1;
+    CK(cudaGetLastError(), "k_mag_center");
+    unsigned long long nk = 0;
+    CK(cudaMemcpyAsync(&nk, ctx->d_nkeep.p, sizeof nk, cudaMemcpyDeviceToHost, s), "mag center");
+    CK(cudaStreamSynchronize(s), "mag center");
+    CK(cudaEventRecord(ctx->ev[1], s), "event");
+    int64_t nkeep = (int64_t)nk;
+    if (st) { st->nlines_used = nkeep; st->nweak = n - nkeep; }
+    // NlinesStep and PACK (synth.f90:1131, 1283-1297)
+    int64_t cap = block_capacity(ctx, sizeof(double3) * nt);
+    int64_t nstep = std::min<int64_t>(n, cap);
+    bool pack = (nstep == n);
+    int64_t nblkscan = (n + 1023) / 1024;
+    ALLOC(ctx->d_counts, sizeof(int) * std::max<int64_t>(nblkscan, 1));
+    ALLOC(ctx->d_offs, sizeof(int64_t) * std::max<int64_t>(nblkscan, 1));
+    ALLOC(ctx->d_total, sizeof(int64_t));
+    ALLOC(ctx->d_idx, sizeof(int64_t) * n);
+    LineView W = LV;
+    int64_t nw = n;
+    const int64_t *zmap = nullptr;
+    if (pack) {
+        fsg_select(s, n, pf, pl, pr, -1, ctx->d_counts.as<int>(), ctx->d_offs.as<int64_t>(), ctx->d_idx.as<int64_t>(),
+                   ctx->d_total.as<int64_t>());
+        nw = nkeep;
+        ALLOC(ctx->d_work, 64 * (size_t)std::max<int64_t>(nw, 1));
+        int32_t *gf, *gl, *gr;
+        fsg_launch_gather_lines(s, LV, ctx->d_idx.as<int64_t>(), nw, ctx->d_work.as<char>(), pf, pl, pr, &W, &gf, &gl, &gr);
+        ctx->launches += 4;
+        pf = gf; pl = gl; pr = gr;
+        W.n = nw;
+        zmap = ctx->d_idx.as<int64_t>();
+    } else {
+        std::vector<int64_t> iota(n);
+        for (int64_t i = 0; i < n; i++) iota[i] = i;
+        ALLOC(ctx->d_zmap, sizeof(int64_t) * n);
+        CK(cudaMemcpyAsync(ctx->d_zmap.p, iota.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, s), "zmap");
+        zmap = ctx->d_zmap.as<int64_t>();
+    }
+    if (nw == 0) return FSG_OK;
+    unsigned long long *d_nw = ctx->d_nkeep.as<unsigned long long>();
+    CK(cudaMemsetAsync(d_nw, 0, sizeof(unsigned long long), s), "wide");
+    fsg_launch_mark_wide(s, A, nw, W.wl, nstep, pf, pl, pr, d_nw);
+    unsigned long long nwide = 0;
+    CK(cudaMemcpyAsync(&nwide, d_nw, sizeof nwide, cudaMemcpyDeviceToHost, s), "wide");
+    ALLOC(ctx->d_lstart, sizeof(int) * nwl); ALLOC(ctx->d_lstop, sizeof(int) * nwl);
+    {
+        std::vector<int> ls(nwl, (int)nw), le(nwl, 1);
+        CK(cudaMemcpyAsync(ctx->d_lstart.p, ls.data(), sizeof(int) * nwl, cudaMemcpyHostToDevice, s), "lstart");
+        CK(cudaMemcpyAsync(ctx->d_lstop.p, le.data(), sizeof(int) * nwl, cudaMemcpyHostToDevice, s), "lstop");
+        CK(cudaStreamSynchronize(s), "lstart");
+    }
+    fsg_launch_span(s, nw, pf, pl, pr, ctx->d_lstart.as<int>(), ctx->d_lstop.as<int>());
+    ctx->launches += 2;
+    ALLOC(ctx->d_evals, sizeof(double));
+    CK(cudaMemsetAsync(ctx->d_evals.p, 0, sizeof(double), s), "evals");
+    double *mlo = ctx->d_maglineopac.as<double>();
+    if (nwide > 0) {
+        ALLOC(ctx->d_widx, sizeof(int64_t) * nwide);
+        fsg_select_wide(s, nw, pf, ctx->d_counts.as<int>(), ctx->d_offs.as<int64_t>(), ctx->d_widx.as<int64_t>(),
+                        ctx->d_total.as<int64_t>());
+        ALLOC(ctx->d_pw, sizeof(double3) * nwide * nt);
+        fsg_launch_mag_params(s, A, W, (int64_t)nwide, ctx->d_widx.as<int64_t>(), 0, pf, ctx->d_pw.as<double3>());
+        fsg_launch_mag_wide(s, A, W.wl, Z, zmap, (int)nwide, ctx->d_widx.as<int64_t>(), pf, pl, pr,
+                            ctx->d_pw.as<double3>(), ctx->tab, mlo);
+        ctx->launches += 5;
+    }
+    std::vector<int> ls(nwl), le(nwl);
+    CK(cudaMemcpyAsync(ls.data(), ctx->d_lstart.p, sizeof(int) * nwl, cudaMemcpyDeviceToHost, s), "lstart");
+    CK(cudaMemcpyAsync(le.data(), ctx->d_lstop.p, sizeof(int) * nwl, cudaMemcpyDeviceToHost, s), "lstop");
+    CK(cudaStreamSynchronize(s), "lstart");
+    ALLOC(ctx->d_p64, sizeof(double3) * (size_t)std::min<int64_t>(nstep, nw) * nt);
+    int64_t iline1 = 1, ilineb = 0, nblocks = 0;
+    int iwl1 = 1;
+    for (;;) {
+        int iwl2;
+        if (nstep >= nw) iwl2 = nwl;
+        else {
+            int64_t ilo = nw + 1, ihi = 0;
+            iwl2 = iwl1 - 1;
+            for (int iwl = iwl1; iwl <= nwl; iwl++) {
+                int64_t ilot = std::min<int64_t>(ilo, ls[iwl - 1]), ihit = std::max<int64_t>(ihi, le[iwl - 1]);
+                if (ihit - ilot + 1 > nstep) break;
+                ilo = ilot; ihi = ihit; iwl2 = iwl;
+            }
+            if (iwl2 < iwl1) {
+                char m[256];
+                snprintf(m, sizeof m, "line opacity segmentation: lines contributing to wavelength point #%d span more "
+                         "than %lld line records; increase limitram", iwl1, (long long)nstep);
+                return fail(ctx, FSG_E_SEGMENT, m);
+            }
+            iline1 = std::min<int64_t>(std::max<int64_t>(ilo, 1), nw);
+        }
+        int64_t iline2 = std::min<int64_t>(iline1 + nstep - 1, nw);
+        int64_t loff = iline1 - 1;
+        if (iline1 != ilineb) {
+            ilineb = iline1;
+            fsg_launch_mag_params(s, A, W, iline2 - loff, nullptr, loff, pf, ctx->d_p64.as<double3>());
+            ctx->launches += 1;
+            nblocks++;
+        }
+        fsg_launch_mag_accum(s, A, W.wl, Z, zmap, iwl1, iwl2, ctx->d_lstart.as<int>(), ctx->d_lstop.as<int>(), pf, pl,
+                             pr, loff, ctx->d_p64.as<double3>(), ctx->tab, mlo, ctx->d_evals.as<double>());
+        ctx->launches += 1;
+        CK(cudaGetLastError(), "mag accumulation");
+        if (iwl2 == nwl) break;
+        iwl1 = iwl2 + 1;
+    }
+    if (pack) {
+        fsg_launch_scatter_flags(s, nw, ctx->d_idx.as<int64_t>(), pf, ctx->d_flags.as<int32_t>());
+        ctx->launches += 1;
+    }
+    double ev = 0;
+    CK(cudaMemcpyAsync(&ev, ctx->d_evals.p, sizeof ev, cudaMemcpyDeviceToHost, s), "evals");
+    CK(cudaEventRecord(ctx->ev[2], s), "event");
+    size_t n4 = sizeof(int32_t) * n;
+    if (flags) CK(cudaMemcpyAsync(flags, ctx->d_flags.p, n4, cudaMemcpyDeviceToHost, s), "flags");
+    if (ileft) CK(cudaMemcpyAsync(ileft, ctx->d_ileft.p, n4, cudaMemcpyDeviceToHost, s), "ileft");
+    if (iright) CK(cudaMemcpyAsync(iright, ctx->d_iright.p, n4, cudaMemcpyDeviceToHost, s), "iright");
+    if (maglineopac)
+        CK(cudaMemcpyAsync(maglineopac, mlo, sizeof(double) * 6 * (size_t)nwl * nt, cudaMemcpyDeviceToHost, s), "mlo");
+    CK(cudaStreamSynchronize(s), "mag lineop");
+    if (st) {
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
+        cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
+        st->ms_center = a; st->ms_accum = b; st->ms_total = a + b;
+        st->nwide = (int64_t)nwide; st->nblocks = nblocks; st->line_evals = ev;
+    }
+    return FSG_OK;
+}
+
+// ---- MagRadTranCalc, plane-parallel (synth.f90:1904-2012) ----------------------------------------
+int fsg_mag_radtran(fsg_ctx *ctx, int bframe, const double *bfield, int nbfield, double *spz, double *spc,
+                    double *sfl, double *sfc) {
+    if (!ctx) return FSG_E_ARG;
+    if (!ctx->have_grid || !ctx->have_atm || !ctx->have_cont || ctx->nmu < 1)
+        return fail(ctx, FSG_E_STATE, "mag_radtran: set grid, atmosphere, continuum and mu first");
+    const int nmu = ctx->nmu;
+    if (!bfield || bframe < 0 || bframe > 2 || (bframe == 2 ? nbfield != 2 * nmu + 1 : nbfield != 3))
+        return fail(ctx, FSG_E_ARG, "mag_radtran: BFIELD needs 3 values (frames 0, 1) or 2*nmu+1 (frame 2)");
+    cudaSetDevice(ctx->device);
+    int rc = ensure_lineopac(ctx); if (rc) return rc;
+    rc = ensure_maglineopac(ctx); if (rc) return rc;
+    std::vector<double> xmu(nmu), geo(5 * nmu);
+    CK(cudaMemcpy(xmu.data(), ctx->d_xmu.p, sizeof(double) * nmu, cudaMemcpyDeviceToHost), "mu");
+    const double d2r = FSG_PI / 180.0;
+    for (int im = 0; im < nmu; im++) {
+        double Sphi, Spsi, Cpsi, CPhi;
+        if (bframe == 1) {
+            Sphi = sin(bfield[1] * d2r); Spsi = sin(bfield[2] * d2r); Cpsi = cos(bfield[2] * d2r); CPhi = cos(bfield[1] * d2r);
+        } else if (bframe == 2) {
+            Sphi = sin(bfield[2 * im + 1] * d2r); Spsi = sin(bfield[2 * im + 2] * d2r);
+            Cpsi = cos(bfield[2 * im + 2] * d2r); CPhi = cos(bfield[2 * im + 1] * d2r);
+        } else {
+            double Fldmod = sqrt(bfield[0] * bfield[0] + bfield[1] * bfield[1] + bfield[2] * bfield[2]);
+            if (Fldmod > 0.0) {
+                double Coslon = xmu[im], Sinlon = sqrt(1.0 - Coslon * Coslon);
+                double Bx = bfield[0] * Sinlon + bfield[2] * Coslon, By = bfield[1];
+                double Bz = bfield[0] * Coslon - bfield[2] * Sinlon, Bt = sqrt(Bx * Bx + By * By);
+                Sphi = Bt / Fldmod; CPhi = Bz / Fldmod;
+                if (Bt > 0.0) { Spsi = By / Bt; Cpsi = Bx / Bt; } else { Spsi = 0.0; Cpsi = 1.0; }
+            } else { Sphi = 0.0; CPhi = 1.0; Spsi = 0.0; Cpsi = 1.0; }
+        }
+        geo[0 * nmu + im] = Sphi * Sphi; geo[1 * nmu + im] = CPhi * CPhi; geo[2 * nmu + im] = CPhi;
+        geo[3 * nmu + im] = 2.0 * Spsi * Cpsi; geo[4 * nmu + im] = Cpsi * Cpsi - Spsi * Spsi;
+    }
+    cudaStream_t s = ctx->stream;
+    ALLOC(ctx->d_geo, sizeof(double) * 5 * nmu);
+    CK(cudaMemcpyAsync(ctx->d_geo.p, geo.data(), sizeof(double) * 5 * nmu, cudaMemcpyHostToDevice, s), "geo");
+    size_t nsp = sizeof(double) * (size_t)ctx->nwl * nmu, nf = sizeof(double) * ctx->nwl;
+    ALLOC(ctx->d_spl, 4 * nsp); ALLOC(ctx->d_spc, nsp); ALLOC(ctx->d_sfl, nf); ALLOC(ctx->d_sfc, nf);
+    AtmView A = fsg_view(ctx);
+    // continuum intensity and flux (LocPrfPP with ContOpac)
+    rc = fsg_launch_radtran(s, A, ctx->d_lineopac.as<double>(), ctx->d_rhox.as<double>(), nmu, ctx->d_xmu.as<double>(),
+                            ctx->d_wmu.as<double>(), nullptr, ctx->d_spc.as<double>(), nullptr, ctx->d_sfc.as<double>());
+    if (rc) return cuda_fail(ctx, cudaGetLastError(), "k_radtran");
+    rc = fsg_launch_stokes(s, A, ctx->d_lineopac.as<double>(), ctx->d_maglineopac.as<double>(), ctx->d_rhox.as<double>(),
+                           nmu, ctx->d_xmu.as<double>(), ctx->d_wmu.as<double>(), ctx->d_geo.as<double>(),
+                           ctx->d_spl.as<double>(), ctx->d_sfl.as<double>());
+    if (rc) return cuda_fail(ctx, cudaGetLastError(), "k_stokes");
+    ctx->launches += 2;
+    if (spz) CK(cudaMemcpyAsync(spz, ctx->d_spl.p, 4 * nsp, cudaMemcpyDeviceToHost, s), "spz");
+    if (spc) CK(cudaMemcpyAsync(spc, ctx->d_spc.p, nsp, cudaMemcpyDeviceToHost, s), "spc");
+    if (sfl) CK(cudaMemcpyAsync(sfl, ctx->d_sfl.p, nf, cudaMemcpyDeviceToHost, s), "sfl");
+    if (sfc) CK(cudaMemcpyAsync(sfc, ctx->d_sfc.p, nf, cudaMemcpyDeviceToHost, s), "sfc");
+    CK(cudaStreamSynchronize(s), "mag radtran");
     return FSG_OK;
 }
 
@@ -887,6 +1200,7 @@ __global__ void k_count_evals(int64_t n, const int32_t *flags, const int32_t *il
 }
 
 double fsg_count_evals(fsg_ctx *ctx, int64_t n) {
+    ctx->launches += 1;
     unsigned long long *d = ctx->d_nkeep.as<unsigned long long>();
     cudaMemsetAsync(d, 0, sizeof(unsigned long long), ctx->stream);
     k_count_evals<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(n, ctx->d_flags.as<int32_t>(),

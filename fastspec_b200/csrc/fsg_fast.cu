@@ -3,14 +3,16 @@
 // The work of LineopCalc's accumulation (LineOpacity1, opacity.f90:297-346) is
 //   LineOpac(t, p) = sum over retained lines l with Ileft(l) <= p <= Iright(l) of
 //                    HVoigt(a(l,t), (lambda_p - lambda_l) / dlD(l,t)) * LinCop(l,t).
-// Here a CTA owns a tile of FAST_TW wavelengths x all depths.  Warp w owns depths
-// [w*D, w*D + D); lane l owns the wavelengths tile0 + l + 32k (k < FAST_P).  Each thread keeps
-// its FAST_P x D sums in registers with Kahan compensation: no shared-memory or global atomics,
-// one read-modify-write of the FP64 LineOpac per tile and launch, deterministic order.
+// Here a CTA owns a tile of TW = 32 P wavelengths x all depths.  Warp w owns depths
+// [w*D, w*D + D); lane l owns the wavelengths tile0 + l + 32k (k < P).  Each thread keeps its
+// P x D sums in registers with Kahan compensation: no shared-memory or global atomics, one
+// read-modify-write of the FP64 LineOpac per tile and launch, deterministic order.
 //
-// Lines are binned by window width (class c holds windows of up to FAST_TW*2^c wavelengths) and
+// Lines are binned by window width (class c holds windows of up to 256 * 2^c wavelengths) and
 // processed class by class, so the candidate line range of a tile [lo, hi] -- the lines of the
-// class whose windows touch it -- stays within a small factor of the lines that do.
+// class whose windows touch it -- stays within a small factor of the lines that do.  Narrow
+// classes use narrow tiles (P = 1 for class 0, 2 for class 1, 4 above) so fewer lanes idle at
+// the window edges.
 //
 // The profile is evaluated in FP32 from the per-(line, depth) FP32 records that k_params_fast
 // derives from the FP64 XlineDepth values: for s = v^2 + a^2 >= 196 (almost every wing point)
@@ -19,8 +21,7 @@
 // exactly as HVoigt branches.
 #include "fsg_internal.cuh"
 
-#define FAST_TW 128
-#define FAST_P 4
+#define CLASS_W0 128      // class c: windows of at most CLASS_W0 * 2^(c+1) wavelengths
 
 __constant__ float c_anode[FSG_NA1];
 __constant__ float c_aida[FSG_NA1];
@@ -34,7 +35,7 @@ int fsg_fast_set_constants(const double *anode_h, const double *aida_h) {
 }
 
 // HVoigt * LinCop in FP32 for the table / continued-fraction region (voigt.f90:81-108)
-__device__ __noinline__ float hv_core32(const float *__restrict__ vtab, float v, float a, float cop) {
+__device__ __forceinline__ float hv_core32(const float *__restrict__ vtab, float v, float a, float cop) {
     float av = fabsf(v);
     if (a < 8.0f && av < 8.0f) {
         float fv = av * 125.0f;
@@ -58,104 +59,126 @@ __device__ __noinline__ float hv_core32(const float *__restrict__ vtab, float v,
     return 0.56418958354775628f * ((p + 0.5f) * di - q * dr) / (dr * dr + di * di) * cop;
 }
 
-template <int D>
+// Kahan-compensated accumulation of one value
+#define KAHAN(S, CC, V) do { float _y = (V) - (CC); float _t = (S) + _y; (CC) = (_t - (S)) - _y; (S) = _t; } while (0)
+
+// One (line, depth) x FAST_P-pixel step.  y = v^2 + a^2 + 1/2 from the pixel's dl^2; the wing
+// branch covers s = y - 1/2 >= 196, the rest goes to the reference's table / continued fraction.
+template <int P, bool MASK>
+__device__ __forceinline__ void line_depth_step(const WingRec &w, const CoreRec *__restrict__ cr,
+                                                const float (&dl2)[P], const bool (&in)[P],
+                                                const float *__restrict__ vtab, float (&s)[P], float (&c)[P]) {
+#pragma unroll
+    for (int k = 0; k < P; k++) {
+        float y = fmaf(dl2[k], w.vv2, w.c2);
+        float val;
+        if (y >= 196.5f) {
+            float t = y - 1.0f;
+            float den = fmaf(t, t, w.twoA);
+            val = (w.c1 * y) * __frcp_rn(den);
+        } else {
+            const CoreRec cc = *cr;
+            val = hv_core32(vtab, sqrtf(dl2[k]) * cc.vv, cc.a, cc.cop);
+        }
+        if (MASK) val = in[k] ? val : 0.0f;
+        KAHAN(s[k], c[k], val);
+    }
+}
+
+template <int D, int P>
 __global__ void __launch_bounds__(32 * 18)
 k_accum_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *__restrict__ hdr,
              const WingRec *__restrict__ wing, const CoreRec *__restrict__ core,
              const int *__restrict__ tile_lo, const int *__restrict__ tile_hi,
              const float *__restrict__ vtab, double *__restrict__ lineopac) {
+    constexpr int TW = 32 * P;
     const int tile = blockIdx.x;
     const int lo = tile_lo[tile], hi = tile_hi[tile];
     if (lo > hi) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int t0 = warp * D;
     if (t0 >= ntau) return;
-    const int p0 = tile * FAST_TW;            // 0-based wavelength index of the tile start
-    double wv[FAST_P];
-    int pix[FAST_P];
+    const int nd = min(D, ntau - t0);
+    const int p0 = tile * TW;                 // 0-based wavelength index of the tile start
+    double wv[P];
+    int pix[P];
 #pragma unroll
-    for (int k = 0; k < FAST_P; k++) {
+    for (int k = 0; k < P; k++) {
         pix[k] = p0 + lane + 32 * k;          // 0-based
         wv[k] = wave[min(pix[k], nwl - 1)];
     }
-    float s[D][FAST_P], c[D][FAST_P];
+    float s[D][P], c[D][P];
 #pragma unroll
     for (int d = 0; d < D; d++)
 #pragma unroll
-        for (int k = 0; k < FAST_P; k++) { s[d][k] = 0.0f; c[d][k] = 0.0f; }
+        for (int k = 0; k < P; k++) { s[d][k] = 0.0f; c[d][k] = 0.0f; }
 
-    const int tile_first = p0 + 1, tile_last = min(p0 + FAST_TW, nwl);   // 1-based bounds
+    const int tile_first = p0 + 1, tile_last = min(p0 + TW, nwl);   // 1-based bounds
     for (int j = lo; j <= hi; j++) {
         const LineHdr h = hdr[j];
-        if (h.iright < tile_first || h.ileft > tile_last) continue;      // window misses the tile
-        float dl2[FAST_P], dl[FAST_P];
-        bool in[FAST_P];
+        if (h.iright < tile_first || h.ileft > tile_last) continue;  // window misses the tile
+        const bool full = (h.ileft <= tile_first) && (h.iright >= tile_last);
+        float dl2[P];
+        bool in[P];
 #pragma unroll
-        for (int k = 0; k < FAST_P; k++) {
+        for (int k = 0; k < P; k++) {
             int p1 = pix[k] + 1;
-            in[k] = (p1 >= h.ileft) && (p1 <= h.iright) && (pix[k] < nwl);
-            dl[k] = (float)(wv[k] - h.wlc);
-            dl2[k] = dl[k] * dl[k];
+            in[k] = (p1 >= h.ileft) && (p1 <= h.iright);
+            float dl = (float)(wv[k] - h.wlc);
+            dl2[k] = dl * dl;
         }
         const WingRec *wr = wing + (size_t)j * ntau + t0;
         const CoreRec *cr = core + (size_t)j * ntau + t0;
+        if (full) {
 #pragma unroll
-        for (int d = 0; d < D; d++) {
-            if (t0 + d < ntau) {
-                const WingRec w = wr[d];
-                const float d0 = cr[d].d0;
-                const float A = w.c2 - 0.5f;
+            for (int d = 0; d < D; d++)
+                if (d < nd) line_depth_step<P, false>(wr[d], cr + d, dl2, in, vtab, s[d], c[d]);
+        } else {
 #pragma unroll
-                for (int k = 0; k < FAST_P; k++) {
-                    float x = dl2[k] * w.vv2;
-                    float val;
-                    if (x + A >= 196.0f) {
-                        float num = x + w.c2;
-                        float den = fmaf(x + w.d1, x, d0);
-                        val = w.c1 * __fdividef(num, den);
-                    } else {
-                        const CoreRec cc = cr[d];
-                        val = hv_core32(vtab, dl[k] * cc.vv, cc.a, cc.cop);
-                    }
-                    val = in[k] ? val : 0.0f;
-                    // Kahan-compensated accumulation
-                    float y = val - c[d][k];
-                    float tt = s[d][k] + y;
-                    c[d][k] = (tt - s[d][k]) - y;
-                    s[d][k] = tt;
-                }
-            }
+            for (int d = 0; d < D; d++)
+                if (d < nd) line_depth_step<P, true>(wr[d], cr + d, dl2, in, vtab, s[d], c[d]);
         }
     }
 #pragma unroll
-    for (int k = 0; k < FAST_P; k++) {
+    for (int k = 0; k < P; k++) {
         if (pix[k] >= nwl) continue;
         double *dst = lineopac + (size_t)pix[k] * ntau + t0;
 #pragma unroll
         for (int d = 0; d < D; d++)
-            if (t0 + d < ntau) dst[d] = dst[d] + ((double)s[d][k] - (double)c[d][k]);
+            if (d < nd) dst[d] = dst[d] + ((double)s[d][k] - (double)c[d][k]);
     }
 }
 
-int fsg_launch_accum_fast(cudaStream_t st, int ntau, int nwl, const double *wave, const LineHdr *hdr,
+// Tile width per window-width class: narrow windows get narrow tiles so fewer lanes idle.
+int fsg_class_pix(int cls) { return cls == 0 ? 1 : (cls == 1 ? 2 : 4); }
+
+int fsg_launch_accum_fast(cudaStream_t st, int cls, int ntau, int nwl, const double *wave, const LineHdr *hdr,
                           const WingRec *wing, const CoreRec *core, const int *tile_lo, const int *tile_hi,
                           const float *vtab, double *lineopac) {
-    const int ntiles = (nwl + FAST_TW - 1) / FAST_TW;
-    // depths per warp: at most 18 warps (576 threads) per CTA
-    int D = (ntau + 17) / 18;
-    if (D < 4) D = 4;
+    const int P = fsg_class_pix(cls);
+    const int TW = 32 * P;
+    const int ntiles = (nwl + TW - 1) / TW;
+    // depths per warp: P x D = 16 evaluations per thread and line, at most 18 warps per CTA
+    int D = 16 / P;
+    if ((ntau + D - 1) / D > 18) D = (ntau + 17) / 18;
     int nwarps = (ntau + D - 1) / D;
-#define LAUNCH_D(DD) k_accum_fast<DD><<<ntiles, 32 * nwarps, 0, st>>>(ntau, nwl, wave, hdr, wing, core, \
-                                                                       tile_lo, tile_hi, vtab, lineopac)
-    switch (D) {
-        case 4: LAUNCH_D(4); break;
-        case 5: LAUNCH_D(5); break;
-        case 6: LAUNCH_D(6); break;
-        case 7: LAUNCH_D(7); break;
-        case 8: LAUNCH_D(8); break;
-        default: return FSG_E_ARG;
+#define LAUNCH(DD, PP) k_accum_fast<DD, PP><<<ntiles, 32 * nwarps, 0, st>>>(ntau, nwl, wave, hdr, wing, core, \
+                                                                             tile_lo, tile_hi, vtab, lineopac)
+    if (P == 1) {
+        if (D == 16) LAUNCH(16, 1); else return FSG_E_ARG;
+    } else if (P == 2) {
+        if (D == 8) LAUNCH(8, 2); else return FSG_E_ARG;
+    } else {
+        switch (D) {
+            case 4: LAUNCH(4, 4); break;
+            case 5: LAUNCH(5, 4); break;
+            case 6: LAUNCH(6, 4); break;
+            case 7: LAUNCH(7, 4); break;
+            case 8: LAUNCH(8, 4); break;
+            default: return FSG_E_ARG;
+        }
     }
-#undef LAUNCH_D
+#undef LAUNCH
     return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
 }
 
@@ -165,28 +188,30 @@ __global__ void k_tile_reset(int ntiles, int *lo, int *hi) {
     if (i < ntiles) { lo[i] = 0x7fffffff; hi[i] = -1; }
 }
 
-__global__ void k_tile_span(int64_t nb, const LineHdr *hdr, int *lo, int *hi) {
+__global__ void k_tile_span(int64_t nb, int tw, const LineHdr *hdr, int *lo, int *hi) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= nb) return;
     LineHdr h = hdr[j];
-    int a = (h.ileft - 1) / FAST_TW, b = (h.iright - 1) / FAST_TW;
+    int a = (h.ileft - 1) / tw, b = (h.iright - 1) / tw;
     for (int t = a; t <= b; t++) { atomicMin(&lo[t], (int)j); atomicMax(&hi[t], (int)j); }
 }
 
-int fsg_fast_tiles(int nwl) { return (nwl + FAST_TW - 1) / FAST_TW; }
+// tile count of the narrowest tiles (sizes the lo/hi arrays)
+int fsg_fast_tiles(int nwl) { return (nwl + 31) / 32; }
 
-void fsg_launch_tile_span(cudaStream_t s, int nwl, int64_t nb, const LineHdr *hdr, int *lo, int *hi) {
-    int ntiles = fsg_fast_tiles(nwl);
+void fsg_launch_tile_span(cudaStream_t s, int cls, int nwl, int64_t nb, const LineHdr *hdr, int *lo, int *hi) {
+    int tw = 32 * fsg_class_pix(cls);
+    int ntiles = (nwl + tw - 1) / tw;
     k_tile_reset<<<(ntiles + 255) / 256, 256, 0, s>>>(ntiles, lo, hi);
-    if (nb > 0) k_tile_span<<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(nb, hdr, lo, hi);
+    if (nb > 0) k_tile_span<<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(nb, tw, hdr, lo, hi);
 }
 
 // ---- window-width classes and order-preserving compaction -----------------------------------
-// class 0: windows up to FAST_TW*2 wavelengths; class c: up to FAST_TW*2^(c+1).
+// class 0: windows up to 256 wavelengths; class c: up to 256 * 2^c.
 __device__ __forceinline__ int width_class(int il, int ir) {
     int w = ir - il + 1;
     int c = 0;
-    while ((FAST_TW << (c + 1)) < w && c < 30) c++;
+    while ((CLASS_W0 << (c + 1)) < w && c < 30) c++;
     return c;
 }
 

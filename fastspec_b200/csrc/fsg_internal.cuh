@@ -70,14 +70,25 @@ struct XCoef {
 
 // Fast-path record of one (line, depth): FP32 wing coefficients of HVoigt * LinCop.
 // For s = v^2 + a^2 >= 196 the reference evaluates (voigt.f90:100-101)
-//   H = a (s + 1/2) / (sqrt(pi) (s^2 - v^2 + a^2 + 1/4)),
-// which with x = v^2 and A = a^2 reads c1 (x + c2) / (x^2 + d1 x + d0), with
-//   c1 = LinCop a / sqrt(pi), c2 = A + 1/2, d1 = 2A - 1, d0 = A^2 + A + 1/4.
-struct __align__(16) WingRec { float vv2, c1, c2, d1; };
-struct __align__(16) CoreRec { float d0, vv, cop, a; };
+//   H = a (s + 1/2) / (sqrt(pi) (s^2 - v^2 + a^2 + 1/4)).
+// With y = s + 1/2 the denominator is exactly (y - 1)^2 + 2 a^2, so
+//   H * LinCop = c1 y / ((y - 1)^2 + twoA),  y = dl^2 vv2 + c2,
+// with vv2 = LinVvgt^2, c2 = a^2 + 1/2, twoA = 2 a^2, c1 = LinCop a / sqrt(pi).
+struct __align__(16) WingRec { float vv2, c2, twoA, c1; };
+// Table / continued-fraction region (s < 196): LinVvgt, LinCop, a.
+struct __align__(16) CoreRec { float vv, cop, a, pad; };
 
 // Line header of a retained line inside a block (fast path).
 struct __align__(16) LineHdr { double wlc; int ileft, iright; };   // wlc = Wlcent (offset)
+
+// Zeeman components of a device line list (CSR by line)
+struct ZView {
+    const int32_t *npi, *nsi;
+    const int64_t *pi_off, *si_off;
+    const float *strpi, *strsi;
+    float *splpi, *splsi;             // shifts scaled to [A] (written by the magnetic central pass)
+    const float *rawpi, *rawsi;       // shifts as read (Lande-type units)
+};
 
 // Error reporting
 std::string fsg_cuda_msg(cudaError_t e, const char *what);

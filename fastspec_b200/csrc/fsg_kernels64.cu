@@ -245,12 +245,11 @@ __global__ void k_params_fast(AtmView A, LineView L, const int64_t *__restrict__
         double a2 = av * av;
         WingRec w;
         w.vv2 = (float)(vv * vv);
-        w.c1 = (float)(cop * av * FSG_SQRTPIINV);
         w.c2 = (float)(a2 + 0.5);
-        w.d1 = (float)(2.0 * a2 - 1.0);
+        w.twoA = (float)(2.0 * a2);
+        w.c1 = (float)(cop * av * FSG_SQRTPIINV);
         CoreRec c;
-        c.d0 = (float)(a2 * a2 + a2 + 0.25);
-        c.vv = (float)vv; c.cop = (float)cop; c.a = (float)av;
+        c.vv = (float)vv; c.cop = (float)cop; c.a = (float)av; c.pad = 0.0f;
         wing[(size_t)j * nt + t] = w;
         core[(size_t)j * nt + t] = c;
     }

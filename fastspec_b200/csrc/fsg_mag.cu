@@ -1,18 +1,464 @@
-// fsg_mag.cu -- magnetic (Zeeman / Faraday-Voigt) path: MagLineopCalc and MagRadTranCalc.
-#include "fsg_internal.cuh"
+// fsg_mag.cu -- magnetic path: MagLineopCalc (Zeeman-split Faraday-Voigt opacity into the six
+// profiles) and MagRadTranCalc (Stokes DELO-Bezier solver, plane-parallel).  Built -fmad=false:
+// FP64 throughout, in the reference's operation order.
+//
+//   k_mag_center    MagLineopCalc central pass (synth.f90:1182-1275): Zeeman shifts scaled to
+//                   FP32 (Kz |B| lambda^2, synth.f90:1193-1194), centre test (LineOpacity2),
+//                   doubling search with MagLineOpacity2 and RefineIdx bisection
+//                   (opacity.f90:468-520, 611-675)
+//   k_mag_accum     MagLineOpacity1 per wavelength (opacity.f90:391-464)
+//   k_mag_wide      MagLineOpacity3 for the wide lines, in line order (synth.f90:1341-1361)
+//   k_stokes        StokesPrfPP (solver.f90:265-394) + Solve4x4 (solver.f90:541-588) and the
+//                   Stokes-I flux quadrature
+#include "fsg_fp64.cuh"
 
-extern "C" {
-int fsg_mag_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, int bframe, const double *bfield, int nbfield,
-                        double *maglineopac, int32_t *flags, int32_t *ileft, int32_t *iright, float *linstr,
-                        fsg_stats *stats) {
-    (void)ctx; (void)lines; (void)bframe; (void)bfield; (void)nbfield; (void)maglineopac; (void)flags;
-    (void)ileft; (void)iright; (void)linstr; (void)stats;
-    return FSG_E_STATE;
+#include <algorithm>
+#include <math.h>
+#include <string.h>
+#include <vector>
+
+// MagLineOpacity2 at one wavelength, max over depths of LineOpac/ContOpacL (opacity.f90:468-520)
+__device__ double mag_lineop2_max(const AtmView &A, const XCoef &XC, double Wl, double wlc, int ihe,
+                                  const ZView &Z, int64_t i, int iwl, double dW, const float *vtab,
+                                  const double *anode, const double *aida) {
+    const int nt = A.ntau;
+    double mx = -1.0e308;
+    const int np = Z.npi[i], ns = Z.nsi[i];
+    const float *spi = Z.splpi + Z.pi_off[i], *ssi = Z.splsi + Z.si_off[i];
+    const float *rpi = Z.strpi + Z.pi_off[i], *rsi = Z.strsi + Z.si_off[i];
+    double dWl0 = Wl - wlc;
+    for (int t = 0; t < nt; t++) {
+        double cop, vv, av;
+        xline_depth(A, t, XC, &cop, &vv, &av);
+        double dWl = dWl0;
+        if (ihe > 0) dWl = dWl0 - A.heshf[(ihe - 1) * nt + t];
+        VLine64 VL = vline64(anode, aida, av);
+        double Pp = 0.0, Ps = 0.0;
+        for (int k = 0; k < np; k++) Pp = Pp + (double)rpi[k] * hvoigt_line64(vtab, VL, (dWl - (double)spi[k]) * vv);
+        for (int k = 0; k < ns; k++) Ps = Ps + (double)rsi[k] * hvoigt_line64(vtab, VL, (dWl - (double)ssi[k]) * vv);
+        double lo = fmax(0.5 * Ps, 0.5 * Pp + 0.25 * Ps) * cop;
+        if (A.motype == 1) lo = lo / A.contstd[t];
+        mx = fmax(mx, lo / cont_center(A, iwl, dW, t));
+    }
+    return mx;
 }
-int fsg_mag_lineop_reset(fsg_ctx *ctx) { (void)ctx; return FSG_E_STATE; }
-int fsg_mag_radtran(fsg_ctx *ctx, int bframe, const double *bfield, int nbfield, double *spz, double *spc,
-                    double *sfl, double *sfc) {
-    (void)ctx; (void)bframe; (void)bfield; (void)nbfield; (void)spz; (void)spc; (void)sfl; (void)sfc;
-    return FSG_E_STATE;
+
+__global__ void k_mag_center(AtmView A, LineView L, ZView Z, double Bsplit, const float *__restrict__ vtab,
+                             const double *__restrict__ anode, const double *__restrict__ aida,
+                             int32_t *flags, int32_t *ileft, int32_t *iright, unsigned long long *nkeep) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L.n) return;
+    const int nt = A.ntau;
+    int f = 0;
+    if (L.ismol && L.ismol[i]) f |= FSG_F_MOL;
+    if (L.gvdw[i] > 10.0f) f |= FSG_F_ABO;
+    double wlc = L.wl[i] - A.wfirst;
+    double w = wlc + A.wfirst;
+    // scale the pattern by Kz |B| lambda^2, rounded to FP32 (synth.f90:1193-1194)
+    const int np = Z.npi[i], ns = Z.nsi[i];
+    double smx_pi = -3.4028234663852886e38, smx_si = -3.4028234663852886e38;
+    for (int k = 0; k < np; k++) {
+        float v = (float)((double)Z.rawpi[Z.pi_off[i] + k] * Bsplit * (w * w));
+        Z.splpi[Z.pi_off[i] + k] = v;
+        smx_pi = fmax(smx_pi, fabs((double)v));
+    }
+    for (int k = 0; k < ns; k++) {
+        float v = (float)((double)Z.rawsi[Z.si_off[i] + k] * Bsplit * (w * w));
+        Z.splsi[Z.si_off[i] + k] = v;
+        smx_si = fmax(smx_si, fabs((double)v));
+    }
+    double SplMax = fmax(smx_si, smx_pi);
+    XCoef XC;
+    xline_setup(A, L, i, wlc, f, &XC);
+    if (XC.IxHe > 0) f |= (XC.IxHe << 8);
+    int ihe = XC.IxHe;
+    int iwl = waveidx(A, wlc);
+    double dW = (wlc - A.wave[iwl - 1]) / (A.wave[iwl] - A.wave[iwl - 1]);
+    // non-magnetic centre opacity (synth.f90:1215-1224)
+    double mx = -1.0e308;
+    for (int t = 0; t < nt; t++) {
+        double cop, vv, av;
+        xline_depth(A, t, XC, &cop, &vv, &av);
+        double dWl = 0.0;
+        if (ihe > 0) dWl = 0.0 - A.heshf[(ihe - 1) * nt + t];
+        double lo = hvoigt64(vtab, anode, aida, av, dWl * vv) * cop;
+        if (A.motype == 1) lo = lo / A.contstd[t];
+        mx = fmax(mx, lo / cont_center(A, iwl, dW, t));
+    }
+    int il = 1, ir = A.nwl;
+    if (mx < A.epsopac) f |= FSG_F_WEAK;
+    else {
+        // doubling search (synth.f90:1233-1272)
+        for (int idw = 0; idw < 64; idw++) {
+            double dWo = (0.2 * ldexp(1.0, idw)) * (wlc + A.wfirst) / 5e3;
+            double Wl = wlc + SplMax + dWo;
+            double m2 = mag_lineop2_max(A, XC, Wl, wlc, ihe, Z, i, iwl, dW, vtab, anode, aida);
+            if (m2 < A.epsopac) {
+                // RefineIdx (opacity.f90:611-675), magnetic branch
+                int isw, ikw;
+                if (wlc > 0.5 * (A.wave[0] + A.wave[A.nwl - 1])) { isw = -1; ikw = 0; }
+                else { isw = 1; ikw = 1; }
+                int ia, ib;
+                if (idw == 0) ia = waveidx(A, wlc + (double)isw * SplMax) + ikw;
+                else {
+                    double d1 = (0.2 * ldexp(1.0, idw - 1)) * (wlc + A.wfirst) / 5e3;
+                    ia = waveidx(A, wlc + (double)isw * (SplMax + d1)) + ikw;
+                }
+                ib = waveidx(A, wlc + (double)isw * (SplMax + dWo)) + ikw;
+                for (int it = 0; it < 64 && abs(ia - ib) > 1; it++) {
+                    int im = (ia + ib) / 2;
+                    double m3 = mag_lineop2_max(A, XC, A.wave[im - 1], wlc, ihe, Z, i, iwl, dW, vtab, anode, aida);
+                    if (m3 < A.epsopac) ib = im; else ia = im;
+                }
+                if (isw == 1) { ir = ia; il = waveidx(A, 2.0 * wlc - A.wave[ia - 1]); }
+                else { il = ia; ir = waveidx(A, 2.0 * wlc - A.wave[ia - 1]) + 1; }
+                break;
+            } else if (wlc - SplMax - dWo < A.wave[0] && wlc + SplMax + dWo > A.wave[A.nwl - 1]) break;
+        }
+    }
+    flags[i] = f; ileft[i] = il; iright[i] = ir;
+    unsigned m = __ballot_sync(__activemask(), !(f & FSG_F_WEAK));
+    if ((threadIdx.x & 31) == (__ffs(__activemask()) - 1) && m) atomicAdd(nkeep, (unsigned long long)__popc(m));
 }
+
+// six profiles of one line at one wavelength for depth t (MagLineOpacity1/3 inner loops)
+__device__ __forceinline__ void mag_profiles_t(const AtmView &A, int t, double Wl, double wlc, int ihe,
+                                               const ZView &Z, int64_t i, double cop, double vv, double av,
+                                               const float2 *fvtab, const double *anode, const double *aida,
+                                               double *m) {
+    VLine64 FL = vline64(anode, aida, av);
+    double Xn = cop, sc = vv, Vbase = (Wl - wlc) * sc;
+    if (ihe > 0) Vbase = Vbase - A.heshf[(ihe - 1) * A.ntau + t] * sc;
+    const int np = Z.npi[i], ns = Z.nsi[i];
+    const float *spi = Z.splpi + Z.pi_off[i], *ssi = Z.splsi + Z.si_off[i];
+    const float *rpi = Z.strpi + Z.pi_off[i], *rsi = Z.strsi + Z.si_off[i];
+    for (int k = 0; k < np; k++) {
+        double V = Vbase - (double)spi[k] * sc, Vg, Fv;
+        fvoigt_line64(fvtab, FL, V, &Vg, &Fv);
+        double Str = Xn * (double)rpi[k];
+        m[0] = m[0] + Str * Vg; m[3] = m[3] + Str * Fv;
+    }
+    int Nsh = ns / 2;
+    for (int k = 0; k < Nsh; k++) {
+        double V = Vbase - (double)ssi[k] * sc, Vg, Fv;
+        fvoigt_line64(fvtab, FL, V, &Vg, &Fv);
+        double Str = Xn * (double)rsi[k];
+        m[1] = m[1] + Str * Vg; m[4] = m[4] + Str * Fv;
+    }
+    for (int k = Nsh; k < ns; k++) {
+        double V = Vbase - (double)ssi[k] * sc, Vg, Fv;
+        fvoigt_line64(fvtab, FL, V, &Vg, &Fv);
+        double Str = Xn * (double)rsi[k];
+        m[2] = m[2] + Str * Vg; m[5] = m[5] + Str * Fv;
+    }
+}
+
+// MagLineOpacity1 (opacity.f90:391-464): one warp per wavelength, lanes stride the depths.
+__global__ void k_mag_accum(AtmView A, const double *__restrict__ wl, ZView Z, const int64_t *__restrict__ zmap,
+                            int iwl1, int iwl2, const int *__restrict__ lstart, const int *__restrict__ lstop,
+                            const int32_t *__restrict__ flags, const int32_t *__restrict__ ileft,
+                            const int32_t *__restrict__ iright, int64_t loff, const double3 *__restrict__ p64,
+                            const float2 *__restrict__ fvtab, const double *__restrict__ anode,
+                            const double *__restrict__ aida, double *mlo, double *evals) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    int iwl = iwl1 + warp;
+    if (iwl > iwl2) return;
+    const int nt = A.ntau;
+    double Wl = A.wave[iwl - 1];
+    double cnt = 0.0;
+    for (int t0 = 0; t0 < nt; t0 += 32) {
+        int t = t0 + lane;
+        double m[6] = { 0, 0, 0, 0, 0, 0 };
+        for (int il = lstart[iwl - 1]; il <= lstop[iwl - 1]; il++) {
+            int f = flags[il - 1];
+            if ((f & FSG_F_WEAK) || (f & FSG_F_WIDE) || iwl < ileft[il - 1] || iwl > iright[il - 1]) continue;
+            if (t < nt) {
+                double3 p = p64[(size_t)(il - 1 - loff) * nt + t];
+                mag_profiles_t(A, t, Wl, wl[il - 1] - A.wfirst, (f >> 8) & 255, Z, zmap[il - 1], p.x, p.y, p.z,
+                               fvtab, anode, aida, m);
+            }
+            if (t0 == 0) cnt += 1.0;
+        }
+        if (t < nt) {
+            double *dst = mlo + ((size_t)(iwl - 1) * nt + t) * 6;
+            for (int q = 0; q < 6; q++) {
+                double v = m[q];
+                if (A.motype == 1) v = v / A.contstd[t];
+                dst[q] = dst[q] + v;
+            }
+        }
+    }
+    if (lane == 0 && cnt > 0.0) atomicAdd(evals, cnt * nt);
+}
+
+// MagLineOpacity3 over the wide lines, in line order, one warp per wavelength
+__global__ void k_mag_wide(AtmView A, const double *__restrict__ wl, ZView Z, const int64_t *__restrict__ zmap,
+                           int nwide, const int64_t *__restrict__ widx, const int32_t *__restrict__ flags,
+                           const int32_t *__restrict__ ileft, const int32_t *__restrict__ iright,
+                           const double3 *__restrict__ pw, const float2 *__restrict__ fvtab,
+                           const double *__restrict__ anode, const double *__restrict__ aida, double *mlo) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    int iwl = 1 + warp;
+    if (iwl > A.nwl) return;
+    const int nt = A.ntau;
+    double Wl = A.wave[iwl - 1];
+    for (int q = 0; q < nwide; q++) {
+        int64_t il = widx[q];
+        if (iwl < ileft[il] || iwl > iright[il]) continue;
+        int ihe = (flags[il] >> 8) & 255;
+        for (int t = lane; t < nt; t += 32) {
+            double m[6] = { 0, 0, 0, 0, 0, 0 };
+            double3 p = pw[(size_t)q * nt + t];
+            mag_profiles_t(A, t, Wl, wl[il] - A.wfirst, ihe, Z, zmap[il], p.x, p.y, p.z, fvtab, anode, aida, m);
+            double *dst = mlo + ((size_t)(iwl - 1) * nt + t) * 6;
+            for (int r = 0; r < 6; r++) {
+                double v = m[r];
+                if (A.motype == 1) v = v / A.contstd[t];
+                dst[r] = dst[r] + v;
+            }
+        }
+    }
+}
+
+__global__ void k_mag_params(AtmView A, LineView L, int64_t n, const int64_t *__restrict__ list, int64_t off,
+                             const int32_t *__restrict__ flags, double3 *p) {
+    int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    int64_t i = list ? list[q] : off + q;
+    int f = flags[i];
+    if (f & FSG_F_WEAK) return;
+    XCoef XC;
+    xline_setup(A, L, i, L.wl[i] - A.wfirst, f, &XC);
+    for (int t = 0; t < A.ntau; t++) {
+        double cop, vv, av;
+        xline_depth(A, t, XC, &cop, &vv, &av);
+        p[(size_t)q * A.ntau + t] = make_double3(cop, vv, av);
+    }
+}
+
+// ================================================================================================
+// StokesPrfPP (solver.f90:265-394).  CTA = one wavelength, warp = one angle.  Lanes build the
+// per-depth propagation data (6 distinct matrix elements), TauStep and CentDer in shared memory;
+// lane 0 runs the sequential DELO sweep with the reference's 4x4 algebra.  CentDer of the full
+// matrix is taken through its 6 distinct elements: CentDer commutes with negation exactly and
+// maps the zero diagonal to zero.
+// ================================================================================================
+#define STK_FIELDS 22   // per depth: PhiI, 6 K, 6 KD, 4 SRC4, 4 SRD, Deltau
+
+__device__ __forceinline__ void centder_pt(const double *D, const double *Y, int stride, int N, int k, double *out) {
+    // Yp at 0-based depth k for one component with values Y[t * stride]
+    if (k == 0) { *out = (Y[stride] - Y[0]) / D[0]; return; }
+    if (k == N - 1) { *out = (Y[(N - 1) * stride] - Y[(N - 2) * stride]) / D[N - 2]; return; }
+    double Dx = D[k - 1], Dx1 = D[k];
+    double InvDx = 1.0 / Dx, InvDx1 = 1.0 / Dx1;
+    double Lambda = (1.0 + Dx1 / (Dx + Dx1)) / 3.0, Lambda1 = 1.0 - Lambda;
+    double Der = (Y[k * stride] - Y[(k - 1) * stride]) * InvDx, Der1 = (Y[(k + 1) * stride] - Y[k * stride]) * InvDx1;
+    *out = (Der * Der1 > 0.0) ? (Der / (Lambda * Der1 + Lambda1 * Der)) * Der1 : 0.0;
+}
+
+// full 4x4 propagation matrix from its 6 distinct elements (solver.f90:311-326), column-major
+__device__ __forceinline__ void build_k(const double *e, double *K) {
+    double PhiQ = e[0], PhiU = e[1], PhiV = e[2], PsiQ = e[3], PsiU = e[4], PsiV = e[5];
+    K[0] = 0.0;   K[4] = PhiQ;  K[8] = PhiU;   K[12] = PhiV;
+    K[1] = PhiQ;  K[5] = 0.0;   K[9] = PsiV;   K[13] = -PsiU;
+    K[2] = PhiU;  K[6] = -PsiV; K[10] = 0.0;   K[14] = PsiQ;
+    K[3] = PhiV;  K[7] = PsiU;  K[11] = -PsiQ; K[15] = 0.0;
+}
+
+__device__ void solve4x4(const double *A, const double *B, double *X) {
+    double M[16], R[4];
+    for (int q = 0; q < 16; q++) M[q] = A[q];
+    for (int q = 0; q < 4; q++) R[q] = B[q];
+#define MM(i, j) M[((i) - 1) + 4 * ((j) - 1)]
+    for (int k = 1; k <= 3; k++) {
+        int ip = k; double p = fabs(MM(k, k));
+        for (int i = k + 1; i <= 4; i++) if (fabs(MM(i, k)) > p) { p = fabs(MM(i, k)); ip = i; }
+        if (ip != k) {
+            for (int j = k; j <= 4; j++) { double sw = MM(k, j); MM(k, j) = MM(ip, j); MM(ip, j) = sw; }
+            double sw = R[k - 1]; R[k - 1] = R[ip - 1]; R[ip - 1] = sw;
+        }
+        p = 1.0 / MM(k, k);
+        for (int i = k + 1; i <= 4; i++) {
+            double f = MM(i, k) * p;
+            for (int j = k + 1; j <= 4; j++) MM(i, j) = MM(i, j) - f * MM(k, j);
+            R[i - 1] = R[i - 1] - f * R[k - 1];
+        }
+    }
+    X[3] = R[3] / MM(4, 4);
+    X[2] = (R[2] - MM(3, 4) * X[3]) / MM(3, 3);
+    X[1] = (R[1] - MM(2, 3) * X[2] - MM(2, 4) * X[3]) / MM(2, 2);
+    X[0] = (R[0] - MM(1, 2) * X[1] - MM(1, 3) * X[2] - MM(1, 4) * X[3]) / MM(1, 1);
+#undef MM
+}
+
+__global__ void k_stokes(AtmView A, const double *__restrict__ lineopac, const double *__restrict__ mlo,
+                         const double *__restrict__ rhox, int nmu, const double *__restrict__ xmu,
+                         const double *__restrict__ wmu, const double *__restrict__ geo, double *spz, double *sfl) {
+    extern __shared__ double sm[];
+    const int iwl = blockIdx.x;                  // 0-based
+    const int im = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int N = A.ntau;
+    double *S = sm + (size_t)im * STK_FIELDS * N;          // this angle's arrays, field-major
+    double *PhiI = S, *Kv = S + N, *KD = S + 7 * N, *SRC4 = S + 13 * N, *SRD = S + 17 * N, *Dt = S + 21 * N;
+    double *Src = sm + (size_t)nmu * STK_FIELDS * N;       // shared Planck source [N]
+    __shared__ double Iout[16];
+    const double PlkC1 = FSG_HC * FSG_VC * 1e13 / FSG_KBOLT;
+    double wl = A.wave[iwl] + A.wfirst;
+    if (threadIdx.x < N) {
+        double C1 = PlkC1 / wl, C2 = exp(50.7649141 - 5.0 * log(wl));
+        Src[threadIdx.x] = C2 / (exp(C1 / A.xi[XI_T * N + threadIdx.x]) - 1.0);
+    }
+    __syncthreads();
+    if (im < nmu) {
+        double SPhi2 = geo[0 * nmu + im], CPhi2 = geo[1 * nmu + im], CPhi = geo[2 * nmu + im];
+        double S2Psi = geo[3 * nmu + im], C2Psi = geo[4 * nmu + im];
+        for (int t = lane; t < N; t += 32) {
+            const double *m = mlo + ((size_t)iwl * N + t) * 6;
+            double Php = m[0], Phb = m[1], Phr = m[2], Psp = m[3], Psb = m[4], Psr = m[5];
+            double PI = 0.5 * (Php * SPhi2 + 0.5 * (Phr + Phb) * (1.0 + CPhi2)) + lineopac[(size_t)iwl * N + t] +
+                        A.contopac[(size_t)iwl * N + t];
+            double InvPhiI = 1.0 / PI;
+            double Sabs = 0.5 * (Php - 0.5 * (Phr + Phb)) * SPhi2;
+            double PhiQ = Sabs * C2Psi * InvPhiI, PhiU = Sabs * S2Psi * InvPhiI;
+            double PhiV = 0.5 * (Phr - Phb) * CPhi * InvPhiI;
+            double Sdis = 0.5 * (Psp - 0.5 * (Psr + Psb)) * SPhi2;
+            double PsiQ = Sdis * C2Psi * InvPhiI, PsiU = Sdis * S2Psi * InvPhiI;
+            double PsiV = 0.5 * (Psr - Psb) * CPhi * InvPhiI;
+            PhiI[t] = PI;
+            Kv[0 * N + t] = PhiQ; Kv[1 * N + t] = PhiU; Kv[2 * N + t] = PhiV;
+            Kv[3 * N + t] = PsiQ; Kv[4 * N + t] = PsiU; Kv[5 * N + t] = PsiV;
+            double sr = Src[t];
+            SRC4[0 * N + t] = sr; SRC4[1 * N + t] = sr * PhiQ; SRC4[2 * N + t] = sr * PhiU; SRC4[3 * N + t] = sr * PhiV;
+        }
+        __syncwarp();
+        // TauStep (solver.f90:591-615) with Xmu(im)
+        double Xmu = xmu[im];
+        for (int t = lane; t < N - 1; t += 32) {
+            if (t == 0) {
+                double Dx1 = (rhox[1] - rhox[0]) / Xmu;
+                double Yp = (PhiI[1] - PhiI[0]) / Dx1;
+                Dt[0] = Dx1 * (PhiI[1] + 2.0 * PhiI[0] + Dx1 / 2.0 * Yp) / 3.0;
+            } else {
+                int k = t + 1;
+                double Dx = (rhox[k - 1] - rhox[k - 2]) / Xmu, Dx1 = (rhox[k] - rhox[k - 1]) / Xmu;
+                double Der = (PhiI[k - 1] - PhiI[k - 2]) / Dx, Der1 = (PhiI[k] - PhiI[k - 1]) / Dx1, Yp;
+                if (Der * Der1 > 0.0) {
+                    double Lambda = (1.0 + Dx1 / (Dx + Dx1)) / 3.0;
+                    Yp = (Der / (Lambda * Der1 + (1.0 - Lambda) * Der)) * Der1;
+                } else Yp = 0.0;
+                Dt[k - 1] = Dx1 * (PhiI[k] + 2.0 * PhiI[k - 1] + Dx1 / 2.0 * Yp) / 3.0;
+            }
+        }
+        __syncwarp();
+        // CentDer of SRC4 (4 rows) and of the 6 distinct matrix elements
+        for (int e = lane; e < 10 * N; e += 32) {
+            int row = e / N, t = e - row * N;
+            if (row < 4) centder_pt(Dt, SRC4 + row * N, 1, N, t, &SRD[row * N + t]);
+            else centder_pt(Dt, Kv + (row - 4) * N, 1, N, t, &KD[(row - 4) * N + t]);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            double K1[16], K0[16], KD0[16], XKA[16], XKB[16], QA[16], QB[16], AA[16], e6[6], d6[6];
+            double XINT2[4] = { SRC4[N - 1], 0.0, 0.0, 0.0 }, XINT1[4];
+            for (int q = 0; q < 6; q++) { e6[q] = Kv[q * N + N - 1]; d6[q] = KD[q * N + N - 1]; }
+            build_k(e6, K0); build_k(d6, KD0);
+            for (int j = 0; j < 4; j++) for (int i = 0; i < 4; i++) {
+                double acc = 0.0;
+                for (int q = 0; q < 4; q++) acc = acc + K0[i + 4 * q] * K0[q + 4 * j];
+                XKB[i + 4 * j] = acc + KD0[i + 4 * j];
+            }
+            for (int q = 0; q < 16; q++) K1[q] = K0[q];         // XK at k1
+            for (int k = N - 2; k >= 0; k--) {
+                int k1 = k + 1;
+                double Dtau = Dt[k], Dtau05 = 0.5 * Dtau, Eps, Alpha, Beta, Gamma;
+                delo_coef(Dtau, Eps, Alpha, Beta, Gamma);
+                Gamma = Gamma * 0.5;
+                for (int q = 0; q < 6; q++) { e6[q] = Kv[q * N + k]; d6[q] = KD[q * N + k]; }
+                build_k(e6, K0); build_k(d6, KD0);
+                for (int q = 0; q < 16; q++) XKA[q] = XKB[q];
+                for (int j = 0; j < 4; j++) for (int i = 0; i < 4; i++) {
+                    double acc = 0.0;
+                    for (int q = 0; q < 4; q++) acc = acc + K0[i + 4 * q] * K0[q + 4 * j];
+                    XKB[i + 4 * j] = acc + KD0[i + 4 * j];
+                }
+                for (int j = 0; j < 4; j++) for (int i = 0; i < 4; i++) {
+                    int e = i + 4 * j;
+                    QA[e] = Dtau05 * XKA[e] + (Dtau05 - 1.0) * K1[e];
+                    QB[e] = -(Dtau05 * XKB[e]) - (Dtau05 + 1.0) * K0[e];
+                    AA[e] = ((i == j) ? 1.0 : 0.0) + Alpha * K0[e] - Gamma * QB[e];
+                }
+                double GD = Gamma * Dtau05;
+                for (int i = 0; i < 4; i++) {
+                    double m1 = 0.0, m2 = 0.0, m3 = 0.0, m4 = 0.0;
+                    for (int q = 0; q < 4; q++) {
+                        m1 = m1 + K1[i + 4 * q] * XINT2[q];
+                        m2 = m2 + QA[i + 4 * q] * XINT2[q];
+                        m3 = m3 + K1[i + 4 * q] * SRC4[q * N + k1];
+                        m4 = m4 + K0[i + 4 * q] * SRC4[q * N + k];
+                    }
+                    XINT1[i] = Eps * XINT2[i] - Beta * m1 + Gamma * m2 + (Beta + Gamma) * SRC4[i * N + k1]
+                             - GD * m3 + (Alpha + Gamma) * SRC4[i * N + k] + GD * m4
+                             + GD * (SRD[i * N + k] - SRD[i * N + k1]);
+                }
+                solve4x4(AA, XINT1, XINT2);
+                for (int q = 0; q < 16; q++) K1[q] = K0[q];
+            }
+            for (int q = 0; q < 4; q++) spz[((size_t)iwl * 4 + q) * nmu + im] = XINT2[q];
+            Iout[im] = XINT2[0];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && sfl) {
+        double a = 0.0;
+        for (int q = 0; q < nmu; q++) a = a + Iout[q] * wmu[q];
+        sfl[iwl] = a;
+    }
+}
+
+// ================================================================================================
+// host drivers
+// ================================================================================================
+struct fsg_ctx;
+AtmView fsg_view(const fsg_ctx *ctx);
+
+size_t fsg_stokes_smem(int nt, int nmu) { return sizeof(double) * ((size_t)nmu * STK_FIELDS * nt + nt); }
+
+int fsg_launch_stokes(cudaStream_t s, const AtmView &A, const double *lineopac, const double *mlo, const double *rhox,
+                      int nmu, const double *xmu, const double *wmu, const double *geo, double *spz, double *sfl) {
+    size_t sm = fsg_stokes_smem(A.ntau, nmu);
+    if (sm > 220 * 1024) return FSG_E_ARG;
+    cudaFuncSetAttribute(k_stokes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    k_stokes<<<A.nwl, 32 * nmu, sm, s>>>(A, lineopac, mlo, rhox, nmu, xmu, wmu, geo, spz, sfl);
+    return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
+}
+
+void fsg_launch_mag_center(cudaStream_t s, const AtmView &A, const LineView &L, const ZView &Z, double Bsplit,
+                           const VoigtTables &T, int32_t *flags, int32_t *ileft, int32_t *iright,
+                           unsigned long long *nkeep) {
+    if (L.n > 0)
+        k_mag_center<<<(unsigned)((L.n + 63) / 64), 64, 0, s>>>(A, L, Z, Bsplit, T.vtab, T.anode, T.aida, flags, ileft,
+                                                                iright, nkeep);
+}
+
+void fsg_launch_mag_params(cudaStream_t s, const AtmView &A, const LineView &L, int64_t n, const int64_t *list,
+                           int64_t off, const int32_t *flags, double3 *p) {
+    if (n > 0) k_mag_params<<<(unsigned)((n + 63) / 64), 64, 0, s>>>(A, L, n, list, off, flags, p);
+}
+
+void fsg_launch_mag_accum(cudaStream_t s, const AtmView &A, const double *wl, const ZView &Z, const int64_t *zmap,
+                          int iwl1, int iwl2, const int *lstart, const int *lstop, const int32_t *flags,
+                          const int32_t *ileft, const int32_t *iright, int64_t loff, const double3 *p64,
+                          const VoigtTables &T, double *mlo, double *evals) {
+    int nw = iwl2 - iwl1 + 1;
+    if (nw > 0)
+        k_mag_accum<<<(nw + 7) / 8, 256, 0, s>>>(A, wl, Z, zmap, iwl1, iwl2, lstart, lstop, flags, ileft, iright, loff,
+                                                 p64, T.fvtab, T.anode, T.aida, mlo, evals);
+}
+
+void fsg_launch_mag_wide(cudaStream_t s, const AtmView &A, const double *wl, const ZView &Z, const int64_t *zmap,
+                         int nwide, const int64_t *widx, const int32_t *flags, const int32_t *ileft,
+                         const int32_t *iright, const double3 *pw, const VoigtTables &T, double *mlo) {
+    if (nwide > 0)
+        k_mag_wide<<<(A.nwl + 7) / 8, 256, 0, s>>>(A, wl, Z, zmap, nwide, widx, flags, ileft, iright, pw, T.fvtab,
+                                                   T.anode, T.aida, mlo);
 }

@@ -392,5 +392,77 @@ def make_pins(gold):
         print(name, "lines", extra.n, "region pixels", i1 - i0 + 1)
 
 
+def mirrored_components(patterns):
+    """Zeeman components as ReadAscMag stores an explicit block with a positive sigma count:
+    pi as read, sigma mirrored (blue = -shift first, then red), ioutils.f90:1393-1410."""
+    npi, nsi, spl_pi, str_pi, spl_si, str_si = [], [], [], [], [], []
+    for spi, rpi, ss, rs in patterns:
+        npi.append(len(spi)); nsi.append(2 * len(ss))
+        spl_pi += list(spi); str_pi += list(rpi)
+        spl_si += list(-np.asarray(ss)) + list(ss); str_si += list(rs) + list(rs)
+    f = lambda a: np.asarray(a, np.float32)
+    return (np.asarray(npi, np.int32), np.asarray(nsi, np.int32), f(spl_pi), f(str_pi), f(spl_si), f(str_si))
+
+
+def make_mag_pin(gold):
+    """Stokes IQUV of seeded Zeeman lines (explicit patterns), BFRAME 1, |B| = 2 kG at
+    inclination 60 deg and azimuth 30 deg, 9 angles, on 6040-6046 A at 0.002 A."""
+    teff, logg, ntau, species, ismol, _, _, vmic, molbrd, _, _ = CONFIGS["magnetic"]
+    model = W.eddington_model(teff, logg, ntau)
+    state = load_state("magnetic")
+    grid = (6000.0, 6043.0, 0.002, 0)
+    region = (6040.0, 6043.0)
+    bfield = (2000.0, 60.0, 30.0)
+    extra = W.zeeman_lines(60, 6040.3, 6042.7, W.SEED0 + 2)
+    pgf = np.load(os.path.join(HERE, "atm_magnetic.npz"))["probe_loggf"]
+    probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
+    merged = merge([probes, extra])
+    pats = zeeman_blocks(merged)
+    for q, (spi, rpi, ss, rs) in enumerate(pats):
+        assert len(spi) >= 1 and len(ss) >= 1, "empty Zeeman branch"
+    with tempfile.TemporaryDirectory() as wd:
+        W.write_krz(os.path.join(wd, "model.krz"), model)
+        merged.write_z(os.path.join(wd, "lines.z"), grid[0], grid[1], patterns=pats)
+        deck = ("wave=%.4f, %.4f, %.6f, %d\nsave=0, 0, 1, 1, 1\nvmic=%.3f\nmolbrd=%d\n"
+                "lines=\n-1  lines.z\n\nmodel=model.krz\nmus=9\nbframe=1\nbfield=%g, %g, %g\n"
+                % (grid + (vmic, molbrd) + bfield))
+        log = run_ref(wd, deck)
+        assert "polarised" in log, log
+        co = fsio.read_opac(os.path.join(wd, "fs_contop.bin"))
+        sp = fsio.read_spec(os.path.join(wd, "fs_spec.bin"))
+        fl = fsio.read_flux(os.path.join(wd, "fs_flux.bin"))
+    for k in ("rhox", "T", "xne", "xna", "rho"):
+        assert np.array_equal(co[k], state[k]), "EOS state differs from the recovered one: " + k
+    assert sp["magnetic"]
+    wave = co["wave"]
+    sel = (wave >= region[0] - 1e-9) & (wave <= region[1] + 1e-9)
+    i0, i1 = (int(x) for x in np.nonzero(sel)[0][[0, -1]])
+    comp = mirrored_components(pats)
+    # the probes' windows must end before the region (oracle, full continuum of this run)
+    g = dict(wmode=grid[3], wstart=grid[0], wend=grid[1], dstep=grid[2])
+    S = oracle.State(g, state, contopac=co["opac"], vmicro=vmic, molbrd=molbrd)
+    npr = probes.n
+    pa = probes.arrays()
+    pc = mirrored_components(pats[:npr])
+    rp = oracle.mag_lineop_calc(S, oracle.Lines(**lines_args(probes), kind=2, zeeman=pc), 1, np.array(bfield))
+    assert rp["iright"].max() < i0 + 1, "probe windows reach the pin region"
+    # keep only the seeded lines (the region's opacity comes from them alone)
+    a = {k: v[npr:] for k, v in merged.arrays().items()}
+    comp = mirrored_components(pats[npr:])
+    np.savez_compressed(
+        os.path.join(gold, "pin_magnetic.npz"),
+        grid=np.array(grid, np.float64), i0=i0, i1=i1, atm="magnetic", bframe=1, bfield=np.array(bfield),
+        species=np.array(["%s %d" % s for s in species]), vmicro=vmic, molbrd=molbrd,
+        contopac=co["opac"][i0:i1 + 1], wave=wave[i0:i1 + 1], xmu=sp["xmu"],
+        spz=sp["spz"][i0:i1 + 1], spc=sp["spc"][i0:i1 + 1], sfl=fl["sfl"][i0:i1 + 1], sfc=fl["sfc"][i0:i1 + 1],
+        z_npi=comp[0], z_nsi=comp[1], z_spl_pi=comp[2], z_str_pi=comp[3], z_spl_si=comp[4], z_str_si=comp[5],
+        **{"line_" + k: v for k, v in a.items()})
+    print("pin_magnetic lines", merged.n, "region pixels", i1 - i0 + 1)
+
+
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "magpin":
+        make_mag_pin(os.path.join(REPO, "tests", "golden"))
+    else:
+        main()
+        make_mag_pin(os.path.join(REPO, "tests", "golden"))

@@ -149,7 +149,10 @@ class LineList:
     Zeeman components (optional): npi, nsi (int), comp arrays CSR by line.
     """
 
-    def __init__(self, species, wl, loggf, elo, lgrad, lgqst, lgvdw, spc, ismol, zeeman=None):
+    def __init__(self, species, wl, loggf, elo, lgrad, lgqst, lgvdw, spc, ismol, zeeman=None, exact=True):
+        """exact=True: values as the reference parses the printed decimals (libm powf, for
+        lists that are also run through the reference); exact=False: FP32 rounding and numpy's
+        vectorised power (large benchmark lists that only the GPU path and the oracle read)."""
         self.species = species
         order = np.argsort(wl, kind="stable")
         self.wl = np.asarray(wl, np.float64)[order]
@@ -159,14 +162,21 @@ class LineList:
         self.spc = np.asarray(spc, np.int32)[order]
         self.ismol = np.asarray(ismol, np.int32)[order]
         t = self._txt
-        self.elo = f32_of_text(t["elo"], "%.4f")
-        self.gf = pow10f(f32_of_text(t["loggf"], "%.3f"))
-        lg = f32_of_text(t["lgrad"], "%.3f")
-        self.grad = np.where((lg < 20.0) & (lg > 0.0), pow10f(lg), lg).astype(np.float32)
-        lq = f32_of_text(t["lgqst"], "%.3f")
-        self.gqst = np.where(lq < 0.0, pow10f(lq), lq).astype(np.float32)
-        lv = f32_of_text(t["lgvdw"], "%.3f")
-        self.gvdw = np.where(lv < 0.0, pow10f(lv), lv).astype(np.float32)
+        if exact:
+            conv, p10 = f32_of_text, pow10f
+        else:
+            conv = lambda v, fmt: np.asarray(v, np.float32)
+            p10 = lambda v: np.power(np.float32(10.0), np.asarray(v, np.float32)).astype(np.float32)
+        self.elo = conv(t["elo"], "%.4f")
+        self.gf = p10(conv(t["loggf"], "%.3f"))
+        lg = conv(t["lgrad"], "%.3f")
+        self.grad = np.where((lg < 20.0) & (lg > 0.0), p10(lg), lg).astype(np.float32)
+        lq = conv(t["lgqst"], "%.3f")
+        self.gqst = np.where(lq < 0.0, p10(lq), lq).astype(np.float32)
+        lv = conv(t["lgvdw"], "%.3f")
+        self.gvdw = np.where(lv < 0.0, p10(lv), lv).astype(np.float32)
+        if not exact:
+            self._txt = None
         self.zeeman = None
         if zeeman is not None:
             jlo, jup, glo, gup = (np.asarray(a)[order] for a in zeeman)
@@ -204,7 +214,7 @@ class LineList:
                     gvdw=self.gvdw, spc=self.spc, ismol=self.ismol)
 
 
-def atomic_lines(n, wmin, wmax, seed, species=ATOMIC_C0, probs=ATOMIC_C0_P):
+def atomic_lines(n, wmin, wmax, seed, species=ATOMIC_C0, probs=ATOMIC_C0_P, exact=True):
     """Config-0 distributions: lambda0 ~ U, species mix, log gf ~ N(-2, 1.2) clipped [-6, 1],
     E_low ~ U(0, 6) eV, log Grad ~ U(7, 9), log G4/Ne ~ U(-7, -4), log G6/NH ~ U(-8, -7)."""
     rng = np.random.default_rng(seed)
@@ -215,10 +225,10 @@ def atomic_lines(n, wmin, wmax, seed, species=ATOMIC_C0, probs=ATOMIC_C0_P):
     lgrad = rng.uniform(7.0, 9.0, n)
     lgqst = rng.uniform(-7.0, -4.0, n)
     lgvdw = rng.uniform(-8.0, -7.0, n)
-    return LineList(species, wl, loggf, elo, lgrad, lgqst, lgvdw, spc, np.zeros(n, np.int32))
+    return LineList(species, wl, loggf, elo, lgrad, lgqst, lgvdw, spc, np.zeros(n, np.int32), exact=exact)
 
 
-def molecular_lines(n, wmin, wmax, seed, species=MOLECULES_C1):
+def molecular_lines(n, wmin, wmax, seed, species=MOLECULES_C1, exact=True):
     """Config-1 distributions: wavenumber uniform over [1e8/wmax, 1e8/wmin] cm^-1 (lambda in A),
     four species at 25 % each, log gf ~ N(-5, 1.5), E_low ~ Exp(1 eV) capped at 5 eV,
     log G6/NH ~ U(-8, -7), radiative damping from the classical fallback (Grad = 0)."""
@@ -229,8 +239,8 @@ def molecular_lines(n, wmin, wmax, seed, species=MOLECULES_C1):
     loggf = rng.normal(-5.0, 1.5, n)
     elo = np.minimum(rng.exponential(1.0, n), 5.0)
     lgvdw = rng.uniform(-8.0, -7.0, n)
-    z = np.zeros(n)
-    return LineList(species, wl, loggf, elo, z, z, lgvdw, spc, np.ones(n, np.int32))
+    z = np.zeros(n, np.float32)
+    return LineList(species, wl, loggf, elo, z, z, lgvdw, spc, np.ones(n, np.int32), exact=exact)
 
 
 def zeeman_lines(n, wmin, wmax, seed):

@@ -77,6 +77,8 @@ typedef struct {
     int64_t nlines_in, nlines_used, nwide, nweak, nblocks;
     double  line_evals;     /* profile evaluations inside windows (x components if magnetic) */
     double  ms_center, ms_params, ms_accum, ms_total;   /* device time per stage [ms] */
+    int64_t accum_launches; /* launches of the accumulation kernel */
+    double  ms_accum_kernels;   /* summed device time of those launches [ms] */
 } fsg_stats;
 
 /* ---- context ------------------------------------------------------------------------- */
@@ -84,6 +86,11 @@ int         fsg_create(const fsg_config *cfg, fsg_ctx **out);
 void        fsg_destroy(fsg_ctx *ctx);
 const char *fsg_last_error(const fsg_ctx *ctx);
 int         fsg_version(void);
+/* Number of kernels this context has launched since it was created (monotonic). */
+int64_t     fsg_kernel_launches(const fsg_ctx *ctx);
+/* The context's CUDA stream (a cudaStream_t, as void*), for callers that time or order work
+ * on it.  Every entry point returns after its work on this stream has completed. */
+void       *fsg_cuda_stream(fsg_ctx *ctx);
 
 /* ---- set-up (the reference's Init, synth.f90:22-331) ------------------------------------ */
 /* Wavelength grid of Init (synth.f90:56-74): wave[] = offsets from wstart.  Returns Nwl in

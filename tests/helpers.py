@@ -52,3 +52,11 @@ def pin_setup(d):
     co[:i0] = d["contopac"][0]
     co[i1 + 1:] = d["contopac"][-1]
     return grid, st, meta, co
+
+
+def mag_pin_setup(d):
+    """(grid, state, contopac full grid, line arrays, zeeman tuple) of the magnetic pin."""
+    grid, st, meta, co = pin_setup(d)
+    lines = pin_lines(d)
+    z = (d["z_npi"], d["z_nsi"], d["z_spl_pi"], d["z_str_pi"], d["z_spl_si"], d["z_str_si"])
+    return grid, st, co, lines, z

@@ -226,9 +226,11 @@ def test_fp64_path_against_reference_pins(fsg, name):
 def test_blocks_equal_single_block(fsg, oracle_mod):
     """A tiny LIMITRAM forces many blocks / segments; results must not change."""
     grid, st, co, L = solar_case(n=800, span=6.0, seed=5)
-    for prec, tol in ((fsg.PREC_MIXED, 1e-6), (fsg.PREC_FP64, 1e-13)):
+    # FP64 blocks hold limitram / (24 B x Ntau) lines: 1e-3 GB -> ~740 of 800 lines, two segments
+    # (much smaller blocks trip the reference's own segmentation error, synth.f90:1035-1040)
+    for prec, tol, ram in ((fsg.PREC_MIXED, 1e-6, 3e-5), (fsg.PREC_FP64, 1e-13, 1e-3)):
         a = ctx_for(fsg, grid, st, co, prec).lineop_calc(fsg_lines(fsg, L))
-        b = ctx_for(fsg, grid, st, co, prec, limitram_gb=3e-5).lineop_calc(fsg_lines(fsg, L))
+        b = ctx_for(fsg, grid, st, co, prec, limitram_gb=ram).lineop_calc(fsg_lines(fsg, L))
         assert b["stats"]["nblocks"] > a["stats"]["nblocks"]
         m = a["lineopac"] > 0
         assert np.array_equal(m, b["lineopac"] > 0)
@@ -323,3 +325,11 @@ def test_call_order_errors(fsg):
         C.lineop_calc(fsg_lines(fsg, L))
     with pytest.raises(fsg.FsgError):
         C.set_contopac(co[:-1])
+
+
+def test_segmentation_overflow_is_reported(fsg):
+    """A block too small for the lines at one wavelength stops with the reference's message."""
+    grid, st, co, L = solar_case(n=800, span=6.0, seed=5)
+    C = ctx_for(fsg, grid, st, co, fsg.PREC_FP64, limitram_gb=3e-5)
+    with pytest.raises(fsg.FsgError, match="segmentation"):
+        C.lineop_calc(fsg_lines(fsg, L))

@@ -1,0 +1,115 @@
+"""GPU parity of the magnetic path (MagLineopCalc + MagRadTranCalc) against the oracle and the
+reference.  Both run in FP64 in the reference's operation order, so:
+  * window indices and flags: identical;
+  * the six Zeeman profiles MagLineOpac: 1e-11 of the local absorption scale (dispersion
+    profiles change sign, so the scale is the max of the absorption profiles at that depth);
+  * Stokes I and Ic: 1e-9 relative; Q, U, V: 1e-9 of Ic (libm ulps amplified by the DELO
+    coefficients just above their Taylor branch, solver.f90:357-370);
+  * against the reference's own Stokes spectra: 1e-8.
+"""
+import numpy as np
+import pytest
+
+import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+def mag_ctx(fsg, grid, st, co, nmu=9, vmicro=1.0, molbrd=0):
+    C = fsg.Context(precision=fsg.PREC_FP64, vmicro=vmicro, molbrd=molbrd)
+    C.set_grid(grid["wmode"], grid["wstart"], grid["wend"], grid["dstep"])
+    C.set_atmosphere(st)
+    C.set_contopac(co)
+    x, w, _ = fsg.mu_quadrature(1, nmu)
+    C.set_mu(x, w)
+    return C, x, w
+
+
+def zeeman_case(n=60, w0=6040.0, span=3.0, seed=31, nmu=9):
+    st, meta = H.load_atm("magnetic")
+    from fastspec_b200 import workloads as W
+    import fastspec_b200 as F
+    import oracle
+    grid = dict(wmode=0, wstart=w0, wend=w0 + span, dstep=0.002)
+    wave = F.make_grid(0, w0, w0 + span, 0.002) + w0
+    co = H.contopac_on(meta, wave)
+    L = W.zeeman_lines(n, w0 + 0.2, w0 + span - 0.2, seed)
+    jlo, jup, glo, gup = L.zeeman
+    pats = []
+    for i in range(L.n):
+        p = oracle.zeeman_pattern(jlo[i], jup[i], glo[i], gup[i])
+        if len(p[0]) == 0 or len(p[2]) == 0:
+            p = oracle.zeeman_pattern(1.0, 0.0, 1.0, 1.0)
+        pats.append(p)
+    import sys, os
+    sys.path.insert(0, os.path.join(H.REPO, "fastspec_b200", "data"))
+    from make_atmospheres import mirrored_components
+    return grid, st, co, L.arrays(), mirrored_components(pats)
+
+
+def run_both(fsg, oracle_mod, grid, st, co, lines, z, bframe, bfield, nmu=9):
+    C, x, w = mag_ctx(fsg, grid, st, co, nmu=nmu)
+    g = C.mag_lineop_calc(fsg.LineList.from_arrays(lines, zeeman=z), bframe, bfield)
+    spz, spc, sfl, sfc = C.mag_radtran(bframe, bfield)
+    S = oracle_mod.State(grid, st, contopac=co, vmicro=1.0)
+    r = oracle_mod.mag_lineop_calc(S, oracle_mod.Lines(**lines, kind=2, zeeman=z), bframe, np.asarray(bfield, float))
+    ospz, ospc = oracle_mod.mag_radtran(S, x, bframe, np.asarray(bfield, float), np.zeros((S.nwl, S.ntau)),
+                                        r["maglineopac"])
+    return g, r, (spz, spc, sfl, sfc), (ospz, ospc), w
+
+
+@pytest.mark.parametrize("bframe,bfield", [(1, [2000.0, 60.0, 30.0]), (0, [1500.0, 800.0, -400.0])])
+def test_mag_lineop_and_stokes_vs_oracle(fsg, oracle_mod, bframe, bfield):
+    grid, st, co, lines, z = zeeman_case()
+    g, r, G, O, w = run_both(fsg, oracle_mod, grid, st, co, lines, z, bframe, bfield)
+    assert np.array_equal(g["flags"], r["flags"])
+    assert np.array_equal(g["ileft"], r["ileft"]) and np.array_equal(g["iright"], r["iright"])
+    m, om = g["maglineopac"], r["maglineopac"]
+    scale = np.maximum(om[..., :3].max(axis=(0, 2)), 1e-300)[None, :, None]
+    assert np.max(np.abs(m - om) / scale) < 1e-11
+    spz, spc, sfl, sfc = G
+    ospz, ospc = O
+    assert np.max(np.abs(spz[:, 0] / ospz[:, 0] - 1)) < 1e-9
+    assert np.max(np.abs(spc / ospc - 1)) < 1e-9
+    for q in (1, 2, 3):
+        assert np.max(np.abs(spz[:, q] - ospz[:, q]) / ospc) < 1e-9
+    osfl, osfc = oracle_mod.disk_integ(w, ospz[:, 0], ospc)
+    assert np.max(np.abs(sfl / osfl - 1)) < 1e-9
+    assert np.max(np.abs(sfc / osfc - 1)) < 1e-9
+
+
+def test_mag_frame2_per_angle_geometry(fsg, oracle_mod):
+    grid, st, co, lines, z = zeeman_case(n=30, seed=33, nmu=5)
+    bfield = [2500.0] + sum([[20.0 * k, 15.0 * k] for k in range(1, 6)], [])
+    g, r, G, O, w = run_both(fsg, oracle_mod, grid, st, co, lines, z, 2, bfield, nmu=5)
+    spz, spc, _, _ = G
+    ospz, ospc = O
+    for q in range(4):
+        assert np.max(np.abs(spz[:, q] - ospz[:, q]) / ospc) < 1e-9
+
+
+def test_mag_against_reference_pin(fsg):
+    d = H.load_pin("pin_magnetic")
+    grid, st, co, lines, z = H.mag_pin_setup(d)
+    C, x, w = mag_ctx(fsg, grid, st, co, nmu=len(d["xmu"]), vmicro=float(d["vmicro"]))
+    assert np.array_equal(x, d["xmu"])
+    bframe, bfield = int(d["bframe"]), d["bfield"]
+    C.mag_lineop_calc(fsg.LineList.from_arrays(lines, zeeman=z), bframe, bfield, want=False)
+    spz, spc, sfl, sfc = C.mag_radtran(bframe, bfield)
+    i0, i1 = int(d["i0"]), int(d["i1"])
+    ref, ic = d["spz"], d["spc"]
+    assert np.max(np.abs(spz[i0:i1 + 1, 0] / ref[:, 0] - 1)) < 1e-8
+    assert np.max(np.abs(spc[i0:i1 + 1] / ic - 1)) < 1e-8
+    for q in (1, 2, 3):
+        assert np.max(np.abs(spz[i0:i1 + 1, q] - ref[:, q]) / ic) < 1e-8
+    assert np.max(np.abs(sfl[i0:i1 + 1] / d["sfl"] - 1)) < 1e-8
+    assert np.max(np.abs(sfc[i0:i1 + 1] / d["sfc"] - 1)) < 1e-8
+
+
+def test_mag_rejects_bad_field(fsg):
+    grid, st, co, lines, z = zeeman_case(n=5)
+    C, x, w = mag_ctx(fsg, grid, st, co)
+    with pytest.raises(fsg.FsgError):
+        C.mag_lineop_calc(fsg.LineList.from_arrays(lines, zeeman=z), 2, [1000.0, 1.0, 2.0])
+    with pytest.raises(fsg.FsgError):
+        C.mag_lineop_calc(fsg.LineList.from_arrays(lines), 1, [1000.0, 1.0, 2.0])

@@ -79,3 +79,25 @@ def test_zeeman_pattern_normal_triplet(oracle_mod):
     spi, rpi, ssi, rsi = oracle_mod.zeeman_pattern(1.0, 0.0, 1.5, 1.5)
     assert len(spi) == 1 and spi[0] == 0 and rpi[0] == 1
     assert len(ssi) == 1 and abs(abs(ssi[0]) - 1.5) < 1e-6
+
+
+def test_oracle_magnetic_pins_reference(oracle_mod):
+    """MagLineopCalc + MagRadTranCalc (Stokes IQUV, BFRAME 1) against the reference's spectra."""
+    d = H.load_pin("pin_magnetic")
+    grid, st, co, lines, z = H.mag_pin_setup(d)
+    S = oracle_mod.State(grid, st, contopac=co, vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]))
+    i0, i1 = int(d["i0"]), int(d["i1"])
+    L = oracle_mod.Lines(**lines, kind=2, zeeman=z)
+    r = oracle_mod.mag_lineop_calc(S, L, int(d["bframe"]), d["bfield"])
+    lo = np.zeros((S.nwl, S.ntau))
+    spz, spc = oracle_mod.mag_radtran(S, d["xmu"], int(d["bframe"]), d["bfield"], lo, r["maglineopac"])
+    ref = d["spz"]
+    ic = d["spc"]
+    # I and Ic relative; Q, U, V relative to the continuum intensity
+    assert np.max(np.abs(spz[i0:i1 + 1, 0] / ref[:, 0] - 1)) < 1e-8
+    assert np.max(np.abs(spc[i0:i1 + 1] / ic - 1)) < 1e-8
+    for q in (1, 2, 3):
+        assert np.max(np.abs(spz[i0:i1 + 1, q] - ref[:, q]) / ic) < 1e-8
+    x, w, _ = oracle_mod.mu_quadrature(1, len(d["xmu"]))
+    sfl, sfc = oracle_mod.disk_integ(w, spz[i0:i1 + 1, 0], spc[i0:i1 + 1])
+    assert np.max(np.abs(sfl / d["sfl"] - 1)) < 1e-8
