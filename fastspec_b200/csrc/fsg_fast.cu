@@ -35,7 +35,7 @@ int fsg_fast_set_constants(const double *anode_h, const double *aida_h) {
 }
 
 // HVoigt * LinCop in FP32 for the table / continued-fraction region (voigt.f90:81-108)
-__device__ __forceinline__ float hv_core32(const float *__restrict__ vtab, float v, float a, float cop) {
+__device__ __noinline__ float hv_core32(const float *__restrict__ vtab, float v, float a, float cop) {
     float av = fabsf(v);
     if (a < 8.0f && av < 8.0f) {
         float fv = av * 125.0f;
@@ -61,29 +61,6 @@ __device__ __forceinline__ float hv_core32(const float *__restrict__ vtab, float
 
 // Kahan-compensated accumulation of one value
 #define KAHAN(S, CC, V) do { float _y = (V) - (CC); float _t = (S) + _y; (CC) = (_t - (S)) - _y; (S) = _t; } while (0)
-
-// One (line, depth) x FAST_P-pixel step.  y = v^2 + a^2 + 1/2 from the pixel's dl^2; the wing
-// branch covers s = y - 1/2 >= 196, the rest goes to the reference's table / continued fraction.
-template <int P, bool MASK>
-__device__ __forceinline__ void line_depth_step(const WingRec &w, const CoreRec *__restrict__ cr,
-                                                const float (&dl2)[P], const bool (&in)[P],
-                                                const float *__restrict__ vtab, float (&s)[P], float (&c)[P]) {
-#pragma unroll
-    for (int k = 0; k < P; k++) {
-        float y = fmaf(dl2[k], w.vv2, w.c2);
-        float val;
-        if (y >= 196.5f) {
-            float t = y - 1.0f;
-            float den = fmaf(t, t, w.twoA);
-            val = (w.c1 * y) * __frcp_rn(den);
-        } else {
-            const CoreRec cc = *cr;
-            val = hv_core32(vtab, sqrtf(dl2[k]) * cc.vv, cc.a, cc.cop);
-        }
-        if (MASK) val = in[k] ? val : 0.0f;
-        KAHAN(s[k], c[k], val);
-    }
-}
 
 template <int D, int P>
 __global__ void __launch_bounds__(32 * 18)
@@ -117,7 +94,6 @@ k_accum_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *
     for (int j = lo; j <= hi; j++) {
         const LineHdr h = hdr[j];
         if (h.iright < tile_first || h.ileft > tile_last) continue;  // window misses the tile
-        const bool full = (h.ileft <= tile_first) && (h.iright >= tile_last);
         float dl2[P];
         bool in[P];
 #pragma unroll
@@ -128,16 +104,43 @@ k_accum_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *
             dl2[k] = dl * dl;
         }
         const WingRec *wr = wing + (size_t)j * ntau + t0;
-        const CoreRec *cr = core + (size_t)j * ntau + t0;
-        if (full) {
+        WingRec w[D];
+#pragma unroll
+        for (int d = 0; d < D; d++) w[d] = wr[min(d, nd - 1)];
+        // wing form for every point, branch-free: one basic block, P x D independent chains
+        float val[D][P];
+        bool core_any = false;
+#pragma unroll
+        for (int d = 0; d < D; d++)
+#pragma unroll
+            for (int k = 0; k < P; k++) {
+                float y = fmaf(dl2[k], w[d].vv2, w[d].c2);
+                float t = y - 1.0f;
+                float den = fmaf(t, t, w[d].twoA);
+                val[d][k] = __fdividef(w[d].c1 * y, den);
+                core_any |= (y < 196.5f);
+            }
+        // rare: points with s < 196 take the reference's table / continued fraction
+        if (core_any) {
+            const CoreRec *cr = core + (size_t)j * ntau + t0;
 #pragma unroll
             for (int d = 0; d < D; d++)
-                if (d < nd) line_depth_step<P, false>(wr[d], cr + d, dl2, in, vtab, s[d], c[d]);
-        } else {
 #pragma unroll
-            for (int d = 0; d < D; d++)
-                if (d < nd) line_depth_step<P, true>(wr[d], cr + d, dl2, in, vtab, s[d], c[d]);
+                for (int k = 0; k < P; k++) {
+                    float y = fmaf(dl2[k], w[d].vv2, w[d].c2);
+                    if (d < nd && y < 196.5f) {
+                        const CoreRec cc = cr[d];
+                        val[d][k] = hv_core32(vtab, sqrtf(dl2[k]) * cc.vv, cc.a, cc.cop);
+                    }
+                }
         }
+#pragma unroll
+        for (int d = 0; d < D; d++)
+#pragma unroll
+            for (int k = 0; k < P; k++) {
+                float v = in[k] ? val[d][k] : 0.0f;
+                KAHAN(s[d][k], c[d][k], v);
+            }
     }
 #pragma unroll
     for (int k = 0; k < P; k++) {
@@ -149,8 +152,8 @@ k_accum_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *
     }
 }
 
-// Tile width per window-width class: narrow windows get narrow tiles so fewer lanes idle.
-int fsg_class_pix(int cls) { return cls == 0 ? 1 : (cls == 1 ? 2 : 4); }
+// Tile width per window-width class: narrow windows get narrower tiles so fewer lanes idle.
+int fsg_class_pix(int cls) { return cls <= 1 ? 2 : 4; }
 
 int fsg_launch_accum_fast(cudaStream_t st, int cls, int ntau, int nwl, const double *wave, const LineHdr *hdr,
                           const WingRec *wing, const CoreRec *core, const int *tile_lo, const int *tile_hi,
