@@ -58,7 +58,7 @@ EXPORTS = [
     "fsg_lineop_calc", "fsg_lineop_calc_dev", "fsg_lineop_reset", "fsg_lineop_get", "fsg_lineop_set",
     "fsg_lineop_device_ptr", "fsg_set_mu", "fsg_radtran", "fsg_radtran_dev", "fsg_mag_lineop_calc",
     "fsg_mag_lineop_reset", "fsg_mag_radtran", "fsg_hvoigt", "fsg_fvoigt", "fsg_voigt_tables",
-    "fsg_locprf_pp", "fsg_mu_quadrature", "fsg_zeeman_pattern",
+    "fsg_locprf_pp", "fsg_locprf_pp_noalloc", "fsg_mu_quadrature", "fsg_zeeman_pattern",
 ]
 
 _lib = None
@@ -112,6 +112,8 @@ def lib():
     L.fsg_fvoigt.argtypes = [C.c_void_p, C.c_int64, _dp, _dp, _dp, _dp]
     L.fsg_voigt_tables.argtypes = [C.c_void_p, _fp, _fp]
     L.fsg_locprf_pp.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp, C.c_int, _dp, _dp, _dp, _dp]
+    L.fsg_locprf_pp_noalloc.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p]
     L.fsg_mu_quadrature.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, C.c_int]
     L.fsg_zeeman_pattern.argtypes = [C.c_float, C.c_float, C.c_float, C.c_float, _ip, _fp, _fp, _ip, _fp, _fp]
     _lib = L

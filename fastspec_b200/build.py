@@ -19,6 +19,7 @@ UNITS = [
     ("fsg_mag.cu", ["-fmad=false"]),
     ("fsg_fast.cu", ["-fmad=true"]),
     ("fsg_api.cu", ["-fmad=false"]),
+    ("fsg_noalloc.cu", ["-fmad=false"]),
 ]
 
 

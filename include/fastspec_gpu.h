@@ -159,6 +159,19 @@ int fsg_voigt_tables(fsg_ctx *ctx, float *vgt, float *fvt);
  * ploc [nprof][nmu]. */
 int fsg_locprf_pp(fsg_ctx *ctx, int nprof, int nmu, const double *xmu, int ntau,
                   const double *xki, const double *src, const double *rhox, double *ploc);
+/* LocPrfPP for callers that cannot allocate device memory (no counterpart in the reference,
+ * which allocates nothing on a device).  Hosts whose device memory belongs to their own pool
+ * allocator (a framework's caching allocator, a Fortran driver that reserves its arrays at
+ * start-up) cannot let a library call cudaMalloc/cudaFree per call: those calls synchronise the
+ * device and fail when the pool holds the memory.  Every pointer is DEVICE memory owned by the
+ * caller (xmu [nmu], xki/src [nprof][ntau], rhox [ntau], ploc [nprof][nmu]); the kernel's work
+ * arrays sit in a fixed 8 MiB device array of the library, so nprof * ntau * 3 may not exceed
+ * 1,048,576 (larger sizes return FSG_E_ARG).  stream is a cudaStream_t (NULL: the default
+ * stream); the call returns after the kernel has finished.  The first call on a device looks up
+ * the array's device address with that device current; make that first call before any stream
+ * capture.  All calls share the array, so calls that overlap on the GPU race. */
+int fsg_locprf_pp_noalloc(int nprof, int nmu, const double *d_xmu, int ntau, const double *d_xki,
+                          const double *d_src, const double *d_rhox, double *d_ploc, void *stream);
 /* MuQuadrature (utils.f90:1273-1330): x (in/out when setnodes == 0), w, r [n+1]. */
 int fsg_mu_quadrature(int quad, int n, double *x, double *w, double *r, int setnodes);
 /* ZeemanPattern (utils.f90:901-1004): outputs hold up to 2*jup+1 entries each. */
