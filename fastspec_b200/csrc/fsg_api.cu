@@ -34,7 +34,9 @@ void fsg_launch_locprf(cudaStream_t, int, int, const double *, int, const double
                        double *, double *);
 int fsg_fast_set_constants(const double *, const double *);
 int fsg_launch_accum_fast(cudaStream_t, int, int, int, const double *, const LineHdr *, const WingRec *,
-                          const CoreRec *, const int *, const int *, const float *, double *);
+                          const int *, const int *, double *, int *);
+void fsg_launch_core_fast(cudaStream_t, int, int, const double *, const LineHdr *, const WingRec *, const CoreRec *,
+                          const int *, const int *, const float *, double *);
 int fsg_fast_tiles(int);
 void fsg_launch_tile_span(cudaStream_t, int, int, int64_t, const LineHdr *, int *, int *);
 int fsg_select(cudaStream_t, int64_t, const int32_t *, const int32_t *, const int32_t *, int, int *, int64_t *,
@@ -113,7 +115,7 @@ struct fsg_ctx {
     DBuf l_wl, l_elo, l_gf, l_grad, l_gqst, l_gvdw, l_spc, l_ismol, l_ihe;
     DBuf d_flags, d_ileft, d_iright, d_idx, d_counts, d_offs, d_total, d_hist, d_nkeep;
     // block buffers
-    DBuf d_wing, d_core, d_hdr, d_tlo, d_thi, d_p64, d_lstart, d_lstop, d_widx, d_pw, d_evals;
+    DBuf d_wing, d_core, d_hdr, d_tlo, d_thi, d_p64, d_lstart, d_lstop, d_widx, d_pw, d_evals, d_err;
     // spectra
     DBuf d_spl, d_spc, d_sfl, d_sfc, d_work, d_a, d_v, d_h, d_l;
     // magnetic
@@ -198,7 +200,7 @@ void fsg_destroy(fsg_ctx *ctx) {
                      &ctx->l_grad, &ctx->l_gqst, &ctx->l_gvdw, &ctx->l_spc, &ctx->l_ismol, &ctx->l_ihe,
                      &ctx->d_flags, &ctx->d_ileft, &ctx->d_iright, &ctx->d_idx, &ctx->d_counts, &ctx->d_offs,
                      &ctx->d_total, &ctx->d_hist, &ctx->d_nkeep, &ctx->d_wing, &ctx->d_core, &ctx->d_hdr,
-                     &ctx->d_tlo, &ctx->d_thi, &ctx->d_p64, &ctx->d_lstart, &ctx->d_lstop, &ctx->d_widx,
+                     &ctx->d_tlo, &ctx->d_thi, &ctx->d_err, &ctx->d_p64, &ctx->d_lstart, &ctx->d_lstop, &ctx->d_widx,
                      &ctx->d_pw, &ctx->d_evals, &ctx->d_spl, &ctx->d_spc, &ctx->d_sfl, &ctx->d_sfc,
                      &ctx->d_work, &ctx->d_a, &ctx->d_v, &ctx->d_h, &ctx->d_l, &ctx->z_npi, &ctx->z_nsi,
                      &ctx->z_pioff, &ctx->z_sioff, &ctx->z_splpi, &ctx->z_strpi, &ctx->z_splsi, &ctx->z_strsi,
@@ -487,6 +489,8 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st) {
     ALLOC(ctx->d_idx, sizeof(int64_t) * std::max<int64_t>(n, 1));
     int ntiles = fsg_fast_tiles(ctx->nwl);
     ALLOC(ctx->d_tlo, sizeof(int) * ntiles); ALLOC(ctx->d_thi, sizeof(int) * ntiles);
+    ALLOC(ctx->d_err, sizeof(int));
+    CK(cudaMemsetAsync(ctx->d_err.p, 0, sizeof(int), s), "err reset");
     size_t per_line = (size_t)nt * (sizeof(WingRec) + sizeof(CoreRec)) + sizeof(LineHdr);
     int64_t cap = block_capacity(ctx, per_line);
     int64_t nblocks = 0;
@@ -511,17 +515,25 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st) {
             cudaEvent_t ea = kevent(), eb = kevent();
             cudaEventRecord(ea, s);
             int rc2 = fsg_launch_accum_fast(s, c, nt, ctx->nwl, ctx->d_wave.as<double>(), ctx->d_hdr.as<LineHdr>(),
-                                            ctx->d_wing.as<WingRec>(), ctx->d_core.as<CoreRec>(), ctx->d_tlo.as<int>(),
-                                            ctx->d_thi.as<int>(), ctx->tab.vtab, ctx->d_lineopac.as<double>());
+                                            ctx->d_wing.as<WingRec>(), ctx->d_tlo.as<int>(), ctx->d_thi.as<int>(),
+                                            ctx->d_lineopac.as<double>(), ctx->d_err.as<int>());
             if (rc2) return cuda_fail(ctx, cudaGetLastError(), "k_accum_fast");
+            // core ranges of the same lines, 32-wavelength tiles
+            fsg_launch_tile_span(s, -1, ctx->nwl, nb, ctx->d_hdr.as<LineHdr>(), ctx->d_tlo.as<int>(), ctx->d_thi.as<int>());
+            fsg_launch_core_fast(s, nt, ctx->nwl, ctx->d_wave.as<double>(), ctx->d_hdr.as<LineHdr>(),
+                                 ctx->d_wing.as<WingRec>(), ctx->d_core.as<CoreRec>(), ctx->d_tlo.as<int>(),
+                                 ctx->d_thi.as<int>(), ctx->tab.vtab, ctx->d_lineopac.as<double>());
             cudaEventRecord(eb, s);
             kt.push_back({ ea, eb });
-            ctx->launches += 4;
+            ctx->launches += 7;
             nblocks++;
         }
     }
     CK(cudaGetLastError(), "fast accumulation");
     CK(cudaStreamSynchronize(s), "fast accumulation");
+    int kerr = 0;
+    CK(cudaMemcpy(&kerr, ctx->d_err.p, sizeof(int), cudaMemcpyDeviceToHost), "err read");
+    if (kerr) return fail(ctx, FSG_E_TIMEOUT, "k_accum_fast: a line-record copy did not complete within its bound");
     double ms = 0.0;
     for (auto &p : kt) { float x = 0; cudaEventElapsedTime(&x, p.first, p.second); ms += x; }
     if (st) { st->nblocks = nblocks; st->accum_launches = (int64_t)kt.size(); st->ms_accum_kernels = ms; }

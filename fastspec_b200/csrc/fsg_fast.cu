@@ -4,9 +4,10 @@
 //   LineOpac(t, p) = sum over retained lines l with Ileft(l) <= p <= Iright(l) of
 //                    HVoigt(a(l,t), (lambda_p - lambda_l) / dlD(l,t)) * LinCop(l,t).
 // Here a CTA owns a tile of TW = 32 P wavelengths x all depths.  Warp w owns depths
-// [w*D, w*D + D); lane l owns the wavelengths tile0 + l + 32k (k < P).  Each thread keeps its
-// P x D sums in registers with Kahan compensation: no shared-memory or global atomics, one
-// read-modify-write of the FP64 LineOpac per tile and launch, deterministic order.
+// [w*D, w*D + D); lane l owns the wavelengths tile0 + l + 32k (k < P).  Each thread owns its
+// P x D sums: FP32 partials in registers over FOLD lines, Kahan-compensated (sum, compensation)
+// pairs in shared memory beyond that.  No atomics, one read-modify-write of the FP64 LineOpac
+// per tile and launch, deterministic order.
 //
 // Lines are binned by window width (class c holds windows of up to 256 * 2^c wavelengths) and
 // processed class by class, so the candidate line range of a tile [lo, hi] -- the lines of the
@@ -35,7 +36,7 @@ int fsg_fast_set_constants(const double *anode_h, const double *aida_h) {
 }
 
 // HVoigt * LinCop in FP32 for the table / continued-fraction region (voigt.f90:81-108)
-__device__ __noinline__ float hv_core32(const float *__restrict__ vtab, float v, float a, float cop) {
+__device__ __forceinline__ float hv_core32(const float *__restrict__ vtab, float v, float a, float cop) {
     float av = fabsf(v);
     if (a < 8.0f && av < 8.0f) {
         float fv = av * 125.0f;
@@ -62,93 +63,221 @@ __device__ __noinline__ float hv_core32(const float *__restrict__ vtab, float v,
 // Kahan-compensated accumulation of one value
 #define KAHAN(S, CC, V) do { float _y = (V) - (CC); float _t = (S) + _y; (CC) = (_t - (S)) - _y; (S) = _t; } while (0)
 
+// Lines folded into the compensated sums at a time: each thread adds up to FOLD lines into FP32
+// register partials, then Kahan-adds every partial into its (sum, compensation) pair in shared
+// memory.  The partials carry at most FOLD terms, so their rounding stays at the FP32 unit
+// roundoff of a few terms; the Kahan pairs carry the long sums.
+#define FOLD 16
+// Candidate lines staged per TMA bulk copy (double-buffered)
+#define CH 16
+// Bound on an mbarrier wait: one second of %globaltimer (a chunk's copy completes in microseconds),
+// and at most WAIT_POLLS polls whatever the timer reads
+#define WAIT_NS 1000000000ull
+#define WAIT_POLLS (1u << 26)
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void tma_bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+// bounded wait for the phase with the given parity; false when the bound was reached
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+    const unsigned a = smem_u32(bar);
+    uint64_t start = 0;
+    for (unsigned it = 0; it < WAIT_POLLS; it++) {
+        unsigned done;
+        asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+                     : "=r"(done) : "r"(a), "r"(parity) : "memory");
+        if (done) return true;
+        if ((it & 255u) == 0) {
+            uint64_t now = global_ns();
+            if (it == 0) start = now;
+            else if (now - start > WAIT_NS) return false;
+        }
+    }
+    return false;
+}
+
+// cp.async.bulk moves multiples of 16 bytes between 16-byte aligned addresses
+static_assert(sizeof(WingRec) % 16 == 0 && sizeof(LineHdr) % 16 == 0, "bulk-copied records: multiples of 16 bytes");
+
+// Issue the bulk copies of chunk c (lines lo + c*CH ...) into buffer b; one thread calls this.
+__device__ __forceinline__ void stage_chunk(int c, int lo, int hi, int ntau, const LineHdr *hdr, const WingRec *wing,
+                                            LineHdr *shdr, WingRec *swing, uint64_t *bar) {
+    int j0 = lo + c * CH;
+    int n = min(CH, hi - j0 + 1);
+    unsigned brec = (unsigned)(n * ntau * (int)sizeof(WingRec)), bhdr = (unsigned)(n * (int)sizeof(LineHdr));
+    mbar_expect_tx(bar, brec + bhdr);
+    tma_bulk_g2s(swing, wing + (size_t)j0 * ntau, brec, bar);
+    tma_bulk_g2s(shdr, hdr + j0, bhdr, bar);
+}
+
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// Wing pass.  Every window point outside the line's core range [cl, cr] has s >= 196 at every
+// depth, so there HVoigt * LinCop is the rational wing form alone:
+//   val = c1 (t + 1) / (t^2 + twoA),  t = dl^2 vv2 + c2m1
+// (three FMAs, one reciprocal, one FMA into the partial sum).  Lines whose window covers the
+// whole tile outside their core range (the common case for wide windows) skip the mask.
 template <int D, int P>
-__global__ void __launch_bounds__(32 * 18)
+__global__ void __launch_bounds__(32 * 18, 1)
 k_accum_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *__restrict__ hdr,
-             const WingRec *__restrict__ wing, const CoreRec *__restrict__ core,
-             const int *__restrict__ tile_lo, const int *__restrict__ tile_hi,
-             const float *__restrict__ vtab, double *__restrict__ lineopac) {
+             const WingRec *__restrict__ wing, const int *__restrict__ tile_lo, const int *__restrict__ tile_hi,
+             double *__restrict__ lineopac, int *__restrict__ err) {
+    // shared memory: wing records [2][CH][ntau] | headers [2][CH] | mbarriers [2] | Kahan pairs
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    WingRec *swing = (WingRec *)smem_raw;
+    LineHdr *shdr = (LineHdr *)(swing + 2 * CH * ntau);
+    uint64_t *bars = (uint64_t *)(shdr + 2 * CH);
+    float2 *ksum = (float2 *)(bars + 2);                 // [D * P][blockDim.x]
     constexpr int TW = 32 * P;
     const int tile = blockIdx.x;
     const int lo = tile_lo[tile], hi = tile_hi[tile];
     if (lo > hi) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int t0 = warp * D;
-    if (t0 >= ntau) return;
-    const int nd = min(D, ntau - t0);
-    const int p0 = tile * TW;                 // 0-based wavelength index of the tile start
-    double wv[P];
+    const int nd = max(0, min(D, ntau - t0));            // warps past the last depth only help staging
+    const int p0 = tile * TW;
+    const int nth = blockDim.x;
+    const int nchunks = (hi - lo + CH) / CH;
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        stage_chunk(0, lo, hi, ntau, hdr, wing, shdr, swing, &bars[0]);
+        if (nchunks > 1) stage_chunk(1, lo, hi, ntau, hdr, wing, shdr + CH, swing + CH * ntau, &bars[1]);
+    }
+    // wavelength offsets as FP32 hi + lo: dl = (wvh - wlh) + (wvl - wll) keeps dl to FP32 relative
+    // accuracy next to the line centre
+    float wvh[P], wvl[P];
     int pix[P];
 #pragma unroll
     for (int k = 0; k < P; k++) {
-        pix[k] = p0 + lane + 32 * k;          // 0-based
-        wv[k] = wave[min(pix[k], nwl - 1)];
+        pix[k] = p0 + lane + 32 * k;
+        double w = wave[min(pix[k], nwl - 1)];
+        wvh[k] = (float)w;
+        wvl[k] = (float)(w - (double)wvh[k]);
     }
-    float s[D][P], c[D][P];
+    float part[D][P];
 #pragma unroll
     for (int d = 0; d < D; d++)
 #pragma unroll
-        for (int k = 0; k < P; k++) { s[d][k] = 0.0f; c[d][k] = 0.0f; }
-
-    const int tile_first = p0 + 1, tile_last = min(p0 + TW, nwl);   // 1-based bounds
-    for (int j = lo; j <= hi; j++) {
-        const LineHdr h = hdr[j];
-        if (h.iright < tile_first || h.ileft > tile_last) continue;  // window misses the tile
-        float dl2[P];
-        bool in[P];
-#pragma unroll
         for (int k = 0; k < P; k++) {
-            int p1 = pix[k] + 1;
-            in[k] = (p1 >= h.ileft) && (p1 <= h.iright);
-            float dl = (float)(wv[k] - h.wlc);
-            dl2[k] = dl * dl;
+            part[d][k] = 0.0f;
+            ksum[(d * P + k) * nth + threadIdx.x] = make_float2(0.0f, 0.0f);
         }
-        const WingRec *wr = wing + (size_t)j * ntau + t0;
-        WingRec w[D];
-#pragma unroll
-        for (int d = 0; d < D; d++) w[d] = wr[min(d, nd - 1)];
-        // wing form for every point, branch-free: one basic block, P x D independent chains
-        float val[D][P];
-        bool core_any = false;
-#pragma unroll
-        for (int d = 0; d < D; d++)
-#pragma unroll
-            for (int k = 0; k < P; k++) {
-                float y = fmaf(dl2[k], w[d].vv2, w[d].c2);
-                float t = y - 1.0f;
-                float den = fmaf(t, t, w[d].twoA);
-                val[d][k] = __fdividef(w[d].c1 * y, den);
-                core_any |= (y < 196.5f);
-            }
-        // rare: points with s < 196 take the reference's table / continued fraction
-        if (core_any) {
-            const CoreRec *cr = core + (size_t)j * ntau + t0;
-#pragma unroll
-            for (int d = 0; d < D; d++)
+    int nfold = 0;
+    const int tile_first = p0 + 1, tile_last = min(p0 + TW, nwl);
+    int failed = -1;                                     // chunk whose copy did not complete
+    for (int c = 0; c < nchunks; c++) {
+        const int b = c & 1;
+        const bool ok = mbar_wait(&bars[b], (unsigned)((c >> 1) & 1));
+        if (__syncthreads_or(!ok)) { failed = c; break; }
+        const LineHdr *ch = shdr + b * CH;
+        const WingRec *cw = swing + b * CH * ntau;
+        const int n = min(CH, hi - (lo + c * CH) + 1);
+        if (nd > 0) {
+            for (int q = 0; q < n; q++) {
+                const LineHdr h = ch[q];
+                if (h.iright < tile_first || h.ileft > tile_last) continue;   // window misses the tile
+                float x[P];
 #pragma unroll
                 for (int k = 0; k < P; k++) {
-                    float y = fmaf(dl2[k], w[d].vv2, w[d].c2);
-                    if (d < nd && y < 196.5f) {
-                        const CoreRec cc = cr[d];
-                        val[d][k] = hv_core32(vtab, sqrtf(dl2[k]) * cc.vv, cc.a, cc.cop);
-                    }
+                    float dl = (wvh[k] - h.wlh) + (wvl[k] - h.wll);
+                    x[k] = dl * dl;
                 }
-        }
+                WingRec w[D];
 #pragma unroll
-        for (int d = 0; d < D; d++)
+                for (int d = 0; d < D; d++) w[d] = cw[q * ntau + t0 + min(d, nd - 1)];
+                const bool full = h.ileft <= tile_first && h.iright >= tile_last &&
+                                  (h.cr < tile_first || h.cl > tile_last);
+                if (full) {
 #pragma unroll
-            for (int k = 0; k < P; k++) {
-                float v = in[k] ? val[d][k] : 0.0f;
-                KAHAN(s[d][k], c[d][k], v);
+                    for (int d = 0; d < D; d++)
+#pragma unroll
+                        for (int k = 0; k < P; k++) {
+                            float t = fmaf(x[k], w[d].vv2, w[d].c2m1);
+                            float den = fmaf(t, t, w[d].twoA);
+                            float num = fmaf(w[d].c1, t, w[d].c1);
+                            part[d][k] = fmaf(num, rcp_approx(den), part[d][k]);
+                        }
+                } else {
+                    bool in[P];
+#pragma unroll
+                    for (int k = 0; k < P; k++) {
+                        int p1 = pix[k] + 1;
+                        in[k] = p1 >= h.ileft && p1 <= h.iright && (p1 < h.cl || p1 > h.cr);
+                    }
+#pragma unroll
+                    for (int d = 0; d < D; d++)
+#pragma unroll
+                        for (int k = 0; k < P; k++) {
+                            float t = fmaf(x[k], w[d].vv2, w[d].c2m1);
+                            float den = fmaf(t, t, w[d].twoA);
+                            float num = fmaf(w[d].c1, t, w[d].c1);
+                            float r = rcp_approx(den);
+                            part[d][k] = fmaf(num, in[k] ? r : 0.0f, part[d][k]);
+                        }
+                }
+                if (++nfold == FOLD) {
+                    nfold = 0;
+#pragma unroll
+                    for (int d = 0; d < D; d++)
+#pragma unroll
+                        for (int k = 0; k < P; k++) {
+                            float2 &qq = ksum[(d * P + k) * nth + threadIdx.x];
+                            float2 sc = qq;
+                            KAHAN(sc.x, sc.y, part[d][k]);
+                            qq = sc;
+                            part[d][k] = 0.0f;
+                        }
+                }
             }
+        }
+        __syncthreads();                                   // every warp is done with buffer b
+        if (threadIdx.x == 0 && c + 2 < nchunks)
+            stage_chunk(c + 2, lo, hi, ntau, hdr, wing, shdr + b * CH, swing + b * CH * ntau, &bars[b]);
     }
+    if (failed >= 0) {
+        // a copy never completed: report, then wait (bounded) for the copies still in flight,
+        // chunks failed and failed + 1, before the CTA's shared memory is released
+        if (threadIdx.x == 0) {
+            atomicExch(err, FSG_E_TIMEOUT);
+            for (int c = failed; c < nchunks && c < failed + 2; c++) mbar_wait(&bars[c & 1], (unsigned)((c >> 1) & 1));
+        }
+        __syncthreads();
+        return;
+    }
+    if (nd <= 0) return;
 #pragma unroll
     for (int k = 0; k < P; k++) {
         if (pix[k] >= nwl) continue;
         double *dst = lineopac + (size_t)pix[k] * ntau + t0;
 #pragma unroll
-        for (int d = 0; d < D; d++)
-            if (d < nd) dst[d] = dst[d] + ((double)s[d][k] - (double)c[d][k]);
+        for (int d = 0; d < D; d++) {
+            float2 sc = ksum[(d * P + k) * nth + threadIdx.x];
+            KAHAN(sc.x, sc.y, part[d][k]);
+            if (d < nd) dst[d] = dst[d] + ((double)sc.x - (double)sc.y);
+        }
     }
 }
 
@@ -156,8 +285,7 @@ k_accum_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *
 int fsg_class_pix(int cls) { return cls <= 1 ? 2 : 4; }
 
 int fsg_launch_accum_fast(cudaStream_t st, int cls, int ntau, int nwl, const double *wave, const LineHdr *hdr,
-                          const WingRec *wing, const CoreRec *core, const int *tile_lo, const int *tile_hi,
-                          const float *vtab, double *lineopac) {
+                          const WingRec *wing, const int *tile_lo, const int *tile_hi, double *lineopac, int *err) {
     const int P = fsg_class_pix(cls);
     const int TW = 32 * P;
     const int ntiles = (nwl + TW - 1) / TW;
@@ -165,11 +293,14 @@ int fsg_launch_accum_fast(cudaStream_t st, int cls, int ntau, int nwl, const dou
     int D = 16 / P;
     if ((ntau + D - 1) / D > 18) D = (ntau + 17) / 18;
     int nwarps = (ntau + D - 1) / D;
-#define LAUNCH(DD, PP) k_accum_fast<DD, PP><<<ntiles, 32 * nwarps, 0, st>>>(ntau, nwl, wave, hdr, wing, core, \
-                                                                             tile_lo, tile_hi, vtab, lineopac)
-    if (P == 1) {
-        if (D == 16) LAUNCH(16, 1); else return FSG_E_ARG;
-    } else if (P == 2) {
+    const size_t smem = sizeof(WingRec) * 2 * CH * (size_t)ntau + sizeof(LineHdr) * 2 * CH + 2 * sizeof(uint64_t) +
+                        sizeof(float2) * (size_t)D * P * 32 * nwarps;
+    if (smem > 200 * 1024) return FSG_E_ARG;
+#define LAUNCH(DD, PP) do { \
+        cudaFuncSetAttribute(k_accum_fast<DD, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+        k_accum_fast<DD, PP><<<ntiles, 32 * nwarps, smem, st>>>(ntau, nwl, wave, hdr, wing, tile_lo, tile_hi, \
+                                                                 lineopac, err); } while (0)
+    if (P == 2) {
         if (D == 8) LAUNCH(8, 2); else return FSG_E_ARG;
     } else {
         switch (D) {
@@ -185,17 +316,82 @@ int fsg_launch_accum_fast(cudaStream_t st, int cls, int ntau, int nwl, const dou
     return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
 }
 
+// Core pass.  Over each line's core range [cl, cr] the full HVoigt branch structure runs point by
+// point: the table lerp or the continued fraction where fl32(t) < 195.5 (s < 196), the wing form
+// elsewhere.  A CTA owns 32 wavelengths x all depths, warp w depths [w*CORE_D, w*CORE_D + CORE_D);
+// Kahan sums in registers.
+#define CORE_D 8
+__global__ void __launch_bounds__(32 * 16)
+k_core_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *__restrict__ hdr,
+            const WingRec *__restrict__ wing, const CoreRec *__restrict__ core, const int *__restrict__ tile_lo,
+            const int *__restrict__ tile_hi, const float *__restrict__ vtab, double *__restrict__ lineopac) {
+    const int tile = blockIdx.x;
+    const int lo = tile_lo[tile], hi = tile_hi[tile];
+    if (lo > hi) return;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t0 = warp * CORE_D;
+    const int nd = min(CORE_D, ntau - t0);
+    if (nd <= 0) return;
+    const int p = tile * 32 + lane;
+    const int tile_first = tile * 32 + 1, tile_last = min(tile * 32 + 32, nwl);
+    const double wd = wave[min(p, nwl - 1)];
+    const float wvh = (float)wd, wvl = (float)(wd - (double)wvh);
+    float sum[CORE_D], cmp[CORE_D];
+#pragma unroll
+    for (int d = 0; d < CORE_D; d++) { sum[d] = 0.0f; cmp[d] = 0.0f; }
+    for (int j = lo; j <= hi; j++) {
+        const LineHdr h = hdr[j];
+        if (h.cr < tile_first || h.cl > tile_last) continue;          // core range misses the tile
+        const int p1 = p + 1;
+        if (p1 < h.cl || p1 > h.cr) continue;
+        const float dl = (wvh - h.wlh) + (wvl - h.wll);
+        const float x = dl * dl;
+        const WingRec *wr = wing + (size_t)j * ntau + t0;
+        const CoreRec *cr = core + (size_t)j * ntau + t0;
+#pragma unroll
+        for (int d = 0; d < CORE_D; d++) {
+            if (d >= nd) break;
+            const WingRec w = wr[d];
+            const float t = fmaf(x, w.vv2, w.c2m1);
+            float v;
+            if (t < 195.5f) {
+                const CoreRec c = cr[d];
+                v = hv_core32(vtab, fabsf(dl) * c.vv, c.a, c.cop);
+            } else {
+                v = fmaf(w.c1, t, w.c1) * rcp_approx(fmaf(t, t, w.twoA));
+            }
+            KAHAN(sum[d], cmp[d], v);
+        }
+    }
+    if (p >= nwl) return;
+    double *dst = lineopac + (size_t)p * ntau + t0;
+#pragma unroll
+    for (int d = 0; d < CORE_D; d++)
+        if (d < nd) dst[d] = dst[d] + ((double)sum[d] - (double)cmp[d]);
+}
+
+void fsg_launch_core_fast(cudaStream_t st, int ntau, int nwl, const double *wave, const LineHdr *hdr,
+                          const WingRec *wing, const CoreRec *core, const int *tile_lo, const int *tile_hi,
+                          const float *vtab, double *lineopac) {
+    const int ntiles = (nwl + 31) / 32;
+    const int nwarps = (ntau + CORE_D - 1) / CORE_D;     // ntau <= 128: at most 16 warps
+    k_core_fast<<<ntiles, 32 * nwarps, 0, st>>>(ntau, nwl, wave, hdr, wing, core, tile_lo, tile_hi, vtab, lineopac);
+}
+
 // ---- tile candidate ranges of one block: lo/hi of the block-local line index -------------------
 __global__ void k_tile_reset(int ntiles, int *lo, int *hi) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < ntiles) { lo[i] = 0x7fffffff; hi[i] = -1; }
 }
 
-__global__ void k_tile_span(int64_t nb, int tw, const LineHdr *hdr, int *lo, int *hi) {
+// windows (core = 0) or core ranges (core = 1) of the block's lines against tiles of tw wavelengths
+__global__ void k_tile_span(int64_t nb, int tw, int use_core, const LineHdr *hdr, int *lo, int *hi) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= nb) return;
     LineHdr h = hdr[j];
-    int a = (h.ileft - 1) / tw, b = (h.iright - 1) / tw;
+    int l = use_core ? h.cl : h.ileft, r = use_core ? h.cr : h.iright;
+    if (l > r) return;
+    int a = (l - 1) / tw, b = (r - 1) / tw;
     for (int t = a; t <= b; t++) { atomicMin(&lo[t], (int)j); atomicMax(&hi[t], (int)j); }
 }
 
@@ -203,10 +399,10 @@ __global__ void k_tile_span(int64_t nb, int tw, const LineHdr *hdr, int *lo, int
 int fsg_fast_tiles(int nwl) { return (nwl + 31) / 32; }
 
 void fsg_launch_tile_span(cudaStream_t s, int cls, int nwl, int64_t nb, const LineHdr *hdr, int *lo, int *hi) {
-    int tw = 32 * fsg_class_pix(cls);
+    int tw = cls < 0 ? 32 : 32 * fsg_class_pix(cls);
     int ntiles = (nwl + tw - 1) / tw;
     k_tile_reset<<<(ntiles + 255) / 256, 256, 0, s>>>(ntiles, lo, hi);
-    if (nb > 0) k_tile_span<<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(nb, tw, hdr, lo, hi);
+    if (nb > 0) k_tile_span<<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(nb, tw, cls < 0 ? 1 : 0, hdr, lo, hi);
 }
 
 // ---- window-width classes and order-preserving compaction -----------------------------------

@@ -71,15 +71,18 @@ struct XCoef {
 // Fast-path record of one (line, depth): FP32 wing coefficients of HVoigt * LinCop.
 // For s = v^2 + a^2 >= 196 the reference evaluates (voigt.f90:100-101)
 //   H = a (s + 1/2) / (sqrt(pi) (s^2 - v^2 + a^2 + 1/4)).
-// With y = s + 1/2 the denominator is exactly (y - 1)^2 + 2 a^2, so
-//   H * LinCop = c1 y / ((y - 1)^2 + twoA),  y = dl^2 vv2 + c2,
-// with vv2 = LinVvgt^2, c2 = a^2 + 1/2, twoA = 2 a^2, c1 = LinCop a / sqrt(pi).
-struct __align__(16) WingRec { float vv2, c2, twoA, c1; };
+// With y = s + 1/2 the denominator is exactly (y - 1)^2 + 2 a^2, so with t = y - 1
+//   H * LinCop = c1 (t + 1) / (t^2 + twoA),  t = dl^2 vv2 + c2m1,
+// with vv2 = LinVvgt^2, c2m1 = a^2 - 1/2, twoA = 2 a^2, c1 = LinCop a / sqrt(pi).
+struct __align__(16) WingRec { float vv2, c2m1, twoA, c1; };
 // Table / continued-fraction region (s < 196): LinVvgt, LinCop, a.
 struct __align__(16) CoreRec { float vv, cop, a, pad; };
 
-// Line header of a retained line inside a block (fast path).
-struct __align__(16) LineHdr { double wlc; int ileft, iright; };   // wlc = Wlcent (offset)
+// Line header of a retained line inside a block (fast path).  The centre offset Wlcent is split
+// into FP32 wlh + wll (wlh = fl32(Wlcent), wll = fl32(Wlcent - wlh)).  [cl, cr] is the core range:
+// every wavelength index of the window where some depth may have s < 196 lies inside it
+// (cl > cr when no depth has a core).
+struct __align__(16) LineHdr { float wlh, wll; int ileft, iright; int cl, cr, pad0, pad1; };
 
 // Zeeman components of a device line list (CSR by line)
 struct ZView {

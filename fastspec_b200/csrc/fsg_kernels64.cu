@@ -224,6 +224,16 @@ void fsg_launch_center(cudaStream_t s, const AtmView &A, const LineView &L, cons
 // ================================================================================================
 // Block refill: per retained line of the block, XlineSetup once then XlineDepth over depths.
 // ================================================================================================
+// first index i in [0, n) with w[i] >= x (n when none)
+__device__ __forceinline__ int lower_index(const double *__restrict__ w, int n, double x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int m = (lo + hi) >> 1;
+        if (w[m] < x) lo = m + 1; else hi = m;
+    }
+    return lo;
+}
+
 __global__ void k_params_fast(AtmView A, LineView L, const int64_t *__restrict__ idx, int64_t j0,
                               int64_t nb, const int32_t *__restrict__ flags,
                               const int32_t *__restrict__ ileft, const int32_t *__restrict__ iright,
@@ -236,8 +246,7 @@ __global__ void k_params_fast(AtmView A, LineView L, const int64_t *__restrict__
     double wlc = L.wl[i] - A.wfirst;
     XCoef XC;
     xline_setup(A, L, i, wlc, f, &XC);
-    LineHdr h; h.wlc = wlc; h.ileft = ileft[i]; h.iright = iright[i];
-    hdr[j] = h;
+    double hcore = -1.0;        // largest |dl| of any depth's core region (s < 196)
     for (int t = 0; t < nt; t++) {
         double cop, vv, av;
         xline_depth(A, t, XC, &cop, &vv, &av);
@@ -245,14 +254,34 @@ __global__ void k_params_fast(AtmView A, LineView L, const int64_t *__restrict__
         double a2 = av * av;
         WingRec w;
         w.vv2 = (float)(vv * vv);
-        w.c2 = (float)(a2 + 0.5);
+        w.c2m1 = (float)(a2 - 0.5);
         w.twoA = (float)(2.0 * a2);
         w.c1 = (float)(cop * av * FSG_SQRTPIINV);
         CoreRec c;
         c.vv = (float)vv; c.cop = (float)cop; c.a = (float)av; c.pad = 0.0f;
         wing[(size_t)j * nt + t] = w;
         core[(size_t)j * nt + t] = c;
+        // the accumulation evaluates the core form where fl32(dl^2 vv2 + c2m1) < 195.5; a margin of
+        // 0.05 in s and 1e-5 in dl covers the FP32 rounding of the records and of dl^2
+        double q = 196.05 - a2;
+        if (q > 0.0) hcore = fmax(hcore, sqrt(q) / vv * (1.0 + 1e-5));
     }
+    LineHdr h;
+    h.wlh = (float)wlc;
+    h.wll = (float)(wlc - (double)h.wlh);
+    h.ileft = ileft[i]; h.iright = iright[i];
+    h.cl = 1; h.cr = 0;
+    if (hcore >= 0.0) {
+        // 1-based indices of the first wavelength >= wlc - hcore and the last <= wlc + hcore,
+        // widened by one wavelength and clipped to the window
+        int a = lower_index(A.wave, A.nwl, wlc - hcore) + 1;
+        int b = lower_index(A.wave, A.nwl, wlc + hcore);
+        if (b < A.nwl && A.wave[b] == wlc + hcore) b++;
+        int cl = max(a - 1, h.ileft), cr = min(b + 1, h.iright);
+        if (cl <= cr) { h.cl = cl; h.cr = cr; }
+    }
+    h.pad0 = 0; h.pad1 = 0;
+    hdr[j] = h;
 }
 
 void fsg_launch_params_fast(cudaStream_t s, const AtmView &A, const LineView &L, const int64_t *idx,
