@@ -34,6 +34,8 @@ sys.path.insert(0, os.path.join(HERE, "tests"))
 
 METRIC = "Voigt line-evals/s (cool-dwarf 1e8-line synthesis)"
 UNIT = "line-evals/s"
+# DRAM bytes per wing evaluation (ncu capture of the wing launches; profiles/k_accum_fast_cooldwarf.md)
+TRAFFIC_PER_WING_EVAL = None
 FLOPS_PER_EVAL = 12          # nominal FP32 work of one wing evaluation (v^2, rational, scale, sum)
 W0, W1, DSTEP, NMU = 5000.0, 25000.0, 1.0, 7
 
@@ -49,6 +51,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--no-plain", action="store_true", help="skip the plain FP64 path comparison")
+    p.add_argument("--plain-lines", type=float, default=1e6)
     return p.parse_args()
 
 
@@ -109,6 +113,67 @@ class ClockSampler:
 
 
 # ---- GPU arm -------------------------------------------------------------------------------------
+def device_lines(F, torch, arr, dev):
+    """Device copies of a line list and the fsg_lines view of them (kind 2, molecular SoA)."""
+    dt = {k: torch.from_numpy(np.ascontiguousarray(v)).to(f"cuda:{dev}") for k, v in arr.items()}
+    dl = F.CLines()
+    dl.n = int(dt["wl"].numel())
+    dl.kind = 2
+    dl.wl = F.C.cast(dt["wl"].data_ptr(), F._dp)
+    for k in ("elo", "gf", "grad", "gqst", "gvdw"):
+        setattr(dl, k, F.C.cast(dt[k].data_ptr(), F._fp))
+    dl.spc = F.C.cast(dt["spc"].data_ptr(), F._ip)
+    dl.ismol = F.C.cast(dt["ismol"].data_ptr(), F._ip)
+    return dt, dl
+
+
+def plain_vs_mixed(F, torch, st, meta, co, dev, nlines):
+    """The same synthesis through the plain FP64 path and the mixed path on a smaller list with the
+    same distributions over the full grid: line-evals/s of each, and the flux difference."""
+    from fastspec_b200 import workloads as W
+    arr = W.molecular_lines(nlines, W0, W1, W.SEED0 + 7, exact=False).arrays()
+    x, w, _ = F.mu_quadrature(1, NMU)
+    out = {}
+    flux = {}
+    for name, prec in (("fp64", F.PREC_FP64), ("mixed", F.PREC_MIXED)):
+        C = F.Context(device=dev, precision=prec, vmicro=meta["vmicro"], molbrd=meta["molbrd"], limitram_gb=24.0)
+        C.set_grid(1, W0, W1, DSTEP)
+        C.set_atmosphere(st)
+        C.set_contopac(co)
+        C.set_mu(x, w)
+        dt, dl = device_lines(F, torch, arr, dev)
+        sfl = torch.empty(C.nwl, dtype=torch.float64, device=f"cuda:{dev}")
+        sfc = torch.empty_like(sfl)
+        stream = torch.cuda.ExternalStream(C.stream_ptr(), device=dev)
+
+        def step():
+            C.lineop_reset()
+            s_ = C.lineop_calc_dev(dl)
+            C.radtran_dev(None, None, sfl.data_ptr(), sfc.data_ptr())
+            return s_
+
+        step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s_ = step()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        ev = s_["line_evals"] if prec == F.PREC_MIXED else None
+        out[name] = {"ms": ms, "ms_accum": s_["ms_accum"], "stats_evals": s_["line_evals"]}
+        flux[name] = sfl.cpu().numpy() / sfc.cpu().numpy()
+        if ev is not None:
+            out["evals"] = ev
+        C.close()
+    ev = out["evals"]
+    return {"sample": "%d lines, same distributions, full grid" % nlines,
+            "fp64_value": ev / (out["fp64"]["ms"] / 1e3), "mixed_value": ev / (out["mixed"]["ms"] / 1e3),
+            "unit": UNIT, "speedup": out["fp64"]["ms"] / out["mixed"]["ms"],
+            "fp64_ms": out["fp64"]["ms"], "mixed_ms": out["mixed"]["ms"],
+            "flux_max_rel_diff": float(np.max(np.abs(flux["mixed"] / flux["fp64"] - 1.0)))}
+
+
 def run_gpu(args, rank, world):
     import torch
     import fastspec_b200 as F
@@ -133,16 +198,7 @@ def run_gpu(args, rank, world):
     stream = torch.cuda.ExternalStream(C.stream_ptr(), device=dev)
 
     # resident device copies of the line list (value arm)
-    dt = {k: torch.from_numpy(np.ascontiguousarray(v)).to(f"cuda:{dev}") for k, v in arr.items()}
-    dl = F.CLines()
-    dl.n = nlines
-    dl.kind = 2
-    for k in ("wl",):
-        setattr(dl, k, F.C.cast(dt[k].data_ptr(), F._dp))
-    for k in ("elo", "gf", "grad", "gqst", "gvdw"):
-        setattr(dl, k, F.C.cast(dt[k].data_ptr(), F._fp))
-    dl.spc = F.C.cast(dt["spc"].data_ptr(), F._ip)
-    dl.ismol = F.C.cast(dt["ismol"].data_ptr(), F._ip)
+    dt, dl = device_lines(F, torch, arr, dev)
     spl = torch.empty((nwl, NMU), dtype=torch.float64, device=f"cuda:{dev}")
     spc = torch.empty_like(spl)
     sfl = torch.empty(nwl, dtype=torch.float64, device=f"cuda:{dev}")
@@ -216,6 +272,9 @@ def run_gpu(args, rank, world):
         h2d = sum(int(v.numel() * v.element_size()) for v in pin.values())
         out.update(ms_e2e=ms_e2e, h2d=h2d, d2h=2 * nwl * 8, flux_check=float(hsfl[nwl // 2].item()))
     C.close()
+    del dt
+    if not args.no_plain and rank == 0:
+        out["plain"] = plain_vs_mixed(F, torch, st, meta, co, dev, int(args.plain_lines))
     return out
 
 
@@ -307,8 +366,9 @@ def main():
     value = world * r["evals"] * K / (r["ms"] / 1e3)
     st = r["stats"]
     nl = max(1, st["accum_launches"])
-    ms_launch = st["ms_accum_kernels"] / nl
-    achieved = (r["evals"] / nl) * FLOPS_PER_EVAL / (ms_launch / 1e3) / 1e12
+    wing_evals = r["evals"] - st["core_evals"]
+    ms_launch = st["ms_wing_kernels"] / nl
+    achieved = (wing_evals / nl) * FLOPS_PER_EVAL / (ms_launch / 1e3) / 1e12
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(HERE, "MEASURED_PEAKS.json")))
@@ -316,6 +376,9 @@ def main():
         pass
     smmax = float(peaks.get("sm_max_mhz", 1965.0))
     fp32_peak = 148 * 128 * 2 * smmax * 1e6 / 1e12
+    # one reciprocal (MUFU) per wing evaluation; 16 MUFU results per SM and clock
+    xu_peak = 148 * 16 * smmax * 1e6
+    xu_achieved = wing_evals / (st["ms_wing_kernels"] / 1e3)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak" if world > 1 else "strong",
@@ -328,11 +391,20 @@ def main():
         "line_evals_per_step": r["evals"],
         "lines_retained": st["nlines_used"],
         "stage_ms": {"center": st["ms_center"], "accumulate": st["ms_accum"],
-                     "accum_kernels": st["ms_accum_kernels"], "accum_launches": st["accum_launches"]},
-        "roofline": {"kernel": "k_accum_fast", "bound": "fp32", "achieved": achieved,
-                     "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                     "accum_kernels": st["ms_accum_kernels"], "wing_kernels": st["ms_wing_kernels"],
+                     "core_kernels": st["ms_core_kernels"], "accum_launches": st["accum_launches"]},
+        "roofline": {"kernel": "k_accum_fast (wing pass)", "bound": "fp32", "achieved": achieved,
+                     "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                     "traffic": (TRAFFIC_PER_WING_EVAL * wing_evals / nl) if TRAFFIC_PER_WING_EVAL else None,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the wing launches, "
+                                       "per evaluation, times the evaluations of one launch",
                      "peak_source": "derived: 148 SMs x 128 FP32 lanes x 2 x %.0f MHz (no FP32 peak is measured)" % smmax,
-                     "flops_per_eval": FLOPS_PER_EVAL},
+                     "flops_per_eval": FLOPS_PER_EVAL, "evals_per_launch": wing_evals / nl,
+                     "ms_per_launch": ms_launch,
+                     "xu": {"achieved": xu_achieved, "peak": xu_peak, "unit": "reciprocals/s",
+                            "frac": xu_achieved / xu_peak}},
+        "core_pass": {"kernel": "k_core_fast", "evals": st["core_evals"], "ms": st["ms_core_kernels"],
+                      "evals_per_s": st["core_evals"] / max(st["ms_core_kernels"], 1e-9) * 1e3},
         "gpu_launches": r["launches"],
         "clocks": r["clocks"],
     }
@@ -341,6 +413,8 @@ def main():
                        "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"]}
     if cpu:
         line["cpu_baseline"] = cpu
+    if "plain" in r:
+        line["plain_fp64"] = r["plain"]
     print(json.dumps(line))
 
 

@@ -45,7 +45,8 @@ class Stats(C.Structure):
     _fields_ = [("nlines_in", C.c_int64), ("nlines_used", C.c_int64), ("nwide", C.c_int64),
                 ("nweak", C.c_int64), ("nblocks", C.c_int64), ("line_evals", C.c_double),
                 ("ms_center", C.c_double), ("ms_params", C.c_double), ("ms_accum", C.c_double),
-                ("ms_total", C.c_double), ("accum_launches", C.c_int64), ("ms_accum_kernels", C.c_double)]
+                ("ms_total", C.c_double), ("accum_launches", C.c_int64), ("ms_accum_kernels", C.c_double),
+                ("ms_wing_kernels", C.c_double), ("ms_core_kernels", C.c_double), ("core_evals", C.c_double)]
 
     def asdict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -35,6 +35,7 @@ void fsg_launch_locprf(cudaStream_t, int, int, const double *, int, const double
 int fsg_fast_set_constants(const double *, const double *);
 int fsg_launch_accum_fast(cudaStream_t, int, int, int, const double *, const LineHdr *, const WingRec *,
                           const int *, const int *, double *, int *);
+void fsg_launch_count_core(cudaStream_t, int64_t, const LineHdr *, unsigned long long *);
 void fsg_launch_core_fast(cudaStream_t, int, int, const double *, const LineHdr *, const WingRec *, const CoreRec *,
                           const int *, const int *, const float *, double *);
 int fsg_fast_tiles(int);
@@ -115,7 +116,7 @@ struct fsg_ctx {
     DBuf l_wl, l_elo, l_gf, l_grad, l_gqst, l_gvdw, l_spc, l_ismol, l_ihe;
     DBuf d_flags, d_ileft, d_iright, d_idx, d_counts, d_offs, d_total, d_hist, d_nkeep;
     // block buffers
-    DBuf d_wing, d_core, d_hdr, d_tlo, d_thi, d_p64, d_lstart, d_lstop, d_widx, d_pw, d_evals, d_err;
+    DBuf d_wing, d_core, d_hdr, d_tlo, d_thi, d_p64, d_lstart, d_lstop, d_widx, d_pw, d_evals, d_err, d_ncore;
     // spectra
     DBuf d_spl, d_spc, d_sfl, d_sfc, d_work, d_a, d_v, d_h, d_l;
     // magnetic
@@ -200,7 +201,7 @@ void fsg_destroy(fsg_ctx *ctx) {
                      &ctx->l_grad, &ctx->l_gqst, &ctx->l_gvdw, &ctx->l_spc, &ctx->l_ismol, &ctx->l_ihe,
                      &ctx->d_flags, &ctx->d_ileft, &ctx->d_iright, &ctx->d_idx, &ctx->d_counts, &ctx->d_offs,
                      &ctx->d_total, &ctx->d_hist, &ctx->d_nkeep, &ctx->d_wing, &ctx->d_core, &ctx->d_hdr,
-                     &ctx->d_tlo, &ctx->d_thi, &ctx->d_err, &ctx->d_p64, &ctx->d_lstart, &ctx->d_lstop, &ctx->d_widx,
+                     &ctx->d_tlo, &ctx->d_thi, &ctx->d_err, &ctx->d_ncore, &ctx->d_p64, &ctx->d_lstart, &ctx->d_lstop, &ctx->d_widx,
                      &ctx->d_pw, &ctx->d_evals, &ctx->d_spl, &ctx->d_spc, &ctx->d_sfl, &ctx->d_sfc,
                      &ctx->d_work, &ctx->d_a, &ctx->d_v, &ctx->d_h, &ctx->d_l, &ctx->z_npi, &ctx->z_nsi,
                      &ctx->z_pioff, &ctx->z_sioff, &ctx->z_splpi, &ctx->z_strpi, &ctx->z_splsi, &ctx->z_strsi,
@@ -473,7 +474,7 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st) {
     fsg_launch_class_hist(s, n, ctx->d_flags.as<int32_t>(), ctx->d_ileft.as<int32_t>(), ctx->d_iright.as<int32_t>(),
                           ctx->d_hist.as<unsigned long long>());
     ctx->launches += 1;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kt;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kt, kc;   // wing pass, core pass
     size_t kev_used = 0;
     auto kevent = [&]() -> cudaEvent_t {
         if (kev_used == ctx->kev.size()) { cudaEvent_t e; cudaEventCreate(&e); ctx->kev.push_back(e); }
@@ -491,6 +492,8 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st) {
     ALLOC(ctx->d_tlo, sizeof(int) * ntiles); ALLOC(ctx->d_thi, sizeof(int) * ntiles);
     ALLOC(ctx->d_err, sizeof(int));
     CK(cudaMemsetAsync(ctx->d_err.p, 0, sizeof(int), s), "err reset");
+    ALLOC(ctx->d_ncore, sizeof(unsigned long long));
+    CK(cudaMemsetAsync(ctx->d_ncore.p, 0, sizeof(unsigned long long), s), "core count reset");
     size_t per_line = (size_t)nt * (sizeof(WingRec) + sizeof(CoreRec)) + sizeof(LineHdr);
     int64_t cap = block_capacity(ctx, per_line);
     int64_t nblocks = 0;
@@ -512,20 +515,23 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st) {
                                    ctx->d_ileft.as<int32_t>(), ctx->d_iright.as<int32_t>(), ctx->d_wing.as<WingRec>(),
                                    ctx->d_core.as<CoreRec>(), ctx->d_hdr.as<LineHdr>());
             fsg_launch_tile_span(s, c, ctx->nwl, nb, ctx->d_hdr.as<LineHdr>(), ctx->d_tlo.as<int>(), ctx->d_thi.as<int>());
-            cudaEvent_t ea = kevent(), eb = kevent();
+            fsg_launch_count_core(s, nb, ctx->d_hdr.as<LineHdr>(), ctx->d_ncore.as<unsigned long long>());
+            cudaEvent_t ea = kevent(), em = kevent(), eb = kevent();
             cudaEventRecord(ea, s);
             int rc2 = fsg_launch_accum_fast(s, c, nt, ctx->nwl, ctx->d_wave.as<double>(), ctx->d_hdr.as<LineHdr>(),
                                             ctx->d_wing.as<WingRec>(), ctx->d_tlo.as<int>(), ctx->d_thi.as<int>(),
                                             ctx->d_lineopac.as<double>(), ctx->d_err.as<int>());
             if (rc2) return cuda_fail(ctx, cudaGetLastError(), "k_accum_fast");
+            cudaEventRecord(em, s);
             // core ranges of the same lines, 32-wavelength tiles
             fsg_launch_tile_span(s, -1, ctx->nwl, nb, ctx->d_hdr.as<LineHdr>(), ctx->d_tlo.as<int>(), ctx->d_thi.as<int>());
             fsg_launch_core_fast(s, nt, ctx->nwl, ctx->d_wave.as<double>(), ctx->d_hdr.as<LineHdr>(),
                                  ctx->d_wing.as<WingRec>(), ctx->d_core.as<CoreRec>(), ctx->d_tlo.as<int>(),
                                  ctx->d_thi.as<int>(), ctx->tab.vtab, ctx->d_lineopac.as<double>());
             cudaEventRecord(eb, s);
-            kt.push_back({ ea, eb });
-            ctx->launches += 7;
+            kt.push_back({ ea, em });
+            kc.push_back({ em, eb });
+            ctx->launches += 8;
             nblocks++;
         }
     }
@@ -534,9 +540,16 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st) {
     int kerr = 0;
     CK(cudaMemcpy(&kerr, ctx->d_err.p, sizeof(int), cudaMemcpyDeviceToHost), "err read");
     if (kerr) return fail(ctx, FSG_E_TIMEOUT, "k_accum_fast: a line-record copy did not complete within its bound");
-    double ms = 0.0;
-    for (auto &p : kt) { float x = 0; cudaEventElapsedTime(&x, p.first, p.second); ms += x; }
-    if (st) { st->nblocks = nblocks; st->accum_launches = (int64_t)kt.size(); st->ms_accum_kernels = ms; }
+    unsigned long long ncore = 0;
+    CK(cudaMemcpy(&ncore, ctx->d_ncore.p, sizeof ncore, cudaMemcpyDeviceToHost), "core count read");
+    double msw = 0.0, msc = 0.0;
+    for (auto &p : kt) { float x = 0; cudaEventElapsedTime(&x, p.first, p.second); msw += x; }
+    for (auto &p : kc) { float x = 0; cudaEventElapsedTime(&x, p.first, p.second); msc += x; }
+    if (st) {
+        st->nblocks = nblocks; st->accum_launches = (int64_t)kt.size(); st->ms_accum_kernels = msw + msc;
+        st->ms_wing_kernels = msw; st->ms_core_kernels = msc;
+        st->core_evals = (double)ncore * nt;
+    }
     return FSG_OK;
 }
 

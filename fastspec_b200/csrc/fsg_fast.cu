@@ -69,7 +69,7 @@ __device__ __forceinline__ float hv_core32(const float *__restrict__ vtab, float
 // roundoff of a few terms; the Kahan pairs carry the long sums.
 #define FOLD 16
 // Candidate lines staged per TMA bulk copy (double-buffered)
-#define CH 16
+#define CH 32
 // Bound on an mbarrier wait: one second of %globaltimer (a chunk's copy completes in microseconds),
 // and at most WAIT_POLLS polls whatever the timer reads
 #define WAIT_NS 1000000000ull
@@ -403,6 +403,19 @@ void fsg_launch_tile_span(cudaStream_t s, int cls, int nwl, int64_t nb, const Li
     int ntiles = (nwl + tw - 1) / tw;
     k_tile_reset<<<(ntiles + 255) / 256, 256, 0, s>>>(ntiles, lo, hi);
     if (nb > 0) k_tile_span<<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(nb, tw, cls < 0 ? 1 : 0, hdr, lo, hi);
+}
+
+// wavelengths inside the core ranges of a block's lines (the core pass's evaluations / ntau)
+__global__ void k_count_core(int64_t nb, const LineHdr *hdr, unsigned long long *acc) {
+    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long v = 0;
+    if (j < nb) { LineHdr h = hdr[j]; if (h.cl <= h.cr) v = (unsigned long long)(h.cr - h.cl + 1); }
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(acc, v);
+}
+
+void fsg_launch_count_core(cudaStream_t s, int64_t nb, const LineHdr *hdr, unsigned long long *acc) {
+    if (nb > 0) k_count_core<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>(nb, hdr, acc);
 }
 
 // ---- window-width classes and order-preserving compaction -----------------------------------

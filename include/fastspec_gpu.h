@@ -79,6 +79,8 @@ typedef struct {
     double  ms_center, ms_params, ms_accum, ms_total;   /* device time per stage [ms] */
     int64_t accum_launches; /* launches of the accumulation kernel */
     double  ms_accum_kernels;   /* summed device time of those launches [ms] */
+    double  ms_wing_kernels, ms_core_kernels;   /* mixed path: the wing and core passes of it [ms] */
+    double  core_evals;     /* mixed path: evaluations inside the lines' core ranges (core pass) */
 } fsg_stats;
 
 /* ---- context ------------------------------------------------------------------------- */
