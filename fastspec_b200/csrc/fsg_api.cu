@@ -15,7 +15,8 @@ void fsg_launch_xline_init(cudaStream_t, int, const double *, const double *, co
 void fsg_launch_center(cudaStream_t, const AtmView &, const LineView &, const VoigtTables &, int32_t *,
                        int32_t *, int32_t *, unsigned long long *);
 void fsg_launch_params_fast(cudaStream_t, const AtmView &, const LineView &, const int64_t *, int64_t, int64_t,
-                            const int32_t *, const int32_t *, const int32_t *, WingRec *, CoreRec *, LineHdr *);
+                            const int32_t *, const int32_t *, const int32_t *, const VoigtTables &, WingRec *,
+                            CoreRec *, LineHdr *);
 void fsg_launch_params_fp64(cudaStream_t, const AtmView &, const LineView &, int64_t, int64_t, const int32_t *,
                             double3 *);
 void fsg_launch_span(cudaStream_t, int64_t, const int32_t *, const int32_t *, const int32_t *, int *, int *);
@@ -36,10 +37,11 @@ int fsg_fast_set_constants(const double *, const double *);
 int fsg_launch_accum_fast(cudaStream_t, int, int, int, const double *, const LineHdr *, const WingRec *,
                           const int *, const int *, double *, int *);
 void fsg_launch_count_core(cudaStream_t, int64_t, const LineHdr *, unsigned long long *);
-void fsg_launch_core_fast(cudaStream_t, int, int, const double *, const LineHdr *, const WingRec *, const CoreRec *,
-                          const int *, const int *, const float *, double *);
+int fsg_launch_core_fast(cudaStream_t, int, int, const double *, const LineHdr *, const WingRec *, const CoreRec *,
+                         const int *, const int *, const float4 *, double *);
 int fsg_fast_tiles(int);
-void fsg_launch_tile_span(cudaStream_t, int, int, int64_t, const LineHdr *, int *, int *);
+size_t fsg_tile_span_scratch(int64_t);
+int fsg_launch_tile_span(cudaStream_t, int, int, int64_t, const LineHdr *, int *, int *, void *, size_t);
 int fsg_select(cudaStream_t, int64_t, const int32_t *, const int32_t *, const int32_t *, int, int *, int64_t *,
                int64_t *, int64_t *);
 void fsg_launch_class_hist(cudaStream_t, int64_t, const int32_t *, const int32_t *, const int32_t *,
@@ -116,7 +118,7 @@ struct fsg_ctx {
     DBuf l_wl, l_elo, l_gf, l_grad, l_gqst, l_gvdw, l_spc, l_ismol, l_ihe;
     DBuf d_flags, d_ileft, d_iright, d_idx, d_counts, d_offs, d_total, d_hist, d_nkeep;
     // block buffers
-    DBuf d_wing, d_core, d_hdr, d_tlo, d_thi, d_p64, d_lstart, d_lstop, d_widx, d_pw, d_evals, d_err, d_ncore;
+    DBuf d_wing, d_core, d_hdr, d_tlo, d_thi, d_p64, d_lstart, d_lstop, d_widx, d_pw, d_evals, d_err, d_ncore, d_span;
     // spectra
     DBuf d_spl, d_spc, d_sfl, d_sfc, d_work, d_a, d_v, d_h, d_l;
     // magnetic
@@ -201,7 +203,7 @@ void fsg_destroy(fsg_ctx *ctx) {
                      &ctx->l_grad, &ctx->l_gqst, &ctx->l_gvdw, &ctx->l_spc, &ctx->l_ismol, &ctx->l_ihe,
                      &ctx->d_flags, &ctx->d_ileft, &ctx->d_iright, &ctx->d_idx, &ctx->d_counts, &ctx->d_offs,
                      &ctx->d_total, &ctx->d_hist, &ctx->d_nkeep, &ctx->d_wing, &ctx->d_core, &ctx->d_hdr,
-                     &ctx->d_tlo, &ctx->d_thi, &ctx->d_err, &ctx->d_ncore, &ctx->d_p64, &ctx->d_lstart, &ctx->d_lstop, &ctx->d_widx,
+                     &ctx->d_tlo, &ctx->d_thi, &ctx->d_err, &ctx->d_ncore, &ctx->d_span, &ctx->d_p64, &ctx->d_lstart, &ctx->d_lstop, &ctx->d_widx,
                      &ctx->d_pw, &ctx->d_evals, &ctx->d_spl, &ctx->d_spc, &ctx->d_sfl, &ctx->d_sfc,
                      &ctx->d_work, &ctx->d_a, &ctx->d_v, &ctx->d_h, &ctx->d_l, &ctx->z_npi, &ctx->z_nsi,
                      &ctx->z_pioff, &ctx->z_sioff, &ctx->z_splpi, &ctx->z_strpi, &ctx->z_splsi, &ctx->z_strsi,
@@ -509,12 +511,15 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st) {
         ALLOC(ctx->d_wing, sizeof(WingRec) * (size_t)bcap * nt);
         ALLOC(ctx->d_core, sizeof(CoreRec) * (size_t)bcap * nt);
         ALLOC(ctx->d_hdr, sizeof(LineHdr) * (size_t)bcap);
+        ALLOC(ctx->d_span, fsg_tile_span_scratch(bcap));
         for (int64_t j0 = 0; j0 < nc; j0 += bcap) {
             int64_t nb = std::min(bcap, nc - j0);
             fsg_launch_params_fast(s, A, LV, ctx->d_idx.as<int64_t>(), j0, nb, ctx->d_flags.as<int32_t>(),
-                                   ctx->d_ileft.as<int32_t>(), ctx->d_iright.as<int32_t>(), ctx->d_wing.as<WingRec>(),
-                                   ctx->d_core.as<CoreRec>(), ctx->d_hdr.as<LineHdr>());
-            fsg_launch_tile_span(s, c, ctx->nwl, nb, ctx->d_hdr.as<LineHdr>(), ctx->d_tlo.as<int>(), ctx->d_thi.as<int>());
+                                   ctx->d_ileft.as<int32_t>(), ctx->d_iright.as<int32_t>(), ctx->tab,
+                                   ctx->d_wing.as<WingRec>(), ctx->d_core.as<CoreRec>(), ctx->d_hdr.as<LineHdr>());
+            if (fsg_launch_tile_span(s, c, ctx->nwl, nb, ctx->d_hdr.as<LineHdr>(), ctx->d_tlo.as<int>(),
+                                     ctx->d_thi.as<int>(), ctx->d_span.p, ctx->d_span.cap))
+                return cuda_fail(ctx, cudaGetLastError(), "tile span");
             fsg_launch_count_core(s, nb, ctx->d_hdr.as<LineHdr>(), ctx->d_ncore.as<unsigned long long>());
             cudaEvent_t ea = kevent(), em = kevent(), eb = kevent();
             cudaEventRecord(ea, s);
@@ -524,14 +529,17 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st) {
             if (rc2) return cuda_fail(ctx, cudaGetLastError(), "k_accum_fast");
             cudaEventRecord(em, s);
             // core ranges of the same lines, 32-wavelength tiles
-            fsg_launch_tile_span(s, -1, ctx->nwl, nb, ctx->d_hdr.as<LineHdr>(), ctx->d_tlo.as<int>(), ctx->d_thi.as<int>());
-            fsg_launch_core_fast(s, nt, ctx->nwl, ctx->d_wave.as<double>(), ctx->d_hdr.as<LineHdr>(),
-                                 ctx->d_wing.as<WingRec>(), ctx->d_core.as<CoreRec>(), ctx->d_tlo.as<int>(),
-                                 ctx->d_thi.as<int>(), ctx->tab.vtab, ctx->d_lineopac.as<double>());
+            if (fsg_launch_tile_span(s, -1, ctx->nwl, nb, ctx->d_hdr.as<LineHdr>(), ctx->d_tlo.as<int>(),
+                                     ctx->d_thi.as<int>(), ctx->d_span.p, ctx->d_span.cap))
+                return cuda_fail(ctx, cudaGetLastError(), "core tile span");
+            rc2 = fsg_launch_core_fast(s, nt, ctx->nwl, ctx->d_wave.as<double>(), ctx->d_hdr.as<LineHdr>(),
+                                       ctx->d_wing.as<WingRec>(), ctx->d_core.as<CoreRec>(), ctx->d_tlo.as<int>(),
+                                       ctx->d_thi.as<int>(), ctx->tab.vtab4, ctx->d_lineopac.as<double>());
+            if (rc2) return cuda_fail(ctx, cudaGetLastError(), "k_core_fast");
             cudaEventRecord(eb, s);
             kt.push_back({ ea, em });
             kc.push_back({ em, eb });
-            ctx->launches += 8;
+            ctx->launches += 16;   // params, 2 x (extract, 2 scans of 2 kernels, search), count, wing, core
             nblocks++;
         }
     }

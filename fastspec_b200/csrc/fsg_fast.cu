@@ -22,6 +22,9 @@
 // exactly as HVoigt branches.
 #include "fsg_internal.cuh"
 
+#include <cub/device/device_scan.cuh>
+#include <algorithm>
+
 #define CLASS_W0 128      // class c: windows of at most CLASS_W0 * 2^(c+1) wavelengths
 
 __constant__ float c_anode[FSG_NA1];
@@ -35,29 +38,13 @@ int fsg_fast_set_constants(const double *anode_h, const double *aida_h) {
     return FSG_OK;
 }
 
-// HVoigt * LinCop in FP32 for the table / continued-fraction region (voigt.f90:81-108)
-__device__ __forceinline__ float hv_core32(const float *__restrict__ vtab, float v, float a, float cop) {
-    float av = fabsf(v);
-    if (a < 8.0f && av < 8.0f) {
-        float fv = av * 125.0f;
-        int iv = min((int)fv, FSG_NVV - 1);
-        float tv = fv - (float)iv, ua;
-        int ia;
-        if (a < c_anode[1]) { ia = 1; ua = a * c_aida[0]; }
-        else {
-            ia = (int)(sqrtf(a) * 141.42135623730951f) + 1;
-            ia = min(ia, FSG_NVA);
-            ua = (a - c_anode[ia - 1]) * c_aida[ia - 1];
-        }
-        const float *p0 = vtab + (ia - 1) * FSG_NV1 + iv, *p1 = p0 + FSG_NV1;
-        float t00 = __ldg(p0), t01 = __ldg(p0 + 1), t10 = __ldg(p1), t11 = __ldg(p1 + 1);
-        float c0 = t00 + tv * (t01 - t00), c1 = t10 + tv * (t11 - t10);
-        return (c0 + ua * (c1 - c0)) * cop;
-    }
+// HVoigt * LinCop in FP32 outside the table (a >= 8 or |v| >= 8, s < 196): the two-term continued
+// fraction of voigt.f90:103-107 at |v| = av
+__device__ __forceinline__ float hv_cf32(float av, float a, float cop) {
     float a2 = a * a, v2 = av * av;
     float p = v2 - a2 - 1.5f, q = 2.0f * av * a;
     float dr = av * p - a * q, di = av * q + a * p;
-    return 0.56418958354775628f * ((p + 0.5f) * di - q * dr) / (dr * dr + di * di) * cop;
+    return 0.56418958354775628f * __fdividef((p + 0.5f) * di - q * dr, dr * dr + di * di) * cop;
 }
 
 // Kahan-compensated accumulation of one value
@@ -318,21 +305,34 @@ int fsg_launch_accum_fast(cudaStream_t st, int cls, int ntau, int nwl, const dou
 
 // Core pass.  Over each line's core range [cl, cr] the full HVoigt branch structure runs point by
 // point: the table lerp or the continued fraction where fl32(t) < 195.5 (s < 196), the wing form
-// elsewhere.  A CTA owns 32 wavelengths x all depths, warp w depths [w*CORE_D, w*CORE_D + CORE_D);
-// Kahan sums in registers.
+// elsewhere.  A CTA owns 32 wavelengths x all depths, warp w depths [w*CORE_D, w*CORE_D + CORE_D),
+// lane l wavelength tile0 + l; Kahan sums in registers.  The four table entries of a lerp come in
+// one 16-byte load from the cell-major copy of VgtTab.
 #define CORE_D 8
-__global__ void __launch_bounds__(32 * 16)
+
+__device__ __forceinline__ float hv_core32(const float4 *__restrict__ vtab4, float av, const CoreRec &c, float twoA) {
+    if (c.ia > 0 && av < 8.0f) {
+        const float fv = av * 125.0f;
+        const int iv = min((int)fv, FSG_NVV - 1);
+        const float tv = fv - (float)iv;
+        const float4 g = __ldg(vtab4 + (c.ia - 1) * FSG_NV1 + iv);
+        const float c0 = g.x + tv * (g.y - g.x), c1 = g.z + tv * (g.w - g.z);
+        return (c0 + c.ua * (c1 - c0)) * c.cop;
+    }
+    return hv_cf32(av, sqrtf(0.5f * twoA), c.cop);
+}
+
+__global__ void __launch_bounds__(512)
 k_core_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *__restrict__ hdr,
             const WingRec *__restrict__ wing, const CoreRec *__restrict__ core, const int *__restrict__ tile_lo,
-            const int *__restrict__ tile_hi, const float *__restrict__ vtab, double *__restrict__ lineopac) {
+            const int *__restrict__ tile_hi, const float4 *__restrict__ vtab4, double *__restrict__ lineopac) {
     const int tile = blockIdx.x;
     const int lo = tile_lo[tile], hi = tile_hi[tile];
     if (lo > hi) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int t0 = warp * CORE_D;
-    const int nd = min(CORE_D, ntau - t0);
-    if (nd <= 0) return;
-    const int p = tile * 32 + lane;
+    const int nd = min(CORE_D, ntau - t0);               // >= 1: blockDim.x / 32 = ceil(ntau / CORE_D)
+    const int p = tile * 32 + lane, p1 = p + 1;
     const int tile_first = tile * 32 + 1, tile_last = min(tile * 32 + 32, nwl);
     const double wd = wave[min(p, nwl - 1)];
     const float wvh = (float)wd, wvl = (float)(wd - (double)wvh);
@@ -342,25 +342,25 @@ k_core_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *_
     for (int j = lo; j <= hi; j++) {
         const LineHdr h = hdr[j];
         if (h.cr < tile_first || h.cl > tile_last) continue;          // core range misses the tile
-        const int p1 = p + 1;
         if (p1 < h.cl || p1 > h.cr) continue;
         const float dl = (wvh - h.wlh) + (wvl - h.wll);
-        const float x = dl * dl;
+        const float x = dl * dl, adl = fabsf(dl);
         const WingRec *wr = wing + (size_t)j * ntau + t0;
         const CoreRec *cr = core + (size_t)j * ntau + t0;
 #pragma unroll
         for (int d = 0; d < CORE_D; d++) {
-            if (d >= nd) break;
-            const WingRec w = wr[d];
-            const float t = fmaf(x, w.vv2, w.c2m1);
-            float v;
-            if (t < 195.5f) {
-                const CoreRec c = cr[d];
-                v = hv_core32(vtab, fabsf(dl) * c.vv, c.a, c.cop);
-            } else {
-                v = fmaf(w.c1, t, w.c1) * rcp_approx(fmaf(t, t, w.twoA));
+            if (d < nd) {
+                const WingRec w = wr[d];
+                const float t = fmaf(x, w.vv2, w.c2m1);
+                float v;
+                if (t < 195.5f) {
+                    const CoreRec c = cr[d];
+                    v = hv_core32(vtab4, adl * c.vv, c, w.twoA);
+                } else {
+                    v = fmaf(w.c1, t, w.c1) * rcp_approx(fmaf(t, t, w.twoA));
+                }
+                KAHAN(sum[d], cmp[d], v);
             }
-            KAHAN(sum[d], cmp[d], v);
         }
     }
     if (p >= nwl) return;
@@ -370,39 +370,84 @@ k_core_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *_
         if (d < nd) dst[d] = dst[d] + ((double)sum[d] - (double)cmp[d]);
 }
 
-void fsg_launch_core_fast(cudaStream_t st, int ntau, int nwl, const double *wave, const LineHdr *hdr,
-                          const WingRec *wing, const CoreRec *core, const int *tile_lo, const int *tile_hi,
-                          const float *vtab, double *lineopac) {
+int fsg_launch_core_fast(cudaStream_t st, int ntau, int nwl, const double *wave, const LineHdr *hdr,
+                         const WingRec *wing, const CoreRec *core, const int *tile_lo, const int *tile_hi,
+                         const float4 *vtab4, double *lineopac) {
     const int ntiles = (nwl + 31) / 32;
     const int nwarps = (ntau + CORE_D - 1) / CORE_D;     // ntau <= 128: at most 16 warps
-    k_core_fast<<<ntiles, 32 * nwarps, 0, st>>>(ntau, nwl, wave, hdr, wing, core, tile_lo, tile_hi, vtab, lineopac);
+    k_core_fast<<<ntiles, 32 * nwarps, 0, st>>>(ntau, nwl, wave, hdr, wing, core, tile_lo, tile_hi, vtab4, lineopac);
+    return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
 }
 
-// ---- tile candidate ranges of one block: lo/hi of the block-local line index -------------------
 __global__ void k_tile_reset(int ntiles, int *lo, int *hi) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < ntiles) { lo[i] = 0x7fffffff; hi[i] = -1; }
 }
 
-// windows (core = 0) or core ranges (core = 1) of the block's lines against tiles of tw wavelengths
-__global__ void k_tile_span(int64_t nb, int tw, int use_core, const LineHdr *hdr, int *lo, int *hi) {
-    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+// ---- tile candidate ranges of one block: lo/hi of the block-local line index -------------------
+// The block's lines are in wavelength order.  With R_j = max_{i<=j} right_i (prefix max) and
+// S_j = min_{i>=j} left_i (suffix min), both non-decreasing in j, the lines whose span [left,
+// right] meets tile [f, l] all lie in [lo, hi] with lo = first j with R_j >= f and hi = last j
+// with S_j <= l; both come from one binary search per tile.  Spans are the windows (use_core = 0)
+// or the core ranges (use_core = 1; lines without one are left out).
+__device__ __forceinline__ void span_of(const LineHdr &h, int use_core, int *l, int *r) {
+    int a = use_core ? h.cl : h.ileft, b = use_core ? h.cr : h.iright;
+    if (a > b) { a = 0x7fffffff; b = -1; }
+    *l = a; *r = b;
+}
+
+// right_j in order, left_j in reverse order (rev[k] = left_{nb-1-k})
+__global__ void k_span_extract(int nb, int use_core, const LineHdr *__restrict__ hdr, int *right, int *rev_left) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= nb) return;
-    LineHdr h = hdr[j];
-    int l = use_core ? h.cl : h.ileft, r = use_core ? h.cr : h.iright;
-    if (l > r) return;
-    int a = (l - 1) / tw, b = (r - 1) / tw;
-    for (int t = a; t <= b; t++) { atomicMin(&lo[t], (int)j); atomicMax(&hi[t], (int)j); }
+    int l, r;
+    span_of(hdr[j], use_core, &l, &r);
+    right[j] = r;
+    rev_left[nb - 1 - j] = l;
+}
+
+// R: prefix max of right (non-decreasing); V: prefix min of reversed left, S_j = V[nb-1-j]
+__global__ void k_tile_search(int nb, int ntiles, int tw, int nwl, const int *__restrict__ R,
+                              const int *__restrict__ V, int *lo, int *hi) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntiles) return;
+    const int f = t * tw + 1, l = min(t * tw + tw, nwl);
+    int a = 0, b = nb;                                   // first j with R_j >= f
+    while (a < b) { int m = (a + b) >> 1; if (R[m] >= f) b = m; else a = m + 1; }
+    const int jlo = a;
+    a = 0; b = nb;                                       // first j with S_j > l
+    while (a < b) { int m = (a + b) >> 1; if (V[nb - 1 - m] > l) b = m; else a = m + 1; }
+    lo[t] = jlo;
+    hi[t] = a - 1;
 }
 
 // tile count of the narrowest tiles (sizes the lo/hi arrays)
 int fsg_fast_tiles(int nwl) { return (nwl + 31) / 32; }
 
-void fsg_launch_tile_span(cudaStream_t s, int cls, int nwl, int64_t nb, const LineHdr *hdr, int *lo, int *hi) {
-    int tw = cls < 0 ? 32 : 32 * fsg_class_pix(cls);
-    int ntiles = (nwl + tw - 1) / tw;
-    k_tile_reset<<<(ntiles + 255) / 256, 256, 0, s>>>(ntiles, lo, hi);
-    if (nb > 0) k_tile_span<<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(nb, tw, cls < 0 ? 1 : 0, hdr, lo, hi);
+// scratch bytes of fsg_launch_tile_span for nb lines
+size_t fsg_tile_span_scratch(int64_t nb) {
+    size_t t1 = 0, t2 = 0;
+    cub::DeviceScan::InclusiveScan(nullptr, t1, (const int *)nullptr, (int *)nullptr, cub::Max(), (int)nb);
+    cub::DeviceScan::InclusiveScan(nullptr, t2, (const int *)nullptr, (int *)nullptr, cub::Min(), (int)nb);
+    return 4 * sizeof(int) * (size_t)nb + std::max(t1, t2) + 256;
+}
+
+int fsg_launch_tile_span(cudaStream_t s, int cls, int nwl, int64_t nb, const LineHdr *hdr, int *lo, int *hi,
+                         void *scratch, size_t scratch_bytes) {
+    const int tw = cls < 0 ? 32 : 32 * fsg_class_pix(cls);
+    const int ntiles = (nwl + tw - 1) / tw;
+    if (nb <= 0) {
+        k_tile_reset<<<(ntiles + 255) / 256, 256, 0, s>>>(ntiles, lo, hi);
+        return FSG_OK;
+    }
+    int *right = (int *)scratch, *revl = right + nb, *R = revl + nb, *V = R + nb;
+    void *tmp = (void *)(((uintptr_t)(V + nb) + 255) & ~(uintptr_t)255);
+    size_t tb = scratch_bytes - ((char *)tmp - (char *)scratch);
+    k_span_extract<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>((int)nb, cls < 0 ? 1 : 0, hdr, right, revl);
+    if (cub::DeviceScan::InclusiveScan(tmp, tb, right, R, cub::Max(), (int)nb, s) != cudaSuccess) return FSG_E_CUDA;
+    if (cub::DeviceScan::InclusiveScan(tmp, tb, revl, V, cub::Min(), (int)nb, s) != cudaSuccess) return FSG_E_CUDA;
+    k_tile_search<<<(ntiles + 255) / 256, 256, 0, s>>>((int)nb, ntiles, tw, nwl, R, V, lo, hi);
+    return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
 }
 
 // wavelengths inside the core ranges of a block's lines (the core pass's evaluations / ntau)

@@ -75,8 +75,10 @@ struct XCoef {
 //   H * LinCop = c1 (t + 1) / (t^2 + twoA),  t = dl^2 vv2 + c2m1,
 // with vv2 = LinVvgt^2, c2m1 = a^2 - 1/2, twoA = 2 a^2, c1 = LinCop a / sqrt(pi).
 struct __align__(16) WingRec { float vv2, c2m1, twoA, c1; };
-// Table / continued-fraction region (s < 196): LinVvgt, LinCop, a.
-struct __align__(16) CoreRec { float vv, cop, a, pad; };
+// Table / continued-fraction region (s < 196): LinVvgt, LinCop and the table row ia (1-based)
+// with its interpolation weight ua as HVoigt derives them from a (voigt.f90:84-92); ia = 0 when
+// a >= 8 (no table).  a itself is recovered as sqrt(twoA / 2) from the wing record.
+struct __align__(16) CoreRec { float vv, cop, ua; int ia; };
 
 // Line header of a retained line inside a block (fast path).  The centre offset Wlcent is split
 // into FP32 wlh + wll (wlh = fl32(Wlcent), wll = fl32(Wlcent - wlh)).  [cl, cr] is the core range:
@@ -99,6 +101,7 @@ std::string fsg_cuda_msg(cudaError_t e, const char *what);
 // Tables in device memory (built by fsg_tables.cu).
 struct VoigtTables {
     float  *vtab;      // [402][1002]
+    float4 *vtab4;     // [401][1002]: (T[r][i], T[r][i+1], T[r+1][i], T[r+1][i+1]) -- one load per lerp
     float2 *fvtab;     // [402][1002] (H, L)
     double *anode, *aida;   // [402] each
 };

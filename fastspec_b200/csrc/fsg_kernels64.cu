@@ -93,9 +93,19 @@ __global__ void k_tables(float *vtab, float2 *fvtab, double *anode, double *aida
     fvtab[ia * FSG_NV1 + iv] = make_float2((float)h, (float)l);
 }
 
+// the four VgtTab entries of one bilinear cell side by side
+__global__ void k_vtab4(const float *vtab, float4 *vtab4) {
+    int iv = blockIdx.x * blockDim.x + threadIdx.x;   // 0..NVV-1
+    int r = blockIdx.y;                               // 0..NVA-1
+    if (iv >= FSG_NVV) return;
+    const float *p0 = vtab + r * FSG_NV1 + iv, *p1 = p0 + FSG_NV1;
+    vtab4[r * FSG_NV1 + iv] = make_float4(p0[0], p0[1], p1[0], p1[1]);
+}
+
 int fsg_build_tables(VoigtTables *t, cudaStream_t s, std::string *err) {
     cudaError_t e;
-    if ((e = cudaMalloc(&t->vtab, sizeof(float) * FSG_NA1 * FSG_NV1)) != cudaSuccess ||
+    if ((e = cudaMalloc(&t->vtab4, sizeof(float4) * FSG_NVA * FSG_NV1)) != cudaSuccess ||
+        (e = cudaMalloc(&t->vtab, sizeof(float) * FSG_NA1 * FSG_NV1)) != cudaSuccess ||
         (e = cudaMalloc(&t->fvtab, sizeof(float2) * FSG_NA1 * FSG_NV1)) != cudaSuccess ||
         (e = cudaMalloc(&t->anode, sizeof(double) * FSG_NA1)) != cudaSuccess ||
         (e = cudaMalloc(&t->aida, sizeof(double) * FSG_NA1)) != cudaSuccess) {
@@ -105,12 +115,14 @@ int fsg_build_tables(VoigtTables *t, cudaStream_t s, std::string *err) {
     dim3 grid((FSG_NV1 + 127) / 128, FSG_NA1);
     k_tables<<<grid, 128, 0, s>>>(t->vtab, t->fvtab, t->anode, t->aida);
     if ((e = cudaGetLastError()) != cudaSuccess) { *err = fsg_cuda_msg(e, "k_tables"); return FSG_E_CUDA; }
+    k_vtab4<<<dim3((FSG_NVV + 127) / 128, FSG_NVA), 128, 0, s>>>(t->vtab, t->vtab4);
+    if ((e = cudaGetLastError()) != cudaSuccess) { *err = fsg_cuda_msg(e, "k_vtab4"); return FSG_E_CUDA; }
     return FSG_OK;
 }
 
 void fsg_free_tables(VoigtTables *t) {
-    cudaFree(t->vtab); cudaFree(t->fvtab); cudaFree(t->anode); cudaFree(t->aida);
-    t->vtab = nullptr; t->fvtab = nullptr; t->anode = nullptr; t->aida = nullptr;
+    cudaFree(t->vtab); cudaFree(t->vtab4); cudaFree(t->fvtab); cudaFree(t->anode); cudaFree(t->aida);
+    t->vtab = nullptr; t->vtab4 = nullptr; t->fvtab = nullptr; t->anode = nullptr; t->aida = nullptr;
 }
 
 // ================================================================================================
@@ -237,11 +249,13 @@ __device__ __forceinline__ int lower_index(const double *__restrict__ w, int n, 
 __global__ void k_params_fast(AtmView A, LineView L, const int64_t *__restrict__ idx, int64_t j0,
                               int64_t nb, const int32_t *__restrict__ flags,
                               const int32_t *__restrict__ ileft, const int32_t *__restrict__ iright,
+                              const double *__restrict__ anode, const double *__restrict__ aida,
                               WingRec *wing, CoreRec *core, LineHdr *hdr) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= nb) return;
     int64_t i = idx[j0 + j];
     const int nt = A.ntau;
+    const float an1 = (float)anode[1], ai0 = (float)aida[0];
     int f = flags[i];
     double wlc = L.wl[i] - A.wfirst;
     XCoef XC;
@@ -258,7 +272,16 @@ __global__ void k_params_fast(AtmView A, LineView L, const int64_t *__restrict__
         w.twoA = (float)(2.0 * a2);
         w.c1 = (float)(cop * av * FSG_SQRTPIINV);
         CoreRec c;
-        c.vv = (float)vv; c.cop = (float)cop; c.a = (float)av; c.pad = 0.0f;
+        c.vv = (float)vv; c.cop = (float)cop;
+        // table row and weight of a in FP32 (sqrt(a) nodes, voigt.f90:84-92); ia = 0: a >= 8
+        const float af = (float)av;
+        if (!(af < 8.0f)) { c.ia = 0; c.ua = 0.0f; }
+        else if (af < an1) { c.ia = 1; c.ua = af * ai0; }
+        else {
+            int ia = min((int)(sqrtf(af) * 141.42135623730951f) + 1, FSG_NVA);
+            c.ia = ia;
+            c.ua = (af - (float)anode[ia - 1]) * (float)aida[ia - 1];
+        }
         wing[(size_t)j * nt + t] = w;
         core[(size_t)j * nt + t] = c;
         // the accumulation evaluates the core form where fl32(dl^2 vv2 + c2m1) < 195.5; a margin of
@@ -286,10 +309,11 @@ __global__ void k_params_fast(AtmView A, LineView L, const int64_t *__restrict__
 
 void fsg_launch_params_fast(cudaStream_t s, const AtmView &A, const LineView &L, const int64_t *idx,
                             int64_t j0, int64_t nb, const int32_t *flags, const int32_t *ileft,
-                            const int32_t *iright, WingRec *wing, CoreRec *core, LineHdr *hdr) {
+                            const int32_t *iright, const VoigtTables &T, WingRec *wing, CoreRec *core,
+                            LineHdr *hdr) {
     if (nb <= 0) return;
     k_params_fast<<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(A, L, idx, j0, nb, flags, ileft, iright,
-                                                               wing, core, hdr);
+                                                               T.anode, T.aida, wing, core, hdr);
 }
 
 // FP64 parameters for the plain path: p64[j][t] = (LinCop, LinVvgt, LinAvgt)
