@@ -34,8 +34,6 @@ sys.path.insert(0, os.path.join(HERE, "tests"))
 
 METRIC = "Voigt line-evals/s (cool-dwarf 1e8-line synthesis)"
 UNIT = "line-evals/s"
-# DRAM bytes per wing evaluation (ncu capture of the wing launches; profiles/k_accum_fast_cooldwarf.md)
-TRAFFIC_PER_WING_EVAL = None
 FLOPS_PER_EVAL = 12          # nominal FP32 work of one wing evaluation (v^2, rational, scale, sum)
 W0, W1, DSTEP, NMU = 5000.0, 25000.0, 1.0, 7
 
@@ -379,6 +377,8 @@ def main():
     # one reciprocal (MUFU) per wing evaluation; 16 MUFU results per SM and clock
     xu_peak = 148 * 16 * smmax * 1e6
     xu_achieved = wing_evals / (st["ms_wing_kernels"] / 1e3)
+    # DRAM bytes of one wing launch: the LineOpac read-modify-write and one read of the records
+    traffic = 2.0 * r["nwl"] * r["ntau"] * 8 + st["nlines_used"] * (r["ntau"] * 16 + 32) / nl
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak" if world > 1 else "strong",
@@ -395,9 +395,11 @@ def main():
                      "core_kernels": st["ms_core_kernels"], "accum_launches": st["accum_launches"]},
         "roofline": {"kernel": "k_accum_fast (wing pass)", "bound": "fp32", "achieved": achieved,
                      "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                     "traffic": (TRAFFIC_PER_WING_EVAL * wing_evals / nl) if TRAFFIC_PER_WING_EVAL else None,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the wing launches, "
-                                       "per evaluation, times the evaluations of one launch",
+                     "traffic": traffic,
+                     "traffic_source": "per launch: LineOpac read + write (2 x nwl x ntau x 8 B) + the records of the "
+                                       "launch's lines (ntau x 16 + 32 B each); ncu dram__bytes_read.sum + "
+                                       "dram__bytes_write.sum of the 12 wing launches of the 1e6-line case = 0.92 x "
+                                       "this model",
                      "peak_source": "derived: 148 SMs x 128 FP32 lanes x 2 x %.0f MHz (no FP32 peak is measured)" % smmax,
                      "flops_per_eval": FLOPS_PER_EVAL, "evals_per_launch": wing_evals / nl,
                      "ms_per_launch": ms_launch,
