@@ -296,20 +296,24 @@ class Context:
     def lineop_reset(self):
         self._ck(self._lib.fsg_lineop_reset(self.h), "fsg_lineop_reset")
 
-    def lineop_calc(self, lines, want_lineopac=True, want_lines=True):
-        """LineopCalc for one list; returns dict(lineopac, flags, ileft, iright, stats)."""
+    def lineop_calc(self, lines, want_lineopac=True, want_lines=True, want_linstr=False):
+        """LineopCalc for one list; returns dict(lineopac, flags, ileft, iright, stats[, linstr]).
+        want_linstr: central line depths of the retained lines (LinStrCalc; needs set_mu)."""
         n = lines.n
         lo = np.zeros((self.nwl, self.ntau)) if want_lineopac else None
         fl = np.zeros(max(n, 1), np.int32) if want_lines else None
         il = np.zeros(max(n, 1), np.int32) if want_lines else None
         ir = np.zeros(max(n, 1), np.int32) if want_lines else None
+        ls = np.zeros(max(n, 1), np.float32) if want_linstr else None
         st = Stats()
         self._ck(self._lib.fsg_lineop_calc(self.h, C.byref(lines.c), _p(lo, C.c_double), _p(fl, C.c_int32),
-                                           _p(il, C.c_int32), _p(ir, C.c_int32), None, C.byref(st)),
+                                           _p(il, C.c_int32), _p(ir, C.c_int32), _p(ls, C.c_float), C.byref(st)),
                  "fsg_lineop_calc")
         out = dict(lineopac=lo, stats=st.asdict())
         if want_lines:
             out.update(flags=fl[:n], ileft=il[:n], iright=ir[:n])
+        if want_linstr:
+            out["linstr"] = ls[:n]
         return out
 
     def lineop_calc_dev(self, dlines):
@@ -338,16 +342,21 @@ class Context:
         v = lambda p: C.c_void_p(p) if p else None
         self._ck(self._lib.fsg_radtran_dev(self.h, v(d_spl), v(d_spc), v(d_sfl), v(d_sfc)), "fsg_radtran_dev")
 
-    def mag_lineop_calc(self, lines, bframe, bfield, want=True):
+    def mag_lineop_calc(self, lines, bframe, bfield, want=True, want_linstr=False):
         n = lines.n
         bf = _f64(bfield)
         mlo = np.zeros((self.nwl, self.ntau, 6)) if want else None
         fl = np.zeros(max(n, 1), np.int32); il = np.zeros(max(n, 1), np.int32); ir = np.zeros(max(n, 1), np.int32)
+        ls = np.zeros(max(n, 1), np.float32) if want_linstr else None
         st = Stats()
         self._ck(self._lib.fsg_mag_lineop_calc(self.h, C.byref(lines.c), int(bframe), _p(bf, C.c_double), len(bf),
                                                _p(mlo, C.c_double), _p(fl, C.c_int32), _p(il, C.c_int32),
-                                               _p(ir, C.c_int32), None, C.byref(st)), "fsg_mag_lineop_calc")
-        return dict(maglineopac=mlo, flags=fl[:n], ileft=il[:n], iright=ir[:n], stats=st.asdict())
+                                               _p(ir, C.c_int32), _p(ls, C.c_float), C.byref(st)),
+                 "fsg_mag_lineop_calc")
+        out = dict(maglineopac=mlo, flags=fl[:n], ileft=il[:n], iright=ir[:n], stats=st.asdict())
+        if want_linstr:
+            out["linstr"] = ls[:n]
+        return out
 
     def mag_radtran(self, bframe, bfield):
         bf = _f64(bfield)

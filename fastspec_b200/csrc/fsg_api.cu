@@ -41,6 +41,9 @@ int fsg_launch_core_fast(cudaStream_t, int, int, const double *, const LineHdr *
                          const int *, const int *, const float4 *, double *);
 int fsg_fast_tiles(int);
 size_t fsg_tile_span_scratch(int64_t);
+size_t fsg_linstr_work(int64_t, int, int);
+void fsg_launch_linstr(cudaStream_t, const AtmView &, const LineView &, const VoigtTables &, const int32_t *, int64_t,
+                       int64_t, int, const double *, const double *, const double *, double *, float *);
 int fsg_launch_tile_span(cudaStream_t, int, int, int64_t, const LineHdr *, int *, int *, void *, size_t);
 int fsg_select(cudaStream_t, int64_t, const int32_t *, const int32_t *, const int32_t *, int, int *, int64_t *,
                int64_t *, int64_t *);
@@ -118,7 +121,7 @@ struct fsg_ctx {
     DBuf l_wl, l_elo, l_gf, l_grad, l_gqst, l_gvdw, l_spc, l_ismol, l_ihe;
     DBuf d_flags, d_ileft, d_iright, d_idx, d_counts, d_offs, d_total, d_hist, d_nkeep;
     // block buffers
-    DBuf d_wing, d_core, d_hdr, d_tlo, d_thi, d_p64, d_lstart, d_lstop, d_widx, d_pw, d_evals, d_err, d_ncore, d_span;
+    DBuf d_wing, d_core, d_hdr, d_tlo, d_thi, d_p64, d_lstart, d_lstop, d_widx, d_pw, d_evals, d_err, d_ncore, d_span, d_lswork, d_linstr;
     // spectra
     DBuf d_spl, d_spc, d_sfl, d_sfc, d_work, d_a, d_v, d_h, d_l;
     // magnetic
@@ -203,7 +206,7 @@ void fsg_destroy(fsg_ctx *ctx) {
                      &ctx->l_grad, &ctx->l_gqst, &ctx->l_gvdw, &ctx->l_spc, &ctx->l_ismol, &ctx->l_ihe,
                      &ctx->d_flags, &ctx->d_ileft, &ctx->d_iright, &ctx->d_idx, &ctx->d_counts, &ctx->d_offs,
                      &ctx->d_total, &ctx->d_hist, &ctx->d_nkeep, &ctx->d_wing, &ctx->d_core, &ctx->d_hdr,
-                     &ctx->d_tlo, &ctx->d_thi, &ctx->d_err, &ctx->d_ncore, &ctx->d_span, &ctx->d_p64, &ctx->d_lstart, &ctx->d_lstop, &ctx->d_widx,
+                     &ctx->d_tlo, &ctx->d_thi, &ctx->d_err, &ctx->d_ncore, &ctx->d_span, &ctx->d_lswork, &ctx->d_linstr, &ctx->d_p64, &ctx->d_lstart, &ctx->d_lstop, &ctx->d_widx,
                      &ctx->d_pw, &ctx->d_evals, &ctx->d_spl, &ctx->d_spc, &ctx->d_sfl, &ctx->d_sfc,
                      &ctx->d_work, &ctx->d_a, &ctx->d_v, &ctx->d_h, &ctx->d_l, &ctx->z_npi, &ctx->z_nsi,
                      &ctx->z_pioff, &ctx->z_sioff, &ctx->z_splpi, &ctx->z_strpi, &ctx->z_splsi, &ctx->z_strsi,
@@ -719,16 +722,39 @@ int fsg_lineop_calc_dev(fsg_ctx *ctx, const fsg_lines *d_lines, fsg_stats *st) {
     return lineop_dev(ctx, d_lines, st);
 }
 
+// LinStrCalc (synth.f90:1774-1822) for the retained lines of the list whose central pass set
+// ctx->d_flags (original order); host output, 0 for rejected lines.  Chunks of at most 2^18 lines.
+static int linstr_calc(fsg_ctx *ctx, const fsg_lines *D, float *linstr) {
+    cudaStream_t s = ctx->stream;
+    const int64_t n = D->n;
+    const int64_t chunk = std::min<int64_t>(n, 1 << 18);
+    ALLOC(ctx->d_lswork, fsg_linstr_work(chunk, ctx->ntau, ctx->nmu));
+    ALLOC(ctx->d_linstr, sizeof(float) * (size_t)n);
+    LineView LV = make_view(D);
+    AtmView A = fsg_view(ctx);
+    for (int64_t i0 = 0; i0 < n; i0 += chunk) {
+        fsg_launch_linstr(s, A, LV, ctx->tab, ctx->d_flags.as<int32_t>(), i0, std::min(chunk, n - i0), ctx->nmu,
+                          ctx->d_xmu.as<double>(), ctx->d_wmu.as<double>(), ctx->d_rhox.as<double>(),
+                          ctx->d_lswork.as<double>(), ctx->d_linstr.as<float>());
+        ctx->launches += 1;
+    }
+    CK(cudaGetLastError(), "k_linstr");
+    CK(cudaMemcpyAsync(linstr, ctx->d_linstr.p, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost, s), "linstr");
+    CK(cudaStreamSynchronize(s), "linstr");
+    return FSG_OK;
+}
+
 int fsg_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, double *lineopac, int32_t *flags, int32_t *ileft,
                     int32_t *iright, float *linstr, fsg_stats *st) {
     int rc = check_lines(ctx, lines); if (rc) return rc;
-    (void)linstr;
+    if (linstr && ctx->nmu < 1) return fail(ctx, FSG_E_STATE, "fsg_lineop_calc: line strengths need fsg_set_mu first");
     cudaSetDevice(ctx->device);
     fsg_lines D;
     if (lines->n > 0) { rc = upload_lines(ctx, lines, &D); if (rc) return rc; }
     else D = *lines;
     rc = lineop_dev(ctx, &D, st); if (rc) return rc;
     cudaStream_t s = ctx->stream;
+    if (linstr && lines->n > 0) { rc = linstr_calc(ctx, &D, linstr); if (rc) return rc; }
     size_t n4 = sizeof(int32_t) * lines->n;
     if (lines->n > 0) {
         if (flags) CK(cudaMemcpyAsync(flags, ctx->d_flags.p, n4, cudaMemcpyDeviceToHost, s), "flags");
@@ -802,8 +828,8 @@ int fsg_mag_lineop_reset(fsg_ctx *ctx) {
 int fsg_mag_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, int bframe, const double *bfield, int nbfield,
                         double *maglineopac, int32_t *flags, int32_t *ileft, int32_t *iright, float *linstr,
                         fsg_stats *st) {
-    (void)linstr;
     int rc = check_lines(ctx, lines); if (rc) return rc;
+    if (linstr && ctx->nmu < 1) return fail(ctx, FSG_E_STATE, "fsg_mag_lineop_calc: line strengths need fsg_set_mu first");
     if (lines->kind != 2) return fail(ctx, FSG_E_ARG, "fsg_mag_lineop_calc: magnetic lists have kind 2");
     if (!bfield || (bframe < 0 || bframe > 2) || nbfield < 3 || (bframe == 2 && nbfield != 2 * ctx->nmu + 1))
         return fail(ctx, FSG_E_ARG, "fsg_mag_lineop_calc: BFIELD needs 3 values (frames 0, 1) or 2*nmu+1 (frame 2)");
@@ -858,6 +884,8 @@ int fsg_mag_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, int bframe, const 
     unsigned long long nk = 0;
     CK(cudaMemcpyAsync(&nk, ctx->d_nkeep.p, sizeof nk, cudaMemcpyDeviceToHost, s), "mag center");
     CK(cudaStreamSynchronize(s), "mag center");
+    // the magnetic driver takes the same non-magnetic central depths (synth.f90:1236-1239)
+    if (linstr) { rc = linstr_calc(ctx, &D, linstr); if (rc) return rc; }
     CK(cudaEventRecord(ctx->ev[1], s), "event");
     int64_t nkeep = (int64_t)nk;
     if (st) { st->nlines_used = nkeep; st->nweak = n - nkeep; }
@@ -891,7 +919,14 @@ int fsg_mag_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, int bframe, const 
         CK(cudaMemcpyAsync(ctx->d_zmap.p, iota.data(), sizeof(int64_t) * n, cudaMemcpyHostToDevice, s), "zmap");
         zmap = ctx->d_zmap.as<int64_t>();
     }
-    if (nw == 0) return FSG_OK;
+    if (nw == 0) {                                   // every line rejected: per-line outputs only
+        size_t n4 = sizeof(int32_t) * n;
+        if (flags) CK(cudaMemcpyAsync(flags, ctx->d_flags.p, n4, cudaMemcpyDeviceToHost, s), "flags");
+        if (ileft) CK(cudaMemcpyAsync(ileft, ctx->d_ileft.p, n4, cudaMemcpyDeviceToHost, s), "ileft");
+        if (iright) CK(cudaMemcpyAsync(iright, ctx->d_iright.p, n4, cudaMemcpyDeviceToHost, s), "iright");
+        CK(cudaStreamSynchronize(s), "mag lineop");
+        return FSG_OK;
+    }
     unsigned long long *d_nw = ctx->d_nkeep.as<unsigned long long>();
     CK(cudaMemsetAsync(d_nw, 0, sizeof(unsigned long long), s), "wide");
     fsg_launch_mark_wide(s, A, nw, W.wl, nstep, pf, pl, pr, d_nw);

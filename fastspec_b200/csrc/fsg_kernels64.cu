@@ -640,12 +640,10 @@ void fsg_launch_fvoigt(cudaStream_t s, int64_t n, const double *a, const double 
 }
 
 // LocPrfPP over independent profiles: one thread per profile (kernel-level entry point)
-__global__ void k_locprf(int nprof, int nmu, const double *xmu, int nt, const double *xki,
-                         const double *src, const double *rhox, double *ploc, double *work) {
-    int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= nprof) return;
-    const double *x = xki + (size_t)p * nt, *y = src + (size_t)p * nt;
-    double *d = work + (size_t)p * 3 * nt, *r = d + nt, *u = r + nt;
+// LocPrfPP (solver.f90:123-179) of one profile: x = Xki, y = Src over nt depths, d/r/u work arrays
+// of nt doubles each; the nmu emergent intensities go to out[0 .. nmu-1]
+__device__ void locprf_one(int nmu, const double *xmu, int nt, const double *x, const double *y,
+                           const double *rhox, double *d, double *r, double *u, double *out) {
     // TauStep
     {
         double Dx1 = (rhox[1] - rhox[0]) / 1.0, Yp = (x[1] - x[0]) / Dx1;
@@ -677,8 +675,72 @@ __global__ void k_locprf(int nprof, int nmu, const double *xmu, int nt, const do
             delo_coef(d[k] * Imu, Eps, Alpha, Beta, Gamma);
             Y = Y * Eps + Alpha * y[k] + Beta * y[k + 1] + Gamma * u[k];
         }
-        ploc[(size_t)p * nmu + im] = Y;
+        out[im] = Y;
     }
+}
+
+__global__ void k_locprf(int nprof, int nmu, const double *xmu, int nt, const double *xki,
+                         const double *src, const double *rhox, double *ploc, double *work) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nprof) return;
+    double *d = work + (size_t)p * 3 * nt;
+    locprf_one(nmu, xmu, nt, xki + (size_t)p * nt, src + (size_t)p * nt, rhox, d, d + nt, d + 2 * nt,
+               ploc + (size_t)p * nmu);
+}
+
+// LinStrCalc (synth.f90:1774-1822), plane-parallel: central depth of each retained line from the
+// continuum and continuum + line intensities at its centre (the centre opacities of the central
+// pass: ContOpac at Wlcent, LineOpacity2 at Wlcent), disk-integrated with Wmu when nmu > 1.
+// One thread per line of [i0, i0 + nl); work holds 6 nt + 2 nmu doubles per thread.
+__global__ void k_linstr(AtmView A, LineView L, const float *__restrict__ vtab, const double *__restrict__ anode,
+                         const double *__restrict__ aida, const int32_t *__restrict__ flags, int64_t i0, int64_t nl,
+                         int nmu, const double *__restrict__ xmu, const double *__restrict__ wmu,
+                         const double *__restrict__ rhox, double *work, float *linstr) {
+    const double PlkC1 = FSG_HC * FSG_VC * 1e13 / FSG_KBOLT;
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nl) return;
+    const int64_t i = i0 + k;
+    const int f = flags[i];
+    if (f & FSG_F_WEAK) { linstr[i] = 0.0f; return; }
+    const int nt = A.ntau;
+    double *xc = work + (size_t)k * (6 * nt + 2 * nmu), *xl = xc + nt, *y = xl + nt, *d = y + nt;
+    double *ic = d + 3 * nt, *il = ic + nmu;
+    double wlc = L.wl[i] - A.wfirst;
+    XCoef XC;
+    xline_setup(A, L, i, wlc, line_input_flags(L, i, 0), &XC);
+    const int ihe = XC.IxHe;
+    int iwl = waveidx(A, wlc);
+    double dW = (wlc - A.wave[iwl - 1]) / (A.wave[iwl] - A.wave[iwl - 1]);
+    const double wl = wlc + A.wfirst;
+    const double C1 = PlkC1 / wl, C2 = exp(50.7649141 - 5.0 * log(wl));
+    for (int t = 0; t < nt; t++) {
+        double cop, vv, av;
+        xline_depth(A, t, XC, &cop, &vv, &av);
+        double dWl = 0.0;
+        if (ihe > 0) dWl = 0.0 - center_shift(A, ihe, t);
+        double lo = hvoigt64(vtab, anode, aida, av, dWl * vv) * cop;
+        if (A.motype == 1) lo = lo / A.contstd[t];
+        double co = cont_center(A, iwl, dW, t);
+        xc[t] = co;
+        xl[t] = co + lo;
+        y[t] = C2 / (exp(C1 / A.xi[XI_T * nt + t]) - 1.0);
+    }
+    locprf_one(nmu, xmu, nt, xc, y, rhox, d, d + nt, d + 2 * nt, ic);
+    locprf_one(nmu, xmu, nt, xl, y, rhox, d, d + nt, d + 2 * nt, il);
+    if (nmu == 1) { linstr[i] = (float)(1.0 - il[0] / ic[0]); return; }
+    double FlxL = 0.0, FlxC = 0.0;
+    for (int m = 0; m < nmu; m++) { FlxL = FlxL + wmu[m] * il[m]; FlxC = FlxC + wmu[m] * ic[m]; }
+    linstr[i] = (float)(1.0 - FlxL / FlxC);
+}
+
+size_t fsg_linstr_work(int64_t nl, int nt, int nmu) { return sizeof(double) * (size_t)nl * (6 * nt + 2 * nmu); }
+
+void fsg_launch_linstr(cudaStream_t s, const AtmView &A, const LineView &L, const VoigtTables &T,
+                       const int32_t *flags, int64_t i0, int64_t nl, int nmu, const double *xmu, const double *wmu,
+                       const double *rhox, double *work, float *linstr) {
+    if (nl > 0)
+        k_linstr<<<(unsigned)((nl + 127) / 128), 128, 0, s>>>(A, L, T.vtab, T.anode, T.aida, flags, i0, nl, nmu,
+                                                              xmu, wmu, rhox, work, linstr);
 }
 
 void fsg_launch_locprf(cudaStream_t s, int nprof, int nmu, const double *xmu, int nt, const double *xki,

@@ -338,20 +338,23 @@ def load_state(name):
     return st
 
 
-def make_pins(gold):
-    """Parity fixtures: reference line opacity and spectra of seeded lists on small grids.
-
-    Each run holds the probe lines first (they fix the species inventory order of the EOS,
-    hence the identical state) and the seeded list in a separate region; the region's line
-    opacity, continuum opacity and spectra are stored with the list."""
-    specs = [
+def pin_specs():
+    return [
         # name, atmosphere, list maker, (wstart, wend, step, wmode), pin region
         ("pin_solar", "solar", lambda: W.atomic_lines(160, 5040.5, 5044.5, W.SEED0 + 0),
          (5000.0, 5045.0, 0.005, 0), (5040.0, 5045.0)),
         ("pin_cooldwarf", "cooldwarf", lambda: W.molecular_lines(400, 9040.5, 9046.5, W.SEED0 + 1),
          (9000.0, 9047.0, 0.3, 1), (9040.0, 9047.0)),
     ]
-    for name, atmname, mk, grid, region in specs:
+
+
+def make_pins(gold):
+    """Parity fixtures: reference line opacity and spectra of seeded lists on small grids.
+
+    Each run holds the probe lines first (they fix the species inventory order of the EOS,
+    hence the identical state) and the seeded list in a separate region; the region's line
+    opacity, continuum opacity and spectra are stored with the list."""
+    for name, atmname, mk, grid, region in pin_specs():
         teff, logg, ntau, species, ismol, _, _, vmic, molbrd, _, _ = CONFIGS[atmname]
         model = W.eddington_model(teff, logg, ntau)
         state = load_state(atmname)
@@ -390,6 +393,30 @@ def make_pins(gold):
             spc=sp["spc"][i0:i1 + 1], sfl=fl["sfl"][i0:i1 + 1], sfc=fl["sfc"][i0:i1 + 1],
             **{"line_" + k: v for k, v in a.items()})
         print(name, "lines", extra.n, "region pixels", i1 - i0 + 1)
+
+
+def make_linst_pins(gold):
+    """Line-strength fixtures: the reference's fs_linst.bin (LinStrCalc, SAVE flag 1) for the decks
+    of make_pins, restricted to the seeded lines (the probes come first in the list)."""
+    for name, atmname, mk, grid, region in pin_specs():
+        teff, logg, ntau, species, ismol, _, _, vmic, molbrd, _, _ = CONFIGS[atmname]
+        model = W.eddington_model(teff, logg, ntau)
+        extra = mk()
+        pgf = np.load(os.path.join(HERE, "atm_%s.npz" % atmname))["probe_loggf"]
+        probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
+        merged = merge([probes, extra])
+        with tempfile.TemporaryDirectory() as wd:
+            W.write_krz(os.path.join(wd, "model.krz"), model)
+            merged.write_z(os.path.join(wd, "lines.z"), grid[0], grid[1])
+            deck = ("wave=%.4f, %.4f, %.6f, %d\nsave=1, 0, 0, 0, 0\nvmic=%.3f\nmolbrd=%d\n"
+                    "lines=\n-1  lines.z\n\nmodel=model.krz\nmus=7\n"
+                    % (grid[0], grid[1], grid[2], grid[3], vmic, molbrd))
+            run_ref(wd, deck)
+            ls = fsio.read_linst(os.path.join(wd, "fs_linst.bin"))
+        sel = ls["wave"] >= extra.arrays()["wl"].min() - 1e-9
+        np.savez_compressed(os.path.join(gold, name + "_linst.npz"), wave=ls["wave"][sel],
+                            strength=ls["strength"][sel], ion=ls["ion"][sel], nprobe_rows=int((~sel).sum()))
+        print(name, "line strengths", int(sel.sum()), "of", extra.n, "seeded lines")
 
 
 def mirrored_components(patterns):
@@ -463,6 +490,8 @@ def make_mag_pin(gold):
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "magpin":
         make_mag_pin(os.path.join(REPO, "tests", "golden"))
+    elif len(sys.argv) > 1 and sys.argv[1] == "linst":
+        make_linst_pins(os.path.join(REPO, "tests", "golden"))
     else:
         main()
         make_mag_pin(os.path.join(REPO, "tests", "golden"))

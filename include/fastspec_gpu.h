@@ -122,7 +122,9 @@ int fsg_set_hestark(fsg_ctx *ctx, int nhe, const double *hegam, const double *he
  * AnalyticWindow + WaveIdx), then the line opacity accumulated onto the device LineOpac.
  * lineopac (host, [nwl][ntau], may be NULL) receives the accumulated total when non-NULL.
  * Per-line outputs (host, length n, may be NULL): LinFlag bits, Ileft, Iright, LinStr
- * (central depths via LinStrCalc when nmu > 0 was given with fsg_set_mu). */
+ * (LinStrCalc, synth.f90:1774-1822: REAL(4) central depth of each retained line from the
+ * continuum and line + continuum intensities at its centre, disk-integrated with the fsg_set_mu
+ * weights when nmu > 1; 0 for rejected lines; FSG_E_STATE without fsg_set_mu). */
 int fsg_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, double *lineopac, int32_t *flags,
                     int32_t *ileft, int32_t *iright, float *linstr, fsg_stats *stats);
 int fsg_lineop_calc_dev(fsg_ctx *ctx, const fsg_lines *d_lines, fsg_stats *stats);
@@ -141,7 +143,8 @@ int fsg_radtran_dev(fsg_ctx *ctx, double *d_spl, double *d_spc, double *d_sfl, d
 
 /* ---- magnetic path ---------------------------------------------------------------------- */
 /* MagLineopCalc (synth.f90:1098-1455): bframe/bfield as BFRAME/BFIELD (3 values for frames
- * 0/1, 2*nmu+1 for frame 2).  Accumulates the device MagLineOpac [nwl][ntau][6]. */
+ * 0/1, 2*nmu+1 for frame 2).  Accumulates the device MagLineOpac [nwl][ntau][6].  linstr as for
+ * fsg_lineop_calc (the magnetic driver uses the same non-magnetic central depths). */
 int fsg_mag_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, int bframe, const double *bfield,
                         int nbfield, double *maglineopac, int32_t *flags, int32_t *ileft,
                         int32_t *iright, float *linstr, fsg_stats *stats);

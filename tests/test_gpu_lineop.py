@@ -208,6 +208,47 @@ def test_mixed_path_against_reference_pins(fsg, oracle_mod, name):
 
 
 @pytest.mark.parametrize("name", ["pin_solar", "pin_cooldwarf"])
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_linstr_against_reference_pins(fsg, name, prec):
+    """LinStrCalc on the GPU (FP64 in both precisions) against the reference's fs_linst.bin:
+    REAL(4) central depths of the retained lines, within 1e-7."""
+    d = H.load_pin(name)
+    ref = H.load_pin(name + "_linst")
+    grid, st, meta, co = H.pin_setup(d)
+    C = ctx_for(fsg, grid, st, co, fsg.PREC_MIXED if prec == "mixed" else fsg.PREC_FP64,
+                vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]), nmu=len(d["xmu"]))
+    g = C.lineop_calc(fsg.LineList.from_arrays(H.pin_lines(d)), want_linstr=True)
+    keep = (g["flags"] & 1) == 0
+    assert keep.sum() == len(ref["wave"])
+    assert np.max(np.abs(d["line_wl"][keep] - ref["wave"])) < 1e-9
+    assert np.max(np.abs(g["linstr"][keep] - ref["strength"])) < 1e-7
+    assert np.all(g["linstr"][~keep] == 0.0)
+
+
+@pytest.mark.parametrize("nmu", [1, 5])
+def test_linstr_vs_oracle(fsg, oracle_mod, nmu):
+    """Single-angle depth (nmu = 1) and disk-integrated depth against the oracle."""
+    grid, st, co, L = solar_case(n=300, seed=41)
+    C = ctx_for(fsg, grid, st, co, fsg.PREC_MIXED, nmu=nmu)
+    g = C.lineop_calc(fsg_lines(fsg, L), want_linstr=True)
+    S = oracle_state(oracle_mod, grid, st, co)
+    x, w, _ = oracle_mod.mu_quadrature(1, nmu)
+    r = oracle_mod.lineop_calc(S, ora_lines(oracle_mod, L), list_type=2, nmu=nmu, xmu=x, wmu=w, want_linstr=True)
+    assert np.array_equal(g["flags"] & 1, r["flags"] & 1)        # the mixed path marks no wide lines
+    assert np.max(np.abs(g["linstr"] - r["linstr"])) < 1e-7
+
+
+def test_linstr_needs_mu(fsg):
+    grid, st, co, L = solar_case(n=20, seed=42)
+    C = fsg.Context()
+    C.set_grid(grid["wmode"], grid["wstart"], grid["wend"], grid["dstep"])
+    C.set_atmosphere(st)
+    C.set_contopac(co)
+    with pytest.raises(fsg.FsgError):
+        C.lineop_calc(fsg_lines(fsg, L), want_linstr=True)
+
+
+@pytest.mark.parametrize("name", ["pin_solar", "pin_cooldwarf"])
 def test_fp64_path_against_reference_pins(fsg, name):
     d = H.load_pin(name)
     grid, st, meta, co = H.pin_setup(d)

@@ -113,3 +113,17 @@ def test_mag_rejects_bad_field(fsg):
         C.mag_lineop_calc(fsg.LineList.from_arrays(lines, zeeman=z), 2, [1000.0, 1.0, 2.0])
     with pytest.raises(fsg.FsgError):
         C.mag_lineop_calc(fsg.LineList.from_arrays(lines), 1, [1000.0, 1.0, 2.0])
+
+
+def test_mag_linstr_vs_oracle(fsg, oracle_mod):
+    """Central depths from the magnetic driver: the non-magnetic LinStrCalc of each retained line."""
+    grid, st, co, lines, z = zeeman_case(n=40, seed=35)
+    C, x, w = mag_ctx(fsg, grid, st, co)
+    g = C.mag_lineop_calc(fsg.LineList.from_arrays(lines, zeeman=z), 1, [2000.0, 60.0, 30.0], want=False,
+                          want_linstr=True)
+    S = oracle_mod.State(grid, st, contopac=co, vmicro=1.0)
+    r = oracle_mod.mag_lineop_calc(S, oracle_mod.Lines(**lines, kind=2, zeeman=z), 1, np.array([2000.0, 60.0, 30.0]),
+                                   nmu=len(x), xmu=x, wmu=w, want_linstr=True)
+    assert np.array_equal(g["flags"] & 1, r["flags"] & 1)
+    assert np.max(np.abs(g["linstr"] - r["linstr"])) < 1e-7
+    assert np.any(g["linstr"] > 0)

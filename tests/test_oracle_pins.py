@@ -54,6 +54,25 @@ def test_oracle_lineop_pins_reference(oracle_mod, name):
     assert np.max(np.abs(sfc / d["sfc"] - 1)) < 1e-8
 
 
+@pytest.mark.parametrize("name", ["pin_solar", "pin_cooldwarf"])
+def test_oracle_linstr_pins_reference(oracle_mod, name):
+    """LinStrCalc (synth.f90:1774-1822): central depths of the retained lines against the reference's
+    fs_linst.bin for the same deck (REAL(4) output; intensities agree to ~1e-9)."""
+    d = H.load_pin(name)
+    ref = H.load_pin(name + "_linst")
+    grid, st, meta, co = H.pin_setup(d)
+    S = oracle_mod.State(grid, st, contopac=co, vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]))
+    x, w, _ = oracle_mod.mu_quadrature(1, len(d["xmu"]))
+    r = oracle_mod.lineop_calc(S, oracle_mod.Lines(**H.pin_lines(d), kind=2), list_type=2, nmu=len(x), xmu=x,
+                               wmu=w, want_linstr=True)
+    keep = (r["flags"] & 1) == 0
+    # the same lines are retained, in list order (the reference writes Wlcent + Wfirst: ~1e-11 off)
+    assert keep.sum() == len(ref["wave"])
+    assert np.max(np.abs(d["line_wl"][keep] - ref["wave"])) < 1e-9
+    assert np.max(np.abs(r["linstr"][keep] - ref["strength"])) < 1e-7
+    assert np.all(ref["strength"] > 0)
+
+
 def test_oracle_blocks_equal_single_block(oracle_mod):
     """Segmented blocks (NlinesStep < Nlines) give the single-block result (synth.f90:1012-1088)."""
     d = H.load_pin("pin_solar")
