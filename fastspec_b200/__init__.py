@@ -60,6 +60,7 @@ EXPORTS = [
     "fsg_lineop_device_ptr", "fsg_set_mu", "fsg_radtran", "fsg_radtran_dev", "fsg_mag_lineop_calc",
     "fsg_mag_lineop_reset", "fsg_mag_radtran", "fsg_hvoigt", "fsg_fvoigt", "fsg_voigt_tables",
     "fsg_locprf_pp", "fsg_locprf_pp_noalloc", "fsg_mu_quadrature", "fsg_zeeman_pattern",
+    "fsg_central_dev", "fsg_accumulate_dev",
 ]
 
 _lib = None
@@ -319,6 +320,22 @@ class Context:
     def lineop_calc_dev(self, dlines):
         st = Stats()
         self._ck(self._lib.fsg_lineop_calc_dev(self.h, C.byref(dlines), C.byref(st)), "fsg_lineop_calc_dev")
+        return st.asdict()
+
+    def central_dev(self, dlines, d_flags, d_ileft, d_iright):
+        """Central pass of a device list into device int32 arrays (pointers); returns the retained count."""
+        nk = C.c_int64(0)
+        v = lambda p: C.cast(C.c_void_p(p), C.POINTER(C.c_int32)) if p else None
+        self._ck(self._lib.fsg_central_dev(self.h, C.byref(dlines), v(d_flags), v(d_ileft), v(d_iright),
+                                           C.byref(nk)), "fsg_central_dev")
+        return nk.value
+
+    def accumulate_dev(self, dlines, d_flags, d_ileft, d_iright, i0, i1):
+        """Accumulate a device list with given windows over wavelengths i0..i1 (1-based, inclusive)."""
+        st = Stats()
+        v = lambda p: C.cast(C.c_void_p(p), C.POINTER(C.c_int32)) if p else None
+        self._ck(self._lib.fsg_accumulate_dev(self.h, C.byref(dlines), v(d_flags), v(d_ileft), v(d_iright), int(i0),
+                                              int(i1), C.byref(st)), "fsg_accumulate_dev")
         return st.asdict()
 
     def lineop_get(self):

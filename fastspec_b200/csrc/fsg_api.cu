@@ -56,7 +56,9 @@ void fsg_launch_gather_lines(cudaStream_t, const LineView &, const int64_t *, in
                              const int32_t *, const int32_t *, LineView *, int32_t **, int32_t **, int32_t **);
 int fsg_select_wide(cudaStream_t, int64_t, const int32_t *, int *, int64_t *, int64_t *, int64_t *);
 void fsg_launch_scatter_flags(cudaStream_t, int64_t, const int64_t *, const int32_t *, int32_t *);
-double fsg_count_evals(fsg_ctx *, int64_t);
+double fsg_count_evals(fsg_ctx *, int64_t, const int32_t *, const int32_t *, const int32_t *, int, int);
+void fsg_launch_range_clip(cudaStream_t, int64_t, const int32_t *, const int32_t *, const int32_t *, int, int,
+                           int32_t *, int32_t *, int32_t *);
 size_t fsg_stokes_smem(int, int);
 int fsg_launch_stokes(cudaStream_t, const AtmView &, const double *, const double *, const double *, int,
                       const double *, const double *, const double *, double *, double *);
@@ -121,7 +123,7 @@ struct fsg_ctx {
     DBuf l_wl, l_elo, l_gf, l_grad, l_gqst, l_gvdw, l_spc, l_ismol, l_ihe;
     DBuf d_flags, d_ileft, d_iright, d_idx, d_counts, d_offs, d_total, d_hist, d_nkeep;
     // block buffers
-    DBuf d_wing, d_core, d_hdr, d_tlo, d_thi, d_p64, d_lstart, d_lstop, d_widx, d_pw, d_evals, d_err, d_ncore, d_span, d_lswork, d_linstr;
+    DBuf d_wing, d_core, d_hdr, d_tlo, d_thi, d_p64, d_lstart, d_lstop, d_widx, d_pw, d_evals, d_err, d_ncore, d_span, d_lswork, d_linstr, d_rflags, d_rleft, d_rright;
     // spectra
     DBuf d_spl, d_spc, d_sfl, d_sfc, d_work, d_a, d_v, d_h, d_l;
     // magnetic
@@ -206,7 +208,7 @@ void fsg_destroy(fsg_ctx *ctx) {
                      &ctx->l_grad, &ctx->l_gqst, &ctx->l_gvdw, &ctx->l_spc, &ctx->l_ismol, &ctx->l_ihe,
                      &ctx->d_flags, &ctx->d_ileft, &ctx->d_iright, &ctx->d_idx, &ctx->d_counts, &ctx->d_offs,
                      &ctx->d_total, &ctx->d_hist, &ctx->d_nkeep, &ctx->d_wing, &ctx->d_core, &ctx->d_hdr,
-                     &ctx->d_tlo, &ctx->d_thi, &ctx->d_err, &ctx->d_ncore, &ctx->d_span, &ctx->d_lswork, &ctx->d_linstr, &ctx->d_p64, &ctx->d_lstart, &ctx->d_lstop, &ctx->d_widx,
+                     &ctx->d_tlo, &ctx->d_thi, &ctx->d_err, &ctx->d_ncore, &ctx->d_span, &ctx->d_lswork, &ctx->d_linstr, &ctx->d_rflags, &ctx->d_rleft, &ctx->d_rright, &ctx->d_p64, &ctx->d_lstart, &ctx->d_lstop, &ctx->d_widx,
                      &ctx->d_pw, &ctx->d_evals, &ctx->d_spl, &ctx->d_spc, &ctx->d_sfl, &ctx->d_sfc,
                      &ctx->d_work, &ctx->d_a, &ctx->d_v, &ctx->d_h, &ctx->d_l, &ctx->z_npi, &ctx->z_nsi,
                      &ctx->z_pioff, &ctx->z_sioff, &ctx->z_splpi, &ctx->z_strpi, &ctx->z_splsi, &ctx->z_strsi,
@@ -469,15 +471,29 @@ static int central_pass(fsg_ctx *ctx, const LineView &LV, int64_t *nkeep) {
 }
 
 // mixed-precision accumulation: classes by window width, blocks within a class
-static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st) {
+// fl/il/ir: LinFlag, Ileft, Iright of the list (device); [i0, i1]: 1-based wavelength range to fill
+// (1..nwl for the whole grid).  Lines are classed by their full windows and evaluated over the part
+// of the window inside the range, so each wavelength of the range sums the same lines in the same
+// order as in a whole-grid run.
+static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st, const int32_t *fl, const int32_t *il,
+                           const int32_t *ir, int i0, int i1) {
     int64_t n = LV.n;
     const int nt = ctx->ntau;
     AtmView A = fsg_view(ctx);
     cudaStream_t s = ctx->stream;
+    const int32_t *sf = fl, *wl_ = il, *wr_ = ir;       // selection flags, evaluated window bounds
+    if (i0 > 1 || i1 < ctx->nwl) {
+        ALLOC(ctx->d_rflags, sizeof(int32_t) * std::max<int64_t>(n, 1));
+        ALLOC(ctx->d_rleft, sizeof(int32_t) * std::max<int64_t>(n, 1));
+        ALLOC(ctx->d_rright, sizeof(int32_t) * std::max<int64_t>(n, 1));
+        fsg_launch_range_clip(s, n, fl, il, ir, i0, i1, ctx->d_rflags.as<int32_t>(), ctx->d_rleft.as<int32_t>(),
+                              ctx->d_rright.as<int32_t>());
+        ctx->launches += 1;
+        sf = ctx->d_rflags.as<int32_t>(); wl_ = ctx->d_rleft.as<int32_t>(); wr_ = ctx->d_rright.as<int32_t>();
+    }
     ALLOC(ctx->d_hist, sizeof(unsigned long long) * 32);
     CK(cudaMemsetAsync(ctx->d_hist.p, 0, sizeof(unsigned long long) * 32, s), "hist");
-    fsg_launch_class_hist(s, n, ctx->d_flags.as<int32_t>(), ctx->d_ileft.as<int32_t>(), ctx->d_iright.as<int32_t>(),
-                          ctx->d_hist.as<unsigned long long>());
+    fsg_launch_class_hist(s, n, sf, il, ir, ctx->d_hist.as<unsigned long long>());
     ctx->launches += 1;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> kt, kc;   // wing pass, core pass
     size_t kev_used = 0;
@@ -488,6 +504,11 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st) {
     unsigned long long hist[32];
     CK(cudaMemcpyAsync(hist, ctx->d_hist.p, sizeof hist, cudaMemcpyDeviceToHost, s), "hist");
     CK(cudaStreamSynchronize(s), "hist");
+    if (st) {                                          // lines evaluated (those meeting the range)
+        int64_t nsel = 0;
+        for (int c = 0; c < 32; c++) nsel += (int64_t)hist[c];
+        st->nlines_used = nsel;
+    }
     int64_t nblkscan = (n + 1023) / 1024;
     ALLOC(ctx->d_counts, sizeof(int) * std::max<int64_t>(nblkscan, 1));
     ALLOC(ctx->d_offs, sizeof(int64_t) * std::max<int64_t>(nblkscan, 1));
@@ -504,7 +525,7 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st) {
     int64_t nblocks = 0;
     for (int c = 0; c < 32; c++) {
         if (!hist[c]) continue;
-        int rc = fsg_select(s, n, ctx->d_flags.as<int32_t>(), ctx->d_ileft.as<int32_t>(), ctx->d_iright.as<int32_t>(), c,
+        int rc = fsg_select(s, n, sf, il, ir, c,
                             ctx->d_counts.as<int>(), ctx->d_offs.as<int64_t>(), ctx->d_idx.as<int64_t>(),
                             ctx->d_total.as<int64_t>());
         if (rc) return cuda_fail(ctx, cudaGetLastError(), "select");
@@ -517,8 +538,7 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st) {
         ALLOC(ctx->d_span, fsg_tile_span_scratch(bcap));
         for (int64_t j0 = 0; j0 < nc; j0 += bcap) {
             int64_t nb = std::min(bcap, nc - j0);
-            fsg_launch_params_fast(s, A, LV, ctx->d_idx.as<int64_t>(), j0, nb, ctx->d_flags.as<int32_t>(),
-                                   ctx->d_ileft.as<int32_t>(), ctx->d_iright.as<int32_t>(), ctx->tab,
+            fsg_launch_params_fast(s, A, LV, ctx->d_idx.as<int64_t>(), j0, nb, fl, wl_, wr_, ctx->tab,
                                    ctx->d_wing.as<WingRec>(), ctx->d_core.as<CoreRec>(), ctx->d_hdr.as<LineHdr>());
             if (fsg_launch_tile_span(s, c, ctx->nwl, nb, ctx->d_hdr.as<LineHdr>(), ctx->d_tlo.as<int>(),
                                      ctx->d_thi.as<int>(), ctx->d_span.p, ctx->d_span.cap))
@@ -700,7 +720,8 @@ static int lineop_dev(fsg_ctx *ctx, const fsg_lines *D, fsg_stats *st) {
     CK(cudaEventRecord(ctx->ev[1], s), "event");
     if (st) { st->nlines_used = nkeep; st->nweak = D->n - nkeep; }
     if (ctx->cfg.precision == FSG_PREC_FP64) rc = accumulate_fp64(ctx, LV, nkeep, st);
-    else rc = accumulate_fast(ctx, LV, st);
+    else rc = accumulate_fast(ctx, LV, st, ctx->d_flags.as<int32_t>(), ctx->d_ileft.as<int32_t>(),
+                              ctx->d_iright.as<int32_t>(), 1, ctx->nwl);
     if (rc) return rc;
     CK(cudaEventRecord(ctx->ev[2], s), "event");
     CK(cudaStreamSynchronize(s), "lineop");
@@ -709,9 +730,59 @@ static int lineop_dev(fsg_ctx *ctx, const fsg_lines *D, fsg_stats *st) {
         cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
         cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
         st->ms_center = a; st->ms_accum = b; st->ms_total = a + b;
-        if (ctx->cfg.precision != FSG_PREC_FP64) {
-            st->line_evals = fsg_count_evals(ctx, D->n);
-        }
+        if (ctx->cfg.precision != FSG_PREC_FP64)
+            st->line_evals = fsg_count_evals(ctx, D->n, ctx->d_flags.as<int32_t>(), ctx->d_ileft.as<int32_t>(),
+                                             ctx->d_iright.as<int32_t>(), 1, ctx->nwl);
+    }
+    return FSG_OK;
+}
+
+// ---- split driver for wavelength sharding: central pass of a subset, accumulation of a range ----
+int fsg_central_dev(fsg_ctx *ctx, const fsg_lines *d_lines, int32_t *d_flags, int32_t *d_ileft, int32_t *d_iright,
+                    int64_t *nkeep) {
+    int rc = check_lines(ctx, d_lines); if (rc) return rc;
+    if (d_lines->n > 0 && (!d_flags || !d_ileft || !d_iright))
+        return fail(ctx, FSG_E_ARG, "fsg_central_dev: output arrays missing");
+    cudaSetDevice(ctx->device);
+    LineView LV = make_view(d_lines);
+    ALLOC(ctx->d_nkeep, sizeof(unsigned long long));
+    CK(cudaMemsetAsync(ctx->d_nkeep.p, 0, sizeof(unsigned long long), ctx->stream), "center");
+    if (d_lines->n > 0) {
+        fsg_launch_center(ctx->stream, fsg_view(ctx), LV, ctx->tab, d_flags, d_ileft, d_iright,
+                          ctx->d_nkeep.as<unsigned long long>());
+        ctx->launches += 1;
+        CK(cudaGetLastError(), "k_center");
+    }
+    unsigned long long nk = 0;
+    CK(cudaMemcpyAsync(&nk, ctx->d_nkeep.p, sizeof nk, cudaMemcpyDeviceToHost, ctx->stream), "center");
+    CK(cudaStreamSynchronize(ctx->stream), "center");
+    if (nkeep) *nkeep = (int64_t)nk;
+    return FSG_OK;
+}
+
+int fsg_accumulate_dev(fsg_ctx *ctx, const fsg_lines *d_lines, const int32_t *d_flags, const int32_t *d_ileft,
+                       const int32_t *d_iright, int i0, int i1, fsg_stats *st) {
+    int rc = check_lines(ctx, d_lines); if (rc) return rc;
+    if (ctx->cfg.precision == FSG_PREC_FP64)
+        return fail(ctx, FSG_E_STATE, "fsg_accumulate_dev: the wavelength-range accumulation is mixed precision only");
+    if (i0 < 1 || i1 > ctx->nwl || i0 > i1) return fail(ctx, FSG_E_ARG, "fsg_accumulate_dev: need 1 <= i0 <= i1 <= nwl");
+    if (d_lines->n > 0 && (!d_flags || !d_ileft || !d_iright))
+        return fail(ctx, FSG_E_ARG, "fsg_accumulate_dev: window arrays missing");
+    cudaSetDevice(ctx->device);
+    rc = ensure_lineopac(ctx); if (rc) return rc;
+    if (st) { memset(st, 0, sizeof *st); st->nlines_in = d_lines->n; }
+    if (d_lines->n == 0) return FSG_OK;
+    cudaStream_t s = ctx->stream;
+    CK(cudaEventRecord(ctx->ev[1], s), "event");
+    rc = accumulate_fast(ctx, make_view(d_lines), st, d_flags, d_ileft, d_iright, i0, i1);
+    if (rc) return rc;
+    CK(cudaEventRecord(ctx->ev[2], s), "event");
+    CK(cudaStreamSynchronize(s), "accumulate");
+    if (st) {
+        float b = 0;
+        cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
+        st->ms_accum = b; st->ms_total = b;
+        st->line_evals = fsg_count_evals(ctx, d_lines->n, d_flags, d_ileft, d_iright, i0, i1);
     }
     return FSG_OK;
 }
@@ -1258,21 +1329,24 @@ int fsg_zeeman_pattern(float jlo, float jup, float glo, float gup, int32_t *npi,
 }  // extern "C"
 
 // ---- eval counting for the stats (sum over retained lines of Ntau x window) -------------------------
-__global__ void k_count_evals(int64_t n, const int32_t *flags, const int32_t *il, const int32_t *ir,
+__global__ void k_count_evals(int64_t n, const int32_t *flags, const int32_t *il, const int32_t *ir, int i0, int i1,
                               unsigned long long *acc) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long v = 0;
-    if (i < n && !(flags[i] & FSG_F_WEAK)) v = (unsigned long long)(ir[i] - il[i] + 1);
+    if (i < n && !(flags[i] & FSG_F_WEAK)) {
+        int a = max(il[i], i0), b = min(ir[i], i1);
+        if (a <= b) v = (unsigned long long)(b - a + 1);
+    }
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if ((threadIdx.x & 31) == 0 && v) atomicAdd(acc, v);
 }
 
-double fsg_count_evals(fsg_ctx *ctx, int64_t n) {
+double fsg_count_evals(fsg_ctx *ctx, int64_t n, const int32_t *fl, const int32_t *il, const int32_t *ir, int i0,
+                       int i1) {
     ctx->launches += 1;
     unsigned long long *d = ctx->d_nkeep.as<unsigned long long>();
     cudaMemsetAsync(d, 0, sizeof(unsigned long long), ctx->stream);
-    k_count_evals<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(n, ctx->d_flags.as<int32_t>(),
-        ctx->d_ileft.as<int32_t>(), ctx->d_iright.as<int32_t>(), d);
+    k_count_evals<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(n, fl, il, ir, i0, i1, d);
     unsigned long long h = 0;
     cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, ctx->stream);
     cudaStreamSynchronize(ctx->stream);

@@ -463,6 +463,22 @@ void fsg_launch_count_core(cudaStream_t s, int64_t nb, const LineHdr *hdr, unsig
     if (nb > 0) k_count_core<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>(nb, hdr, acc);
 }
 
+// Restriction to the wavelength range [i0, i1]: lines whose window misses it are marked weak for the
+// selection, the others keep their flags and get the window clipped to the range.
+__global__ void k_range_clip(int64_t n, const int32_t *fl, const int32_t *il, const int32_t *ir, int i0, int i1,
+                             int32_t *rf, int32_t *rl, int32_t *rr) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int f = fl[i], a = max(il[i], i0), b = min(ir[i], i1);
+    if (a > b) f |= FSG_F_WEAK;
+    rf[i] = f; rl[i] = a; rr[i] = b;
+}
+
+void fsg_launch_range_clip(cudaStream_t s, int64_t n, const int32_t *fl, const int32_t *il, const int32_t *ir, int i0,
+                           int i1, int32_t *rf, int32_t *rl, int32_t *rr) {
+    if (n > 0) k_range_clip<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, fl, il, ir, i0, i1, rf, rl, rr);
+}
+
 // ---- window-width classes and order-preserving compaction -----------------------------------
 // class 0: windows up to 256 wavelengths; class c: up to 256 * 2^c.
 __device__ __forceinline__ int width_class(int il, int ir) {

@@ -128,6 +128,19 @@ int fsg_set_hestark(fsg_ctx *ctx, int nhe, const double *hegam, const double *he
 int fsg_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, double *lineopac, int32_t *flags,
                     int32_t *ileft, int32_t *iright, float *linstr, fsg_stats *stats);
 int fsg_lineop_calc_dev(fsg_ctx *ctx, const fsg_lines *d_lines, fsg_stats *stats);
+/* LineopCalc split for wavelength sharding (no counterpart call in the reference, whose driver does
+ * both steps in one routine, synth.f90:833-907 and 1000-1090):
+ * fsg_central_dev runs the central pass (weak-line tests, AnalyticWindow, WaveIdx) of a device
+ * list into caller-owned device arrays LinFlag / Ileft / Iright (n each) and returns the retained
+ * count; fsg_accumulate_dev accumulates a device list whose windows are given onto the device
+ * LineOpac, over wavelength indices i0..i1 (1-based, inclusive) only.  Each wavelength of the range
+ * sums the same lines in the same order as a whole-grid fsg_lineop_calc_dev (equal to rounding:
+ * the Kahan groups of a tile cut by the range ends, and the blocks of a class, may differ); other
+ * wavelengths are left as they are.  Mixed precision only (FSG_E_STATE otherwise). */
+int fsg_central_dev(fsg_ctx *ctx, const fsg_lines *d_lines, int32_t *d_flags, int32_t *d_ileft,
+                    int32_t *d_iright, int64_t *nkeep);
+int fsg_accumulate_dev(fsg_ctx *ctx, const fsg_lines *d_lines, const int32_t *d_flags,
+                       const int32_t *d_ileft, const int32_t *d_iright, int i0, int i1, fsg_stats *stats);
 /* Zero / read / write the device LineOpac accumulator ([nwl][ntau]; OPACITY= re-entry). */
 int fsg_lineop_reset(fsg_ctx *ctx);
 int fsg_lineop_get(fsg_ctx *ctx, double *lineopac);

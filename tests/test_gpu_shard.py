@@ -1,0 +1,80 @@
+"""The device side of wavelength sharding on one GPU: fsg_central_dev over slices of a list gives the
+whole-list windows, and fsg_accumulate_dev over adjacent wavelength ranges rebuilds the whole-grid
+LineOpac (mixed-precision tolerance: the Kahan groups of the tiles cut by a range end differ)."""
+import numpy as np
+import pytest
+import torch
+
+import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+
+def cooldwarf_case(n=4000, w0=9000.0, span=10.0, seed=23):
+    from fastspec_b200 import workloads as W
+    import fastspec_b200 as F
+    st, meta = H.load_atm("cooldwarf")
+    grid = dict(wmode=1, wstart=w0, wend=w0 + span, dstep=1.0)
+    co = H.contopac_on(meta, F.make_grid(1, w0, w0 + span, 1.0) + w0)
+    return grid, st, co, W.molecular_lines(n, w0 - 3, w0 + span + 3, seed).arrays()
+
+
+def make(fsg, grid, st, co, prec=None):
+    C = fsg.Context(precision=fsg.PREC_MIXED if prec is None else prec, vmicro=1.0, molbrd=1)
+    C.set_grid(grid["wmode"], grid["wstart"], grid["wend"], grid["dstep"])
+    C.set_atmosphere(st)
+    C.set_contopac(co)
+    x, w, _ = fsg.mu_quadrature(1, 7)
+    C.set_mu(x, w)
+    return C
+
+
+def test_central_slices_and_range_accumulation(fsg):
+    from fastspec_b200 import shard
+    grid, st, co, arr = cooldwarf_case()
+    C = make(fsg, grid, st, co)
+    full = C.lineop_calc(fsg.LineList.from_arrays(arr))
+    _, _, sfl, sfc = C.radtran()
+    dt = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in arr.items()}
+    B = shard.GpuBackend(fsg, C, dt)
+    n = B.n
+    parts = [B.central(*shard.line_slice(n, 3, r)) for r in range(3)]
+    win = torch.cat(parts, dim=1)[:, :n].cpu().numpy()
+    assert np.array_equal(win[0], full["flags"])
+    assert np.array_equal(win[1], full["ileft"]) and np.array_equal(win[2], full["iright"])
+    wt = torch.from_numpy(win).cuda()
+    ranges = shard.balanced_ranges(shard.pixel_cost(wt, C.nwl), 3)
+    assert ranges[0][0] == 1 and ranges[-1][1] == C.nwl
+    C.lineop_reset()
+    flux = []
+    for i0, i1 in ranges:
+        st_ = C.accumulate_dev(B.full, wt[0].data_ptr(), wt[1].data_ptr(), wt[2].data_ptr(), i0, i1)
+        assert st_["line_evals"] > 0
+    lo = C.lineop_get()
+    ref = full["lineopac"]
+    assert np.max(np.abs(lo - ref) / (ref + co)) < 2e-7
+    # one range alone leaves the rest of LineOpac untouched, and its flux matches the whole-grid flux
+    i0, i1 = ranges[1]
+    C.lineop_reset()
+    C.accumulate_dev(B.full, wt[0].data_ptr(), wt[1].data_ptr(), wt[2].data_ptr(), i0, i1)
+    lo1 = C.lineop_get()
+    assert np.all(lo1[:i0 - 1] == 0) and np.all(lo1[i1:] == 0)
+    f = B.flux(i0, i1).cpu().numpy()
+    assert np.max(np.abs(f[0] / sfl[i0 - 1:i1] - 1)) < 1e-6
+    assert np.max(np.abs(f[1] / sfc[i0 - 1:i1] - 1)) < 1e-12
+
+
+def test_range_accumulation_rejects_fp64_and_bad_ranges(fsg):
+    grid, st, co, arr = cooldwarf_case(n=50)
+    C = make(fsg, grid, st, co, prec=fsg.PREC_FP64)
+    dt = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in arr.items()}
+    from fastspec_b200 import shard
+    B = shard.GpuBackend(fsg, C, dt)
+    win = B.central(0, B.n, B.n)
+    with pytest.raises(fsg.FsgError):
+        C.accumulate_dev(B.full, win[0].data_ptr(), win[1].data_ptr(), win[2].data_ptr(), 1, C.nwl)
+    C2 = make(fsg, grid, st, co)
+    with pytest.raises(fsg.FsgError):
+        C2.accumulate_dev(B.full, win[0].data_ptr(), win[1].data_ptr(), win[2].data_ptr(), 0, C2.nwl)
+    with pytest.raises(fsg.FsgError):
+        C2.accumulate_dev(B.full, win[0].data_ptr(), win[1].data_ptr(), win[2].data_ptr(), 5, 4)
