@@ -52,6 +52,24 @@ class Stats(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("tile_pix", C.c_int32), ("wing_ctas", C.c_int32), ("core_ctas", C.c_int32),
+                ("ms_wing", C.c_double), ("ms_core", C.c_double)]
+
+    def asdict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("natm", C.c_int32), ("nlines_candidate", C.c_int64), ("line_evals", C.c_double),
+                ("ms_total", C.c_double), ("tuning", BatchTuning)]
+
+    def asdict(self):
+        d = {f: getattr(self, f) for f, _ in self._fields_ if f != "tuning"}
+        d["tuning"] = self.tuning.asdict()
+        return d
+
+
 # every symbol the header declares (checked by the CPU test suite)
 EXPORTS = [
     "fsg_create", "fsg_destroy", "fsg_last_error", "fsg_version", "fsg_kernel_launches", "fsg_cuda_stream", "fsg_make_grid", "fsg_set_grid",
@@ -60,7 +78,8 @@ EXPORTS = [
     "fsg_lineop_device_ptr", "fsg_set_mu", "fsg_radtran", "fsg_radtran_dev", "fsg_mag_lineop_calc",
     "fsg_mag_lineop_reset", "fsg_mag_radtran", "fsg_hvoigt", "fsg_fvoigt", "fsg_voigt_tables",
     "fsg_locprf_pp", "fsg_locprf_pp_noalloc", "fsg_mu_quadrature", "fsg_zeeman_pattern",
-    "fsg_central_dev", "fsg_accumulate_dev",
+    "fsg_central_dev", "fsg_accumulate_dev", "fsg_batch_create", "fsg_batch_tune", "fsg_batch_set_tuning",
+    "fsg_batch_run", "fsg_batch_flux", "fsg_batch_stream", "fsg_batch_last_error", "fsg_batch_destroy",
 ]
 
 _lib = None
@@ -118,6 +137,18 @@ def lib():
                                         C.c_void_p, C.c_void_p, C.c_void_p]
     L.fsg_mu_quadrature.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, C.c_int]
     L.fsg_zeeman_pattern.argtypes = [C.c_float, C.c_float, C.c_float, C.c_float, _ip, _fp, _fp, _ip, _fp, _fp]
+    L.fsg_batch_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(CLines), C.c_double,
+                                   C.POINTER(C.c_void_p)]
+    L.fsg_batch_tune.argtypes = [C.c_void_p, C.POINTER(BatchTuning)]
+    L.fsg_batch_set_tuning.argtypes = [C.c_void_p, C.POINTER(BatchTuning)]
+    L.fsg_batch_run.argtypes = [C.c_void_p, C.POINTER(BatchStats)]
+    L.fsg_batch_flux.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
+    L.fsg_batch_stream.argtypes = [C.c_void_p]
+    L.fsg_batch_stream.restype = C.c_void_p
+    L.fsg_batch_last_error.argtypes = [C.c_void_p]
+    L.fsg_batch_last_error.restype = C.c_char_p
+    L.fsg_batch_destroy.argtypes = [C.c_void_p]
+    L.fsg_batch_destroy.restype = None
     _lib = L
     return L
 
@@ -409,3 +440,59 @@ class Context:
                                          _p(src, C.c_double), _p(rhox, C.c_double), _p(out, C.c_double)),
                  "fsg_locprf_pp")
         return out
+
+
+class Batch:
+    """Batched synthesis (fsg_batch_*): many contexts (grid, atmosphere, continuum and mu set, mixed
+    precision) and one line list sorted by wavelength.  run() replays one CUDA graph of the whole
+    batch (tuned and captured on the first call); flux(i) reads atmosphere i's flux."""
+
+    def __init__(self, contexts, lines, margin=10.0):
+        self._lib = lib()
+        self.contexts = list(contexts)
+        self.lines = lines
+        hs = (C.c_void_p * len(self.contexts))(*[c.h.value for c in self.contexts])
+        h = C.c_void_p()
+        rc = self._lib.fsg_batch_create(hs, len(self.contexts), C.byref(lines.c), float(margin), C.byref(h))
+        if rc != 0:
+            raise FsgError("fsg_batch_create (%d): %s" % (rc, self._lib.fsg_batch_last_error(None).decode()))
+        self.h = h
+
+    def _ck(self, rc, what):
+        if rc != 0:
+            raise FsgError("%s (%d): %s" % (what, rc, self._lib.fsg_batch_last_error(self.h).decode()))
+
+    def tune(self):
+        t = BatchTuning()
+        self._ck(self._lib.fsg_batch_tune(self.h, C.byref(t)), "fsg_batch_tune")
+        return t.asdict()
+
+    def set_tuning(self, tuning):
+        t = BatchTuning(int(tuning["tile_pix"]), int(tuning["wing_ctas"]), int(tuning["core_ctas"]),
+                        float(tuning.get("ms_wing", 0.0)), float(tuning.get("ms_core", 0.0)))
+        self._ck(self._lib.fsg_batch_set_tuning(self.h, C.byref(t)), "fsg_batch_set_tuning")
+
+    def run(self):
+        st = BatchStats()
+        self._ck(self._lib.fsg_batch_run(self.h, C.byref(st)), "fsg_batch_run")
+        return st.asdict()
+
+    def flux(self, i):
+        n = self.contexts[i].nwl
+        sfl = np.zeros(n); sfc = np.zeros(n)
+        self._ck(self._lib.fsg_batch_flux(self.h, int(i), _p(sfl, C.c_double), _p(sfc, C.c_double)), "fsg_batch_flux")
+        return sfl, sfc
+
+    def stream_ptr(self):
+        return self._lib.fsg_batch_stream(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._lib.fsg_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -39,6 +39,13 @@ int fsg_launch_accum_fast(cudaStream_t, int, int, int, const double *, const Lin
 void fsg_launch_count_core(cudaStream_t, int64_t, const LineHdr *, unsigned long long *);
 int fsg_launch_core_fast(cudaStream_t, int, int, const double *, const LineHdr *, const WingRec *, const CoreRec *,
                          const int *, const int *, const float4 *, double *);
+struct WingJob { int ntau, nwl; const double *wave; const LineHdr *hdr; const WingRec *wing;
+                 const int *tile_lo, *tile_hi; double *lineopac; };
+struct CoreJob { int ntau, nwl; const double *wave; const LineHdr *hdr; const WingRec *wing; const CoreRec *core;
+                 const int *tile_lo, *tile_hi; double *lineopac; };
+int fsg_launch_accum_batch(cudaStream_t, int, int, const WingJob *, const int *, int, int, unsigned *, int *);
+int fsg_launch_core_batch(cudaStream_t, int, const CoreJob *, const int *, int, int, const float4 *, unsigned *);
+int fsg_class_pix(int);
 int fsg_fast_tiles(int);
 size_t fsg_tile_span_scratch(int64_t);
 size_t fsg_linstr_work(int64_t, int, int);
@@ -57,6 +64,7 @@ void fsg_launch_gather_lines(cudaStream_t, const LineView &, const int64_t *, in
 int fsg_select_wide(cudaStream_t, int64_t, const int32_t *, int *, int64_t *, int64_t *, int64_t *);
 void fsg_launch_scatter_flags(cudaStream_t, int64_t, const int64_t *, const int32_t *, int32_t *);
 double fsg_count_evals(fsg_ctx *, int64_t, const int32_t *, const int32_t *, const int32_t *, int, int);
+static double count_windows(fsg_ctx *, int64_t, const int32_t *, const int32_t *, const int32_t *, int, int);
 void fsg_launch_range_clip(cudaStream_t, int64_t, const int32_t *, const int32_t *, const int32_t *, int, int,
                            int32_t *, int32_t *, int32_t *);
 size_t fsg_stokes_smem(int, int);
@@ -174,6 +182,7 @@ int fsg_create(const fsg_config *cfg, fsg_ctx **out) {
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) { cudaGetLastError(); return FSG_E_CUDA; }
     if (cfg->device < 0 || cfg->device >= ndev) return FSG_E_ARG;
     if (cfg->precision != FSG_PREC_MIXED && cfg->precision != FSG_PREC_FP64) return FSG_E_ARG;
+    cudaGetLastError();                                 // an earlier caller's error is not this context's
     fsg_ctx *ctx = new fsg_ctx();
     ctx->cfg = *cfg;
     if (ctx->cfg.epsopac <= 0) ctx->cfg.epsopac = 1e-4;
@@ -1326,6 +1335,359 @@ int fsg_zeeman_pattern(float jlo, float jup, float glo, float gup, int32_t *npi,
     return FSG_OK;
 }
 
+
+// ================================================================================================
+// Batched synthesis: many atmospheres (each an fsg_ctx with grid, atmosphere, continuum and mu
+// set), one shared line list.  Per atmosphere: central pass and block refill of the lines in its
+// span (plus a margin), tile ranges; then ONE persistent wing-pass launch and ONE persistent
+// core-pass launch take (atmosphere, tile) items from device work queues; then the formal solver
+// and flux of each atmosphere.  The whole sequence has no host synchronisation and is captured
+// once as a CUDA graph; later runs replay it.  The tile width and the CTA counts of the persistent
+// launches are chosen by timing the candidates on the first run (fsg_batch_tune).
+// ================================================================================================
+static thread_local std::string g_batch_err;        // failure of the last fsg_batch_create on this thread
+
+struct BAtm {
+    fsg_ctx *ctx = nullptr;
+    int64_t c0 = 0, cn = 0;                    // candidate lines [c0, c0 + cn) of the shared list
+    DBuf flags, il, ir, wing, core, hdr, wtlo, wthi, ctlo, cthi, span, sfl, sfc;
+};
+
+struct fsg_batch {
+    fsg_ctx *own = nullptr;                    // stream, shared list, error text
+    std::vector<BAtm> atm;
+    fsg_lines dlines{};
+    int ntau_max = 0;
+    DBuf idx, jobs_w, jobs_c, tile0_w, tile0_c, queue, err, nk, evals;
+    fsg_batch_tuning tune{};
+    int tuned = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    double line_evals = 0.0;
+    cudaEvent_t ev[6] = { nullptr, nullptr, nullptr, nullptr, nullptr, nullptr };
+};
+
+static LineView batch_view(const fsg_batch *b, const BAtm &a) {
+    fsg_lines D = b->dlines;
+    D.n = a.cn;
+    D.wl += a.c0; D.elo += a.c0; D.gf += a.c0; D.grad += a.c0; D.gqst += a.c0; D.gvdw += a.c0; D.spc += a.c0;
+    if (D.ismol) D.ismol += a.c0;
+    if (D.ihe) D.ihe += a.c0;
+    return make_view(&D);
+}
+
+// the per-atmosphere stages up to the tile ranges (wing tiles of P wavelengths per lane)
+static int batch_prepare(fsg_batch *b, int P) {
+    fsg_ctx *ctx = b->own;
+    cudaStream_t s = ctx->stream;
+    for (auto &a : b->atm) {
+        if (a.cn == 0) continue;
+        fsg_ctx *c = a.ctx;
+        AtmView A = fsg_view(c);
+        LineView LV = batch_view(b, a);
+        fsg_launch_center(s, A, LV, c->tab, a.flags.as<int32_t>(), a.il.as<int32_t>(), a.ir.as<int32_t>(),
+                          b->nk.as<unsigned long long>());
+        fsg_launch_params_fast(s, A, LV, b->idx.as<int64_t>(), 0, a.cn, a.flags.as<int32_t>(), a.il.as<int32_t>(),
+                               a.ir.as<int32_t>(), c->tab, a.wing.as<WingRec>(), a.core.as<CoreRec>(),
+                               a.hdr.as<LineHdr>());
+        if (fsg_launch_tile_span(s, P == 2 ? 0 : 2, c->nwl, a.cn, a.hdr.as<LineHdr>(), a.wtlo.as<int>(),
+                                 a.wthi.as<int>(), a.span.p, a.span.cap) ||
+            fsg_launch_tile_span(s, -1, c->nwl, a.cn, a.hdr.as<LineHdr>(), a.ctlo.as<int>(), a.cthi.as<int>(),
+                                 a.span.p, a.span.cap))
+            return cuda_fail(ctx, cudaGetLastError(), "batch tile ranges");
+    }
+    CK(cudaGetLastError(), "batch prepare");
+    return FSG_OK;
+}
+
+// job tables and queue prefix sums for wing tiles of P wavelengths per lane (host, then uploaded)
+static int batch_jobs(fsg_batch *b, int P) {
+    fsg_ctx *ctx = b->own;
+    std::vector<WingJob> jw; std::vector<CoreJob> jc;
+    std::vector<int> tw(1, 0), tc(1, 0);
+    for (auto &a : b->atm) {
+        fsg_ctx *c = a.ctx;
+        if (a.cn == 0) continue;
+        jw.push_back(WingJob{ c->ntau, c->nwl, c->d_wave.as<double>(), a.hdr.as<LineHdr>(), a.wing.as<WingRec>(),
+                              a.wtlo.as<int>(), a.wthi.as<int>(), c->d_lineopac.as<double>() });
+        jc.push_back(CoreJob{ c->ntau, c->nwl, c->d_wave.as<double>(), a.hdr.as<LineHdr>(), a.wing.as<WingRec>(),
+                              a.core.as<CoreRec>(), a.ctlo.as<int>(), a.cthi.as<int>(), c->d_lineopac.as<double>() });
+        tw.push_back(tw.back() + (c->nwl + 32 * P - 1) / (32 * P));
+        tc.push_back(tc.back() + (c->nwl + 31) / 32);
+    }
+    ALLOC(b->jobs_w, sizeof(WingJob) * std::max<size_t>(jw.size(), 1));
+    ALLOC(b->jobs_c, sizeof(CoreJob) * std::max<size_t>(jc.size(), 1));
+    ALLOC(b->tile0_w, sizeof(int) * tw.size()); ALLOC(b->tile0_c, sizeof(int) * tc.size());
+    cudaStream_t s = ctx->stream;
+    if (!jw.empty()) {
+        CK(cudaMemcpyAsync(b->jobs_w.p, jw.data(), sizeof(WingJob) * jw.size(), cudaMemcpyHostToDevice, s), "jobs");
+        CK(cudaMemcpyAsync(b->jobs_c.p, jc.data(), sizeof(CoreJob) * jc.size(), cudaMemcpyHostToDevice, s), "jobs");
+    }
+    CK(cudaMemcpyAsync(b->tile0_w.p, tw.data(), sizeof(int) * tw.size(), cudaMemcpyHostToDevice, s), "jobs");
+    CK(cudaMemcpyAsync(b->tile0_c.p, tc.data(), sizeof(int) * tc.size(), cudaMemcpyHostToDevice, s), "jobs");
+    CK(cudaStreamSynchronize(s), "jobs");
+    return FSG_OK;
+}
+
+// accumulation (zeroed LineOpac, the two persistent launches), then solver and flux per atmosphere;
+// ev: optional events around the wing and core launches
+static int batch_accumulate_solve(fsg_batch *b, const fsg_batch_tuning &t, cudaEvent_t *ev) {
+    fsg_ctx *ctx = b->own;
+    cudaStream_t s = ctx->stream;
+    int njobs = 0;
+    for (auto &a : b->atm) {
+        fsg_ctx *c = a.ctx;
+        CK(cudaMemsetAsync(c->d_lineopac.p, 0, sizeof(double) * (size_t)c->nwl * c->ntau, s), "batch reset");
+        if (a.cn) njobs++;
+    }
+    CK(cudaMemsetAsync(b->queue.p, 0, 2 * sizeof(unsigned), s), "queue reset");
+    if (njobs) {
+        if (ev) cudaEventRecord(ev[0], s);
+        if (fsg_launch_accum_batch(s, t.tile_pix / 32, b->ntau_max, b->jobs_w.as<WingJob>(), b->tile0_w.as<int>(),
+                                   njobs, t.wing_ctas, b->queue.as<unsigned>(), b->err.as<int>()))
+            return cuda_fail(ctx, cudaGetLastError(), "k_accum_batch");
+        if (ev) cudaEventRecord(ev[1], s);
+        if (fsg_launch_core_batch(s, b->ntau_max, b->jobs_c.as<CoreJob>(), b->tile0_c.as<int>(), njobs, t.core_ctas,
+                                  b->atm[0].ctx->tab.vtab4, b->queue.as<unsigned>() + 1))
+            return cuda_fail(ctx, cudaGetLastError(), "k_core_batch");
+        if (ev) cudaEventRecord(ev[2], s);
+    }
+    for (auto &a : b->atm) {
+        fsg_ctx *c = a.ctx;
+        if (fsg_launch_radtran(s, fsg_view(c), c->d_lineopac.as<double>(), c->d_rhox.as<double>(), c->nmu,
+                               c->d_xmu.as<double>(), c->d_wmu.as<double>(), nullptr, nullptr, a.sfl.as<double>(),
+                               a.sfc.as<double>()))
+            return cuda_fail(ctx, cudaGetLastError(), "k_radtran (batch)");
+    }
+    CK(cudaGetLastError(), "batch");
+    return FSG_OK;
+}
+
+int fsg_batch_create(fsg_ctx *const *atms, int natm, const fsg_lines *lines, double margin, fsg_batch **out) {
+    if (!atms || natm < 1 || !lines || !out || margin < 0) return FSG_E_ARG;
+    *out = nullptr;
+    fsg_config cfg = atms[0]->cfg;
+    fsg_batch *b = new fsg_batch();
+    int rc = fsg_create(&cfg, &b->own);
+    if (rc) { delete b; g_batch_err = "fsg_batch_create: context creation failed"; return rc; }
+    fsg_ctx *ctx = b->own;
+    auto bail = [&](int code, const char *m) {
+        g_batch_err = m ? m : ctx->err;
+        fsg_batch_destroy(b);
+        return code;
+    };
+    for (int i = 0; i < natm; i++) {
+        fsg_ctx *c = atms[i];
+        if (!c || c->device != ctx->device) return bail(FSG_E_ARG, "fsg_batch_create: contexts must share one device");
+        if (c->cfg.precision != FSG_PREC_MIXED) return bail(FSG_E_STATE, "fsg_batch_create: mixed precision only");
+        if (!c->have_grid || !c->have_atm || !c->have_cont || c->nmu < 1)
+            return bail(FSG_E_STATE, "fsg_batch_create: set grid, atmosphere, continuum and mu of every context");
+        if (c->ntau > 128) return bail(FSG_E_ARG, "fsg_batch_create: ntau <= 128");
+    }
+    rc = check_lines(atms[0], lines); if (rc) return bail(rc, atms[0]->err.c_str());
+    int nspc_min = atms[0]->nspc;
+    for (int i = 1; i < natm; i++) nspc_min = std::min(nspc_min, atms[i]->nspc);
+    for (int64_t i = 0; i < lines->n; i++) {
+        if (i > 0 && lines->wl[i] < lines->wl[i - 1])
+            return bail(FSG_E_ARG, "fsg_batch_create: the line list must be sorted by wavelength");
+        if (lines->spc[i] < 0 || lines->spc[i] >= nspc_min)
+            return bail(FSG_E_ARG, "fsg_batch_create: a species index is outside some atmosphere's species");
+    }
+    cudaSetDevice(ctx->device);
+    if (lines->n > 0) { rc = upload_lines(ctx, lines, &b->dlines); if (rc) return bail(rc, nullptr); }
+    int64_t cmax = 0;
+    b->atm.resize(natm);
+    for (int i = 0; i < natm; i++) {
+        BAtm &a = b->atm[i];
+        fsg_ctx *c = atms[i];
+        a.ctx = c;
+        b->ntau_max = std::max(b->ntau_max, c->ntau);
+        // candidates: lines with centres in [first wavelength - margin, last wavelength + margin]
+        double w0 = c->wstart - margin, w1 = c->wend + margin;
+        const double *wl = lines->wl;
+        a.c0 = std::lower_bound(wl, wl + lines->n, w0) - wl;
+        a.cn = (std::upper_bound(wl, wl + lines->n, w1) - wl) - a.c0;
+        cmax = std::max(cmax, a.cn);
+        int rca = ensure_lineopac(c); if (rca) return bail(rca, c->err.c_str());
+        size_t nt = c->ntau, cn = std::max<int64_t>(a.cn, 1);
+        if (a.flags.ensure(4 * cn) || a.il.ensure(4 * cn) || a.ir.ensure(4 * cn) ||
+            a.wing.ensure(sizeof(WingRec) * cn * nt) || a.core.ensure(sizeof(CoreRec) * cn * nt) ||
+            a.hdr.ensure(sizeof(LineHdr) * cn) || a.wtlo.ensure(4 * (size_t)fsg_fast_tiles(c->nwl)) ||
+            a.wthi.ensure(4 * (size_t)fsg_fast_tiles(c->nwl)) || a.ctlo.ensure(4 * (size_t)fsg_fast_tiles(c->nwl)) ||
+            a.cthi.ensure(4 * (size_t)fsg_fast_tiles(c->nwl)) || a.span.ensure(fsg_tile_span_scratch(cn)) ||
+            a.sfl.ensure(8 * (size_t)c->nwl) || a.sfc.ensure(8 * (size_t)c->nwl))
+            return bail(FSG_E_NOMEM, "fsg_batch_create: device allocation failed");
+    }
+    std::vector<int64_t> iota(std::max<int64_t>(cmax, 1));
+    for (int64_t i = 0; i < (int64_t)iota.size(); i++) iota[i] = i;
+    if (b->idx.ensure(sizeof(int64_t) * iota.size()) || b->queue.ensure(2 * sizeof(unsigned)) ||
+        b->err.ensure(sizeof(int)) || b->nk.ensure(sizeof(unsigned long long)))
+        return bail(FSG_E_NOMEM, "fsg_batch_create: device allocation failed");
+    if (cudaMemcpy(b->idx.p, iota.data(), sizeof(int64_t) * iota.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemset(b->err.p, 0, sizeof(int)) != cudaSuccess)
+        return bail(FSG_E_CUDA, "fsg_batch_create: upload failed");
+    for (int i = 0; i < 6; i++) cudaEventCreate(&b->ev[i]);
+    b->tune.tile_pix = 128;
+    b->tune.wing_ctas = 148;
+    b->tune.core_ctas = 4 * 148;
+    int nsm = 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device) == cudaSuccess && nsm > 0) {
+        b->tune.wing_ctas = nsm;
+        b->tune.core_ctas = 4 * nsm;
+    }
+    *out = b;
+    return FSG_OK;
+}
+
+const char *fsg_batch_last_error(const fsg_batch *b) { return b ? b->own->err.c_str() : g_batch_err.c_str(); }
+
+// windows and line evaluations of the batch (after a prepare): counted once, outside the graph
+static int batch_count(fsg_batch *b) {
+    fsg_ctx *ctx = b->own;
+    double ev = 0;
+    for (auto &a : b->atm) {
+        if (!a.cn) continue;
+        ev += count_windows(ctx, a.cn, a.flags.as<int32_t>(), a.il.as<int32_t>(), a.ir.as<int32_t>(), 1, a.ctx->nwl) *
+              a.ctx->ntau;
+    }
+    b->line_evals = ev;
+    return FSG_OK;
+}
+
+int fsg_batch_tune(fsg_batch *b, fsg_batch_tuning *result) {
+    if (!b) return FSG_E_ARG;
+    fsg_ctx *ctx = b->own;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
+    // (1) wing pass: tile width x CTAs per SM, core pass at 4 CTAs per SM; (2) core pass CTAs
+    fsg_batch_tuning best{ 128, nsm, 4 * nsm, 1e300, 1e300 };
+    const int pix[2] = { 64, 128 };
+    auto trial = [&](const fsg_batch_tuning &t, float *mw, float *mc) -> int {
+        int rc2 = batch_accumulate_solve(b, t, b->ev); if (rc2) return rc2;
+        CK(cudaStreamSynchronize(s), "batch tune");
+        cudaEventElapsedTime(mw, b->ev[0], b->ev[1]);
+        cudaEventElapsedTime(mc, b->ev[1], b->ev[2]);
+        return FSG_OK;
+    };
+    for (int ip = 0; ip < 2; ip++) {
+        int rc = batch_prepare(b, pix[ip] / 32); if (rc) return rc;
+        rc = batch_jobs(b, pix[ip] / 32); if (rc) return rc;
+        for (int wm = 1; wm <= 2; wm++) {
+            fsg_batch_tuning t{ pix[ip], wm * nsm, 4 * nsm, 0.0, 0.0 };
+            float mw = 0, mc = 0;
+            rc = trial(t, &mw, &mc); if (rc) return rc;
+            if (mw < best.ms_wing) { best.tile_pix = t.tile_pix; best.wing_ctas = t.wing_ctas; best.ms_wing = mw; }
+        }
+    }
+    int rc = batch_prepare(b, best.tile_pix / 32); if (rc) return rc;
+    rc = batch_jobs(b, best.tile_pix / 32); if (rc) return rc;
+    for (int cm = 2; cm <= 8; cm *= 2) {
+        fsg_batch_tuning t = best;
+        t.core_ctas = cm * nsm;
+        float mw = 0, mc = 0;
+        rc = trial(t, &mw, &mc); if (rc) return rc;
+        if (mc < best.ms_core) { best.core_ctas = t.core_ctas; best.ms_core = mc; }
+    }
+    int kerr = 0;
+    CK(cudaMemcpy(&kerr, b->err.p, sizeof(int), cudaMemcpyDeviceToHost), "batch err");
+    if (kerr) return fail(ctx, FSG_E_TIMEOUT, "k_accum_batch: a line-record copy did not complete within its bound");
+    b->tune = best;
+    b->tuned = 1;
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    if (result) *result = best;
+    return FSG_OK;
+}
+
+int fsg_batch_set_tuning(fsg_batch *b, const fsg_batch_tuning *t) {
+    if (!b || !t || (t->tile_pix != 64 && t->tile_pix != 128) || t->wing_ctas < 1 || t->core_ctas < 1)
+        return FSG_E_ARG;
+    b->tune = *t;
+    b->tuned = 1;
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+    if (b->graph) { cudaGraphDestroy(b->graph); b->graph = nullptr; }
+    return FSG_OK;
+}
+
+int fsg_batch_run(fsg_batch *b, fsg_batch_stats *st) {
+    if (!b) return FSG_E_ARG;
+    fsg_ctx *ctx = b->own;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    int rc;
+    if (!b->tuned) { rc = fsg_batch_tune(b, nullptr); if (rc) return rc; }
+    if (!b->exec) {
+        const int P = b->tune.tile_pix / 32;
+        rc = batch_jobs(b, P); if (rc) return rc;
+        rc = batch_prepare(b, P); if (rc) return rc;   // outside the graph once: counts and attributes
+        CK(cudaStreamSynchronize(s), "batch");
+        batch_count(b);
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture");
+        rc = batch_prepare(b, P);
+        if (!rc) rc = batch_accumulate_solve(b, b->tune, nullptr);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(s, &g);
+        if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "graph capture");
+        b->graph = g;
+        CK(cudaGraphInstantiate(&b->exec, g, 0), "graph instantiate");
+    }
+    CK(cudaEventRecord(b->ev[3], s), "event");
+    CK(cudaGraphLaunch(b->exec, s), "graph launch");
+    CK(cudaEventRecord(b->ev[4], s), "event");
+    CK(cudaStreamSynchronize(s), "batch run");
+    int kerr = 0;
+    CK(cudaMemcpy(&kerr, b->err.p, sizeof(int), cudaMemcpyDeviceToHost), "batch err");
+    if (kerr) return fail(ctx, FSG_E_TIMEOUT, "k_accum_batch: a line-record copy did not complete within its bound");
+    if (st) {
+        memset(st, 0, sizeof *st);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, b->ev[3], b->ev[4]);
+        st->ms_total = ms;
+        st->line_evals = b->line_evals;
+        for (auto &a : b->atm) st->nlines_candidate += a.cn;
+        st->natm = (int)b->atm.size();
+        st->tuning = b->tune;
+    }
+    return FSG_OK;
+}
+
+int fsg_batch_flux(fsg_batch *b, int iatm, double *sfl, double *sfc) {
+    if (!b || iatm < 0 || iatm >= (int)b->atm.size()) return FSG_E_ARG;
+    fsg_ctx *ctx = b->own;
+    cudaSetDevice(ctx->device);
+    BAtm &a = b->atm[iatm];
+    size_t nb = sizeof(double) * (size_t)a.ctx->nwl;
+    if (sfl) CK(cudaMemcpyAsync(sfl, a.sfl.p, nb, cudaMemcpyDeviceToHost, ctx->stream), "batch flux");
+    if (sfc) CK(cudaMemcpyAsync(sfc, a.sfc.p, nb, cudaMemcpyDeviceToHost, ctx->stream), "batch flux");
+    CK(cudaStreamSynchronize(ctx->stream), "batch flux");
+    return FSG_OK;
+}
+
+void *fsg_batch_stream(fsg_batch *b) { return b ? (void *)b->own->stream : nullptr; }
+
+void fsg_batch_destroy(fsg_batch *b) {
+    if (!b) return;
+    cudaSetDevice(b->own->device);
+    cudaStreamSynchronize(b->own->stream);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (auto &a : b->atm) {
+        DBuf *bufs[] = { &a.flags, &a.il, &a.ir, &a.wing, &a.core, &a.hdr, &a.wtlo, &a.wthi, &a.ctlo, &a.cthi,
+                         &a.span, &a.sfl, &a.sfc };
+        for (DBuf *d : bufs) d->release();
+    }
+    DBuf *bufs[] = { &b->idx, &b->jobs_w, &b->jobs_c, &b->tile0_w, &b->tile0_c, &b->queue, &b->err, &b->nk,
+                     &b->evals };
+    for (DBuf *d : bufs) d->release();
+    for (int i = 0; i < 6; i++) if (b->ev[i]) cudaEventDestroy(b->ev[i]);
+    fsg_destroy(b->own);
+    cudaGetLastError();
+    delete b;
+}
+
 }  // extern "C"
 
 // ---- eval counting for the stats (sum over retained lines of Ntau x window) -------------------------
@@ -1343,6 +1705,13 @@ __global__ void k_count_evals(int64_t n, const int32_t *flags, const int32_t *il
 
 double fsg_count_evals(fsg_ctx *ctx, int64_t n, const int32_t *fl, const int32_t *il, const int32_t *ir, int i0,
                        int i1) {
+    return count_windows(ctx, n, fl, il, ir, i0, i1) * ctx->ntau;
+}
+
+// retained-window wavelengths (inside [i0, i1]) of n lines
+static double count_windows(fsg_ctx *ctx, int64_t n, const int32_t *fl, const int32_t *il, const int32_t *ir, int i0,
+                            int i1) {
+    if (ctx->d_nkeep.ensure(sizeof(unsigned long long)) != FSG_OK) return 0.0;
     ctx->launches += 1;
     unsigned long long *d = ctx->d_nkeep.as<unsigned long long>();
     cudaMemsetAsync(d, 0, sizeof(unsigned long long), ctx->stream);
@@ -1350,5 +1719,5 @@ double fsg_count_evals(fsg_ctx *ctx, int64_t n, const int32_t *fl, const int32_t
     unsigned long long h = 0;
     cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, ctx->stream);
     cudaStreamSynchronize(ctx->stream);
-    return (double)h * ctx->ntau;
+    return (double)h;
 }

@@ -122,36 +122,51 @@ __device__ __forceinline__ float rcp_approx(float x) {
 //   val = c1 (t + 1) / (t^2 + twoA),  t = dl^2 vv2 + c2m1
 // (three FMAs, one reciprocal, one FMA into the partial sum).  Lines whose window covers the
 // whole tile outside their core range (the common case for wide windows) skip the mask.
+// One wing-pass job: the line records and tiles of one LineOpac (one atmosphere and grid).
+struct WingJob {
+    int ntau, nwl;
+    const double *wave;
+    const LineHdr *hdr;
+    const WingRec *wing;
+    const int *tile_lo, *tile_hi;
+    double *lineopac;
+};
+
+// shared memory of the wing pass for at most ntau_max depths:
+// wing records [2][CH][ntau_max] | headers [2][CH] | mbarriers [2] | Kahan pairs [D * P][blockDim.x]
+__host__ __device__ inline size_t wing_smem_recs(int ntau_max) {
+    return sizeof(WingRec) * 2 * CH * (size_t)ntau_max + sizeof(LineHdr) * 2 * CH;
+}
+
+// One tile of one job.  Called by every thread of the CTA with the mbarriers initialised; kk counts
+// the chunks the CTA has consumed so far (their buffer and phase parity), across tiles.  Returns
+// false after a copy did not complete within its bound (error reported in *err).
 template <int D, int P>
-__global__ void __launch_bounds__(32 * 18, 1)
-k_accum_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *__restrict__ hdr,
-             const WingRec *__restrict__ wing, const int *__restrict__ tile_lo, const int *__restrict__ tile_hi,
-             double *__restrict__ lineopac, int *__restrict__ err) {
-    // shared memory: wing records [2][CH][ntau] | headers [2][CH] | mbarriers [2] | Kahan pairs
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+__device__ __forceinline__ bool wing_tile(const WingJob &J, int tile, unsigned char *smem_raw, int ntau_max,
+                                          unsigned &kk, int *err) {
+    const int ntau = J.ntau, nwl = J.nwl;
+    const double *__restrict__ wave = J.wave;
+    const LineHdr *__restrict__ hdr = J.hdr;
+    const WingRec *__restrict__ wing = J.wing;
     WingRec *swing = (WingRec *)smem_raw;
-    LineHdr *shdr = (LineHdr *)(swing + 2 * CH * ntau);
+    LineHdr *shdr = (LineHdr *)(swing + 2 * CH * ntau_max);
     uint64_t *bars = (uint64_t *)(shdr + 2 * CH);
     float2 *ksum = (float2 *)(bars + 2);                 // [D * P][blockDim.x]
     constexpr int TW = 32 * P;
-    const int tile = blockIdx.x;
-    const int lo = tile_lo[tile], hi = tile_hi[tile];
-    if (lo > hi) return;
+    const int lo = J.tile_lo[tile], hi = J.tile_hi[tile];
+    if (lo > hi) return true;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int t0 = warp * D;
     const int nd = max(0, min(D, ntau - t0));            // warps past the last depth only help staging
     const int p0 = tile * TW;
     const int nth = blockDim.x;
     const int nchunks = (hi - lo + CH) / CH;
+    // chunk c of this tile is the CTA's chunk g = kk + c: buffer g & 1, phase parity (g >> 1) & 1
     if (threadIdx.x == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        stage_chunk(0, lo, hi, ntau, hdr, wing, shdr, swing, &bars[0]);
-        if (nchunks > 1) stage_chunk(1, lo, hi, ntau, hdr, wing, shdr + CH, swing + CH * ntau, &bars[1]);
+        for (int c = 0; c < 2 && c < nchunks; c++) {
+            const int b = (kk + c) & 1;
+            stage_chunk(c, lo, hi, ntau, hdr, wing, shdr + b * CH, swing + b * CH * ntau_max, &bars[b]);
+        }
     }
     // wavelength offsets as FP32 hi + lo: dl = (wvh - wlh) + (wvl - wll) keeps dl to FP32 relative
     // accuracy next to the line centre
@@ -176,11 +191,12 @@ k_accum_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *
     const int tile_first = p0 + 1, tile_last = min(p0 + TW, nwl);
     int failed = -1;                                     // chunk whose copy did not complete
     for (int c = 0; c < nchunks; c++) {
-        const int b = c & 1;
-        const bool ok = mbar_wait(&bars[b], (unsigned)((c >> 1) & 1));
+        const unsigned g = kk + c;
+        const int b = g & 1;
+        const bool ok = mbar_wait(&bars[b], (g >> 1) & 1);
         if (__syncthreads_or(!ok)) { failed = c; break; }
         const LineHdr *ch = shdr + b * CH;
-        const WingRec *cw = swing + b * CH * ntau;
+        const WingRec *cw = swing + b * CH * ntau_max;
         const int n = min(CH, hi - (lo + c * CH) + 1);
         if (nd > 0) {
             for (int q = 0; q < n; q++) {
@@ -242,23 +258,27 @@ k_accum_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *
         }
         __syncthreads();                                   // every warp is done with buffer b
         if (threadIdx.x == 0 && c + 2 < nchunks)
-            stage_chunk(c + 2, lo, hi, ntau, hdr, wing, shdr + b * CH, swing + b * CH * ntau, &bars[b]);
+            stage_chunk(c + 2, lo, hi, ntau, hdr, wing, shdr + b * CH, swing + b * CH * ntau_max, &bars[b]);
     }
     if (failed >= 0) {
         // a copy never completed: report, then wait (bounded) for the copies still in flight,
         // chunks failed and failed + 1, before the CTA's shared memory is released
         if (threadIdx.x == 0) {
             atomicExch(err, FSG_E_TIMEOUT);
-            for (int c = failed; c < nchunks && c < failed + 2; c++) mbar_wait(&bars[c & 1], (unsigned)((c >> 1) & 1));
+            for (int c = failed; c < nchunks && c < failed + 2; c++) {
+                const unsigned g = kk + c;
+                mbar_wait(&bars[g & 1], (g >> 1) & 1);
+            }
         }
         __syncthreads();
-        return;
+        return false;
     }
-    if (nd <= 0) return;
+    kk += nchunks;
+    if (nd <= 0) return true;
 #pragma unroll
     for (int k = 0; k < P; k++) {
         if (pix[k] >= nwl) continue;
-        double *dst = lineopac + (size_t)pix[k] * ntau + t0;
+        double *dst = J.lineopac + (size_t)pix[k] * ntau + t0;
 #pragma unroll
         for (int d = 0; d < D; d++) {
             float2 sc = ksum[(d * P + k) * nth + threadIdx.x];
@@ -266,39 +286,106 @@ k_accum_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *
             if (d < nd) dst[d] = dst[d] + ((double)sc.x - (double)sc.y);
         }
     }
+    return true;
+}
+
+__device__ __forceinline__ void wing_bars_init(unsigned char *smem_raw, int ntau_max) {
+    uint64_t *bars = (uint64_t *)(smem_raw + wing_smem_recs(ntau_max));
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+}
+
+// one tile per CTA (blockIdx.x)
+template <int D, int P>
+__global__ void __launch_bounds__(32 * 18, 1)
+k_accum_fast(WingJob J, int *__restrict__ err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    if (J.tile_lo[blockIdx.x] > J.tile_hi[blockIdx.x]) return;
+    wing_bars_init(smem_raw, J.ntau);
+    unsigned kk = 0;
+    wing_tile<D, P>(J, blockIdx.x, smem_raw, J.ntau, kk, err);
+}
+
+// Persistent form for many jobs (batched atmospheres): CTAs take (job, tile) items from a device
+// work queue (*queue, zero at launch) until jobs[njobs - 1] is done; tile0[j] is the first item of
+// job j (prefix sums of the jobs' tile counts, tile0[njobs] = total).
+template <int D, int P>
+__global__ void __launch_bounds__(32 * 18, 1)
+k_accum_batch(const WingJob *__restrict__ jobs, const int *__restrict__ tile0, int njobs, int ntau_max,
+              unsigned *queue, int *__restrict__ err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ int s_item;
+    wing_bars_init(smem_raw, ntau_max);
+    unsigned kk = 0;
+    const int total = tile0[njobs];
+    for (;;) {
+        if (threadIdx.x == 0) s_item = (int)atomicAdd(queue, 1u);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= total) break;
+        int a = 0, b = njobs - 1;                          // job with tile0[a] <= item < tile0[a + 1]
+        while (a < b) { int m = (a + b + 1) >> 1; if (tile0[m] <= item) a = m; else b = m - 1; }
+        const WingJob J = jobs[a];
+        if (!wing_tile<D, P>(J, item - tile0[a], smem_raw, ntau_max, kk, err)) break;
+    }
 }
 
 // Tile width per window-width class: narrow windows get narrower tiles so fewer lanes idle.
 int fsg_class_pix(int cls) { return cls <= 1 ? 2 : 4; }
+
+// depths per warp for P wavelengths per lane: P x D = 16 evaluations per thread and line, at most
+// 18 warps per CTA
+static int wing_depths(int P, int ntau) {
+    int D = 16 / P;
+    if ((ntau + D - 1) / D > 18) D = (ntau + 17) / 18;
+    return D;
+}
+
+size_t fsg_wing_smem(int P, int ntau_max) {
+    const int D = wing_depths(P, ntau_max), nwarps = (ntau_max + D - 1) / D;
+    return wing_smem_recs(ntau_max) + 2 * sizeof(uint64_t) + sizeof(float2) * (size_t)D * P * 32 * nwarps;
+}
+
+#define WING_DISPATCH(P, D, LAUNCH) do { \
+        if (P == 2) { if (D == 8) LAUNCH(8, 2); else return FSG_E_ARG; } \
+        else switch (D) { case 4: LAUNCH(4, 4); break; case 5: LAUNCH(5, 4); break; case 6: LAUNCH(6, 4); break; \
+                          case 7: LAUNCH(7, 4); break; case 8: LAUNCH(8, 4); break; default: return FSG_E_ARG; } \
+    } while (0)
 
 int fsg_launch_accum_fast(cudaStream_t st, int cls, int ntau, int nwl, const double *wave, const LineHdr *hdr,
                           const WingRec *wing, const int *tile_lo, const int *tile_hi, double *lineopac, int *err) {
     const int P = fsg_class_pix(cls);
     const int TW = 32 * P;
     const int ntiles = (nwl + TW - 1) / TW;
-    // depths per warp: P x D = 16 evaluations per thread and line, at most 18 warps per CTA
-    int D = 16 / P;
-    if ((ntau + D - 1) / D > 18) D = (ntau + 17) / 18;
-    int nwarps = (ntau + D - 1) / D;
-    const size_t smem = sizeof(WingRec) * 2 * CH * (size_t)ntau + sizeof(LineHdr) * 2 * CH + 2 * sizeof(uint64_t) +
-                        sizeof(float2) * (size_t)D * P * 32 * nwarps;
+    const int D = wing_depths(P, ntau);
+    const int nwarps = (ntau + D - 1) / D;
+    const size_t smem = fsg_wing_smem(P, ntau);
     if (smem > 200 * 1024) return FSG_E_ARG;
+    WingJob J{ ntau, nwl, wave, hdr, wing, tile_lo, tile_hi, lineopac };
 #define LAUNCH(DD, PP) do { \
         cudaFuncSetAttribute(k_accum_fast<DD, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-        k_accum_fast<DD, PP><<<ntiles, 32 * nwarps, smem, st>>>(ntau, nwl, wave, hdr, wing, tile_lo, tile_hi, \
-                                                                 lineopac, err); } while (0)
-    if (P == 2) {
-        if (D == 8) LAUNCH(8, 2); else return FSG_E_ARG;
-    } else {
-        switch (D) {
-            case 4: LAUNCH(4, 4); break;
-            case 5: LAUNCH(5, 4); break;
-            case 6: LAUNCH(6, 4); break;
-            case 7: LAUNCH(7, 4); break;
-            case 8: LAUNCH(8, 4); break;
-            default: return FSG_E_ARG;
-        }
-    }
+        k_accum_fast<DD, PP><<<ntiles, 32 * nwarps, smem, st>>>(J, err); } while (0)
+    WING_DISPATCH(P, D, LAUNCH);
+#undef LAUNCH
+    return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
+}
+
+// the persistent wing pass over njobs jobs (device array), P wavelengths per lane, ctas CTAs
+int fsg_launch_accum_batch(cudaStream_t st, int P, int ntau_max, const WingJob *jobs, const int *tile0, int njobs,
+                           int ctas, unsigned *queue, int *err) {
+    const int D = wing_depths(P, ntau_max);
+    const int nwarps = (ntau_max + D - 1) / D;
+    const size_t smem = fsg_wing_smem(P, ntau_max);
+    if (smem > 200 * 1024) return FSG_E_ARG;
+#define LAUNCH(DD, PP) do { \
+        cudaFuncSetAttribute(k_accum_batch<DD, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+        k_accum_batch<DD, PP><<<ctas, 32 * nwarps, smem, st>>>(jobs, tile0, njobs, ntau_max, queue, err); } while (0)
+    WING_DISPATCH(P, D, LAUNCH);
 #undef LAUNCH
     return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
 }
@@ -322,31 +409,40 @@ __device__ __forceinline__ float hv_core32(const float4 *__restrict__ vtab4, flo
     return hv_cf32(av, sqrtf(0.5f * twoA), c.cop);
 }
 
-__global__ void __launch_bounds__(512)
-k_core_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *__restrict__ hdr,
-            const WingRec *__restrict__ wing, const CoreRec *__restrict__ core, const int *__restrict__ tile_lo,
-            const int *__restrict__ tile_hi, const float4 *__restrict__ vtab4, double *__restrict__ lineopac) {
-    const int tile = blockIdx.x;
-    const int lo = tile_lo[tile], hi = tile_hi[tile];
+// One core-pass job: as WingJob plus the core records; tiles of 32 wavelengths
+struct CoreJob {
+    int ntau, nwl;
+    const double *wave;
+    const LineHdr *hdr;
+    const WingRec *wing;
+    const CoreRec *core;
+    const int *tile_lo, *tile_hi;
+    double *lineopac;
+};
+
+__device__ __forceinline__ void core_tile(const CoreJob &J, int tile, const float4 *__restrict__ vtab4) {
+    const int ntau = J.ntau, nwl = J.nwl;
+    const int lo = J.tile_lo[tile], hi = J.tile_hi[tile];
     if (lo > hi) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int t0 = warp * CORE_D;
-    const int nd = min(CORE_D, ntau - t0);               // >= 1: blockDim.x / 32 = ceil(ntau / CORE_D)
+    const int nd = min(CORE_D, ntau - t0);
+    if (nd <= 0) return;                                 // no barrier below: warps may leave early
     const int p = tile * 32 + lane, p1 = p + 1;
     const int tile_first = tile * 32 + 1, tile_last = min(tile * 32 + 32, nwl);
-    const double wd = wave[min(p, nwl - 1)];
+    const double wd = J.wave[min(p, nwl - 1)];
     const float wvh = (float)wd, wvl = (float)(wd - (double)wvh);
     float sum[CORE_D], cmp[CORE_D];
 #pragma unroll
     for (int d = 0; d < CORE_D; d++) { sum[d] = 0.0f; cmp[d] = 0.0f; }
     for (int j = lo; j <= hi; j++) {
-        const LineHdr h = hdr[j];
+        const LineHdr h = J.hdr[j];
         if (h.cr < tile_first || h.cl > tile_last) continue;          // core range misses the tile
         if (p1 < h.cl || p1 > h.cr) continue;
         const float dl = (wvh - h.wlh) + (wvl - h.wll);
         const float x = dl * dl, adl = fabsf(dl);
-        const WingRec *wr = wing + (size_t)j * ntau + t0;
-        const CoreRec *cr = core + (size_t)j * ntau + t0;
+        const WingRec *wr = J.wing + (size_t)j * ntau + t0;
+        const CoreRec *cr = J.core + (size_t)j * ntau + t0;
 #pragma unroll
         for (int d = 0; d < CORE_D; d++) {
             if (d < nd) {
@@ -364,10 +460,34 @@ k_core_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *_
         }
     }
     if (p >= nwl) return;
-    double *dst = lineopac + (size_t)p * ntau + t0;
+    double *dst = J.lineopac + (size_t)p * ntau + t0;
 #pragma unroll
     for (int d = 0; d < CORE_D; d++)
         if (d < nd) dst[d] = dst[d] + ((double)sum[d] - (double)cmp[d]);
+}
+
+__global__ void __launch_bounds__(512)
+k_core_fast(CoreJob J, const float4 *__restrict__ vtab4) {
+    core_tile(J, blockIdx.x, vtab4);
+}
+
+// persistent form: each warp takes (job, tile) items from the queue and does its depths of them;
+// a CTA of nwarps warps covers nwarps * CORE_D depths, so every item is taken by whole CTAs
+__global__ void __launch_bounds__(512)
+k_core_batch(const CoreJob *__restrict__ jobs, const int *__restrict__ tile0, int njobs,
+             const float4 *__restrict__ vtab4, unsigned *queue) {
+    __shared__ int s_item;
+    const int total = tile0[njobs];
+    for (;;) {
+        if (threadIdx.x == 0) s_item = (int)atomicAdd(queue, 1u);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= total) break;
+        int a = 0, b = njobs - 1;
+        while (a < b) { int m = (a + b + 1) >> 1; if (tile0[m] <= item) a = m; else b = m - 1; }
+        core_tile(jobs[a], item - tile0[a], vtab4);
+    }
 }
 
 int fsg_launch_core_fast(cudaStream_t st, int ntau, int nwl, const double *wave, const LineHdr *hdr,
@@ -375,7 +495,15 @@ int fsg_launch_core_fast(cudaStream_t st, int ntau, int nwl, const double *wave,
                          const float4 *vtab4, double *lineopac) {
     const int ntiles = (nwl + 31) / 32;
     const int nwarps = (ntau + CORE_D - 1) / CORE_D;     // ntau <= 128: at most 16 warps
-    k_core_fast<<<ntiles, 32 * nwarps, 0, st>>>(ntau, nwl, wave, hdr, wing, core, tile_lo, tile_hi, vtab4, lineopac);
+    CoreJob J{ ntau, nwl, wave, hdr, wing, core, tile_lo, tile_hi, lineopac };
+    k_core_fast<<<ntiles, 32 * nwarps, 0, st>>>(J, vtab4);
+    return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
+}
+
+int fsg_launch_core_batch(cudaStream_t st, int ntau_max, const CoreJob *jobs, const int *tile0, int njobs,
+                          int ctas, const float4 *vtab4, unsigned *queue) {
+    const int nwarps = (ntau_max + CORE_D - 1) / CORE_D;
+    k_core_batch<<<ctas, 32 * nwarps, 0, st>>>(jobs, tile0, njobs, vtab4, queue);
     return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
 }
 

@@ -294,7 +294,8 @@ __global__ void k_params_fast(AtmView A, LineView L, const int64_t *__restrict__
     h.wll = (float)(wlc - (double)h.wlh);
     h.ileft = ileft[i]; h.iright = iright[i];
     h.cl = 1; h.cr = 0;
-    if (hcore >= 0.0) {
+    if (f & FSG_F_WEAK) { h.ileft = 1; h.iright = 0; }    // rejected line (batched lists): empty window
+    else if (hcore >= 0.0) {
         // 1-based indices of the first wavelength >= wlc - hcore and the last <= wlc + hcore,
         // widened by one wavelength and clipped to the window
         int a = lower_index(A.wave, A.nwl, wlc - hcore) + 1;

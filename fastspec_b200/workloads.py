@@ -14,6 +14,7 @@ the reference program and uploaded to the GPU path bit-identically.
 import ctypes
 import ctypes.util
 import math
+import os
 
 import numpy as np
 
@@ -258,3 +259,78 @@ def zeeman_lines(n, wmin, wmax, seed):
     L.zeeman = (f32_of_text(jlo, "%.1f"), f32_of_text(jup, "%.1f"),
                 f32_of_text(glo, "%.3f"), f32_of_text(gup, "%.3f"))
     return L
+
+
+# ---- batched grid: many atmospheres sharing one atomic line list -------------------------------
+# Element of each config-0 species and the solar-state file the batch states are derived from.
+_BATCH_ELEMENTS = ["Fe", "Ti", "Cr", "Ni", "Ca"]
+_R_BATCH = 5.0e5
+
+
+def _solar_state():
+    d = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "atm_solar.npz"))
+    return {k: d[k] for k in d.files}
+
+
+def batch_atmosphere(teff, logg, ntau, abund, base=None):
+    """Atmospheric state of one member of the batched grid, derived from the solar state (EOS of the
+    reference, 56 depths) by a documented stand-in for the host EOS: quantities interpolated to
+    ntau depths over the same log tau range; T scaled by Teff / 5777; densities by (g / g_sun)^0.6;
+    electron density additionally by (Teff / 5777)^6; FractionPF of neutral species by the Saha
+    factor Ne (T_sun / T)^1.5 exp(5040 chi (1/T - 1/T_sun)) relative to the solar state, of ions
+    unchanged, both times the element's abundance factor 10^abund[element]; the continuum opacity
+    knots scale with the electron density (H-minus).  abund: dict element -> dex offset.
+    Returns (state dict for Context.set_atmosphere, continuum dict(cont_wave, cont_opac))."""
+    s = _solar_state() if base is None else base
+    n0 = len(s["T"])
+    x0 = np.linspace(0.0, 1.0, n0)
+    x = np.linspace(0.0, 1.0, ntau)
+    li = lambda v: np.exp(np.interp(x, x0, np.log(np.abs(v) + 1e-300)))
+    ft = teff / 5777.0
+    fg = 10.0 ** (0.6 * (logg - 4.44))
+    T = np.interp(x, x0, s["T"]) * ft
+    Tsun = np.interp(x, x0, s["T"])
+    xne = li(s["xne"]) * fg * ft ** 6
+    xne_sun = li(s["xne"])
+    st = dict(rhox=li(s["rhox"]) * fg, T=T, xne=xne, xna=li(s["xna"]) * fg, rho=li(s["rho"]) * fg,
+              xamass=s["xamass"].astype(np.float32), potion=s["potion"].astype(np.float32),
+              ion=s["ion"].astype(np.int32),
+              frac_h1=(li(s["frac_h1"]) * fg).astype(np.float32),
+              frac_he1=(np.interp(x, x0, s["frac_he1"]) * fg).astype(np.float32),
+              frac_h2=np.zeros(ntau, np.float32))
+    fpf = np.empty((ntau, len(s["species"])), np.float32)
+    for k, name in enumerate(s["species"]):
+        el, ion = str(name).split()
+        base_f = li(s["fractionpf"][:, k])
+        f = base_f * 10.0 ** abund.get(el, 0.0)
+        if int(ion) == 1:
+            chi = float(s["potion"][k])
+            f = f * (xne / xne_sun) * (Tsun / T) ** 1.5 * np.exp(5040.0 * chi * (1.0 / T - 1.0 / Tsun))
+        fpf[:, k] = f
+    st["fractionpf"] = fpf
+    ko = np.empty((len(s["cont_wave"]), ntau))
+    lk = np.log(s["cont_opac"])
+    for w in range(lk.shape[0]):
+        ko[w] = np.exp(np.interp(x, x0, lk[w])) * (xne / xne_sun)
+    return st, dict(cont_wave=s["cont_wave"], cont_opac=ko)
+
+
+def batch_grid(n=256, seed=SEED0 + 3):
+    """The batched configuration: n atmospheres with depth counts U{48..80}, Teff U(3800, 7500) K,
+    log g U(3.5, 5.0), abundance offsets N(0, 0.2) dex per element, and wavelength spans U(20, 200) A
+    at R = 5e5 (Wmode 1, dstep = c / R) starting U(3000, 9000 - span).  Returns a list of dicts
+    (teff, logg, ntau, abund, grid dict, state, cont)."""
+    rng = np.random.default_rng(seed)
+    base = _solar_state()
+    out = []
+    for i in range(n):
+        ntau = int(rng.integers(48, 81))
+        teff = float(rng.uniform(3800.0, 7500.0))
+        logg = float(rng.uniform(3.5, 5.0))
+        abund = {el: float(v) for el, v in zip(_BATCH_ELEMENTS, rng.normal(0.0, 0.2, len(_BATCH_ELEMENTS)))}
+        span = float(rng.uniform(20.0, 200.0))
+        w0 = float(rng.uniform(3000.0, 9000.0 - span))
+        st, cont = batch_atmosphere(teff, logg, ntau, abund, base)
+        grid = dict(wmode=1, wstart=w0, wend=w0 + span, dstep=2.99792458e5 / _R_BATCH)
+        out.append(dict(teff=teff, logg=logg, ntau=ntau, abund=abund, grid=grid, state=st, cont=cont))
+    return out

@@ -196,6 +196,40 @@ int fsg_mu_quadrature(int quad, int n, double *x, double *w, double *r, int setn
 int fsg_zeeman_pattern(float jlo, float jup, float glo, float gup, int32_t *npi, float *spi,
                        float *rpi, int32_t *nsig, float *ssig, float *rsig);
 
+
+/* ---- batched synthesis ---------------------------------------------------------------------
+ * Many atmospheres (each a context with grid, atmosphere, continuum and mu set; mixed precision)
+ * and one line list sorted by wavelength: per atmosphere the lines with centres inside its grid
+ * +- margin [A] take the central pass and block refill, then one persistent wing-pass launch and
+ * one persistent core-pass launch take (atmosphere, tile) items from device work queues, then the
+ * formal solver and flux run per atmosphere.  The sequence has no host synchronisation; the
+ * first fsg_batch_run tunes it (unless fsg_batch_set_tuning gave a choice), captures it as a CUDA
+ * graph and replays it; later runs replay.  No counterpart in the reference, which synthesises
+ * one atmosphere per run (fastspec.f90:192-449). */
+typedef struct fsg_batch fsg_batch;
+typedef struct {
+    int32_t tile_pix;       /* wing-pass tile width: 64 or 128 wavelengths */
+    int32_t wing_ctas, core_ctas;   /* CTAs of the persistent wing / core launches */
+    double  ms_wing, ms_core;       /* their times in the tuning run [ms] */
+} fsg_batch_tuning;
+typedef struct {
+    int32_t natm;
+    int64_t nlines_candidate;       /* lines taken by the atmospheres (sum) */
+    double  line_evals;             /* profile evaluations inside windows (sum) */
+    double  ms_total;               /* device time of one graph replay [ms] */
+    fsg_batch_tuning tuning;
+} fsg_batch_stats;
+/* On failure *out stays NULL and fsg_batch_last_error(NULL) gives the reason. */
+int  fsg_batch_create(fsg_ctx *const *atms, int natm, const fsg_lines *lines, double margin, fsg_batch **out);
+int  fsg_batch_tune(fsg_batch *b, fsg_batch_tuning *result);
+int  fsg_batch_set_tuning(fsg_batch *b, const fsg_batch_tuning *t);
+int  fsg_batch_run(fsg_batch *b, fsg_batch_stats *stats);
+/* Flux (line + continuum, continuum; [nwl] each) of atmosphere iatm after a run. */
+int  fsg_batch_flux(fsg_batch *b, int iatm, double *sfl, double *sfc);
+void *fsg_batch_stream(fsg_batch *b);
+const char *fsg_batch_last_error(const fsg_batch *b);
+void fsg_batch_destroy(fsg_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

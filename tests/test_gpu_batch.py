@@ -1,0 +1,92 @@
+"""Batched synthesis on the GPU (fsg_batch_*): each atmosphere's flux against the oracle run on the
+same candidate lines (mixed-path flux tolerance 1e-5) and against the single-context path; graph
+replays are deterministic; a given tuning is applied."""
+import numpy as np
+import pytest
+
+import helpers as H
+
+pytestmark = pytest.mark.gpu
+
+MARGIN = 10.0
+
+
+def small_batch(fsg, natm=4, span=3.0, nlines=120_000, seed=5):
+    from fastspec_b200 import workloads as W
+    import fastspec_b200 as F
+    members = W.batch_grid(natm, seed=W.SEED0 + 50 + seed)
+    lines = W.atomic_lines(nlines, 3000.0, 9000.0, W.SEED0 + 60 + seed)
+    order = np.argsort(lines.arrays()["wl"], kind="stable")
+    arr = {k: np.ascontiguousarray(v[order]) for k, v in lines.arrays().items()}
+    ctxs, cases = [], []
+    x, w, _ = fsg.mu_quadrature(1, 7)
+    for m in members:
+        g = dict(m["grid"])
+        g["wend"] = g["wstart"] + span
+        wave = F.make_grid(1, g["wstart"], g["wend"], g["dstep"]) + g["wstart"]
+        co = H.contopac_on(m["cont"], wave)
+        C = fsg.Context(vmicro=1.0)
+        C.set_grid(1, g["wstart"], g["wend"], g["dstep"])
+        C.set_atmosphere(m["state"])
+        C.set_contopac(co)
+        C.set_mu(x, w)
+        ctxs.append(C)
+        cases.append((g, m["state"], co))
+    return ctxs, cases, arr
+
+
+def candidates(arr, g):
+    sel = (arr["wl"] >= g["wstart"] - MARGIN) & (arr["wl"] <= g["wend"] + MARGIN)
+    return {k: np.ascontiguousarray(v[sel]) for k, v in arr.items()}
+
+
+def test_batch_flux_vs_oracle_and_single_context(fsg, oracle_mod):
+    ctxs, cases, arr = small_batch(fsg)
+    B = fsg.Batch(ctxs, fsg.LineList.from_arrays(arr), margin=MARGIN)
+    st = B.run()
+    assert st["natm"] == len(ctxs) and st["line_evals"] > 0 and st["ms_total"] > 0
+    assert st["tuning"]["tile_pix"] in (64, 128)
+    x, w, _ = oracle_mod.mu_quadrature(1, 7)
+    for i, (g, state, co) in enumerate(cases):
+        sfl, sfc = B.flux(i)
+        cand = candidates(arr, g)
+        S = oracle_mod.State(g, state, contopac=co, vmicro=1.0)
+        r = oracle_mod.lineop_calc(S, oracle_mod.Lines(**cand, kind=2), list_type=2)
+        osfl, osfc = oracle_mod.disk_integ(w, *oracle_mod.radtran(S, x, r["lineopac"]))
+        assert np.max(np.abs(sfl / osfl - 1)) < 1e-5
+        assert np.max(np.abs(sfc / osfc - 1)) < 1e-9
+        # the single-context mixed path on the same candidate list
+        C = ctxs[i]
+        C.lineop_reset()
+        C.lineop_calc(fsg.LineList.from_arrays(cand), want_lineopac=False, want_lines=False)
+        _, _, csfl, _ = C.radtran()
+        assert np.max(np.abs(sfl / csfl - 1)) < 1e-6
+    B.close()
+
+
+def test_batch_replay_and_given_tuning(fsg):
+    ctxs, cases, arr = small_batch(fsg, natm=3, seed=6)
+    B = fsg.Batch(ctxs, fsg.LineList.from_arrays(arr), margin=MARGIN)
+    B.run()
+    f1 = [B.flux(i)[0] for i in range(3)]
+    B.run()
+    f2 = [B.flux(i)[0] for i in range(3)]
+    for a, b in zip(f1, f2):
+        assert np.array_equal(a, b)
+    B.set_tuning({"tile_pix": 64, "wing_ctas": 148, "core_ctas": 296})
+    st = B.run()
+    assert st["tuning"]["tile_pix"] == 64 and st["tuning"]["core_ctas"] == 296
+    f3 = [B.flux(i)[0] for i in range(3)]
+    for a, b in zip(f1, f3):
+        assert np.max(np.abs(a / b - 1)) < 1e-6
+    B.close()
+
+
+def test_batch_rejects_bad_inputs(fsg):
+    ctxs, cases, arr = small_batch(fsg, natm=2, seed=7, nlines=2000)
+    bad = {k: v[::-1].copy() for k, v in arr.items()}                  # not sorted
+    with pytest.raises(fsg.FsgError):
+        fsg.Batch(ctxs, fsg.LineList.from_arrays(bad))
+    C = fsg.Context(precision=fsg.PREC_FP64)
+    with pytest.raises(fsg.FsgError):
+        fsg.Batch([C], fsg.LineList.from_arrays(arr))
