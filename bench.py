@@ -53,6 +53,9 @@ def parse():
     p.add_argument("--shard", action="store_true",
                    help="run the wavelength-sharded synthesis even on one GPU (a process group of one)")
     p.add_argument("--plain-lines", type=float, default=1e6)
+    p.add_argument("--no-batched", action="store_true", help="skip the batched-grid measurement")
+    p.add_argument("--batch-atm", type=int, default=256)
+    p.add_argument("--batch-lines", type=float, default=2e6)
     return p.parse_args()
 
 
@@ -172,6 +175,72 @@ def plain_vs_mixed(F, torch, st, meta, co, dev, nlines):
             "unit": UNIT, "speedup": out["fp64"]["ms"] / out["mixed"]["ms"],
             "fp64_ms": out["fp64"]["ms"], "mixed_ms": out["mixed"]["ms"],
             "flux_max_rel_diff": float(np.max(np.abs(flux["mixed"] / flux["fp64"] - 1.0)))}
+
+
+def batched_grid(F, torch, dev, natm, nlines, steps, warmup):
+    """The batched configuration: natm atmospheres (depths 48-80, Teff 3800-7500 K, spans 20-200 A at
+    R = 5e5) sharing one atomic list of nlines over 3000-9000 A, synthesised by one CUDA-graph
+    replay of fsg_batch_run (persistent work-queue kernels, tiles from the autotuner); compared with
+    the same atmospheres synthesised one context at a time through fsg_lineop_calc_dev."""
+    from fastspec_b200 import workloads as W
+    members = W.batch_grid(natm)
+    lines = W.atomic_lines(int(nlines), 3000.0, 9000.0, W.SEED0 + 3, exact=False)
+    arr = lines.arrays()
+    order = np.argsort(arr["wl"], kind="stable")
+    arr = {k: np.ascontiguousarray(v[order]) for k, v in arr.items()}
+    LL = F.LineList.from_arrays(arr)
+    x, w, _ = F.mu_quadrature(1, NMU)
+    ctxs = []
+    for m in members:
+        g = m["grid"]
+        wave = F.make_grid(1, g["wstart"], g["wend"], g["dstep"]) + g["wstart"]
+        lk = np.log(m["cont"]["cont_opac"])
+        co = np.exp(np.stack([np.interp(wave, m["cont"]["cont_wave"], lk[:, t]) for t in range(m["ntau"])], axis=1))
+        C = F.Context(device=dev, vmicro=1.0)
+        C.set_grid(1, g["wstart"], g["wend"], g["dstep"])
+        C.set_atmosphere(m["state"])
+        C.set_contopac(co)
+        C.set_mu(x, w)
+        ctxs.append(C)
+    B = F.Batch(ctxs, LL, margin=10.0)
+    t0 = time.perf_counter()
+    tuning = B.tune()
+    tune_s = time.perf_counter() - t0
+    st = B.run()                                   # captures the graph
+    for _ in range(max(0, warmup - 1)):
+        B.run()
+    bs = torch.cuda.ExternalStream(B.stream_ptr(), device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(bs)
+    for _ in range(steps):
+        st = B.run()
+    e1.record(bs)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    # the same atmospheres one context at a time (device line list per atmosphere's candidates)
+    wl = arr["wl"]
+    t_seq = 0.0
+    for C, m in zip(ctxs, members):
+        g = m["grid"]
+        a0, a1 = np.searchsorted(wl, g["wstart"] - 10.0), np.searchsorted(wl, g["wend"] + 10.0, side="right")
+        sub = F.LineList.from_arrays({k: np.ascontiguousarray(v[a0:a1]) for k, v in arr.items()})
+        C.lineop_reset()
+        r = C.lineop_calc(sub, want_lineopac=False, want_lines=False)
+        t_seq += r["stats"]["ms_total"]
+    nwl_tot = sum(c.nwl for c in ctxs)
+    out = {"config": "%d atmospheres (48-80 depths, Teff 3800-7500 K, spans 20-200 A at R=5e5, %d wavelengths in all), "
+                     "%d shared atomic lines 3000-9000 A, 7 mu" % (natm, nwl_tot, int(nlines)),
+           "spectra_per_s": natm / (ms / 1e3), "line_evals_per_s": st["line_evals"] / (ms / 1e3),
+           "ms_per_batch": ms, "line_evals": st["line_evals"], "candidate_lines": st["nlines_candidate"],
+           "tuning": tuning, "tuning_s": tune_s, "graph": True,
+           "sequential_line_ms": t_seq,
+           "note": "sequential_line_ms: the same line opacities one context at a time (fsg_lineop_calc, "
+                   "device time of central pass + accumulation, no solver)"}
+    B.close()
+    for C in ctxs:
+        C.close()
+    return out
 
 
 def run_gpu(args, rank, world):
@@ -309,6 +378,8 @@ def run_gpu(args, rank, world):
     del dt
     if not args.no_plain and rank == 0:
         out["plain"] = plain_vs_mixed(F, torch, st, meta, co, dev, int(args.plain_lines))
+    if not args.no_batched and rank == 0:
+        out["batched"] = batched_grid(F, torch, dev, args.batch_atm, args.batch_lines, args.steps, args.warmup)
     return out
 
 
@@ -459,6 +530,8 @@ def main():
         line["cpu_baseline"] = cpu
     if "plain" in r:
         line["plain_fp64"] = r["plain"]
+    if "batched" in r:
+        line["batched"] = r["batched"]
     print(json.dumps(line))
 
 
