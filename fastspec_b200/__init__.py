@@ -80,6 +80,7 @@ EXPORTS = [
     "fsg_locprf_pp", "fsg_locprf_pp_noalloc", "fsg_mu_quadrature", "fsg_zeeman_pattern",
     "fsg_central_dev", "fsg_accumulate_dev", "fsg_batch_create", "fsg_batch_tune", "fsg_batch_set_tuning",
     "fsg_batch_run", "fsg_batch_flux", "fsg_batch_stream", "fsg_batch_last_error", "fsg_batch_destroy",
+    "fsg_set_vmicro", "fsg_set_fractionpf", "fsg_adjoint_dev",
 ]
 
 _lib = None
@@ -368,6 +369,19 @@ class Context:
         self._ck(self._lib.fsg_accumulate_dev(self.h, C.byref(dlines), v(d_flags), v(d_ileft), v(d_iright), int(i0),
                                               int(i1), C.byref(st)), "fsg_accumulate_dev")
         return st.asdict()
+
+    def set_fractionpf(self, fractionpf):
+        fpf = _f32(fractionpf)
+        self._ck(self._lib.fsg_set_fractionpf(self.h, _p(fpf, C.c_float)), "fsg_set_fractionpf")
+
+    def set_vmicro(self, vmicro):
+        self._ck(self._lib.fsg_set_vmicro(self.h, C.c_double(float(vmicro))), "fsg_set_vmicro")
+
+    def adjoint_dev(self, dlines, d_gflux, d_glin, d_gvmic, d_gkappa=None):
+        """dL/dSfL (device pointer, [nwl]) -> per-line dL/d ln gf and vmicro shares (device pointers)."""
+        v = lambda p: C.c_void_p(p) if p else None
+        self._ck(self._lib.fsg_adjoint_dev(self.h, C.byref(dlines), v(d_gflux), v(d_gkappa), v(d_glin), v(d_gvmic)),
+                 "fsg_adjoint_dev")
 
     def lineop_get(self):
         lo = np.zeros((self.nwl, self.ntau))

@@ -20,6 +20,7 @@ UNITS = [
     ("fsg_fast.cu", ["-fmad=true"]),
     ("fsg_api.cu", ["-fmad=false"]),
     ("fsg_noalloc.cu", ["-fmad=false"]),
+    ("fsg_adjoint.cu", ["-fmad=false"]),
 ]
 
 

@@ -48,6 +48,10 @@ int fsg_launch_core_batch(cudaStream_t, int, const CoreJob *, const int *, int, 
 int fsg_class_pix(int);
 int fsg_fast_tiles(int);
 size_t fsg_tile_span_scratch(int64_t);
+size_t fsg_adjoint_work(int, int);
+int fsg_launch_adjoint(cudaStream_t, const AtmView &, const LineView &, const VoigtTables &, const double *,
+                       const double *, int, const double *, const double *, const int32_t *, const int32_t *,
+                       const int32_t *, const double *, double *, double *, double, double *, double *);
 size_t fsg_linstr_work(int64_t, int, int);
 void fsg_launch_linstr(cudaStream_t, const AtmView &, const LineView &, const VoigtTables &, const int32_t *, int64_t,
                        int64_t, int, const double *, const double *, const double *, double *, float *);
@@ -131,7 +135,7 @@ struct fsg_ctx {
     DBuf l_wl, l_elo, l_gf, l_grad, l_gqst, l_gvdw, l_spc, l_ismol, l_ihe;
     DBuf d_flags, d_ileft, d_iright, d_idx, d_counts, d_offs, d_total, d_hist, d_nkeep;
     // block buffers
-    DBuf d_wing, d_core, d_hdr, d_tlo, d_thi, d_p64, d_lstart, d_lstop, d_widx, d_pw, d_evals, d_err, d_ncore, d_span, d_lswork, d_linstr, d_rflags, d_rleft, d_rright;
+    DBuf d_wing, d_core, d_hdr, d_tlo, d_thi, d_p64, d_lstart, d_lstop, d_widx, d_pw, d_evals, d_err, d_ncore, d_span, d_lswork, d_linstr, d_rflags, d_rleft, d_rright, d_gkappa, d_adjwork;
     // spectra
     DBuf d_spl, d_spc, d_sfl, d_sfc, d_work, d_a, d_v, d_h, d_l;
     // magnetic
@@ -217,7 +221,7 @@ void fsg_destroy(fsg_ctx *ctx) {
                      &ctx->l_grad, &ctx->l_gqst, &ctx->l_gvdw, &ctx->l_spc, &ctx->l_ismol, &ctx->l_ihe,
                      &ctx->d_flags, &ctx->d_ileft, &ctx->d_iright, &ctx->d_idx, &ctx->d_counts, &ctx->d_offs,
                      &ctx->d_total, &ctx->d_hist, &ctx->d_nkeep, &ctx->d_wing, &ctx->d_core, &ctx->d_hdr,
-                     &ctx->d_tlo, &ctx->d_thi, &ctx->d_err, &ctx->d_ncore, &ctx->d_span, &ctx->d_lswork, &ctx->d_linstr, &ctx->d_rflags, &ctx->d_rleft, &ctx->d_rright, &ctx->d_p64, &ctx->d_lstart, &ctx->d_lstop, &ctx->d_widx,
+                     &ctx->d_tlo, &ctx->d_thi, &ctx->d_err, &ctx->d_ncore, &ctx->d_span, &ctx->d_lswork, &ctx->d_linstr, &ctx->d_rflags, &ctx->d_rleft, &ctx->d_rright, &ctx->d_gkappa, &ctx->d_adjwork, &ctx->d_p64, &ctx->d_lstart, &ctx->d_lstop, &ctx->d_widx,
                      &ctx->d_pw, &ctx->d_evals, &ctx->d_spl, &ctx->d_spc, &ctx->d_sfl, &ctx->d_sfc,
                      &ctx->d_work, &ctx->d_a, &ctx->d_v, &ctx->d_h, &ctx->d_l, &ctx->z_npi, &ctx->z_nsi,
                      &ctx->z_pioff, &ctx->z_sioff, &ctx->z_splpi, &ctx->z_strpi, &ctx->z_splsi, &ctx->z_strsi,
@@ -1335,6 +1339,48 @@ int fsg_zeeman_pattern(float jlo, float jup, float glo, float gup, int32_t *npi,
     return FSG_OK;
 }
 
+
+// ---- derivatives of the flux (adjoint of RadTranCalc + DiskInteg and of the line opacity) --------
+int fsg_set_fractionpf(fsg_ctx *ctx, const float *fractionpf) {
+    if (!ctx || !fractionpf) return FSG_E_ARG;
+    if (!ctx->have_atm) return fail(ctx, FSG_E_STATE, "fsg_set_fractionpf: set the atmosphere first");
+    const int nt = ctx->ntau, ns = ctx->nspc;
+    std::vector<float> fpf((size_t)ns * nt);
+    for (int t = 0; t < nt; t++) for (int k = 0; k < ns; k++) fpf[(size_t)k * nt + t] = fractionpf[(size_t)t * ns + k];
+    cudaSetDevice(ctx->device);
+    CK(cudaMemcpyAsync(ctx->d_fpf.p, fpf.data(), sizeof(float) * fpf.size(), cudaMemcpyHostToDevice, ctx->stream),
+       "fractionpf upload");
+    CK(cudaStreamSynchronize(ctx->stream), "fractionpf upload");
+    return FSG_OK;
+}
+
+int fsg_set_vmicro(fsg_ctx *ctx, double vmicro) {
+    if (!ctx || !(vmicro >= 0.0)) return fail(ctx, FSG_E_ARG, "fsg_set_vmicro: vmicro >= 0");
+    ctx->cfg.vmicro = vmicro;
+    return FSG_OK;
+}
+
+int fsg_adjoint_dev(fsg_ctx *ctx, const fsg_lines *d_lines, const double *d_gflux, double *d_gkappa, double *d_glin,
+                    double *d_gvmic) {
+    int rc = check_lines(ctx, d_lines); if (rc) return rc;
+    if (ctx->nmu < 1) return fail(ctx, FSG_E_STATE, "fsg_adjoint_dev: set mu first");
+    if (!d_gflux || !d_glin || !d_gvmic) return fail(ctx, FSG_E_ARG, "fsg_adjoint_dev: null argument");
+    if (ctx->d_flags.cap < sizeof(int32_t) * (size_t)d_lines->n)
+        return fail(ctx, FSG_E_STATE, "fsg_adjoint_dev: run fsg_lineop_calc(_dev) on this list first");
+    cudaSetDevice(ctx->device);
+    rc = ensure_lineopac(ctx); if (rc) return rc;
+    const size_t ng = sizeof(double) * (size_t)ctx->nwl * ctx->ntau;
+    if (!d_gkappa) { ALLOC(ctx->d_gkappa, ng); d_gkappa = ctx->d_gkappa.as<double>(); }
+    ALLOC(ctx->d_adjwork, fsg_adjoint_work(ctx->nwl, ctx->ntau));
+    rc = fsg_launch_adjoint(ctx->stream, fsg_view(ctx), make_view(d_lines), ctx->tab, ctx->d_lineopac.as<double>(),
+                            ctx->d_rhox.as<double>(), ctx->nmu, ctx->d_xmu.as<double>(), ctx->d_wmu.as<double>(),
+                            ctx->d_flags.as<int32_t>(), ctx->d_ileft.as<int32_t>(), ctx->d_iright.as<int32_t>(),
+                            d_gflux, d_gkappa, ctx->d_adjwork.as<double>(), ctx->cfg.vmicro, d_glin, d_gvmic);
+    ctx->launches += 2;
+    if (rc) return cuda_fail(ctx, cudaGetLastError(), "adjoint");
+    CK(cudaStreamSynchronize(ctx->stream), "adjoint");
+    return FSG_OK;
+}
 
 // ================================================================================================
 // Batched synthesis: many atmospheres (each an fsg_ctx with grid, atmosphere, continuum and mu

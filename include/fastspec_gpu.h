@@ -197,6 +197,22 @@ int fsg_zeeman_pattern(float jlo, float jup, float glo, float gup, int32_t *npi,
                        float *rpi, int32_t *nsig, float *ssig, float *rsig);
 
 
+/* ---- derivatives (no counterpart in the reference) ---------------------------------------------
+ * fsg_set_vmicro changes the microturbulence of later calls [km/s]; fsg_set_fractionpf replaces the
+ * FractionPF of fsg_set_atmosphere ([ntau][nspc]) and keeps the rest of the atmosphere.
+ * fsg_adjoint_dev: given d_gflux = dL/dSfL [nwl] (device) for the flux of the last fsg_radtran(_dev)
+ * of this context, computes with one backward sweep of the DELO-Bezier solver per wavelength
+ * d_gkappa = dL/dLineOpac [nwl][ntau] (may be NULL: kept inside the context), and per line of the
+ * device list d_lines -- which must be the list of the last fsg_lineop_calc(_dev), whose windows it
+ * uses -- d_glin[l] = sum dL/dLineOpac * H * LinCop (= dL/d ln gf_l and, summed over an element's
+ * lines, dL/d ln abundance with the continuum and the EOS held fixed) and d_gvmic[l] = the line's
+ * share of dL/dvmicro.  Profiles are recomputed (FP64, the reference's tables), their v and a
+ * derivatives from the Faddeeva relation dw/dz = -2 z w + 2i/sqrt(pi). */
+int fsg_set_vmicro(fsg_ctx *ctx, double vmicro);
+int fsg_set_fractionpf(fsg_ctx *ctx, const float *fractionpf);
+int fsg_adjoint_dev(fsg_ctx *ctx, const fsg_lines *d_lines, const double *d_gflux, double *d_gkappa,
+                    double *d_glin, double *d_gvmic);
+
 /* ---- batched synthesis ---------------------------------------------------------------------
  * Many atmospheres (each a context with grid, atmosphere, continuum and mu set; mixed precision)
  * and one line list sorted by wavelength: per atmosphere the lines with centres inside its grid
