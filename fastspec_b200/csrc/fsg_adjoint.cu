@@ -9,6 +9,7 @@
 // gives dL/dkappa for every depth and wavelength.  k_line_adjoint then recomputes every retained
 // line's profile over its window (nothing is stored from the forward) and reduces
 //   glin_l  = sum_{t, lambda} dL/dkappa * H * LinCop          (= dL/dln(gf), = dL/dln(abundance))
+// (H and L from FvTab, the FP32 table of the Faraday-Voigt pair: H agrees with VgtTab's to ~1e-7)
 //   gvmic_l = sum_{t, lambda} dL/dkappa * dLinCop H / dvmic
 // with H, L from the reference's tables and asymptotics and the Faddeeva derivative
 // dw/dz = -2 z w + 2i/sqrt(pi), w = H + iL, z = v + ia:
@@ -197,21 +198,36 @@ k_line_adjoint(AtmView A, LineView L, const float *__restrict__ vtab, const floa
     }
     __syncwarp();
     const int il = ileft[i], ir = iright[i];
-    const int64_t ne = (int64_t)(ir - il + 1) * nt;
     double sl = 0.0, sv = 0.0;
     const double isp2 = 2.0 * FSG_SQRTPIINV;
-    for (int64_t e = lane; e < ne; e += 32) {
-        const int iw = il - 1 + (int)(e / nt), t = (int)(e % nt);
-        const double g = gkappa[(size_t)iw * nt + t];
-        if (g == 0.0) continue;
-        const double v = (A.wave[iw] - wlc - shf[t]) * vv[t], a = av[t];
+    // lanes over depths (t = lane, lane + 32, ...), a loop over the window's wavelengths: the
+    // dL/dkappa reads of a wavelength are contiguous across the lanes
+    for (int t = lane; t < nt; t += 32) {
+        const double c = cop[t], vvt = vv[t], a = av[t], qt = q[t], off = wlc + shf[t];
         const VLine64 VL = vline64(anode, aida, a);
-        const double H = hvoigt_line64(vtab, VL, v);
-        double Hf, Lf;
-        fvoigt_line64(fvtab, VL, v, &Hf, &Lf);
-        const double Hv = -2.0 * (v * Hf - a * Lf), Ha = 2.0 * (v * Lf + a * Hf) - isp2;
-        sl += g * H * cop[t];
-        sv += g * cop[t] * q[t] * (-v * Hv - a * Ha - H);
+        double s1 = 0.0, s2 = 0.0;
+        const float af = (float)a, a2f = af * af;
+        for (int iw = il - 1; iw < ir; iw++) {
+            const double g = gkappa[(size_t)iw * nt + t];
+            const double v = (A.wave[iw] - off) * vvt;
+            const float vf = (float)v, sf = vf * vf + a2f;
+            if (sf >= 196.0f) {
+                // wing: the rational (H, L) pair of FVoigt (voigt.f90:256-352) in FP32 (the gradient needs no more)
+                const float w = 0.56418958f / (sf * sf - vf * vf + a2f + 0.25f);
+                const float Hf = af * (sf + 0.5f) * w, Lf = vf * (sf - 0.5f) * w;
+                const float Hv = -2.0f * (vf * Hf - af * Lf), Ha = 2.0f * (vf * Lf + af * Hf) - (float)isp2;
+                s1 += g * (double)Hf;
+                s2 += g * (double)(-vf * Hv - af * Ha - Hf);
+            } else {
+                double Hf, Lf;
+                fvoigt_line64(fvtab, VL, v, &Hf, &Lf);
+                const double Hv = -2.0 * (v * Hf - a * Lf), Ha = 2.0 * (v * Lf + a * Hf) - isp2;
+                s1 += g * Hf;
+                s2 += g * (-v * Hv - a * Ha - Hf);
+            }
+        }
+        sl += s1 * c;
+        sv += s2 * c * qt;
     }
     // window edges: the depth giving W, and the edge profiles weighted by dL/dkappa
     const double iSqrtPi = FSG_SQRTPIINV;
