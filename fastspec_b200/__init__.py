@@ -242,7 +242,7 @@ class LineList:
     @classmethod
     def from_arrays(cls, a, kind=2, zeeman=None):
         return cls(a["wl"], a["elo"], a["gf"], a["grad"], a["gqst"], a["gvdw"], a["spc"], kind=kind,
-                   ismol=a.get("ismol"), zeeman=zeeman)
+                   ismol=a.get("ismol"), ihe=a.get("ihe"), zeeman=zeeman)
 
 
 class Context:
@@ -373,6 +373,12 @@ class Context:
     def set_fractionpf(self, fractionpf):
         fpf = _f32(fractionpf)
         self._ck(self._lib.fsg_set_fractionpf(self.h, _p(fpf, C.c_float)), "fsg_set_fractionpf")
+
+    def set_hestark(self, hegam, heshf, spc_he1):
+        """He I Stark broadening and shift tables [nhe][ntau] (hestark.f90) and the He I species index."""
+        g = _f64(hegam); h = _f64(heshf)
+        self._ck(self._lib.fsg_set_hestark(self.h, g.shape[0], _p(g, C.c_double), _p(h, C.c_double), int(spc_he1)),
+                 "fsg_set_hestark")
 
     def set_vmicro(self, vmicro):
         self._ck(self._lib.fsg_set_vmicro(self.h, C.c_double(float(vmicro))), "fsg_set_vmicro")

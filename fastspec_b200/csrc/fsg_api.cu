@@ -579,6 +579,24 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st, cons
             nblocks++;
         }
     }
+    // He I lines with Stark-shifted profiles (hestark.f90): the FP64 per-wavelength kernel of the
+    // wide lines, which applies the per-depth shift (opacity.f90:297-346)
+    if (ctx->nhe > 0) {
+        int rc3 = fsg_select(s, n, sf, il, ir, -3, ctx->d_counts.as<int>(), ctx->d_offs.as<int64_t>(),
+                             ctx->d_idx.as<int64_t>(), ctx->d_total.as<int64_t>());
+        if (rc3) return cuda_fail(ctx, cudaGetLastError(), "select He I lines");
+        int64_t nhl = 0;
+        CK(cudaMemcpyAsync(&nhl, ctx->d_total.p, sizeof nhl, cudaMemcpyDeviceToHost, s), "He I lines");
+        CK(cudaStreamSynchronize(s), "He I lines");
+        ctx->launches += 3;
+        if (nhl > 0) {
+            ALLOC(ctx->d_pw, sizeof(double3) * nhl * nt);
+            ALLOC(ctx->d_evals, sizeof(double));
+            fsg_launch_wide_fp64(s, A, LV, (int)nhl, ctx->d_idx.as<int64_t>(), sf, wl_, wr_, ctx->d_pw.as<double3>(),
+                                 ctx->tab, i0, i1, ctx->d_lineopac.as<double>(), ctx->d_evals.as<double>());
+            ctx->launches += 2;
+        }
+    }
     CK(cudaGetLastError(), "fast accumulation");
     CK(cudaStreamSynchronize(s), "fast accumulation");
     int kerr = 0;
@@ -1531,6 +1549,12 @@ int fsg_batch_create(fsg_ctx *const *atms, int natm, const fsg_lines *lines, dou
         if (c->ntau > 128) return bail(FSG_E_ARG, "fsg_batch_create: ntau <= 128");
     }
     rc = check_lines(atms[0], lines); if (rc) return bail(rc, atms[0]->err.c_str());
+    bool has_he = false;
+    for (int i = 0; i < natm; i++) has_he = has_he || atms[i]->nhe > 0;
+    if (has_he && lines->ihe)
+        for (int64_t i = 0; i < lines->n; i++)
+            if (lines->ihe[i] > 0)
+                return bail(FSG_E_ARG, "fsg_batch_create: He I Stark-shifted lines are not batched");
     int nspc_min = atms[0]->nspc;
     for (int i = 1; i < natm; i++) nspc_min = std::min(nspc_min, atms[i]->nspc);
     for (int64_t i = 0; i < lines->n; i++) {

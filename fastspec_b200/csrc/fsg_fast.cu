@@ -617,12 +617,14 @@ __device__ __forceinline__ int width_class(int il, int ir) {
 }
 
 #define SCAN_BS 1024
-// selection predicate: cls >= 0 retained lines of that width class, -1 every retained line,
-// -2 retained wide lines (flag bit 3)
+// selection predicate: cls >= 0 retained lines of that width class (He I shifted lines excluded),
+// -1 every retained line, -2 retained wide lines (flag bit 3), -3 retained He I shifted lines
 __device__ __forceinline__ int sel_pred(int f, int il, int ir, int cls) {
     if (f & FSG_F_WEAK) return 0;
     if (cls == -1) return 1;
     if (cls == -2) return (f & FSG_F_WIDE) != 0;
+    if (cls == -3) return ((f >> 8) & 255) != 0;         // He I lines with Stark-shifted profiles
+    if ((f >> 8) & 255) return 0;                        // ... which the FP32 classes leave out
     return width_class(il, ir) == cls;
 }
 // Count retained lines of class `cls` (cls < 0: every retained line) per CTA of SCAN_BS lines.
@@ -703,7 +705,7 @@ int fsg_select(cudaStream_t s, int64_t n, const int32_t *flags, const int32_t *i
 __global__ void k_class_hist(int64_t n, const int32_t *flags, const int32_t *il, const int32_t *ir,
                              unsigned long long *hist) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || (flags[i] & FSG_F_WEAK)) return;
+    if (i >= n || (flags[i] & FSG_F_WEAK) || ((flags[i] >> 8) & 255)) return;
     atomicAdd(&hist[width_class(il[i], ir[i])], 1ull);
 }
 

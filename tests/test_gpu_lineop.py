@@ -374,3 +374,30 @@ def test_segmentation_overflow_is_reported(fsg):
     C = ctx_for(fsg, grid, st, co, fsg.PREC_FP64, limitram_gb=3e-5)
     with pytest.raises(fsg.FsgError, match="segmentation"):
         C.lineop_calc(fsg_lines(fsg, L))
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_he_stark_shifted_lines(fsg, oracle_mod, prec):
+    """He I lines with per-depth Stark widths and shifts (hestark.f90 tables, opacity.f90:297-346):
+    species 0 stands in for He I, a third of its lines carry table indices 1..3."""
+    grid, st, co, L = solar_case(n=300, seed=61)
+    a = dict(L.arrays())
+    rng = np.random.default_rng(61)
+    ihe = np.zeros(len(a["wl"]), np.int32)
+    sel = np.nonzero(a["spc"] == 0)[0][::3]
+    ihe[sel] = rng.integers(1, 4, len(sel))
+    a["ihe"] = ihe
+    nt = len(st["T"])
+    depth = np.linspace(0.0, 1.0, nt)
+    hegam = np.stack([1e9 * (1 + k) * (1 + 3 * depth) for k in range(3)])
+    heshf = np.stack([(0.02 + 0.03 * k) * (0.2 + depth) for k in range(3)])
+    C = ctx_for(fsg, grid, st, co, fsg.PREC_MIXED if prec == "mixed" else fsg.PREC_FP64)
+    C.set_hestark(hegam, heshf, 0)
+    g = C.lineop_calc(fsg.LineList.from_arrays(a))
+    S = oracle_mod.State(grid, st, contopac=co, vmicro=1.0, hegam=hegam, heshf=heshf, spc_he1=0)
+    r = oracle_mod.lineop_calc(S, oracle_mod.Lines(**a, kind=2), list_type=2)
+    assert np.any((r["flags"] >> 8) & 255)
+    assert np.array_equal(g["flags"] & ~8, r["flags"] & ~8)
+    assert np.array_equal(g["ileft"], r["ileft"]) and np.array_equal(g["iright"], r["iright"])
+    tol = 2e-6 if prec == "mixed" else 1e-11
+    assert np.max(np.abs(g["lineopac"] - r["lineopac"]) / (r["lineopac"] + co)) < tol
