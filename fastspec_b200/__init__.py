@@ -80,7 +80,7 @@ EXPORTS = [
     "fsg_locprf_pp", "fsg_locprf_pp_noalloc", "fsg_mu_quadrature", "fsg_zeeman_pattern",
     "fsg_central_dev", "fsg_accumulate_dev", "fsg_batch_create", "fsg_batch_tune", "fsg_batch_set_tuning",
     "fsg_batch_run", "fsg_batch_flux", "fsg_batch_stream", "fsg_batch_last_error", "fsg_batch_destroy",
-    "fsg_set_vmicro", "fsg_set_fractionpf", "fsg_adjoint_dev",
+    "fsg_set_vmicro", "fsg_set_fractionpf", "fsg_adjoint_dev", "fsg_disk_integ_conv", "fsg_disk_integ_conv_dev",
 ]
 
 _lib = None
@@ -369,6 +369,22 @@ class Context:
         self._ck(self._lib.fsg_accumulate_dev(self.h, C.byref(dlines), v(d_flags), v(d_ileft), v(d_iright), int(i0),
                                               int(i1), C.byref(st)), "fsg_accumulate_dev")
         return st.asdict()
+
+    def disk_integ_conv(self, radii, vsini=0.0, vmacro=0.0, vgau=0.0):
+        """RadTranCalc + DiskInteg with broadening: (sfl, sfc) [nwl]."""
+        r = _f64(radii)
+        sfl = np.zeros(self.nwl); sfc = np.zeros(self.nwl)
+        self._ck(self._lib.fsg_disk_integ_conv(self.h, _p(r, C.c_double), C.c_double(vsini), C.c_double(vmacro),
+                                               C.c_double(vgau), _p(sfl, C.c_double), _p(sfc, C.c_double)),
+                 "fsg_disk_integ_conv")
+        return sfl, sfc
+
+    def disk_integ_conv_dev(self, radii, vsini, vmacro, vgau, d_spl, d_spc, d_sfl, d_sfc):
+        r = _f64(radii)
+        v = C.c_void_p
+        self._ck(self._lib.fsg_disk_integ_conv_dev(self.h, _p(r, C.c_double), C.c_double(vsini), C.c_double(vmacro),
+                                                   C.c_double(vgau), v(d_spl), v(d_spc), v(d_sfl), v(d_sfc)),
+                 "fsg_disk_integ_conv_dev")
 
     def set_fractionpf(self, fractionpf):
         fpf = _f32(fractionpf)

@@ -48,6 +48,7 @@ int fsg_launch_core_batch(cudaStream_t, int, const CoreJob *, const int *, int, 
 int fsg_class_pix(int);
 int fsg_fast_tiles(int);
 size_t fsg_tile_span_scratch(int64_t);
+void fsg_launch_conv(cudaStream_t, int, const double *, int, const double *, int, double *, const double *, double);
 size_t fsg_adjoint_work(int, int);
 int fsg_launch_adjoint(cudaStream_t, const AtmView &, const LineView &, const VoigtTables &, const double *,
                        const double *, int, const double *, const double *, const int32_t *, const int32_t *,
@@ -117,7 +118,7 @@ struct fsg_ctx {
     double h_anode[FSG_NA1], h_aida[FSG_NA1];
     // grid
     int have_grid = 0, wmode = 0, nwl = 0;
-    double wstart = 0, wend = 0, dstep = 0, rstep = 0, wfirst = 0;
+    double wstart = 0, wend = 0, dstep = 0, rstep = 0, wfirst = 0, wlast = 0;
     DBuf d_wave;
     // atmosphere
     int have_atm = 0, ntau = 0, nspc = 0;
@@ -135,7 +136,7 @@ struct fsg_ctx {
     DBuf l_wl, l_elo, l_gf, l_grad, l_gqst, l_gvdw, l_spc, l_ismol, l_ihe;
     DBuf d_flags, d_ileft, d_iright, d_idx, d_counts, d_offs, d_total, d_hist, d_nkeep;
     // block buffers
-    DBuf d_wing, d_core, d_hdr, d_tlo, d_thi, d_p64, d_lstart, d_lstop, d_widx, d_pw, d_evals, d_err, d_ncore, d_span, d_lswork, d_linstr, d_rflags, d_rleft, d_rright, d_gkappa, d_adjwork;
+    DBuf d_wing, d_core, d_hdr, d_tlo, d_thi, d_p64, d_lstart, d_lstop, d_widx, d_pw, d_evals, d_err, d_ncore, d_span, d_lswork, d_linstr, d_rflags, d_rleft, d_rright, d_gkappa, d_adjwork, d_cbuf, d_ctaps;
     // spectra
     DBuf d_spl, d_spc, d_sfl, d_sfc, d_work, d_a, d_v, d_h, d_l;
     // magnetic
@@ -221,7 +222,7 @@ void fsg_destroy(fsg_ctx *ctx) {
                      &ctx->l_grad, &ctx->l_gqst, &ctx->l_gvdw, &ctx->l_spc, &ctx->l_ismol, &ctx->l_ihe,
                      &ctx->d_flags, &ctx->d_ileft, &ctx->d_iright, &ctx->d_idx, &ctx->d_counts, &ctx->d_offs,
                      &ctx->d_total, &ctx->d_hist, &ctx->d_nkeep, &ctx->d_wing, &ctx->d_core, &ctx->d_hdr,
-                     &ctx->d_tlo, &ctx->d_thi, &ctx->d_err, &ctx->d_ncore, &ctx->d_span, &ctx->d_lswork, &ctx->d_linstr, &ctx->d_rflags, &ctx->d_rleft, &ctx->d_rright, &ctx->d_gkappa, &ctx->d_adjwork, &ctx->d_p64, &ctx->d_lstart, &ctx->d_lstop, &ctx->d_widx,
+                     &ctx->d_tlo, &ctx->d_thi, &ctx->d_err, &ctx->d_ncore, &ctx->d_span, &ctx->d_lswork, &ctx->d_linstr, &ctx->d_rflags, &ctx->d_rleft, &ctx->d_rright, &ctx->d_gkappa, &ctx->d_adjwork, &ctx->d_cbuf, &ctx->d_ctaps, &ctx->d_p64, &ctx->d_lstart, &ctx->d_lstop, &ctx->d_widx,
                      &ctx->d_pw, &ctx->d_evals, &ctx->d_spl, &ctx->d_spc, &ctx->d_sfl, &ctx->d_sfc,
                      &ctx->d_work, &ctx->d_a, &ctx->d_v, &ctx->d_h, &ctx->d_l, &ctx->z_npi, &ctx->z_nsi,
                      &ctx->z_pioff, &ctx->z_sioff, &ctx->z_splpi, &ctx->z_strpi, &ctx->z_splsi, &ctx->z_strsi,
@@ -256,7 +257,7 @@ int fsg_set_grid(fsg_ctx *ctx, int wmode, double wstart, double wend, double dst
     if (!ctx || !wave || nwl < 2 || (wmode != 0 && wmode != 1) || dstep <= 0) return fail(ctx, FSG_E_ARG, "fsg_set_grid: bad arguments");
     cudaSetDevice(ctx->device);
     ctx->wmode = wmode; ctx->wstart = wstart; ctx->wend = wend; ctx->dstep = dstep; ctx->nwl = nwl;
-    ctx->rstep = dstep / FSG_VC; ctx->wfirst = wstart;
+    ctx->rstep = dstep / FSG_VC; ctx->wfirst = wstart; ctx->wlast = wstart + wave[nwl - 1];
     ALLOC(ctx->d_wave, sizeof(double) * nwl);
     CK(cudaMemcpyAsync(ctx->d_wave.p, wave, sizeof(double) * nwl, cudaMemcpyHostToDevice, ctx->stream), "grid upload");
     CK(cudaStreamSynchronize(ctx->stream), "grid upload");
@@ -1357,6 +1358,139 @@ int fsg_zeeman_pattern(float jlo, float jup, float glo, float gup, int32_t *npi,
     return FSG_OK;
 }
 
+
+// ---- disk integration with broadening (convol.f90:67-300) ------------------------------------------
+// SemiArea (utils.f90:1435-1445): area under the semicircle of radius R from -R to V
+static double semi_area(double R, double V) {
+    if (R <= 0.0) return 0.0;
+    double X = std::max(-R, std::min(R, V));
+    return 0.5 * (X * std::sqrt(std::max(0.0, (R - X) * (R + X))) + R * R * std::asin(X / R));
+}
+
+// Gaussian taps exp(max(-20, -(i - j - 1)^2 / (2 sig^2))), i = 1..2j+1, normalised (convol.f90:186-196, 266-275)
+static std::vector<double> gauss_taps(double sig, int j) {
+    std::vector<double> k(2 * j + 1);
+    double norm = 0.0;
+    for (int i = 1; i <= 2 * j + 1; i++) {
+        double arg = std::max(-20.0, -0.5 * ((i - j - 1) / sig) * ((i - j - 1) / sig));
+        k[i - 1] = std::exp(arg);
+        norm = norm + k[i - 1];
+    }
+    for (auto &v : k) v = v / norm;
+    return k;
+}
+
+int fsg_disk_integ_conv_dev(fsg_ctx *ctx, const double *radii, double vsini, double vmacro, double vgau,
+                            const double *d_spl, const double *d_spc, double *d_sfl, double *d_sfc) {
+    if (!ctx || !radii || !d_spl || !d_spc || !d_sfl || !d_sfc || vsini < 0 || vmacro < 0 || vgau < 0)
+        return fail(ctx, FSG_E_ARG, "fsg_disk_integ_conv_dev: bad arguments");
+    if (!ctx->have_grid || ctx->nmu < 1) return fail(ctx, FSG_E_STATE, "fsg_disk_integ_conv_dev: set grid and mu first");
+    cudaSetDevice(ctx->device);
+    const int nwl = ctx->nwl, nmu = ctx->nmu;
+    std::vector<double> xmu(nmu), wmu(nmu);
+    CK(cudaMemcpy(xmu.data(), ctx->d_xmu.p, sizeof(double) * nmu, cudaMemcpyDeviceToHost), "mu");
+    CK(cudaMemcpy(wmu.data(), ctx->d_wmu.p, sizeof(double) * nmu, cudaMemcpyDeviceToHost), "mu");
+    const double dv = ctx->wmode == 0 ? 2.0 * ctx->dstep / (ctx->wfirst + ctx->wlast) * FSG_VC : ctx->dstep;
+    const double sigma = vmacro / dv / std::sqrt(2.0);
+    const int nmk = std::max(3, std::min((int)(10.0 * sigma), (int)((nwl - 3) / 2)));
+    const int nm = 2 * nmk + 1, nrk_max = 2 * (int)(vsini * std::max(1.0, radii[nmu]) / dv) + 3;
+    ALLOC(ctx->d_cbuf, sizeof(double) * 4 * (size_t)nwl);
+    ALLOC(ctx->d_ctaps, sizeof(double) * (size_t)(nmu * (nrk_max + nm) + 2 * nm + 8));
+    double *tL = ctx->d_cbuf.as<double>(), *tC = tL + nwl, *uL = tC + nwl, *uC = uL + nwl;
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemsetAsync(d_sfl, 0, sizeof(double) * nwl, s), "flux reset");
+    CK(cudaMemsetAsync(d_sfc, 0, sizeof(double) * nwl, s), "flux reset");
+    // all taps of all annuli in one upload: [rotation | macroturbulence] per annulus
+    std::vector<double> taps;
+    std::vector<int> roff(nmu), rn(nmu, 0), moff(nmu), mn(nmu, 0);
+    for (int im = 0; im < nmu; im++) {
+        if (vsini > 0.0) {
+            const double R1 = vsini * radii[im], R2 = vsini * radii[im + 1];
+            const int nrk = 2 * (int)(R2 / dv) + 3;
+            std::vector<double> rk(nrk);
+            double norm = 0.0;
+            for (int i = 1; i <= nrk; i++) {
+                const double V = std::fabs(dv * (i - 1 - (nrk - 1) / 2));
+                rk[i - 1] = semi_area(R2, V + 0.5 * dv) - semi_area(R2, V - 0.5 * dv) - semi_area(R1, V + 0.5 * dv) +
+                            semi_area(R1, V - 0.5 * dv);
+                norm = norm + rk[i - 1];
+            }
+            if (R2 > 0.5 * dv) {                      // otherwise every velocity falls in the central pixel
+                roff[im] = (int)taps.size(); rn[im] = nrk;
+                for (double v : rk) taps.push_back(v / norm);
+            }
+        }
+        if (vmacro > 0.0) {
+            const double sigr = sigma * xmu[im], sigt = sigma * std::sqrt(1.0 - xmu[im] * xmu[im]);
+            std::vector<double> mr(nm, 0.0), mt(nm, 0.0);
+            if (sigr > 0.0) mr = gauss_taps(sigr, nmk); else mr[nmk] = 1.0;
+            if (sigt > 0.0) mt = gauss_taps(sigt, nmk); else mt[nmk] = 1.0;
+            moff[im] = (int)taps.size(); mn[im] = nm;
+            for (int i = 0; i < nm; i++) taps.push_back(0.5 * mr[i] + 0.5 * mt[i]);
+        }
+    }
+    const int unit = (int)taps.size();
+    taps.push_back(1.0);
+    int goff = 0, gn = 0;
+    if (vgau > 0.0) {
+        double fwhm = vgau > 1000.0 ? FSG_VC / vgau : vgau;
+        double sp = ctx->wmode == 0 ? fwhm * (ctx->wfirst + ctx->wlast) / FSG_VC / 2.0 / ctx->dstep : fwhm / ctx->dstep;
+        double sig = sp / (2.0 * std::sqrt(2.0 * std::log(2.0)));
+        int j = std::max(3, std::min((int)(10.0 * sig), (int)((nwl - 3.0) / 2.0)));
+        std::vector<double> gk = gauss_taps(sig, j);
+        goff = (int)taps.size(); gn = 2 * j + 1;
+        for (double v : gk) taps.push_back(v);
+    }
+    ALLOC(ctx->d_ctaps, sizeof(double) * taps.size());
+    CK(cudaMemcpyAsync(ctx->d_ctaps.p, taps.data(), sizeof(double) * taps.size(), cudaMemcpyHostToDevice, s), "taps");
+    const double *dk = ctx->d_ctaps.as<double>();
+    for (int im = 0; im < nmu; im++) {
+        // SiL, SiC: the annulus intensities (stride nmu), rotation, macroturbulence, then the flux sum
+        const double *iL = d_spl + im, *iC = d_spc + im;
+        int st = nmu;
+        if (rn[im]) {
+            fsg_launch_conv(s, nwl, iL, st, dk + roff[im], rn[im], tL, nullptr, 0.0);
+            fsg_launch_conv(s, nwl, iC, st, dk + roff[im], rn[im], tC, nullptr, 0.0);
+            iL = tL; iC = tC; st = 1;
+        }
+        if (mn[im]) {
+            double *oL = (iL == tL) ? uL : tL, *oC = (iC == tC) ? uC : tC;
+            fsg_launch_conv(s, nwl, iL, st, dk + moff[im], mn[im], oL, nullptr, 0.0);
+            fsg_launch_conv(s, nwl, iC, st, dk + moff[im], mn[im], oC, nullptr, 0.0);
+            iL = oL; iC = oC; st = 1;
+        }
+        // SfL = SfL + SiL Wmu (convol.f90:230-231)
+        fsg_launch_conv(s, nwl, iL, st, dk + unit, 1, d_sfl, d_sfl, wmu[im]);
+        fsg_launch_conv(s, nwl, iC, st, dk + unit, 1, d_sfc, d_sfc, wmu[im]);
+        ctx->launches += 2 + (rn[im] ? 2 : 0) + (mn[im] ? 2 : 0);
+    }
+    if (gn) {                                           // ConvolGau of the flux (convol.f90:236-240)
+        CK(cudaMemcpyAsync(tL, d_sfl, sizeof(double) * nwl, cudaMemcpyDeviceToDevice, s), "gau");
+        CK(cudaMemcpyAsync(tC, d_sfc, sizeof(double) * nwl, cudaMemcpyDeviceToDevice, s), "gau");
+        fsg_launch_conv(s, nwl, tL, 1, dk + goff, gn, d_sfl, nullptr, 0.0);
+        fsg_launch_conv(s, nwl, tC, 1, dk + goff, gn, d_sfc, nullptr, 0.0);
+        ctx->launches += 2;
+    }
+    CK(cudaGetLastError(), "disk integration");
+    CK(cudaStreamSynchronize(s), "disk integration");
+    return FSG_OK;
+}
+
+int fsg_disk_integ_conv(fsg_ctx *ctx, const double *radii, double vsini, double vmacro, double vgau, double *sfl,
+                        double *sfc) {
+    if (!ctx || !sfl || !sfc) return fail(ctx, FSG_E_ARG, "fsg_disk_integ_conv: null output");
+    cudaSetDevice(ctx->device);
+    size_t nsp = sizeof(double) * (size_t)ctx->nwl * std::max(ctx->nmu, 1), nf = sizeof(double) * ctx->nwl;
+    ALLOC(ctx->d_spl, nsp); ALLOC(ctx->d_spc, nsp); ALLOC(ctx->d_sfl, nf); ALLOC(ctx->d_sfc, nf);
+    int rc = radtran_dev(ctx, ctx->d_spl.as<double>(), ctx->d_spc.as<double>(), nullptr, nullptr);
+    if (rc) return rc;
+    rc = fsg_disk_integ_conv_dev(ctx, radii, vsini, vmacro, vgau, ctx->d_spl.as<double>(), ctx->d_spc.as<double>(),
+                                 ctx->d_sfl.as<double>(), ctx->d_sfc.as<double>());
+    if (rc) return rc;
+    CK(cudaMemcpy(sfl, ctx->d_sfl.p, nf, cudaMemcpyDeviceToHost), "flux");
+    CK(cudaMemcpy(sfc, ctx->d_sfc.p, nf, cudaMemcpyDeviceToHost), "flux");
+    return FSG_OK;
+}
 
 // ---- derivatives of the flux (adjoint of RadTranCalc + DiskInteg and of the line opacity) --------
 int fsg_set_fractionpf(fsg_ctx *ctx, const float *fractionpf) {

@@ -778,3 +778,26 @@ void fsg_launch_mark_wide(cudaStream_t s, const AtmView &A, int64_t n, const dou
                           int32_t *flags, const int32_t *ileft, const int32_t *iright, unsigned long long *nwide) {
     if (n > 0) k_mark_wide<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(A, n, wl, nstep, flags, ileft, iright, nwide);
 }
+
+// ================================================================================================
+// Convolution with a short kernel over a spectrum padded with its end values (convol.f90:143-165,
+// 206-227, 277-294): out(i) = sum_j in(clamp(i + j - h)) kern(j), h = (n - 1) / 2, in order of j;
+// with acc: out(i) = acc(i) + sum * w (the flux sum of the annuli).  One thread per wavelength.
+// ================================================================================================
+__global__ void k_conv(int nwl, const double *__restrict__ in, int st, const double *__restrict__ kern, int n,
+                       double *out, const double *acc, double w) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nwl) return;
+    const int h = (int)((n - 1.0) / 2.0);
+    double sm = 0.0;
+    for (int j = 0; j < n; j++) {
+        int m = min(max(i + j - h, 0), nwl - 1);
+        sm = sm + in[(size_t)m * st] * kern[j];
+    }
+    out[i] = acc ? acc[i] + sm * w : sm;
+}
+
+void fsg_launch_conv(cudaStream_t s, int nwl, const double *in, int st, const double *kern, int n, double *out,
+                     const double *acc, double w) {
+    if (nwl > 0) k_conv<<<(nwl + 255) / 256, 256, 0, s>>>(nwl, in, st, kern, n, out, acc, w);
+}

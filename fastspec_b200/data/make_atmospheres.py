@@ -419,6 +419,43 @@ def make_linst_pins(gold):
         print(name, "line strengths", int(sel.sum()), "of", extra.n, "seeded lines")
 
 
+def make_convol_pin(gold):
+    """Broadening fixtures: the reference's intensities (fs_spec.bin) and its broadened flux
+    (fs_flux.bin, IntegConvol / DiskInteg with CONVOL = Vsini, Vmacro, Vgau) of the same run, for
+    a Wmode 0 and a Wmode 1 grid and several broadening settings."""
+    cases = [
+        # name, atmosphere, lines, (wstart, wend, step, wmode), convol settings
+        ("solar", "solar", lambda: W.atomic_lines(160, 5040.5, 5044.5, W.SEED0 + 0), (5040.0, 5045.0, 0.005, 0),
+         [(30.0, 4.0, 60000.0), (0.0, 3.0, 0.0), (12.0, 0.0, 0.0), (0.0, 0.0, 0.15)]),
+        ("cooldwarf", "cooldwarf", lambda: W.molecular_lines(400, 9040.5, 9046.5, W.SEED0 + 1),
+         (9040.0, 9047.0, 0.3, 1), [(8.0, 2.0, 3.0), (25.0, 0.0, 100000.0)]),
+    ]
+    out = {}
+    for name, atmname, mk, grid, settings in cases:
+        teff, logg, ntau, species, ismol, _, _, vmic, molbrd, _, _ = CONFIGS[atmname]
+        model = W.eddington_model(teff, logg, ntau)
+        lines = mk()
+        for k, (vs, vm, vg) in enumerate(settings):
+            with tempfile.TemporaryDirectory() as wd:
+                W.write_krz(os.path.join(wd, "model.krz"), model)
+                lines.write_z(os.path.join(wd, "lines.z"), grid[0], grid[1])
+                deck = ("wave=%.4f, %.4f, %.6f, %d\nsave=0, 0, 0, 1, 1\nvmic=%.3f\nmolbrd=%d\n"
+                        "lines=\n-1  lines.z\n\nmodel=model.krz\nmus=7\nconvol=%g, %g, %g\n"
+                        % (grid[0], grid[1], grid[2], grid[3], vmic, molbrd, vs, vm, vg))
+                run_ref(wd, deck)
+                sp = fsio.read_spec(os.path.join(wd, "fs_spec.bin"))
+                fl = fsio.read_flux(os.path.join(wd, "fs_flux.bin"))
+            key = "%s_%d" % (name, k)
+            out[key + "_spl"] = sp["spl"]; out[key + "_spc"] = sp["spc"]
+            out[key + "_sfl"] = fl["sfl"]; out[key + "_sfc"] = fl["sfc"]
+            out[key + "_wave"] = fl["wave"] if "wave" in fl else sp["wave"]
+            out[key + "_xmu"] = sp["xmu"]
+            out[key + "_grid"] = np.array(grid, np.float64)
+            out[key + "_convol"] = np.array([vs, vm, vg], np.float64)
+    np.savez_compressed(os.path.join(gold, "pin_convol.npz"), **out)
+    print("pin_convol", sorted(set(k.rsplit("_", 1)[0] for k in out)))
+
+
 def mirrored_components(patterns):
     """Zeeman components as ReadAscMag stores an explicit block with a positive sigma count:
     pi as read, sigma mirrored (blue = -shift first, then red), ioutils.f90:1393-1410."""
@@ -490,6 +527,8 @@ def make_mag_pin(gold):
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "magpin":
         make_mag_pin(os.path.join(REPO, "tests", "golden"))
+    elif len(sys.argv) > 1 and sys.argv[1] == "convol":
+        make_convol_pin(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "linst":
         make_linst_pins(os.path.join(REPO, "tests", "golden"))
     else:

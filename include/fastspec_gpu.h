@@ -154,6 +154,16 @@ int fsg_set_mu(fsg_ctx *ctx, int nmu, const double *xmu, const double *wmu);
 int fsg_radtran(fsg_ctx *ctx, double *spl, double *spc, double *sfl, double *sfc);
 int fsg_radtran_dev(fsg_ctx *ctx, double *d_spl, double *d_spc, double *d_sfl, double *d_sfc);
 
+/* DiskInteg with broadening (convol.f90:67-300): rotation (vsini [km/s], annulus kernels from the
+ * nmu + 1 projected radii of fsg_mu_quadrature), radial-tangential macroturbulence (vmacro
+ * [km/s]), then Gaussian broadening of the flux (vgau: FWHM [km/s], or a resolving power when
+ * > 1000).  _dev: spl/spc [nwl][nmu] and sfl/sfc [nwl] on the device; the host form runs
+ * RadTranCalc on the device LineOpac first and returns the broadened flux. */
+int fsg_disk_integ_conv_dev(fsg_ctx *ctx, const double *radii, double vsini, double vmacro, double vgau,
+                            const double *d_spl, const double *d_spc, double *d_sfl, double *d_sfc);
+int fsg_disk_integ_conv(fsg_ctx *ctx, const double *radii, double vsini, double vmacro, double vgau,
+                        double *sfl, double *sfc);
+
 /* ---- magnetic path ---------------------------------------------------------------------- */
 /* MagLineopCalc (synth.f90:1098-1455): bframe/bfield as BFRAME/BFIELD (3 values for frames
  * 0/1, 2*nmu+1 for frame 2).  Accumulates the device MagLineOpac [nwl][ntau][6].  linstr as for

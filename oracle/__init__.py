@@ -356,6 +356,33 @@ def disk_integ(wmu, spl, spc):
     return sfl, sfc
 
 
+def grid_dv(grid, wave_abs):
+    """Velocity step of the grid as DiskInteg takes it (convol.f90:86-91)."""
+    if grid["wmode"] == 0:
+        return 2.0 * grid["dstep"] / (wave_abs[0] + wave_abs[-1]) * 299792.458
+    return grid["dstep"]
+
+
+def gauss_sigma_pix(grid, wave_abs, vgau):
+    """ConvolGau's Fwhm / step in pixels (convol.f90:259-264); vgau > 1000 is a resolving power."""
+    if vgau > 1000:
+        vgau = 299792.458 / vgau
+    if grid["wmode"] == 0:
+        return vgau * (wave_abs[0] + wave_abs[-1]) / 299792.458 / 2.0 / grid["dstep"]
+    return vgau / grid["dstep"]
+
+
+def disk_integ_conv(xmu, wmu, radii, spl, spc, dv, vsini, vmacro, gsig):
+    """DiskInteg with rotation, radial-tangential macroturbulence and Gaussian broadening."""
+    xmu = _f64(xmu); wmu = _f64(wmu); radii = _f64(radii); spl = _f64(spl); spc = _f64(spc)
+    nwl, nmu = spl.shape
+    sfl = np.zeros(nwl); sfc = np.zeros(nwl)
+    lib().or_disk_integ_conv(nmu, nwl, _p(xmu, C.c_double), _p(wmu, C.c_double), _p(radii, C.c_double),
+                             C.c_double(dv), C.c_double(vsini), C.c_double(vmacro), C.c_double(gsig),
+                             _p(spl, C.c_double), _p(spc, C.c_double), _p(sfl, C.c_double), _p(sfc, C.c_double))
+    return sfl, sfc
+
+
 def zeeman_pattern(jlo, jup, glo, gup):
     m = int(round(2 * jup)) + 1
     npi, nsi = C.c_int(), C.c_int()

@@ -1394,3 +1394,126 @@ void or_zeeman_pattern(float jlo, float jup, float glo, float gup, int *npi, flo
     for (int i = 0; i < Np; i++) { spi[i] = (float)gp[i]; rpi[i] = (float)rp[i]; }
     for (int i = 0; i < Ns; i++) { ssig[i] = (float)gs[i]; rsig[i] = (float)rs[i]; }
 }
+
+
+/* ---- disk integration with broadening (convol.f90:67-300) ------------------------------------ */
+
+/* SemiArea (utils.f90:1435-1445): area under a semicircle of radius R from -R to V */
+static double semi_area(double R, double V) {
+    if (R <= 0.0) return 0.0;
+    double X = fmax(-R, fmin(R, V));
+    return 0.5 * (X * sqrt(fmax(0.0, (R - X) * (R + X))) + R * R * asin(X / R));
+}
+
+/* out(i) = sum_j T(i + j - 1 - h) kern(j), T the spectrum padded with its end values, h = (n - 1) / 2;
+ * in/out with stride st between wavelengths */
+static void conv_padded(int nwl, const double *in, int st_in, const double *kern, int n, double *out) {
+    int h = (int)((n - 1.0) / 2.0);
+    for (int i = 0; i < nwl; i++) {
+        double sm = 0.0;
+        for (int j = 0; j < n; j++) {
+            int m = i + j - h;
+            m = m < 0 ? 0 : (m >= nwl ? nwl - 1 : m);
+            sm = sm + in[(size_t)m * st_in] * kern[j];
+        }
+        out[i] = sm;
+    }
+}
+
+static int gauss_kernel(double sig, int nmax, double *k) {   /* returns Ng = 2 j + 1 */
+    int j = (int)(10.0 * sig);
+    int lim = (int)((nmax - 3.0) / 2.0);
+    if (j > lim) j = lim;
+    if (j < 3) j = 3;
+    int ng = 2 * j + 1;
+    double norm = 0.0;
+    for (int i = 1; i <= ng; i++) {
+        double arg = fmax(-20.0, -0.5 * ((i - j - 1) / sig) * ((i - j - 1) / sig));
+        k[i - 1] = exp(arg);
+        norm = norm + k[i - 1];
+    }
+    for (int i = 0; i < ng; i++) k[i] = k[i] / norm;
+    return ng;
+}
+
+void or_convol_gau(int nw, double *S, double sigma_pix) {
+    double sig = sigma_pix / (2.0 * sqrt(2.0 * log(2.0)));
+    int j = (int)(10.0 * sig), lim = (int)((nw - 3.0) / 2.0);
+    if (j > lim) j = lim;
+    if (j < 3) j = 3;
+    double *k = (double *)malloc(sizeof(double) * (2 * j + 1));
+    double *T = (double *)malloc(sizeof(double) * nw);
+    int ng = 2 * j + 1;
+    double norm = 0.0;
+    for (int i = 1; i <= ng; i++) {
+        double arg = fmax(-20.0, -0.5 * ((i - j - 1) / sig) * ((i - j - 1) / sig));
+        k[i - 1] = exp(arg);
+        norm = norm + k[i - 1];
+    }
+    for (int i = 0; i < ng; i++) k[i] = k[i] / norm;
+    memcpy(T, S, sizeof(double) * nw);
+    conv_padded(nw, T, 1, k, ng, S);
+    free(k); free(T);
+}
+
+void or_disk_integ_conv(int nmu, int nwl, const double *xmu, const double *wmu, const double *radii, double dv,
+                        double vsini, double vmacro, double gsig, const double *spl, const double *spc,
+                        double *sfl, double *sfc) {
+    double sigma = vmacro / dv / sqrt(2.0);
+    int nmk = (int)(10.0 * sigma), lim = (int)((nwl - 3) / 2);
+    if (nmk > lim) nmk = lim;
+    if (nmk < 3) nmk = 3;
+    int nm = 2 * nmk + 1;
+    int nrk_max = 2 * (int)(vsini / dv) + 3;
+    double *rk = (double *)malloc(sizeof(double) * (nrk_max + 2));
+    double *mk = (double *)malloc(sizeof(double) * nm), *mr = (double *)malloc(sizeof(double) * nm);
+    double *mt = (double *)malloc(sizeof(double) * nm);
+    double *siL = (double *)malloc(sizeof(double) * nwl), *siC = (double *)malloc(sizeof(double) * nwl);
+    double *tL = (double *)malloc(sizeof(double) * nwl), *tC = (double *)malloc(sizeof(double) * nwl);
+    for (int i = 0; i < nwl; i++) { sfl[i] = 0.0; sfc[i] = 0.0; }
+    for (int im = 0; im < nmu; im++) {
+        for (int i = 0; i < nwl; i++) { siL[i] = spl[(size_t)i * nmu + im]; siC[i] = spc[(size_t)i * nmu + im]; }
+        if (vsini > 0.0) {
+            double R1 = vsini * radii[im], R2 = vsini * radii[im + 1];
+            int nrk = 2 * (int)(R2 / dv) + 3;
+            double norm = 0.0;
+            for (int i = 1; i <= nrk; i++) {
+                double V = fabs(dv * (i - 1 - (nrk - 1) / 2));
+                rk[i - 1] = semi_area(R2, V + 0.5 * dv) - semi_area(R2, V - 0.5 * dv) -
+                            semi_area(R1, V + 0.5 * dv) + semi_area(R1, V - 0.5 * dv);
+                norm = norm + rk[i - 1];
+            }
+            for (int i = 0; i < nrk; i++) rk[i] = rk[i] / norm;
+            if (R2 > 0.5 * dv) {
+                memcpy(tL, siL, sizeof(double) * nwl); memcpy(tC, siC, sizeof(double) * nwl);
+                conv_padded(nwl, tL, 1, rk, nrk, siL);
+                conv_padded(nwl, tC, 1, rk, nrk, siC);
+            }
+        }
+        if (vmacro > 0.0) {
+            double sigr = sigma * xmu[im], sigt = sigma * sqrt(1.0 - xmu[im] * xmu[im]);
+            double nr = 0.0, nt = 0.0;
+            for (int i = 1; i <= nm; i++) {
+                if (sigr > 0.0) {
+                    double a = fmax(-20.0, -0.5 * ((i - nmk - 1) / sigr) * ((i - nmk - 1) / sigr));
+                    mr[i - 1] = exp(a); nr = nr + mr[i - 1];
+                }
+                if (sigt > 0.0) {
+                    double a = fmax(-20.0, -0.5 * ((i - nmk - 1) / sigt) * ((i - nmk - 1) / sigt));
+                    mt[i - 1] = exp(a); nt = nt + mt[i - 1];
+                }
+            }
+            for (int i = 0; i < nm; i++) {
+                mr[i] = sigr > 0.0 ? mr[i] / nr : (i == nmk ? 1.0 : 0.0);
+                mt[i] = sigt > 0.0 ? mt[i] / nt : (i == nmk ? 1.0 : 0.0);
+                mk[i] = 0.5 * mr[i] + 0.5 * mt[i];
+            }
+            memcpy(tL, siL, sizeof(double) * nwl); memcpy(tC, siC, sizeof(double) * nwl);
+            conv_padded(nwl, tL, 1, mk, nm, siL);
+            conv_padded(nwl, tC, 1, mk, nm, siC);
+        }
+        for (int i = 0; i < nwl; i++) { sfl[i] = sfl[i] + siL[i] * wmu[im]; sfc[i] = sfc[i] + siC[i] * wmu[im]; }
+    }
+    if (gsig > 0.0) { or_convol_gau(nwl, sfl, gsig); or_convol_gau(nwl, sfc, gsig); }
+    free(rk); free(mk); free(mr); free(mt); free(siL); free(siC); free(tL); free(tC);
+}

@@ -137,6 +137,15 @@ void or_mag_radtran(const or_state *s, int nmu, const double *xmu, int bframe,
 /* Quadrature (utils.f90:1273-1431) and disk integration (convol.f90:67-246, no broadening) */
 int  or_mu_quadrature(int quad, int n, double *x, double *w, double *r, int setnodes);
 void or_gauss_mu(int quad, int n, double *x, double *w);
+/* DiskInteg with broadening (convol.f90:67-246) and ConvolGau (convol.f90:249-300).  dv: velocity
+ * step of the grid [km/s] (2 Dstep / (Wfirst + Wlast) c for Wmode 0, Dstep for Wmode 1); gsig: the
+ * Gaussian sigma in pixels of ConvolGau before the FWHM->sigma factor (Fwhm / step).  radii: the
+ * nmu + 1 projected annulus radii of MuQuadrature.  spl/spc [nwl][nmu] in, sfl/sfc [nwl] out. */
+void or_disk_integ_conv(int nmu, int nwl, const double *xmu, const double *wmu, const double *radii, double dv,
+                        double vsini, double vmacro, double gsig, const double *spl, const double *spc,
+                        double *sfl, double *sfc);
+/* ConvolGau of one spectrum in place (convol.f90:249-300); sigma_pix = Fwhm / step. */
+void or_convol_gau(int nw, double *S, double sigma_pix);
 void or_disk_integ(int nmu, int nwl, const double *wmu, const double *spl, const double *spc,
                    double *sfl, double *sfc);
 

@@ -120,3 +120,26 @@ def test_oracle_magnetic_pins_reference(oracle_mod):
     x, w, _ = oracle_mod.mu_quadrature(1, len(d["xmu"]))
     sfl, sfc = oracle_mod.disk_integ(w, spz[i0:i1 + 1, 0], spc[i0:i1 + 1])
     assert np.max(np.abs(sfl / d["sfl"] - 1)) < 1e-8
+
+
+def convol_cases():
+    d = H.load_pin("pin_convol")
+    return d, sorted(set(k.rsplit("_", 1)[0] for k in d))
+
+
+@pytest.mark.parametrize("case", ["solar_0", "solar_1", "solar_2", "solar_3", "cooldwarf_0", "cooldwarf_1"])
+def test_oracle_disk_integ_convol_pins_reference(oracle_mod, case):
+    """DiskInteg with rotation, radial-tangential macroturbulence and Gaussian broadening
+    (convol.f90:67-300) of the reference's own intensities against its broadened flux."""
+    d = H.load_pin("pin_convol")
+    g = d[case + "_grid"]
+    grid = dict(wmode=int(g[3]), wstart=g[0], wend=g[1], dstep=g[2])
+    vs, vm, vg = d[case + "_convol"]
+    x, w, r = oracle_mod.mu_quadrature(1, 7)
+    assert np.max(np.abs(x - d[case + "_xmu"])) == 0.0
+    wave = d[case + "_wave"]
+    dv = oracle_mod.grid_dv(grid, wave)
+    gsig = oracle_mod.gauss_sigma_pix(grid, wave, vg) if vg > 0 else 0.0
+    sfl, sfc = oracle_mod.disk_integ_conv(x, w, r, d[case + "_spl"], d[case + "_spc"], dv, vs, vm, gsig)
+    assert np.max(np.abs(sfl / d[case + "_sfl"] - 1)) < 1e-12
+    assert np.max(np.abs(sfc / d[case + "_sfc"] - 1)) < 1e-12
