@@ -54,7 +54,7 @@ __device__ __forceinline__ float hv_cf32(float av, float a, float cop) {
 // register partials, then Kahan-adds every partial into its (sum, compensation) pair in shared
 // memory.  The partials carry at most FOLD terms, so their rounding stays at the FP32 unit
 // roundoff of a few terms; the Kahan pairs carry the long sums.
-#define FOLD 16
+#define FOLD 32
 // Candidate lines staged per TMA bulk copy (double-buffered)
 #define CH 32
 // Bound on an mbarrier wait: one second of %globaltimer (a chunk's copy completes in microseconds),
@@ -395,7 +395,7 @@ int fsg_launch_accum_batch(cudaStream_t st, int P, int ntau_max, const WingJob *
 // elsewhere.  A CTA owns 32 wavelengths x all depths, warp w depths [w*CORE_D, w*CORE_D + CORE_D),
 // lane l wavelength tile0 + l; Kahan sums in registers.  The four table entries of a lerp come in
 // one 16-byte load from the cell-major copy of VgtTab.
-#define CORE_D 8
+#define CORE_D 4
 
 __device__ __forceinline__ float hv_core32(const float4 *__restrict__ vtab4, float av, const CoreRec &c, float twoA) {
     if (c.ia > 0 && av < 8.0f) {
@@ -466,14 +466,14 @@ __device__ __forceinline__ void core_tile(const CoreJob &J, int tile, const floa
         if (d < nd) dst[d] = dst[d] + ((double)sum[d] - (double)cmp[d]);
 }
 
-__global__ void __launch_bounds__(512)
+__global__ void __launch_bounds__(1024)
 k_core_fast(CoreJob J, const float4 *__restrict__ vtab4) {
     core_tile(J, blockIdx.x, vtab4);
 }
 
 // persistent form: each warp takes (job, tile) items from the queue and does its depths of them;
 // a CTA of nwarps warps covers nwarps * CORE_D depths, so every item is taken by whole CTAs
-__global__ void __launch_bounds__(512)
+__global__ void __launch_bounds__(1024)
 k_core_batch(const CoreJob *__restrict__ jobs, const int *__restrict__ tile0, int njobs,
              const float4 *__restrict__ vtab4, unsigned *queue) {
     __shared__ int s_item;
@@ -494,7 +494,7 @@ int fsg_launch_core_fast(cudaStream_t st, int ntau, int nwl, const double *wave,
                          const WingRec *wing, const CoreRec *core, const int *tile_lo, const int *tile_hi,
                          const float4 *vtab4, double *lineopac) {
     const int ntiles = (nwl + 31) / 32;
-    const int nwarps = (ntau + CORE_D - 1) / CORE_D;     // ntau <= 128: at most 16 warps
+    const int nwarps = (ntau + CORE_D - 1) / CORE_D;     // ntau <= 128: at most 32 warps
     CoreJob J{ ntau, nwl, wave, hdr, wing, core, tile_lo, tile_hi, lineopac };
     k_core_fast<<<ntiles, 32 * nwarps, 0, st>>>(J, vtab4);
     return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
