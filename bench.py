@@ -57,6 +57,7 @@ def parse():
     p.add_argument("--batch-atm", type=int, default=256)
     p.add_argument("--batch-lines", type=float, default=2e6)
     p.add_argument("--no-fit", action="store_true", help="skip the differentiable-fit measurement")
+    p.add_argument("--no-stokes", action="store_true", help="skip the polarised (Stokes) synthesis measurement")
     return p.parse_args()
 
 
@@ -282,9 +283,21 @@ def differentiable_fit(F, torch, dev, steps, warmup):
         c.backward()
         return float(c.detach()), lg.grad, da.grad, vm.grad
 
+    def forward_only():
+        with torch.no_grad():
+            f = AD.synth_flux(M, torch.tensor(loggf0), torch.zeros(ne, dtype=torch.float64),
+                              torch.tensor(float(d["vmicro"])))
+            return float((((f - fobs) * 300.0) ** 2).sum())
+
     for _ in range(warmup):
         step_fn()
+        forward_only()
     torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        forward_only()
+    torch.cuda.synchronize()
+    ms_fwd = (time.perf_counter() - t0) * 1e3 / steps
     t0 = time.perf_counter()
     for _ in range(steps):
         c, gl, ga, gv = step_fn()
@@ -292,10 +305,57 @@ def differentiable_fit(F, torch, dev, steps, warmup):
     ms = (time.perf_counter() - t0) * 1e3 / steps
     out = {"config": "solar-like 56-depth atmosphere, 1e5 atomic lines 4800-5300 A at 0.005 A (%d wavelengths), "
                      "7 mu; chi-square gradients w.r.t. 30 abundances, 1e5 log gf, vmicro" % M.C.nwl,
-           "steps_per_s": 1e3 / ms, "ms_per_step": ms, "chi2": c, "n_params": int(len(loggf0) + ne + 1),
+           "steps_per_s": 1e3 / ms, "ms_per_step": ms, "ms_forward": ms_fwd, "gradient_cost_over_forward": ms / ms_fwd,
+           "chi2": c, "n_params": int(len(loggf0) + ne + 1),
            "grad_norm_loggf": float(torch.linalg.norm(gl)), "grad_vmicro": float(gv),
            "timing": "wall clock of forward + adjoint per step with device synchronisation"}
     M.close()
+    return out
+
+
+def stokes_synthesis(F, torch, dev, steps, warmup):
+    """The polarised configuration: 5000 Zeeman lines over 6000-6100 A at 0.002 A (50,001
+    wavelengths), the Teff = 5000 K, log g = 4.5 atmosphere (56 depths), BFRAME 1 with |B| = 2 kG at
+    inclination 60 deg and azimuth 30 deg, 9 angles: MagLineopCalc (FP64) + MagRadTranCalc (4x4
+    DELO-Bezier) + Stokes-I flux, host arrays in and out."""
+    from fastspec_b200 import workloads as W
+    d = np.load(os.path.join(HERE, "fastspec_b200", "data", "atm_magnetic.npz"))
+    st = {k: d[k] for k in ("rhox", "T", "xne", "xna", "rho", "fractionpf", "xamass", "potion", "ion", "frac_h1",
+                            "frac_he1")}
+    w0, w1, step = 6000.0, 6100.0, 0.002
+    wave = F.make_grid(0, w0, w1, step) + w0
+    lk = np.log(d["cont_opac"])
+    co = np.exp(np.stack([np.interp(wave, d["cont_wave"], lk[:, t]) for t in range(lk.shape[1])], axis=1))
+    L = W.zeeman_lines(5000, w0, w1, W.SEED0 + 2)
+    z = W.zeeman_components(L, F.zeeman_pattern)
+    LL = F.LineList.from_arrays(L.arrays(), zeeman=z)
+    C = F.Context(device=dev, precision=F.PREC_FP64, vmicro=float(d["vmicro"]))
+    C.set_grid(0, w0, w1, step)
+    C.set_atmosphere(st)
+    C.set_contopac(co)
+    x, w, _ = F.mu_quadrature(1, 9)
+    C.set_mu(x, w)
+    bf = [2000.0, 60.0, 30.0]
+
+    def one():
+        C._ck(C._lib.fsg_mag_lineop_reset(C.h), "reset")
+        r = C.mag_lineop_calc(LL, 1, bf, want=False)
+        C.mag_radtran(1, bf)
+        return r["stats"]
+
+    for _ in range(warmup):
+        one()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        stt = one()
+    ms = (time.perf_counter() - t0) * 1e3 / steps
+    out = {"config": "5000 Zeeman lines 6000-6100 A at 0.002 A (%d wavelengths), 56 depths, BFRAME 1 2 kG 60/30 deg, "
+                     "9 mu, FP64 opacity + 4x4 DELO-Bezier" % C.nwl,
+           "spectra_per_s": 1e3 / ms, "ms_per_spectrum": ms, "line_evals": stt["line_evals"],
+           "line_evals_per_s": stt["line_evals"] / (ms / 1e3),
+           "ms_lineop": stt["ms_total"], "timing": "wall clock per Stokes IQUV synthesis, host arrays in and out"}
+    C.close()
     return out
 
 
@@ -434,6 +494,8 @@ def run_gpu(args, rank, world):
     del dt
     if not args.no_plain and rank == 0:
         out["plain"] = plain_vs_mixed(F, torch, st, meta, co, dev, int(args.plain_lines))
+    if not args.no_stokes and rank == 0:
+        out["stokes"] = stokes_synthesis(F, torch, dev, args.steps, args.warmup)
     if not args.no_fit and rank == 0:
         out["fit"] = differentiable_fit(F, torch, dev, args.steps, args.warmup)
     if not args.no_batched and rank == 0:
@@ -678,6 +740,8 @@ def main():
         line["batched"] = r["batched"]
     if "fit" in r:
         line["differentiable_fit"] = r["fit"]
+    if "stokes" in r:
+        line["stokes"] = r["stokes"]
     print(json.dumps(line))
 
 

@@ -261,6 +261,25 @@ def zeeman_lines(n, wmin, wmax, seed):
     return L
 
 
+def zeeman_components(L, pattern):
+    """Zeeman components of a zeeman_lines list in the CSR form of fsg_lines: pi as the pattern gives
+    them, sigma mirrored (blue = -shift first, then red) as the reader stores an explicit block
+    (ioutils.f90:1393-1410).  pattern(jlo, jup, glo, gup) -> (pi shifts, pi strengths, sigma shifts,
+    sigma strengths), e.g. fastspec_b200.zeeman_pattern; a line without pi or sigma components
+    takes the normal triplet of J 1 -> 0, g = 1."""
+    jlo, jup, glo, gup = L.zeeman
+    npi, nsi, spl_pi, str_pi, spl_si, str_si = [], [], [], [], [], []
+    for i in range(L.n):
+        spi, rpi, ss, rs = pattern(float(jlo[i]), float(jup[i]), float(glo[i]), float(gup[i]))
+        if len(spi) == 0 or len(ss) == 0:
+            spi, rpi, ss, rs = pattern(1.0, 0.0, 1.0, 1.0)
+        npi.append(len(spi)); nsi.append(2 * len(ss))
+        spl_pi += list(spi); str_pi += list(rpi)
+        spl_si += list(-np.asarray(ss)) + list(ss); str_si += list(rs) + list(rs)
+    f = lambda a: np.asarray(a, np.float32)
+    return (np.asarray(npi, np.int32), np.asarray(nsi, np.int32), f(spl_pi), f(str_pi), f(spl_si), f(str_si))
+
+
 # ---- batched grid: many atmospheres sharing one atomic line list -------------------------------
 # Element of each config-0 species and the solar-state file the batch states are derived from.
 _BATCH_ELEMENTS = ["Fe", "Ti", "Cr", "Ni", "Ca"]
