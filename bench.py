@@ -329,33 +329,43 @@ def stokes_synthesis(F, torch, dev, steps, warmup):
     L = W.zeeman_lines(5000, w0, w1, W.SEED0 + 2)
     z = W.zeeman_components(L, F.zeeman_pattern)
     LL = F.LineList.from_arrays(L.arrays(), zeeman=z)
-    C = F.Context(device=dev, precision=F.PREC_FP64, vmicro=float(d["vmicro"]))
-    C.set_grid(0, w0, w1, step)
-    C.set_atmosphere(st)
-    C.set_contopac(co)
     x, w, _ = F.mu_quadrature(1, 9)
-    C.set_mu(x, w)
     bf = [2000.0, 60.0, 30.0]
+    out = {"config": "5000 Zeeman lines 6000-6100 A at 0.002 A, 56 depths, BFRAME 1 2 kG 60/30 deg, 9 mu, "
+                     "4x4 DELO-Bezier; host arrays in and out",
+           "timing": "wall clock per Stokes IQUV synthesis (MagLineopCalc + MagRadTranCalc + Stokes-I flux)"}
+    spz = {}
+    for name, prec in (("fp64", F.PREC_FP64), ("mixed", F.PREC_MIXED)):
+        C = F.Context(device=dev, precision=prec, vmicro=float(d["vmicro"]))
+        C.set_grid(0, w0, w1, step)
+        C.set_atmosphere(st)
+        C.set_contopac(co)
+        C.set_mu(x, w)
 
-    def one():
-        C._ck(C._lib.fsg_mag_lineop_reset(C.h), "reset")
-        r = C.mag_lineop_calc(LL, 1, bf, want=False)
-        C.mag_radtran(1, bf)
-        return r["stats"]
+        def one():
+            C._ck(C._lib.fsg_mag_lineop_reset(C.h), "reset")
+            r = C.mag_lineop_calc(LL, 1, bf, want=False)
+            sp = C.mag_radtran(1, bf)
+            return r["stats"], sp
 
-    for _ in range(warmup):
-        one()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        stt = one()
-    ms = (time.perf_counter() - t0) * 1e3 / steps
-    out = {"config": "5000 Zeeman lines 6000-6100 A at 0.002 A (%d wavelengths), 56 depths, BFRAME 1 2 kG 60/30 deg, "
-                     "9 mu, FP64 opacity + 4x4 DELO-Bezier" % C.nwl,
-           "spectra_per_s": 1e3 / ms, "ms_per_spectrum": ms, "line_evals": stt["line_evals"],
-           "line_evals_per_s": stt["line_evals"] / (ms / 1e3),
-           "ms_lineop": stt["ms_total"], "timing": "wall clock per Stokes IQUV synthesis, host arrays in and out"}
-    C.close()
+        for _ in range(warmup):
+            one()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            stt, sp = one()
+        ms = (time.perf_counter() - t0) * 1e3 / steps
+        spz[name] = sp
+        out[name] = {"spectra_per_s": 1e3 / ms, "ms_per_spectrum": ms, "ms_lineop": stt["ms_total"],
+                     "ms_center": stt["ms_center"], "ms_accum": stt["ms_accum"],
+                     "line_evals": stt["line_evals"], "line_evals_per_s": stt["line_evals"] / (stt["ms_total"] / 1e3)}
+        out["nwl"] = C.nwl
+        C.close()
+    a, b = spz["mixed"], spz["fp64"]
+    out["mixed_vs_fp64"] = {"stokes_I_max_rel": float(np.max(np.abs(a[0][:, 0] / b[0][:, 0] - 1))),
+                            "stokes_QUV_max_over_Ic": float(max(np.max(np.abs(a[0][:, q] - b[0][:, q]) / b[1])
+                                                                for q in (1, 2, 3))),
+                            "flux_max_rel": float(np.max(np.abs(a[2] / b[2] - 1)))}
     return out
 
 

@@ -21,6 +21,7 @@ UNITS = [
     ("fsg_api.cu", ["-fmad=false"]),
     ("fsg_noalloc.cu", ["-fmad=false"]),
     ("fsg_adjoint.cu", ["-fmad=false"]),
+    ("fsg_magfast.cu", ["-fmad=true"]),
 ]
 
 

@@ -48,6 +48,13 @@ int fsg_launch_core_batch(cudaStream_t, int, const CoreJob *, const int *, int, 
 int fsg_class_pix(int);
 int fsg_fast_tiles(int);
 size_t fsg_tile_span_scratch(int64_t);
+int fsg_launch_tile_span_tw(cudaStream_t, int, int, int, int64_t, const LineHdr *, int *, int *, void *, size_t);
+void fsg_launch_mag_params_fast(cudaStream_t, const AtmView &, const LineView &, const int64_t *, int64_t, int64_t,
+                                const int32_t *, const int32_t *, const int32_t *, const VoigtTables &, void *,
+                                LineHdr *, int64_t *);
+size_t fsg_mag_rec_bytes();
+int fsg_launch_mag_fast(cudaStream_t, const AtmView &, const LineHdr *, const void *, const int64_t *, const ZView &,
+                        const int *, const int *, const VoigtTables &, double *);
 void fsg_launch_conv(cudaStream_t, int, const double *, int, const double *, int, double *, const double *, double);
 size_t fsg_adjoint_work(int, int);
 int fsg_launch_adjoint(cudaStream_t, const AtmView &, const LineView &, const VoigtTables &, const double *,
@@ -992,6 +999,57 @@ int fsg_mag_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, int bframe, const 
     CK(cudaEventRecord(ctx->ev[1], s), "event");
     int64_t nkeep = (int64_t)nk;
     if (st) { st->nlines_used = nkeep; st->nweak = n - nkeep; }
+    if (ctx->cfg.precision == FSG_PREC_MIXED) {
+        // mixed precision: retained lines in blocks, FP32 Faraday-Voigt on 32-wavelength tiles
+        int64_t nblkscan = (n + 1023) / 1024;
+        ALLOC(ctx->d_counts, sizeof(int) * std::max<int64_t>(nblkscan, 1));
+        ALLOC(ctx->d_offs, sizeof(int64_t) * std::max<int64_t>(nblkscan, 1));
+        ALLOC(ctx->d_total, sizeof(int64_t));
+        ALLOC(ctx->d_idx, sizeof(int64_t) * n);
+        if (fsg_select(s, n, pf, pl, pr, -1, ctx->d_counts.as<int>(), ctx->d_offs.as<int64_t>(),
+                       ctx->d_idx.as<int64_t>(), ctx->d_total.as<int64_t>()))
+            return cuda_fail(ctx, cudaGetLastError(), "select");
+        ctx->launches += 3;
+        const size_t per_line = fsg_mag_rec_bytes() * nt + sizeof(LineHdr) + sizeof(int64_t);
+        const int64_t bcap = std::min<int64_t>(std::max<int64_t>(nkeep, 1), block_capacity(ctx, per_line));
+        ALLOC(ctx->d_wing, fsg_mag_rec_bytes() * (size_t)bcap * nt);
+        ALLOC(ctx->d_hdr, sizeof(LineHdr) * (size_t)bcap);
+        ALLOC(ctx->d_zmap, sizeof(int64_t) * (size_t)bcap);
+        ALLOC(ctx->d_span, fsg_tile_span_scratch(bcap));
+        ALLOC(ctx->d_tlo, sizeof(int) * (size_t)fsg_fast_tiles(nwl)); ALLOC(ctx->d_thi, sizeof(int) * (size_t)fsg_fast_tiles(nwl));
+        double *mlo = ctx->d_maglineopac.as<double>();
+        int64_t nblocks = 0;
+        for (int64_t j0 = 0; j0 < nkeep; j0 += bcap) {
+            const int64_t nb = std::min(bcap, nkeep - j0);
+            fsg_launch_mag_params_fast(s, A, LV, ctx->d_idx.as<int64_t>(), j0, nb, pf, pl, pr, ctx->tab, ctx->d_wing.p,
+                                       ctx->d_hdr.as<LineHdr>(), ctx->d_zmap.as<int64_t>());
+            if (fsg_launch_tile_span_tw(s, 32, 0, nwl, nb, ctx->d_hdr.as<LineHdr>(), ctx->d_tlo.as<int>(),
+                                        ctx->d_thi.as<int>(), ctx->d_span.p, ctx->d_span.cap) ||
+                fsg_launch_mag_fast(s, A, ctx->d_hdr.as<LineHdr>(), ctx->d_wing.p, ctx->d_zmap.as<int64_t>(), Z,
+                                    ctx->d_tlo.as<int>(), ctx->d_thi.as<int>(), ctx->tab, mlo))
+                return cuda_fail(ctx, cudaGetLastError(), "k_mag_fast");
+            ctx->launches += 8;
+            nblocks++;
+        }
+        CK(cudaEventRecord(ctx->ev[2], s), "event");
+        size_t n4 = sizeof(int32_t) * n;
+        if (flags) CK(cudaMemcpyAsync(flags, ctx->d_flags.p, n4, cudaMemcpyDeviceToHost, s), "flags");
+        if (ileft) CK(cudaMemcpyAsync(ileft, ctx->d_ileft.p, n4, cudaMemcpyDeviceToHost, s), "ileft");
+        if (iright) CK(cudaMemcpyAsync(iright, ctx->d_iright.p, n4, cudaMemcpyDeviceToHost, s), "iright");
+        if (maglineopac)
+            CK(cudaMemcpyAsync(maglineopac, mlo, sizeof(double) * 6 * (size_t)nwl * nt, cudaMemcpyDeviceToHost, s), "mlo");
+        CK(cudaStreamSynchronize(s), "mag lineop");
+        if (st) {
+            float a = 0, b = 0;
+            cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
+            cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
+            st->ms_center = a; st->ms_accum = b; st->ms_total = a + b;
+            st->nblocks = nblocks;
+            st->line_evals = count_windows(ctx, n, ctx->d_flags.as<int32_t>(), ctx->d_ileft.as<int32_t>(),
+                                           ctx->d_iright.as<int32_t>(), 1, nwl) * nt;
+        }
+        return FSG_OK;
+    }
     // NlinesStep and PACK (synth.f90:1131, 1283-1297)
     int64_t cap = block_capacity(ctx, sizeof(double3) * nt);
     int64_t nstep = std::min<int64_t>(n, cap);

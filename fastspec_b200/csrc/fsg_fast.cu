@@ -560,9 +560,18 @@ size_t fsg_tile_span_scratch(int64_t nb) {
     return 4 * sizeof(int) * (size_t)nb + std::max(t1, t2) + 256;
 }
 
+int fsg_launch_tile_span_tw(cudaStream_t s, int tw, int use_core, int nwl, int64_t nb, const LineHdr *hdr, int *lo,
+                            int *hi, void *scratch, size_t scratch_bytes);
+
 int fsg_launch_tile_span(cudaStream_t s, int cls, int nwl, int64_t nb, const LineHdr *hdr, int *lo, int *hi,
                          void *scratch, size_t scratch_bytes) {
-    const int tw = cls < 0 ? 32 : 32 * fsg_class_pix(cls);
+    return fsg_launch_tile_span_tw(s, cls < 0 ? 32 : 32 * fsg_class_pix(cls), cls < 0 ? 1 : 0, nwl, nb, hdr, lo, hi,
+                                   scratch, scratch_bytes);
+}
+
+// tile ranges for tiles of tw wavelengths over the windows (use_core = 0) or the core ranges
+int fsg_launch_tile_span_tw(cudaStream_t s, int tw, int use_core, int nwl, int64_t nb, const LineHdr *hdr, int *lo,
+                            int *hi, void *scratch, size_t scratch_bytes) {
     const int ntiles = (nwl + tw - 1) / tw;
     if (nb <= 0) {
         k_tile_reset<<<(ntiles + 255) / 256, 256, 0, s>>>(ntiles, lo, hi);
@@ -571,7 +580,7 @@ int fsg_launch_tile_span(cudaStream_t s, int cls, int nwl, int64_t nb, const Lin
     int *right = (int *)scratch, *revl = right + nb, *R = revl + nb, *V = R + nb;
     void *tmp = (void *)(((uintptr_t)(V + nb) + 255) & ~(uintptr_t)255);
     size_t tb = scratch_bytes - ((char *)tmp - (char *)scratch);
-    k_span_extract<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>((int)nb, cls < 0 ? 1 : 0, hdr, right, revl);
+    k_span_extract<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>((int)nb, use_core, hdr, right, revl);
     if (cub::DeviceScan::InclusiveScan(tmp, tb, right, R, cub::Max(), (int)nb, s) != cudaSuccess) return FSG_E_CUDA;
     if (cub::DeviceScan::InclusiveScan(tmp, tb, revl, V, cub::Min(), (int)nb, s) != cudaSuccess) return FSG_E_CUDA;
     k_tile_search<<<(ntiles + 255) / 256, 256, 0, s>>>((int)nb, ntiles, tw, nwl, R, V, lo, hi);

@@ -15,8 +15,8 @@ import helpers as H
 pytestmark = pytest.mark.gpu
 
 
-def mag_ctx(fsg, grid, st, co, nmu=9, vmicro=1.0, molbrd=0):
-    C = fsg.Context(precision=fsg.PREC_FP64, vmicro=vmicro, molbrd=molbrd)
+def mag_ctx(fsg, grid, st, co, nmu=9, vmicro=1.0, molbrd=0, prec=None):
+    C = fsg.Context(precision=fsg.PREC_FP64 if prec is None else prec, vmicro=vmicro, molbrd=molbrd)
     C.set_grid(grid["wmode"], grid["wstart"], grid["wend"], grid["dstep"])
     C.set_atmosphere(st)
     C.set_contopac(co)
@@ -127,3 +127,40 @@ def test_mag_linstr_vs_oracle(fsg, oracle_mod):
     assert np.array_equal(g["flags"] & 1, r["flags"] & 1)
     assert np.max(np.abs(g["linstr"] - r["linstr"])) < 1e-7
     assert np.any(g["linstr"] > 0)
+
+
+@pytest.mark.parametrize("bframe,bfield", [(1, [2000.0, 60.0, 30.0]), (0, [1500.0, 800.0, -400.0])])
+def test_mixed_mag_vs_oracle(fsg, oracle_mod, bframe, bfield):
+    """Mixed precision (FP32 Faraday-Voigt on tiles, FP64 sums per line): the six planes within 2e-6
+    of the local absorption scale, Stokes I and Q/U/V within 1e-5 (of Ic)."""
+    grid, st, co, lines, z = zeeman_case()
+    C, x, w = mag_ctx(fsg, grid, st, co, prec=fsg.PREC_MIXED)
+    g = C.mag_lineop_calc(fsg.LineList.from_arrays(lines, zeeman=z), bframe, bfield)
+    spz, spc, sfl, sfc = C.mag_radtran(bframe, bfield)
+    S = oracle_mod.State(grid, st, contopac=co, vmicro=1.0)
+    r = oracle_mod.mag_lineop_calc(S, oracle_mod.Lines(**lines, kind=2, zeeman=z), bframe, np.asarray(bfield, float))
+    ospz, ospc = oracle_mod.mag_radtran(S, x, bframe, np.asarray(bfield, float), np.zeros((S.nwl, S.ntau)),
+                                        r["maglineopac"])
+    assert np.array_equal(g["flags"] & 1, r["flags"] & 1)
+    assert np.array_equal(g["ileft"], r["ileft"]) and np.array_equal(g["iright"], r["iright"])
+    m, om = g["maglineopac"], r["maglineopac"]
+    scale = np.maximum(om[..., :3].max(axis=(0, 2)), 1e-300)[None, :, None]
+    assert np.max(np.abs(m - om) / scale) < 2e-6
+    assert np.max(np.abs(spz[:, 0] / ospz[:, 0] - 1)) < 1e-5
+    for q in (1, 2, 3):
+        assert np.max(np.abs(spz[:, q] - ospz[:, q]) / ospc) < 1e-5
+
+
+def test_mixed_mag_against_reference_pin(fsg):
+    d = H.load_pin("pin_magnetic")
+    grid, st, co, lines, z = H.mag_pin_setup(d)
+    C, x, w = mag_ctx(fsg, grid, st, co, nmu=len(d["xmu"]), vmicro=float(d["vmicro"]), prec=fsg.PREC_MIXED)
+    bframe, bfield = int(d["bframe"]), d["bfield"]
+    C.mag_lineop_calc(fsg.LineList.from_arrays(lines, zeeman=z), bframe, bfield, want=False)
+    spz, spc, sfl, sfc = C.mag_radtran(bframe, bfield)
+    i0, i1 = int(d["i0"]), int(d["i1"])
+    ref, ic = d["spz"], d["spc"]
+    assert np.max(np.abs(spz[i0:i1 + 1, 0] / ref[:, 0] - 1)) < 1e-5
+    for q in (1, 2, 3):
+        assert np.max(np.abs(spz[i0:i1 + 1, q] - ref[:, q]) / ic) < 1e-5
+    assert np.max(np.abs(sfl[i0:i1 + 1] / d["sfl"] - 1)) < 1e-5
