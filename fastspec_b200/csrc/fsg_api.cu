@@ -149,6 +149,8 @@ struct fsg_ctx {
     // magnetic
     DBuf z_npi, z_nsi, z_pioff, z_sioff, z_splpi, z_strpi, z_splsi, z_strsi, d_zsc, z_rawpi, z_rawsi, d_zmap, d_geo;
     cudaEvent_t ev[8];
+    cudaStream_t cstream = nullptr;            // host->device line uploads, overlapped with the central pass
+    std::vector<cudaEvent_t> cev;
     int64_t launches = 0;
     std::vector<cudaEvent_t> kev;
 };
@@ -205,6 +207,7 @@ int fsg_create(const fsg_config *cfg, fsg_ctx **out) {
         cudaGetLastError(); delete ctx; return FSG_E_CUDA;
     }
     for (int i = 0; i < 8; i++) cudaEventCreate(&ctx->ev[i]);
+    cudaStreamCreateWithFlags(&ctx->cstream, cudaStreamNonBlocking);
     std::string e;
     int rc = fsg_build_tables(&ctx->tab, ctx->stream, &e);
     if (rc == FSG_OK) {
@@ -236,6 +239,8 @@ void fsg_destroy(fsg_ctx *ctx) {
                      &ctx->d_zsc, &ctx->z_rawpi, &ctx->z_rawsi, &ctx->d_zmap, &ctx->d_geo };
     for (DBuf *b : bufs) b->release();
     for (int i = 0; i < 8; i++) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
+    for (cudaEvent_t e : ctx->cev) cudaEventDestroy(e);
+    if (ctx->cstream) { cudaStreamSynchronize(ctx->cstream); cudaStreamDestroy(ctx->cstream); }
     for (cudaEvent_t e : ctx->kev) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -420,6 +425,22 @@ static LineView make_view(const fsg_lines *L) {
     v.n = L->n; v.kind = L->kind; v.wl = L->wl; v.elo = L->elo; v.gf = L->gf; v.grad = L->grad;
     v.gqst = L->gqst; v.gvdw = L->gvdw; v.spc = L->spc; v.ismol = L->ismol; v.ihe = L->ihe;
     return v;
+}
+
+// device buffers for a host list (no copy: central_pass_streamed uploads)
+static int device_lines(fsg_ctx *ctx, const fsg_lines *L, fsg_lines *D) {
+    int64_t n = L->n;
+    size_t n8 = sizeof(double) * n, n4 = sizeof(float) * n;
+    ALLOC(ctx->l_wl, n8); ALLOC(ctx->l_elo, n4); ALLOC(ctx->l_gf, n4); ALLOC(ctx->l_grad, n4);
+    ALLOC(ctx->l_gqst, n4); ALLOC(ctx->l_gvdw, n4); ALLOC(ctx->l_spc, n4);
+    *D = *L;
+    D->wl = ctx->l_wl.as<double>(); D->elo = ctx->l_elo.as<float>(); D->gf = ctx->l_gf.as<float>();
+    D->grad = ctx->l_grad.as<float>(); D->gqst = ctx->l_gqst.as<float>(); D->gvdw = ctx->l_gvdw.as<float>();
+    D->spc = ctx->l_spc.as<int32_t>();
+    D->ismol = nullptr; D->ihe = nullptr;
+    if (L->ismol) { ALLOC(ctx->l_ismol, n4); D->ismol = ctx->l_ismol.as<int32_t>(); }
+    if (L->ihe) { ALLOC(ctx->l_ihe, n4); D->ihe = ctx->l_ihe.as<int32_t>(); }
+    return FSG_OK;
 }
 
 static int upload_lines(fsg_ctx *ctx, const fsg_lines *L, fsg_lines *D) {
@@ -747,7 +768,58 @@ static int accumulate_fp64(fsg_ctx *ctx, const LineView &LV, int64_t nkeep, fsg_
     return FSG_OK;
 }
 
-static int lineop_dev(fsg_ctx *ctx, const fsg_lines *D, fsg_stats *st) {
+// The host list streams to the device in chunks on the copy stream; the central pass of each chunk
+// starts on the compute stream as soon as its copy has landed (pinned host memory overlaps both).
+#define UPLOAD_CHUNK ((int64_t)1 << 23)
+static int central_pass_streamed(fsg_ctx *ctx, const fsg_lines *H, const fsg_lines *D, int64_t *nkeep) {
+    const int64_t n = D->n;
+    ALLOC(ctx->d_flags, sizeof(int32_t) * std::max<int64_t>(n, 1));
+    ALLOC(ctx->d_ileft, sizeof(int32_t) * std::max<int64_t>(n, 1));
+    ALLOC(ctx->d_iright, sizeof(int32_t) * std::max<int64_t>(n, 1));
+    ALLOC(ctx->d_nkeep, sizeof(unsigned long long));
+    cudaStream_t s = ctx->stream, c = ctx->cstream;
+    CK(cudaMemsetAsync(ctx->d_nkeep.p, 0, sizeof(unsigned long long), s), "center");
+    const int64_t nch = (n + UPLOAD_CHUNK - 1) / UPLOAD_CHUNK;
+    while ((int64_t)ctx->cev.size() < nch) { cudaEvent_t e; cudaEventCreateWithFlags(&e, cudaEventDisableTiming); ctx->cev.push_back(e); }
+    // the copy stream must not overwrite buffers the compute stream still reads from a previous call
+    CK(cudaEventRecord(ctx->ev[7], s), "event");
+    CK(cudaStreamWaitEvent(c, ctx->ev[7], 0), "event");
+    AtmView A = fsg_view(ctx);
+    for (int64_t k = 0; k < nch; k++) {
+        const int64_t a = k * UPLOAD_CHUNK, m = std::min(UPLOAD_CHUNK, n - a);
+        auto cp = [&](void *dst, const void *src, size_t esz) {
+            return cudaMemcpyAsync((char *)dst + a * esz, (const char *)src + a * esz, m * esz, cudaMemcpyHostToDevice, c);
+        };
+        CK(cp((void *)D->wl, H->wl, 8), "line upload");
+        CK(cp((void *)D->elo, H->elo, 4), "line upload");
+        CK(cp((void *)D->gf, H->gf, 4), "line upload");
+        CK(cp((void *)D->grad, H->grad, 4), "line upload");
+        CK(cp((void *)D->gqst, H->gqst, 4), "line upload");
+        CK(cp((void *)D->gvdw, H->gvdw, 4), "line upload");
+        CK(cp((void *)D->spc, H->spc, 4), "line upload");
+        if (H->ismol) CK(cp((void *)D->ismol, H->ismol, 4), "line upload");
+        if (H->ihe) CK(cp((void *)D->ihe, H->ihe, 4), "line upload");
+        CK(cudaEventRecord(ctx->cev[k], c), "event");
+        CK(cudaStreamWaitEvent(s, ctx->cev[k], 0), "event");
+        fsg_lines Dk = *D;
+        Dk.n = m;
+        Dk.wl += a; Dk.elo += a; Dk.gf += a; Dk.grad += a; Dk.gqst += a; Dk.gvdw += a; Dk.spc += a;
+        if (Dk.ismol) Dk.ismol += a;
+        if (Dk.ihe) Dk.ihe += a;
+        fsg_launch_center(s, A, make_view(&Dk), ctx->tab, ctx->d_flags.as<int32_t>() + a, ctx->d_ileft.as<int32_t>() + a,
+                          ctx->d_iright.as<int32_t>() + a, ctx->d_nkeep.as<unsigned long long>());
+        ctx->launches += 1;
+    }
+    CK(cudaGetLastError(), "k_center");
+    unsigned long long nk = 0;
+    CK(cudaMemcpyAsync(&nk, ctx->d_nkeep.p, sizeof nk, cudaMemcpyDeviceToHost, s), "center");
+    CK(cudaStreamSynchronize(s), "center");
+    *nkeep = (int64_t)nk;
+    return FSG_OK;
+}
+
+// D: device list; H: the host list it is uploaded from during the central pass (NULL: D is resident)
+static int lineop_dev(fsg_ctx *ctx, const fsg_lines *D, fsg_stats *st, const fsg_lines *H = nullptr) {
     LineView LV = make_view(D);
     int rc = ensure_lineopac(ctx); if (rc) return rc;
     if (st) { memset(st, 0, sizeof *st); st->nlines_in = D->n; }
@@ -755,7 +827,8 @@ static int lineop_dev(fsg_ctx *ctx, const fsg_lines *D, fsg_stats *st) {
     cudaStream_t s = ctx->stream;
     CK(cudaEventRecord(ctx->ev[0], s), "event");
     int64_t nkeep = 0;
-    rc = central_pass(ctx, LV, &nkeep); if (rc) return rc;
+    rc = H ? central_pass_streamed(ctx, H, D, &nkeep) : central_pass(ctx, LV, &nkeep);
+    if (rc) return rc;
     CK(cudaEventRecord(ctx->ev[1], s), "event");
     if (st) { st->nlines_used = nkeep; st->nweak = D->n - nkeep; }
     if (ctx->cfg.precision == FSG_PREC_FP64) rc = accumulate_fp64(ctx, LV, nkeep, st);
@@ -860,9 +933,9 @@ int fsg_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, double *lineopac, int3
     if (linstr && ctx->nmu < 1) return fail(ctx, FSG_E_STATE, "fsg_lineop_calc: line strengths need fsg_set_mu first");
     cudaSetDevice(ctx->device);
     fsg_lines D;
-    if (lines->n > 0) { rc = upload_lines(ctx, lines, &D); if (rc) return rc; }
+    if (lines->n > 0) { rc = device_lines(ctx, lines, &D); if (rc) return rc; }
     else D = *lines;
-    rc = lineop_dev(ctx, &D, st); if (rc) return rc;
+    rc = lineop_dev(ctx, &D, st, lines->n > 0 ? lines : nullptr); if (rc) return rc;
     cudaStream_t s = ctx->stream;
     if (linstr && lines->n > 0) { rc = linstr_calc(ctx, &D, linstr); if (rc) return rc; }
     size_t n4 = sizeof(int32_t) * lines->n;
