@@ -33,7 +33,6 @@ void fsg_launch_fvoigt(cudaStream_t, int64_t, const double *, const double *, do
                        const VoigtTables &);
 void fsg_launch_locprf(cudaStream_t, int, int, const double *, int, const double *, const double *, const double *,
                        double *, double *);
-int fsg_fast_set_constants(const double *, const double *);
 int fsg_launch_accum_fast(cudaStream_t, int, int, int, const double *, const LineHdr *, const WingRec *,
                           const int *, const int *, double *, int *);
 void fsg_launch_count_core(cudaStream_t, int64_t, const LineHdr *, unsigned long long *);
@@ -214,7 +213,6 @@ int fsg_create(const fsg_config *cfg, fsg_ctx **out) {
         if (cudaMemcpyAsync(ctx->h_anode, ctx->tab.anode, sizeof ctx->h_anode, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
             cudaMemcpyAsync(ctx->h_aida, ctx->tab.aida, sizeof ctx->h_aida, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
             cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = FSG_E_CUDA;
-        else rc = fsg_fast_set_constants(ctx->h_anode, ctx->h_aida);
     }
     if (rc != FSG_OK) { fsg_destroy(ctx); return rc; }
     *out = ctx;

@@ -3,40 +3,28 @@
 // The work of LineopCalc's accumulation (LineOpacity1, opacity.f90:297-346) is
 //   LineOpac(t, p) = sum over retained lines l with Ileft(l) <= p <= Iright(l) of
 //                    HVoigt(a(l,t), (lambda_p - lambda_l) / dlD(l,t)) * LinCop(l,t).
-// Here a CTA owns a tile of TW = 32 P wavelengths x all depths.  Warp w owns depths
-// [w*D, w*D + D); lane l owns the wavelengths tile0 + l + 32k (k < P).  Each thread owns its
-// P x D sums: FP32 partials in registers over FOLD lines, Kahan-compensated (sum, compensation)
-// pairs in shared memory beyond that.  No atomics, one read-modify-write of the FP64 LineOpac
-// per tile and launch, deterministic order.
+// It is split by the branch HVoigt takes.  Each line has a core range (every wavelength of its
+// window where some depth may have s = v^2 + a^2 < 196); outside it every depth takes the
+// reference's rational wing form (voigt.f90:100-101).
 //
-// Lines are binned by window width (class c holds windows of up to 256 * 2^c wavelengths) and
-// processed class by class, so the candidate line range of a tile [lo, hi] -- the lines of the
-// class whose windows touch it -- stays within a small factor of the lines that do.  Narrow
-// classes use narrow tiles (P = 1 for class 0, 2 for class 1, 4 above) so fewer lanes idle at
-// the window edges.
+// Wing pass (k_accum_fast): a CTA owns a tile of TW = 32 P wavelengths x all depths; warp w owns
+// depths [w*D, w*D + D), lane l the wavelengths tile0 + l + 32k (k < P).  Line headers and wing
+// records arrive in shared memory by bulk copies; each thread keeps P x D FP32 partials over FOLD
+// lines, folded into Kahan (sum, compensation) pairs in shared memory.  Lines are binned by window
+// width (class c holds windows of up to 256 * 2^c wavelengths) and processed class by class, so a
+// tile's candidate range stays close to the lines that touch it; narrow classes use 64-wavelength
+// tiles, wide ones 128.
 //
-// The profile is evaluated in FP32 from the per-(line, depth) FP32 records that k_params_fast
-// derives from the FP64 XlineDepth values: for s = v^2 + a^2 >= 196 (almost every wing point)
-// the reference's rational form (voigt.f90:100-101) as c1 (x + c2) / (x^2 + d1 x + d0), x = v^2;
-// below that the table lerp (|v| < 8, a < 8) or the two-term continued fraction (voigt.f90:103-107),
-// exactly as HVoigt branches.
+// Core pass (k_core_fast): over the core ranges, 32-wavelength tiles, the table lerp (|v| < 8,
+// a < 8), the two-term continued fraction (voigt.f90:103-107) or the wing form, point by point,
+// exactly as HVoigt branches.  No atomics; one read-modify-write of the FP64 LineOpac per tile and
+// launch; deterministic order.
 #include "fsg_internal.cuh"
 
 #include <cub/device/device_scan.cuh>
 #include <algorithm>
 
 #define CLASS_W0 128      // class c: windows of at most CLASS_W0 * 2^(c+1) wavelengths
-
-__constant__ float c_anode[FSG_NA1];
-__constant__ float c_aida[FSG_NA1];
-
-int fsg_fast_set_constants(const double *anode_h, const double *aida_h) {
-    float a[FSG_NA1], b[FSG_NA1];
-    for (int i = 0; i < FSG_NA1; i++) { a[i] = (float)anode_h[i]; b[i] = (float)aida_h[i]; }
-    if (cudaMemcpyToSymbol(c_anode, a, sizeof a) != cudaSuccess) return FSG_E_CUDA;
-    if (cudaMemcpyToSymbol(c_aida, b, sizeof b) != cudaSuccess) return FSG_E_CUDA;
-    return FSG_OK;
-}
 
 // HVoigt * LinCop in FP32 outside the table (a >= 8 or |v| >= 8, s < 196): the two-term continued
 // fraction of voigt.f90:103-107 at |v| = av
