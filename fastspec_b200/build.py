@@ -22,6 +22,7 @@ UNITS = [
     ("fsg_noalloc.cu", ["-fmad=false"]),
     ("fsg_adjoint.cu", ["-fmad=false"]),
     ("fsg_magfast.cu", ["-fmad=true"]),
+    ("fsg_adjoint_line.cu", ["-fmad=true"]),
 ]
 
 

@@ -55,7 +55,7 @@ size_t fsg_mag_rec_bytes();
 int fsg_launch_mag_fast(cudaStream_t, const AtmView &, const LineHdr *, const void *, const int64_t *, const ZView &,
                         const int *, const int *, const VoigtTables &, double *);
 void fsg_launch_conv(cudaStream_t, int, const double *, int, const double *, int, double *, const double *, double);
-size_t fsg_adjoint_work(int, int);
+size_t fsg_adjoint_work(int, int, int64_t);
 int fsg_launch_adjoint(cudaStream_t, const AtmView &, const LineView &, const VoigtTables &, const double *,
                        const double *, int, const double *, const double *, const int32_t *, const int32_t *,
                        const int32_t *, const double *, double *, double *, double, double *, double *);
@@ -1652,7 +1652,7 @@ int fsg_adjoint_dev(fsg_ctx *ctx, const fsg_lines *d_lines, const double *d_gflu
     rc = ensure_lineopac(ctx); if (rc) return rc;
     const size_t ng = sizeof(double) * (size_t)ctx->nwl * ctx->ntau;
     if (!d_gkappa) { ALLOC(ctx->d_gkappa, ng); d_gkappa = ctx->d_gkappa.as<double>(); }
-    ALLOC(ctx->d_adjwork, fsg_adjoint_work(ctx->nwl, ctx->ntau));
+    ALLOC(ctx->d_adjwork, fsg_adjoint_work(ctx->nwl, ctx->ntau, d_lines->n));
     rc = fsg_launch_adjoint(ctx->stream, fsg_view(ctx), make_view(d_lines), ctx->tab, ctx->d_lineopac.as<double>(),
                             ctx->d_rhox.as<double>(), ctx->nmu, ctx->d_xmu.as<double>(), ctx->d_wmu.as<double>(),
                             ctx->d_flags.as<int32_t>(), ctx->d_ileft.as<int32_t>(), ctx->d_iright.as<int32_t>(),

@@ -86,6 +86,16 @@ __device__ __forceinline__ void fvoigt_line64(const float2 *__restrict__ ftab, V
 }
 
 // ---- grid ---------------------------------------------------------------------------------
+// first index i in [0, n) with w[i] >= x (n when none)
+__device__ __forceinline__ int lower_index(const double *__restrict__ w, int n, double x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        int m = (lo + hi) >> 1;
+        if (w[m] < x) lo = m + 1; else hi = m;
+    }
+    return lo;
+}
+
 // WaveIdx (opacity.f90:594-608); 1-based
 __device__ __forceinline__ int waveidx(const AtmView &A, double wavein) {
     if (A.wmode == 0) {

@@ -236,15 +236,6 @@ void fsg_launch_center(cudaStream_t s, const AtmView &A, const LineView &L, cons
 // ================================================================================================
 // Block refill: per retained line of the block, XlineSetup once then XlineDepth over depths.
 // ================================================================================================
-// first index i in [0, n) with w[i] >= x (n when none)
-__device__ __forceinline__ int lower_index(const double *__restrict__ w, int n, double x) {
-    int lo = 0, hi = n;
-    while (lo < hi) {
-        int m = (lo + hi) >> 1;
-        if (w[m] < x) lo = m + 1; else hi = m;
-    }
-    return lo;
-}
 
 __global__ void k_params_fast(AtmView A, LineView L, const int64_t *__restrict__ idx, int64_t j0,
                               int64_t nb, const int32_t *__restrict__ flags,
