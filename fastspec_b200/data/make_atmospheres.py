@@ -524,8 +524,107 @@ def make_mag_pin(gold):
     print("pin_magnetic lines", merged.n, "region pixels", i1 - i0 + 1)
 
 
+SPHERE_RADIUS = {"solar": 3.0e10, "magnetic": 5.0e10}
+
+
+def sphere_model(atmname):
+    """The configuration's model atmosphere as a spherical model: layer heights from hydrostatics
+    (workloads.model_heights) and a radius small enough that the outermost angle of the default
+    Gauss-Legendre set is a grazing ray while every other ray reaches the bottom layer."""
+    teff, logg, ntau = CONFIGS[atmname][:3]
+    model = W.eddington_model(teff, logg, ntau)
+    return model, SPHERE_RADIUS[atmname], W.model_heights(model["rhox"], model["rho"])
+
+
+def make_sphere_pins(gold):
+    """Spherical fixtures (pin_sphere.npz): the decks of pin_solar and pin_magnetic with the model
+    written as a spherical one.  Scalar: line opacity, continuum, intensities, flux and line strengths
+    of one run (SAVE 1,1,1,1,1).  Polarised: Stokes IQUV with the field in the stellar frame
+    (BFRAME 0), whose projection changes along the curved rays."""
+    out = {}
+    # scalar
+    name, atmname, mk, grid, region = pin_specs()[0]
+    teff, logg, ntau, species, ismol, _, _, vmic, molbrd, _, _ = CONFIGS[atmname]
+    model, radius, height = sphere_model(atmname)
+    state = load_state(atmname)
+    extra = mk()
+    pgf = np.load(os.path.join(HERE, "atm_%s.npz" % atmname))["probe_loggf"]
+    probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
+    merged = merge([probes, extra])
+    with tempfile.TemporaryDirectory() as wd:
+        W.write_krz(os.path.join(wd, "model.krz"), model, radius=radius, height=height)
+        merged.write_z(os.path.join(wd, "lines.z"), grid[0], grid[1])
+        deck = ("wave=%.4f, %.4f, %.6f, %d\nsave=1, 1, 1, 1, 1\nvmic=%.3f\nmolbrd=%d\n"
+                "lines=\n-1  lines.z\n\nmodel=model.krz\nmus=7\n" % (grid + (vmic, molbrd)))
+        log = run_ref(wd, deck)
+        assert "Spherical" in log, log
+        lo = fsio.read_opac(os.path.join(wd, "fs_lineop.bin"))
+        co = fsio.read_opac(os.path.join(wd, "fs_contop.bin"))
+        sp = fsio.read_spec(os.path.join(wd, "fs_spec.bin"))
+        fl = fsio.read_flux(os.path.join(wd, "fs_flux.bin"))
+        ls = fsio.read_linst(os.path.join(wd, "fs_linst.bin"))
+    for k in ("rhox", "T", "xne", "xna", "rho"):
+        assert np.array_equal(lo[k], state[k]), "EOS state differs from the recovered one: " + k
+    g = oracle.sphere_init(state["rhox"], height, radius, sp["xmu"])
+    assert 0 < g["graz"].sum() < len(g["graz"]), "want grazing and normal rays"
+    wave = lo["wave"]
+    sel = (wave >= region[0] - 1e-9) & (wave <= region[1] + 1e-9)
+    i0, i1 = (int(x) for x in np.nonzero(sel)[0][[0, -1]])
+    lsel = ls["wave"] >= extra.arrays()["wl"].min() - 1e-9
+    out.update(s_grid=np.array(grid, np.float64), s_i0=i0, s_i1=i1, s_radius=radius, s_height=height,
+               s_contopac=co["opac"][i0:i1 + 1], s_lineopac=lo["opac"][i0:i1 + 1], s_wave=wave[i0:i1 + 1],
+               s_xmu=sp["xmu"], s_spl=sp["spl"][i0:i1 + 1], s_spc=sp["spc"][i0:i1 + 1],
+               s_sfl=fl["sfl"][i0:i1 + 1], s_sfc=fl["sfc"][i0:i1 + 1], s_linst_wave=ls["wave"][lsel],
+               s_linst=ls["strength"][lsel])
+    print("sphere scalar: region pixels", i1 - i0 + 1, "grazing rays", int(g["graz"].sum()),
+          "line strengths", int(lsel.sum()))
+    # polarised, stellar-frame field
+    teff, logg, ntau, species, ismol, _, _, vmic, molbrd, _, _ = CONFIGS["magnetic"]
+    model, radius, height = sphere_model("magnetic")
+    state = load_state("magnetic")
+    grid = (6000.0, 6043.0, 0.002, 0)
+    region = (6040.0, 6043.0)
+    bfield = (1500.0, 800.0, -600.0)
+    extra = W.zeeman_lines(60, 6040.3, 6042.7, W.SEED0 + 2)
+    pgf = np.load(os.path.join(HERE, "atm_magnetic.npz"))["probe_loggf"]
+    probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
+    merged = merge([probes, extra])
+    pats = zeeman_blocks(merged)
+    with tempfile.TemporaryDirectory() as wd:
+        W.write_krz(os.path.join(wd, "model.krz"), model, radius=radius, height=height)
+        merged.write_z(os.path.join(wd, "lines.z"), grid[0], grid[1], patterns=pats)
+        deck = ("wave=%.4f, %.4f, %.6f, %d\nsave=0, 0, 1, 1, 1\nvmic=%.3f\nmolbrd=%d\n"
+                "lines=\n-1  lines.z\n\nmodel=model.krz\nmus=9\nbframe=0\nbfield=%g, %g, %g\n"
+                % (grid + (vmic, molbrd) + bfield))
+        log = run_ref(wd, deck)
+        assert "Spherical polarised" in log, log
+        co = fsio.read_opac(os.path.join(wd, "fs_contop.bin"))
+        sp = fsio.read_spec(os.path.join(wd, "fs_spec.bin"))
+        fl = fsio.read_flux(os.path.join(wd, "fs_flux.bin"))
+    for k in ("rhox", "T", "xne", "xna", "rho"):
+        assert np.array_equal(co[k], state[k]), "EOS state differs from the recovered one: " + k
+    g = oracle.sphere_init(state["rhox"], height, radius, sp["xmu"])
+    assert 0 < g["graz"].sum() < len(g["graz"]), "want grazing and normal rays"
+    wave = co["wave"]
+    sel = (wave >= region[0] - 1e-9) & (wave <= region[1] + 1e-9)
+    i0, i1 = (int(x) for x in np.nonzero(sel)[0][[0, -1]])
+    npr = probes.n
+    a = {k: v[npr:] for k, v in merged.arrays().items()}
+    comp = mirrored_components(pats[npr:])
+    out.update(m_grid=np.array(grid, np.float64), m_i0=i0, m_i1=i1, m_radius=radius, m_height=height,
+               m_bframe=0, m_bfield=np.array(bfield), m_contopac=co["opac"][i0:i1 + 1], m_wave=wave[i0:i1 + 1],
+               m_xmu=sp["xmu"], m_spz=sp["spz"][i0:i1 + 1], m_spc=sp["spc"][i0:i1 + 1],
+               m_sfl=fl["sfl"][i0:i1 + 1], m_sfc=fl["sfc"][i0:i1 + 1],
+               z_npi=comp[0], z_nsi=comp[1], z_spl_pi=comp[2], z_str_pi=comp[3], z_spl_si=comp[4],
+               z_str_si=comp[5], **{"mline_" + k: v for k, v in a.items()})
+    np.savez_compressed(os.path.join(gold, "pin_sphere.npz"), **out)
+    print("sphere polarised: region pixels", i1 - i0 + 1, "grazing rays", int(g["graz"].sum()))
+
+
 if __name__ == "__main__":
-    if len(sys.argv) > 1 and sys.argv[1] == "magpin":
+    if len(sys.argv) > 1 and sys.argv[1] == "sphere":
+        make_sphere_pins(os.path.join(REPO, "tests", "golden"))
+    elif len(sys.argv) > 1 and sys.argv[1] == "magpin":
         make_mag_pin(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "convol":
         make_convol_pin(os.path.join(REPO, "tests", "golden"))

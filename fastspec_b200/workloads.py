@@ -118,20 +118,31 @@ def eddington_model(teff, logg, ntau, logtau_min=-5.0, logtau_max=2.0, metal=1e-
                 xne=xne, xna=xna, rho=rho)
 
 
-def write_krz(path, model, abund=None, title="synthetic Eddington-grey model"):
-    """Write a plane-parallel `.krz` model (the format ReadModel parses, ioutils.f90:1614-1748)."""
+def write_krz(path, model, abund=None, title="synthetic Eddington-grey model", radius=None, height=None):
+    """Write a `.krz` model (the format ReadModel parses, ioutils.f90:1614-1748): plane-parallel, or
+    spherical with `radius` [cm] in the header and the layer heights [cm] as a sixth column."""
     ab = list(abund if abund is not None else SOLAR30) + [-20.0] * (99 - len(SOLAR30))
+    sph = radius is not None and radius > 0
     with open(path, "w") as f:
         f.write("TITLE %s\n" % title)
-        f.write("T EFF= %.0f. GRAV= %.2f  MODEL TYPE= 0 WLSTD= 5000 PLANE-PARALLEL.\n"
-                % (model["teff"], model["logg"]))
+        geo = ("SPHERICAL RADIUS= %.9E" % radius) if sph else "PLANE-PARALLEL."
+        f.write("T EFF= %.0f. GRAV= %.2f  MODEL TYPE= 0 WLSTD= 5000 %s\n" % (model["teff"], model["logg"], geo))
         f.write(" 1 1 1 1 1 1 1 1 1 1 1 1 1 0 1 0 0 0 0 0 - OPACITY SWITCHES\n")
         for i in range(0, 99, 10):
             f.write(" ".join("%7.3f" % a for a in ab[i:i + 10]))
             f.write(" %d\n" % model["ntau"] if i + 10 >= 99 else "\n")
         for i in range(model["ntau"]):
-            f.write(" %.9E, %8.1f, %.6E, %.6E, %.6E,\n" % (
+            f.write(" %.9E, %8.1f, %.6E, %.6E, %.6E," % (
                 model["rhox"][i], model["T"][i], model["xne"][i], model["xna"][i], model["rho"][i]))
+            f.write(" %.9E,\n" % height[i] if sph else "\n")
+
+
+def model_heights(rhox, rho):
+    """Layer heights [cm] of a hydrostatic model, 0 at the top and decreasing inward:
+    dh = -d(rhox) / rho by the trapezoid rule in 1/rho."""
+    rhox = np.asarray(rhox, np.float64); rho = np.asarray(rho, np.float64)
+    dh = np.diff(rhox) * 0.5 * (1.0 / rho[1:] + 1.0 / rho[:-1])
+    return -np.concatenate([[0.0], np.cumsum(dh)])
 
 
 # ---- line lists ------------------------------------------------------------------------------

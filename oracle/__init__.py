@@ -37,6 +37,8 @@ class _State(C.Structure):
         ("h2brd", C.c_double), ("vwmol", C.c_double), ("molbrd", C.c_int),
         ("x_nprtb", _dp), ("x_gvwprt", _dp), ("x_temp6", _dp), ("x_temp3", _dp), ("x_kbt", _dp),
         ("x_kbet", _dp), ("x_vturb2", C.c_double),
+        ("radius", C.c_double), ("sph_nmu", C.c_int), ("sph_ntau", _ip), ("sph_graz", _ip),
+        ("sph_map", _ip), ("sph_rhox", _dp), ("sph_muloc", _dp),
     ]
 
 
@@ -222,6 +224,23 @@ class State:
                     temp3=g(self.s.x_temp3), kbt=g(self.s.x_kbt), kbet=g(self.s.x_kbet),
                     vturb2=self.s.x_vturb2)
 
+    def set_sphere(self, radius, height, xmu):
+        """Spherical geometry (ReadModel's RADIUS and layer heights, ioutils.f90:1630-1700) with the
+        rays of SphereInit for the angles xmu; radius <= 0 returns to plane-parallel."""
+        k = self._keep
+        if radius <= 0:
+            self.s.radius = -1.0; self.s.sph_nmu = 0
+            return None
+        g = sphere_init(self._keep["rhox"], height, radius, xmu)
+        for name in ("ntau_mu", "graz", "map"):
+            k["sph_" + name] = g[name]
+        k["sph_rhox"] = g["rhox_mu"]; k["sph_muloc"] = g["mu_loc"]; k["height"] = _f64(height)
+        self.s.sph_ntau = _p(k["sph_ntau_mu"], C.c_int); self.s.sph_graz = _p(k["sph_graz"], C.c_int)
+        self.s.sph_map = _p(k["sph_map"], C.c_int); self.s.sph_rhox = _p(k["sph_rhox"], C.c_double)
+        self.s.sph_muloc = _p(k["sph_muloc"], C.c_double); self.s.height = _p(k["height"], C.c_double)
+        self.s.sph_nmu = len(xmu); self.s.radius = float(radius)
+        return g
+
     def __del__(self):
         try:
             lib().or_state_free(C.byref(self.s))
@@ -310,8 +329,14 @@ def mag_lineop_calc(state, lines, bframe, bfield, nlines_lim=0, nmu=0, xmu=None,
                 stats={f: getattr(st, f) for f, _ in _Stats._fields_})
 
 
+def _check_rays(state, nmu):
+    if state.s.radius > 0 and state.s.sph_nmu != nmu:
+        raise ValueError("spherical state: the rays were set for %d angles, not %d" % (state.s.sph_nmu, nmu))
+
+
 def radtran(state, xmu, lineopac, want_spc=True):
     xmu = _f64(xmu); nmu = len(xmu)
+    _check_rays(state, nmu)
     lo = _f64(lineopac)
     spl = np.zeros((state.nwl, nmu)); spc = np.zeros((state.nwl, nmu)) if want_spc else None
     lib().or_radtran(C.byref(state.s), nmu, _p(xmu, C.c_double), _p(lo, C.c_double),
@@ -321,11 +346,30 @@ def radtran(state, xmu, lineopac, want_spc=True):
 
 def mag_radtran(state, xmu, bframe, bfield, lineopac, maglineopac):
     xmu = _f64(xmu); nmu = len(xmu)
+    _check_rays(state, nmu)
     bf = _f64(bfield); lo = _f64(lineopac); mlo = _f64(maglineopac)
     spz = np.zeros((state.nwl, 4, nmu)); spc = np.zeros((state.nwl, nmu))
     lib().or_mag_radtran(C.byref(state.s), nmu, _p(xmu, C.c_double), int(bframe), _p(bf, C.c_double),
                          _p(lo, C.c_double), _p(mlo, C.c_double), _p(spz, C.c_double), _p(spc, C.c_double))
     return spz, spc
+
+
+def sphere_init(rhox, height, radius, xmu):
+    """SphereInit (solver.f90:45-120): ray geometry per angle; map is 1-based as MapMu."""
+    rhox = _f64(rhox); height = _f64(height); xmu = _f64(xmu)
+    nt, nmu = len(rhox), len(xmu)
+    out = dict(ntau_mu=np.zeros(nmu, np.int32), graz=np.zeros(nmu, np.int32),
+               map=np.zeros((nmu, 2 * nt), np.int32), rhox_mu=np.zeros((nmu, 2 * nt)),
+               mu_loc=np.zeros((nmu, 2 * nt)))
+    rc = lib().or_sphere_init(nt, _p(rhox, C.c_double), _p(height, C.c_double), C.c_double(radius), nmu,
+                              _p(xmu, C.c_double), _p(out["ntau_mu"], C.c_int), _p(out["graz"], C.c_int),
+                              _p(out["map"], C.c_int), _p(out["rhox_mu"], C.c_double),
+                              _p(out["mu_loc"], C.c_double))
+    if rc == -1:
+        raise ValueError("SphereInit: mu = 0 rays are unsupported for spherical models")
+    if rc == -2:
+        raise ValueError("SphereInit: grazing ray tangent in the top model layer")
+    return out
 
 
 def locprf_pp(xmu, xki, src, rhox):

@@ -530,6 +530,90 @@ void or_locprf_pp(double *Ploc, const double *Xmu, int Nmu, const double *Xki, c
     free(Srd);
 }
 
+/* SphereInit (solver.f90:45-120).  Ray im (impact parameter p = R_top sqrt(1 - mu^2)) crosses the
+ * layers 1..n on its near half; a grazing ray (p > R_bottom) turns at the shell below layer n and
+ * comes back through layers n..1, so its points n+1..2n mirror 1..n.  Column mass along the ray
+ * grows by the radial step times (r_k + r_k-1) / (z_k + z_k-1), z = sqrt(r^2 - p^2) in the factored
+ * form, and by chord x dm/dr across the tangent shell. */
+int or_sphere_init(int ntau, const double *rhox, const double *height, double radius, int nmu,
+                   const double *xmu, int *ntau_mu, int *graz, int *map, double *rhox_mu, double *mu_loc) {
+    const int M = 2 * ntau;
+    double *Rk = (double *)malloc(sizeof(double) * ntau);
+    for (int k = 0; k < ntau; k++) Rk[k] = radius + height[k];
+    int rc = 0;
+    for (int im = 0; im < nmu && rc == 0; im++) {
+        int *mp = map + (size_t)im * M;
+        double *rm = rhox_mu + (size_t)im * M, *ml = mu_loc + (size_t)im * M;
+        for (int k = 0; k < M; k++) { mp[k] = 0; rm[k] = 0.0; ml[k] = 0.0; }
+        if (xmu[im] <= 0.0) { rc = -1; break; }
+        double P = Rk[0] * sqrt((1.0 - xmu[im]) * (1.0 + xmu[im]));
+        int g = P > Rk[ntau - 1], n = ntau;
+        if (g) {
+            int kt = 2;
+            while (kt <= ntau && !(P >= Rk[kt - 1])) kt++;
+            n = kt - 1;
+            if (n < 2) { rc = -2; break; }
+        }
+        rm[0] = rhox[0] / xmu[im];
+        double Zk1 = sqrt((Rk[0] - P) * (Rk[0] + P));
+        ml[0] = Zk1 / Rk[0];
+        mp[0] = 1;
+        for (int k = 2; k <= n; k++) {
+            double Zk = sqrt((Rk[k - 1] - P) * (Rk[k - 1] + P));
+            rm[k - 1] = rm[k - 2] + (rhox[k - 1] - rhox[k - 2]) * (Rk[k - 1] + Rk[k - 2]) / (Zk + Zk1);
+            ml[k - 1] = Zk / Rk[k - 1];
+            mp[k - 1] = k;
+            Zk1 = Zk;
+        }
+        graz[im] = g;
+        if (!g) { ntau_mu[im] = ntau; continue; }
+        double Chord = 2.0 * sqrt((Rk[n - 1] - P) * (Rk[n - 1] + P));
+        rm[n] = rm[n - 1] + Chord * (rhox[n] - rhox[n - 1]) / (Rk[n - 1] - Rk[n]);
+        mp[n] = n;
+        ml[n] = -ml[n - 1];
+        for (int k = n + 2; k <= 2 * n; k++) {
+            rm[k - 1] = rm[k - 2] + (rm[2 * n - k + 1] - rm[2 * n - k]);
+            mp[k - 1] = 2 * n + 1 - k;
+            ml[k - 1] = -ml[2 * n - k];
+        }
+        ntau_mu[im] = 2 * n;
+    }
+    free(Rk);
+    return rc;
+}
+
+/* DeloScalar (solver.f90:220-261): emergent intensity along one ray from its optical-depth steps,
+ * source function and boundary intensity Y0 */
+static double delo_scalar(const double *Deltau, const double *Src, int N, double Y0) {
+    double *Srd = (double *)malloc(sizeof(double) * N);
+    or_centder(Deltau, Src, 1, N, Srd);
+    double Y = Y0;
+    for (int k = N - 2; k >= 0; k--) {
+        double Dtau = Deltau[k], Eps, Alpha, Beta, Gamma;
+        delo_coef(Dtau, &Eps, &Alpha, &Beta, &Gamma);
+        double U = 0.5 * (Src[k] + 0.5 * Dtau * Srd[k] + Src[k + 1] - 0.5 * Dtau * Srd[k + 1]);
+        Y = Y * Eps + Alpha * Src[k] + Beta * Src[k + 1] + Gamma * U;
+    }
+    free(Srd);
+    return Y;
+}
+
+/* LocPrfSph (solver.f90:182-216): opacity and source gathered along each ray (MapMu), TauStep on the
+ * ray's column mass with mu = 1, zero incoming intensity for grazing rays, Src(N) otherwise */
+void or_locprf_sph(const or_state *s, double *Ploc, const double *Xki, const double *Src) {
+    const int M = 2 * s->ntau;
+    double *XkiR = (double *)malloc(sizeof(double) * 3 * M), *SrcR = XkiR + M, *Deltau = SrcR + M;
+    for (int im = 0; im < s->sph_nmu; im++) {
+        const int N = s->sph_ntau[im];
+        const int *mp = s->sph_map + (size_t)im * M;
+        for (int k = 0; k < N; k++) { XkiR[k] = Xki[mp[k] - 1]; SrcR[k] = Src[mp[k] - 1]; }
+        or_taustep(s->sph_rhox + (size_t)im * M, XkiR, 1.0, N, Deltau);
+        double Y = s->sph_graz[im] ? 0.0 : SrcR[N - 1];
+        Ploc[im] = delo_scalar(Deltau, SrcR, N, Y);
+    }
+    free(XkiR);
+}
+
 /* Solve4x4 (solver.f90:541-588): A column-major A[i + 4*j] */
 void or_solve4x4(const double *A, const double *B, double *X) {
     double M[16], R[4];
@@ -563,10 +647,12 @@ static void planck(const or_state *s, double wl, double *Src) {
     for (int t = 0; t < s->ntau; t++) Src[t] = C2 / (exp(C1 / s->T[t]) - 1.0);
 }
 
-/* RadTranCalc, plane-parallel (synth.f90:1825-1866) */
+/* RadTranCalc (synth.f90:1825-1901): LocPrfPP for plane-parallel models, LocPrfSph along the rays
+ * of s for spherical ones (radius > 0) */
 void or_radtran(const or_state *s, int nmu, const double *xmu, const double *lineopac,
                 double *spl, double *spc) {
     int nt = s->ntau;
+    const int sph = s->radius > 0.0;
     #pragma omp parallel
     {
         double *Src = (double *)malloc(sizeof(double) * 2 * nt), *Xki = Src + nt;
@@ -574,24 +660,33 @@ void or_radtran(const or_state *s, int nmu, const double *xmu, const double *lin
         for (int iwl = 0; iwl < s->nwl; iwl++) {
             planck(s, s->wave[iwl] + s->wfirst, Src);
             const double *co = s->contopac + (size_t)iwl * nt;
-            if (spc) { for (int t = 0; t < nt; t++) Xki[t] = co[t];
-                       or_locprf_pp(spc + (size_t)iwl * nmu, xmu, nmu, Xki, Src, s->rhox, nt); }
+            if (spc) {
+                for (int t = 0; t < nt; t++) Xki[t] = co[t];
+                if (sph) or_locprf_sph(s, spc + (size_t)iwl * nmu, Xki, Src);
+                else or_locprf_pp(spc + (size_t)iwl * nmu, xmu, nmu, Xki, Src, s->rhox, nt);
+            }
             for (int t = 0; t < nt; t++) Xki[t] = co[t] + lineopac[(size_t)iwl * nt + t];
-            or_locprf_pp(spl + (size_t)iwl * nmu, xmu, nmu, Xki, Src, s->rhox, nt);
+            if (sph) or_locprf_sph(s, spl + (size_t)iwl * nmu, Xki, Src);
+            else or_locprf_pp(spl + (size_t)iwl * nmu, xmu, nmu, Xki, Src, s->rhox, nt);
         }
         free(Src);
     }
 }
 
-/* LinStrCalc, plane-parallel (synth.f90:1774-1822) */
+/* LinStrCalc (synth.f90:1774-1822) */
 static float linstr_calc(const or_state *s, double Wl, const double *LineOpacL,
                          const double *ContOpacL, int nmu, const double *xmu, const double *wmu) {
     int nt = s->ntau;
     double Src[nt], Xki[nt], IntL[nmu > 0 ? nmu : 1], IntC[nmu > 0 ? nmu : 1];
     planck(s, Wl, Src);
-    or_locprf_pp(IntC, xmu, nmu, ContOpacL, Src, s->rhox, nt);
     for (int t = 0; t < nt; t++) Xki[t] = ContOpacL[t] + LineOpacL[t];
-    or_locprf_pp(IntL, xmu, nmu, Xki, Src, s->rhox, nt);
+    if (s->radius > 0.0) {
+        or_locprf_sph(s, IntC, ContOpacL, Src);
+        or_locprf_sph(s, IntL, Xki, Src);
+    } else {
+        or_locprf_pp(IntC, xmu, nmu, ContOpacL, Src, s->rhox, nt);
+        or_locprf_pp(IntL, xmu, nmu, Xki, Src, s->rhox, nt);
+    }
     if (nmu == 1) return (float)(1.0 - IntL[0] / IntC[0]);
     double FlxL = 0.0, FlxC = 0.0;
     for (int i = 0; i < nmu; i++) { FlxL = FlxL + wmu[i] * IntL[i]; FlxC = FlxC + wmu[i] * IntC[i]; }
@@ -1140,6 +1235,80 @@ done:
     return 0;
 }
 
+/* The DELO-Bezier sweep of StokesPrfPP / StokesPrfSph (solver.f90:341-390, 486-534) along one ray of N
+ * points: XK/XKD [N][16] column-major 4x4 per point, SRC4/SRD [N][4], Deltau [N-1]; XINT2 holds the
+ * boundary Stokes vector on entry and the emergent one on return */
+static void stokes_sweep(int N, const double *XK, const double *XKD, const double *SRC4, const double *SRD,
+                         const double *Deltau, double *XINT2) {
+#define K(i, j, t) XK[(t) * 16 + ((i) - 1) + 4 * ((j) - 1)]
+#define KD(i, j, t) XKD[(t) * 16 + ((i) - 1) + 4 * ((j) - 1)]
+    double XINT1[4], XKA[16], XKB[16], QA[16], QB[16], AA[16];
+    for (int j = 1; j <= 4; j++) for (int i = 1; i <= 4; i++) {
+        double acc = 0.0;
+        for (int k = 1; k <= 4; k++) acc = acc + K(i, k, N - 1) * K(k, j, N - 1);
+        XKB[(i - 1) + 4 * (j - 1)] = acc + KD(i, j, N - 1);
+    }
+    for (int k = N - 2; k >= 0; k--) {
+        int k1 = k + 1;
+        double Dtau = Deltau[k], Dtau05 = 0.5 * Dtau, Eps, Alpha, Beta, Gamma;
+        delo_coef(Dtau, &Eps, &Alpha, &Beta, &Gamma);
+        Gamma = Gamma * 0.5;
+        memcpy(XKA, XKB, sizeof XKA);
+        for (int j = 1; j <= 4; j++) for (int i = 1; i <= 4; i++) {
+            double acc = 0.0;
+            for (int q = 1; q <= 4; q++) acc = acc + K(i, q, k) * K(q, j, k);
+            XKB[(i - 1) + 4 * (j - 1)] = acc + KD(i, j, k);
+        }
+        for (int j = 1; j <= 4; j++) for (int i = 1; i <= 4; i++) {
+            int e = (i - 1) + 4 * (j - 1);
+            QA[e] = Dtau05 * XKA[e] + (Dtau05 - 1.0) * K(i, j, k1);
+            QB[e] = -(Dtau05 * XKB[e]) - (Dtau05 + 1.0) * K(i, j, k);
+            AA[e] = ((i == j) ? 1.0 : 0.0) + Alpha * K(i, j, k) - Gamma * QB[e];
+        }
+        double GD = Gamma * Dtau05;
+        for (int i = 1; i <= 4; i++) {
+            double m1 = 0.0, m2 = 0.0, m3 = 0.0, m4 = 0.0;
+            for (int q = 1; q <= 4; q++) {
+                m1 = m1 + K(i, q, k1) * XINT2[q - 1];
+                m2 = m2 + QA[(i - 1) + 4 * (q - 1)] * XINT2[q - 1];
+                m3 = m3 + K(i, q, k1) * SRC4[4 * k1 + q - 1];
+                m4 = m4 + K(i, q, k) * SRC4[4 * k + q - 1];
+            }
+            XINT1[i - 1] = Eps * XINT2[i - 1] - Beta * m1 + Gamma * m2 + (Beta + Gamma) * SRC4[4 * k1 + i - 1]
+                         - GD * m3 + (Alpha + Gamma) * SRC4[4 * k + i - 1] + GD * m4
+                         + GD * (SRD[4 * k + i - 1] - SRD[4 * k1 + i - 1]);
+        }
+        or_solve4x4(AA, XINT1, XINT2);
+    }
+#undef K
+#undef KD
+}
+
+/* Propagation matrix normalised by PhiI and source vector at one point (solver.f90:296-330, 431-465):
+ * m = MagLineOpac(:, ia), lop/cop the line and continuum opacity there, geometry g = (SPhi2, CPhi2,
+ * CPhi, S2Psi, C2Psi) of this point; writes the 4x4 K (column-major) and SRC4, returns PhiI */
+static double stokes_point(const double *m, double lop, double cop, double Src, const double *g,
+                           double *K16, double *S4) {
+    double Php = m[0], Phb = m[1], Phr = m[2], Psp = m[3], Psb = m[4], Psr = m[5];
+    double SPhi2 = g[0], CPhi2 = g[1], CPhi = g[2], S2Psi = g[3], C2Psi = g[4];
+    double PhiI = 0.5 * (Php * SPhi2 + 0.5 * (Phr + Phb) * (1.0 + CPhi2)) + lop + cop;
+    double InvPhiI = 1.0 / PhiI;
+    double Sabs = 0.5 * (Php - 0.5 * (Phr + Phb)) * SPhi2;
+    double PhiQ = Sabs * C2Psi * InvPhiI, PhiU = Sabs * S2Psi * InvPhiI;
+    double PhiV = 0.5 * (Phr - Phb) * CPhi * InvPhiI;
+    double Sdis = 0.5 * (Psp - 0.5 * (Psr + Psb)) * SPhi2;
+    double PsiQ = Sdis * C2Psi * InvPhiI, PsiU = Sdis * S2Psi * InvPhiI;
+    double PsiV = 0.5 * (Psr - Psb) * CPhi * InvPhiI;
+#define K(i, j) K16[((i) - 1) + 4 * ((j) - 1)]
+    K(1,1) = 0.0;   K(1,2) = PhiQ;  K(1,3) = PhiU;  K(1,4) = PhiV;
+    K(2,1) = PhiQ;  K(2,2) = 0.0;   K(2,3) = PsiV;  K(2,4) = -PsiU;
+    K(3,1) = PhiU;  K(3,2) = -PsiV; K(3,3) = 0.0;   K(3,4) = PsiQ;
+    K(4,1) = PhiV;  K(4,2) = PsiU;  K(4,3) = -PsiQ; K(4,4) = 0.0;
+#undef K
+    S4[0] = Src; S4[1] = Src * PhiQ; S4[2] = Src * PhiU; S4[3] = Src * PhiV;
+    return PhiI;
+}
+
 /* StokesPrfPP (solver.f90:265-394); M6 = MagLineOpac(:, :, iwl) as [ntau][6] */
 static void stokes_prf_pp(const or_state *s, const double *M6, const double *lop, const double *cop,
                           const double *Src, int nmu, const double *xmu, const double *SPhi2,
@@ -1148,113 +1317,96 @@ static void stokes_prf_pp(const or_state *s, const double *M6, const double *lop
     int N = s->ntau;
     double *XK = (double *)malloc(sizeof(double) * (16 * N * 2 + N * 10));
     double *XKD = XK + 16 * N, *XKI = XKD + 16 * N, *Deltau = XKI + N, *SRC4 = Deltau + N, *SRD = SRC4 + 4 * N;
-#define K(i, j, t) XK[(t) * 16 + ((i) - 1) + 4 * ((j) - 1)]
-#define KD(i, j, t) XKD[(t) * 16 + ((i) - 1) + 4 * ((j) - 1)]
     for (int im = 0; im < nmu; im++) {
-        for (int t = 0; t < N; t++) {
-            const double *m = M6 + 6 * t;
-            double Php = m[0], Phb = m[1], Phr = m[2], Psp = m[3], Psb = m[4], Psr = m[5];
-            double PhiI = 0.5 * (Php * SPhi2[im] + 0.5 * (Phr + Phb) * (1.0 + CPhi2[im])) + lop[t] + cop[t];
-            double InvPhiI = 1.0 / PhiI;
-            double Sabs = 0.5 * (Php - 0.5 * (Phr + Phb)) * SPhi2[im];
-            double PhiQ = Sabs * C2Psi[im] * InvPhiI, PhiU = Sabs * S2Psi[im] * InvPhiI;
-            double PhiV = 0.5 * (Phr - Phb) * CPhi[im] * InvPhiI;
-            double Sdis = 0.5 * (Psp - 0.5 * (Psr + Psb)) * SPhi2[im];
-            double PsiQ = Sdis * C2Psi[im] * InvPhiI, PsiU = Sdis * S2Psi[im] * InvPhiI;
-            double PsiV = 0.5 * (Psr - Psb) * CPhi[im] * InvPhiI;
-            XKI[t] = PhiI;
-            K(1,1,t) = 0.0;   K(1,2,t) = PhiQ;  K(1,3,t) = PhiU;  K(1,4,t) = PhiV;
-            K(2,1,t) = PhiQ;  K(2,2,t) = 0.0;   K(2,3,t) = PsiV;  K(2,4,t) = -PsiU;
-            K(3,1,t) = PhiU;  K(3,2,t) = -PsiV; K(3,3,t) = 0.0;   K(3,4,t) = PsiQ;
-            K(4,1,t) = PhiV;  K(4,2,t) = PsiU;  K(4,3,t) = -PsiQ; K(4,4,t) = 0.0;
-            SRC4[4 * t + 0] = Src[t]; SRC4[4 * t + 1] = Src[t] * PhiQ;
-            SRC4[4 * t + 2] = Src[t] * PhiU; SRC4[4 * t + 3] = Src[t] * PhiV;
-        }
+        double g[5] = { SPhi2[im], CPhi2[im], CPhi[im], S2Psi[im], C2Psi[im] };
+        for (int t = 0; t < N; t++) XKI[t] = stokes_point(M6 + 6 * t, lop[t], cop[t], Src[t], g, XK + 16 * t, SRC4 + 4 * t);
         or_taustep(s->rhox, XKI, xmu[im], N, Deltau);
         or_centder(Deltau, SRC4, 4, N, SRD);
         or_centder(Deltau, XK, 16, N, XKD);
-        double XINT2[4] = { SRC4[4 * (N - 1)], 0.0, 0.0, 0.0 }, XINT1[4];
-        double XKA[16], XKB[16], QA[16], QB[16], AA[16];
-        for (int j = 1; j <= 4; j++) for (int i = 1; i <= 4; i++) {
-            double acc = 0.0;
-            for (int k = 1; k <= 4; k++) acc = acc + K(i, k, N - 1) * K(k, j, N - 1);
-            XKB[(i - 1) + 4 * (j - 1)] = acc + KD(i, j, N - 1);
-        }
-        for (int k = N - 2; k >= 0; k--) {
-            int k1 = k + 1;
-            double Dtau = Deltau[k], Dtau05 = 0.5 * Dtau, Eps, Alpha, Beta, Gamma;
-            delo_coef(Dtau, &Eps, &Alpha, &Beta, &Gamma);
-            Gamma = Gamma * 0.5;
-            memcpy(XKA, XKB, sizeof XKA);
-            for (int j = 1; j <= 4; j++) for (int i = 1; i <= 4; i++) {
-                double acc = 0.0;
-                for (int q = 1; q <= 4; q++) acc = acc + K(i, q, k) * K(q, j, k);
-                XKB[(i - 1) + 4 * (j - 1)] = acc + KD(i, j, k);
-            }
-            for (int j = 1; j <= 4; j++) for (int i = 1; i <= 4; i++) {
-                int e = (i - 1) + 4 * (j - 1);
-                QA[e] = Dtau05 * XKA[e] + (Dtau05 - 1.0) * K(i, j, k1);
-                QB[e] = -(Dtau05 * XKB[e]) - (Dtau05 + 1.0) * K(i, j, k);
-                AA[e] = ((i == j) ? 1.0 : 0.0) + Alpha * K(i, j, k) - Gamma * QB[e];
-            }
-            double GD = Gamma * Dtau05;
-            for (int i = 1; i <= 4; i++) {
-                double m1 = 0.0, m2 = 0.0, m3 = 0.0, m4 = 0.0;
-                for (int q = 1; q <= 4; q++) {
-                    m1 = m1 + K(i, q, k1) * XINT2[q - 1];
-                    m2 = m2 + QA[(i - 1) + 4 * (q - 1)] * XINT2[q - 1];
-                    m3 = m3 + K(i, q, k1) * SRC4[4 * k1 + q - 1];
-                    m4 = m4 + K(i, q, k) * SRC4[4 * k + q - 1];
-                }
-                XINT1[i - 1] = Eps * XINT2[i - 1] - Beta * m1 + Gamma * m2 + (Beta + Gamma) * SRC4[4 * k1 + i - 1]
-                             - GD * m3 + (Alpha + Gamma) * SRC4[4 * k + i - 1] + GD * m4
-                             + GD * (SRD[4 * k + i - 1] - SRD[4 * k1 + i - 1]);
-            }
-            or_solve4x4(AA, XINT1, XINT2);
-        }
+        double XINT2[4] = { SRC4[4 * (N - 1)], 0.0, 0.0, 0.0 };
+        stokes_sweep(N, XK, XKD, SRC4, SRD, Deltau, XINT2);
         for (int q = 0; q < 4; q++) Stokes[q * nmu + im] = XINT2[q];
     }
-#undef K
-#undef KD
     free(XK);
 }
 
-/* MagRadTranCalc plane-parallel (synth.f90:1904-2012) */
+/* StokesPrfSph (solver.f90:402-538): the same along the rays of s; geometry G [5][nmu][2 ntau] per ray
+ * point (SPhi2S, CPhi2S, CPhiS, S2PsiS, C2PsiS); zero incoming Stokes vector for grazing rays */
+static void stokes_prf_sph(const or_state *s, const double *M6, const double *lop, const double *cop,
+                           const double *Src, const double *G, double *Stokes /*[4][nmu]*/) {
+    const int M = 2 * s->ntau, nmu = s->sph_nmu;
+    double *XK = (double *)malloc(sizeof(double) * (16 * M * 2 + M * 10));
+    double *XKD = XK + 16 * M, *XKI = XKD + 16 * M, *Deltau = XKI + M, *SRC4 = Deltau + M, *SRD = SRC4 + 4 * M;
+    for (int im = 0; im < nmu; im++) {
+        const int N = s->sph_ntau[im];
+        const int *mp = s->sph_map + (size_t)im * M;
+        for (int k = 0; k < N; k++) {
+            int ia = mp[k] - 1;
+            size_t o = (size_t)im * M + k, st = (size_t)nmu * M;
+            double g[5] = { G[o], G[st + o], G[2 * st + o], G[3 * st + o], G[4 * st + o] };
+            XKI[k] = stokes_point(M6 + 6 * ia, lop[ia], cop[ia], Src[ia], g, XK + 16 * k, SRC4 + 4 * k);
+        }
+        or_taustep(s->sph_rhox + (size_t)im * M, XKI, 1.0, N, Deltau);
+        or_centder(Deltau, SRC4, 4, N, SRD);
+        or_centder(Deltau, XK, 16, N, XKD);
+        double XINT2[4] = { s->sph_graz[im] ? 0.0 : SRC4[4 * (N - 1)], 0.0, 0.0, 0.0 };
+        stokes_sweep(N, XK, XKD, SRC4, SRD, Deltau, XINT2);
+        for (int q = 0; q < 4; q++) Stokes[q * nmu + im] = XINT2[q];
+    }
+    free(XK);
+}
+
+/* Field projection of MagRadTranCalc (synth.f90:1931-1993, 2022-2087) for one disk position or ray
+ * point: frame 1 and 2 give (gamma, psi) directly (j = the angle index for frame 2), frame 0 projects
+ * the stellar-frame field with the local cosine Coslon */
+static void field_geometry(int bframe, const double *bfield, int j, double Coslon, double *g) {
+    const double d2r = C_PI / 180.0;
+    double Sphi, Spsi, Cpsi, Cg;
+    if (bframe == 1) {
+        Sphi = sin(bfield[1] * d2r); Spsi = sin(bfield[2] * d2r); Cpsi = cos(bfield[2] * d2r); Cg = cos(bfield[1] * d2r);
+    } else if (bframe == 2) {
+        Sphi = sin(bfield[2 * j + 1] * d2r); Spsi = sin(bfield[2 * j + 2] * d2r);
+        Cpsi = cos(bfield[2 * j + 2] * d2r); Cg = cos(bfield[2 * j + 1] * d2r);
+    } else {
+        double Fldmod = sqrt(bfield[0] * bfield[0] + bfield[1] * bfield[1] + bfield[2] * bfield[2]);
+        if (Fldmod > 0.0) {
+            double Sinlon = sqrt(1.0 - Coslon * Coslon);
+            double Bx = bfield[0] * Sinlon + bfield[2] * Coslon, By = bfield[1];
+            double Bz = bfield[0] * Coslon - bfield[2] * Sinlon, Bt = sqrt(Bx * Bx + By * By);
+            Sphi = Bt / Fldmod; Cg = Bz / Fldmod;
+            if (Bt > 0.0) { Spsi = By / Bt; Cpsi = Bx / Bt; } else { Spsi = 0.0; Cpsi = 1.0; }
+        } else { Sphi = 0.0; Cg = 1.0; Spsi = 0.0; Cpsi = 1.0; }
+    }
+    g[0] = Sphi * Sphi; g[1] = Cg * Cg; g[2] = Cg; g[3] = 2.0 * Spsi * Cpsi; g[4] = Cpsi * Cpsi - Spsi * Spsi;
+}
+
+/* MagRadTranCalc (synth.f90:1904-2111): StokesPrfPP with one projection per angle for plane-parallel
+ * models; StokesPrfSph with the projection at every ray point for spherical ones */
 void or_mag_radtran(const or_state *s, int nmu, const double *xmu, int bframe,
                     const double *bfield, const double *lineopac, const double *maglineopac,
                     double *spz, double *spc) {
+    const int sph = s->radius > 0.0, nt = s->ntau, M = 2 * nt;
     double SPhi2[nmu], CPhi2[nmu], CPhi[nmu], S2Psi[nmu], C2Psi[nmu];
-    const double d2r = C_PI / 180.0;
-    if (bframe == 1) {
-        double Sphi = sin(bfield[1] * d2r), Spsi = sin(bfield[2] * d2r), Cpsi = cos(bfield[2] * d2r);
-        double cg = cos(bfield[1] * d2r);
+    double *G = NULL;
+    if (!sph) {
         for (int im = 0; im < nmu; im++) {
-            CPhi[im] = cg; SPhi2[im] = Sphi * Sphi; CPhi2[im] = cg * cg;
-            S2Psi[im] = 2.0 * Spsi * Cpsi; C2Psi[im] = Cpsi * Cpsi - Spsi * Spsi;
-        }
-    } else if (bframe == 2) {
-        for (int im = 0; im < nmu; im++) {
-            double Sphi = sin(bfield[2 * im + 1] * d2r), Spsi = sin(bfield[2 * im + 2] * d2r);
-            double Cpsi = cos(bfield[2 * im + 2] * d2r);
-            CPhi[im] = cos(bfield[2 * im + 1] * d2r); SPhi2[im] = Sphi * Sphi; CPhi2[im] = CPhi[im] * CPhi[im];
-            S2Psi[im] = 2.0 * Spsi * Cpsi; C2Psi[im] = Cpsi * Cpsi - Spsi * Spsi;
+            double g[5];
+            field_geometry(bframe, bfield, im, xmu[im], g);
+            SPhi2[im] = g[0]; CPhi2[im] = g[1]; CPhi[im] = g[2]; S2Psi[im] = g[3]; C2Psi[im] = g[4];
         }
     } else {
-        double Fldmod = sqrt(bfield[0] * bfield[0] + bfield[1] * bfield[1] + bfield[2] * bfield[2]);
+        /* frame 1 fills every point of every ray, frames 2 and 0 the points each ray has */
+        size_t st = (size_t)nmu * M;
+        G = (double *)calloc(5 * st, sizeof(double));
         for (int im = 0; im < nmu; im++) {
-            double Sphi, Spsi, Cpsi;
-            if (Fldmod > 0.0) {
-                double Coslon = xmu[im], Sinlon = sqrt(1.0 - Coslon * Coslon);
-                double Bx = bfield[0] * Sinlon + bfield[2] * Coslon, By = bfield[1];
-                double Bz = bfield[0] * Coslon - bfield[2] * Sinlon, Bt = sqrt(Bx * Bx + By * By);
-                Sphi = Bt / Fldmod; CPhi[im] = Bz / Fldmod;
-                if (Bt > 0.0) { Spsi = By / Bt; Cpsi = Bx / Bt; } else { Spsi = 0.0; Cpsi = 1.0; }
-            } else { Sphi = 0.0; CPhi[im] = 1.0; Spsi = 0.0; Cpsi = 1.0; }
-            SPhi2[im] = Sphi * Sphi; CPhi2[im] = CPhi[im] * CPhi[im];
-            S2Psi[im] = 2.0 * Spsi * Cpsi; C2Psi[im] = Cpsi * Cpsi - Spsi * Spsi;
+            int np = (bframe == 1) ? M : s->sph_ntau[im];
+            for (int k = 0; k < np; k++) {
+                double g[5];
+                field_geometry(bframe, bfield, im, s->sph_muloc[(size_t)im * M + k], g);
+                for (int q = 0; q < 5; q++) G[q * st + (size_t)im * M + k] = g[q];
+            }
         }
     }
-    int nt = s->ntau;
     #pragma omp parallel
     {
         double *Src = (double *)malloc(sizeof(double) * nt);
@@ -1262,12 +1414,19 @@ void or_mag_radtran(const or_state *s, int nmu, const double *xmu, int bframe,
         for (int iwl = 0; iwl < s->nwl; iwl++) {
             planck(s, s->wave[iwl] + s->wfirst, Src);
             const double *co = s->contopac + (size_t)iwl * nt;
-            if (spc) or_locprf_pp(spc + (size_t)iwl * nmu, xmu, nmu, co, Src, s->rhox, nt);
-            stokes_prf_pp(s, maglineopac + (size_t)iwl * nt * 6, lineopac + (size_t)iwl * nt, co, Src,
-                          nmu, xmu, SPhi2, CPhi2, CPhi, S2Psi, C2Psi, spz + (size_t)iwl * 4 * nmu);
+            if (sph) {
+                if (spc) or_locprf_sph(s, spc + (size_t)iwl * nmu, co, Src);
+                stokes_prf_sph(s, maglineopac + (size_t)iwl * nt * 6, lineopac + (size_t)iwl * nt, co, Src, G,
+                               spz + (size_t)iwl * 4 * nmu);
+            } else {
+                if (spc) or_locprf_pp(spc + (size_t)iwl * nmu, xmu, nmu, co, Src, s->rhox, nt);
+                stokes_prf_pp(s, maglineopac + (size_t)iwl * nt * 6, lineopac + (size_t)iwl * nt, co, Src,
+                              nmu, xmu, SPhi2, CPhi2, CPhi, S2Psi, C2Psi, spz + (size_t)iwl * 4 * nmu);
+            }
         }
         free(Src);
     }
+    free(G);
 }
 
 /* ---- quadrature and disk integration ---------------------------------------------------- */

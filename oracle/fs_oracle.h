@@ -71,7 +71,23 @@ typedef struct {
     /* XlineInit state (opacity.f90:65-93) */
     double *x_nprtb, *x_gvwprt, *x_temp6, *x_temp3, *x_kbt, *x_kbet;
     double  x_vturb2;
+
+    /* geometry (shared.f90:527, solver.f90:27-33): radius <= 0 is plane-parallel; otherwise
+     * the rays of or_sphere_init for sph_nmu angles, arrays [nmu][2*ntau] (NtauMu, GrazMu,
+     * MapMu 1-based, RhoxMu, MuLoc) */
+    double  radius;
+    int     sph_nmu;
+    const int    *sph_ntau, *sph_graz, *sph_map;
+    const double *sph_rhox, *sph_muloc;
 } or_state;
+
+/* SphereInit (solver.f90:45-120): rays of a spherical model for the nmu angles xmu; layer radii
+ * radius + height[k].  Outputs [nmu] (ntau_mu, graz) and [nmu][2*ntau] (map 1-based, rhox_mu,
+ * mu_loc).  Returns 0; -1 for an angle mu <= 0; -2 for a grazing ray tangent in the top layer. */
+int or_sphere_init(int ntau, const double *rhox, const double *height, double radius, int nmu,
+                   const double *xmu, int *ntau_mu, int *graz, int *map, double *rhox_mu, double *mu_loc);
+/* LocPrfSph (solver.f90:182-216) + DeloScalar (solver.f90:220-261) over the rays of s */
+void or_locprf_sph(const or_state *s, double *Ploc, const double *Xki, const double *Src);
 
 /* ---- Line list (SoA; LineData records shared.f90:451-482) ----------------------------- */
 typedef struct {
@@ -126,10 +142,12 @@ void or_locprf_pp(double *ploc, const double *xmu, int nmu, const double *xki,
                   const double *src, const double *rhox, int ntau);
 void or_solve4x4(const double *a /*[4][4] col-major*/, const double *b, double *x);
 
-/* RadTranCalc (synth.f90:1825-1901): spl/spc [nwl][nmu] */
+/* RadTranCalc (synth.f90:1825-1901): spl/spc [nwl][nmu]; spherical (s->radius > 0) along the rays
+ * of s, whose angles must be xmu */
 void or_radtran(const or_state *s, int nmu, const double *xmu, const double *lineopac,
                 double *spl, double *spc);
-/* MagRadTranCalc (synth.f90:1904-2012), plane-parallel: spz [nwl][4][nmu], spc [nwl][nmu] */
+/* MagRadTranCalc (synth.f90:1904-2111): spz [nwl][4][nmu], spc [nwl][nmu]; spherical when
+ * s->radius > 0 (StokesPrfSph along the rays of s) */
 void or_mag_radtran(const or_state *s, int nmu, const double *xmu, int bframe,
                     const double *bfield, const double *lineopac, const double *maglineopac,
                     double *spz, double *spc);

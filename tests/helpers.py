@@ -60,3 +60,19 @@ def mag_pin_setup(d):
     lines = pin_lines(d)
     z = (d["z_npi"], d["z_nsi"], d["z_spl_pi"], d["z_str_pi"], d["z_spl_si"], d["z_str_si"])
     return grid, st, co, lines, z
+
+
+def sphere_pin(part):
+    """One half of pin_sphere.npz as a pin dict: part "s" (scalar, solar atmosphere, the pin_solar
+    list) or "m" (polarised, magnetic atmosphere, stellar-frame field, Zeeman lines)."""
+    d = load_pin("pin_sphere")
+    out = {k[2:]: v for k, v in d.items() if k.startswith(part + "_")}
+    out["atm"] = "solar" if part == "s" else "magnetic"
+    if part == "s":
+        out.update({k: v for k, v in load_pin("pin_solar").items() if k.startswith("line_")})
+        out["vmicro"], out["molbrd"] = 1.0, 0
+    else:
+        out.update({"line_" + k[6:]: v for k, v in d.items() if k.startswith("mline_")})
+        out.update({k: v for k, v in d.items() if k.startswith("z_")})
+        out["vmicro"], out["molbrd"] = 1.0, 0
+    return out
