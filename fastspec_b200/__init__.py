@@ -124,6 +124,7 @@ def lib():
     L.fsg_lineop_device_ptr.argtypes = [C.c_void_p]
     L.fsg_lineop_device_ptr.restype = C.c_void_p
     L.fsg_set_mu.argtypes = [C.c_void_p, C.c_int, _dp, _dp]
+    L.fsg_set_geometry.argtypes = [C.c_void_p, C.c_double, _dp]
     L.fsg_radtran.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
     L.fsg_radtran_dev.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.fsg_mag_lineop_calc.argtypes = [C.c_void_p, C.POINTER(CLines), C.c_int, _dp, C.c_int, _dp, _ip, _ip,
@@ -320,6 +321,13 @@ class Context:
 
     def set_contopac_dev(self, ptr):
         self._ck(self._lib.fsg_set_contopac_dev(self.h, C.c_void_p(ptr)), "fsg_set_contopac_dev")
+
+    def set_geometry(self, radius, height=None):
+        """fsg_set_geometry: spherical model of the given radius [cm] and layer heights [cm]
+        (after set_atmosphere, which resets the model to plane-parallel); radius <= 0: plane-parallel."""
+        h = None if height is None else _f64(height)
+        self._keep["height"] = h
+        self._ck(self._lib.fsg_set_geometry(self.h, float(radius), _p(h, C.c_double)), "fsg_set_geometry")
 
     def set_mu(self, xmu, wmu):
         xmu = _f64(xmu); wmu = _f64(wmu)

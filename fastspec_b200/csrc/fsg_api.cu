@@ -61,7 +61,11 @@ int fsg_launch_adjoint(cudaStream_t, const AtmView &, const LineView &, const Vo
                        const int32_t *, const double *, double *, double *, double, double *, double *);
 size_t fsg_linstr_work(int64_t, int, int);
 void fsg_launch_linstr(cudaStream_t, const AtmView &, const LineView &, const VoigtTables &, const int32_t *, int64_t,
-                       int64_t, int, const double *, const double *, const double *, double *, float *);
+                       int64_t, int, const double *, const double *, const double *, const RayView &, double *, float *);
+int fsg_launch_radtran_sph(cudaStream_t, const AtmView &, const double *, const RayView &, const double *, double *,
+                           double *, double *, double *);
+int fsg_launch_stokes_sph(cudaStream_t, const AtmView &, const double *, const double *, const RayView &,
+                          const double *, const double *, double *, double *);
 int fsg_launch_tile_span(cudaStream_t, int, int, int64_t, const LineHdr *, int *, int *, void *, size_t);
 int fsg_select(cudaStream_t, int64_t, const int32_t *, const int32_t *, const int32_t *, int, int *, int64_t *,
                int64_t *, int64_t *);
@@ -136,6 +140,14 @@ struct fsg_ctx {
     // mu
     int nmu = 0;
     DBuf d_xmu, d_wmu;
+    std::vector<double> h_xmu;
+    // geometry: radius <= 0 plane-parallel; spherical rays (SphereInit) rebuilt when mu, the
+    // atmosphere or the geometry change
+    double radius = -1.0;
+    std::vector<double> h_rhox, h_height, h_muloc;
+    std::vector<int> h_ray_n;
+    int rays_ok = 0;
+    DBuf d_ray_n, d_ray_graz, d_ray_map, d_ray_m, d_ray_geo;
     // accumulators
     DBuf d_lineopac, d_maglineopac;
     // line list staging + per-line outputs
@@ -234,7 +246,8 @@ void fsg_destroy(fsg_ctx *ctx) {
                      &ctx->d_pw, &ctx->d_evals, &ctx->d_spl, &ctx->d_spc, &ctx->d_sfl, &ctx->d_sfc,
                      &ctx->d_work, &ctx->d_a, &ctx->d_v, &ctx->d_h, &ctx->d_l, &ctx->z_npi, &ctx->z_nsi,
                      &ctx->z_pioff, &ctx->z_sioff, &ctx->z_splpi, &ctx->z_strpi, &ctx->z_splsi, &ctx->z_strsi,
-                     &ctx->d_zsc, &ctx->z_rawpi, &ctx->z_rawsi, &ctx->d_zmap, &ctx->d_geo };
+                     &ctx->d_zsc, &ctx->z_rawpi, &ctx->z_rawsi, &ctx->d_zmap, &ctx->d_geo,
+                     &ctx->d_ray_n, &ctx->d_ray_graz, &ctx->d_ray_map, &ctx->d_ray_m, &ctx->d_ray_geo };
     for (DBuf *b : bufs) b->release();
     for (int i = 0; i < 8; i++) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
     for (cudaEvent_t e : ctx->cev) cudaEventDestroy(e);
@@ -315,6 +328,26 @@ int fsg_set_atmosphere(fsg_ctx *ctx, int ntau, const double *rhox, const double 
     CK(cudaGetLastError(), "k_xline_init");
     CK(cudaStreamSynchronize(s), "atm upload");
     ctx->have_atm = 1; ctx->have_cont = 0;
+    // a new model is plane-parallel until fsg_set_geometry says otherwise (ReadModel, ioutils.f90:1622)
+    ctx->h_rhox.assign(rhox, rhox + ntau);
+    ctx->radius = -1.0; ctx->h_height.clear(); ctx->rays_ok = 0;
+    return FSG_OK;
+}
+
+int fsg_set_geometry(fsg_ctx *ctx, double radius, const double *height) {
+    if (!ctx) return FSG_E_ARG;
+    if (!ctx->have_atm) return fail(ctx, FSG_E_STATE, "fsg_set_geometry: set the atmosphere first");
+    ctx->rays_ok = 0;
+    if (radius <= 0.0) { ctx->radius = -1.0; ctx->h_height.clear(); return FSG_OK; }
+    const int nt = ctx->ntau;
+    if (!height) return fail(ctx, FSG_E_ARG, "fsg_set_geometry: a spherical model needs the layer heights");
+    if (radius < 1e9 || radius > 1e15) return fail(ctx, FSG_E_ARG, "fsg_set_geometry: implausible model radius");
+    for (int t = 1; t < nt; t++)
+        if (!(height[t] < height[t - 1]))
+            return fail(ctx, FSG_E_ARG, "fsg_set_geometry: heights of a spherical model do not decrease inward");
+    if (!(radius + height[nt - 1] > 0.0)) return fail(ctx, FSG_E_ARG, "fsg_set_geometry: negative layer radius");
+    ctx->radius = radius;
+    ctx->h_height.assign(height, height + nt);
     return FSG_OK;
 }
 
@@ -373,6 +406,79 @@ int fsg_set_mu(fsg_ctx *ctx, int nmu, const double *xmu, const double *wmu) {
     CK(cudaMemcpyAsync(ctx->d_wmu.p, wmu, sizeof(double) * nmu, cudaMemcpyHostToDevice, ctx->stream), "mu upload");
     CK(cudaStreamSynchronize(ctx->stream), "mu upload");
     ctx->nmu = nmu;
+    ctx->h_xmu.assign(xmu, xmu + nmu);
+    ctx->rays_ok = 0;
+    return FSG_OK;
+}
+
+// SphereInit (solver.f90:45-120) on the host, once per model and angle set (set-up, as in the
+// reference's Init, synth.f90:306): for ray im with impact parameter p = r_top sqrt(1 - mu^2), the
+// column mass along the ray grows by the radial step times (r_k + r_k-1) / (z_k + z_k-1), z the
+// distance sqrt(r^2 - p^2) in the factored form; a ray with p above the bottom radius turns inside the
+// shell below its deepest layer n (the chord times dm/dr crosses it) and comes back through n..1 with
+// mirrored steps and the local cosine negated.  Uploads RayView arrays [nmu][2 ntau]; R->nmu = 0 for a
+// plane-parallel model.
+static int rays_prepare(fsg_ctx *ctx, RayView *R) {
+    memset(R, 0, sizeof *R);
+    if (ctx->radius <= 0.0) return FSG_OK;
+    const int nt = ctx->ntau, nmu = ctx->nmu, M = 2 * nt;
+    R->nmu = nmu; R->stride = M;
+    if (!ctx->rays_ok) {
+        std::vector<double> rk(nt), rm((size_t)nmu * M, 0.0), ml((size_t)nmu * M, 0.0);
+        std::vector<int> n(nmu), gz(nmu), mp((size_t)nmu * M, 0);
+        for (int k = 0; k < nt; k++) rk[k] = ctx->radius + ctx->h_height[k];
+        const double *rhox = ctx->h_rhox.data();
+        for (int im = 0; im < nmu; im++) {
+            const double mu = ctx->h_xmu[im];
+            double *m = &rm[(size_t)im * M], *c = &ml[(size_t)im * M];
+            int *q = &mp[(size_t)im * M];
+            if (!(mu > 0.0)) return fail(ctx, FSG_E_ARG, "SphereInit: mu = 0 rays are unsupported for spherical models");
+            const double P = rk[0] * sqrt((1.0 - mu) * (1.0 + mu));
+            const int g = P > rk[nt - 1];
+            int deep = nt;
+            if (g) {
+                int kt = 2;
+                while (kt <= nt && !(P >= rk[kt - 1])) kt++;
+                deep = kt - 1;
+                if (deep < 2) return fail(ctx, FSG_E_ARG, "SphereInit: grazing ray tangent in the top model layer");
+            }
+            m[0] = rhox[0] / mu;
+            double z1 = sqrt((rk[0] - P) * (rk[0] + P));
+            c[0] = z1 / rk[0];
+            for (int k = 1; k < deep; k++) {
+                double z = sqrt((rk[k] - P) * (rk[k] + P));
+                m[k] = m[k - 1] + (rhox[k] - rhox[k - 1]) * (rk[k] + rk[k - 1]) / (z + z1);
+                c[k] = z / rk[k];
+                q[k] = k;
+                z1 = z;
+            }
+            gz[im] = g;
+            n[im] = nt;
+            if (!g) continue;
+            double chord = 2.0 * sqrt((rk[deep - 1] - P) * (rk[deep - 1] + P));
+            m[deep] = m[deep - 1] + chord * (rhox[deep] - rhox[deep - 1]) / (rk[deep - 1] - rk[deep]);
+            q[deep] = deep - 1;
+            c[deep] = -c[deep - 1];
+            for (int k = deep + 1; k < 2 * deep; k++) {          // the far half mirrors the near one
+                m[k] = m[k - 1] + (m[2 * deep - k] - m[2 * deep - k - 1]);
+                q[k] = 2 * deep - 1 - k;
+                c[k] = -c[2 * deep - 1 - k];
+            }
+            n[im] = 2 * deep;
+        }
+        ALLOC(ctx->d_ray_n, sizeof(int) * nmu); ALLOC(ctx->d_ray_graz, sizeof(int) * nmu);
+        ALLOC(ctx->d_ray_map, sizeof(int) * mp.size()); ALLOC(ctx->d_ray_m, sizeof(double) * rm.size());
+        cudaStream_t s = ctx->stream;
+        CK(cudaMemcpyAsync(ctx->d_ray_n.p, n.data(), sizeof(int) * nmu, cudaMemcpyHostToDevice, s), "rays");
+        CK(cudaMemcpyAsync(ctx->d_ray_graz.p, gz.data(), sizeof(int) * nmu, cudaMemcpyHostToDevice, s), "rays");
+        CK(cudaMemcpyAsync(ctx->d_ray_map.p, mp.data(), sizeof(int) * mp.size(), cudaMemcpyHostToDevice, s), "rays");
+        CK(cudaMemcpyAsync(ctx->d_ray_m.p, rm.data(), sizeof(double) * rm.size(), cudaMemcpyHostToDevice, s), "rays");
+        CK(cudaStreamSynchronize(s), "rays");
+        ctx->h_muloc.swap(ml); ctx->h_ray_n.swap(n);
+        ctx->rays_ok = 1;
+    }
+    R->n = ctx->d_ray_n.as<int>(); R->graz = ctx->d_ray_graz.as<int>();
+    R->map = ctx->d_ray_map.as<int>(); R->m = ctx->d_ray_m.as<double>();
     return FSG_OK;
 }
 
@@ -913,9 +1019,11 @@ static int linstr_calc(fsg_ctx *ctx, const fsg_lines *D, float *linstr) {
     ALLOC(ctx->d_linstr, sizeof(float) * (size_t)n);
     LineView LV = make_view(D);
     AtmView A = fsg_view(ctx);
+    RayView R;
+    int rc = rays_prepare(ctx, &R); if (rc) return rc;
     for (int64_t i0 = 0; i0 < n; i0 += chunk) {
         fsg_launch_linstr(s, A, LV, ctx->tab, ctx->d_flags.as<int32_t>(), i0, std::min(chunk, n - i0), ctx->nmu,
-                          ctx->d_xmu.as<double>(), ctx->d_wmu.as<double>(), ctx->d_rhox.as<double>(),
+                          ctx->d_xmu.as<double>(), ctx->d_wmu.as<double>(), ctx->d_rhox.as<double>(), R,
                           ctx->d_lswork.as<double>(), ctx->d_linstr.as<float>());
         ctx->launches += 1;
     }
@@ -953,8 +1061,14 @@ static int radtran_dev(fsg_ctx *ctx, double *spl, double *spc, double *sfl, doub
         return fail(ctx, FSG_E_STATE, "radtran: set grid, atmosphere, continuum and mu first");
     int rc = ensure_lineopac(ctx); if (rc) return rc;
     AtmView A = fsg_view(ctx);
-    rc = fsg_launch_radtran(ctx->stream, A, ctx->d_lineopac.as<double>(), ctx->d_rhox.as<double>(), ctx->nmu,
-                            ctx->d_xmu.as<double>(), ctx->d_wmu.as<double>(), spl, spc, sfl, sfc);
+    RayView R;
+    rc = rays_prepare(ctx, &R); if (rc) return rc;
+    if (R.nmu > 0)
+        rc = fsg_launch_radtran_sph(ctx->stream, A, ctx->d_lineopac.as<double>(), R, ctx->d_wmu.as<double>(), spl, spc,
+                                    sfl, sfc);
+    else
+        rc = fsg_launch_radtran(ctx->stream, A, ctx->d_lineopac.as<double>(), ctx->d_rhox.as<double>(), ctx->nmu,
+                                ctx->d_xmu.as<double>(), ctx->d_wmu.as<double>(), spl, spc, sfl, sfc);
     ctx->launches += 1;
     if (rc) return cuda_fail(ctx, cudaGetLastError(), "k_radtran");
     return FSG_OK;
@@ -1251,7 +1365,60 @@ int fsg_mag_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, int bframe, const 
     return FSG_OK;
 }
 
-// ---- MagRadTranCalc, plane-parallel (synth.f90:1904-2012) ----------------------------------------
+// ---- MagRadTranCalc (synth.f90:1904-2111) --------------------------------------------------------------
+// Field projection for one disk position or ray point (synth.f90:1931-1993, 2022-2087): frames 1 and 2
+// give (gamma, psi) directly (j = the angle's pair for frame 2), frame 0 projects the stellar-frame
+// field with the local cosine Coslon.  g = (SPhi2, CPhi2, CPhi, S2Psi, C2Psi).
+static void field_geometry(int bframe, const double *bfield, int j, double Coslon, double *g) {
+    const double d2r = FSG_PI / 180.0;
+    double Sphi, Spsi, Cpsi, CPhi;
+    if (bframe == 1) {
+        Sphi = sin(bfield[1] * d2r); Spsi = sin(bfield[2] * d2r); Cpsi = cos(bfield[2] * d2r); CPhi = cos(bfield[1] * d2r);
+    } else if (bframe == 2) {
+        Sphi = sin(bfield[2 * j + 1] * d2r); Spsi = sin(bfield[2 * j + 2] * d2r);
+        Cpsi = cos(bfield[2 * j + 2] * d2r); CPhi = cos(bfield[2 * j + 1] * d2r);
+    } else {
+        double Fldmod = sqrt(bfield[0] * bfield[0] + bfield[1] * bfield[1] + bfield[2] * bfield[2]);
+        if (Fldmod > 0.0) {
+            double Sinlon = sqrt(1.0 - Coslon * Coslon);
+            double Bx = bfield[0] * Sinlon + bfield[2] * Coslon, By = bfield[1];
+            double Bz = bfield[0] * Coslon - bfield[2] * Sinlon, Bt = sqrt(Bx * Bx + By * By);
+            Sphi = Bt / Fldmod; CPhi = Bz / Fldmod;
+            if (Bt > 0.0) { Spsi = By / Bt; Cpsi = Bx / Bt; } else { Spsi = 0.0; Cpsi = 1.0; }
+        } else { Sphi = 0.0; CPhi = 1.0; Spsi = 0.0; Cpsi = 1.0; }
+    }
+    g[0] = Sphi * Sphi; g[1] = CPhi * CPhi; g[2] = CPhi; g[3] = 2.0 * Spsi * Cpsi; g[4] = Cpsi * Cpsi - Spsi * Spsi;
+}
+
+// MagRadTranCalc for spherical models (synth.f90:2013-2108): continuum by LocPrfSph, Stokes vector by
+// StokesPrfSph with the projection at every ray point (frame 0 follows the local radial direction).
+static int mag_radtran_sph(fsg_ctx *ctx, const RayView &R, int bframe, const double *bfield, double *spz,
+                           double *spc, double *sfl, double *sfc) {
+    const int nmu = ctx->nmu, M = R.stride;
+    const size_t gs = (size_t)nmu * M;
+    std::vector<double> geo(5 * gs, 0.0);
+    for (int im = 0; im < nmu; im++)
+        for (int k = 0; k < ctx->h_ray_n[im]; k++) {
+            double g[5];
+            field_geometry(bframe, bfield, im, ctx->h_muloc[(size_t)im * M + k], g);
+            for (int q = 0; q < 5; q++) geo[q * gs + (size_t)im * M + k] = g[q];
+        }
+    cudaStream_t s = ctx->stream;
+    ALLOC(ctx->d_ray_geo, sizeof(double) * geo.size());
+    CK(cudaMemcpyAsync(ctx->d_ray_geo.p, geo.data(), sizeof(double) * geo.size(), cudaMemcpyHostToDevice, s), "geo");
+    AtmView A = fsg_view(ctx);
+    int rc = fsg_launch_radtran_sph(s, A, ctx->d_lineopac.as<double>(), R, ctx->d_wmu.as<double>(), nullptr, spc,
+                                    nullptr, sfc);
+    if (rc) return cuda_fail(ctx, cudaGetLastError(), "k_radtran_sph");
+    rc = fsg_launch_stokes_sph(s, A, ctx->d_lineopac.as<double>(), ctx->d_maglineopac.as<double>(), R,
+                               ctx->d_wmu.as<double>(), ctx->d_ray_geo.as<double>(), spz, sfl);
+    if (rc == FSG_E_ARG) return fail(ctx, FSG_E_ARG, "mag_radtran: too many depths for the spherical Stokes kernel");
+    if (rc) return cuda_fail(ctx, cudaGetLastError(), "k_stokes_sph");
+    ctx->launches += sfl ? 3 : 2;
+    return FSG_OK;
+}
+
+
 int fsg_mag_radtran(fsg_ctx *ctx, int bframe, const double *bfield, int nbfield, double *spz, double *spc,
                     double *sfl, double *sfc) {
     if (!ctx) return FSG_E_ARG;
@@ -1263,6 +1430,22 @@ int fsg_mag_radtran(fsg_ctx *ctx, int bframe, const double *bfield, int nbfield,
     cudaSetDevice(ctx->device);
     int rc = ensure_lineopac(ctx); if (rc) return rc;
     rc = ensure_maglineopac(ctx); if (rc) return rc;
+    RayView R;
+    rc = rays_prepare(ctx, &R); if (rc) return rc;
+    if (R.nmu > 0) {
+        size_t nsp = sizeof(double) * (size_t)ctx->nwl * nmu, nf = sizeof(double) * ctx->nwl;
+        ALLOC(ctx->d_spl, 4 * nsp); ALLOC(ctx->d_spc, nsp); ALLOC(ctx->d_sfl, nf); ALLOC(ctx->d_sfc, nf);
+        rc = mag_radtran_sph(ctx, R, bframe, bfield, ctx->d_spl.as<double>(), ctx->d_spc.as<double>(),
+                             ctx->d_sfl.as<double>(), ctx->d_sfc.as<double>());
+        if (rc) return rc;
+        cudaStream_t s = ctx->stream;
+        if (spz) CK(cudaMemcpyAsync(spz, ctx->d_spl.p, 4 * nsp, cudaMemcpyDeviceToHost, s), "spz");
+        if (spc) CK(cudaMemcpyAsync(spc, ctx->d_spc.p, nsp, cudaMemcpyDeviceToHost, s), "spc");
+        if (sfl) CK(cudaMemcpyAsync(sfl, ctx->d_sfl.p, nf, cudaMemcpyDeviceToHost, s), "sfl");
+        if (sfc) CK(cudaMemcpyAsync(sfc, ctx->d_sfc.p, nf, cudaMemcpyDeviceToHost, s), "sfc");
+        CK(cudaStreamSynchronize(s), "mag radtran");
+        return FSG_OK;
+    }
     std::vector<double> xmu(nmu), geo(5 * nmu);
     CK(cudaMemcpy(xmu.data(), ctx->d_xmu.p, sizeof(double) * nmu, cudaMemcpyDeviceToHost), "mu");
     const double d2r = FSG_PI / 180.0;
@@ -1645,6 +1828,7 @@ int fsg_adjoint_dev(fsg_ctx *ctx, const fsg_lines *d_lines, const double *d_gflu
                     double *d_gvmic) {
     int rc = check_lines(ctx, d_lines); if (rc) return rc;
     if (ctx->nmu < 1) return fail(ctx, FSG_E_STATE, "fsg_adjoint_dev: set mu first");
+    if (ctx->radius > 0.0) return fail(ctx, FSG_E_STATE, "fsg_adjoint_dev: plane-parallel models only");
     if (!d_gflux || !d_glin || !d_gvmic) return fail(ctx, FSG_E_ARG, "fsg_adjoint_dev: null argument");
     if (ctx->d_flags.cap < sizeof(int32_t) * (size_t)d_lines->n)
         return fail(ctx, FSG_E_STATE, "fsg_adjoint_dev: run fsg_lineop_calc(_dev) on this list first");
@@ -1810,6 +1994,7 @@ int fsg_batch_create(fsg_ctx *const *atms, int natm, const fsg_lines *lines, dou
         if (!c->have_grid || !c->have_atm || !c->have_cont || c->nmu < 1)
             return bail(FSG_E_STATE, "fsg_batch_create: set grid, atmosphere, continuum and mu of every context");
         if (c->ntau > 128) return bail(FSG_E_ARG, "fsg_batch_create: ntau <= 128");
+        if (c->radius > 0.0) return bail(FSG_E_ARG, "fsg_batch_create: plane-parallel models only");
     }
     rc = check_lines(atms[0], lines); if (rc) return bail(rc, atms[0]->err.c_str());
     bool has_he = false;

@@ -254,3 +254,57 @@ __device__ __forceinline__ void delo_coef(double Dtau, double &Eps, double &Alph
         Gamma = (2.0 * Dtau - 4.0 + (2.0 * Dtau + 4.0) * Eps) * Idtau2;
     }
 }
+
+// ---- spherical rays ---------------------------------------------------------------------------
+// TauStep (solver.f90:591-615) at point j of a ray (mu = 1 on the ray's column mass m, opacity x by
+// layer read through the map): the step from point j to j + 1, 0 <= j <= N - 2.
+__device__ __forceinline__ double ray_taustep(const int *mp, const double *m, const double *x, int j) {
+    if (j == 0) {
+        double x0 = x[mp[0]], x1 = x[mp[1]];
+        double Dx1 = m[1] - m[0], Yp = (x1 - x0) / Dx1;
+        return Dx1 * (x1 + 2.0 * x0 + Dx1 / 2.0 * Yp) / 3.0;
+    }
+    double xa = x[mp[j - 1]], xb = x[mp[j]], xc = x[mp[j + 1]];
+    double Dx = m[j] - m[j - 1], Dx1 = m[j + 1] - m[j];
+    double Der = (xb - xa) / Dx, Der1 = (xc - xb) / Dx1, Yp;
+    if (Der * Der1 > 0.0) {
+        double Lambda = (1.0 + Dx1 / (Dx + Dx1)) / 3.0;
+        Yp = (Der / (Lambda * Der1 + (1.0 - Lambda) * Der)) * Der1;
+    } else Yp = 0.0;
+    return Dx1 * (xc + 2.0 * xb + Dx1 / 2.0 * Yp) / 3.0;
+}
+
+// CentDer (solver.f90:618-647) at an interior point from the steps on either side and three values
+__device__ __forceinline__ double centder3(double Dx, double Dx1, double ya, double yb, double yc) {
+    double InvDx = 1.0 / Dx, InvDx1 = 1.0 / Dx1;
+    double Lambda = (1.0 + Dx1 / (Dx + Dx1)) / 3.0, Lambda1 = 1.0 - Lambda;
+    double Der = (yb - ya) * InvDx, Der1 = (yc - yb) * InvDx1;
+    return (Der * Der1 > 0.0) ? (Der / (Lambda * Der1 + Lambda1 * Der)) * Der1 : 0.0;
+}
+
+// LocPrfSph + DeloScalar (solver.f90:182-261) along ray im: opacity x and source y by layer.  The
+// reference builds Deltau and Srd as arrays and then sweeps; here one backward pass computes each step,
+// derivative and Bezier term U where the sweep reaches it, from the same operands, so the values are
+// the same and no per-ray arrays are needed.  Grazing rays start from zero intensity at the far side.
+__device__ __forceinline__ double delo_ray(const RayView &R, int im, const double *x, const double *y) {
+    const int N = R.n[im];
+    const int *mp = R.map + (size_t)im * R.stride;
+    const double *m = R.m + (size_t)im * R.stride;
+    double dcur = ray_taustep(mp, m, x, N - 2);                  // Deltau(N-1)
+    double yhi = y[mp[N - 1]], ylo = y[mp[N - 2]];
+    double srd_hi = (yhi - ylo) / dcur;                         // Srd(N)
+    double Y = R.graz[im] ? 0.0 : yhi;
+    for (int j = N - 2; j >= 0; j--) {
+        double yj = y[mp[j]], yj1 = y[mp[j + 1]], srd_j, dprev = 0.0;
+        if (j > 0) {
+            dprev = ray_taustep(mp, m, x, j - 1);
+            srd_j = centder3(dprev, dcur, y[mp[j - 1]], yj, yj1);
+        } else srd_j = (yj1 - yj) / dcur;
+        double Eps, Alpha, Beta, Gamma;
+        delo_coef(dcur, Eps, Alpha, Beta, Gamma);
+        double U = 0.5 * (yj + 0.5 * dcur * srd_j + yj1 - 0.5 * dcur * srd_hi);
+        Y = Y * Eps + Alpha * yj + Beta * yj1 + Gamma * U;
+        srd_hi = srd_j; dcur = dprev;
+    }
+    return Y;
+}

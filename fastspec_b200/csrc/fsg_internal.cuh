@@ -95,6 +95,15 @@ struct ZView {
     const float *rawpi, *rawsi;       // shifts as read (Lande-type units)
 };
 
+// Rays of a spherical model (SphereInit, solver.f90:45-120), device arrays [nmu][stride], stride =
+// 2 ntau.  Ray im has n[im] points (ntau, or 2 n for a grazing ray that turns below layer n); point k
+// samples layer map[im][k] (0-based) at column mass m[im][k] along the ray.  nmu = 0: plane-parallel.
+struct RayView {
+    int nmu, stride;
+    const int *n, *graz, *map;
+    const double *m;
+};
+
 // Error reporting
 std::string fsg_cuda_msg(cudaError_t e, const char *what);
 

@@ -9,6 +9,8 @@
 //   k_span, k_accum_fp64, k_wide_fp64   plain FP64 LineOpacity1 gather (opacity.f90:297-346)
 //                   and the wide-line accumulation (synth.f90:981-1001)
 //   k_radtran       RadTranCalc (synth.f90:1825-1866) + DiskInteg quadrature (convol.f90:233-234)
+//   k_radtran_sph   RadTranCalc for spherical models (synth.f90:1868-1898): LocPrfSph along each ray
+//   k_linstr        LinStrCalc (synth.f90:1774-1822), both geometries
 #include "fsg_fp64.cuh"
 
 #include <stdio.h>
@@ -597,6 +599,56 @@ int fsg_launch_radtran(cudaStream_t s, const AtmView &A, const double *lineopac,
     return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
 }
 
+// RadTranCalc for spherical models (synth.f90:1868-1898): LocPrfSph along each ray.  A CTA stages
+// RT_LW wavelengths' opacity columns and Planck source as k_radtran does; then one thread per
+// (wavelength, kind, ray) runs delo_ray, whose steps come from that ray's own column-mass scale.
+// With spl and sfl null only the continuum is solved (as MagRadTranCalc needs).
+__global__ void k_radtran_sph(AtmView A, const double *__restrict__ lineopac, RayView R,
+                              const double *__restrict__ wmu, double *spl, double *spc, double *sfl, double *sfc) {
+    extern __shared__ double sm[];
+    const int nt = A.ntau, nmu = R.nmu;
+    const int w0 = blockIdx.x * RT_LW;
+    const int nw = min(RT_LW, A.nwl - w0);
+    const int nk = (spl || sfl) ? 2 : 1;                    // kinds computed: 0 continuum, 1 line
+    double *X = sm, *S = X + 2 * RT_LW * nt, *I = S + RT_LW * nt;   // X[kind][w][t], S[w][t], I[kind][w][mu]
+    const double PlkC1 = FSG_HC * FSG_VC * 1e13 / FSG_KBOLT;
+    for (int e = threadIdx.x; e < nw * nt; e += blockDim.x) {
+        int w = e / nt, t = e - w * nt;
+        size_t g = (size_t)(w0 + w) * nt + t;
+        double c = A.contopac[g];
+        X[(0 * RT_LW + w) * nt + t] = c;
+        if (nk == 2) X[(1 * RT_LW + w) * nt + t] = c + lineopac[g];
+        double wl = A.wave[w0 + w] + A.wfirst;
+        double C1 = PlkC1 / wl, C2 = exp(50.7649141 - 5.0 * log(wl));
+        S[w * nt + t] = C2 / (exp(C1 / A.xi[XI_T * nt + t]) - 1.0);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nk * nw * nmu; e += blockDim.x) {
+        int kw = e / nmu, im = e - kw * nmu;
+        int kind = kw / nw, w = kw % nw;
+        double Y = delo_ray(R, im, X + (kind * RT_LW + w) * nt, S + w * nt);
+        I[(kind * RT_LW + w) * nmu + im] = Y;
+        double *out = (kind == 0) ? spc : spl;
+        if (out) out[(size_t)(w0 + w) * nmu + im] = Y;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nk * nw; e += blockDim.x) {
+        int kind = e / nw, w = e % nw;
+        double a = 0.0;
+        for (int im = 0; im < nmu; im++) a = a + I[(kind * RT_LW + w) * nmu + im] * wmu[im];
+        double *out = (kind == 0) ? sfc : sfl;
+        if (out) out[w0 + w] = a;
+    }
+}
+
+int fsg_launch_radtran_sph(cudaStream_t s, const AtmView &A, const double *lineopac, const RayView &R,
+                           const double *wmu, double *spl, double *spc, double *sfl, double *sfc) {
+    size_t sm = sizeof(double) * ((size_t)3 * RT_LW * A.ntau + 2 * RT_LW * R.nmu);
+    int nb = (A.nwl + RT_LW - 1) / RT_LW;
+    k_radtran_sph<<<nb, 128, sm, s>>>(A, lineopac, R, wmu, spl, spc, sfl, sfc);
+    return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
+}
+
 // ================================================================================================
 // Elemental HVoigt / FVoigt over arrays (kernel-level entry points)
 // ================================================================================================
@@ -680,14 +732,14 @@ __global__ void k_locprf(int nprof, int nmu, const double *xmu, int nt, const do
                ploc + (size_t)p * nmu);
 }
 
-// LinStrCalc (synth.f90:1774-1822), plane-parallel: central depth of each retained line from the
+// LinStrCalc (synth.f90:1774-1822): central depth of each retained line from the
 // continuum and continuum + line intensities at its centre (the centre opacities of the central
 // pass: ContOpac at Wlcent, LineOpacity2 at Wlcent), disk-integrated with Wmu when nmu > 1.
 // One thread per line of [i0, i0 + nl); work holds 6 nt + 2 nmu doubles per thread.
 __global__ void k_linstr(AtmView A, LineView L, const float *__restrict__ vtab, const double *__restrict__ anode,
                          const double *__restrict__ aida, const int32_t *__restrict__ flags, int64_t i0, int64_t nl,
                          int nmu, const double *__restrict__ xmu, const double *__restrict__ wmu,
-                         const double *__restrict__ rhox, double *work, float *linstr) {
+                         const double *__restrict__ rhox, RayView R, double *work, float *linstr) {
     const double PlkC1 = FSG_HC * FSG_VC * 1e13 / FSG_KBOLT;
     int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nl) return;
@@ -717,8 +769,12 @@ __global__ void k_linstr(AtmView A, LineView L, const float *__restrict__ vtab, 
         xl[t] = co + lo;
         y[t] = C2 / (exp(C1 / A.xi[XI_T * nt + t]) - 1.0);
     }
-    locprf_one(nmu, xmu, nt, xc, y, rhox, d, d + nt, d + 2 * nt, ic);
-    locprf_one(nmu, xmu, nt, xl, y, rhox, d, d + nt, d + 2 * nt, il);
+    if (R.nmu > 0) {                       // spherical: LocPrfSph (synth.f90:1801-1803)
+        for (int m = 0; m < nmu; m++) { ic[m] = delo_ray(R, m, xc, y); il[m] = delo_ray(R, m, xl, y); }
+    } else {
+        locprf_one(nmu, xmu, nt, xc, y, rhox, d, d + nt, d + 2 * nt, ic);
+        locprf_one(nmu, xmu, nt, xl, y, rhox, d, d + nt, d + 2 * nt, il);
+    }
     if (nmu == 1) { linstr[i] = (float)(1.0 - il[0] / ic[0]); return; }
     double FlxL = 0.0, FlxC = 0.0;
     for (int m = 0; m < nmu; m++) { FlxL = FlxL + wmu[m] * il[m]; FlxC = FlxC + wmu[m] * ic[m]; }
@@ -729,10 +785,10 @@ size_t fsg_linstr_work(int64_t nl, int nt, int nmu) { return sizeof(double) * (s
 
 void fsg_launch_linstr(cudaStream_t s, const AtmView &A, const LineView &L, const VoigtTables &T,
                        const int32_t *flags, int64_t i0, int64_t nl, int nmu, const double *xmu, const double *wmu,
-                       const double *rhox, double *work, float *linstr) {
+                       const double *rhox, const RayView &R, double *work, float *linstr) {
     if (nl > 0)
         k_linstr<<<(unsigned)((nl + 127) / 128), 128, 0, s>>>(A, L, T.vtab, T.anode, T.aida, flags, i0, nl, nmu,
-                                                              xmu, wmu, rhox, work, linstr);
+                                                              xmu, wmu, rhox, R, work, linstr);
 }
 
 void fsg_launch_locprf(cudaStream_t s, int nprof, int nmu, const double *xmu, int nt, const double *xki,

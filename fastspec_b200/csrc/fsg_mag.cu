@@ -1,5 +1,5 @@
 // fsg_mag.cu -- magnetic path: MagLineopCalc (Zeeman-split Faraday-Voigt opacity into the six
-// profiles) and MagRadTranCalc (Stokes DELO-Bezier solver, plane-parallel).  Built -fmad=false:
+// profiles) and MagRadTranCalc (Stokes DELO-Bezier solver, plane-parallel and spherical).  Built -fmad=false:
 // FP64 throughout, in the reference's operation order.
 //
 //   k_mag_center    MagLineopCalc central pass (synth.f90:1182-1275): Zeeman shifts scaled to
@@ -10,6 +10,7 @@
 //   k_mag_wide      MagLineOpacity3 for the wide lines, in line order (synth.f90:1341-1361)
 //   k_stokes        StokesPrfPP (solver.f90:265-394) + Solve4x4 (solver.f90:541-588) and the
 //                   Stokes-I flux quadrature
+//   k_stokes_sph    StokesPrfSph (solver.f90:402-538) along the rays of a spherical model
 #include "fsg_fp64.cuh"
 
 #include <algorithm>
@@ -291,6 +292,78 @@ __device__ void solve4x4(const double *A, const double *B, double *X) {
 #undef MM
 }
 
+// The DELO-Bezier sweep of StokesPrfPP / StokesPrfSph (solver.f90:341-390, 486-534) over the N points of
+// one ray, run by one thread from the per-point fields in shared memory (field-major, leading dimension
+// ld): Kv / KD the 6 distinct propagation elements and their derivatives, SRC4 / SRD the source vector
+// and its derivative, Dt the optical-depth steps.  XINT2 holds the boundary Stokes vector on entry and
+// the emergent one on return.
+__device__ void stokes_sweep(int N, int ld, const double *Kv, const double *KD, const double *SRC4,
+                             const double *SRD, const double *Dt, double *XINT2) {
+    double K1[16], K0[16], KD0[16], XKA[16], XKB[16], QA[16], QB[16], AA[16], e6[6], d6[6], XINT1[4];
+    for (int q = 0; q < 6; q++) { e6[q] = Kv[q * ld + N - 1]; d6[q] = KD[q * ld + N - 1]; }
+    build_k(e6, K0); build_k(d6, KD0);
+    for (int j = 0; j < 4; j++) for (int i = 0; i < 4; i++) {
+        double acc = 0.0;
+        for (int q = 0; q < 4; q++) acc = acc + K0[i + 4 * q] * K0[q + 4 * j];
+        XKB[i + 4 * j] = acc + KD0[i + 4 * j];
+    }
+    for (int q = 0; q < 16; q++) K1[q] = K0[q];         // XK at k1
+    for (int k = N - 2; k >= 0; k--) {
+        int k1 = k + 1;
+        double Dtau = Dt[k], Dtau05 = 0.5 * Dtau, Eps, Alpha, Beta, Gamma;
+        delo_coef(Dtau, Eps, Alpha, Beta, Gamma);
+        Gamma = Gamma * 0.5;
+        for (int q = 0; q < 6; q++) { e6[q] = Kv[q * ld + k]; d6[q] = KD[q * ld + k]; }
+        build_k(e6, K0); build_k(d6, KD0);
+        for (int q = 0; q < 16; q++) XKA[q] = XKB[q];
+        for (int j = 0; j < 4; j++) for (int i = 0; i < 4; i++) {
+            double acc = 0.0;
+            for (int q = 0; q < 4; q++) acc = acc + K0[i + 4 * q] * K0[q + 4 * j];
+            XKB[i + 4 * j] = acc + KD0[i + 4 * j];
+        }
+        for (int j = 0; j < 4; j++) for (int i = 0; i < 4; i++) {
+            int e = i + 4 * j;
+            QA[e] = Dtau05 * XKA[e] + (Dtau05 - 1.0) * K1[e];
+            QB[e] = -(Dtau05 * XKB[e]) - (Dtau05 + 1.0) * K0[e];
+            AA[e] = ((i == j) ? 1.0 : 0.0) + Alpha * K0[e] - Gamma * QB[e];
+        }
+        double GD = Gamma * Dtau05;
+        for (int i = 0; i < 4; i++) {
+            double m1 = 0.0, m2 = 0.0, m3 = 0.0, m4 = 0.0;
+            for (int q = 0; q < 4; q++) {
+                m1 = m1 + K1[i + 4 * q] * XINT2[q];
+                m2 = m2 + QA[i + 4 * q] * XINT2[q];
+                m3 = m3 + K1[i + 4 * q] * SRC4[q * ld + k1];
+                m4 = m4 + K0[i + 4 * q] * SRC4[q * ld + k];
+            }
+            XINT1[i] = Eps * XINT2[i] - Beta * m1 + Gamma * m2 + (Beta + Gamma) * SRC4[i * ld + k1]
+                     - GD * m3 + (Alpha + Gamma) * SRC4[i * ld + k] + GD * m4
+                     + GD * (SRD[i * ld + k] - SRD[i * ld + k1]);
+        }
+        solve4x4(AA, XINT1, XINT2);
+        for (int q = 0; q < 16; q++) K1[q] = K0[q];
+    }
+}
+
+// propagation matrix elements normalised by PhiI and the source vector at one point (solver.f90:296-330,
+// 431-465): m = MagLineOpac(:, ia), g = (SPhi2, CPhi2, CPhi, S2Psi, C2Psi); returns PhiI
+__device__ __forceinline__ double stokes_point(const double *m, double lop, double cop, double sr, const double *g,
+                                               double *e6, double *s4) {
+    double Php = m[0], Phb = m[1], Phr = m[2], Psp = m[3], Psb = m[4], Psr = m[5];
+    double SPhi2 = g[0], CPhi2 = g[1], CPhi = g[2], S2Psi = g[3], C2Psi = g[4];
+    double PI = 0.5 * (Php * SPhi2 + 0.5 * (Phr + Phb) * (1.0 + CPhi2)) + lop + cop;
+    double InvPhiI = 1.0 / PI;
+    double Sabs = 0.5 * (Php - 0.5 * (Phr + Phb)) * SPhi2;
+    double PhiQ = Sabs * C2Psi * InvPhiI, PhiU = Sabs * S2Psi * InvPhiI;
+    double PhiV = 0.5 * (Phr - Phb) * CPhi * InvPhiI;
+    double Sdis = 0.5 * (Psp - 0.5 * (Psr + Psb)) * SPhi2;
+    double PsiQ = Sdis * C2Psi * InvPhiI, PsiU = Sdis * S2Psi * InvPhiI;
+    double PsiV = 0.5 * (Psr - Psb) * CPhi * InvPhiI;
+    e6[0] = PhiQ; e6[1] = PhiU; e6[2] = PhiV; e6[3] = PsiQ; e6[4] = PsiU; e6[5] = PsiV;
+    s4[0] = sr; s4[1] = sr * PhiQ; s4[2] = sr * PhiU; s4[3] = sr * PhiV;
+    return PI;
+}
+
 __global__ void k_stokes(AtmView A, const double *__restrict__ lineopac, const double *__restrict__ mlo,
                          const double *__restrict__ rhox, int nmu, const double *__restrict__ xmu,
                          const double *__restrict__ wmu, const double *__restrict__ geo, double *spz, double *sfl) {
@@ -358,51 +431,8 @@ __global__ void k_stokes(AtmView A, const double *__restrict__ lineopac, const d
         }
         __syncwarp();
         if (lane == 0) {
-            double K1[16], K0[16], KD0[16], XKA[16], XKB[16], QA[16], QB[16], AA[16], e6[6], d6[6];
-            double XINT2[4] = { SRC4[N - 1], 0.0, 0.0, 0.0 }, XINT1[4];
-            for (int q = 0; q < 6; q++) { e6[q] = Kv[q * N + N - 1]; d6[q] = KD[q * N + N - 1]; }
-            build_k(e6, K0); build_k(d6, KD0);
-            for (int j = 0; j < 4; j++) for (int i = 0; i < 4; i++) {
-                double acc = 0.0;
-                for (int q = 0; q < 4; q++) acc = acc + K0[i + 4 * q] * K0[q + 4 * j];
-                XKB[i + 4 * j] = acc + KD0[i + 4 * j];
-            }
-            for (int q = 0; q < 16; q++) K1[q] = K0[q];         // XK at k1
-            for (int k = N - 2; k >= 0; k--) {
-                int k1 = k + 1;
-                double Dtau = Dt[k], Dtau05 = 0.5 * Dtau, Eps, Alpha, Beta, Gamma;
-                delo_coef(Dtau, Eps, Alpha, Beta, Gamma);
-                Gamma = Gamma * 0.5;
-                for (int q = 0; q < 6; q++) { e6[q] = Kv[q * N + k]; d6[q] = KD[q * N + k]; }
-                build_k(e6, K0); build_k(d6, KD0);
-                for (int q = 0; q < 16; q++) XKA[q] = XKB[q];
-                for (int j = 0; j < 4; j++) for (int i = 0; i < 4; i++) {
-                    double acc = 0.0;
-                    for (int q = 0; q < 4; q++) acc = acc + K0[i + 4 * q] * K0[q + 4 * j];
-                    XKB[i + 4 * j] = acc + KD0[i + 4 * j];
-                }
-                for (int j = 0; j < 4; j++) for (int i = 0; i < 4; i++) {
-                    int e = i + 4 * j;
-                    QA[e] = Dtau05 * XKA[e] + (Dtau05 - 1.0) * K1[e];
-                    QB[e] = -(Dtau05 * XKB[e]) - (Dtau05 + 1.0) * K0[e];
-                    AA[e] = ((i == j) ? 1.0 : 0.0) + Alpha * K0[e] - Gamma * QB[e];
-                }
-                double GD = Gamma * Dtau05;
-                for (int i = 0; i < 4; i++) {
-                    double m1 = 0.0, m2 = 0.0, m3 = 0.0, m4 = 0.0;
-                    for (int q = 0; q < 4; q++) {
-                        m1 = m1 + K1[i + 4 * q] * XINT2[q];
-                        m2 = m2 + QA[i + 4 * q] * XINT2[q];
-                        m3 = m3 + K1[i + 4 * q] * SRC4[q * N + k1];
-                        m4 = m4 + K0[i + 4 * q] * SRC4[q * N + k];
-                    }
-                    XINT1[i] = Eps * XINT2[i] - Beta * m1 + Gamma * m2 + (Beta + Gamma) * SRC4[i * N + k1]
-                             - GD * m3 + (Alpha + Gamma) * SRC4[i * N + k] + GD * m4
-                             + GD * (SRD[i * N + k] - SRD[i * N + k1]);
-                }
-                solve4x4(AA, XINT1, XINT2);
-                for (int q = 0; q < 16; q++) K1[q] = K0[q];
-            }
+            double XINT2[4] = { SRC4[N - 1], 0.0, 0.0, 0.0 };
+            stokes_sweep(N, N, Kv, KD, SRC4, SRD, Dt, XINT2);
             for (int q = 0; q < 4; q++) spz[((size_t)iwl * 4 + q) * nmu + im] = XINT2[q];
             Iout[im] = XINT2[0];
         }
@@ -413,6 +443,79 @@ __global__ void k_stokes(AtmView A, const double *__restrict__ lineopac, const d
         for (int q = 0; q < nmu; q++) a = a + Iout[q] * wmu[q];
         sfl[iwl] = a;
     }
+}
+
+// StokesPrfSph (solver.f90:402-538).  CTA = one wavelength x a group of rays (grid.y), warp = one ray.
+// Lanes gather the six profiles, line and continuum opacity and source of the layer each ray point
+// samples, with the field projection of that point (geo [5][nmu][stride]); TauStep runs on the ray's
+// column mass (mu = 1); lane 0 sweeps from zero incoming light for grazing rays, Src(N) otherwise.
+__global__ void k_stokes_sph(AtmView A, const double *__restrict__ lineopac, const double *__restrict__ mlo,
+                             RayView R, const double *__restrict__ geo, int rays_per_cta, double *spz) {
+    extern __shared__ double sm[];
+    const int iwl = blockIdx.x, nt = A.ntau, M = R.stride, nmu = R.nmu;
+    const int wi = threadIdx.x >> 5, lane = threadIdx.x & 31, im = blockIdx.y * rays_per_cta + wi;
+    double *Src = sm;                                              // Planck source by layer [nt]
+    double *S = sm + nt + (size_t)wi * STK_FIELDS * M;            // this ray's fields, leading dim M
+    double *PhiI = S, *Kv = S + M, *KD = S + 7 * M, *SRC4 = S + 13 * M, *SRD = S + 17 * M, *Dt = S + 21 * M;
+    const double PlkC1 = FSG_HC * FSG_VC * 1e13 / FSG_KBOLT;
+    const double wl = A.wave[iwl] + A.wfirst;
+    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+        double C1 = PlkC1 / wl, C2 = exp(50.7649141 - 5.0 * log(wl));
+        Src[t] = C2 / (exp(C1 / A.xi[XI_T * nt + t]) - 1.0);
+    }
+    __syncthreads();
+    if (im >= nmu) return;
+    const int N = R.n[im];
+    const int *mp = R.map + (size_t)im * M;
+    const double *m = R.m + (size_t)im * M;
+    const size_t gs = (size_t)nmu * M, go = (size_t)im * M;
+    for (int t = lane; t < N; t += 32) {
+        const int ia = mp[t];
+        const size_t o = (size_t)iwl * nt + ia;
+        double g[5] = { geo[go + t], geo[gs + go + t], geo[2 * gs + go + t], geo[3 * gs + go + t], geo[4 * gs + go + t] };
+        double e6[6], s4[4];
+        PhiI[t] = stokes_point(mlo + o * 6, lineopac[o], A.contopac[o], Src[ia], g, e6, s4);
+        for (int q = 0; q < 6; q++) Kv[q * M + t] = e6[q];
+        for (int q = 0; q < 4; q++) SRC4[q * M + t] = s4[q];
+    }
+    __syncwarp();
+    // TauStep (solver.f90:591-615) on the ray's column mass
+    for (int t = lane; t < N - 1; t += 32) {
+        if (t == 0) {
+            double Dx1 = m[1] - m[0], Yp = (PhiI[1] - PhiI[0]) / Dx1;
+            Dt[0] = Dx1 * (PhiI[1] + 2.0 * PhiI[0] + Dx1 / 2.0 * Yp) / 3.0;
+        } else {
+            double Dx = m[t] - m[t - 1], Dx1 = m[t + 1] - m[t];
+            double Der = (PhiI[t] - PhiI[t - 1]) / Dx, Der1 = (PhiI[t + 1] - PhiI[t]) / Dx1, Yp;
+            if (Der * Der1 > 0.0) {
+                double Lambda = (1.0 + Dx1 / (Dx + Dx1)) / 3.0;
+                Yp = (Der / (Lambda * Der1 + (1.0 - Lambda) * Der)) * Der1;
+            } else Yp = 0.0;
+            Dt[t] = Dx1 * (PhiI[t + 1] + 2.0 * PhiI[t] + Dx1 / 2.0 * Yp) / 3.0;
+        }
+    }
+    __syncwarp();
+    for (int e = lane; e < 10 * N; e += 32) {
+        int row = e / N, t = e - row * N;
+        if (row < 4) centder_pt(Dt, SRC4 + row * M, 1, N, t, &SRD[row * M + t]);
+        else centder_pt(Dt, Kv + (row - 4) * M, 1, N, t, &KD[(row - 4) * M + t]);
+    }
+    __syncwarp();
+    if (lane == 0) {
+        double XINT2[4] = { R.graz[im] ? 0.0 : SRC4[N - 1], 0.0, 0.0, 0.0 };
+        stokes_sweep(N, M, Kv, KD, SRC4, SRD, Dt, XINT2);
+        for (int q = 0; q < 4; q++) spz[((size_t)iwl * 4 + q) * nmu + im] = XINT2[q];
+    }
+}
+
+// Stokes-I flux of the spherical path: Sf = sum over mu of SpZ(mu, 1) Wmu (convol.f90:233-234)
+__global__ void k_stokes_flux(int nwl, int nmu, const double *__restrict__ spz, const double *__restrict__ wmu,
+                              double *sfl) {
+    int iwl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (iwl >= nwl) return;
+    double a = 0.0;
+    for (int q = 0; q < nmu; q++) a = a + spz[(size_t)iwl * 4 * nmu + q] * wmu[q];
+    sfl[iwl] = a;
 }
 
 // ================================================================================================
@@ -429,6 +532,20 @@ int fsg_launch_stokes(cudaStream_t s, const AtmView &A, const double *lineopac, 
     if (sm > 220 * 1024) return FSG_E_ARG;
     cudaFuncSetAttribute(k_stokes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     k_stokes<<<A.nwl, 32 * nmu, sm, s>>>(A, lineopac, mlo, rhox, nmu, xmu, wmu, geo, spz, sfl);
+    return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
+}
+
+int fsg_launch_stokes_sph(cudaStream_t s, const AtmView &A, const double *lineopac, const double *mlo,
+                          const RayView &R, const double *wmu, const double *geo, double *spz, double *sfl) {
+    const size_t per_ray = sizeof(double) * STK_FIELDS * (size_t)R.stride, base = sizeof(double) * A.ntau;
+    const size_t cap = 200 * 1024;
+    if (base + per_ray > cap) return FSG_E_ARG;
+    int g = (int)std::min<size_t>((size_t)R.nmu, (cap - base) / per_ray);
+    size_t sm = base + per_ray * g;
+    cudaFuncSetAttribute(k_stokes_sph, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    dim3 grid(A.nwl, (R.nmu + g - 1) / g);
+    k_stokes_sph<<<grid, 32 * g, sm, s>>>(A, lineopac, mlo, R, geo, g, spz);
+    if (sfl) k_stokes_flux<<<(A.nwl + 127) / 128, 128, 0, s>>>(A.nwl, R.nmu, spz, wmu, sfl);
     return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
 }
 

@@ -110,6 +110,15 @@ int fsg_set_atmosphere(fsg_ctx *ctx, int ntau, const double *rhox, const double 
                        const float *fractionpf, const float *xamass, const float *potion,
                        const int32_t *ion, const float *frac_h1, const float *frac_he1,
                        const float *frac_h2);
+/* Model geometry (ReadModel, ioutils.f90:1630-1700; SphereInit, solver.f90:45-120): radius [cm] > 0
+ * makes the model spherical with layer heights height [ntau] [cm] above the radius (decreasing inward,
+ * radius + height > 0, 1e9 <= radius <= 1e15, as ReadModel checks); radius <= 0 returns to plane-parallel
+ * (height may then be NULL).  fsg_set_atmosphere resets the model to plane-parallel, as reading a new
+ * model does, so call this after it.  The rays (one per angle of fsg_set_mu) are built on the host at
+ * the next RadTranCalc / LinStrCalc / MagRadTranCalc call, which then solve along them (LocPrfSph,
+ * StokesPrfSph; errors: an angle mu <= 0, a ray tangent in the top layer).  The adjoint and the batched
+ * path take plane-parallel models only.  Replaces Radius/Atmos%Height (shared.f90:520-527). */
+int fsg_set_geometry(fsg_ctx *ctx, double radius, const double *height);
 /* Continuum opacity ContOpac [nwl][ntau] (ContopCalc output, synth.f90:642-674), ContOpacStd
  * [ntau] (may be NULL when motype == 0) and the model type (Motype). */
 int fsg_set_contopac(fsg_ctx *ctx, const double *contopac, const double *contopac_std, int motype);
@@ -149,7 +158,8 @@ const double *fsg_lineop_device_ptr(fsg_ctx *ctx);
 
 /* Limb angles and flux weights used by RadTranCalc, LinStrCalc and the disk integration. */
 int fsg_set_mu(fsg_ctx *ctx, int nmu, const double *xmu, const double *wmu);
-/* RadTranCalc (synth.f90:1825-1901) + DiskInteg without broadening (convol.f90:111-235):
+/* RadTranCalc (synth.f90:1825-1901; plane-parallel or spherical, fsg_set_geometry) + DiskInteg without
+ * broadening (convol.f90:111-235):
  * spl/spc [nwl][nmu], sfl/sfc [nwl]; any output may be NULL.  Uses the device LineOpac. */
 int fsg_radtran(fsg_ctx *ctx, double *spl, double *spc, double *sfl, double *sfc);
 int fsg_radtran_dev(fsg_ctx *ctx, double *d_spl, double *d_spc, double *d_sfl, double *d_sfc);
@@ -172,7 +182,7 @@ int fsg_mag_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, int bframe, const 
                         int nbfield, double *maglineopac, int32_t *flags, int32_t *ileft,
                         int32_t *iright, float *linstr, fsg_stats *stats);
 int fsg_mag_lineop_reset(fsg_ctx *ctx);
-/* MagRadTranCalc plane-parallel (synth.f90:1904-2012): spz [nwl][4][nmu], spc [nwl][nmu],
+/* MagRadTranCalc (synth.f90:1904-2111; plane-parallel or spherical): spz [nwl][4][nmu], spc [nwl][nmu],
  * and the Stokes-I flux sfl / continuum flux sfc [nwl] (may be NULL). */
 int fsg_mag_radtran(fsg_ctx *ctx, int bframe, const double *bfield, int nbfield, double *spz,
                     double *spc, double *sfl, double *sfc);
