@@ -621,8 +621,53 @@ def make_sphere_pins(gold):
     print("sphere polarised: region pixels", i1 - i0 + 1, "grazing rays", int(g["graz"].sum()))
 
 
+def make_h5_pin(gold):
+    """HDF5 fixture (pin_solar_h5.npz): the pin_solar list written by fsio.write_hdf5_lines (the
+    reference's columnar /Lines layout) and read by the reference program as an atomic HDF5 list
+    (ReadHDF, ioutils.f90:524-1159) after the probe list; the region's line opacity, continuum and
+    spectra.  Pins the writer (the reference's HDF5 library accepts the file) and the atomic-list path
+    (LineTypeAtm records, wide lines) of the oracle and the GPU."""
+    name, atmname, mk, grid, region = pin_specs()[0]
+    teff, logg, ntau, species, ismol, _, _, vmic, molbrd, _, _ = CONFIGS[atmname]
+    model = W.eddington_model(teff, logg, ntau)
+    state = load_state(atmname)
+    extra = mk()
+    pgf = np.load(os.path.join(HERE, "atm_%s.npz" % atmname))["probe_loggf"]
+    probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
+    t = extra._txt
+    with tempfile.TemporaryDirectory() as wd:
+        W.write_krz(os.path.join(wd, "model.krz"), model)
+        probes.write_z(os.path.join(wd, "probes.z"), grid[0], grid[1])
+        fsio.write_hdf5_lines(os.path.join(wd, "lines.h5"), extra.species, extra.spc, extra.wl,
+                              W.f32_of_text(t["elo"], "%.4f"), W.f32_of_text(t["loggf"], "%.3f"),
+                              W.f32_of_text(t["lgrad"], "%.3f"), W.f32_of_text(t["lgqst"], "%.3f"),
+                              W.f32_of_text(t["lgvdw"], "%.3f"), provenance="pin_solar seeded list")
+        deck = ("wave=%.4f, %.4f, %.6f, %d\nsave=0, 1, 1, 1, 1\nvmic=%.3f\nmolbrd=%d\n"
+                "lines=\n-1  probes.z\n-1  lines.h5\n\nmodel=model.krz\nmus=7\n" % (grid + (vmic, molbrd)))
+        log = run_ref(wd, deck)
+        assert "File: lines.h5" in log and "Lines read: %d" % extra.n in log, log
+        lo = fsio.read_opac(os.path.join(wd, "fs_lineop.bin"))
+        co = fsio.read_opac(os.path.join(wd, "fs_contop.bin"))
+        sp = fsio.read_spec(os.path.join(wd, "fs_spec.bin"))
+        fl = fsio.read_flux(os.path.join(wd, "fs_flux.bin"))
+    for k in ("rhox", "T", "xne", "xna", "rho"):
+        assert np.array_equal(lo[k], state[k]), "EOS state differs from the recovered one: " + k
+    wave = lo["wave"]
+    sel = (wave >= region[0] - 1e-9) & (wave <= region[1] + 1e-9)
+    i0, i1 = (int(x) for x in np.nonzero(sel)[0][[0, -1]])
+    np.savez_compressed(
+        os.path.join(gold, "pin_solar_h5.npz"), grid=np.array(grid, np.float64), i0=i0, i1=i1, atm=atmname,
+        vmicro=vmic, molbrd=molbrd, contopac=co["opac"][i0:i1 + 1], lineopac=lo["opac"][i0:i1 + 1],
+        wave=wave[i0:i1 + 1], xmu=sp["xmu"], spl=sp["spl"][i0:i1 + 1], spc=sp["spc"][i0:i1 + 1],
+        sfl=fl["sfl"][i0:i1 + 1], sfc=fl["sfc"][i0:i1 + 1],
+        **{"txt_" + k: np.asarray(v) for k, v in t.items()}, line_wl=extra.wl, line_spc=extra.spc)
+    print("pin_solar_h5: region pixels", i1 - i0 + 1, "lines", extra.n)
+
+
 if __name__ == "__main__":
-    if len(sys.argv) > 1 and sys.argv[1] == "sphere":
+    if len(sys.argv) > 1 and sys.argv[1] == "h5":
+        make_h5_pin(os.path.join(REPO, "tests", "golden"))
+    elif len(sys.argv) > 1 and sys.argv[1] == "sphere":
         make_sphere_pins(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "magpin":
         make_mag_pin(os.path.join(REPO, "tests", "golden"))

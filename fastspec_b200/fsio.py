@@ -112,3 +112,86 @@ def write_linst(path, species, ion, wave, strength, append=False):
         np.asarray(ion, "<i4").tofile(f)
         np.asarray(wave, "<f8").tofile(f)
         np.asarray(strength, "<f4").tofile(f)
+
+
+# ---- line lists in the reference's HDF5 layout (group /Lines, one dataset per column) ----------
+
+MAXION = 5      # highest ionisation stage the reference's EOS supports (lines above it are dropped)
+
+
+def read_hdf5_lines(path, species, exact=True):
+    """A FastSpec HDF5 line list as the library's SoA records, converted as ReadHDF converts them
+    (ioutils.f90:889-1000 atomic / Zeeman, 790-812 molecular): gf = 10.0**LGGF; atomic Grad =
+    10.0**GRAD for 0 < GRAD < 20, Gqst / Gvdw = 10.0**x for x < 0 (a positive GVDW is the packed ABO
+    parameter), all in single precision (libm powf when exact, numpy's power otherwise); atomic lines
+    above ionisation stage 5 are dropped.  Molecular single-species lists take GRAD as stored and no
+    Stark / van der Waals parameters.
+
+    species: the caller's species table, a list of (name, ion) in the order of the FractionPF columns
+    of its atmosphere state; each line's index into it (spc) is -1 for a species the table lacks.
+    Returns dict(wl, elo, gf, grad, gqst, gvdw, spc, ismol, kind, attrs[, jlo, jup, glo, gup]) with
+    kind 0 (atomic list) or 1 (molecular list), the fsg_lines kinds."""
+    from . import hdf5
+    from .workloads import pow10f
+    cols, attrs, _ = hdf5.read_lines(path)
+    p10 = pow10f if exact else (lambda v: np.power(np.float32(10.0), np.asarray(v, np.float32)).astype(np.float32))
+    f32 = lambda a: np.asarray(a, np.float32)
+    table = {(str(n), int(i)): k for k, (n, i) in enumerate(species)}
+    if "EL" not in cols:                                 # single-species molecular list
+        n = len(cols["W"])
+        k = table.get((str(attrs.get("NAME", "")).strip(), int(attrs.get("ION", 1))), -1)
+        z = np.zeros(n, np.float32)
+        return dict(wl=np.asarray(cols["W"], np.float64), elo=f32(cols["E"]), gf=p10(f32(cols["LGGF"])),
+                    grad=f32(cols["GRAD"]), gqst=z, gvdw=z.copy(), spc=np.full(n, k, np.int32),
+                    ismol=np.ones(n, np.int32), kind=1, attrs=attrs)
+    keep = np.asarray(cols["ION"]) <= MAXION
+    el = np.asarray(cols["EL"])[keep]
+    ion = np.asarray(cols["ION"], np.int32)[keep]
+    lg, lq, lv = f32(cols["GRAD"])[keep], f32(cols["GQST"])[keep], f32(cols["GVDW"])[keep]
+    out = dict(wl=np.asarray(cols["W"], np.float64)[keep], elo=f32(cols["E"])[keep],
+               gf=p10(f32(cols["LGGF"])[keep]),
+               grad=np.where((lg < 20.0) & (lg > 0.0), p10(lg), lg).astype(np.float32),
+               gqst=np.where(lq < 0.0, p10(lq), lq).astype(np.float32),
+               gvdw=np.where(lv < 0.0, p10(lv), lv).astype(np.float32),
+               spc=np.array([table.get((str(e).strip(), int(i)), -1) for e, i in zip(el, ion)], np.int32),
+               ismol=np.zeros(int(keep.sum()), np.int32), kind=0, attrs=attrs)
+    for c in ("JLO", "JUP", "GLO", "GUP"):
+        if c in cols:
+            out[c.lower()] = f32(cols[c])[keep]
+    return out
+
+
+def write_hdf5_lines(path, species, spc, wl, elo, loggf, lgrad, lgqst, lgvdw, wl_vac=0, provenance="",
+                     zeeman=None):
+    """Write an atomic line list in the reference's HDF5 layout (the columns and group attributes of
+    vald2hdf.py: EL, ION, W, E, LGGF, GRAD, GQST, GVDW, plus JLO, JUP, GLO, GUP when zeeman =
+    (jlo, jup, glo, gup) is given), contiguous and unfiltered; the damping columns hold the logarithms
+    (or the packed ABO parameter) as VALD gives them.  Lines must be sorted by wavelength."""
+    import datetime
+    from . import hdf5
+    wl = np.asarray(wl, np.float64)
+    if len(wl) > 1 and np.any(np.diff(wl) < 0):
+        raise ValueError("write_hdf5_lines: lines must be sorted by wavelength")
+    spc = np.asarray(spc)
+    width = max(len(n) for n, _ in species) + 1
+    cols = dict(EL=np.array([species[k][0] for k in spc], "S%d" % width),
+                ION=np.array([species[k][1] for k in spc], np.int16), W=wl,
+                E=np.asarray(elo, np.float32), LGGF=np.asarray(loggf, np.float32),
+                GRAD=np.asarray(lgrad, np.float32), GQST=np.asarray(lgqst, np.float32),
+                GVDW=np.asarray(lgvdw, np.float32))
+    units = dict(EL="element symbol", ION="ionization stage (1 = neutral)",
+                 W="Angstrom (air or vacuum per the WL_VAC attribute)", E="eV (lower-level excitation energy)",
+                 LGGF="log10(gf) (dimensionless)", GRAD="log10(radiative damping /s) (VALD Rad.)",
+                 GQST="log10(Stark damping /s per electron at 1e4 K) (VALD Stark)",
+                 GVDW="VALD Waals: packed ABO sigma.alpha if >0, else log10(vdW damping /s per H atom at 1e4 K)")
+    if zeeman is not None:
+        for c, a in zip(("JLO", "JUP", "GLO", "GUP"), zeeman):
+            cols[c] = np.asarray(a, np.float32)
+            units[c] = "dimensionless"
+    n = len(wl)
+    attrs = dict(NL=np.int32(n), NAME="atom Zeeman" if zeeman is not None else "atom", WL_VAC=np.int16(wl_vac),
+                 HFLAG=np.int16(0), FILE=str(path).rsplit("/", 1)[-1].rsplit(".", 1)[0],
+                 DATE=datetime.date.today().isoformat(), PROVENANCE=provenance,
+                 FORMAT_VERSION="z-1.0" if zeeman is not None else "a-1.0",
+                 WMIN=np.float64(wl[0] if n else 0.0), WMAX=np.float64(wl[-1] if n else 0.0))
+    hdf5.write_lines(path, cols, attrs, units)

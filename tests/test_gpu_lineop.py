@@ -401,3 +401,26 @@ def test_he_stark_shifted_lines(fsg, oracle_mod, prec):
     assert np.array_equal(g["ileft"], r["ileft"]) and np.array_equal(g["iright"], r["iright"])
     tol = 2e-6 if prec == "mixed" else 1e-11
     assert np.max(np.abs(g["lineopac"] - r["lineopac"]) / (r["lineopac"] + co)) < tol
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_hdf5_list_against_reference_pin(fsg, tmp_path, prec):
+    """A line list in the reference's HDF5 layout, read by fsio.read_hdf5_lines as an atomic list
+    (kind 0), through the GPU path: the reference program's line opacity and flux for the same file
+    (tests/golden/pin_solar_h5.npz); windows identical, FP64 1e-8, mixed within the mixed bars."""
+    from test_hdf5 import hdf5_pin_lines
+    d, r = hdf5_pin_lines(tmp_path)
+    grid, st, meta, co = H.pin_setup(d)
+    C = ctx_for(fsg, grid, st, co, fsg.PREC_MIXED if prec == "mixed" else fsg.PREC_FP64,
+                vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]))
+    a = {k: r[k] for k in ("wl", "elo", "gf", "grad", "gqst", "gvdw", "spc", "ismol")}
+    g = C.lineop_calc(fsg.LineList.from_arrays(a, kind=r["kind"]))
+    i0, i1 = int(d["i0"]), int(d["i1"])
+    lo, ref = g["lineopac"][i0:i1 + 1], d["lineopac"]
+    assert np.array_equal(lo > 0, ref > 0)
+    if prec == "fp64":
+        assert np.max(np.abs(lo[ref > 0] / ref[ref > 0] - 1)) < 1e-8
+    else:
+        assert np.max(np.abs(lo - ref) / (ref + d["contopac"])) < 2e-6
+    spl, spc, sfl, sfc = C.radtran()
+    assert np.max(np.abs(sfl[i0:i1 + 1] / d["sfl"] - 1)) < (1e-8 if prec == "fp64" else 1e-5)

@@ -1,0 +1,128 @@
+"""Line lists in the reference's HDF5 layout (fastspec_b200/hdf5.py, fsio.read_hdf5_lines /
+write_hdf5_lines), on the CPU.
+
+* The reader against the reference's own example lists (examples/lines/*.h5, written by its h5py
+  converters: chunked, shuffled, gzip-compressed columns): the first 300 records equal the values
+  parsed from the text sources the reference converted (tests/golden/hdf5_examples.npz, made by
+  tests/golden/make_hdf5_golden.py).  Skipped where the reference tree is absent.
+* The writer: round trip, and the pin of the reference program reading a written file
+  (tests/golden/pin_solar_h5.npz, fastspec_b200/data/make_atmospheres.py h5): the oracle's atomic-list
+  path on the list read back gives the reference's line opacity and spectra.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import helpers as H
+
+EXAMPLES = "/root/reference/examples/lines"
+
+
+def _golden():
+    return np.load(os.path.join(H.GOLD, "hdf5_examples.npz"))
+
+
+@pytest.mark.skipif(not os.path.isdir(EXAMPLES), reason="reference example line lists not present")
+@pytest.mark.parametrize("name", ["VALD_all_500-600.h5", "VALD_all_500-600.zh5"])
+def test_reader_atomic_lists_match_text_source(name):
+    from fastspec_b200 import hdf5
+    g = _golden()
+    cols, attrs, units = hdf5.read_lines(os.path.join(EXAMPLES, name))
+    n = len(g["vald_w"])
+    assert attrs["NL"] == len(cols["W"]) == 136370 and attrs["NAME"].startswith("atom")
+    assert attrs["WMIN"] == cols["W"][0] and attrs["WMAX"] == cols["W"][-1]
+    assert np.all(np.diff(cols["W"]) >= 0)
+    assert np.array_equal(cols["EL"][:n], g["vald_el"]) and np.array_equal(cols["ION"][:n], g["vald_ion"])
+    assert np.array_equal(cols["W"][:n], g["vald_w"])
+    for k in ("LGGF", "E", "GRAD", "GQST", "GVDW"):
+        assert np.array_equal(cols[k][:n], g["vald_" + k.lower()]), k
+    if name.endswith(".zh5"):
+        assert np.array_equal(cols["JLO"][:n], g["vald_jlo"]) and np.array_equal(cols["JUP"][:n], g["vald_jup"])
+        for k in ("GLO", "GUP"):          # the converter fills unknown factors and flags forbidden lines
+            t, h = g["vald_" + k.lower()], cols[k][:n]
+            known = (t != 99.0) & (h != 99.0)
+            assert known.sum() > 250 and np.array_equal(t[known], h[known])
+    assert units["W"].startswith("Angstrom")
+
+
+@pytest.mark.skipif(not os.path.isdir(EXAMPLES), reason="reference example line lists not present")
+def test_reader_molecular_list_matches_text_source():
+    from fastspec_b200 import hdf5, fsio
+    g = _golden()
+    cols, attrs, units = hdf5.read_lines(os.path.join(EXAMPLES, "56Fe1H_Exomol_Irw.h5"))
+    n = len(g["feh_w"])
+    assert attrs["NAME"] == "FeH" and attrs["ION"] == 1 and attrs["WL_VAC"] == 1
+    assert np.max(np.abs(cols["W"][:n] - g["feh_w"])) < 1e-9
+    for k in ("E", "LGGF", "GU", "GRAD"):
+        assert np.array_equal(cols[k][:n], g["feh_" + k.lower()]), k
+    r = fsio.read_hdf5_lines(os.path.join(EXAMPLES, "56Fe1H_Exomol_Irw.h5"), [("FeH", 1)], exact=False)
+    assert r["kind"] == 1 and np.all(r["spc"] == 0) and np.all(r["ismol"] == 1)
+    assert np.array_equal(r["grad"], cols["GRAD"])               # molecular GRAD is taken as stored
+    assert np.allclose(r["gf"], 10.0 ** cols["LGGF"].astype(np.float64), rtol=1e-6)
+
+
+def test_writer_round_trip(tmp_path):
+    from fastspec_b200 import fsio, hdf5, workloads as W
+    L = W.zeeman_lines(50, 6000.0, 6005.0, W.SEED0 + 7)
+    t = L._txt
+    p = str(tmp_path / "z.zh5")
+    f = lambda k, fmt: W.f32_of_text(t[k], fmt)
+    fsio.write_hdf5_lines(p, L.species, L.spc, L.wl, f("elo", "%.4f"), f("loggf", "%.3f"), f("lgrad", "%.3f"),
+                          f("lgqst", "%.3f"), f("lgvdw", "%.3f"), zeeman=L.zeeman, provenance="round trip")
+    cols, attrs, units = hdf5.read_lines(p)
+    assert attrs["NL"] == L.n and attrs["NAME"] == "atom Zeeman" and attrs["FORMAT_VERSION"] == "z-1.0"
+    assert attrs["PROVENANCE"] == "round trip" and attrs["WMIN"] == L.wl[0] and attrs["WMAX"] == L.wl[-1]
+    assert np.array_equal(cols["W"], L.wl)
+    r = fsio.read_hdf5_lines(p, L.species)
+    for k in ("wl", "elo", "gf", "grad", "gqst", "gvdw", "spc"):
+        assert np.array_equal(r[k], getattr(L, k)), k
+    for q, k in enumerate(("jlo", "jup", "glo", "gup")):
+        assert np.array_equal(r[k], np.asarray(L.zeeman[q], np.float32)), k
+    # a species missing from the caller's table is marked -1; an empty list round-trips
+    r2 = fsio.read_hdf5_lines(p, L.species[:1])
+    assert np.all((r2["spc"] == 0) | (r2["spc"] == -1)) and np.any(r2["spc"] == -1)
+    e = str(tmp_path / "e.h5")
+    fsio.write_hdf5_lines(e, L.species, [], [], [], [], [], [], [])
+    ce, ae, _ = hdf5.read_lines(e)
+    assert ae["NL"] == 0 and len(ce["W"]) == 0
+    with pytest.raises(hdf5.HDF5Error):
+        bad = tmp_path / "bad.h5"
+        bad.write_bytes(b"not an hdf5 file at all")
+        hdf5.read_lines(str(bad))
+    with pytest.raises(ValueError):
+        fsio.write_hdf5_lines(e, L.species, L.spc[::-1], L.wl[::-1], *(np.zeros(L.n),) * 5)
+
+
+def hdf5_pin_lines(tmp_path):
+    """The pin_solar_h5 list written to an HDF5 file and read back as SoA records (atomic list)."""
+    from fastspec_b200 import fsio, workloads as W
+    d = H.load_pin("pin_solar_h5")
+    st, meta = H.load_atm("solar")
+    species = [(s.split()[0], int(s.split()[1])) for s in meta["species"]]
+    p = str(tmp_path / "lines.h5")
+    f = lambda k, fmt: W.f32_of_text(d["txt_" + k], fmt)
+    fsio.write_hdf5_lines(p, species, d["line_spc"], d["line_wl"], f("elo", "%.4f"), f("loggf", "%.3f"),
+                          f("lgrad", "%.3f"), f("lgqst", "%.3f"), f("lgvdw", "%.3f"))
+    return d, fsio.read_hdf5_lines(p, species)
+
+
+def test_oracle_hdf5_list_against_reference_pin(oracle_mod, tmp_path):
+    """The reference read the same written file as an atomic HDF5 list (LineTypeAtm records, wide lines
+    taken out of blocking): the oracle's atomic-list path on the records read back reproduces its line
+    opacity (windows identical) and spectra."""
+    d, r = hdf5_pin_lines(tmp_path)
+    grid, st, meta, co = H.pin_setup(d)
+    S = oracle_mod.State(grid, st, contopac=co, vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]))
+    L = oracle_mod.Lines(**{k: r[k] for k in ("wl", "elo", "gf", "grad", "gqst", "gvdw", "spc", "ismol")}, kind=0)
+    o = oracle_mod.lineop_calc(S, L, list_type=0)
+    i0, i1 = int(d["i0"]), int(d["i1"])
+    lo, ref = o["lineopac"][i0:i1 + 1], d["lineopac"]
+    assert np.array_equal(lo > 0, ref > 0)
+    assert np.max(np.abs(lo[ref > 0] / ref[ref > 0] - 1)) < 1e-8
+    assert o["stats"]["nwide"] > 0                              # the atomic path's wide lines were exercised
+    spl, spc = oracle_mod.radtran(S, d["xmu"], o["lineopac"])
+    assert np.max(np.abs(spl[i0:i1 + 1] / d["spl"] - 1)) < 1e-8
+    x, w, _ = oracle_mod.mu_quadrature(1, len(d["xmu"]))
+    sfl, _ = oracle_mod.disk_integ(w, spl[i0:i1 + 1], spc[i0:i1 + 1])
+    assert np.max(np.abs(sfl / d["sfl"] - 1)) < 1e-8
