@@ -157,9 +157,9 @@ void fsg_launch_xline_init(cudaStream_t s, int nt, const double *T, const double
 }
 
 // ================================================================================================
-// Central pass (synth.f90:833-907).  One thread per line, three sweeps over depth that recompute
-// XlineDepth instead of holding Ntau-long arrays: (1) LinCop bound test against the continuum,
-// (2) single-line opacity at the line centre (LineOpacity2), (3) AnalyticWindow.
+// Central pass (synth.f90:833-907).  One thread per line and one sweep over depth: XlineDepth once per
+// depth feeds the LinCop bound test against the continuum, the single-line opacity at the line centre
+// (LineOpacity2) and AnalyticWindow; no Ntau-long arrays are held.
 // ================================================================================================
 __device__ __forceinline__ double center_shift(const AtmView &A, int ihe, int t) {
     return (ihe > 0) ? A.heshf[(ihe - 1) * A.ntau + t] : 0.0;
@@ -179,48 +179,38 @@ __global__ void k_center(AtmView A, LineView L, const float *__restrict__ vtab,
     int ihe = XC.IxHe;
     int iwl = waveidx(A, wlc);
     double dW = (wlc - A.wave[iwl - 1]) / (A.wave[iwl] - A.wave[iwl - 1]);
-    // (1) upper bound: H(a, v) <= 1 (synth.f90:876-887)
-    double mx = -1.0e308;
+    // One sweep over depth gives the three maxima the reference takes in turn (synth.f90:876-907):
+    // (1) the upper bound LinCop / ContOpac (H(a, v) <= 1), (2) the single-line opacity at the line
+    // centre (LineOpacity2 at Wl = Wlcent) and (3) the AnalyticWindow half-width (opacity.f90:678-710).
+    // Each is a maximum over depths of per-depth values that do not depend on the others, so computing
+    // XlineDepth once per depth for all three gives the reference's tests and windows exactly; the
+    // later maxima are used only when the earlier tests keep the line.
+    const double iSqrtPi = 0.5641895835477563;
+    double mx1 = -1.0e308, mx2 = -1.0e308, dWwin = 0.0;
     for (int t = 0; t < nt; t++) {
-        double dopl;
-        double cop = xline_cop(A, t, XC, &dopl);
-        double co = cont_center(A, iwl, dW, t);
-        double r = (A.motype == 1) ? cop / (co * A.contstd[t]) : cop / co;
-        mx = fmax(mx, r);
+        double cop, vv, av;
+        xline_depth(A, t, XC, &cop, &vv, &av);
+        const double co = cont_center(A, iwl, dW, t);
+        mx1 = fmax(mx1, (A.motype == 1) ? cop / (co * A.contstd[t]) : cop / co);
+        double dWl = 0.0;
+        if (ihe > 0) dWl = 0.0 - center_shift(A, ihe, t);
+        double lo = hvoigt64(vtab, anode, aida, av, dWl * vv) * cop;
+        if (A.motype == 1) lo = lo / A.contstd[t];
+        mx2 = fmax(mx2, lo / co);
+        double r = cop / (A.epsopac * co);
+        if (A.motype == 1) r = r / A.contstd[t];
+        if (r <= 1.0) continue;
+        double w = sqrt(log(r) + fmax(0.0, av * (r * iSqrtPi - av))) / vv;
+        if (ihe > 0) w = w + fabs(center_shift(A, ihe, t));
+        dWwin = fmax(dWwin, w);
     }
     int il = 1, ir = A.nwl;
-    if (mx < A.epsopac) { f |= FSG_F_WEAK; }
-    else {
-        // (2) centre opacity (synth.f90:890-898; LineOpacity2 at Wl = Wlcent)
-        mx = -1.0e308;
-        for (int t = 0; t < nt; t++) {
-            double cop, vv, av;
-            xline_depth(A, t, XC, &cop, &vv, &av);
-            double dWl = 0.0;
-            if (ihe > 0) dWl = 0.0 - center_shift(A, ihe, t);
-            double lo = hvoigt64(vtab, anode, aida, av, dWl * vv) * cop;
-            if (A.motype == 1) lo = lo / A.contstd[t];
-            mx = fmax(mx, lo / cont_center(A, iwl, dW, t));
-        }
-        if (mx < A.epsopac) { f |= FSG_F_WEAK; }
-        else {
-            // (3) AnalyticWindow (opacity.f90:678-710) + WaveIdx (synth.f90:904-906)
-            const double iSqrtPi = 0.5641895835477563;
-            double dWwin = 0.0;
-            for (int t = 0; t < nt; t++) {
-                double cop, vv, av;
-                xline_depth(A, t, XC, &cop, &vv, &av);
-                double r = cop / (A.epsopac * cont_center(A, iwl, dW, t));
-                if (A.motype == 1) r = r / A.contstd[t];
-                if (r <= 1.0) continue;
-                double w = sqrt(log(r) + fmax(0.0, av * (r * iSqrtPi - av))) / vv;
-                if (ihe > 0) w = w + fabs(center_shift(A, ihe, t));
-                dWwin = fmax(dWwin, w);
-            }
-            il = waveidx(A, wlc - dWwin);
-            ir = waveidx(A, wlc + dWwin) + 1;
-            if (ir > A.nwl) ir = A.nwl;
-        }
+    if (mx1 < A.epsopac || mx2 < A.epsopac) {
+        f |= FSG_F_WEAK;
+    } else {
+        il = waveidx(A, wlc - dWwin);                      // WaveIdx (synth.f90:904-906)
+        ir = waveidx(A, wlc + dWwin) + 1;
+        if (ir > A.nwl) ir = A.nwl;
     }
     flags[i] = f; ileft[i] = il; iright[i] = ir;
     // warp-aggregated count of retained lines
