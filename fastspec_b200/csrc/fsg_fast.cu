@@ -78,7 +78,8 @@ __device__ __forceinline__ float sqrt_approx(float x) {
 // depth, so there HVoigt * LinCop is the rational wing form alone:
 //   val = c1 (t + 1) / (t^2 + twoA),  t = dl^2 vv2 + c2m1
 // (three FMAs, one reciprocal, one FMA into the partial sum).  Lines whose window covers the
-// whole tile outside their core range (the common case for wide windows) skip the mask.
+// whole tile outside their core range (the common case for wide windows) skip the mask; for the others
+// the masked points get an x for which the term is exactly 0, so one body serves both.
 // One wing-pass job: the line records and tiles of one LineOpac (one atmosphere and grid).
 struct WingJob {
     int ntau, nwl;
@@ -170,34 +171,26 @@ __device__ __forceinline__ bool wing_tile(const WingJob &J, int tile, unsigned c
                 for (int d = 0; d < D; d++) w[d] = cw[q * ntau + t0 + min(d, nd - 1)];
                 const bool full = h.ileft <= tile_first && h.iright >= tile_last &&
                                   (h.cr < tile_first || h.cl > tile_last);
-                if (full) {
-#pragma unroll
-                    for (int d = 0; d < D; d++)
-#pragma unroll
-                        for (int k = 0; k < P; k++) {
-                            float t = fmaf(x[k], w[d].vv2, w[d].c2m1);
-                            float den = fmaf(t, t, w[d].twoA);
-                            float num = fmaf(w[d].c1, t, w[d].c1);
-                            part[d][k] = fmaf(num, rcp_approx(den), part[d][k]);
-                        }
-                } else {
-                    bool in[P];
+                if (!full) {
+                    // points outside the window or inside the core range take the header's offset x,
+                    // for which the wing term is exactly 0: one body serves every tile
+                    const float xm = __int_as_float(h.pad0);
 #pragma unroll
                     for (int k = 0; k < P; k++) {
-                        int p1 = pix[k] + 1;
-                        in[k] = p1 >= h.ileft && p1 <= h.iright && (p1 < h.cl || p1 > h.cr);
+                        const int p1 = pix[k] + 1;
+                        const bool in = p1 >= h.ileft && p1 <= h.iright && (p1 < h.cl || p1 > h.cr);
+                        x[k] = in ? x[k] : xm;
                     }
-#pragma unroll
-                    for (int d = 0; d < D; d++)
-#pragma unroll
-                        for (int k = 0; k < P; k++) {
-                            float t = fmaf(x[k], w[d].vv2, w[d].c2m1);
-                            float den = fmaf(t, t, w[d].twoA);
-                            float num = fmaf(w[d].c1, t, w[d].c1);
-                            float r = rcp_approx(den);
-                            part[d][k] = fmaf(num, in[k] ? r : 0.0f, part[d][k]);
-                        }
                 }
+#pragma unroll
+                for (int d = 0; d < D; d++)
+#pragma unroll
+                    for (int k = 0; k < P; k++) {
+                        float t = fmaf(x[k], w[d].vv2, w[d].c2m1);
+                        float den = fmaf(t, t, w[d].twoA);
+                        float num = fmaf(w[d].c1, t, w[d].c1);
+                        part[d][k] = fmaf(num, rcp_approx(den), part[d][k]);
+                    }
                 if (++nfold == FOLD) {
                     nfold = 0;
 #pragma unroll

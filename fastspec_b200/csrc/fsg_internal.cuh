@@ -83,7 +83,9 @@ struct __align__(16) CoreRec { float vv, cop, ua; int ia; };
 // Line header of a retained line inside a block (fast path).  The centre offset Wlcent is split
 // into FP32 wlh + wll (wlh = fl32(Wlcent), wll = fl32(Wlcent - wlh)).  [cl, cr] is the core range:
 // every wavelength index of the window where some depth may have s < 196 lies inside it
-// (cl > cr when no depth has a core).
+// (cl > cr when no depth has a core).  pad0 holds, in the wing pass's headers, the FP32 bits of the
+// x = dl^2 that makes every depth's wing term exactly 0 (points outside the window or inside the core
+// range of a partly covered tile); the magnetic pass keeps its He I table index there.
 struct __align__(16) LineHdr { float wlh, wll; int ileft, iright; int cl, cr, pad0, pad1; };
 
 // Zeeman components of a device line list (CSR by line)

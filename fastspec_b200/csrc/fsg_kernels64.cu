@@ -244,6 +244,7 @@ __global__ void k_params_fast(AtmView A, LineView L, const int64_t *__restrict__
     XCoef XC;
     xline_setup(A, L, i, wlc, f, &XC);
     double hcore = -1.0;        // largest |dl| of any depth's core region (s < 196)
+    float vv2min = 3.0e38f;     // smallest FP32 vv2 over depths (the wing pass's mask offset)
     for (int t = 0; t < nt; t++) {
         double cop, vv, av;
         xline_depth(A, t, XC, &cop, &vv, &av);
@@ -254,6 +255,7 @@ __global__ void k_params_fast(AtmView A, LineView L, const int64_t *__restrict__
         w.c2m1 = (float)(a2 - 0.5);
         w.twoA = (float)(2.0 * a2);
         w.c1 = (float)(cop * av * FSG_SQRTPIINV);
+        vv2min = fminf(vv2min, w.vv2);
         CoreRec c;
         c.vv = (float)vv; c.cop = (float)cop;
         // table row and weight of a in FP32 (sqrt(a) nodes, voigt.f90:84-92); ia = 0: a >= 8
@@ -287,7 +289,11 @@ __global__ void k_params_fast(AtmView A, LineView L, const int64_t *__restrict__
         int cl = max(a - 1, h.ileft), cr = min(b + 1, h.iright);
         if (cl <= cr) { h.cl = cl; h.cr = cr; }
     }
-    h.pad0 = 0; h.pad1 = 0;
+    // x offset that silences a point in the wing pass: with dl^2 replaced by 1e19 / min vv2, every
+    // depth has t >= 1e19, so t^2 >= 1e38 and the FP32 reciprocal (flush-to-zero) is exactly 0 while
+    // c1 (t + 1) stays finite; the point then adds exactly 0
+    h.pad0 = __float_as_int(1.0e19f / vv2min);
+    h.pad1 = 0;
     hdr[j] = h;
 }
 
