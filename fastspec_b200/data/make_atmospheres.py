@@ -664,8 +664,68 @@ def make_h5_pin(gold):
     print("pin_solar_h5: region pixels", i1 - i0 + 1, "lines", extra.n)
 
 
+def zh5_seeded():
+    """The Zeeman list of the .zh5 fixture: pin_magnetic's seeded lines with three Lande factors set to
+    the converters' 99 (unknown), which the reader turns into unsplit lines."""
+    extra = W.zeeman_lines(60, 6040.3, 6042.7, W.SEED0 + 2)
+    jlo, jup, glo, gup = (np.asarray(a, np.float32).copy() for a in extra.zeeman)
+    glo[[5, 23]] = 99.0
+    gup[41] = 99.0
+    return extra, (jlo, jup, glo, gup)
+
+
+def make_zh5_pin(gold):
+    """Zeeman HDF5 fixture (pin_magnetic_zh5.npz): the probes and pin_magnetic's seeded lines written by
+    fsio.write_hdf5_lines as one .zh5 list (J and Lande factor columns; the reference builds the
+    splitting patterns itself, ioutils.f90:997-1031), Stokes IQUV with BFRAME 1, |B| = 2 kG at 60/30 deg,
+    9 angles, on 6040-6043 A at 0.002 A."""
+    teff, logg, ntau, species, ismol, _, _, vmic, molbrd, _, _ = CONFIGS["magnetic"]
+    model = W.eddington_model(teff, logg, ntau)
+    state = load_state("magnetic")
+    grid = (6000.0, 6043.0, 0.002, 0)
+    region = (6040.0, 6043.0)
+    bfield = (2000.0, 60.0, 30.0)
+    extra, z = zh5_seeded()
+    pgf = np.load(os.path.join(HERE, "atm_magnetic.npz"))["probe_loggf"]
+    probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
+    merged = merge([probes, extra])
+    npr = probes.n
+    zz = [np.concatenate([np.full(npr, v, np.float32), a]) for v, a in zip((1.0, 1.0, 99.0, 99.0), z)]
+    t = merged._txt
+    with tempfile.TemporaryDirectory() as wd:
+        W.write_krz(os.path.join(wd, "model.krz"), model)
+        fsio.write_hdf5_lines(os.path.join(wd, "lines.zh5"), merged.species, merged.spc, merged.wl,
+                              W.f32_of_text(t["elo"], "%.4f"), W.f32_of_text(t["loggf"], "%.3f"),
+                              W.f32_of_text(t["lgrad"], "%.3f"), W.f32_of_text(t["lgqst"], "%.3f"),
+                              W.f32_of_text(t["lgvdw"], "%.3f"), zeeman=zz, provenance="pin_magnetic seeded list")
+        deck = ("wave=%.4f, %.4f, %.6f, %d\nsave=0, 0, 1, 1, 1\nvmic=%.3f\nmolbrd=%d\n"
+                "lines=\n-1  lines.zh5\n\nmodel=model.krz\nmus=9\nbframe=1\nbfield=%g, %g, %g\n"
+                % (grid + (vmic, molbrd) + bfield))
+        log = run_ref(wd, deck)
+        assert "polarised" in log and "Lines read: %d" % merged.n in log, log
+        co = fsio.read_opac(os.path.join(wd, "fs_contop.bin"))
+        sp = fsio.read_spec(os.path.join(wd, "fs_spec.bin"))
+        fl = fsio.read_flux(os.path.join(wd, "fs_flux.bin"))
+    for k in ("rhox", "T", "xne", "xna", "rho"):
+        assert np.array_equal(co[k], state[k]), "EOS state differs from the recovered one: " + k
+    wave = co["wave"]
+    sel = (wave >= region[0] - 1e-9) & (wave <= region[1] + 1e-9)
+    i0, i1 = (int(x) for x in np.nonzero(sel)[0][[0, -1]])
+    te = extra._txt
+    np.savez_compressed(
+        os.path.join(gold, "pin_magnetic_zh5.npz"), grid=np.array(grid, np.float64), i0=i0, i1=i1,
+        atm="magnetic", bframe=1, bfield=np.array(bfield), vmicro=vmic, molbrd=molbrd,
+        contopac=co["opac"][i0:i1 + 1], wave=wave[i0:i1 + 1], xmu=sp["xmu"], spz=sp["spz"][i0:i1 + 1],
+        spc=sp["spc"][i0:i1 + 1], sfl=fl["sfl"][i0:i1 + 1], sfc=fl["sfc"][i0:i1 + 1],
+        line_wl=extra.wl, line_spc=extra.spc, jlo=z[0], jup=z[1], glo=z[2], gup=z[3],
+        **{"txt_" + k: np.asarray(v) for k, v in te.items()})
+    print("pin_magnetic_zh5: region pixels", i1 - i0 + 1, "lines", merged.n)
+
+
 if __name__ == "__main__":
-    if len(sys.argv) > 1 and sys.argv[1] == "h5":
+    if len(sys.argv) > 1 and sys.argv[1] == "zh5":
+        make_zh5_pin(os.path.join(REPO, "tests", "golden"))
+    elif len(sys.argv) > 1 and sys.argv[1] == "h5":
         make_h5_pin(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "sphere":
         make_sphere_pins(os.path.join(REPO, "tests", "golden"))

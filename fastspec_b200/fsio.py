@@ -130,7 +130,8 @@ def read_hdf5_lines(path, species, exact=True):
     species: the caller's species table, a list of (name, ion) in the order of the FractionPF columns
     of its atmosphere state; each line's index into it (spc) is -1 for a species the table lacks.
     Returns dict(wl, elo, gf, grad, gqst, gvdw, spc, ismol, kind, attrs[, jlo, jup, glo, gup]) with
-    kind 0 (atomic list) or 1 (molecular list), the fsg_lines kinds."""
+    kind 0 (atomic list), 1 (molecular list) or 2 (Zeeman list, whose components hdf5_zeeman_components
+    builds), the fsg_lines kinds."""
     from . import hdf5
     from .workloads import pow10f
     cols, attrs, _ = hdf5.read_lines(path)
@@ -158,6 +159,8 @@ def read_hdf5_lines(path, species, exact=True):
     for c in ("JLO", "JUP", "GLO", "GUP"):
         if c in cols:
             out[c.lower()] = f32(cols[c])[keep]
+    if "jlo" in out:
+        out["kind"] = 2                                  # Zeeman list: the magnetic records (LineTypeMag)
     return out
 
 
@@ -195,3 +198,24 @@ def write_hdf5_lines(path, species, spc, wl, elo, loggf, lgrad, lgqst, lgvdw, wl
                  FORMAT_VERSION="z-1.0" if zeeman is not None else "a-1.0",
                  WMIN=np.float64(wl[0] if n else 0.0), WMAX=np.float64(wl[-1] if n else 0.0))
     hdf5.write_lines(path, cols, attrs, units)
+
+
+def hdf5_zeeman_components(records, pattern):
+    """Zeeman components of a Zeeman HDF5 list (records of read_hdf5_lines with jlo, jup, glo, gup) in
+    the CSR form of fsg_lines, built as ReadHDF builds them (ioutils.f90:997-1031): a line with a Lande
+    factor above 90 (the converters' 99 for unknown or forbidden) is one unshifted pi component of
+    strength 1 and an unshifted sigma pair; otherwise the pattern's pi components as computed and its
+    sigma branch mirrored, blue (negative shifts) first.  pattern(jlo, jup, glo, gup) -> (pi shifts,
+    pi strengths, sigma shifts, sigma strengths), e.g. fastspec_b200.zeeman_pattern."""
+    jlo, jup, glo, gup = (records[k] for k in ("jlo", "jup", "glo", "gup"))
+    npi, nsi, spl_pi, str_pi, spl_si, str_si = [], [], [], [], [], []
+    for i in range(len(jlo)):
+        if glo[i] > 90.0 or gup[i] > 90.0:
+            spi, rpi, ss, rs = [0.0], [1.0], [0.0], [1.0]
+        else:
+            spi, rpi, ss, rs = pattern(float(jlo[i]), float(jup[i]), float(glo[i]), float(gup[i]))
+        npi.append(len(spi)); nsi.append(2 * len(ss))
+        spl_pi += list(spi); str_pi += list(rpi)
+        spl_si += list(-np.asarray(ss, np.float32)) + list(ss); str_si += list(rs) + list(rs)
+    f = lambda a: np.asarray(a, np.float32)
+    return (np.asarray(npi, np.int32), np.asarray(nsi, np.int32), f(spl_pi), f(str_pi), f(spl_si), f(str_si))

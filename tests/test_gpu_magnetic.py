@@ -164,3 +164,22 @@ def test_mixed_mag_against_reference_pin(fsg):
     for q in (1, 2, 3):
         assert np.max(np.abs(spz[i0:i1 + 1, q] - ref[:, q]) / ic) < 1e-5
     assert np.max(np.abs(sfl[i0:i1 + 1] / d["sfl"] - 1)) < 1e-5
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_zh5_list_against_reference_pin(fsg, tmp_path, prec):
+    """A Zeeman HDF5 list read by fsio.read_hdf5_lines, its splitting built from J and the Lande
+    factors with the library's fsg_zeeman_pattern, through the GPU magnetic path: the reference's
+    Stokes IQUV for the same file (tests/golden/pin_magnetic_zh5.npz)."""
+    from test_hdf5 import zh5_pin_lines
+    d, r, z = zh5_pin_lines(tmp_path, fsg.zeeman_pattern)
+    grid, st, meta, co = H.pin_setup(d)
+    C, x, w = mag_ctx(fsg, grid, st, co, nmu=len(d["xmu"]), prec=fsg.PREC_FP64 if prec == "fp64" else fsg.PREC_MIXED)
+    a = {k: r[k] for k in ("wl", "elo", "gf", "grad", "gqst", "gvdw", "spc", "ismol")}
+    C.mag_lineop_calc(fsg.LineList.from_arrays(a, kind=r["kind"], zeeman=z), int(d["bframe"]), d["bfield"])
+    spz, spc, sfl, sfc = C.mag_radtran(int(d["bframe"]), d["bfield"])
+    i0, i1 = int(d["i0"]), int(d["i1"])
+    tol = 1e-8 if prec == "fp64" else 1e-5
+    for q in range(4):
+        assert np.max(np.abs(spz[i0:i1 + 1, q] - d["spz"][:, q]) / d["spc"]) < tol
+    assert np.max(np.abs(sfl[i0:i1 + 1] / d["sfl"] - 1)) < tol

@@ -126,3 +126,41 @@ def test_oracle_hdf5_list_against_reference_pin(oracle_mod, tmp_path):
     x, w, _ = oracle_mod.mu_quadrature(1, len(d["xmu"]))
     sfl, _ = oracle_mod.disk_integ(w, spl[i0:i1 + 1], spc[i0:i1 + 1])
     assert np.max(np.abs(sfl / d["sfl"] - 1)) < 1e-8
+
+
+def zh5_pin_lines(tmp_path, pattern):
+    """pin_magnetic_zh5's seeded lines written as a Zeeman HDF5 list and read back: records and the
+    CSR Zeeman components built from the J and Lande factor columns with `pattern`."""
+    from fastspec_b200 import fsio, workloads as W
+    d = H.load_pin("pin_magnetic_zh5")
+    st, meta = H.load_atm("magnetic")
+    species = [(s.split()[0], int(s.split()[1])) for s in meta["species"]]
+    p = str(tmp_path / "lines.zh5")
+    f = lambda k, fmt: W.f32_of_text(d["txt_" + k], fmt)
+    fsio.write_hdf5_lines(p, species, d["line_spc"], d["line_wl"], f("elo", "%.4f"), f("loggf", "%.3f"),
+                          f("lgrad", "%.3f"), f("lgqst", "%.3f"), f("lgvdw", "%.3f"),
+                          zeeman=(d["jlo"], d["jup"], d["glo"], d["gup"]))
+    r = fsio.read_hdf5_lines(p, species)
+    return d, r, fsio.hdf5_zeeman_components(r, pattern)
+
+
+def test_oracle_zh5_list_against_reference_pin(oracle_mod, tmp_path):
+    """A Zeeman HDF5 list (the reference derives each line's splitting from J and the Lande factors; a
+    factor of 99 marks an unsplit line): the oracle's magnetic path on the records and components read
+    back reproduces the reference's Stokes IQUV for the same file (1e-8 of Ic)."""
+    d, r, z = zh5_pin_lines(tmp_path, oracle_mod.zeeman_pattern)
+    assert r["kind"] == 2 and np.sum(z[0] == 1) >= 3
+    grid, st, meta, co = H.pin_setup(d)
+    S = oracle_mod.State(grid, st, contopac=co, vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]))
+    L = oracle_mod.Lines(**{k: r[k] for k in ("wl", "elo", "gf", "grad", "gqst", "gvdw", "spc", "ismol")},
+                         kind=2, zeeman=z)
+    o = oracle_mod.mag_lineop_calc(S, L, int(d["bframe"]), d["bfield"])
+    spz, spc = oracle_mod.mag_radtran(S, d["xmu"], int(d["bframe"]), d["bfield"], np.zeros((S.nwl, S.ntau)),
+                                      o["maglineopac"])
+    i0, i1 = int(d["i0"]), int(d["i1"])
+    ref, ic = d["spz"], d["spc"]
+    for q in range(4):
+        assert np.max(np.abs(spz[i0:i1 + 1, q] - ref[:, q]) / ic) < 1e-8
+    x, w, _ = oracle_mod.mu_quadrature(1, len(d["xmu"]))
+    sfl, _ = oracle_mod.disk_integ(w, spz[i0:i1 + 1, 0], spc[i0:i1 + 1])
+    assert np.max(np.abs(sfl / d["sfl"] - 1)) < 1e-8
