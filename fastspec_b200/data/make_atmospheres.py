@@ -722,8 +722,61 @@ def make_zh5_pin(gold):
     print("pin_magnetic_zh5: region pixels", i1 - i0 + 1, "lines", merged.n)
 
 
+MOL_CODES = {"TiO": "0822.000000", "H2O": "010108.000000", "CO": "0608.000000", "OH": "0108.000000"}
+
+
+def make_mol_h5_pin(gold):
+    """Molecular HDF5 fixture (pin_cooldwarf_h5.npz): pin_cooldwarf's seeded lines as four
+    single-species molecular lists (fsio.write_hdf5_molecular, the mol2hdf.py layout: no Stark or van
+    der Waals columns, GRAD linear with 0 for the classical value), read by the reference program with
+    the isotopic factor 1 after the probe list; the region's line opacity, continuum and spectra."""
+    name, atmname, mk, grid, region = pin_specs()[1]
+    teff, logg, ntau, species, ismol, _, _, vmic, molbrd, _, _ = CONFIGS[atmname]
+    model = W.eddington_model(teff, logg, ntau)
+    state = load_state(atmname)
+    extra = mk()
+    pgf = np.load(os.path.join(HERE, "atm_%s.npz" % atmname))["probe_loggf"]
+    probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
+    t = extra._txt
+    entries = []
+    with tempfile.TemporaryDirectory() as wd:
+        W.write_krz(os.path.join(wd, "model.krz"), model)
+        probes.write_z(os.path.join(wd, "probes.z"), grid[0], grid[1])
+        for k, (nm, ion) in enumerate(species):
+            sel = extra.spc == k
+            fn = "%s.h5" % nm.lower()
+            fsio.write_hdf5_molecular(os.path.join(wd, fn), nm, ion, MOL_CODES[nm], extra.wl[sel],
+                                      W.f32_of_text(t["elo"][sel], "%.4f"), W.f32_of_text(t["loggf"][sel], "%.3f"),
+                                      np.zeros(int(sel.sum()), np.float32), provenance="pin_cooldwarf seeded list")
+            entries.append("1.0  %s" % fn)
+        deck = ("wave=%.4f, %.4f, %.6f, %d\nsave=0, 1, 1, 1, 1\nvmic=%.3f\nmolbrd=%d\n"
+                "lines=\n-1  probes.z\n%s\n\nmodel=model.krz\nmus=7\n"
+                % (grid + (vmic, molbrd) + ("\n".join(entries),)))
+        log = run_ref(wd, deck)
+        assert all(("File: %s" % e.split()[1]) in log for e in entries), log
+        lo = fsio.read_opac(os.path.join(wd, "fs_lineop.bin"))
+        co = fsio.read_opac(os.path.join(wd, "fs_contop.bin"))
+        sp = fsio.read_spec(os.path.join(wd, "fs_spec.bin"))
+        fl = fsio.read_flux(os.path.join(wd, "fs_flux.bin"))
+    for k in ("rhox", "T", "xne", "xna", "rho"):
+        assert np.array_equal(lo[k], state[k]), "EOS state differs from the recovered one: " + k
+    wave = lo["wave"]
+    sel = (wave >= region[0] - 1e-9) & (wave <= region[1] + 1e-9)
+    i0, i1 = (int(x) for x in np.nonzero(sel)[0][[0, -1]])
+    np.savez_compressed(
+        os.path.join(gold, "pin_cooldwarf_h5.npz"), grid=np.array(grid, np.float64), i0=i0, i1=i1, atm=atmname,
+        vmicro=vmic, molbrd=molbrd, contopac=co["opac"][i0:i1 + 1], lineopac=lo["opac"][i0:i1 + 1],
+        wave=wave[i0:i1 + 1], xmu=sp["xmu"], spl=sp["spl"][i0:i1 + 1], spc=sp["spc"][i0:i1 + 1],
+        sfl=fl["sfl"][i0:i1 + 1], sfc=fl["sfc"][i0:i1 + 1], line_wl=extra.wl, line_spc=extra.spc,
+        **{"txt_" + k: np.asarray(v) for k, v in t.items()})
+    print("pin_cooldwarf_h5: region pixels", i1 - i0 + 1, "lines", extra.n)
+    print(log[-600:])
+
+
 if __name__ == "__main__":
-    if len(sys.argv) > 1 and sys.argv[1] == "zh5":
+    if len(sys.argv) > 1 and sys.argv[1] == "molh5":
+        make_mol_h5_pin(os.path.join(REPO, "tests", "golden"))
+    elif len(sys.argv) > 1 and sys.argv[1] == "zh5":
         make_zh5_pin(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "h5":
         make_h5_pin(os.path.join(REPO, "tests", "golden"))

@@ -219,3 +219,25 @@ def hdf5_zeeman_components(records, pattern):
         spl_si += list(-np.asarray(ss, np.float32)) + list(ss); str_si += list(rs) + list(rs)
     f = lambda a: np.asarray(a, np.float32)
     return (np.asarray(npi, np.int32), np.asarray(nsi, np.int32), f(spl_pi), f(str_pi), f(spl_si), f(str_si))
+
+
+def write_hdf5_molecular(path, name, ion, code, wl, elo, loggf, grad, wl_vac=0, provenance=""):
+    """Write a single-species molecular line list in the reference's HDF5 layout (the columns and
+    group attributes of mol2hdf.py: W, E, LGGF, GRAD (linear radiative damping, 0 for the classical
+    value); NL, ID (species code), NAME (the molecule as the EOS names it), ION, WL_VAC, FILE, DATE,
+    PROVENANCE, FORMAT_VERSION, WMIN, WMAX), contiguous and unfiltered.  Lines sorted by wavelength."""
+    import datetime
+    from . import hdf5
+    wl = np.asarray(wl, np.float64)
+    if len(wl) > 1 and np.any(np.diff(wl) < 0):
+        raise ValueError("write_hdf5_molecular: lines must be sorted by wavelength")
+    cols = dict(W=wl, E=np.asarray(elo, np.float32), LGGF=np.asarray(loggf, np.float32),
+                GRAD=np.asarray(grad, np.float32))
+    units = dict(W="Angstrom (air or vacuum per the WL_VAC attribute)", E="eV (lower-level excitation energy)",
+                 LGGF="log10(gf) (dimensionless)", GRAD="1/s (radiative damping constant, linear)")
+    n = len(wl)
+    attrs = dict(NL=np.int32(n), ID=str(code), NAME=str(name), ION=np.int32(ion), WL_VAC=np.int16(wl_vac),
+                 FILE=str(path).rsplit("/", 1)[-1].rsplit(".", 1)[0], DATE=datetime.date.today().isoformat(),
+                 PROVENANCE=provenance, FORMAT_VERSION="m-1.1",
+                 WMIN=np.float64(wl[0] if n else 0.0), WMAX=np.float64(wl[-1] if n else 0.0))
+    hdf5.write_lines(path, cols, attrs, units)

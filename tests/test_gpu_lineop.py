@@ -424,3 +424,27 @@ def test_hdf5_list_against_reference_pin(fsg, tmp_path, prec):
         assert np.max(np.abs(lo - ref) / (ref + d["contopac"])) < 2e-6
     spl, spc, sfl, sfc = C.radtran()
     assert np.max(np.abs(sfl[i0:i1 + 1] / d["sfl"] - 1)) < (1e-8 if prec == "fp64" else 1e-5)
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_molecular_h5_lists_against_reference_pin(fsg, tmp_path, prec):
+    """Four single-species molecular HDF5 lists (kind 1) through fsg_lineop_calc one after the other
+    (the device LineOpac accumulates): the reference's line opacity and flux for the same files (FP64
+    path within 2e-7: one-ulp differences of some lines' FP32 gf, as for the oracle)."""
+    from test_hdf5 import mol_h5_pin_lists
+    d, lists = mol_h5_pin_lists(tmp_path)
+    grid, st, meta, co = H.pin_setup(d)
+    C = ctx_for(fsg, grid, st, co, fsg.PREC_MIXED if prec == "mixed" else fsg.PREC_FP64,
+                vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]))
+    for r in lists:
+        a = {k: r[k] for k in ("wl", "elo", "gf", "grad", "gqst", "gvdw", "spc", "ismol")}
+        g = C.lineop_calc(fsg.LineList.from_arrays(a, kind=r["kind"]))
+    i0, i1 = int(d["i0"]), int(d["i1"])
+    lo, ref = g["lineopac"][i0:i1 + 1], d["lineopac"]
+    assert np.array_equal(lo > 0, ref > 0)
+    if prec == "fp64":
+        assert np.max(np.abs(lo[ref > 0] / ref[ref > 0] - 1)) < 2e-7
+    else:
+        assert np.max(np.abs(lo - ref) / (ref + d["contopac"])) < 2e-6
+    spl, spc, sfl, sfc = C.radtran()
+    assert np.max(np.abs(sfl[i0:i1 + 1] / d["sfl"] - 1)) < (2e-7 if prec == "fp64" else 1e-5)
