@@ -733,7 +733,11 @@ def main():
                      "flops_per_eval": FLOPS_PER_EVAL, "evals_per_launch": wing_evals / nl,
                      "ms_per_launch": ms_launch,
                      "xu": {"achieved": xu_achieved, "peak": xu_peak, "unit": "reciprocals/s",
-                            "frac": xu_achieved / xu_peak}},
+                            "frac": xu_achieved / xu_peak},
+                     # the same launch against the measured copy bandwidth: far from HBM-bound
+                     "hbm": {"achieved": traffic / (ms_launch / 1e3) / 1e9,
+                             "peak": float(peaks.get("hbm_gbs", 6650.0)), "unit": "GB/s",
+                             "frac": traffic / (ms_launch / 1e3) / 1e9 / float(peaks.get("hbm_gbs", 6650.0))}},
         "core_pass": {"kernel": "k_core_fast", "evals": st["core_evals"], "ms": st["ms_core_kernels"],
                       "evals_per_s": st["core_evals"] / max(st["ms_core_kernels"], 1e-9) * 1e3},
         "gpu_launches": r["launches"],
