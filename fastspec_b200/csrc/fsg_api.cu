@@ -82,9 +82,10 @@ double fsg_count_evals(fsg_ctx *, int64_t, const int32_t *, const int32_t *, con
 static double count_windows(fsg_ctx *, int64_t, const int32_t *, const int32_t *, const int32_t *, int, int);
 void fsg_launch_range_clip(cudaStream_t, int64_t, const int32_t *, const int32_t *, const int32_t *, int, int,
                            int32_t *, int32_t *, int32_t *);
-size_t fsg_stokes_smem(int, int);
 int fsg_launch_stokes(cudaStream_t, const AtmView &, const double *, const double *, const double *, int,
-                      const double *, const double *, const double *, double *, double *);
+                      const double *, const double *, const double *, double *, double *, double *, int);
+size_t fsg_stokes_work(int, int, int);
+int fsg_stokes_chunk(int, int, int, size_t);
 void fsg_launch_mag_center(cudaStream_t, const AtmView &, const LineView &, const ZView &, double, const VoigtTables &,
                            int32_t *, int32_t *, int32_t *, unsigned long long *);
 void fsg_launch_mag_params(cudaStream_t, const AtmView &, const LineView &, int64_t, const int64_t *, int64_t,
@@ -159,6 +160,7 @@ struct fsg_ctx {
     DBuf d_spl, d_spc, d_sfl, d_sfc, d_work, d_a, d_v, d_h, d_l;
     // magnetic
     DBuf z_npi, z_nsi, z_pioff, z_sioff, z_splpi, z_strpi, z_splsi, z_strsi, d_zsc, z_rawpi, z_rawsi, d_zmap, d_geo;
+    DBuf d_stkwork;                            // per-thread work arrays of the Stokes solver
     cudaEvent_t ev[8];
     cudaStream_t cstream = nullptr;            // host->device line uploads, overlapped with the central pass
     std::vector<cudaEvent_t> cev;
@@ -247,7 +249,8 @@ void fsg_destroy(fsg_ctx *ctx) {
                      &ctx->d_work, &ctx->d_a, &ctx->d_v, &ctx->d_h, &ctx->d_l, &ctx->z_npi, &ctx->z_nsi,
                      &ctx->z_pioff, &ctx->z_sioff, &ctx->z_splpi, &ctx->z_strpi, &ctx->z_splsi, &ctx->z_strsi,
                      &ctx->d_zsc, &ctx->z_rawpi, &ctx->z_rawsi, &ctx->d_zmap, &ctx->d_geo,
-                     &ctx->d_ray_n, &ctx->d_ray_graz, &ctx->d_ray_map, &ctx->d_ray_m, &ctx->d_ray_geo };
+                     &ctx->d_ray_n, &ctx->d_ray_graz, &ctx->d_ray_map, &ctx->d_ray_m, &ctx->d_ray_geo,
+                     &ctx->d_stkwork };
     for (DBuf *b : bufs) b->release();
     for (int i = 0; i < 8; i++) if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
     for (cudaEvent_t e : ctx->cev) cudaEventDestroy(e);
@@ -1479,10 +1482,13 @@ int fsg_mag_radtran(fsg_ctx *ctx, int bframe, const double *bfield, int nbfield,
     rc = fsg_launch_radtran(s, A, ctx->d_lineopac.as<double>(), ctx->d_rhox.as<double>(), nmu, ctx->d_xmu.as<double>(),
                             ctx->d_wmu.as<double>(), nullptr, ctx->d_spc.as<double>(), nullptr, ctx->d_sfc.as<double>());
     if (rc) return cuda_fail(ctx, cudaGetLastError(), "k_radtran");
+    // chunks of wavelengths whose per-thread work arrays take at most 2 GiB
+    const int chunk = fsg_stokes_chunk(ctx->ntau, nmu, ctx->nwl, (size_t)2 << 30);
+    ALLOC(ctx->d_stkwork, fsg_stokes_work(ctx->ntau, nmu, chunk));
     rc = fsg_launch_stokes(s, A, ctx->d_lineopac.as<double>(), ctx->d_maglineopac.as<double>(), ctx->d_rhox.as<double>(),
                            nmu, ctx->d_xmu.as<double>(), ctx->d_wmu.as<double>(), ctx->d_geo.as<double>(),
-                           ctx->d_spl.as<double>(), ctx->d_sfl.as<double>());
-    if (rc) return cuda_fail(ctx, cudaGetLastError(), "k_stokes");
+                           ctx->d_spl.as<double>(), ctx->d_sfl.as<double>(), ctx->d_stkwork.as<double>(), chunk);
+    if (rc) return cuda_fail(ctx, cudaGetLastError(), "k_stokes_thr");
     ctx->launches += 2;
     if (spz) CK(cudaMemcpyAsync(spz, ctx->d_spl.p, 4 * nsp, cudaMemcpyDeviceToHost, s), "spz");
     if (spc) CK(cudaMemcpyAsync(spc, ctx->d_spc.p, nsp, cudaMemcpyDeviceToHost, s), "spc");

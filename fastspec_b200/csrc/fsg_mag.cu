@@ -8,8 +8,8 @@
 //                   (opacity.f90:468-520, 611-675)
 //   k_mag_accum     MagLineOpacity1 per wavelength (opacity.f90:391-464)
 //   k_mag_wide      MagLineOpacity3 for the wide lines, in line order (synth.f90:1341-1361)
-//   k_stokes        StokesPrfPP (solver.f90:265-394) + Solve4x4 (solver.f90:541-588) and the
-//                   Stokes-I flux quadrature
+//   k_stokes_thr    StokesPrfPP (solver.f90:265-394) + Solve4x4 (solver.f90:541-588), one thread per
+//                   (wavelength, angle); k_stokes_flux the Stokes-I flux quadrature
 //   k_stokes_sph    StokesPrfSph (solver.f90:402-538) along the rays of a spherical model
 #include "fsg_fp64.cuh"
 
@@ -238,11 +238,12 @@ __global__ void k_mag_params(AtmView A, LineView L, int64_t n, const int64_t *__
 }
 
 // ================================================================================================
-// StokesPrfPP (solver.f90:265-394).  CTA = one wavelength, warp = one angle.  Lanes build the
-// per-depth propagation data (6 distinct matrix elements), TauStep and CentDer in shared memory;
-// lane 0 runs the sequential DELO sweep with the reference's 4x4 algebra.  CentDer of the full
-// matrix is taken through its 6 distinct elements: CentDer commutes with negation exactly and
-// maps the zero diagonal to zero.
+// Stokes solvers (solver.f90:265-538).  The per-depth propagation data are the 6 distinct elements of
+// the normalised 4x4 matrix, the source vector, their CentDer derivatives and the TauStep steps;
+// CentDer of the full matrix is taken through its 6 distinct elements (CentDer commutes with negation
+// exactly and maps the zero diagonal to zero).  k_stokes_thr (plane-parallel) gives every thread one
+// (wavelength, angle) sweep over per-thread work arrays in global memory; k_stokes_sph (spherical
+// rays, up to 2 ntau points) keeps each ray's data in shared memory and lane 0 of its warp sweeps.
 // ================================================================================================
 #define STK_FIELDS 22   // per depth: PhiI, 6 K, 6 KD, 4 SRC4, 4 SRD, Deltau
 
@@ -298,9 +299,9 @@ __device__ void solve4x4(const double *A, const double *B, double *X) {
 // and its derivative, Dt the optical-depth steps.  XINT2 holds the boundary Stokes vector on entry and
 // the emergent one on return.
 __device__ void stokes_sweep(int N, int ld, const double *Kv, const double *KD, const double *SRC4,
-                             const double *SRD, const double *Dt, double *XINT2) {
+                             const double *SRD, const double *Dt, double *XINT2, size_t es = 1) {
     double K1[16], K0[16], KD0[16], XKA[16], XKB[16], QA[16], QB[16], AA[16], e6[6], d6[6], XINT1[4];
-    for (int q = 0; q < 6; q++) { e6[q] = Kv[q * ld + N - 1]; d6[q] = KD[q * ld + N - 1]; }
+    for (int q = 0; q < 6; q++) { e6[q] = Kv[(q * ld + N - 1) * es]; d6[q] = KD[(q * ld + N - 1) * es]; }
     build_k(e6, K0); build_k(d6, KD0);
     for (int j = 0; j < 4; j++) for (int i = 0; i < 4; i++) {
         double acc = 0.0;
@@ -310,10 +311,10 @@ __device__ void stokes_sweep(int N, int ld, const double *Kv, const double *KD, 
     for (int q = 0; q < 16; q++) K1[q] = K0[q];         // XK at k1
     for (int k = N - 2; k >= 0; k--) {
         int k1 = k + 1;
-        double Dtau = Dt[k], Dtau05 = 0.5 * Dtau, Eps, Alpha, Beta, Gamma;
+        double Dtau = Dt[k * es], Dtau05 = 0.5 * Dtau, Eps, Alpha, Beta, Gamma;
         delo_coef(Dtau, Eps, Alpha, Beta, Gamma);
         Gamma = Gamma * 0.5;
-        for (int q = 0; q < 6; q++) { e6[q] = Kv[q * ld + k]; d6[q] = KD[q * ld + k]; }
+        for (int q = 0; q < 6; q++) { e6[q] = Kv[(q * ld + k) * es]; d6[q] = KD[(q * ld + k) * es]; }
         build_k(e6, K0); build_k(d6, KD0);
         for (int q = 0; q < 16; q++) XKA[q] = XKB[q];
         for (int j = 0; j < 4; j++) for (int i = 0; i < 4; i++) {
@@ -333,12 +334,12 @@ __device__ void stokes_sweep(int N, int ld, const double *Kv, const double *KD, 
             for (int q = 0; q < 4; q++) {
                 m1 = m1 + K1[i + 4 * q] * XINT2[q];
                 m2 = m2 + QA[i + 4 * q] * XINT2[q];
-                m3 = m3 + K1[i + 4 * q] * SRC4[q * ld + k1];
-                m4 = m4 + K0[i + 4 * q] * SRC4[q * ld + k];
+                m3 = m3 + K1[i + 4 * q] * SRC4[(q * ld + k1) * es];
+                m4 = m4 + K0[i + 4 * q] * SRC4[(q * ld + k) * es];
             }
-            XINT1[i] = Eps * XINT2[i] - Beta * m1 + Gamma * m2 + (Beta + Gamma) * SRC4[i * ld + k1]
-                     - GD * m3 + (Alpha + Gamma) * SRC4[i * ld + k] + GD * m4
-                     + GD * (SRD[i * ld + k] - SRD[i * ld + k1]);
+            XINT1[i] = Eps * XINT2[i] - Beta * m1 + Gamma * m2 + (Beta + Gamma) * SRC4[(i * ld + k1) * es]
+                     - GD * m3 + (Alpha + Gamma) * SRC4[(i * ld + k) * es] + GD * m4
+                     + GD * (SRD[(i * ld + k) * es] - SRD[(i * ld + k1) * es]);
         }
         solve4x4(AA, XINT1, XINT2);
         for (int q = 0; q < 16; q++) K1[q] = K0[q];
@@ -364,85 +365,74 @@ __device__ __forceinline__ double stokes_point(const double *m, double lop, doub
     return PI;
 }
 
-__global__ void k_stokes(AtmView A, const double *__restrict__ lineopac, const double *__restrict__ mlo,
-                         const double *__restrict__ rhox, int nmu, const double *__restrict__ xmu,
-                         const double *__restrict__ wmu, const double *__restrict__ geo, double *spz, double *sfl) {
-    extern __shared__ double sm[];
-    const int iwl = blockIdx.x;                  // 0-based
-    const int im = threadIdx.x >> 5, lane = threadIdx.x & 31;
+// StokesPrfPP, one thread per (wavelength, angle) from the first wavelength iwl0 on: each thread builds
+// its propagation data, TauStep and CentDer over depth into its own global work arrays (STK_FIELDS x
+// ntau doubles, element stride = the launch's thread count T, so that the threads of a warp touch
+// consecutive addresses) and runs the sequential 4x4 sweep itself; every lane of every warp sweeps.
+// The reference's operations, in its order.
+__global__ void __launch_bounds__(128)
+k_stokes_thr(AtmView A, const double *__restrict__ lineopac, const double *__restrict__ mlo,
+             const double *__restrict__ rhox, int nmu, const double *__restrict__ xmu,
+             const double *__restrict__ geo, int iwl0, int nwl_chunk, double *work, double *spz) {
+    const size_t T = (size_t)gridDim.x * blockDim.x;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= nwl_chunk * nmu) return;
+    const int iwl = iwl0 + g / nmu, im = g - (g / nmu) * nmu;
     const int N = A.ntau;
-    double *S = sm + (size_t)im * STK_FIELDS * N;          // this angle's arrays, field-major
-    double *PhiI = S, *Kv = S + N, *KD = S + 7 * N, *SRC4 = S + 13 * N, *SRD = S + 17 * N, *Dt = S + 21 * N;
-    double *Src = sm + (size_t)nmu * STK_FIELDS * N;       // shared Planck source [N]
-    __shared__ double Iout[16];
+    double *W = work + g;
+#define F(f, t) W[((size_t)(f) * N + (t)) * T]
     const double PlkC1 = FSG_HC * FSG_VC * 1e13 / FSG_KBOLT;
-    double wl = A.wave[iwl] + A.wfirst;
-    if (threadIdx.x < N) {
-        double C1 = PlkC1 / wl, C2 = exp(50.7649141 - 5.0 * log(wl));
-        Src[threadIdx.x] = C2 / (exp(C1 / A.xi[XI_T * N + threadIdx.x]) - 1.0);
+    const double wl = A.wave[iwl] + A.wfirst;
+    const double C1 = PlkC1 / wl, C2 = exp(50.7649141 - 5.0 * log(wl));
+    const double gm[5] = { geo[0 * nmu + im], geo[1 * nmu + im], geo[2 * nmu + im], geo[3 * nmu + im],
+                           geo[4 * nmu + im] };
+    for (int t = 0; t < N; t++) {
+        const size_t o = (size_t)iwl * N + t;
+        const double sr = C2 / (exp(C1 / A.xi[XI_T * N + t]) - 1.0);
+        double e6[6], s4[4];
+        F(0, t) = stokes_point(mlo + o * 6, lineopac[o], A.contopac[o], sr, gm, e6, s4);
+        for (int q = 0; q < 6; q++) F(1 + q, t) = e6[q];
+        for (int q = 0; q < 4; q++) F(13 + q, t) = s4[q];
     }
-    __syncthreads();
-    if (im < nmu) {
-        double SPhi2 = geo[0 * nmu + im], CPhi2 = geo[1 * nmu + im], CPhi = geo[2 * nmu + im];
-        double S2Psi = geo[3 * nmu + im], C2Psi = geo[4 * nmu + im];
-        for (int t = lane; t < N; t += 32) {
-            const double *m = mlo + ((size_t)iwl * N + t) * 6;
-            double Php = m[0], Phb = m[1], Phr = m[2], Psp = m[3], Psb = m[4], Psr = m[5];
-            double PI = 0.5 * (Php * SPhi2 + 0.5 * (Phr + Phb) * (1.0 + CPhi2)) + lineopac[(size_t)iwl * N + t] +
-                        A.contopac[(size_t)iwl * N + t];
-            double InvPhiI = 1.0 / PI;
-            double Sabs = 0.5 * (Php - 0.5 * (Phr + Phb)) * SPhi2;
-            double PhiQ = Sabs * C2Psi * InvPhiI, PhiU = Sabs * S2Psi * InvPhiI;
-            double PhiV = 0.5 * (Phr - Phb) * CPhi * InvPhiI;
-            double Sdis = 0.5 * (Psp - 0.5 * (Psr + Psb)) * SPhi2;
-            double PsiQ = Sdis * C2Psi * InvPhiI, PsiU = Sdis * S2Psi * InvPhiI;
-            double PsiV = 0.5 * (Psr - Psb) * CPhi * InvPhiI;
-            PhiI[t] = PI;
-            Kv[0 * N + t] = PhiQ; Kv[1 * N + t] = PhiU; Kv[2 * N + t] = PhiV;
-            Kv[3 * N + t] = PsiQ; Kv[4 * N + t] = PsiU; Kv[5 * N + t] = PsiV;
-            double sr = Src[t];
-            SRC4[0 * N + t] = sr; SRC4[1 * N + t] = sr * PhiQ; SRC4[2 * N + t] = sr * PhiU; SRC4[3 * N + t] = sr * PhiV;
+    // TauStep (solver.f90:591-615) with Xmu(im)
+    const double Xmu = xmu[im];
+    for (int t = 0; t < N - 1; t++) {
+        if (t == 0) {
+            double Dx1 = (rhox[1] - rhox[0]) / Xmu;
+            double Yp = (F(0, 1) - F(0, 0)) / Dx1;
+            F(21, 0) = Dx1 * (F(0, 1) + 2.0 * F(0, 0) + Dx1 / 2.0 * Yp) / 3.0;
+        } else {
+            const int k = t + 1;
+            double Dx = (rhox[k - 1] - rhox[k - 2]) / Xmu, Dx1 = (rhox[k] - rhox[k - 1]) / Xmu;
+            double Der = (F(0, k - 1) - F(0, k - 2)) / Dx, Der1 = (F(0, k) - F(0, k - 1)) / Dx1, Yp;
+            if (Der * Der1 > 0.0) {
+                double Lambda = (1.0 + Dx1 / (Dx + Dx1)) / 3.0;
+                Yp = (Der / (Lambda * Der1 + (1.0 - Lambda) * Der)) * Der1;
+            } else Yp = 0.0;
+            F(21, k - 1) = Dx1 * (F(0, k) + 2.0 * F(0, k - 1) + Dx1 / 2.0 * Yp) / 3.0;
         }
-        __syncwarp();
-        // TauStep (solver.f90:591-615) with Xmu(im)
-        double Xmu = xmu[im];
-        for (int t = lane; t < N - 1; t += 32) {
-            if (t == 0) {
-                double Dx1 = (rhox[1] - rhox[0]) / Xmu;
-                double Yp = (PhiI[1] - PhiI[0]) / Dx1;
-                Dt[0] = Dx1 * (PhiI[1] + 2.0 * PhiI[0] + Dx1 / 2.0 * Yp) / 3.0;
-            } else {
-                int k = t + 1;
-                double Dx = (rhox[k - 1] - rhox[k - 2]) / Xmu, Dx1 = (rhox[k] - rhox[k - 1]) / Xmu;
-                double Der = (PhiI[k - 1] - PhiI[k - 2]) / Dx, Der1 = (PhiI[k] - PhiI[k - 1]) / Dx1, Yp;
-                if (Der * Der1 > 0.0) {
-                    double Lambda = (1.0 + Dx1 / (Dx + Dx1)) / 3.0;
-                    Yp = (Der / (Lambda * Der1 + (1.0 - Lambda) * Der)) * Der1;
-                } else Yp = 0.0;
-                Dt[k - 1] = Dx1 * (PhiI[k] + 2.0 * PhiI[k - 1] + Dx1 / 2.0 * Yp) / 3.0;
+    }
+    // CentDer (solver.f90:618-647) of SRC4 (fields 13-16 -> 17-20) and of the 6 elements (1-6 -> 7-12)
+    for (int row = 0; row < 10; row++) {
+        const int fi = row < 4 ? 13 + row : 1 + (row - 4), fo = row < 4 ? 17 + row : 7 + (row - 4);
+        for (int k = 0; k < N; k++) {
+            double out;
+            if (k == 0) out = (F(fi, 1) - F(fi, 0)) / F(21, 0);
+            else if (k == N - 1) out = (F(fi, N - 1) - F(fi, N - 2)) / F(21, N - 2);
+            else {
+                double Dx = F(21, k - 1), Dx1 = F(21, k);
+                double InvDx = 1.0 / Dx, InvDx1 = 1.0 / Dx1;
+                double Lambda = (1.0 + Dx1 / (Dx + Dx1)) / 3.0, Lambda1 = 1.0 - Lambda;
+                double Der = (F(fi, k) - F(fi, k - 1)) * InvDx, Der1 = (F(fi, k + 1) - F(fi, k)) * InvDx1;
+                out = (Der * Der1 > 0.0) ? (Der / (Lambda * Der1 + Lambda1 * Der)) * Der1 : 0.0;
             }
-        }
-        __syncwarp();
-        // CentDer of SRC4 (4 rows) and of the 6 distinct matrix elements
-        for (int e = lane; e < 10 * N; e += 32) {
-            int row = e / N, t = e - row * N;
-            if (row < 4) centder_pt(Dt, SRC4 + row * N, 1, N, t, &SRD[row * N + t]);
-            else centder_pt(Dt, Kv + (row - 4) * N, 1, N, t, &KD[(row - 4) * N + t]);
-        }
-        __syncwarp();
-        if (lane == 0) {
-            double XINT2[4] = { SRC4[N - 1], 0.0, 0.0, 0.0 };
-            stokes_sweep(N, N, Kv, KD, SRC4, SRD, Dt, XINT2);
-            for (int q = 0; q < 4; q++) spz[((size_t)iwl * 4 + q) * nmu + im] = XINT2[q];
-            Iout[im] = XINT2[0];
+            F(fo, k) = out;
         }
     }
-    __syncthreads();
-    if (threadIdx.x == 0 && sfl) {
-        double a = 0.0;
-        for (int q = 0; q < nmu; q++) a = a + Iout[q] * wmu[q];
-        sfl[iwl] = a;
-    }
+    double XINT2[4] = { F(13, N - 1), 0.0, 0.0, 0.0 };
+    stokes_sweep(N, N, &F(1, 0), &F(7, 0), &F(13, 0), &F(17, 0), &F(21, 0), XINT2, T);
+    for (int q = 0; q < 4; q++) spz[((size_t)iwl * 4 + q) * nmu + im] = XINT2[q];
+#undef F
 }
 
 // StokesPrfSph (solver.f90:402-538).  CTA = one wavelength x a group of rays (grid.y), warp = one ray.
@@ -524,14 +514,32 @@ __global__ void k_stokes_flux(int nwl, int nmu, const double *__restrict__ spz, 
 struct fsg_ctx;
 AtmView fsg_view(const fsg_ctx *ctx);
 
-size_t fsg_stokes_smem(int nt, int nmu) { return sizeof(double) * ((size_t)nmu * STK_FIELDS * nt + nt); }
+// per-thread work arrays of k_stokes_thr for one chunk of nwl_chunk wavelengths
+size_t fsg_stokes_work(int nt, int nmu, int nwl_chunk) {
+    const size_t nthr = ((size_t)nwl_chunk * nmu + 127) / 128 * 128;
+    return sizeof(double) * STK_FIELDS * (size_t)nt * nthr;
+}
 
+// the most wavelengths (at least 1, at most nwl) whose work arrays fit in max_bytes
+int fsg_stokes_chunk(int nt, int nmu, int nwl, size_t max_bytes) {
+    const size_t per_wl = sizeof(double) * STK_FIELDS * (size_t)nt * nmu;
+    size_t c = max_bytes / per_wl;
+    if (c > (size_t)nwl) c = (size_t)nwl;
+    return c < 1 ? 1 : (int)c;
+}
+
+// StokesPrfPP over the grid: k_stokes_thr in chunks of nwl_chunk wavelengths whose work arrays fit `work`
+// (fsg_stokes_work bytes), then the Stokes-I flux.
 int fsg_launch_stokes(cudaStream_t s, const AtmView &A, const double *lineopac, const double *mlo, const double *rhox,
-                      int nmu, const double *xmu, const double *wmu, const double *geo, double *spz, double *sfl) {
-    size_t sm = fsg_stokes_smem(A.ntau, nmu);
-    if (sm > 220 * 1024) return FSG_E_ARG;
-    cudaFuncSetAttribute(k_stokes, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    k_stokes<<<A.nwl, 32 * nmu, sm, s>>>(A, lineopac, mlo, rhox, nmu, xmu, wmu, geo, spz, sfl);
+                      int nmu, const double *xmu, const double *wmu, const double *geo, double *spz, double *sfl,
+                      double *work, int nwl_chunk) {
+    if (nwl_chunk < 1) return FSG_E_ARG;
+    for (int w0 = 0; w0 < A.nwl; w0 += nwl_chunk) {
+        const int nw = std::min(nwl_chunk, A.nwl - w0);
+        const int nb = (nwl_chunk * nmu + 127) / 128;      // the grid of a full chunk: fixed element stride
+        k_stokes_thr<<<nb, 128, 0, s>>>(A, lineopac, mlo, rhox, nmu, xmu, geo, w0, nw, work, spz);
+    }
+    if (sfl) k_stokes_flux<<<(A.nwl + 127) / 128, 128, 0, s>>>(A.nwl, nmu, spz, wmu, sfl);
     return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
 }
 
