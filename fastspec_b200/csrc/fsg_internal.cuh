@@ -114,6 +114,7 @@ struct VoigtTables {
     float  *vtab;      // [402][1002]
     float4 *vtab4;     // [401][1002]: (T[r][i], T[r][i+1], T[r+1][i], T[r+1][i+1]) -- one load per lerp
     float2 *fvtab;     // [402][1002] (H, L)
+    float4 *fvtab2;    // [402][1002]: (H, L) at v nodes i and i + 1 of a row -- one 16-byte load per row of a lerp
     double *anode, *aida;   // [402] each
 };
 int fsg_build_tables(VoigtTables *t, cudaStream_t s, std::string *err);

@@ -104,11 +104,21 @@ __global__ void k_vtab4(const float *vtab, float4 *vtab4) {
     vtab4[r * FSG_NV1 + iv] = make_float4(p0[0], p0[1], p1[0], p1[1]);
 }
 
+// (H, L) at two neighbouring v nodes side by side (the last node repeated at the row end)
+__global__ void k_fvtab2(const float2 *fvtab, float4 *fvtab2) {
+    int iv = blockIdx.x * blockDim.x + threadIdx.x;   // 0..NV1-1
+    int r = blockIdx.y;                               // 0..NA1-1
+    if (iv >= FSG_NV1) return;
+    const float2 a = fvtab[r * FSG_NV1 + iv], b = fvtab[r * FSG_NV1 + min(iv + 1, FSG_NV1 - 1)];
+    fvtab2[r * FSG_NV1 + iv] = make_float4(a.x, a.y, b.x, b.y);
+}
+
 int fsg_build_tables(VoigtTables *t, cudaStream_t s, std::string *err) {
     cudaError_t e;
     if ((e = cudaMalloc(&t->vtab4, sizeof(float4) * FSG_NVA * FSG_NV1)) != cudaSuccess ||
         (e = cudaMalloc(&t->vtab, sizeof(float) * FSG_NA1 * FSG_NV1)) != cudaSuccess ||
         (e = cudaMalloc(&t->fvtab, sizeof(float2) * FSG_NA1 * FSG_NV1)) != cudaSuccess ||
+        (e = cudaMalloc(&t->fvtab2, sizeof(float4) * FSG_NA1 * FSG_NV1)) != cudaSuccess ||
         (e = cudaMalloc(&t->anode, sizeof(double) * FSG_NA1)) != cudaSuccess ||
         (e = cudaMalloc(&t->aida, sizeof(double) * FSG_NA1)) != cudaSuccess) {
         *err = fsg_cuda_msg(e, "table allocation");
@@ -119,12 +129,14 @@ int fsg_build_tables(VoigtTables *t, cudaStream_t s, std::string *err) {
     if ((e = cudaGetLastError()) != cudaSuccess) { *err = fsg_cuda_msg(e, "k_tables"); return FSG_E_CUDA; }
     k_vtab4<<<dim3((FSG_NVV + 127) / 128, FSG_NVA), 128, 0, s>>>(t->vtab, t->vtab4);
     if ((e = cudaGetLastError()) != cudaSuccess) { *err = fsg_cuda_msg(e, "k_vtab4"); return FSG_E_CUDA; }
+    k_fvtab2<<<dim3((FSG_NV1 + 127) / 128, FSG_NA1), 128, 0, s>>>(t->fvtab, t->fvtab2);
+    if ((e = cudaGetLastError()) != cudaSuccess) { *err = fsg_cuda_msg(e, "k_fvtab2"); return FSG_E_CUDA; }
     return FSG_OK;
 }
 
 void fsg_free_tables(VoigtTables *t) {
-    cudaFree(t->vtab); cudaFree(t->vtab4); cudaFree(t->fvtab); cudaFree(t->anode); cudaFree(t->aida);
-    t->vtab = nullptr; t->vtab4 = nullptr; t->fvtab = nullptr; t->anode = nullptr; t->aida = nullptr;
+    cudaFree(t->vtab); cudaFree(t->vtab4); cudaFree(t->fvtab); cudaFree(t->fvtab2); cudaFree(t->anode); cudaFree(t->aida);
+    t->vtab = nullptr; t->vtab4 = nullptr; t->fvtab = nullptr; t->fvtab2 = nullptr; t->anode = nullptr; t->aida = nullptr;
 }
 
 // ================================================================================================

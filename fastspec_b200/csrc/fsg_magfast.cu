@@ -55,27 +55,34 @@ __global__ void k_mag_params_fast(AtmView A, LineView L, const int64_t *__restri
     zidx[j] = i;
 }
 
-// FVoigt (H, L) in FP32 at v (signed), L odd in v
-__device__ __forceinline__ void fv32(const float2 *__restrict__ fvtab, const MagRec &r, float v, float &H, float &L) {
+__device__ __forceinline__ float rcp_approx_m(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+// FVoigt (H, L) in FP32 at v (signed), L odd in v.  The table lerp takes each row's two v nodes in one
+// 16-byte load (fvtab2); the wing and continued-fraction forms take one approximate reciprocal.
+__device__ __forceinline__ void fv32(const float4 *__restrict__ fvtab2, const MagRec &r, float v, float &H, float &L) {
     const float av = fabsf(v), a = r.a, a2 = a * a, v2 = av * av, s = v2 + a2;
     if (r.ia > 0 && av < 8.0f) {
         const float fv = av * 125.0f;
         const int iv = min((int)fv, FSG_NVV - 1);
         const float tv = fv - (float)iv;
-        const float2 *p0 = fvtab + (r.ia - 1) * FSG_NV1 + iv, *p1 = p0 + FSG_NV1;
-        const float2 t00 = __ldg(p0), t01 = __ldg(p0 + 1), t10 = __ldg(p1), t11 = __ldg(p1 + 1);
-        const float h0 = t00.x + tv * (t01.x - t00.x), h1 = t10.x + tv * (t11.x - t10.x);
-        const float l0 = t00.y + tv * (t01.y - t00.y), l1 = t10.y + tv * (t11.y - t10.y);
+        const float4 *p0 = fvtab2 + (r.ia - 1) * FSG_NV1 + iv;
+        const float4 g0 = __ldg(p0), g1 = __ldg(p0 + FSG_NV1);      // (H_i, L_i, H_i+1, L_i+1) of rows ia, ia+1
+        const float h0 = g0.x + tv * (g0.z - g0.x), h1 = g1.x + tv * (g1.z - g1.x);
+        const float l0 = g0.y + tv * (g0.w - g0.y), l1 = g1.y + tv * (g1.w - g1.y);
         H = h0 + r.ua * (h1 - h0);
         L = l0 + r.ua * (l1 - l0);
     } else if (s >= 196.0f) {
-        const float w = 0.56418958354775628f / (s * s - v2 + a2 + 0.25f);
+        const float w = 0.56418958354775628f * rcp_approx_m(s * s - v2 + a2 + 0.25f);
         H = w * a * (s + 0.5f);
         L = w * av * (s - 0.5f);
     } else {
         const float p = v2 - a2 - 1.5f, q = 2.0f * av * a;
         const float dr = av * p - a * q, di = av * q + a * p;
-        const float w = 0.56418958354775628f / (dr * dr + di * di);
+        const float w = 0.56418958354775628f * rcp_approx_m(dr * dr + di * di);
         H = w * ((p + 0.5f) * di - q * dr);
         L = w * ((p + 0.5f) * dr + q * di);
     }
@@ -85,7 +92,7 @@ __device__ __forceinline__ void fv32(const float2 *__restrict__ fvtab, const Mag
 __global__ void __launch_bounds__(32 * MAG_W)
 k_mag_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *__restrict__ hdr,
            const MagRec *__restrict__ rec, const int64_t *__restrict__ zidx, ZView Z, const double *__restrict__ heshf,
-           const int *__restrict__ tile_lo, const int *__restrict__ tile_hi, const float2 *__restrict__ fvtab,
+           const int *__restrict__ tile_lo, const int *__restrict__ tile_hi, const float4 *__restrict__ fvtab2,
            double *__restrict__ mlo) {
     const int tile = blockIdx.x;
     const int lo = tile_lo[tile], hi = tile_hi[tile];
@@ -131,7 +138,7 @@ k_mag_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *__
 #pragma unroll
             for (int d = 0; d < MAG_D; d++) {
                 float H, L;
-                fv32(fvtab, r[d], vb[d] - sp * r[d].vv, H, L);
+                fv32(fvtab2, r[d], vb[d] - sp * r[d].vv, H, L);
                 s[d][0] += st * H; s[d][3] += st * L;
             }
         }
@@ -141,7 +148,7 @@ k_mag_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *__
 #pragma unroll
             for (int d = 0; d < MAG_D; d++) {
                 float H, L;
-                fv32(fvtab, r[d], vb[d] - sp * r[d].vv, H, L);
+                fv32(fvtab2, r[d], vb[d] - sp * r[d].vv, H, L);
                 if (qa == 1) { s[d][1] += st * H; s[d][4] += st * L; }
                 else { s[d][2] += st * H; s[d][5] += st * L; }
             }
@@ -175,6 +182,6 @@ int fsg_launch_mag_fast(cudaStream_t s, const AtmView &A, const LineHdr *hdr, co
                         const ZView &Z, const int *tlo, const int *thi, const VoigtTables &T, double *mlo) {
     const dim3 grid((A.nwl + 31) / 32, (A.ntau + MAG_W * MAG_D - 1) / (MAG_W * MAG_D));
     k_mag_fast<<<grid, 32 * MAG_W, 0, s>>>(A.ntau, A.nwl, A.wave, hdr, (const MagRec *)rec, zidx, Z, A.heshf, tlo,
-                                              thi, T.fvtab, mlo);
+                                              thi, T.fvtab2, mlo);
     return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
 }
