@@ -65,7 +65,7 @@ void fsg_launch_linstr(cudaStream_t, const AtmView &, const LineView &, const Vo
 int fsg_launch_radtran_sph(cudaStream_t, const AtmView &, const double *, const RayView &, const double *, double *,
                            double *, double *, double *);
 int fsg_launch_stokes_sph(cudaStream_t, const AtmView &, const double *, const double *, const RayView &,
-                          const double *, const double *, double *, double *);
+                          const double *, const double *, double *, double *, double *, int);
 int fsg_launch_tile_span(cudaStream_t, int, int, int64_t, const LineHdr *, int *, int *, void *, size_t);
 int fsg_select(cudaStream_t, int64_t, const int32_t *, const int32_t *, const int32_t *, int, int *, int64_t *,
                int64_t *, int64_t *);
@@ -1413,9 +1413,12 @@ static int mag_radtran_sph(fsg_ctx *ctx, const RayView &R, int bframe, const dou
     int rc = fsg_launch_radtran_sph(s, A, ctx->d_lineopac.as<double>(), R, ctx->d_wmu.as<double>(), nullptr, spc,
                                     nullptr, sfc);
     if (rc) return cuda_fail(ctx, cudaGetLastError(), "k_radtran_sph");
+    // chunks of wavelengths whose per-thread work arrays (rays of up to 2 ntau points) take at most 2 GiB
+    const int chunk = fsg_stokes_chunk(M, nmu, ctx->nwl, (size_t)2 << 30);
+    ALLOC(ctx->d_stkwork, fsg_stokes_work(M, nmu, chunk));
     rc = fsg_launch_stokes_sph(s, A, ctx->d_lineopac.as<double>(), ctx->d_maglineopac.as<double>(), R,
-                               ctx->d_wmu.as<double>(), ctx->d_ray_geo.as<double>(), spz, sfl);
-    if (rc == FSG_E_ARG) return fail(ctx, FSG_E_ARG, "mag_radtran: too many depths for the spherical Stokes kernel");
+                               ctx->d_wmu.as<double>(), ctx->d_ray_geo.as<double>(), spz, sfl,
+                               ctx->d_stkwork.as<double>(), chunk);
     if (rc) return cuda_fail(ctx, cudaGetLastError(), "k_stokes_sph");
     ctx->launches += sfl ? 3 : 2;
     return FSG_OK;

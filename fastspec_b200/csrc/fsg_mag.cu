@@ -10,7 +10,8 @@
 //   k_mag_wide      MagLineOpacity3 for the wide lines, in line order (synth.f90:1341-1361)
 //   k_stokes_thr    StokesPrfPP (solver.f90:265-394) + Solve4x4 (solver.f90:541-588), one thread per
 //                   (wavelength, angle); k_stokes_flux the Stokes-I flux quadrature
-//   k_stokes_sph    StokesPrfSph (solver.f90:402-538) along the rays of a spherical model
+//   k_stokes_sph    StokesPrfSph (solver.f90:402-538) along the rays of a spherical model, one thread per
+//                   (wavelength, ray)
 #include "fsg_fp64.cuh"
 
 #include <algorithm>
@@ -241,9 +242,9 @@ __global__ void k_mag_params(AtmView A, LineView L, int64_t n, const int64_t *__
 // Stokes solvers (solver.f90:265-538).  The per-depth propagation data are the 6 distinct elements of
 // the normalised 4x4 matrix, the source vector, their CentDer derivatives and the TauStep steps;
 // CentDer of the full matrix is taken through its 6 distinct elements (CentDer commutes with negation
-// exactly and maps the zero diagonal to zero).  k_stokes_thr (plane-parallel) gives every thread one
-// (wavelength, angle) sweep over per-thread work arrays in global memory; k_stokes_sph (spherical
-// rays, up to 2 ntau points) keeps each ray's data in shared memory and lane 0 of its warp sweeps.
+// exactly and maps the zero diagonal to zero).  k_stokes_thr (plane-parallel) and k_stokes_sph (spherical
+// rays of up to 2 ntau points) give every thread one (wavelength, angle) sweep over per-thread work
+// arrays in global memory.
 // ================================================================================================
 #define STK_FIELDS 22   // per depth: PhiI, 6 K, 6 KD, 4 SRC4, 4 SRD, Deltau
 
@@ -435,67 +436,75 @@ k_stokes_thr(AtmView A, const double *__restrict__ lineopac, const double *__res
 #undef F
 }
 
-// StokesPrfSph (solver.f90:402-538).  CTA = one wavelength x a group of rays (grid.y), warp = one ray.
-// Lanes gather the six profiles, line and continuum opacity and source of the layer each ray point
-// samples, with the field projection of that point (geo [5][nmu][stride]); TauStep runs on the ray's
-// column mass (mu = 1); lane 0 sweeps from zero incoming light for grazing rays, Src(N) otherwise.
-__global__ void k_stokes_sph(AtmView A, const double *__restrict__ lineopac, const double *__restrict__ mlo,
-                             RayView R, const double *__restrict__ geo, int rays_per_cta, double *spz) {
-    extern __shared__ double sm[];
-    const int iwl = blockIdx.x, nt = A.ntau, M = R.stride, nmu = R.nmu;
-    const int wi = threadIdx.x >> 5, lane = threadIdx.x & 31, im = blockIdx.y * rays_per_cta + wi;
-    double *Src = sm;                                              // Planck source by layer [nt]
-    double *S = sm + nt + (size_t)wi * STK_FIELDS * M;            // this ray's fields, leading dim M
-    double *PhiI = S, *Kv = S + M, *KD = S + 7 * M, *SRC4 = S + 13 * M, *SRD = S + 17 * M, *Dt = S + 21 * M;
-    const double PlkC1 = FSG_HC * FSG_VC * 1e13 / FSG_KBOLT;
-    const double wl = A.wave[iwl] + A.wfirst;
-    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
-        double C1 = PlkC1 / wl, C2 = exp(50.7649141 - 5.0 * log(wl));
-        Src[t] = C2 / (exp(C1 / A.xi[XI_T * nt + t]) - 1.0);
-    }
-    __syncthreads();
-    if (im >= nmu) return;
+// StokesPrfSph (solver.f90:402-538), one thread per (wavelength, ray) from the first wavelength iwl0
+// on, with per-thread work arrays as k_stokes_thr (up to 2 ntau points per ray).  Each point gathers the
+// six profiles, line and continuum opacity and source of the layer it samples, with the field
+// projection of that point (geo [5][nmu][stride]); TauStep runs on the ray's column mass (mu = 1); the
+// sweep starts from zero incoming light for grazing rays, Src(N) otherwise.
+__global__ void __launch_bounds__(128)
+k_stokes_sph(AtmView A, const double *__restrict__ lineopac, const double *__restrict__ mlo, RayView R,
+             const double *__restrict__ geo, int iwl0, int nwl_chunk, double *work, double *spz) {
+    const size_t T = (size_t)gridDim.x * blockDim.x;
+    const int nmu = R.nmu, M = R.stride, nt = A.ntau;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= nwl_chunk * nmu) return;
+    const int iwl = iwl0 + g / nmu, im = g - (g / nmu) * nmu;
     const int N = R.n[im];
     const int *mp = R.map + (size_t)im * M;
     const double *m = R.m + (size_t)im * M;
+    double *W = work + g;
+#define F(f, t) W[((size_t)(f) * M + (t)) * T]
+    const double PlkC1 = FSG_HC * FSG_VC * 1e13 / FSG_KBOLT;
+    const double wl = A.wave[iwl] + A.wfirst;
+    const double C1 = PlkC1 / wl, C2 = exp(50.7649141 - 5.0 * log(wl));
     const size_t gs = (size_t)nmu * M, go = (size_t)im * M;
-    for (int t = lane; t < N; t += 32) {
+    for (int t = 0; t < N; t++) {
         const int ia = mp[t];
         const size_t o = (size_t)iwl * nt + ia;
-        double g[5] = { geo[go + t], geo[gs + go + t], geo[2 * gs + go + t], geo[3 * gs + go + t], geo[4 * gs + go + t] };
+        const double sr = C2 / (exp(C1 / A.xi[XI_T * nt + ia]) - 1.0);
+        const double gm[5] = { geo[go + t], geo[gs + go + t], geo[2 * gs + go + t], geo[3 * gs + go + t],
+                               geo[4 * gs + go + t] };
         double e6[6], s4[4];
-        PhiI[t] = stokes_point(mlo + o * 6, lineopac[o], A.contopac[o], Src[ia], g, e6, s4);
-        for (int q = 0; q < 6; q++) Kv[q * M + t] = e6[q];
-        for (int q = 0; q < 4; q++) SRC4[q * M + t] = s4[q];
+        F(0, t) = stokes_point(mlo + o * 6, lineopac[o], A.contopac[o], sr, gm, e6, s4);
+        for (int q = 0; q < 6; q++) F(1 + q, t) = e6[q];
+        for (int q = 0; q < 4; q++) F(13 + q, t) = s4[q];
     }
-    __syncwarp();
     // TauStep (solver.f90:591-615) on the ray's column mass
-    for (int t = lane; t < N - 1; t += 32) {
+    for (int t = 0; t < N - 1; t++) {
         if (t == 0) {
-            double Dx1 = m[1] - m[0], Yp = (PhiI[1] - PhiI[0]) / Dx1;
-            Dt[0] = Dx1 * (PhiI[1] + 2.0 * PhiI[0] + Dx1 / 2.0 * Yp) / 3.0;
+            double Dx1 = m[1] - m[0], Yp = (F(0, 1) - F(0, 0)) / Dx1;
+            F(21, 0) = Dx1 * (F(0, 1) + 2.0 * F(0, 0) + Dx1 / 2.0 * Yp) / 3.0;
         } else {
             double Dx = m[t] - m[t - 1], Dx1 = m[t + 1] - m[t];
-            double Der = (PhiI[t] - PhiI[t - 1]) / Dx, Der1 = (PhiI[t + 1] - PhiI[t]) / Dx1, Yp;
+            double Der = (F(0, t) - F(0, t - 1)) / Dx, Der1 = (F(0, t + 1) - F(0, t)) / Dx1, Yp;
             if (Der * Der1 > 0.0) {
                 double Lambda = (1.0 + Dx1 / (Dx + Dx1)) / 3.0;
                 Yp = (Der / (Lambda * Der1 + (1.0 - Lambda) * Der)) * Der1;
             } else Yp = 0.0;
-            Dt[t] = Dx1 * (PhiI[t + 1] + 2.0 * PhiI[t] + Dx1 / 2.0 * Yp) / 3.0;
+            F(21, t) = Dx1 * (F(0, t + 1) + 2.0 * F(0, t) + Dx1 / 2.0 * Yp) / 3.0;
         }
     }
-    __syncwarp();
-    for (int e = lane; e < 10 * N; e += 32) {
-        int row = e / N, t = e - row * N;
-        if (row < 4) centder_pt(Dt, SRC4 + row * M, 1, N, t, &SRD[row * M + t]);
-        else centder_pt(Dt, Kv + (row - 4) * M, 1, N, t, &KD[(row - 4) * M + t]);
+    // CentDer (solver.f90:618-647) of SRC4 (fields 13-16 -> 17-20) and of the 6 elements (1-6 -> 7-12)
+    for (int row = 0; row < 10; row++) {
+        const int fi = row < 4 ? 13 + row : 1 + (row - 4), fo = row < 4 ? 17 + row : 7 + (row - 4);
+        for (int k = 0; k < N; k++) {
+            double out;
+            if (k == 0) out = (F(fi, 1) - F(fi, 0)) / F(21, 0);
+            else if (k == N - 1) out = (F(fi, N - 1) - F(fi, N - 2)) / F(21, N - 2);
+            else {
+                double Dx = F(21, k - 1), Dx1 = F(21, k);
+                double InvDx = 1.0 / Dx, InvDx1 = 1.0 / Dx1;
+                double Lambda = (1.0 + Dx1 / (Dx + Dx1)) / 3.0, Lambda1 = 1.0 - Lambda;
+                double Der = (F(fi, k) - F(fi, k - 1)) * InvDx, Der1 = (F(fi, k + 1) - F(fi, k)) * InvDx1;
+                out = (Der * Der1 > 0.0) ? (Der / (Lambda * Der1 + Lambda1 * Der)) * Der1 : 0.0;
+            }
+            F(fo, k) = out;
+        }
     }
-    __syncwarp();
-    if (lane == 0) {
-        double XINT2[4] = { R.graz[im] ? 0.0 : SRC4[N - 1], 0.0, 0.0, 0.0 };
-        stokes_sweep(N, M, Kv, KD, SRC4, SRD, Dt, XINT2);
-        for (int q = 0; q < 4; q++) spz[((size_t)iwl * 4 + q) * nmu + im] = XINT2[q];
-    }
+    double XINT2[4] = { R.graz[im] ? 0.0 : F(13, N - 1), 0.0, 0.0, 0.0 };
+    stokes_sweep(N, M, &F(1, 0), &F(7, 0), &F(13, 0), &F(17, 0), &F(21, 0), XINT2, T);
+    for (int q = 0; q < 4; q++) spz[((size_t)iwl * 4 + q) * nmu + im] = XINT2[q];
+#undef F
 }
 
 // Stokes-I flux of the spherical path: Sf = sum over mu of SpZ(mu, 1) Wmu (convol.f90:233-234)
@@ -544,15 +553,14 @@ int fsg_launch_stokes(cudaStream_t s, const AtmView &A, const double *lineopac, 
 }
 
 int fsg_launch_stokes_sph(cudaStream_t s, const AtmView &A, const double *lineopac, const double *mlo,
-                          const RayView &R, const double *wmu, const double *geo, double *spz, double *sfl) {
-    const size_t per_ray = sizeof(double) * STK_FIELDS * (size_t)R.stride, base = sizeof(double) * A.ntau;
-    const size_t cap = 200 * 1024;
-    if (base + per_ray > cap) return FSG_E_ARG;
-    int g = (int)std::min<size_t>((size_t)R.nmu, (cap - base) / per_ray);
-    size_t sm = base + per_ray * g;
-    cudaFuncSetAttribute(k_stokes_sph, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    dim3 grid(A.nwl, (R.nmu + g - 1) / g);
-    k_stokes_sph<<<grid, 32 * g, sm, s>>>(A, lineopac, mlo, R, geo, g, spz);
+                          const RayView &R, const double *wmu, const double *geo, double *spz, double *sfl,
+                          double *work, int nwl_chunk) {
+    if (nwl_chunk < 1) return FSG_E_ARG;
+    for (int w0 = 0; w0 < A.nwl; w0 += nwl_chunk) {
+        const int nw = std::min(nwl_chunk, A.nwl - w0);
+        const int nb = (nwl_chunk * R.nmu + 127) / 128;     // the grid of a full chunk: fixed element stride
+        k_stokes_sph<<<nb, 128, 0, s>>>(A, lineopac, mlo, R, geo, w0, nw, work, spz);
+    }
     if (sfl) k_stokes_flux<<<(A.nwl + 127) / 128, 128, 0, s>>>(A.nwl, R.nmu, spz, wmu, sfl);
     return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
 }
