@@ -2,7 +2,7 @@
 // profiles) and MagRadTranCalc (Stokes DELO-Bezier solver, plane-parallel and spherical).  Built -fmad=false:
 // FP64 throughout, in the reference's operation order.
 //
-//   k_mag_center    MagLineopCalc central pass (synth.f90:1182-1275): Zeeman shifts scaled to
+//   k_mag_center    MagLineopCalc central pass (synth.f90:1182-1275), one warp per line: Zeeman shifts scaled to
 //                   FP32 (Kz |B| lambda^2, synth.f90:1193-1194), centre test (LineOpacity2),
 //                   doubling search with MagLineOpacity2 and RefineIdx bisection
 //                   (opacity.f90:468-520, 611-675)
@@ -20,16 +20,17 @@
 #include <vector>
 
 // MagLineOpacity2 at one wavelength, max over depths of LineOpac/ContOpacL (opacity.f90:468-520)
+// over the depths t0, t0 + tstep, ... (a lane's share when a warp takes the line)
 __device__ double mag_lineop2_max(const AtmView &A, const XCoef &XC, double Wl, double wlc, int ihe,
                                   const ZView &Z, int64_t i, int iwl, double dW, const float *vtab,
-                                  const double *anode, const double *aida) {
+                                  const double *anode, const double *aida, int t0 = 0, int tstep = 1) {
     const int nt = A.ntau;
     double mx = -1.0e308;
     const int np = Z.npi[i], ns = Z.nsi[i];
     const float *spi = Z.splpi + Z.pi_off[i], *ssi = Z.splsi + Z.si_off[i];
     const float *rpi = Z.strpi + Z.pi_off[i], *rsi = Z.strsi + Z.si_off[i];
     double dWl0 = Wl - wlc;
-    for (int t = 0; t < nt; t++) {
+    for (int t = t0; t < nt; t += tstep) {
         double cop, vv, av;
         xline_depth(A, t, XC, &cop, &vv, &av);
         double dWl = dWl0;
@@ -45,11 +46,28 @@ __device__ double mag_lineop2_max(const AtmView &A, const XCoef &XC, double Wl, 
     return mx;
 }
 
+__device__ __forceinline__ double warp_max(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// MagLineOpacity2's maximum over depths (opacity.f90:468-520), the lanes of a warp over the depths
+__device__ __forceinline__ double mag_lineop2_max_warp(const AtmView &A, const XCoef &XC, double Wl, double wlc,
+                                                       int ihe, const ZView &Z, int64_t i, int iwl, double dW,
+                                                       const float *vtab, const double *anode, const double *aida,
+                                                       int lane) {
+    return warp_max(mag_lineop2_max(A, XC, Wl, wlc, ihe, Z, i, iwl, dW, vtab, anode, aida, lane, 32));
+}
+
+// Magnetic central pass, one warp per line: the lanes share the depth loops of the centre test and of
+// every MagLineOpacity2 evaluation of the window search (maxima over depths, so the lanes' partial
+// maxima combine exactly), the search itself is warp-uniform.
 __global__ void k_mag_center(AtmView A, LineView L, ZView Z, double Bsplit, const float *__restrict__ vtab,
                              const double *__restrict__ anode, const double *__restrict__ aida,
                              int32_t *flags, int32_t *ileft, int32_t *iright, unsigned long long *nkeep) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= L.n) return;
+    const int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (i >= L.n) return;                                // whole warps leave together
     const int nt = A.ntau;
     int f = 0;
     if (L.ismol && L.ismol[i]) f |= FSG_F_MOL;
@@ -59,17 +77,18 @@ __global__ void k_mag_center(AtmView A, LineView L, ZView Z, double Bsplit, cons
     // scale the pattern by Kz |B| lambda^2, rounded to FP32 (synth.f90:1193-1194)
     const int np = Z.npi[i], ns = Z.nsi[i];
     double smx_pi = -3.4028234663852886e38, smx_si = -3.4028234663852886e38;
-    for (int k = 0; k < np; k++) {
+    for (int k = lane; k < np; k += 32) {
         float v = (float)((double)Z.rawpi[Z.pi_off[i] + k] * Bsplit * (w * w));
         Z.splpi[Z.pi_off[i] + k] = v;
         smx_pi = fmax(smx_pi, fabs((double)v));
     }
-    for (int k = 0; k < ns; k++) {
+    for (int k = lane; k < ns; k += 32) {
         float v = (float)((double)Z.rawsi[Z.si_off[i] + k] * Bsplit * (w * w));
         Z.splsi[Z.si_off[i] + k] = v;
         smx_si = fmax(smx_si, fabs((double)v));
     }
-    double SplMax = fmax(smx_si, smx_pi);
+    const double SplMax = fmax(warp_max(smx_si), warp_max(smx_pi));
+    __syncwarp();                                        // every lane's scaled shifts are visible below
     XCoef XC;
     xline_setup(A, L, i, wlc, f, &XC);
     if (XC.IxHe > 0) f |= (XC.IxHe << 8);
@@ -78,7 +97,7 @@ __global__ void k_mag_center(AtmView A, LineView L, ZView Z, double Bsplit, cons
     double dW = (wlc - A.wave[iwl - 1]) / (A.wave[iwl] - A.wave[iwl - 1]);
     // non-magnetic centre opacity (synth.f90:1215-1224)
     double mx = -1.0e308;
-    for (int t = 0; t < nt; t++) {
+    for (int t = lane; t < nt; t += 32) {
         double cop, vv, av;
         xline_depth(A, t, XC, &cop, &vv, &av);
         double dWl = 0.0;
@@ -87,6 +106,7 @@ __global__ void k_mag_center(AtmView A, LineView L, ZView Z, double Bsplit, cons
         if (A.motype == 1) lo = lo / A.contstd[t];
         mx = fmax(mx, lo / cont_center(A, iwl, dW, t));
     }
+    mx = warp_max(mx);
     int il = 1, ir = A.nwl;
     if (mx < A.epsopac) f |= FSG_F_WEAK;
     else {
@@ -94,7 +114,7 @@ __global__ void k_mag_center(AtmView A, LineView L, ZView Z, double Bsplit, cons
         for (int idw = 0; idw < 64; idw++) {
             double dWo = (0.2 * ldexp(1.0, idw)) * (wlc + A.wfirst) / 5e3;
             double Wl = wlc + SplMax + dWo;
-            double m2 = mag_lineop2_max(A, XC, Wl, wlc, ihe, Z, i, iwl, dW, vtab, anode, aida);
+            double m2 = mag_lineop2_max_warp(A, XC, Wl, wlc, ihe, Z, i, iwl, dW, vtab, anode, aida, lane);
             if (m2 < A.epsopac) {
                 // RefineIdx (opacity.f90:611-675), magnetic branch
                 int isw, ikw;
@@ -109,7 +129,8 @@ __global__ void k_mag_center(AtmView A, LineView L, ZView Z, double Bsplit, cons
                 ib = waveidx(A, wlc + (double)isw * (SplMax + dWo)) + ikw;
                 for (int it = 0; it < 64 && abs(ia - ib) > 1; it++) {
                     int im = (ia + ib) / 2;
-                    double m3 = mag_lineop2_max(A, XC, A.wave[im - 1], wlc, ihe, Z, i, iwl, dW, vtab, anode, aida);
+                    double m3 = mag_lineop2_max_warp(A, XC, A.wave[im - 1], wlc, ihe, Z, i, iwl, dW, vtab, anode,
+                                                     aida, lane);
                     if (m3 < A.epsopac) ib = im; else ia = im;
                 }
                 if (isw == 1) { ir = ia; il = waveidx(A, 2.0 * wlc - A.wave[ia - 1]); }
@@ -118,9 +139,10 @@ __global__ void k_mag_center(AtmView A, LineView L, ZView Z, double Bsplit, cons
             } else if (wlc - SplMax - dWo < A.wave[0] && wlc + SplMax + dWo > A.wave[A.nwl - 1]) break;
         }
     }
-    flags[i] = f; ileft[i] = il; iright[i] = ir;
-    unsigned m = __ballot_sync(__activemask(), !(f & FSG_F_WEAK));
-    if ((threadIdx.x & 31) == (__ffs(__activemask()) - 1) && m) atomicAdd(nkeep, (unsigned long long)__popc(m));
+    if (lane == 0) {
+        flags[i] = f; ileft[i] = il; iright[i] = ir;
+        if (!(f & FSG_F_WEAK)) atomicAdd(nkeep, 1ull);
+    }
 }
 
 // six profiles of one line at one wavelength for depth t (MagLineOpacity1/3 inner loops)
@@ -569,7 +591,7 @@ void fsg_launch_mag_center(cudaStream_t s, const AtmView &A, const LineView &L, 
                            const VoigtTables &T, int32_t *flags, int32_t *ileft, int32_t *iright,
                            unsigned long long *nkeep) {
     if (L.n > 0)
-        k_mag_center<<<(unsigned)((L.n + 63) / 64), 64, 0, s>>>(A, L, Z, Bsplit, T.vtab, T.anode, T.aida, flags, ileft,
+        k_mag_center<<<(unsigned)((L.n + 3) / 4), 128, 0, s>>>(A, L, Z, Bsplit, T.vtab, T.anode, T.aida, flags, ileft,
                                                                 iright, nkeep);
 }
 
