@@ -183,3 +183,67 @@ def test_zh5_list_against_reference_pin(fsg, tmp_path, prec):
     for q in range(4):
         assert np.max(np.abs(spz[i0:i1 + 1, q] - d["spz"][:, q]) / d["spc"]) < tol
     assert np.max(np.abs(sfl[i0:i1 + 1] / d["sfl"] - 1)) < tol
+
+
+def _state_on_depths(name, nt_new):
+    """The atmosphere state interpolated to nt_new depths (log Rhox uniform between its ends; every
+    quantity log-linear in Rhox), with its continuum knots likewise: a synthetic state at the library's
+    depth limit for the maximum-size tests."""
+    st, meta = H.load_atm(name)
+    x = np.log(st["rhox"])
+    xn = np.linspace(x[0], x[-1], nt_new)
+    out = {"rhox": np.exp(xn)}
+    for k in ("T", "xne", "xna", "rho"):
+        out[k] = np.exp(np.interp(xn, x, np.log(st[k])))
+    for k in ("frac_h1", "frac_he1"):
+        out[k] = np.exp(np.interp(xn, x, np.log(np.maximum(st[k].astype(np.float64), 1e-300)))).astype(np.float32)
+    out["frac_h2"] = np.zeros(nt_new, np.float32)
+    f = st["fractionpf"].astype(np.float64)
+    out["fractionpf"] = np.stack([np.exp(np.interp(xn, x, np.log(f[:, s]))) for s in range(f.shape[1])],
+                                 axis=1).astype(np.float32)
+    for k in ("xamass", "potion", "ion"):
+        out[k] = st[k]
+    lk = np.log(meta["cont_opac"])
+    meta = dict(meta)
+    meta["cont_opac"] = np.exp(np.stack([np.interp(xn, x, lk[j]) for j in range(lk.shape[0])], axis=0))
+    return out, meta
+
+
+def test_max_sizes_stokes_vs_oracle(fsg, oracle_mod):
+    """At the library's limits (128 depths, 16 angles): MagLineopCalc + the Stokes solver (frame 0) and
+    the scalar RadTranCalc against the oracle, FP64."""
+    import fastspec_b200 as F
+    from fastspec_b200 import workloads as W
+    st, meta = _state_on_depths("magnetic", 128)
+    w0, span = 6040.0, 1.5
+    grid = dict(wmode=0, wstart=w0, wend=w0 + span, dstep=0.002)
+    co = H.contopac_on(meta, F.make_grid(0, w0, w0 + span, 0.002) + w0)
+    L = W.zeeman_lines(25, w0 + 0.2, w0 + span - 0.2, W.SEED0 + 77)
+    import sys, os
+    sys.path.insert(0, os.path.join(H.REPO, "fastspec_b200", "data"))
+    from make_atmospheres import mirrored_components
+    jlo, jup, glo, gup = L.zeeman
+    pats = []
+    for i in range(L.n):
+        p = oracle_mod.zeeman_pattern(jlo[i], jup[i], glo[i], gup[i])
+        pats.append(p if len(p[0]) and len(p[2]) else oracle_mod.zeeman_pattern(1.0, 0.0, 1.0, 1.0))
+    z = mirrored_components(pats)
+    lines = L.arrays()
+    bframe, bfield = 0, np.array([1200.0, -700.0, 500.0])
+    C, x, w = mag_ctx(fsg, grid, st, co, nmu=16)
+    g = C.mag_lineop_calc(fsg.LineList.from_arrays(lines, zeeman=z), bframe, bfield)
+    spz, spc, sfl, sfc = C.mag_radtran(bframe, bfield)
+    S = oracle_mod.State(grid, st, contopac=co, vmicro=1.0)
+    r = oracle_mod.mag_lineop_calc(S, oracle_mod.Lines(**lines, kind=2, zeeman=z), bframe, bfield)
+    assert np.array_equal(g["ileft"], r["ileft"]) and np.array_equal(g["iright"], r["iright"])
+    ospz, ospc = oracle_mod.mag_radtran(S, x, bframe, bfield, np.zeros((S.nwl, S.ntau)), r["maglineopac"])
+    assert spz.shape == (S.nwl, 4, 16)
+    assert np.max(np.abs(spz[:, 0] / ospz[:, 0] - 1)) < 1e-9
+    for q in (1, 2, 3):
+        assert np.max(np.abs(spz[:, q] - ospz[:, q]) / ospc) < 1e-9
+    # the scalar solver on the same state with a non-magnetic list
+    C.lineop_calc(fsg.LineList.from_arrays(lines))
+    spl, spc2, sfl2, sfc2 = C.radtran()
+    r2 = oracle_mod.lineop_calc(S, oracle_mod.Lines(**lines, kind=2), list_type=2)
+    ospl, ospc2 = oracle_mod.radtran(S, x, r2["lineopac"])
+    assert np.max(np.abs(spl / ospl - 1)) < 1e-9 and np.max(np.abs(spc2 / ospc2 - 1)) < 1e-9
