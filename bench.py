@@ -14,9 +14,10 @@ summed over retained lines), plus spectra/s.  `value` times the mixed-precision 
 line list resident in HBM; `e2e` times the public C-ABI call with host (pinned) buffers, the
 host->device copy of the line list and the device->host read of the flux inside each step.
 
---impl reference: the reference's CPU implementation of the path timed on this host.  The
-reference is Fortran with no compiler here, so this is the FP64 C restatement (oracle/) with
-OpenMP on all host threads, on a bounded wavelength sample of the same workload.
+--impl reference: the reference's CPU implementation of the path timed on this host: its own
+OpenMP executable (copied unmodified to baseline/_ref by the build; there is no Fortran compiler to
+build it) on all host threads, on a bounded wavelength sample of the same workload, or, without the
+executable, the FP64 C restatement (oracle/) with OpenMP.
 """
 import argparse
 import json
@@ -183,7 +184,8 @@ def batched_grid(F, torch, dev, natm, nlines, steps, warmup):
     """The batched configuration: natm atmospheres (depths 48-80, Teff 3800-7500 K, spans 20-200 A at
     R = 5e5) sharing one atomic list of nlines over 3000-9000 A, synthesised by one CUDA-graph
     replay of fsg_batch_run (persistent work-queue kernels, tiles from the autotuner); compared with
-    the same atmospheres synthesised one context at a time through fsg_lineop_calc_dev."""
+    the same atmospheres synthesised one context at a time through fsg_lineop_calc_dev, and with the
+    plain FP64 path on a sample of eight of them."""
     from fastspec_b200 import workloads as W
     members = W.batch_grid(natm)
     lines = W.atomic_lines(int(nlines), 3000.0, 9000.0, W.SEED0 + 3, exact=False)
@@ -192,12 +194,13 @@ def batched_grid(F, torch, dev, natm, nlines, steps, warmup):
     arr = {k: np.ascontiguousarray(v[order]) for k, v in arr.items()}
     LL = F.LineList.from_arrays(arr)
     x, w, _ = F.mu_quadrature(1, NMU)
-    ctxs = []
+    ctxs, conts = [], []
     for m in members:
         g = m["grid"]
         wave = F.make_grid(1, g["wstart"], g["wend"], g["dstep"]) + g["wstart"]
         lk = np.log(m["cont"]["cont_opac"])
         co = np.exp(np.stack([np.interp(wave, m["cont"]["cont_wave"], lk[:, t]) for t in range(m["ntau"])], axis=1))
+        conts.append(co)
         C = F.Context(device=dev, vmicro=1.0)
         C.set_grid(1, g["wstart"], g["wend"], g["dstep"])
         C.set_atmosphere(m["state"])
@@ -230,6 +233,23 @@ def batched_grid(F, torch, dev, natm, nlines, steps, warmup):
         C.lineop_reset()
         r = C.lineop_calc(sub, want_lineopac=False, want_lines=False)
         t_seq += r["stats"]["ms_total"]
+    # the plain FP64 path on every natm/8-th atmosphere, one context at a time (line opacity only: the
+    # solver is left out of its time, which favours the FP64 side of the ratio)
+    samp = list(range(0, natm, max(1, natm // 8)))
+    t64 = 0.0
+    for k in samp:
+        m, g = members[k], members[k]["grid"]
+        C64 = F.Context(device=dev, precision=F.PREC_FP64, vmicro=1.0)
+        C64.set_grid(1, g["wstart"], g["wend"], g["dstep"])
+        C64.set_atmosphere(m["state"])
+        C64.set_contopac(conts[k])
+        C64.set_mu(x, w)
+        a0, a1 = np.searchsorted(wl, g["wstart"] - 10.0), np.searchsorted(wl, g["wend"] + 10.0, side="right")
+        sub = F.LineList.from_arrays({kk: np.ascontiguousarray(v[a0:a1]) for kk, v in arr.items()})
+        r = C64.lineop_calc(sub, want_lineopac=False, want_lines=False)
+        t64 += r["stats"]["ms_total"]
+        C64.close()
+    fp64_sps = len(samp) / (t64 / 1e3)
     nwl_tot = sum(c.nwl for c in ctxs)
     out = {"config": "%d atmospheres (48-80 depths, Teff 3800-7500 K, spans 20-200 A at R=5e5, %d wavelengths in all), "
                      "%d shared atomic lines 3000-9000 A, 7 mu" % (natm, nwl_tot, int(nlines)),
@@ -237,6 +257,9 @@ def batched_grid(F, torch, dev, natm, nlines, steps, warmup):
            "ms_per_batch": ms, "line_evals": st["line_evals"], "candidate_lines": st["nlines_candidate"],
            "tuning": tuning, "tuning_s": tune_s, "graph": True,
            "sequential_line_ms": t_seq,
+           "plain_fp64_sample": {"atmospheres": len(samp), "spectra_per_s": fp64_sps,
+                                 "ms_line_per_atmosphere": t64 / len(samp)},
+           "batched_over_plain_fp64": (natm / (ms / 1e3)) / fp64_sps,
            "note": "sequential_line_ms: the same line opacities one context at a time (fsg_lineop_calc, "
                    "device time of central pass + accumulation, no solver)"}
     B.close()
