@@ -73,7 +73,8 @@ class BatchStats(C.Structure):
 # every symbol the header declares (checked by the CPU test suite)
 EXPORTS = [
     "fsg_create", "fsg_destroy", "fsg_last_error", "fsg_version", "fsg_kernel_launches", "fsg_cuda_stream", "fsg_make_grid", "fsg_set_grid",
-    "fsg_set_atmosphere", "fsg_set_contopac", "fsg_set_contopac_dev", "fsg_set_hestark",
+    "fsg_set_atmosphere", "fsg_set_contopac", "fsg_set_contopac_dev", "fsg_set_hestark", "fsg_hestark_tables",
+    "fsg_he_match_idx",
     "fsg_lineop_calc", "fsg_lineop_calc_dev", "fsg_lineop_reset", "fsg_lineop_get", "fsg_lineop_set",
     "fsg_lineop_device_ptr", "fsg_set_mu", "fsg_radtran", "fsg_radtran_dev", "fsg_mag_lineop_calc",
     "fsg_mag_lineop_reset", "fsg_mag_radtran", "fsg_hvoigt", "fsg_fvoigt", "fsg_voigt_tables",
@@ -116,6 +117,8 @@ def lib():
     L.fsg_set_contopac.argtypes = [C.c_void_p, _dp, _dp, C.c_int]
     L.fsg_set_contopac_dev.argtypes = [C.c_void_p, C.c_void_p]
     L.fsg_set_hestark.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.c_int]
+    L.fsg_hestark_tables.argtypes = [C.c_int, _dp, _dp, _fp, _fp, _dp, _dp]
+    L.fsg_he_match_idx.argtypes = [C.c_long, _dp, _fp, _ip, C.c_int, C.c_double, _ip]
     L.fsg_lineop_calc.argtypes = [C.c_void_p, C.POINTER(CLines), _dp, _ip, _ip, _ip, _fp, C.POINTER(Stats)]
     L.fsg_lineop_calc_dev.argtypes = [C.c_void_p, C.POINTER(CLines), C.POINTER(Stats)]
     L.fsg_lineop_reset.argtypes = [C.c_void_p]
@@ -206,6 +209,36 @@ def zeeman_pattern(jlo, jup, glo, gup):
     return spi[:npi.value], rpi[:npi.value], ssi[:nsi.value], rsi[:nsi.value]
 
 
+HE_NTAB = 37
+
+
+def hestark_tables(T, xne, frac_hii, frac_heii):
+    """HeStarkInit (hestark.f90:332-370) through fsg_hestark_tables: (HeGam [rad/s], HeShf [A]) of the
+    37 tabulated He I lines, each [37][ntau], from T, Xne and the FP32 H II and He II densities."""
+    T = _f64(T); xne = _f64(xne); hii = _f32(frac_hii); heii = _f32(frac_heii)
+    nt = len(T)
+    if not (len(xne) == len(hii) == len(heii) == nt):
+        raise FsgError("hestark_tables: T, xne, frac_hii and frac_heii differ in length")
+    g = np.zeros((HE_NTAB, nt)); h = np.zeros((HE_NTAB, nt))
+    rc = lib().fsg_hestark_tables(nt, _p(T, C.c_double), _p(xne, C.c_double), _p(hii, C.c_float),
+                                  _p(heii, C.c_float), _p(g, C.c_double), _p(h, C.c_double))
+    if rc != 0:
+        raise FsgError("fsg_hestark_tables failed (%d): empty atmosphere or T <= 0" % rc)
+    return g, h
+
+
+def he_match_idx(wl, elo, spc, spc_he1, wfirst=0.0):
+    """HeMatchIdx (hestark.f90:376-389) at XlineSetup (opacity.f90:176) through fsg_he_match_idx: the
+    table entry 1..37 of each line of species spc_he1 (0: none), the ihe column of a LineList."""
+    wl = _f64(wl); elo = _f32(elo); spc = _i32(spc)
+    out = np.zeros(max(len(wl), 1), np.int32)
+    rc = lib().fsg_he_match_idx(len(wl), _p(wl, C.c_double), _p(elo, C.c_float), _p(spc, C.c_int32),
+                                int(spc_he1), float(wfirst), _p(out, C.c_int32))
+    if rc != 0:
+        raise FsgError("fsg_he_match_idx failed (%d)" % rc)
+    return out[:len(wl)]
+
+
 class LineList:
     """Host SoA line list in the reference's stored precision (wl FP64, the rest FP32).
 
@@ -239,6 +272,19 @@ class LineList:
             s.pi_off = _p(k["pi_off"], C.c_int64); s.si_off = _p(k["si_off"], C.c_int64)
         self.c = s
         self.n = n
+
+    def _with_he_match(self, spc_he1, wfirst):
+        """The list with its ihe column from he_match_idx when it has none (XlineSetup's table match)."""
+        if self.c.ihe:
+            return self
+        k = self._keep
+        ihe = he_match_idx(k["wl"], k["elo"], k["spc"], spc_he1, wfirst)
+        out = LineList.__new__(LineList)
+        out._keep = dict(k, ihe=ihe)
+        out.c = CLines.from_buffer_copy(self.c)
+        out.c.ihe = _p(ihe, C.c_int32)
+        out.n = self.n
+        return out
 
     @classmethod
     def from_arrays(cls, a, kind=2, zeeman=None):
@@ -309,7 +355,7 @@ class Context:
             _p(x["xamass"], C.c_float), _p(x["potion"], C.c_float), _p(x["ion"], C.c_int32),
             _p(x["h1"], C.c_float), _p(x["he1"], C.c_float), _p(x["h2"], C.c_float)), "fsg_set_atmosphere")
         self.ntau = ntau
-        self.rhox = a["rhox"]; self.T = a["T"]
+        self.rhox = a["rhox"]; self.T = a["T"]; self.xne = a["xne"]
 
     def set_contopac(self, contopac, contopac_std=None, motype=0):
         co = _f64(contopac)
@@ -347,6 +393,7 @@ class Context:
         ir = np.zeros(max(n, 1), np.int32) if want_lines else None
         ls = np.zeros(max(n, 1), np.float32) if want_linstr else None
         st = Stats()
+        lines = self._he(lines)
         self._ck(self._lib.fsg_lineop_calc(self.h, C.byref(lines.c), _p(lo, C.c_double), _p(fl, C.c_int32),
                                            _p(il, C.c_int32), _p(ir, C.c_int32), _p(ls, C.c_float), C.byref(st)),
                  "fsg_lineop_calc")
@@ -399,10 +446,25 @@ class Context:
         self._ck(self._lib.fsg_set_fractionpf(self.h, _p(fpf, C.c_float)), "fsg_set_fractionpf")
 
     def set_hestark(self, hegam, heshf, spc_he1):
-        """He I Stark broadening and shift tables [nhe][ntau] (hestark.f90) and the He I species index."""
+        """He I Stark broadening and shift tables [nhe][ntau] (hestark.f90) and the He I species index;
+        the lists' ihe columns pick the entries."""
         g = _f64(hegam); h = _f64(heshf)
         self._ck(self._lib.fsg_set_hestark(self.h, g.shape[0], _p(g, C.c_double), _p(h, C.c_double), int(spc_he1)),
                  "fsg_set_hestark")
+        self._he_spc = None
+
+    def hestark_init(self, frac_hii, frac_heii, spc_he1):
+        """HeStarkInit for the current atmosphere (as XlineInit runs it, opacity.f90:91): the 37 tabulated
+        He I lines' widths and shifts from its T, Xne and the FP32 H II and He II densities, uploaded with
+        fsg_set_hestark; from then on lists without an ihe column are matched to the table as XlineSetup
+        does (opacity.f90:176).  Call again after set_atmosphere."""
+        g, h = hestark_tables(self.T, self.xne, frac_hii, frac_heii)
+        self.set_hestark(g, h, spc_he1)
+        self._he_spc = int(spc_he1)
+
+    def _he(self, lines):
+        spc = getattr(self, "_he_spc", None)
+        return lines if spc is None else lines._with_he_match(spc, self.wfirst)
 
     def set_vmicro(self, vmicro):
         self._ck(self._lib.fsg_set_vmicro(self.h, C.c_double(float(vmicro))), "fsg_set_vmicro")
@@ -441,6 +503,7 @@ class Context:
         fl = np.zeros(max(n, 1), np.int32); il = np.zeros(max(n, 1), np.int32); ir = np.zeros(max(n, 1), np.int32)
         ls = np.zeros(max(n, 1), np.float32) if want_linstr else None
         st = Stats()
+        lines = self._he(lines)
         self._ck(self._lib.fsg_mag_lineop_calc(self.h, C.byref(lines.c), int(bframe), _p(bf, C.c_double), len(bf),
                                                _p(mlo, C.c_double), _p(fl, C.c_int32), _p(il, C.c_int32),
                                                _p(ir, C.c_int32), _p(ls, C.c_float), C.byref(st)),

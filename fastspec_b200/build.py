@@ -23,6 +23,7 @@ UNITS = [
     ("fsg_adjoint.cu", ["-fmad=false"]),
     ("fsg_magfast.cu", ["-fmad=true"]),
     ("fsg_adjoint_line.cu", ["-fmad=true"]),
+    ("fsg_hestark.cpp", ["-Xcompiler", "-ffp-contract=off"]),
 ]
 
 
@@ -49,7 +50,7 @@ def build(force=False, verbose=False, ptxas_v=False):
         src = os.path.join(CSRC, f)
         if not os.path.exists(src):
             continue
-        obj = os.path.join(objdir, f.replace(".cu", ".o"))
+        obj = os.path.join(objdir, os.path.splitext(f)[0] + ".o")
         cmd = [NVCC] + COMMON + flags + (["-Xptxas", "-v"] if ptxas_v else []) + ["-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))

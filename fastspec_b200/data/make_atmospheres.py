@@ -773,8 +773,170 @@ def make_mol_h5_pin(gold):
     print(log[-600:])
 
 
+# ---- hot atmosphere with tabulated He I Stark lines (hestark.f90) -------------------------------
+HOT = dict(teff=15000.0, logg=4.0, ntau=48, species=[("He", 1)], wl0=5000.0, dstep=0.01, vmic=1.0, molbrd=0)
+HE_POTION = 24.5874
+
+
+def he_lines(wl, elo, loggf, lgrad=None, lgqst=None, lgvdw=None):
+    n = len(wl)
+    full = lambda v, d: np.full(n, d) if v is None else np.asarray(v, np.float64)
+    return W.LineList(HOT["species"], np.asarray(wl, np.float64), np.asarray(loggf, np.float64),
+                      np.asarray(elo, np.float64), full(lgrad, 5.0), full(lgqst, -30.0), full(lgvdw, -30.0),
+                      np.zeros(n, np.int32), np.zeros(n, np.int32))
+
+
+def he_run(model, probes, lines, grid, wd, save_spec=False):
+    """Reference run of probes + lines on grid (w0, w1, dstep): (line opacity, continuum[, spec, flux])."""
+    merged = merge([probes, lines])
+    W.write_krz(os.path.join(wd, "model.krz"), model)
+    merged.write_z(os.path.join(wd, "lines.z"), grid[0], grid[1])
+    deck = ("wave=%.4f, %.4f, %.6f, 0\nsave=0, 1, 1, %d, %d\nvmic=%.3f\nmolbrd=%d\n"
+            "lines=\n-1  lines.z\n\nmodel=model.krz\nmus=%d\n"
+            % (grid[0], grid[1], grid[2], int(save_spec), int(save_spec), HOT["vmic"], HOT["molbrd"],
+               7 if save_spec else 0))
+    log = run_ref(wd, deck)
+    out = [fsio.read_opac(os.path.join(wd, "fs_lineop.bin")), fsio.read_opac(os.path.join(wd, "fs_contop.bin"))]
+    if save_spec:
+        out += [fsio.read_spec(os.path.join(wd, "fs_spec.bin")), fsio.read_flux(os.path.join(wd, "fs_flux.bin"))]
+    return out + [log]
+
+
+def f32_from_bits(b):
+    return np.asarray(b, np.int32).view(np.float32)
+
+
+def recover_he_density(state, co, grid, line, lo_ref, known, target, d_range=(5.0, 12.0)):
+    """One FP32 density per depth (H II or He II: `target`) from a single tabulated He I line's reference
+    line opacity.  The feature is the line opacity summed over the wing pixels 5-12 A either side of the
+    centre, which grows monotonically with the damping parameter while it stays below the pixels' v
+    (H ~ a / (sqrt(pi) (a^2 + v^2))), hence with the density between 0 and twice the electron density
+    (each proton or He II ion has given an electron); bisection runs on the bit patterns of positive
+    FP32 numbers, all depths at once, and ends on the FP32 value of least mismatch among the final
+    neighbours."""
+    g = dict(wmode=0, wstart=grid[0], wend=grid[1], dstep=grid[2])
+    nt = len(state["T"])
+    wave = lo_ref["wave"]
+    dl = np.abs(wave - line.wl[0])
+    px = np.nonzero((dl >= d_range[0]) & (dl <= d_range[1]))[0]
+    assert np.all(lo_ref["opac"][px] > 0), "feature pixels outside the reference window"
+    s_ref = lo_ref["opac"][px].sum(axis=0)
+    L = oracle.Lines(**lines_args(line), kind=2)
+
+    def feature(x32):
+        dens = dict(known)
+        dens[target] = x32
+        hg, hs = oracle.hestark_init(state["T"], state["xne"], dens["hii"], dens["heii"])
+        st = oracle.State(g, state, contopac=co, vmicro=HOT["vmic"], molbrd=HOT["molbrd"], hegam=hg,
+                          heshf=hs, spc_he1=0)
+        r = oracle.lineop_calc(st, L, list_type=2)
+        return r["lineopac"][px].sum(axis=0)
+
+    lo_b = np.zeros(nt, np.int64)
+    hi_b = (2.0 * state["xne"]).astype(np.float32).view(np.int32).astype(np.int64)
+    while np.any(hi_b - lo_b > 1):
+        mid = (lo_b + hi_b) // 2
+        up = feature(f32_from_bits(mid)) >= s_ref
+        hi_b = np.where(up, mid, hi_b)
+        lo_b = np.where(up, lo_b, mid)
+    best = None
+    for cand in (hi_b - 1, hi_b, hi_b + 1):
+        dev = np.abs(feature(f32_from_bits(cand)) / s_ref - 1.0)
+        if best is None:
+            best = (dev, cand.copy())
+        else:
+            take = dev < best[0]
+            best = (np.where(take, dev, best[0]), np.where(take, cand, best[1]))
+    return f32_from_bits(best[1]), best[0]
+
+
+def make_hot_he(gold):
+    """Hot atmosphere (Teff 15000 K, log g 4.0, 48 depths, He I only) and the He I Stark pin.
+
+    State: recover() with He I probes at 5000 A (FractionPF, masses, Nprtb).  The proton and He II
+    densities that HeStarkInit (hestark.f90:332-370) reads are EOS outputs the program does not write;
+    they are recovered from two single-line runs: the DS84 line at 3819.60 A (electrons + protons, no
+    He II term) gives Fraction(H II), then the DS90 line at 4471.5 A gives Fraction(He II).
+    Pin (pin_hot_he.npz): tabulated lines of both tables (3867.5, 3871.79, 3888.7, 3926.53, 3935.9 A),
+    near misses in wavelength (> 1 A) and in lower level energy (> 0.01 eV), two lines matching one entry,
+    and seeded non-tabulated He I lines, on 3855-3945 A; the whole grid's line and continuum opacity and
+    the spectra."""
+    model = W.eddington_model(HOT["teff"], HOT["logg"], HOT["ntau"])
+    species = HOT["species"]
+    POTION[("He", 1)] = HE_POTION
+    with tempfile.TemporaryDirectory() as wd:
+        r = recover(model, species, 0, HOT["wl0"], HOT["dstep"], HOT["vmic"], HOT["molbrd"], wd)
+    state, atm = r["state"], r["atm"]
+    pgf = r["probe_loggf"]
+    probes = probe_list(species, HOT["wl0"], 2.0, ismol=0, loggf=pgf)
+    nt = len(state["T"])
+    known = dict(hii=np.zeros(nt, np.float32), heii=np.zeros(nt, np.float32))
+    for target, wl, elo, grid in (("hii", 3819.60, 20.96409, (3805.0, 3835.0, 0.01)),
+                                  ("heii", 4471.5, 20.96409, (4455.0, 4488.0, 0.01))):
+        grid = (wl - 14.0, wl + 14.0, 0.01)
+        line = he_lines([wl], [elo], [0.5])
+        with tempfile.TemporaryDirectory() as wd:
+            lo, co, _ = he_run(model, probes, line, grid, wd)
+        for k in ("rhox", "T", "xne", "xna", "rho"):
+            assert np.array_equal(lo[k], state[k]), "EOS state differs: " + k
+        x, dev = recover_he_density(state, co["opac"], grid, line, lo, known, target)
+        known[target] = x
+        print("  %s: %s .. %s, feature mismatch max %.2e (median %.2e)"
+              % (target, x[0], x[-1], dev.max(), np.median(dev)))
+    # pin run
+    tab = [(3867.5, 20.96409), (3871.79, 21.21802), (3888.7, 19.81961), (3926.53, 21.21802), (3935.9, 21.21802)]
+    near = [(3890.0, 19.81961),     # 1.3 A from 3888.7: no entry
+            (3868.2, 19.81961),     # within 1 A of 3867.5, lower level 1.14 eV off: no entry
+            (3926.0, 21.2160),      # second line on entry 35 (0.53 A, 0.002 eV off)
+            (3889.65, 19.8196),     # 0.95 A from 3888.7: entry 10
+            (3936.95, 21.2180)]     # 1.05 A from 3935.9: no entry
+    rng = np.random.default_rng(W.SEED0 + 40)
+    nr = 30
+    wl = [w for w, _ in tab + near] + list(np.round(rng.uniform(3857.0, 3943.0, nr), 3))
+    elo = [e for _, e in tab + near] + list(np.round(rng.uniform(19.5, 23.0, nr), 4))
+    loggf = [-0.3, -0.8, 0.2, -1.0, -0.6, -0.5, -0.4, -0.9, -0.7, -0.5] + list(np.round(rng.normal(-1.5, 0.6, nr), 3))
+    lgqst = [-30.0] * 10 + list(np.round(rng.uniform(-6.0, -4.5, nr), 3))
+    lgvdw = [-30.0] * 10 + list(np.round(rng.uniform(-8.0, -7.0, nr), 3))
+    lgrad = [8.5] * 10 + list(np.round(rng.uniform(7.0, 9.0, nr), 3))
+    pin = he_lines(wl, elo, loggf, lgrad, lgqst, lgvdw)
+    grid = (3855.0, 3945.0, 0.05)
+    with tempfile.TemporaryDirectory() as wd:
+        lo, co, sp, fl, log = he_run(model, probes, pin, grid, wd, save_spec=True)
+    for k in ("rhox", "T", "xne", "xna", "rho"):
+        assert np.array_equal(lo[k], state[k]), "EOS state differs: " + k
+    g = dict(wmode=0, wstart=grid[0], wend=grid[1], dstep=grid[2])
+    hg, hs = oracle.hestark_init(state["T"], state["xne"], known["hii"], known["heii"])
+    st = oracle.State(g, state, contopac=co["opac"], vmicro=HOT["vmic"], molbrd=HOT["molbrd"], hegam=hg,
+                      heshf=hs, spc_he1=0)
+    res = oracle.lineop_calc(st, oracle.Lines(**lines_args(pin), kind=2), list_type=2)
+    ref = lo["opac"]
+    assert np.array_equal(res["lineopac"] > 0, ref > 0), "window pattern differs"
+    m = ref > 0
+    rel = np.max(np.abs(res["lineopac"][m] / ref[m] - 1.0))
+    ihe = np.array([oracle.he_match_idx(w, e) for w, e in zip(pin.wl, pin.elo)], np.int32)
+    print("  pin: %d lines (%d matched), line opacity max rel %.2e" % (pin.n, int((ihe > 0).sum()), rel))
+    kidx = np.unique(np.linspace(0, len(co["wave"]) - 1, 61).round().astype(int))
+    np.savez_compressed(
+        os.path.join(HERE, "atm_hot.npz"), teff=HOT["teff"], logg=HOT["logg"],
+        species=np.array(["%s %d" % s for s in species]), ismol=0, vmicro=HOT["vmic"], molbrd=HOT["molbrd"],
+        rhox=state["rhox"], T=state["T"], xne=state["xne"], xna=state["xna"], rho=state["rho"],
+        fractionpf=state["fractionpf"], xamass=state["xamass"], potion=state["potion"], ion=state["ion"],
+        frac_h1=state["frac_h1"], frac_he1=state["frac_he1"], frac_hii=known["hii"], frac_heii=known["heii"],
+        nprtb=r["nprtb"], cont_wave=co["wave"][kidx], cont_opac=co["opac"][kidx], probe_rel=r["rel"],
+        probe_loggf=pgf, model_rhox=model["rhox"], model_T=model["T"])
+    a = pin.arrays()
+    np.savez_compressed(
+        os.path.join(gold, "pin_hot_he.npz"), grid=np.array(grid + (0,), np.float64), i0=0, i1=len(lo["wave"]) - 1,
+        atm="hot", vmicro=HOT["vmic"], molbrd=HOT["molbrd"], contopac=co["opac"], lineopac=ref,
+        wave=lo["wave"], xmu=sp["xmu"], spl=sp["spl"], spc=sp["spc"], sfl=fl["sfl"], sfc=fl["sfc"],
+        ihe_expected=ihe, **{"line_" + k: v for k, v in a.items()})
+    print(log[-400:])
+
+
 if __name__ == "__main__":
-    if len(sys.argv) > 1 and sys.argv[1] == "molh5":
+    if len(sys.argv) > 1 and sys.argv[1] == "hot":
+        make_hot_he(os.path.join(REPO, "tests", "golden"))
+    elif len(sys.argv) > 1 and sys.argv[1] == "molh5":
         make_mol_h5_pin(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "zh5":
         make_zh5_pin(os.path.join(REPO, "tests", "golden"))

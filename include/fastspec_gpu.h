@@ -123,8 +123,26 @@ int fsg_set_geometry(fsg_ctx *ctx, double radius, const double *height);
  * [ntau] (may be NULL when motype == 0) and the model type (Motype). */
 int fsg_set_contopac(fsg_ctx *ctx, const double *contopac, const double *contopac_std, int motype);
 int fsg_set_contopac_dev(fsg_ctx *ctx, const double *d_contopac);
-/* He I Stark widths/shifts HeGam/HeShf [nhe][ntau] (hestark.f90:332-370), optional. */
+/* He I Stark widths/shifts HeGam/HeShf [nhe][ntau] (hestark.f90:332-370), optional; spc_he1 is the
+ * 0-based index of He I among the species (IdxSpc(Ix%He1)).  Lines of that species take the Stark
+ * width and shift of table entry ihe (fsg_lines.ihe, 1..nhe; 0 or ihe == NULL: none). */
 int fsg_set_hestark(fsg_ctx *ctx, int nhe, const double *hegam, const double *heshf, int spc_he1);
+
+/* HeStarkInit (hestark.f90:332-370), on the host, no context: HeGam [rad/s] and HeShf [A] of the
+ * FSG_HE_NTAB tabulated He I lines (Dimitrijevic & Sahal-Brechot 1990 entries 1-32, 1984 entries
+ * 33-37), [FSG_HE_NTAB][ntau], from T [K], Xne and the FP32 number densities of protons (Fraction
+ * of H II) and He II ions, by three-point Lagrange interpolation in log10 T.  The tables go to
+ * fsg_set_hestark with nhe = FSG_HE_NTAB.  FSG_E_ARG for null pointers, ntau < 1 or T <= 0. */
+#define FSG_HE_NTAB 37
+int fsg_hestark_tables(int ntau, const double *T, const double *xne, const float *frac_hii,
+                       const float *frac_heii, double *hegam, double *heshf);
+/* HeMatchIdx (hestark.f90:376-389) at its XlineSetup call site (opacity.f90:176), on the host, no
+ * context: ihe[i] = the first table entry 1..FSG_HE_NTAB whose centre lies within 1 A of the line's
+ * WaveL = (wl[i] - wfirst) + wfirst and whose lower level energy lies within 0.01 eV of elo[i], for
+ * lines of species spc_he1; 0 otherwise.  wfirst is the grid's first wavelength (fsg_set_grid's
+ * wstart).  The result is the ihe column of fsg_lines. */
+int fsg_he_match_idx(long n, const double *wl, const float *elo, const int32_t *spc, int spc_he1,
+                     double wfirst, int32_t *ihe);
 
 /* ---- hot path ------------------------------------------------------------------------- */
 /* LineopCalc (synth.f90:747-1095): central pass (XlineSetup/XlineDepth, weak-line rejection,

@@ -97,6 +97,8 @@ def lib():
         L.or_disk_integ.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp]
         L.or_zeeman_pattern.argtypes = [C.c_float, C.c_float, C.c_float, C.c_float, _ip, _fp, _fp,
                                         _ip, _fp, _fp]
+        L.or_hestark_init.argtypes = [C.c_int, _dp, _dp, _fp, _fp, _dp, _dp]
+        L.or_he_match_idx.argtypes = [C.c_double, C.c_double]
         _lib = L
     return _lib
 
@@ -370,6 +372,25 @@ def sphere_init(rhox, height, radius, xmu):
     if rc == -2:
         raise ValueError("SphereInit: grazing ray tangent in the top model layer")
     return out
+
+
+HE_NTAB = 37
+
+
+def hestark_init(T, xne, frac_hii, frac_heii):
+    """HeStarkInit (hestark.f90:332-370): (HeGam [rad/s], HeShf [A]) of the 37 tabulated He I lines,
+    each [37][ntau], from T, Xne and the FP32 H II and He II densities (Fraction)."""
+    T = _f64(T); xne = _f64(xne); hii = _f32(frac_hii); heii = _f32(frac_heii)
+    nt = len(T)
+    g = np.zeros((HE_NTAB, nt)); h = np.zeros((HE_NTAB, nt))
+    lib().or_hestark_init(nt, _p(T, C.c_double), _p(xne, C.c_double), _p(hii, C.c_float), _p(heii, C.c_float),
+                          _p(g, C.c_double), _p(h, C.c_double))
+    return g, h
+
+
+def he_match_idx(wave_air, elo):
+    """HeMatchIdx (hestark.f90:376-389): table entry 1..37, or 0."""
+    return int(lib().or_he_match_idx(float(wave_air), float(elo)))
 
 
 def locprf_pp(xmu, xki, src, rhox):

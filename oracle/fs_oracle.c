@@ -320,6 +320,58 @@ double or_air2vac(double la) {
     return (la > 1999.352) ? la * N : la;
 }
 
+/* ---- tabulated He I Stark broadening (hestark.f90) --------------------------------------
+ * The published width/shift tables are data shared with the library (one header); the
+ * interpolation and assembly below are this file's own restatement. */
+#include "../fastspec_b200/csrc/fsg_hestark_tables.h"
+
+/* LagWt3 (hestark.f90:394-415): three-point Lagrange weights on knots t[0..n-1] at x; the
+ * returned j is the reference's 1-based knot index (value = w0 F(j) + w1 F(j-1) + w2 F(j-2)) */
+static int he_lagwt3(const double *t, int n, double x, double *w0, double *w1, double *w2) {
+    int j = n;
+    for (int it = 3; it <= n; it++)
+        if (t[it - 1] > x) { j = it; break; }
+    double tj = t[j - 1], tj1 = t[j - 2], tj2 = t[j - 3];
+    double Tj = (tj - tj1) * (tj - tj2) * (tj1 - tj2);
+    *w0 = (x - tj2) * (x - tj1) * (tj1 - tj2) / Tj;
+    *w1 = (x - tj2) * (tj - x) * (tj - tj2) / Tj;
+    *w2 = (x - tj1) * (x - tj) * (tj - tj1) / Tj;
+    return j;
+}
+
+/* HeStarkInit (hestark.f90:332-370); HeGamCnv = 1.884e3 (hestark.f90:39) */
+void or_hestark_init(int ntau, const double *T, const double *xne, const float *frac_hii,
+                     const float *frac_heii, double *hegam, double *heshf) {
+    for (int t = 0; t < ntau; t++) {
+        double Tlg = log10(T[t]), Xne = xne[t], Xnp = (double)frac_hii[t], Xnhe2 = (double)frac_heii[t];
+        for (int k = 0; k < FSG_HE_NTAB; k++) {
+            const fsg_he_line *e = &FSG_HE_TAB[k];
+            int ds90 = k < FSG_HE_NDS90;
+            double w0, w1, w2;
+            int j = he_lagwt3(ds90 ? FSG_HE_LOGT90 : FSG_HE_LOGT84, e->nknot, Tlg, &w0, &w1, &w2) - 1;
+#define LAG(a) (w0 * (a)[j] + w1 * (a)[j - 1] + w2 * (a)[j - 2])
+            double g, sh;
+            if (ds90) {
+                g = (LAG(e->w[0]) * Xne + LAG(e->w[1]) * Xnp + LAG(e->w[2]) * Xnhe2) * 1.884e3 / (e->wlc * e->wlc);
+                sh = (LAG(e->s[0]) * Xne + LAG(e->s[1]) * Xnp + LAG(e->s[2]) * Xnhe2) * 1e-16;
+            } else {
+                g = (LAG(e->w[0]) * Xne + LAG(e->w[1]) * Xnp) * 1.884e3 / (e->wlc * e->wlc);
+                sh = (LAG(e->s[0]) * Xne + LAG(e->s[1]) * Xnp) * 1e-16;
+            }
+#undef LAG
+            hegam[(size_t)k * ntau + t] = g > 0.0 ? g : 0.0;   /* MAX(Gam, 0d0) */
+            heshf[(size_t)k * ntau + t] = sh;
+        }
+    }
+}
+
+/* HeMatchIdx (hestark.f90:376-389): HeMatchTol 1 A, HeEloTol 0.01 eV (hestark.f90:31, 36) */
+int or_he_match_idx(double wave_air, double elo) {
+    for (int k = 0; k < FSG_HE_NTAB; k++)
+        if (fabs(wave_air - FSG_HE_TAB[k].wlc) <= 1.0 && fabs(elo - FSG_HE_TAB[k].elo) <= 0.01) return k + 1;
+    return 0;
+}
+
 /* XlineInit (opacity.f90:65-93) */
 void or_xline_init(or_state *s) {
     int nt = s->ntau;
@@ -380,7 +432,10 @@ static void xline_setup(const or_state *s, const or_lines *L, long i, double wlc
         double t1 = (double)(IonL * IonL) * Hie / (pot - Eup);
         double t2 = (double)(IonL * IonL) * Hie / (pot - Elo);
         double Enu4 = t1 * t1, Enl4 = t2 * t2;
-        if (L->ihe && ispc == s->spc_he1) XC->IxHe = L->ihe[i];
+        /* opacity.f90:176: a He I line matching a table entry (HeMatchIdx); an explicit entry
+         * list L->ihe overrides the match */
+        if (ispc == s->spc_he1)
+            XC->IxHe = L->ihe ? L->ihe[i] : (s->nhe == FSG_HE_NTAB ? or_he_match_idx(WaveL, Elo) : 0);
         if (XC->IxHe > 0) XC->MdQst = 3;
         else if (GqstL > 0.0) { XC->MdQst = 0; XC->Cqst = GqstL; }
         else if (IsMol) XC->MdQst = 9;

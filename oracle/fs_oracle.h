@@ -110,6 +110,13 @@ typedef struct {
     double wide_evals;
 } or_stats;
 
+/* HeStarkInit (hestark.f90:332-370): per-depth Stark widths [rad/s] and shifts [A] of the 37
+ * tabulated He I lines, [37][ntau], from T, Xne and the FP32 proton (H II) and He II densities. */
+void or_hestark_init(int ntau, const double *T, const double *xne, const float *frac_hii,
+                     const float *frac_heii, double *hegam, double *heshf);
+/* HeMatchIdx (hestark.f90:376-389): table entry 1..37 within 1 A and 0.01 eV, else 0 */
+int  or_he_match_idx(double wave_air, double elo);
+
 int  or_grid_init(or_state *s);          /* allocates s->wave; returns nwl or <0 */
 void or_xline_init(or_state *s);         /* allocates x_* */
 void or_state_free(or_state *s);

@@ -404,6 +404,33 @@ def test_he_stark_shifted_lines(fsg, oracle_mod, prec):
 
 
 @pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_hot_he_lines_against_reference_pin(fsg, prec):
+    """Tabulated He I Stark lines in a Teff 15000 K atmosphere (hestark.f90): Context.hestark_init builds
+    the 37 lines' widths and shifts on the host (fsg_hestark_tables) and the lists' table entries come
+    from fsg_he_match_idx; line opacity, windows and flux against the reference program's run
+    (tests/golden/pin_hot_he.npz).  FP64 1e-8; mixed within the mixed bars (the tabulated lines take
+    the FP64 per-depth-shift kernel, the others the FP32 passes)."""
+    from test_hestark import hot_state
+    d = H.load_pin("pin_hot_he")
+    grid, st, meta, co = H.pin_setup(d)
+    _, _, hii, heii = hot_state()
+    C = ctx_for(fsg, grid, st, co, fsg.PREC_MIXED if prec == "mixed" else fsg.PREC_FP64,
+                vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]))
+    C.hestark_init(hii, heii, 0)
+    g = C.lineop_calc(fsg.LineList.from_arrays(H.pin_lines(d)))
+    assert np.array_equal((g["flags"] >> 8) & 255, d["ihe_expected"])
+    lo, ref = g["lineopac"], d["lineopac"]
+    assert np.array_equal(lo > 0, ref > 0)
+    if prec == "fp64":
+        assert np.max(np.abs(lo[ref > 0] / ref[ref > 0] - 1)) < 1e-8
+    else:
+        assert np.max(np.abs(lo - ref) / (ref + d["contopac"])) < 2e-6
+    spl, spc, sfl, sfc = C.radtran()
+    assert np.max(np.abs(sfl / d["sfl"] - 1)) < (1e-8 if prec == "fp64" else 1e-5)
+    C.close()
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
 def test_hdf5_list_against_reference_pin(fsg, tmp_path, prec):
     """A line list in the reference's HDF5 layout, read by fsio.read_hdf5_lines as an atomic list
     (kind 0), through the GPU path: the reference program's line opacity and flux for the same file
