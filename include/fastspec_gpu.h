@@ -55,7 +55,7 @@ typedef struct {
 /* Line list, structure of arrays (LineData records, shared.f90:451-482).
  * kind: 0 LineTypeAtm (HDF atomic), 1 LineTypeMol (single-species molecular), 2 LineTypeMag
  * (ASCII .z / magnetic).  ismol: molecule flag of LineTypeMag records (IsMolecule).
- * ihe: He I Stark table entry (HeMatchIdx, 1-based) or 0; may be NULL.
+ * ihe: He I Stark table entry (HeMatchIdx, 1-based; fsg_he_match_idx fills it) or 0; may be NULL.
  * Zeeman components (magnetic lists only; NULL otherwise): line i owns npi[i] pi components at
  * spl_pi[pi_off[i] ...] / str_pi[...] and nsi[i] sigma components (blue half first, then red,
  * as ReadAscMag stores them, ioutils.f90:1393-1410).  Shifts are in the reader's units
