@@ -850,6 +850,27 @@ def recover_he_density(state, co, grid, line, lo_ref, known, target, d_range=(5.
     return f32_from_bits(best[1]), best[0]
 
 
+def he_pin_list():
+    """Tabulated lines of both tables (3867.5, 3871.79, 3888.7, 3926.53, 3935.9 A), near misses in
+    wavelength (> 1 A) and lower level energy (> 0.01 eV), two lines on one entry, and 30 seeded
+    He I lines (classical Stark and van der Waals constants given) on 3857-3943 A."""
+    tab = [(3867.5, 20.96409), (3871.79, 21.21802), (3888.7, 19.81961), (3926.53, 21.21802), (3935.9, 21.21802)]
+    near = [(3890.0, 19.81961),     # 1.3 A from 3888.7: no entry
+            (3868.2, 19.81961),     # within 1 A of 3867.5, lower level 1.14 eV off: no entry
+            (3926.0, 21.2160),      # second line on entry 35 (0.53 A, 0.002 eV off)
+            (3889.65, 19.8196),     # 0.95 A from 3888.7: entry 10
+            (3936.95, 21.2180)]     # 1.05 A from 3935.9: no entry
+    rng = np.random.default_rng(W.SEED0 + 40)
+    nr = 30
+    wl = [w for w, _ in tab + near] + list(np.round(rng.uniform(3857.0, 3943.0, nr), 3))
+    elo = [e for _, e in tab + near] + list(np.round(rng.uniform(19.5, 23.0, nr), 4))
+    loggf = [-0.3, -0.8, 0.2, -1.0, -0.6, -0.5, -0.4, -0.9, -0.7, -0.5] + list(np.round(rng.normal(-1.5, 0.6, nr), 3))
+    lgqst = [-30.0] * 10 + list(np.round(rng.uniform(-6.0, -4.5, nr), 3))
+    lgvdw = [-30.0] * 10 + list(np.round(rng.uniform(-8.0, -7.0, nr), 3))
+    lgrad = [8.5] * 10 + list(np.round(rng.uniform(7.0, 9.0, nr), 3))
+    return he_lines(wl, elo, loggf, lgrad, lgqst, lgvdw)
+
+
 def make_hot_he(gold):
     """Hot atmosphere (Teff 15000 K, log g 4.0, 48 depths, He I only) and the He I Stark pin.
 
@@ -884,21 +905,7 @@ def make_hot_he(gold):
         print("  %s: %s .. %s, feature mismatch max %.2e (median %.2e)"
               % (target, x[0], x[-1], dev.max(), np.median(dev)))
     # pin run
-    tab = [(3867.5, 20.96409), (3871.79, 21.21802), (3888.7, 19.81961), (3926.53, 21.21802), (3935.9, 21.21802)]
-    near = [(3890.0, 19.81961),     # 1.3 A from 3888.7: no entry
-            (3868.2, 19.81961),     # within 1 A of 3867.5, lower level 1.14 eV off: no entry
-            (3926.0, 21.2160),      # second line on entry 35 (0.53 A, 0.002 eV off)
-            (3889.65, 19.8196),     # 0.95 A from 3888.7: entry 10
-            (3936.95, 21.2180)]     # 1.05 A from 3935.9: no entry
-    rng = np.random.default_rng(W.SEED0 + 40)
-    nr = 30
-    wl = [w for w, _ in tab + near] + list(np.round(rng.uniform(3857.0, 3943.0, nr), 3))
-    elo = [e for _, e in tab + near] + list(np.round(rng.uniform(19.5, 23.0, nr), 4))
-    loggf = [-0.3, -0.8, 0.2, -1.0, -0.6, -0.5, -0.4, -0.9, -0.7, -0.5] + list(np.round(rng.normal(-1.5, 0.6, nr), 3))
-    lgqst = [-30.0] * 10 + list(np.round(rng.uniform(-6.0, -4.5, nr), 3))
-    lgvdw = [-30.0] * 10 + list(np.round(rng.uniform(-8.0, -7.0, nr), 3))
-    lgrad = [8.5] * 10 + list(np.round(rng.uniform(7.0, 9.0, nr), 3))
-    pin = he_lines(wl, elo, loggf, lgrad, lgqst, lgvdw)
+    pin = he_pin_list()
     grid = (3855.0, 3945.0, 0.05)
     with tempfile.TemporaryDirectory() as wd:
         lo, co, sp, fl, log = he_run(model, probes, pin, grid, wd, save_spec=True)
@@ -933,9 +940,68 @@ def make_hot_he(gold):
     print(log[-400:])
 
 
+def make_hot_he_mag(gold):
+    """Stokes IQUV of the pin_hot_he list as Zeeman lines (seeded J and Lande factors, explicit
+    patterns) in the hot atmosphere, BFRAME 1 with |B| = 3 kG at inclination 45 deg and azimuth 20 deg,
+    9 angles, on 3855-3945 A at 0.05 A (pin_hot_he_mag.npz).  Pins the tabulated He I widths and shifts
+    in the magnetic driver (MagLineOpacity1/2 with the per-depth shift, opacity.f90:391-520)."""
+    d = np.load(os.path.join(REPO, "tests", "golden", "pin_hot_he.npz"))
+    a = np.load(os.path.join(HERE, "atm_hot.npz"))
+    model = W.eddington_model(HOT["teff"], HOT["logg"], HOT["ntau"])
+    state = load_state("hot")
+    POTION[("He", 1)] = HE_POTION
+    # the list alone (He I is the only species, so the EOS inventory is the probe runs')
+    merged = he_pin_list()
+    rng = np.random.default_rng(W.SEED0 + 41)
+    n = merged.n
+    jlo = rng.integers(0, 5, n).astype(np.float64)
+    jup = np.clip(jlo + rng.integers(-1, 2, n), 0, 4)
+    jup[(jlo == 0) & (jup == 0)] = 1.0
+    glo, gup = rng.uniform(0.0, 2.5, n), rng.uniform(0.0, 2.5, n)
+    merged.zeeman = (W.f32_of_text(jlo, "%.1f"), W.f32_of_text(jup, "%.1f"),
+                     W.f32_of_text(glo, "%.3f"), W.f32_of_text(gup, "%.3f"))
+    pats = zeeman_blocks(merged)
+    grid = (3855.0, 3945.0, 0.05, 0)
+    bfield = (3000.0, 45.0, 20.0)
+    with tempfile.TemporaryDirectory() as wd:
+        W.write_krz(os.path.join(wd, "model.krz"), model)
+        merged.write_z(os.path.join(wd, "lines.z"), grid[0], grid[1], patterns=pats)
+        deck = ("wave=%.4f, %.4f, %.6f, %d\nsave=0, 0, 1, 1, 1\nvmic=%.3f\nmolbrd=%d\n"
+                "lines=\n-1  lines.z\n\nmodel=model.krz\nmus=9\nbframe=1\nbfield=%g, %g, %g\n"
+                % (grid + (HOT["vmic"], HOT["molbrd"]) + bfield))
+        log = run_ref(wd, deck)
+        assert "polarised" in log, log
+        co = fsio.read_opac(os.path.join(wd, "fs_contop.bin"))
+        sp = fsio.read_spec(os.path.join(wd, "fs_spec.bin"))
+        fl = fsio.read_flux(os.path.join(wd, "fs_flux.bin"))
+    for k in ("rhox", "T", "xne", "xna", "rho"):
+        assert np.array_equal(co[k], state[k]), "EOS state differs from the recovered one: " + k
+    assert sp["magnetic"]
+    la = merged.arrays()
+    assert np.array_equal(la["wl"], d["line_wl"]) and np.array_equal(la["elo"], d["line_elo"])
+    comp = mirrored_components(pats)
+    g = dict(wmode=0, wstart=grid[0], wend=grid[1], dstep=grid[2])
+    hg, hs = oracle.hestark_init(state["T"], state["xne"], a["frac_hii"], a["frac_heii"])
+    S = oracle.State(g, state, contopac=co["opac"], vmicro=HOT["vmic"], molbrd=HOT["molbrd"], hegam=hg,
+                     heshf=hs, spc_he1=0)
+    r = oracle.mag_lineop_calc(S, oracle.Lines(**la, kind=2, zeeman=comp), 1, np.array(bfield))
+    spz, spc = oracle.mag_radtran(S, sp["xmu"], 1, np.array(bfield), np.zeros((S.nwl, S.ntau)), r["maglineopac"])
+    ic = sp["spc"]
+    err = max(np.max(np.abs(spz[:, q] - sp["spz"][:, q]) / ic) for q in range(4))
+    print("  magnetic He I pin: %d lines, Stokes max err %.2e of Ic" % (merged.n, err))
+    np.savez_compressed(
+        os.path.join(gold, "pin_hot_he_mag.npz"), grid=np.array(grid, np.float64), i0=0, i1=len(co["wave"]) - 1,
+        atm="hot", bframe=1, bfield=np.array(bfield), vmicro=HOT["vmic"], molbrd=HOT["molbrd"],
+        contopac=co["opac"], wave=co["wave"], xmu=sp["xmu"], spz=sp["spz"], spc=sp["spc"], sfl=fl["sfl"],
+        sfc=fl["sfc"], z_npi=comp[0], z_nsi=comp[1], z_spl_pi=comp[2], z_str_pi=comp[3], z_spl_si=comp[4],
+        z_str_si=comp[5], **{"line_" + k: v for k, v in la.items()})
+
+
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "hot":
         make_hot_he(os.path.join(REPO, "tests", "golden"))
+    elif len(sys.argv) > 1 and sys.argv[1] == "hotmag":
+        make_hot_he_mag(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "molh5":
         make_mol_h5_pin(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "zh5":

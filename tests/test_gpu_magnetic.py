@@ -167,6 +167,32 @@ def test_mixed_mag_against_reference_pin(fsg):
 
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_hot_he_zeeman_lines_against_reference_pin(fsg, prec):
+    """Tabulated He I Stark lines as Zeeman lines in a Teff 15000 K atmosphere, 3 kG, BFRAME 1
+    (hestark.f90 + MagLineOpacity1/2): Context.hestark_init builds the widths and shifts and matches the
+    list to the table; the reference's Stokes IQUV (tests/golden/pin_hot_he_mag.npz).  FP64 1e-8 and
+    mixed 1e-5 (I relative; Q, U, V relative to Ic), as for the other magnetic pins."""
+    from test_hestark import hot_state
+    d = H.load_pin("pin_hot_he_mag")
+    grid, st, co, lines, z = H.mag_pin_setup(d)
+    _, _, hii, heii = hot_state()
+    C, x, w = mag_ctx(fsg, grid, st, co, nmu=len(d["xmu"]), vmicro=float(d["vmicro"]),
+                      prec=fsg.PREC_FP64 if prec == "fp64" else fsg.PREC_MIXED)
+    C.hestark_init(hii, heii, 0)
+    bframe, bfield = int(d["bframe"]), d["bfield"]
+    g = C.mag_lineop_calc(fsg.LineList.from_arrays(lines, zeeman=z), bframe, bfield, want=False)
+    assert int((((g["flags"] >> 8) & 255) > 0).sum()) == 7
+    spz, spc, sfl, sfc = C.mag_radtran(bframe, bfield)
+    ref, ic = d["spz"], d["spc"]
+    tol = 1e-8 if prec == "fp64" else 1e-5
+    assert np.max(np.abs(spz[:, 0] / ref[:, 0] - 1)) < tol
+    assert np.max(np.abs(spc / ic - 1)) < 1e-8
+    for q in (1, 2, 3):
+        assert np.max(np.abs(spz[:, q] - ref[:, q]) / ic) < tol
+    assert np.max(np.abs(sfl / d["sfl"] - 1)) < tol
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_zh5_list_against_reference_pin(fsg, tmp_path, prec):
     """A Zeeman HDF5 list read by fsio.read_hdf5_lines, its splitting built from J and the Lande
     factors with the library's fsg_zeeman_pattern, through the GPU magnetic path: the reference's

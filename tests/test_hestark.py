@@ -92,3 +92,27 @@ def test_oracle_hot_he_pin_reference(fsg, oracle_mod):
     S0 = oracle_mod.State(grid, st, contopac=co, vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]))
     r0 = oracle_mod.lineop_calc(S0, oracle_mod.Lines(**lines, kind=2), list_type=2)
     assert np.max(np.abs(r0["lineopac"] - ref)) > 1e-2 * np.max(ref)
+
+
+def test_oracle_hot_he_magnetic_pin_reference(fsg, oracle_mod):
+    """The same He I list as Zeeman lines (explicit patterns) in a 3 kG field, BFRAME 1, 9 angles: the
+    oracle's MagLineopCalc + MagRadTranCalc with the tabulated widths and shifts against the reference's
+    Stokes IQUV (tests/golden/pin_hot_he_mag.npz); I and Ic relative, Q, U, V relative to Ic."""
+    d = H.load_pin("pin_hot_he_mag")
+    grid, st, co, lines, z = H.mag_pin_setup(d)
+    _, _, hii, heii = hot_state()
+    g, h = fsg.hestark_tables(st["T"], st["xne"], hii, heii)
+    S = oracle_mod.State(grid, st, contopac=co, vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]),
+                         hegam=g, heshf=h, spc_he1=0)
+    bframe, bfield = int(d["bframe"]), d["bfield"]
+    r = oracle_mod.mag_lineop_calc(S, oracle_mod.Lines(**lines, kind=2, zeeman=z), bframe, bfield)
+    assert int((((r["flags"] >> 8) & 255) > 0).sum()) == 7
+    spz, spc = oracle_mod.mag_radtran(S, d["xmu"], bframe, bfield, np.zeros((S.nwl, S.ntau)), r["maglineopac"])
+    ref, ic = d["spz"], d["spc"]
+    assert np.max(np.abs(spz[:, 0] / ref[:, 0] - 1)) < 1e-8
+    assert np.max(np.abs(spc / ic - 1)) < 1e-8
+    for q in (1, 2, 3):
+        assert np.max(np.abs(spz[:, q] - ref[:, q]) / ic) < 1e-8
+    x, w, _ = oracle_mod.mu_quadrature(1, len(d["xmu"]))
+    sfl, _ = oracle_mod.disk_integ(w, spz[:, 0], spc)
+    assert np.max(np.abs(sfl / d["sfl"] - 1)) < 1e-8
