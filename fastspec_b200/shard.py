@@ -1,4 +1,5 @@
-"""Wavelength sharding of one synthesis over the ranks of a torch.distributed process group.
+"""Sharding over the ranks of a torch.distributed process group: the wavelength axis of one
+synthesis (`run`) and the batch axis of many independent syntheses (`run_batch`).
 
 One synthesis (one atmosphere, one line list, one grid) splits along the wavelength axis, the
 sharding the reference's own loop structure allows (LineopCalc's accumulation, synth.f90:1075-1080,
@@ -16,6 +17,12 @@ and RadTranCalc, synth.f90:1825-1866, are independent per wavelength once the wi
 The arithmetic of each wavelength is the one of a single-GPU run; only which GPU does it changes.
 The work is done by a backend: `GpuBackend` drives the CUDA library through its device entry
 points (fsg_central_dev, fsg_accumulate_dev, fsg_radtran_dev).
+
+Batch axis: atmospheres, abundance sets and angle sets of a grid are independent syntheses.  They
+are split over the ranks by a static partition on estimated cost (wavelengths x depths x candidate
+lines, longest first to the least loaded rank), each rank runs its share (`BatchGpuBackend`: one
+batched CUDA graph over its atmospheres), and the fluxes are gathered to rank 0 in the grid's order.
+No opacity crosses between GPUs.
 """
 import ctypes as C
 
@@ -137,3 +144,78 @@ class GpuBackend:
     def flux(self, i0, i1):
         self.C.radtran_dev(None, None, self.sfl.data_ptr(), self.sfc.data_ptr())
         return torch.stack([self.sfl[i0 - 1:i1], self.sfc[i0 - 1:i1]])
+
+
+# ---- batch axis ------------------------------------------------------------------------------
+
+def batch_cost(nwl, ntau, nlines):
+    """Work estimate of one synthesis of a batch: wavelengths x depths x candidate lines."""
+    return float(nwl) * float(ntau) * float(max(int(nlines), 1))
+
+
+def batch_partition(costs, world):
+    """Static partition of independent syntheses over `world` ranks: in order of decreasing cost (ties:
+    lower index first) each goes to the rank with the least summed cost so far (ties: lower rank).
+    Returns one ascending index list per rank; every rank derives the same lists from the same costs.
+    The largest load exceeds the best possible by at most the largest single cost."""
+    order = sorted(range(len(costs)), key=lambda i: (-float(costs[i]), i))
+    load = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        parts[r].append(i)
+        load[r] += float(costs[i])
+    return [sorted(p) for p in parts]
+
+
+def run_batch(backend, costs, sizes, group=None, device=None):
+    """Batch-axis sharding.  costs[i] and sizes[i] (wavelength count) of every synthesis are known on
+    every rank; rank r runs batch_partition's share r through backend.synthesize(indices), which returns
+    one float64 [2, sizes[i]] tensor (line+continuum flux, continuum flux) per index, on `device`.  The
+    shares are packed, padded to the longest, and gathered to rank 0 (one collective).  Returns (list of
+    [2, sizes[i]] tensors in the original order on rank 0, None on the other ranks; this rank's indices)."""
+    world = dist.get_world_size(group)
+    rank = dist.get_rank(group)
+    parts = batch_partition(costs, world)
+    mine = parts[rank]
+    out = backend.synthesize(mine) if mine else []
+    lens = [sum(2 * int(sizes[i]) for i in p) for p in parts]
+    buf = torch.zeros(max(max(lens), 1), dtype=torch.float64, device=device)
+    if mine:
+        flat = torch.cat([f.reshape(-1).to(torch.float64) for f in out])
+        assert flat.numel() == lens[rank], "backend returned fluxes of the wrong size"
+        buf[:flat.numel()] = flat
+    bufs = [torch.empty_like(buf) for _ in range(world)] if rank == 0 else None
+    dist.gather(buf, bufs, dst=0, group=group)
+    if rank != 0:
+        return None, mine
+    res = [None] * len(costs)
+    for p, b in zip(parts, bufs):
+        off = 0
+        for i in p:
+            n = int(sizes[i])
+            res[i] = b[off:off + 2 * n].reshape(2, n)
+            off += 2 * n
+    return res, mine
+
+
+class BatchGpuBackend:
+    """The batched CUDA path as the backend of `run_batch`: make_context(i) returns synthesis i's mixed-
+    precision Context (grid, atmosphere, continuum, mu set); one fastspec_b200.Batch over this rank's
+    contexts and the shared line list runs them in one graph replay; the fluxes come back as float64
+    tensors on `device`."""
+
+    def __init__(self, F, make_context, lines, device, margin=10.0):
+        self.F, self.make_context, self.lines, self.device, self.margin = F, make_context, lines, device, margin
+        self.batch = None
+
+    def synthesize(self, idx):
+        self.contexts = [self.make_context(i) for i in idx]
+        self.batch = self.F.Batch(self.contexts, self.lines, self.margin)
+        self.stats = self.batch.run()
+        out = []
+        for k in range(len(idx)):
+            sfl, sfc = self.batch.flux(k)
+            out.append(torch.from_numpy(np.stack([sfl, sfc])).to(self.device))
+        return out
+

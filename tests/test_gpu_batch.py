@@ -90,3 +90,59 @@ def test_batch_rejects_bad_inputs(fsg):
     C = fsg.Context(precision=fsg.PREC_FP64)
     with pytest.raises(fsg.FsgError):
         fsg.Batch([C], fsg.LineList.from_arrays(arr))
+
+
+def test_batch_axis_shares(fsg):
+    """Batch-axis sharding (fastspec_b200.shard) with the batched CUDA path as backend: the two shares
+    of a 2-rank cost partition, each run as its own batched graph, give every atmosphere's flux of the
+    whole batch (1e-6: the tuner may tile a different batch differently; continuum 1e-12); run_batch in
+    a process group of one (gloo, fluxes gathered on the host) returns them in the grid's order."""
+    import socket
+    import torch.distributed as dist
+    from fastspec_b200 import shard
+    ctxs, cases, arr = small_batch(fsg, natm=5, seed=8)
+    lines = fsg.LineList.from_arrays(arr)
+    B = fsg.Batch(ctxs, lines, margin=MARGIN)
+    B.run()
+    whole = [np.stack(B.flux(i)) for i in range(len(ctxs))]
+    B.close()
+    sizes = [c.nwl for c in ctxs]
+    costs = [shard.batch_cost(c.nwl, c.ntau, len(candidates(arr, g)["wl"])) for c, (g, _, _) in zip(ctxs, cases)]
+    x, w, _ = fsg.mu_quadrature(1, 7)
+
+    def make_context(i):
+        g, state, co = cases[i]
+        C = fsg.Context(vmicro=1.0)
+        C.set_grid(1, g["wstart"], g["wend"], g["dstep"])
+        C.set_atmosphere(state)
+        C.set_contopac(co)
+        C.set_mu(x, w)
+        return C
+
+    def check(i, f):
+        f = f.cpu().numpy()
+        assert f.shape == whole[i].shape
+        assert np.max(np.abs(f[0] / whole[i][0] - 1)) < 1e-6
+        assert np.max(np.abs(f[1] / whole[i][1] - 1)) < 1e-12
+
+    parts = shard.batch_partition(costs, 2)
+    assert all(parts) and sorted(sum(parts, [])) == list(range(len(ctxs)))
+    for p in parts:
+        be = shard.BatchGpuBackend(fsg, make_context, lines, "cuda")
+        for i, f in zip(p, be.synthesize(p)):
+            check(i, f)
+        be.batch.close()
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    dist.init_process_group("gloo", init_method="tcp://127.0.0.1:%d" % port, rank=0, world_size=1)
+    try:
+        be = shard.BatchGpuBackend(fsg, make_context, lines, "cpu")
+        res, mine = shard.run_batch(be, costs, sizes)
+        be.batch.close()
+    finally:
+        dist.destroy_process_group()
+    assert mine == list(range(len(ctxs)))
+    for i, f in enumerate(res):
+        check(i, f)

@@ -1,6 +1,7 @@
-"""Wavelength sharding of one synthesis (fastspec_b200.shard) on two CPU ranks over gloo, with the
-oracle as the backend: the orchestration (line slices, the window all-gather, the balanced
-wavelength ranges, the flux gather) must reproduce the single-process oracle synthesis."""
+"""Sharding (fastspec_b200.shard) on two and three CPU ranks over gloo, with the oracle as the
+backend.  Wavelength axis: the orchestration (line slices, the window all-gather, the balanced
+wavelength ranges, the flux gather) must reproduce the single-process oracle synthesis.  Batch axis:
+the cost partition and the gather to rank 0 must return every synthesis of the batch unchanged."""
 import os
 import socket
 
@@ -115,3 +116,93 @@ def test_balanced_ranges_and_slices():
     win = torch.tensor([[0, 1, 0], [2, 1, 5], [4, 9, 5]], dtype=torch.int32)
     c = shard.pixel_cost(win, 6)
     assert c.tolist() == [0, 1, 1, 1, 1, 0]
+
+
+# ---- batch axis ------------------------------------------------------------------------------
+
+def batch_cases():
+    """Six small independent syntheses of the solar state: different spans, steps, angle sets and
+    microturbulence, one line list covering all of them."""
+    from fastspec_b200 import workloads as W
+    import fastspec_b200 as F
+    st, meta = H.load_atm("solar")
+    specs = [(5000.0, 1.0, 0.005, 7, 1.0), (5001.0, 2.5, 0.01, 5, 0.5), (5002.0, 0.5, 0.005, 3, 2.0),
+             (5000.5, 3.0, 0.02, 7, 1.5), (5003.0, 1.0, 0.0025, 9, 1.0), (5001.5, 0.2, 0.005, 7, 0.0)]
+    cases = []
+    for w0, span, dstep, nmu, vmic in specs:
+        grid = dict(wmode=0, wstart=w0, wend=w0 + span, dstep=dstep)
+        co = H.contopac_on(meta, F.make_grid(0, w0, w0 + span, dstep) + w0)
+        cases.append((grid, co, nmu, vmic))
+    return st, cases, W.atomic_lines(200, 4999.0, 5005.0, 23).arrays()
+
+
+class OracleBatchBackend:
+    def __init__(self, oracle, st, cases, arrays):
+        self.o, self.st, self.cases, self.a = oracle, st, cases, arrays
+
+    def one(self, i):
+        grid, co, nmu, vmic = self.cases[i]
+        S = self.o.State(grid, self.st, contopac=co, vmicro=vmic)
+        r = self.o.lineop_calc(S, self.o.Lines(**self.a, kind=2), list_type=2)
+        x, w, _ = self.o.mu_quadrature(1, nmu)
+        return np.stack(self.o.disk_integ(w, *self.o.radtran(S, x, r["lineopac"])))
+
+    def synthesize(self, idx):
+        return [torch.from_numpy(self.one(i)) for i in idx]
+
+
+def batch_inputs(oracle):
+    from fastspec_b200 import shard
+    st, cases, arr = batch_cases()
+    sizes = [oracle.State(g, st).nwl for g, _, _, _ in cases]
+    costs = [shard.batch_cost(n, len(st["T"]), len(arr["wl"])) for n in sizes]
+    return st, cases, arr, sizes, costs
+
+
+def batch_worker(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import oracle
+    from fastspec_b200 import shard
+    st, cases, arr, sizes, costs = batch_inputs(oracle)
+    res, mine = shard.run_batch(OracleBatchBackend(oracle, st, cases, arr), costs, sizes)
+    np.save(out + ".mine%d.npy" % rank, np.array(mine, np.int64))
+    if rank == 0:
+        np.savez(out, *[r.numpy() for r in res])
+    else:
+        assert res is None
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_batch_axis_returns_every_synthesis(tmp_path, oracle_mod, world):
+    out = str(tmp_path / "batch.npz")
+    mp.start_processes(batch_worker, args=(world, free_port(), out), nprocs=world, join=True,
+                       start_method="spawn")
+    r = np.load(out)
+    st, cases, arr, sizes, costs = batch_inputs(oracle_mod)
+    be = OracleBatchBackend(oracle_mod, st, cases, arr)
+    assert len(r.files) == len(cases)
+    for i in range(len(cases)):
+        # each synthesis ran whole on one rank: the same arithmetic, bit for bit
+        assert np.array_equal(r["arr_%d" % i], be.one(i))
+    mine = [np.load(out + ".mine%d.npy" % k).tolist() for k in range(world)]
+    assert sorted(sum(mine, [])) == list(range(len(cases)))
+    assert all(len(m) > 0 for m in mine)
+
+
+def test_batch_partition():
+    from fastspec_b200 import shard
+    costs = [5.0, 1.0, 9.0, 3.0, 3.0, 7.0, 2.0]
+    parts = shard.batch_partition(costs, 3)
+    assert sorted(sum(parts, [])) == list(range(len(costs)))
+    loads = [sum(costs[i] for i in p) for p in parts]
+    assert max(loads) - sum(costs) / 3 <= max(costs)
+    assert parts == shard.batch_partition(list(costs), 3)              # deterministic
+    assert 2 in parts[0] and sorted(loads) == [10.0, 10.0, 10.0]        # the largest to rank 0; even here
+    assert shard.batch_partition(costs, 1) == [list(range(len(costs)))]
+    assert shard.batch_partition([1.0], 3) == [[0], [], []]              # more ranks than syntheses
+    assert shard.batch_cost(100, 50, 0) == 5000.0
+
