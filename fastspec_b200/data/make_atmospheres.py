@@ -44,8 +44,10 @@ BIN = "/root/reference/src/fastspec_Linux_x86_64"
 
 AMASS = {"H": 1.00794, "He": 4.002602, "C": 12.0107, "N": 14.0067, "O": 15.9994,
          "Ca": 40.078, "Ti": 47.867, "Cr": 51.9961, "Fe": 55.845, "Ni": 58.6934}
-POTION = {("Fe", 1): 7.9024, ("Fe", 2): 16.1878, ("Ti", 1): 6.8281, ("Cr", 1): 6.7665,
-          ("Ni", 1): 7.6399, ("Ca", 1): 6.1132, ("TiO", 1): 6.4, ("H2O", 1): 12.621,
+# Ionisation potentials [eV]: the atomic ones are the reference EOS's own values as recover_potion
+# finds them (they enter only the classical Stark and Unsold constants; molecules have neither).
+POTION = {("Fe", 1): 7.902, ("Fe", 2): 16.199, ("Ti", 1): 6.819, ("Cr", 1): 6.764,
+          ("Ni", 1): 7.64, ("Ca", 1): 6.11, ("TiO", 1): 6.4, ("H2O", 1): 12.621,
           ("CO", 1): 14.014, ("OH", 1): 13.017}
 COMPOSITION = {"TiO": [("Ti", 1), ("O", 1)], "H2O": [("H", 2), ("O", 1)],
                "CO": [("C", 1), ("O", 1)], "OH": [("O", 1), ("H", 1)]}
@@ -775,7 +777,7 @@ def make_mol_h5_pin(gold):
 
 # ---- hot atmosphere with tabulated He I Stark lines (hestark.f90) -------------------------------
 HOT = dict(teff=15000.0, logg=4.0, ntau=48, species=[("He", 1)], wl0=5000.0, dstep=0.01, vmic=1.0, molbrd=0)
-HE_POTION = 24.5874
+HE_POTION = 24.581
 
 
 def he_lines(wl, elo, loggf, lgrad=None, lgqst=None, lgvdw=None):
@@ -997,8 +999,157 @@ def make_hot_he_mag(gold):
         z_str_si=comp[5], **{"line_" + k: v for k, v in la.items()})
 
 
+def recover_potion(atmname, model, species, state, wl0, dstep, vmic, molbrd, probe_loggf):
+    """The FP32 ionisation potential PotIon of every atomic species, as the reference's EOS holds it.
+
+    One probe per species 8 A apart (E_low = 0, G_rad 1e5, log gf 2.5 dex above the FractionPF probe,
+    a zero Stark constant so XlineSetup takes the classical treatment, opacity.f90:187-193, whose
+    constant 2.26e-7 (5.42e-7 for ions) x (Ion^2 Hie / (PotIon - Eup))^2 falls with PotIon).  Per
+    species, a bisection over the bit patterns of FP32 numbers in [3, 60] eV matches the probe's line
+    opacity summed over its window pixels 0.1 A or more from the centre (the wing grows with the Stark
+    width); the value of least profile mismatch among the final neighbours is kept.  Returns the potion
+    array and the largest relative profile mismatch per species."""
+    n = len(species)
+    wl = wl0 + 8.0 * (1 + np.arange(n))
+    wend = wl0 + 8.0 * (n + 1)
+    L = W.LineList(species, wl, np.asarray(probe_loggf[:n]) + 2.5, np.zeros(n), np.full(n, 5.0), np.zeros(n),
+                   np.full(n, -30.0), np.arange(n, dtype=np.int32), np.zeros(n, np.int32))
+    with tempfile.TemporaryDirectory() as wd:
+        W.write_krz(os.path.join(wd, "model.krz"), model)
+        L.write_z(os.path.join(wd, "lines.z"), wl0, wend)
+        deck = ("wave=%.4f, %.4f, %.6f, 0\nsave=0, 1, 1, 0, 0\nvmic=%.3f\nmolbrd=%d\n"
+                "lines=\n-1  lines.z\n\nmodel=model.krz\nmus=0\n" % (wl0, wend, dstep, vmic, molbrd))
+        run_ref(wd, deck)
+        lo = fsio.read_opac(os.path.join(wd, "fs_lineop.bin"))
+        co = fsio.read_opac(os.path.join(wd, "fs_contop.bin"))
+    for k in ("rhox", "T", "xne", "xna", "rho"):
+        assert np.array_equal(lo[k], state[k]), "EOS state differs: " + k
+    g = dict(wmode=0, wstart=wl0, wend=wend, dstep=dstep)
+    wave, ref = lo["wave"], lo["opac"]
+    nz = ref.max(axis=1) > 0
+    pot = np.asarray(state["potion"], np.float32).copy()
+    a = L.arrays()
+    devs = []
+    for k in range(n):
+        Lk = oracle.Lines(**{q: np.ascontiguousarray(v[k:k + 1]) for q, v in a.items()}, kind=2)
+        dl = np.abs(wave - wl[k])
+        win = nz & (dl < 3.9)
+        px = np.nonzero(win & (dl >= 0.1))[0]
+        assert len(px) > 0, "probe window narrower than 0.1 A"
+        sref = ref[px].sum()
+
+        def profile(p):
+            st = dict(state)
+            pp = pot.copy()
+            pp[k] = p
+            st["potion"] = pp
+            S = oracle.State(g, st, contopac=co["opac"], vmicro=vmic, molbrd=molbrd)
+            return oracle.lineop_calc(S, Lk, list_type=2)["lineopac"]
+
+        lob, hib = int(np.float32(3.0).view(np.int32)), int(np.float32(60.0).view(np.int32))
+        while hib - lob > 1:
+            mid = (lob + hib) // 2
+            if profile(np.int32(mid).view(np.float32))[px].sum() > sref:
+                lob = mid
+            else:
+                hib = mid
+        best = None
+        m = ref[win] > 0
+        for c in (lob - 1, lob, hib, hib + 1):
+            p = np.int32(c).view(np.float32)
+            dev = np.max(np.abs(profile(p)[win][m] / ref[win][m] - 1))
+            if best is None or dev < best[0]:
+                best = (dev, p)
+        pot[k] = best[1]
+        devs.append(best[0])
+        print("  %-4s %d  PotIon %.6g (guess %.6g), profile max rel %.1e"
+              % (species[k][0], species[k][1], pot[k], state["potion"][k], best[0]))
+    return pot, np.array(devs)
+
+
+def make_modes_pin(gold):
+    """Broadening modes and options (pin_solar_modes.npz): the pin_solar list with a quarter of its lines
+    on the classical Stark constant (zero Stark input), a quarter on Unsold van der Waals (zero input),
+    one in eight on ABO (sigma.alpha above 10), run with EPSOPAC 3e-3 and VWFUDGE 1.8 (opacity.f90:
+    185-227, 239-293); needs the recovered ionisation potentials."""
+    name, atmname, mk, grid, region = pin_specs()[0]
+    teff, logg, ntau, species, ismol, _, _, vmic, molbrd, _, _ = CONFIGS[atmname]
+    model = W.eddington_model(teff, logg, ntau)
+    state = load_state(atmname)
+    base = mk()
+    t = base._txt
+    lgq = np.array(t["lgqst"], np.float64)
+    lgv = np.array(t["lgvdw"], np.float64)
+    lgq[1::4] = 0.0
+    lgv[2::4] = 0.0
+    rng = np.random.default_rng(W.SEED0 + 42)
+    abo = np.arange(3, base.n, 8)
+    lgv[abo] = np.round(rng.uniform(200.0, 400.0, len(abo))) + np.round(rng.uniform(0.2, 0.4, len(abo)), 3)
+    extra = W.LineList(species, base.wl, t["loggf"], t["elo"], t["lgrad"], lgq, lgv, base.spc, base.ismol)
+    pgf = np.load(os.path.join(HERE, "atm_%s.npz" % atmname))["probe_loggf"]
+    probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
+    merged = merge([probes, extra])
+    eps, vwf = 3e-3, 1.8
+    with tempfile.TemporaryDirectory() as wd:
+        W.write_krz(os.path.join(wd, "model.krz"), model)
+        merged.write_z(os.path.join(wd, "lines.z"), grid[0], grid[1])
+        deck = ("wave=%.4f, %.4f, %.6f, %d\nsave=0, 1, 1, 1, 1\nvmic=%.3f\nmolbrd=%d\nepsopac=%g\nvwfudge=%g\n"
+                "lines=\n-1  lines.z\n\nmodel=model.krz\nmus=7\n" % (grid + (vmic, molbrd, eps, vwf)))
+        run_ref(wd, deck)
+        lo = fsio.read_opac(os.path.join(wd, "fs_lineop.bin"))
+        co = fsio.read_opac(os.path.join(wd, "fs_contop.bin"))
+        sp = fsio.read_spec(os.path.join(wd, "fs_spec.bin"))
+        fl = fsio.read_flux(os.path.join(wd, "fs_flux.bin"))
+    for k in ("rhox", "T", "xne", "xna", "rho"):
+        assert np.array_equal(lo[k], state[k]), "EOS state differs from the recovered one: " + k
+    wave = lo["wave"]
+    sel = (wave >= region[0] - 1e-9) & (wave <= region[1] + 1e-9)
+    i0, i1 = (int(x) for x in np.nonzero(sel)[0][[0, -1]])
+    g = dict(wmode=grid[3], wstart=grid[0], wend=grid[1], dstep=grid[2])
+    S = oracle.State(g, state, contopac=co["opac"], vmicro=vmic, molbrd=molbrd, epsopac=eps, vwfudge=vwf)
+    r = oracle.lineop_calc(S, oracle.Lines(**lines_args(merged), kind=2), list_type=2)
+    ref = lo["opac"]
+    m = ref > 0
+    print("  modes pin: pattern equal %s, line opacity max rel %.2e"
+          % (np.array_equal(r["lineopac"] > 0, m), np.max(np.abs(r["lineopac"][m] / ref[m] - 1))))
+    a = extra.arrays()
+    np.savez_compressed(
+        os.path.join(gold, "pin_solar_modes.npz"),
+        grid=np.array(grid, np.float64), i0=i0, i1=i1, atm=atmname, epsopac=eps, vwfudge=vwf,
+        species=np.array(["%s %d" % s for s in species]), vmicro=vmic, molbrd=molbrd,
+        contopac=co["opac"][i0:i1 + 1], lineopac=ref[i0:i1 + 1], wave=wave[i0:i1 + 1], xmu=sp["xmu"],
+        spl=sp["spl"][i0:i1 + 1], spc=sp["spc"][i0:i1 + 1], sfl=fl["sfl"][i0:i1 + 1], sfc=fl["sfc"][i0:i1 + 1],
+        **{"line_" + k: v for k, v in a.items()})
+
+
+def update_potion():
+    """Replace the guessed ionisation potentials of the atomic atmospheres' states with the recovered
+    ones (atm_solar, atm_magnetic, atm_hot)."""
+    for name in ("solar", "magnetic", "hot"):
+        path = os.path.join(HERE, "atm_%s.npz" % name)
+        d = dict(np.load(path))
+        if name == "hot":
+            teff, logg, ntau, species, wl0, dstep, vmic, molbrd = (HOT["teff"], HOT["logg"], HOT["ntau"],
+                                                                   HOT["species"], HOT["wl0"], HOT["dstep"],
+                                                                   HOT["vmic"], HOT["molbrd"])
+        else:
+            teff, logg, ntau, species, _, wl0, dstep, vmic, molbrd, _, _ = CONFIGS[name]
+        print(name)
+        model = W.eddington_model(teff, logg, ntau)
+        pot, dev = recover_potion(name, model, species, load_state(name), wl0, dstep, vmic, molbrd,
+                                  d["probe_loggf"])
+        assert dev.max() < 1e-12, "ionisation potential not recovered"
+        d["potion"] = pot
+        d["potion_profile_dev"] = dev
+        np.savez_compressed(path, **d)
+
+
 if __name__ == "__main__":
-    if len(sys.argv) > 1 and sys.argv[1] == "hot":
+    if len(sys.argv) > 1 and sys.argv[1] == "potion":
+        update_potion()
+    elif len(sys.argv) > 1 and sys.argv[1] == "modes":
+        make_modes_pin(os.path.join(REPO, "tests", "golden"))
+    elif len(sys.argv) > 1 and sys.argv[1] == "hot":
         make_hot_he(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "hotmag":
         make_hot_he_mag(os.path.join(REPO, "tests", "golden"))

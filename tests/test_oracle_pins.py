@@ -54,6 +54,30 @@ def test_oracle_lineop_pins_reference(oracle_mod, name):
     assert np.max(np.abs(sfc / d["sfc"] - 1)) < 1e-8
 
 
+def test_oracle_broadening_modes_pin_reference(oracle_mod):
+    """Classical Stark (zero Stark input), Unsold (zero van der Waals input) and ABO (sigma.alpha) lines
+    with EPSOPAC 3e-3 and VWFUDGE 1.8 (opacity.f90:185-227, 239-293) against the reference's run
+    (tests/golden/pin_solar_modes.npz), on the solar state with the EOS's own ionisation potentials."""
+    d = H.load_pin("pin_solar_modes")
+    grid, st, meta, co = H.pin_setup(d)
+    S = oracle_mod.State(grid, st, contopac=co, vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]),
+                         epsopac=float(d["epsopac"]), vwfudge=float(d["vwfudge"]))
+    i0, i1 = int(d["i0"]), int(d["i1"])
+    lines = H.pin_lines(d)
+    assert np.sum(lines["gqst"] == 0) > 20 and np.sum(lines["gvdw"] == 0) > 20 and np.sum(lines["gvdw"] > 10) > 10
+    r = oracle_mod.lineop_calc(S, oracle_mod.Lines(**lines, kind=2), list_type=2)
+    assert np.sum((r["flags"] >> 2) & 1) == np.sum(lines["gvdw"] > 10)
+    lo, ref = r["lineopac"][i0:i1 + 1], d["lineopac"]
+    assert np.array_equal(lo > 0, ref > 0)
+    m = ref > 0
+    assert np.max(np.abs(lo[m] / ref[m] - 1)) < 1e-8
+    spl, spc = oracle_mod.radtran(S, d["xmu"], r["lineopac"])
+    assert np.max(np.abs(spl[i0:i1 + 1] / d["spl"] - 1)) < 1e-8
+    x, w, _ = oracle_mod.mu_quadrature(1, len(d["xmu"]))
+    sfl, sfc = oracle_mod.disk_integ(w, spl[i0:i1 + 1], spc[i0:i1 + 1])
+    assert np.max(np.abs(sfl / d["sfl"] - 1)) < 1e-8
+
+
 @pytest.mark.parametrize("name", ["pin_solar", "pin_cooldwarf"])
 def test_oracle_linstr_pins_reference(oracle_mod, name):
     """LinStrCalc (synth.f90:1774-1822): central depths of the retained lines against the reference's
