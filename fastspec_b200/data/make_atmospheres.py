@@ -336,7 +336,7 @@ def load_state(name):
     keys = ("rhox", "T", "xne", "xna", "rho", "fractionpf", "xamass", "potion", "ion",
             "frac_h1", "frac_he1")
     st = {k: d[k] for k in keys}
-    st["frac_h2"] = np.zeros(len(d["T"]), np.float32)
+    st["frac_h2"] = d["frac_h2"] if "frac_h2" in d.files else np.zeros(len(d["T"]), np.float32)
     return st
 
 
@@ -1122,6 +1122,103 @@ def make_modes_pin(gold):
         **{"line_" + k: v for k, v in a.items()})
 
 
+def update_h2(name="cooldwarf", h2brd=1.0):
+    """The H2 molecule density Fraction(Hmol) of a state, which XlineInit adds to the van der Waals
+    perturbers with weight H2Brd * 0.874307 (opacity.f90:82): the recover() probes run again with
+    H2BRD set; the van der Waals probe's centre gives the perturber density as in recover(), and its
+    excess over the H2-free one, / (H2Brd * 0.874307), is the FP32 density.  The oracle must then
+    reproduce the whole probe run with H2BRD."""
+    teff, logg, ntau, species, ismol, wl0, dstep, vmic, molbrd, _, _ = CONFIGS[name]
+    path = os.path.join(HERE, "atm_%s.npz" % name)
+    d = dict(np.load(path))
+    model = W.eddington_model(teff, logg, ntau)
+    state = load_state(name)
+    nsp = len(species)
+    probes = probe_list(species, wl0, 2.0, vdw_species=0, ismol=ismol, loggf=d["probe_loggf"])
+    wend = wl0 + 2.0 * (nsp + 2)
+    with tempfile.TemporaryDirectory() as wd:
+        W.write_krz(os.path.join(wd, "model.krz"), model)
+        probes.write_z(os.path.join(wd, "lines.z"), wl0, wend)
+        deck = ("wave=%.4f, %.4f, %.6f, 0\nsave=0, 1, 1, 0, 0\nvmic=%.3f\nmolbrd=%d\nh2brd=%g\n"
+                "lines=\n-1  lines.z\n\nmodel=model.krz\nmus=0\n" % (wl0, wend, dstep, vmic, molbrd, h2brd))
+        run_ref(wd, deck)
+        lo = fsio.read_opac(os.path.join(wd, "fs_lineop.bin"))
+        co = fsio.read_opac(os.path.join(wd, "fs_contop.bin"))
+    for k in ("rhox", "T", "xne", "xna", "rho"):
+        assert np.array_equal(lo[k], state[k]), "EOS state differs: " + k
+    grid = dict(wmode=0, wstart=wl0, wend=wend, dstep=dstep)
+    st = oracle.State(grid, state, contopac=co["opac"], vmicro=vmic, molbrd=molbrd)
+    L = oracle.Lines(**lines_args(probes), kind=2)
+    kv = nsp
+    cop, vv, av0 = oracle.xline(st, L, kv)
+    wave = st.wave + st.wfirst
+    ic = int(np.argmin(np.abs(wave - probes.wl[kv])))
+    a = invert_h0(lo["opac"][ic] / cop, av0)
+    WaveL = probes.wl[kv]
+    dopl = 1.0 / (vv * WaveL)
+    gam = a * (dopl / WaveL * (4.0 * 299792.458e13 * np.pi))
+    nprtb = (gam - float(probes.grad[kv])) / (float(probes.gvdw[kv]) * (lo["T"] / 1e4) ** 0.3)
+    base = state["frac_h1"].astype(np.float64) + 0.412265 * state["frac_he1"].astype(np.float64)
+    frac_h2 = ((nprtb - base) / (h2brd * 0.874307)).astype(np.float32)
+    st2 = dict(state, frac_h2=frac_h2)
+    S = oracle.State(grid, st2, contopac=co["opac"], vmicro=vmic, molbrd=molbrd, h2brd=h2brd)
+    r = oracle.lineop_calc(S, L, list_type=2)
+    m = lo["opac"] > 0
+    rel = np.max(np.abs(r["lineopac"][m] / lo["opac"][m] - 1))
+    print("  %s: n(H2) %.3e .. %.3e (%.0f%% .. %.0f%% of the perturbers), probe run reproduced to %.1e"
+          % (name, frac_h2[0], frac_h2[-1], 100 * h2brd * 0.874307 * frac_h2[0] / nprtb[0],
+             100 * h2brd * 0.874307 * frac_h2[-1] / nprtb[-1], rel))
+    d["frac_h2"] = frac_h2
+    d["h2_probe_rel"] = rel
+    np.savez_compressed(path, **d)
+
+
+def make_mol_opts_pin(gold):
+    """Molecular broadening options (pin_cooldwarf_opts.npz): the pin_cooldwarf list with H2BRD 1.5 (H2 in
+    the van der Waals perturbers, opacity.f90:82) and VWMOL 4e-8 (one van der Waals constant for every
+    molecular line, opacity.f90:229-234), MolBrd on; needs the recovered H2 density."""
+    name, atmname, mk, grid, region = pin_specs()[1]
+    teff, logg, ntau, species, ismol, _, _, vmic, molbrd, _, _ = CONFIGS[atmname]
+    model = W.eddington_model(teff, logg, ntau)
+    state = load_state(atmname)
+    extra = mk()
+    pgf = np.load(os.path.join(HERE, "atm_%s.npz" % atmname))["probe_loggf"]
+    probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
+    merged = merge([probes, extra])
+    h2brd, vwmol = 1.5, 4e-8
+    with tempfile.TemporaryDirectory() as wd:
+        W.write_krz(os.path.join(wd, "model.krz"), model)
+        merged.write_z(os.path.join(wd, "lines.z"), grid[0], grid[1])
+        deck = ("wave=%.4f, %.4f, %.6f, %d\nsave=0, 1, 1, 1, 1\nvmic=%.3f\nmolbrd=%d\nh2brd=%g\nvwmol=%g\n"
+                "lines=\n-1  lines.z\n\nmodel=model.krz\nmus=7\n" % (grid + (vmic, molbrd, h2brd, vwmol)))
+        run_ref(wd, deck)
+        lo = fsio.read_opac(os.path.join(wd, "fs_lineop.bin"))
+        co = fsio.read_opac(os.path.join(wd, "fs_contop.bin"))
+        sp = fsio.read_spec(os.path.join(wd, "fs_spec.bin"))
+        fl = fsio.read_flux(os.path.join(wd, "fs_flux.bin"))
+    for k in ("rhox", "T", "xne", "xna", "rho"):
+        assert np.array_equal(lo[k], state[k]), "EOS state differs from the recovered one: " + k
+    wave = lo["wave"]
+    sel = (wave >= region[0] - 1e-9) & (wave <= region[1] + 1e-9)
+    i0, i1 = (int(x) for x in np.nonzero(sel)[0][[0, -1]])
+    g = dict(wmode=grid[3], wstart=grid[0], wend=grid[1], dstep=grid[2])
+    S = oracle.State(g, state, contopac=co["opac"], vmicro=vmic, molbrd=molbrd, h2brd=h2brd, vwmol=vwmol)
+    r = oracle.lineop_calc(S, oracle.Lines(**lines_args(merged), kind=2), list_type=2)
+    ref = lo["opac"][i0:i1 + 1]
+    m = ref > 0
+    lor = r["lineopac"][i0:i1 + 1]
+    print("  molecular options pin: pattern equal %s, line opacity max rel %.2e"
+          % (np.array_equal(lor > 0, m), np.max(np.abs(lor[m] / ref[m] - 1))))
+    a = extra.arrays()
+    np.savez_compressed(
+        os.path.join(gold, "pin_cooldwarf_opts.npz"),
+        grid=np.array(grid, np.float64), i0=i0, i1=i1, atm=atmname, h2brd=h2brd, vwmol=vwmol,
+        species=np.array(["%s %d" % s for s in species]), vmicro=vmic, molbrd=molbrd,
+        contopac=co["opac"][i0:i1 + 1], lineopac=ref, wave=wave[i0:i1 + 1], xmu=sp["xmu"],
+        spl=sp["spl"][i0:i1 + 1], spc=sp["spc"][i0:i1 + 1], sfl=fl["sfl"][i0:i1 + 1], sfc=fl["sfc"][i0:i1 + 1],
+        **{"line_" + k: v for k, v in a.items()})
+
+
 def update_potion():
     """Replace the guessed ionisation potentials of the atomic atmospheres' states with the recovered
     ones (atm_solar, atm_magnetic, atm_hot)."""
@@ -1147,6 +1244,10 @@ def update_potion():
 if __name__ == "__main__":
     if len(sys.argv) > 1 and sys.argv[1] == "potion":
         update_potion()
+    elif len(sys.argv) > 1 and sys.argv[1] == "h2":
+        update_h2()
+    elif len(sys.argv) > 1 and sys.argv[1] == "molopts":
+        make_mol_opts_pin(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "modes":
         make_modes_pin(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "hot":

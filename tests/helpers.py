@@ -13,7 +13,7 @@ STATE_KEYS = ("rhox", "T", "xne", "xna", "rho", "fractionpf", "xamass", "potion"
 def load_atm(name):
     d = np.load(os.path.join(DATA, "atm_%s.npz" % name))
     st = {k: d[k] for k in STATE_KEYS}
-    st["frac_h2"] = np.zeros(len(d["T"]), np.float32)
+    st["frac_h2"] = d["frac_h2"] if "frac_h2" in d.files else np.zeros(len(d["T"]), np.float32)
     meta = dict(vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]), cont_wave=d["cont_wave"],
                 cont_opac=d["cont_opac"], species=[str(s) for s in d["species"]])
     return st, meta

@@ -430,6 +430,32 @@ def test_broadening_modes_against_reference_pin(fsg, prec):
 
 
 @pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_molecular_options_against_reference_pin(fsg, prec):
+    """H2BRD 1.5 (H2 among the van der Waals perturbers of XlineInit) and VWMOL 4e-8 on the cool-dwarf
+    list through the GPU path: the reference's line opacity, windows and flux
+    (tests/golden/pin_cooldwarf_opts.npz); FP64 1e-8, mixed within the mixed bars."""
+    d = H.load_pin("pin_cooldwarf_opts")
+    grid, st, meta, co = H.pin_setup(d)
+    C = fsg.Context(precision=fsg.PREC_MIXED if prec == "mixed" else fsg.PREC_FP64, vmicro=float(d["vmicro"]),
+                    molbrd=int(d["molbrd"]), h2brd=float(d["h2brd"]), vwmol=float(d["vwmol"]))
+    C.set_grid(grid["wmode"], grid["wstart"], grid["wend"], grid["dstep"])
+    C.set_atmosphere(st)
+    C.set_contopac(co)
+    x, w, _ = fsg.mu_quadrature(1, len(d["xmu"]))
+    C.set_mu(x, w)
+    g = C.lineop_calc(fsg.LineList.from_arrays(H.pin_lines(d)))
+    i0, i1 = int(d["i0"]), int(d["i1"])
+    lo, ref = g["lineopac"][i0:i1 + 1], d["lineopac"]
+    assert np.array_equal(lo > 0, ref > 0)
+    if prec == "fp64":
+        assert np.max(np.abs(lo[ref > 0] / ref[ref > 0] - 1)) < 1e-8
+    else:
+        assert np.max(np.abs(lo - ref) / (ref + d["contopac"])) < 2e-6
+    spl, spc, sfl, sfc = C.radtran()
+    assert np.max(np.abs(sfl[i0:i1 + 1] / d["sfl"] - 1)) < (1e-8 if prec == "fp64" else 1e-5)
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
 def test_hot_he_lines_against_reference_pin(fsg, prec):
     """Tabulated He I Stark lines in a Teff 15000 K atmosphere (hestark.f90): Context.hestark_init builds
     the 37 lines' widths and shifts on the host (fsg_hestark_tables) and the lists' table entries come

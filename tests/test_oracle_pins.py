@@ -78,6 +78,31 @@ def test_oracle_broadening_modes_pin_reference(oracle_mod):
     assert np.max(np.abs(sfl / d["sfl"] - 1)) < 1e-8
 
 
+def test_oracle_molecular_options_pin_reference(oracle_mod):
+    """H2BRD 1.5 (H2 molecules among the van der Waals perturbers, opacity.f90:82, with the H2 density
+    recovered from the reference) and VWMOL 4e-8 (opacity.f90:229-234) on the cool-dwarf list against
+    the reference's run (tests/golden/pin_cooldwarf_opts.npz)."""
+    d = H.load_pin("pin_cooldwarf_opts")
+    grid, st, meta, co = H.pin_setup(d)
+    assert np.all(st["frac_h2"] > 0)
+    S = oracle_mod.State(grid, st, contopac=co, vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]),
+                         h2brd=float(d["h2brd"]), vwmol=float(d["vwmol"]))
+    i0, i1 = int(d["i0"]), int(d["i1"])
+    r = oracle_mod.lineop_calc(S, oracle_mod.Lines(**H.pin_lines(d), kind=2), list_type=2)
+    lo, ref = r["lineopac"][i0:i1 + 1], d["lineopac"]
+    assert np.array_equal(lo > 0, ref > 0)
+    m = ref > 0
+    assert np.max(np.abs(lo[m] / ref[m] - 1)) < 1e-8
+    spl, spc = oracle_mod.radtran(S, d["xmu"], r["lineopac"])
+    x, w, _ = oracle_mod.mu_quadrature(1, len(d["xmu"]))
+    sfl, sfc = oracle_mod.disk_integ(w, spl[i0:i1 + 1], spc[i0:i1 + 1])
+    assert np.max(np.abs(sfl / d["sfl"] - 1)) < 1e-8
+    # both options change the result: without them the same list differs
+    S0 = oracle_mod.State(grid, st, contopac=co, vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]))
+    r0 = oracle_mod.lineop_calc(S0, oracle_mod.Lines(**H.pin_lines(d), kind=2), list_type=2)
+    assert np.max(np.abs(r0["lineopac"][i0:i1 + 1][m] / ref[m] - 1)) > 1e-3
+
+
 @pytest.mark.parametrize("name", ["pin_solar", "pin_cooldwarf"])
 def test_oracle_linstr_pins_reference(oracle_mod, name):
     """LinStrCalc (synth.f90:1774-1822): central depths of the retained lines against the reference's
