@@ -88,20 +88,23 @@ def write_flux(path, wave, sfl, sfc):
 
 
 def read_linst(path):
-    species, ion, wave, strength = [], [], [], []
+    """fs_linst.bin -> dict(species, ion, wave, strength) over all line lists, and nrec: the record
+    count of each list in file order (write_linst with append=True rebuilds the file list by list)."""
+    species, ion, wave, strength, nrec = [], [], [], [], []
     with open(path, "rb") as f:
         while True:
             n = np.fromfile(f, "<i4", 1)
             if n.size == 0:
                 break
             n = int(n[0])
+            nrec.append(n)
             species.append(np.char.strip(np.fromfile(f, "S8", n).astype("U8")))
             ion.append(np.fromfile(f, "<i4", n))
             wave.append(np.fromfile(f, "<f8", n))
             strength.append(np.fromfile(f, "<f4", n))
     cat = lambda x, d: np.concatenate(x) if x else np.zeros(0, d)
     return dict(species=cat(species, "U8"), ion=cat(ion, "<i4"), wave=cat(wave, "<f8"),
-                strength=cat(strength, "<f4"))
+                strength=cat(strength, "<f4"), nrec=np.array(nrec, np.int64))
 
 
 def write_linst(path, species, ion, wave, strength, append=False):
