@@ -421,6 +421,34 @@ def make_linst_pins(gold):
         print(name, "line strengths", int(sel.sum()), "of", extra.n, "seeded lines")
 
 
+def make_mag_linst_pin(gold):
+    """Line strengths of the magnetic driver (MagLineopCalc with SAVE flag 1, synth.f90:1098-1455): the
+    pin_magnetic deck with BFRAME 1 and the explicit Zeeman patterns, its fs_linst.bin restricted to the
+    seeded lines (pin_magnetic_linst.npz)."""
+    teff, logg, ntau, species, ismol, _, _, vmic, molbrd, _, _ = CONFIGS["magnetic"]
+    model = W.eddington_model(teff, logg, ntau)
+    grid = (6000.0, 6043.0, 0.002, 0)
+    bfield = (2000.0, 60.0, 30.0)
+    extra = W.zeeman_lines(60, 6040.3, 6042.7, W.SEED0 + 2)
+    pgf = np.load(os.path.join(HERE, "atm_magnetic.npz"))["probe_loggf"]
+    probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
+    merged = merge([probes, extra])
+    pats = zeeman_blocks(merged)
+    with tempfile.TemporaryDirectory() as wd:
+        W.write_krz(os.path.join(wd, "model.krz"), model)
+        merged.write_z(os.path.join(wd, "lines.z"), grid[0], grid[1], patterns=pats)
+        deck = ("wave=%.4f, %.4f, %.6f, %d\nsave=1, 0, 0, 0, 0\nvmic=%.3f\nmolbrd=%d\n"
+                "lines=\n-1  lines.z\n\nmodel=model.krz\nmus=9\nbframe=1\nbfield=%g, %g, %g\n"
+                % (grid + (vmic, molbrd) + bfield))
+        log = run_ref(wd, deck)
+        assert "polarised" in log, log
+        ls = fsio.read_linst(os.path.join(wd, "fs_linst.bin"))
+    sel = ls["wave"] >= extra.arrays()["wl"].min() - 1e-9
+    np.savez_compressed(os.path.join(gold, "pin_magnetic_linst.npz"), wave=ls["wave"][sel],
+                        strength=ls["strength"][sel], ion=ls["ion"][sel], nprobe_rows=int((~sel).sum()))
+    print("pin_magnetic line strengths", int(sel.sum()), "of", extra.n, "seeded lines")
+
+
 def make_convol_pin(gold):
     """Broadening fixtures: the reference's intensities (fs_spec.bin) and its broadened flux
     (fs_flux.bin, IntegConvol / DiskInteg with CONVOL = Vsini, Vmacro, Vgau) of the same run, for
@@ -1266,6 +1294,8 @@ if __name__ == "__main__":
         make_mag_pin(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "convol":
         make_convol_pin(os.path.join(REPO, "tests", "golden"))
+    elif len(sys.argv) > 1 and sys.argv[1] == "maglinst":
+        make_mag_linst_pin(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "linst":
         make_linst_pins(os.path.join(REPO, "tests", "golden"))
     else:

@@ -106,6 +106,20 @@ def test_mag_against_reference_pin(fsg):
     assert np.max(np.abs(sfc[i0:i1 + 1] / d["sfc"] - 1)) < 1e-8
 
 
+def test_mag_linstr_against_reference_pin(fsg):
+    """Line strengths of the magnetic driver on the GPU against the reference's fs_linst.bin for the
+    pin_magnetic deck (tests/golden/pin_magnetic_linst.npz)."""
+    d = H.load_pin("pin_magnetic")
+    ref = H.load_pin("pin_magnetic_linst")
+    grid, st, co, lines, z = H.mag_pin_setup(d)
+    C, x, w = mag_ctx(fsg, grid, st, co, nmu=len(d["xmu"]), vmicro=float(d["vmicro"]))
+    g = C.mag_lineop_calc(fsg.LineList.from_arrays(lines, zeeman=z), int(d["bframe"]), d["bfield"], want=False,
+                          want_linstr=True)
+    keep = (g["flags"] & 1) == 0
+    assert keep.sum() == len(ref["wave"])
+    assert np.max(np.abs(g["linstr"][keep] - ref["strength"])) < 1e-7
+
+
 def test_mag_rejects_bad_field(fsg):
     grid, st, co, lines, z = zeeman_case(n=5)
     C, x, w = mag_ctx(fsg, grid, st, co)

@@ -122,6 +122,22 @@ def test_oracle_linstr_pins_reference(oracle_mod, name):
     assert np.all(ref["strength"] > 0)
 
 
+def test_oracle_magnetic_linstr_pin_reference(oracle_mod):
+    """Line strengths from the magnetic driver (MagLineopCalc, SAVE flag 1) against the reference's
+    fs_linst.bin for the pin_magnetic deck (9 angles, BFRAME 1)."""
+    d = H.load_pin("pin_magnetic")
+    ref = H.load_pin("pin_magnetic_linst")
+    grid, st, co, lines, z = H.mag_pin_setup(d)
+    S = oracle_mod.State(grid, st, contopac=co, vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]))
+    x, w, _ = oracle_mod.mu_quadrature(1, len(d["xmu"]))
+    r = oracle_mod.mag_lineop_calc(S, oracle_mod.Lines(**lines, kind=2, zeeman=z), int(d["bframe"]), d["bfield"],
+                                   nmu=len(x), xmu=x, wmu=w, want_linstr=True)
+    keep = (r["flags"] & 1) == 0
+    assert keep.sum() == len(ref["wave"])
+    assert np.max(np.abs(d["line_wl"][keep] - ref["wave"])) < 1e-9
+    assert np.max(np.abs(r["linstr"][keep] - ref["strength"])) < 1e-7
+
+
 def test_oracle_blocks_equal_single_block(oracle_mod):
     """Segmented blocks (NlinesStep < Nlines) give the single-block result (synth.f90:1012-1088)."""
     d = H.load_pin("pin_solar")
