@@ -16,7 +16,7 @@ file format (version 0 superblock) that these files use:
   chunked with a version 1 B-tree of chunk nodes), the filter pipeline (deflate, shuffle, fletcher32
   skipped) and attribute messages (versions 1-3);
 * writing: the same structures with contiguous, unfiltered datasets, which any HDF5 reader accepts
-  (the reference program reads them; ``make_atmospheres.py`` checks that).
+  (the reference program reads them; ``tests/golden/make_atmospheres.py`` checks that).
 
 All multi-byte fields are little-endian, offsets and lengths 8 bytes.
 """

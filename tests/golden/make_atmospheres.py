@@ -21,8 +21,10 @@ once, and stores what it computed:
     inverted on the table's bilinear lerp for a, a -> Gamma_6 -> Nprtb;
   * the continuum opacity on coarse knots spanning each configuration's range.
 
+The states go to fastspec_b200/data/atm_*.npz (the benchmark workloads and the tests use them).
 Also writes parity fixtures (tests/golden/pin_*.npz): line lists run through the reference
 with the reference's line opacity, windows and spectra, for the oracle/GPU parity tests.
+Test infrastructure: the oracle serves as the inversion model here.
 
 Needs the reference at /root/reference (this container only); the outputs are committed.
 """
@@ -35,6 +37,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
+DATA = os.path.join(REPO, "fastspec_b200", "data")
 sys.path.insert(0, REPO)
 
 import oracle  # noqa: E402  (fixture generation: the oracle is the inversion model)
@@ -307,7 +310,7 @@ CONFIGS = {
 
 
 def main():
-    outdir = HERE
+    outdir = DATA
     gold = os.path.join(REPO, "tests", "golden")
     os.makedirs(gold, exist_ok=True)
     oracle.build()
@@ -332,7 +335,7 @@ def main():
 
 
 def load_state(name):
-    d = np.load(os.path.join(HERE, "atm_%s.npz" % name))
+    d = np.load(os.path.join(DATA, "atm_%s.npz" % name))
     keys = ("rhox", "T", "xne", "xna", "rho", "fractionpf", "xamass", "potion", "ion",
             "frac_h1", "frac_he1")
     st = {k: d[k] for k in keys}
@@ -361,7 +364,7 @@ def make_pins(gold):
         model = W.eddington_model(teff, logg, ntau)
         state = load_state(atmname)
         extra = mk()
-        pgf = np.load(os.path.join(HERE, "atm_%s.npz" % atmname))["probe_loggf"]
+        pgf = np.load(os.path.join(DATA, "atm_%s.npz" % atmname))["probe_loggf"]
         probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
         merged = merge([probes, extra])
         with tempfile.TemporaryDirectory() as wd:
@@ -404,7 +407,7 @@ def make_linst_pins(gold):
         teff, logg, ntau, species, ismol, _, _, vmic, molbrd, _, _ = CONFIGS[atmname]
         model = W.eddington_model(teff, logg, ntau)
         extra = mk()
-        pgf = np.load(os.path.join(HERE, "atm_%s.npz" % atmname))["probe_loggf"]
+        pgf = np.load(os.path.join(DATA, "atm_%s.npz" % atmname))["probe_loggf"]
         probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
         merged = merge([probes, extra])
         with tempfile.TemporaryDirectory() as wd:
@@ -430,7 +433,7 @@ def make_mag_linst_pin(gold):
     grid = (6000.0, 6043.0, 0.002, 0)
     bfield = (2000.0, 60.0, 30.0)
     extra = W.zeeman_lines(60, 6040.3, 6042.7, W.SEED0 + 2)
-    pgf = np.load(os.path.join(HERE, "atm_magnetic.npz"))["probe_loggf"]
+    pgf = np.load(os.path.join(DATA, "atm_magnetic.npz"))["probe_loggf"]
     probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
     merged = merge([probes, extra])
     pats = zeeman_blocks(merged)
@@ -508,7 +511,7 @@ def make_mag_pin(gold):
     region = (6040.0, 6043.0)
     bfield = (2000.0, 60.0, 30.0)
     extra = W.zeeman_lines(60, 6040.3, 6042.7, W.SEED0 + 2)
-    pgf = np.load(os.path.join(HERE, "atm_magnetic.npz"))["probe_loggf"]
+    pgf = np.load(os.path.join(DATA, "atm_magnetic.npz"))["probe_loggf"]
     probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
     merged = merge([probes, extra])
     pats = zeeman_blocks(merged)
@@ -578,7 +581,7 @@ def make_sphere_pins(gold):
     model, radius, height = sphere_model(atmname)
     state = load_state(atmname)
     extra = mk()
-    pgf = np.load(os.path.join(HERE, "atm_%s.npz" % atmname))["probe_loggf"]
+    pgf = np.load(os.path.join(DATA, "atm_%s.npz" % atmname))["probe_loggf"]
     probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
     merged = merge([probes, extra])
     with tempfile.TemporaryDirectory() as wd:
@@ -616,7 +619,7 @@ def make_sphere_pins(gold):
     region = (6040.0, 6043.0)
     bfield = (1500.0, 800.0, -600.0)
     extra = W.zeeman_lines(60, 6040.3, 6042.7, W.SEED0 + 2)
-    pgf = np.load(os.path.join(HERE, "atm_magnetic.npz"))["probe_loggf"]
+    pgf = np.load(os.path.join(DATA, "atm_magnetic.npz"))["probe_loggf"]
     probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
     merged = merge([probes, extra])
     pats = zeeman_blocks(merged)
@@ -662,7 +665,7 @@ def make_h5_pin(gold):
     model = W.eddington_model(teff, logg, ntau)
     state = load_state(atmname)
     extra = mk()
-    pgf = np.load(os.path.join(HERE, "atm_%s.npz" % atmname))["probe_loggf"]
+    pgf = np.load(os.path.join(DATA, "atm_%s.npz" % atmname))["probe_loggf"]
     probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
     t = extra._txt
     with tempfile.TemporaryDirectory() as wd:
@@ -716,7 +719,7 @@ def make_zh5_pin(gold):
     region = (6040.0, 6043.0)
     bfield = (2000.0, 60.0, 30.0)
     extra, z = zh5_seeded()
-    pgf = np.load(os.path.join(HERE, "atm_magnetic.npz"))["probe_loggf"]
+    pgf = np.load(os.path.join(DATA, "atm_magnetic.npz"))["probe_loggf"]
     probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
     merged = merge([probes, extra])
     npr = probes.n
@@ -765,7 +768,7 @@ def make_mol_h5_pin(gold):
     model = W.eddington_model(teff, logg, ntau)
     state = load_state(atmname)
     extra = mk()
-    pgf = np.load(os.path.join(HERE, "atm_%s.npz" % atmname))["probe_loggf"]
+    pgf = np.load(os.path.join(DATA, "atm_%s.npz" % atmname))["probe_loggf"]
     probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
     t = extra._txt
     entries = []
@@ -954,7 +957,7 @@ def make_hot_he(gold):
     print("  pin: %d lines (%d matched), line opacity max rel %.2e" % (pin.n, int((ihe > 0).sum()), rel))
     kidx = np.unique(np.linspace(0, len(co["wave"]) - 1, 61).round().astype(int))
     np.savez_compressed(
-        os.path.join(HERE, "atm_hot.npz"), teff=HOT["teff"], logg=HOT["logg"],
+        os.path.join(DATA, "atm_hot.npz"), teff=HOT["teff"], logg=HOT["logg"],
         species=np.array(["%s %d" % s for s in species]), ismol=0, vmicro=HOT["vmic"], molbrd=HOT["molbrd"],
         rhox=state["rhox"], T=state["T"], xne=state["xne"], xna=state["xna"], rho=state["rho"],
         fractionpf=state["fractionpf"], xamass=state["xamass"], potion=state["potion"], ion=state["ion"],
@@ -976,7 +979,7 @@ def make_hot_he_mag(gold):
     9 angles, on 3855-3945 A at 0.05 A (pin_hot_he_mag.npz).  Pins the tabulated He I widths and shifts
     in the magnetic driver (MagLineOpacity1/2 with the per-depth shift, opacity.f90:391-520)."""
     d = np.load(os.path.join(REPO, "tests", "golden", "pin_hot_he.npz"))
-    a = np.load(os.path.join(HERE, "atm_hot.npz"))
+    a = np.load(os.path.join(DATA, "atm_hot.npz"))
     model = W.eddington_model(HOT["teff"], HOT["logg"], HOT["ntau"])
     state = load_state("hot")
     POTION[("He", 1)] = HE_POTION
@@ -1114,7 +1117,7 @@ def make_modes_pin(gold):
     abo = np.arange(3, base.n, 8)
     lgv[abo] = np.round(rng.uniform(200.0, 400.0, len(abo))) + np.round(rng.uniform(0.2, 0.4, len(abo)), 3)
     extra = W.LineList(species, base.wl, t["loggf"], t["elo"], t["lgrad"], lgq, lgv, base.spc, base.ismol)
-    pgf = np.load(os.path.join(HERE, "atm_%s.npz" % atmname))["probe_loggf"]
+    pgf = np.load(os.path.join(DATA, "atm_%s.npz" % atmname))["probe_loggf"]
     probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
     merged = merge([probes, extra])
     eps, vwf = 3e-3, 1.8
@@ -1157,7 +1160,7 @@ def update_h2(name="cooldwarf", h2brd=1.0):
     excess over the H2-free one, / (H2Brd * 0.874307), is the FP32 density.  The oracle must then
     reproduce the whole probe run with H2BRD."""
     teff, logg, ntau, species, ismol, wl0, dstep, vmic, molbrd, _, _ = CONFIGS[name]
-    path = os.path.join(HERE, "atm_%s.npz" % name)
+    path = os.path.join(DATA, "atm_%s.npz" % name)
     d = dict(np.load(path))
     model = W.eddington_model(teff, logg, ntau)
     state = load_state(name)
@@ -1210,7 +1213,7 @@ def make_mol_opts_pin(gold):
     model = W.eddington_model(teff, logg, ntau)
     state = load_state(atmname)
     extra = mk()
-    pgf = np.load(os.path.join(HERE, "atm_%s.npz" % atmname))["probe_loggf"]
+    pgf = np.load(os.path.join(DATA, "atm_%s.npz" % atmname))["probe_loggf"]
     probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
     merged = merge([probes, extra])
     h2brd, vwmol = 1.5, 4e-8
@@ -1251,7 +1254,7 @@ def update_potion():
     """Replace the guessed ionisation potentials of the atomic atmospheres' states with the recovered
     ones (atm_solar, atm_magnetic, atm_hot)."""
     for name in ("solar", "magnetic", "hot"):
-        path = os.path.join(HERE, "atm_%s.npz" % name)
+        path = os.path.join(DATA, "atm_%s.npz" % name)
         d = dict(np.load(path))
         if name == "hot":
             teff, logg, ntau, species, wl0, dstep, vmic, molbrd = (HOT["teff"], HOT["logg"], HOT["ntau"],

@@ -89,7 +89,7 @@ def test_stokes_errors(fsg, oracle_mod, prec):
     import fastspec_b200 as F
     from fastspec_b200 import workloads as W
     import sys
-    sys.path.insert(0, os.path.join(H.REPO, "fastspec_b200", "data"))
+    sys.path.insert(0, H.GOLD)
     from make_atmospheres import mirrored_components
     st, meta = H.load_atm("magnetic")
     w0, w1 = 6000.0, 6006.0

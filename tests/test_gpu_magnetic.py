@@ -42,7 +42,7 @@ def zeeman_case(n=60, w0=6040.0, span=3.0, seed=31, nmu=9):
             p = oracle.zeeman_pattern(1.0, 0.0, 1.0, 1.0)
         pats.append(p)
     import sys, os
-    sys.path.insert(0, os.path.join(H.REPO, "fastspec_b200", "data"))
+    sys.path.insert(0, H.GOLD)
     from make_atmospheres import mirrored_components
     return grid, st, co, L.arrays(), mirrored_components(pats)
 
@@ -260,7 +260,7 @@ def test_max_sizes_stokes_vs_oracle(fsg, oracle_mod):
     co = H.contopac_on(meta, F.make_grid(0, w0, w0 + span, 0.002) + w0)
     L = W.zeeman_lines(25, w0 + 0.2, w0 + span - 0.2, W.SEED0 + 77)
     import sys, os
-    sys.path.insert(0, os.path.join(H.REPO, "fastspec_b200", "data"))
+    sys.path.insert(0, H.GOLD)
     from make_atmospheres import mirrored_components
     jlo, jup, glo, gup = L.zeeman
     pats = []

@@ -6,7 +6,7 @@ write_hdf5_lines), on the CPU.
   parsed from the text sources the reference converted (tests/golden/hdf5_examples.npz, made by
   tests/golden/make_hdf5_golden.py).  Skipped where the reference tree is absent.
 * The writer: round trip, and the pin of the reference program reading a written file
-  (tests/golden/pin_solar_h5.npz, fastspec_b200/data/make_atmospheres.py h5): the oracle's atomic-list
+  (tests/golden/pin_solar_h5.npz, tests/golden/make_atmospheres.py h5): the oracle's atomic-list
   path on the list read back gives the reference's line opacity and spectra.
 """
 import os

@@ -1,5 +1,5 @@
 """The CPU oracle against the reference program's own outputs (fixtures in tests/golden and
-fastspec_b200/data, generated by fastspec_b200/data/make_atmospheres.py).
+fastspec_b200/data, generated by tests/golden/make_atmospheres.py).
 
 Tolerances: window indices are integers and must be identical; FP64 values differ only through
 libm ulps (the reference's gfortran build uses glibc's vectorised exp/log in some loops), which

@@ -1,6 +1,6 @@
 """Spherical geometry of the CPU oracle (SphereInit, LocPrfSph / DeloScalar, StokesPrfSph) against the
 reference program's own spherical runs (tests/golden/pin_sphere.npz, made by
-fastspec_b200/data/make_atmospheres.py sphere).
+tests/golden/make_atmospheres.py sphere).
 
 The fixture models are the solar-type and magnetic atmospheres written as spherical models whose
 radius makes the outermost Gauss-Legendre angle a grazing ray (6 and 2n points along it) while the
