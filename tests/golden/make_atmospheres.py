@@ -452,6 +452,62 @@ def make_mag_linst_pin(gold):
     print("pin_magnetic line strengths", int(sel.sum()), "of", extra.n, "seeded lines")
 
 
+def make_reentry_pin(gold):
+    """OPACITY= re-entry (ReadOpac, ioutils.f90:1878-1927; fastspec.f90:215): a line opacity file
+    written by fsio.write_opac, holding the ORACLE's line opacity of list A on the pin_solar grid, is
+    given to the reference program with list B; its output line opacity is the file plus B's opacity
+    (LineopCalc adds to the array ReadOpac filled).  Pins the file writer (the reference accepts the
+    grid and reads the array) and the accumulate-onto-loaded-opacity semantics
+    (pin_solar_reentry.npz: the region's output line opacity, continuum and flux, lists A and B)."""
+    name, atmname, mk, grid, region = pin_specs()[0]
+    teff, logg, ntau, species, ismol, _, _, vmic, molbrd, _, _ = CONFIGS[atmname]
+    model = W.eddington_model(teff, logg, ntau)
+    state = load_state(atmname)
+    la = W.atomic_lines(90, 5040.5, 5044.5, W.SEED0 + 43)
+    lb = W.atomic_lines(70, 5040.5, 5044.5, W.SEED0 + 44)
+    pgf = np.load(os.path.join(DATA, "atm_%s.npz" % atmname))["probe_loggf"]
+    probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
+    g = dict(wmode=grid[3], wstart=grid[0], wend=grid[1], dstep=grid[2])
+    with tempfile.TemporaryDirectory() as wd:
+        W.write_krz(os.path.join(wd, "model.krz"), model)
+        # continuum of the grid (probes only)
+        probes.write_z(os.path.join(wd, "p.z"), grid[0], grid[1])
+        run_ref(wd, "wave=%.4f, %.4f, %.6f, %d\nsave=0, 1, 1, 0, 0\nvmic=%.3f\nmolbrd=%d\n"
+                    "lines=\n-1  p.z\n\nmodel=model.krz\nmus=0\n" % (grid + (vmic, molbrd)))
+        lo0 = fsio.read_opac(os.path.join(wd, "fs_lineop.bin"))
+        co = fsio.read_opac(os.path.join(wd, "fs_contop.bin"))
+        S = oracle.State(g, state, contopac=co["opac"], vmicro=vmic, molbrd=molbrd)
+        ra = oracle.lineop_calc(S, oracle.Lines(**lines_args(la), kind=2), list_type=2)
+        fsio.write_opac(os.path.join(wd, "opac_a.bin"), lo0["wave"], ra["lineopac"], lo0["rhox"], lo0["T"],
+                        lo0["xne"], lo0["xna"], lo0["rho"])
+        merged = merge([probes, lb])
+        merged.write_z(os.path.join(wd, "lines.z"), grid[0], grid[1])
+        log = run_ref(wd, "wave=%.4f, %.4f, %.6f, %d\nsave=0, 1, 1, 1, 1\nvmic=%.3f\nmolbrd=%d\n"
+                          "opacity=opac_a.bin\nlines=\n-1  lines.z\n\nmodel=model.krz\nmus=7\n"
+                          % (grid + (vmic, molbrd)))
+        assert "Added line opacity from" in log, log
+        lo = fsio.read_opac(os.path.join(wd, "fs_lineop.bin"))
+        sp = fsio.read_spec(os.path.join(wd, "fs_spec.bin"))
+        fl = fsio.read_flux(os.path.join(wd, "fs_flux.bin"))
+    for k in ("rhox", "T", "xne", "xna", "rho"):
+        assert np.array_equal(lo[k], state[k]), "EOS state differs from the recovered one: " + k
+    wave = lo["wave"]
+    sel = (wave >= region[0] - 1e-9) & (wave <= region[1] + 1e-9)
+    i0, i1 = (int(x) for x in np.nonzero(sel)[0][[0, -1]])
+    rb = oracle.lineop_calc(S, oracle.Lines(**lines_args(lb), kind=2), list_type=2, lineopac=ra["lineopac"].copy())
+    ref = lo["opac"][i0:i1 + 1]
+    m = ref > 0
+    mine = rb["lineopac"][i0:i1 + 1]
+    print("  re-entry pin: pattern equal %s, line opacity max rel %.2e"
+          % (np.array_equal(mine > 0, m), np.max(np.abs(mine[m] / ref[m] - 1))))
+    A, B = la.arrays(), lb.arrays()
+    np.savez_compressed(
+        os.path.join(gold, "pin_solar_reentry.npz"), grid=np.array(grid, np.float64), i0=i0, i1=i1,
+        atm=atmname, vmicro=vmic, molbrd=molbrd, contopac=co["opac"][i0:i1 + 1], lineopac=ref,
+        wave=wave[i0:i1 + 1], xmu=sp["xmu"], sfl=fl["sfl"][i0:i1 + 1], sfc=fl["sfc"][i0:i1 + 1],
+        **{"a_" + k: v for k, v in A.items()}, **{"line_" + k: v for k, v in B.items()})
+
+
 def make_convol_pin(gold):
     """Broadening fixtures: the reference's intensities (fs_spec.bin) and its broadened flux
     (fs_flux.bin, IntegConvol / DiskInteg with CONVOL = Vsini, Vmacro, Vgau) of the same run, for
@@ -1297,6 +1353,8 @@ if __name__ == "__main__":
         make_mag_pin(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "convol":
         make_convol_pin(os.path.join(REPO, "tests", "golden"))
+    elif len(sys.argv) > 1 and sys.argv[1] == "reentry":
+        make_reentry_pin(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "maglinst":
         make_mag_linst_pin(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "linst":

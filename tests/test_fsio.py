@@ -64,3 +64,27 @@ def test_line_strength_file_round_trip(tmp_path):
         fsio.write_linst(out, r["species"][sl], r["ion"][sl], r["wave"][sl], r["strength"][sl], append=k > 0)
         a += n
     assert open(out, "rb").read() == g["linst"]
+
+
+def test_opacity_reentry_pin_reference(oracle_mod, tmp_path):
+    """OPACITY= re-entry: the reference program read a file that fsio.write_opac wrote (the oracle's line
+    opacity of list A on the pin_solar grid) and added list B (tests/golden/pin_solar_reentry.npz).  The
+    same steps here: the oracle's A, written and read back through fsio, then B accumulated onto it."""
+    from fastspec_b200 import fsio
+    d = H.load_pin("pin_solar_reentry")
+    grid, st, meta, co = H.pin_setup(d)
+    S = oracle_mod.State(grid, st, contopac=co, vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]))
+    A = {k[2:]: d[k] for k in d if k.startswith("a_")}
+    ra = oracle_mod.lineop_calc(S, oracle_mod.Lines(**A, kind=2), list_type=2)
+    p = str(tmp_path / "opac_a.bin")
+    wave = S.wave + S.wfirst
+    fsio.write_opac(p, wave, ra["lineopac"], st["rhox"], st["T"], st["xne"], st["xna"], st["rho"])
+    back = fsio.read_opac(p)
+    assert np.array_equal(back["opac"], ra["lineopac"]) and np.array_equal(back["wave"], wave)
+    rb = oracle_mod.lineop_calc(S, oracle_mod.Lines(**H.pin_lines(d), kind=2), list_type=2,
+                                lineopac=back["opac"].copy())
+    i0, i1 = int(d["i0"]), int(d["i1"])
+    lo, ref = rb["lineopac"][i0:i1 + 1], d["lineopac"]
+    assert np.array_equal(lo > 0, ref > 0)
+    m = ref > 0
+    assert np.max(np.abs(lo[m] / ref[m] - 1)) < 1e-8

@@ -456,6 +456,35 @@ def test_molecular_options_against_reference_pin(fsg, prec):
 
 
 @pytest.mark.parametrize("prec", ["mixed", "fp64"])
+def test_opacity_reentry_against_reference_pin(fsg, tmp_path, prec):
+    """OPACITY= re-entry through the library: list A's device line opacity (fsg_lineop_get) written by
+    fsio.write_opac and read back, loaded into a fresh context (fsg_lineop_set), list B accumulated onto
+    it; the reference program did the same with the file of the oracle's A
+    (tests/golden/pin_solar_reentry.npz).  FP64 1e-8; mixed 4e-6 (two lists, each within the 2e-6 bar)."""
+    from fastspec_b200 import fsio
+    d = H.load_pin("pin_solar_reentry")
+    grid, st, meta, co = H.pin_setup(d)
+    prc = fsg.PREC_MIXED if prec == "mixed" else fsg.PREC_FP64
+    C = ctx_for(fsg, grid, st, co, prc, vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]))
+    A = {k[2:]: d[k] for k in d if k.startswith("a_")}
+    C.lineop_calc(fsg.LineList.from_arrays(A), want_lines=False)
+    p = str(tmp_path / "opac_a.bin")
+    fsio.write_opac(p, C.wave + C.wfirst, C.lineop_get(), st["rhox"], st["T"], st["xne"], st["xna"], st["rho"])
+    C2 = ctx_for(fsg, grid, st, co, prc, vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]))
+    C2.lineop_set(fsio.read_opac(p)["opac"])
+    g = C2.lineop_calc(fsg.LineList.from_arrays(H.pin_lines(d)))
+    i0, i1 = int(d["i0"]), int(d["i1"])
+    lo, ref = g["lineopac"][i0:i1 + 1], d["lineopac"]
+    assert np.array_equal(lo > 0, ref > 0)
+    if prec == "fp64":
+        assert np.max(np.abs(lo[ref > 0] / ref[ref > 0] - 1)) < 1e-8
+    else:
+        assert np.max(np.abs(lo - ref) / (ref + d["contopac"])) < 4e-6
+    spl, spc, sfl, sfc = C2.radtran()
+    assert np.max(np.abs(sfl[i0:i1 + 1] / d["sfl"] - 1)) < (1e-8 if prec == "fp64" else 1e-5)
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp64"])
 def test_hot_he_lines_against_reference_pin(fsg, prec):
     """Tabulated He I Stark lines in a Teff 15000 K atmosphere (hestark.f90): Context.hestark_init builds
     the 37 lines' widths and shifts on the host (fsg_hestark_tables) and the lists' table entries come
