@@ -198,6 +198,54 @@ def mu_quadrature(quad, n, x=None):
     return x, w, r
 
 
+def mu_quad_type(xmu):
+    """MuQuadType (utils.f90:1337-1354): the quadrature (1 Gauss-Legendre, 2 Gauss-Radau) whose nodes
+    are the given angles to 1e-6, else 0 (also for fewer than two angles)."""
+    xmu = _f64(xmu)
+    n = len(xmu)
+    if n < 2:
+        return 0
+    for q in (1, 2):
+        xg, _, _ = mu_quadrature(q, n)
+        if np.max(np.abs(xmu - xg)) < 1e-6:
+            return q
+    return 0
+
+
+def convolve_spec_file(spec_path, vsini, vmacro, vgau, flux_path=None, device=0):
+    """The reference's post-processing mode (`fastspec <fs_spec.bin> Vsini Vmacro Vgau`,
+    fastspec.f90:75-134): read the intensities (ReadSpec's grid and angle order, fsio.spec_grid), take
+    the quadrature from the angles (MuQuadType), disk-integrate with rotation, radial-tangential
+    macroturbulence and Gaussian broadening on the device (fsg_disk_integ_conv_dev; Vgau above 1000 is
+    a resolving power) and return (wave, sfl, sfc); with flux_path, also write fs_flux.bin there."""
+    import torch
+    from . import fsio
+    if vsini < 0 or vmacro < 0 or vgau < 0:
+        raise FsgError("convolve_spec_file: invalid convolution parameters")
+    g = fsio.spec_grid(fsio.read_spec(spec_path))
+    nmu = len(g["xmu"])
+    x, w, r = mu_quadrature(mu_quad_type(g["xmu"]), nmu, x=g["xmu"])
+    C = Context(device=device)
+    try:
+        C.set_grid(g["wmode"], g["wstart"], g["wend"], g["dstep"], wave=g["wave"])
+        C.set_mu(x, w)
+        dev = torch.device("cuda", device)
+        spl = torch.from_numpy(g["spl"]).to(dev)
+        spc = torch.from_numpy(g["spc"]).to(dev)
+        sfl = torch.empty(len(g["wave"]), dtype=torch.float64, device=dev)
+        sfc = torch.empty_like(sfl)
+        torch.cuda.synchronize(dev)
+        C.disk_integ_conv_dev(r, float(vsini), float(vmacro), float(vgau), spl.data_ptr(), spc.data_ptr(),
+                              sfl.data_ptr(), sfc.data_ptr())
+        sfl, sfc = sfl.cpu().numpy(), sfc.cpu().numpy()
+    finally:
+        C.close()
+    wave = g["wave"] + g["wstart"]
+    if flux_path is not None:
+        fsio.write_flux(flux_path, wave, sfl, sfc)
+    return wave, sfl, sfc
+
+
 def zeeman_pattern(jlo, jup, glo, gup):
     m = int(round(2 * jup)) + 1
     npi, nsi = C.c_int32(), C.c_int32()

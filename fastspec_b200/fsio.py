@@ -71,6 +71,35 @@ def write_spec(path, wave, xmu, spl, spc, spz=None):
                 np.ascontiguousarray(spz[:, q, :]).tofile(f)
 
 
+def spec_grid(spec):
+    """The grid and angles ReadSpec (ioutils.f90:1930-1984) derives from an intensity file read by
+    read_spec: the angles in descending order (its exchange sort, the spectra permuted alike), Wfirst =
+    the first wavelength, offsets from it, and the step and mode (Wmode 1 with a velocity step when the
+    first and last steps differ by more than 1e-6 A, else Wmode 0 with the first step).  Returns
+    dict(wmode, wstart, wend, dstep, wave (offsets), xmu, spl, spc)."""
+    xmu = np.asarray(spec["xmu"], np.float64)
+    n = len(xmu)
+    perm = list(range(n))
+    for i in range(n - 1):
+        for j in range(i + 1, n):
+            if xmu[perm[j]] > xmu[perm[i]]:
+                perm[i], perm[j] = perm[j], perm[i]
+    wave_abs = np.asarray(spec["wave"], np.float64)
+    if len(wave_abs) < 2 or n < 1:
+        raise ValueError("intensity file needs two wavelengths and one angle")
+    wfirst = float(wave_abs[0])
+    wave = wave_abs - wfirst
+    if abs((wave[1] - wave[0]) - (wave[-1] - wave[-2])) > 1e-6:
+        dstep = 2.0 * (wave[1] - wave[0]) / (wave[0] + wave[1] + 2.0 * wfirst) * 299792.458
+        wmode = 1
+    else:
+        dstep = wave[1] - wave[0]
+        wmode = 0
+    return dict(wmode=wmode, wstart=wfirst, wend=float(wave_abs[-1]), dstep=float(dstep), wave=wave,
+                xmu=xmu[perm], spl=np.ascontiguousarray(spec["spl"][:, perm]),
+                spc=np.ascontiguousarray(spec["spc"][:, perm]))
+
+
 def read_flux(path):
     with open(path, "rb") as f:
         nwl = int(np.fromfile(f, "<i4", 1)[0])

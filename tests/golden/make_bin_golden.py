@@ -4,7 +4,8 @@
 Runs the reference's shipped executable (this container only) on two tiny decks with the solar
 model: (1) two ASCII line lists, SAVE=1,1,1,1,1 (line and continuum opacity, intensities, flux and
 the line strengths of both lists); (2) a Zeeman list in a 2 kG field, SAVE=0,0,1,1,1 (Stokes
-intensities and flux).  The files' bytes go to tests/golden/fs_outputs.npz, which is committed.
+intensities and flux); and the post-processing mode (fastspec <fs_spec.bin> Vsini Vmacro Vgau) on
+each intensity file (broadened flux).  The files' bytes go to tests/golden/fs_outputs.npz, which is committed.
 """
 import os
 import subprocess
@@ -20,6 +21,8 @@ from fastspec_b200 import workloads as W  # noqa: E402
 
 BIN = "/root/reference/src/fastspec_Linux_x86_64"
 OUT = os.path.join(HERE, "fs_outputs.npz")
+# post-processing runs (Vsini, Vmacro, Vgau) on the two intensity files: a resolving power, a FWHM
+CONV = {"conv_a": (15.0, 3.0, 60000.0), "conv_b": (5.0, 0.0, 2.5)}
 
 
 def run(wd, deck):
@@ -28,6 +31,14 @@ def run(wd, deck):
     r = subprocess.run([BIN, "in.dat"], cwd=wd, capture_output=True, text=True)
     if r.returncode != 0 or "Total time" not in r.stdout:
         raise RuntimeError(r.stdout + r.stderr)
+
+
+def convolve(wd, spec, vsini, vmacro, vgau):
+    """The post-processing mode: fastspec <intensity file> Vsini Vmacro Vgau -> fs_flux.bin."""
+    r = subprocess.run([BIN, spec, "%g" % vsini, "%g" % vmacro, "%g" % vgau], cwd=wd, capture_output=True, text=True)
+    if r.returncode != 0 or "Convolution and disk-integration" not in r.stdout:
+        raise RuntimeError(r.stdout + r.stderr)
+    return raw(wd, "fs_flux.bin")
 
 
 def raw(wd, name):
@@ -49,6 +60,7 @@ def main():
         for k, f in (("lineop", "fs_lineop.bin"), ("contop", "fs_contop.bin"), ("spec", "fs_spec.bin"),
                      ("flux", "fs_flux.bin"), ("linst", "fs_linst.bin")):
             out[k] = raw(wd, f)
+        out["conv_a"] = convolve(wd, "fs_spec.bin", *CONV["conv_a"])
     with tempfile.TemporaryDirectory() as wd:
         W.write_krz(os.path.join(wd, "model.krz"), model)
         z = W.zeeman_lines(6, 6000.1, 6000.9, W.SEED0 + 72)
@@ -60,6 +72,7 @@ def main():
                 "lines=\n-1  z.z\n\nmodel=model.krz\nmus=3\nbframe=1\nbfield=2000, 60, 30\n")
         out["spec_mag"] = raw(wd, "fs_spec.bin")
         out["flux_mag"] = raw(wd, "fs_flux.bin")
+        out["conv_b"] = convolve(wd, "fs_spec.bin", *CONV["conv_b"])
     np.savez_compressed(OUT, **out)
     print(OUT, {k: v.size for k, v in out.items()})
 

@@ -88,3 +88,40 @@ def test_opacity_reentry_pin_reference(oracle_mod, tmp_path):
     assert np.array_equal(lo > 0, ref > 0)
     m = ref > 0
     assert np.max(np.abs(lo[m] / ref[m] - 1)) < 1e-8
+
+
+CONV = {"conv_a": ("spec", 15.0, 3.0, 60000.0), "conv_b": ("spec_mag", 5.0, 0.0, 2.5)}
+
+
+def test_post_processing_mode_oracle(fsg, oracle_mod, tmp_path):
+    """The reference's post-processing mode (fastspec <fs_spec.bin> Vsini Vmacro Vgau,
+    fastspec.f90:75-134) on two of its intensity files: ReadSpec's grid and angle order (fsio.spec_grid),
+    the quadrature from the angles (mu_quad_type) and the oracle's broadened disk integration give the
+    reference's fs_flux.bin."""
+    from fastspec_b200 import fsio
+    g = golden()
+    for key, (spec, vs, vm, vg) in CONV.items():
+        s = fsio.spec_grid(fsio.read_spec(put(tmp_path, spec + ".bin", g[spec])))
+        assert s["wmode"] == 0 and list(s["xmu"]) == sorted(s["xmu"], reverse=True)
+        assert fsg.mu_quad_type(s["xmu"]) == 1
+        x, w, r = fsg.mu_quadrature(1, len(s["xmu"]), x=s["xmu"])
+        grid = dict(wmode=s["wmode"], wstart=s["wstart"], wend=s["wend"], dstep=s["dstep"])
+        wave = s["wave"] + s["wstart"]
+        sfl, sfc = oracle_mod.disk_integ_conv(x, w, r, s["spl"], s["spc"], oracle_mod.grid_dv(grid, wave), vs, vm,
+                                              oracle_mod.gauss_sigma_pix(grid, wave, vg))
+        ref = fsio.read_flux(put(tmp_path, key + ".bin", g[key]))
+        assert np.array_equal(ref["wave"], wave)
+        assert np.max(np.abs(sfl / ref["sfl"] - 1)) < 1e-12
+        assert np.max(np.abs(sfc / ref["sfc"] - 1)) < 1e-12
+
+
+def test_spec_grid_orders_angles_and_detects_log_grids():
+    from fastspec_b200 import fsio
+    wave = 5000.0 * np.exp(np.arange(6) * 1e-5)
+    spl = np.arange(18, dtype=float).reshape(6, 3)
+    s = fsio.spec_grid(dict(xmu=np.array([0.2, 0.9, 0.5]), wave=wave, spl=spl, spc=spl + 100))
+    assert s["wmode"] == 1 and abs(s["dstep"] - 1e-5 * 299792.458) < 1e-6
+    assert list(s["xmu"]) == [0.9, 0.5, 0.2] and list(s["spl"][0]) == [1.0, 2.0, 0.0]
+    u = fsio.spec_grid(dict(xmu=np.array([1.0]), wave=5000.0 + 0.01 * np.arange(4), spl=np.zeros((4, 1)),
+                            spc=np.ones((4, 1))))
+    assert u["wmode"] == 0 and abs(u["dstep"] - 0.01) < 1e-12

@@ -58,3 +58,30 @@ def test_synthesis_with_broadening_vs_oracle(fsg, oracle_mod):
                                             oracle_mod.gauss_sigma_pix(grid, wave, 80000.0))
     assert np.max(np.abs(sfl / osfl - 1)) < 1e-9
     assert np.max(np.abs(sfc / osfc - 1)) < 1e-9
+
+
+@pytest.mark.parametrize("key", ["conv_a", "conv_b"])
+def test_convolve_spec_file_against_reference(fsg, tmp_path, key):
+    """fastspec_b200.convolve_spec_file, the post-processing mode on the device, against the reference's
+    own run of it on the same intensity file (tests/golden/fs_outputs.npz); writes fs_flux.bin."""
+    from fastspec_b200 import fsio
+    d = np.load(H.GOLD + "/fs_outputs.npz")
+    spec, vs, vm, vg = {"conv_a": ("spec", 15.0, 3.0, 60000.0), "conv_b": ("spec_mag", 5.0, 0.0, 2.5)}[key]
+    sp = str(tmp_path / "fs_spec.bin")
+    with open(sp, "wb") as f:
+        f.write(d[spec].tobytes())
+    out = str(tmp_path / "fs_flux.bin")
+    wave, sfl, sfc = fsg.convolve_spec_file(sp, vs, vm, vg, flux_path=out)
+    ref = fsio.read_flux(_put(tmp_path, d[key].tobytes()))
+    assert np.array_equal(wave, ref["wave"])
+    assert np.max(np.abs(sfl / ref["sfl"] - 1)) < 1e-12
+    assert np.max(np.abs(sfc / ref["sfc"] - 1)) < 1e-12
+    back = fsio.read_flux(out)
+    assert np.array_equal(back["sfl"], sfl) and np.array_equal(back["wave"], wave)
+
+
+def _put(tmp_path, data):
+    p = str(tmp_path / "ref_flux.bin")
+    with open(p, "wb") as f:
+        f.write(data)
+    return p
