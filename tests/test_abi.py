@@ -62,3 +62,15 @@ def test_zeeman_pattern_matches_oracle(fsg, oracle_mod):
         b = oracle_mod.zeeman_pattern(jlo, jup, glo, gup)
         for x, y in zip(a, b):
             assert np.array_equal(x, y)
+
+
+def test_mu_quad_type(fsg):
+    """MuQuadType (utils.f90:1337-1354): which rule the angles of an intensity file follow."""
+    for q in (1, 2):
+        for n in (2, 5, 9):
+            x, _, _ = fsg.mu_quadrature(q, n)
+            assert fsg.mu_quad_type(x) == q
+            assert fsg.mu_quad_type(x + 2e-6) == 0
+    assert fsg.mu_quad_type([1.0]) == 0
+    assert fsg.mu_quad_type([0.9, 0.5, 0.1]) == 0
+

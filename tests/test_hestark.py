@@ -116,3 +116,18 @@ def test_oracle_hot_he_magnetic_pin_reference(fsg, oracle_mod):
     x, w, _ = oracle_mod.mu_quadrature(1, len(d["xmu"]))
     sfl, _ = oracle_mod.disk_integ(w, spz[:, 0], spc)
     assert np.max(np.abs(sfl / d["sfl"] - 1)) < 1e-8
+
+
+def test_line_list_table_match_column(fsg):
+    """Context.lineop_calc after hestark_init passes a copy of the list with the ihe column of
+    fsg_he_match_idx (host logic; the caller's list keeps no column, an explicit column wins)."""
+    d = H.load_pin("pin_hot_he")
+    a = H.pin_lines(d)
+    L = fsg.LineList.from_arrays(a)
+    M = L._with_he_match(0, 3855.0)
+    assert not L.c.ihe and M.c.ihe and M.n == L.n
+    got = np.ctypeslib.as_array(M.c.ihe, shape=(M.n,))
+    assert np.array_equal(got, d["ihe_expected"])
+    assert M._keep["wl"] is L._keep["wl"]                       # the other columns are shared, not copied
+    E = fsg.LineList.from_arrays(dict(a, ihe=np.zeros(len(a["wl"]), np.int32)))
+    assert E._with_he_match(0, 3855.0) is E
