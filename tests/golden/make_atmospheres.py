@@ -424,6 +424,52 @@ def make_linst_pins(gold):
         print(name, "line strengths", int(sel.sum()), "of", extra.n, "seeded lines")
 
 
+MAG_FRAMES = {
+    # stellar frame: (Br, Bm, Bp) projected at each disk position (synth.f90:1960-1980)
+    0: (1500.0, 800.0, -600.0),
+    # observer frame per angle: |B| then (gamma, psi) for each of the 9 angles (synth.f90:1948-1959)
+    2: (2500.0,) + tuple(v for k in range(9) for v in (10.0 + 17.0 * k, -40.0 + 11.0 * k)),
+}
+
+
+def make_mag_frames_pin(gold):
+    """Stokes IQUV of the pin_magnetic list with the field in the stellar frame (BFRAME 0) and given per
+    angle in the observer frame (BFRAME 2), 9 angles, plane-parallel (pin_magnetic_frames.npz; the
+    BFRAME 1 run is pin_magnetic.npz)."""
+    teff, logg, ntau, species, ismol, _, _, vmic, molbrd, _, _ = CONFIGS["magnetic"]
+    model = W.eddington_model(teff, logg, ntau)
+    state = load_state("magnetic")
+    grid = (6000.0, 6043.0, 0.002, 0)
+    region = (6040.0, 6043.0)
+    extra = W.zeeman_lines(60, 6040.3, 6042.7, W.SEED0 + 2)
+    pgf = np.load(os.path.join(DATA, "atm_magnetic.npz"))["probe_loggf"]
+    probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
+    merged = merge([probes, extra])
+    pats = zeeman_blocks(merged)
+    out = {}
+    for frame, bfield in MAG_FRAMES.items():
+        with tempfile.TemporaryDirectory() as wd:
+            W.write_krz(os.path.join(wd, "model.krz"), model)
+            merged.write_z(os.path.join(wd, "lines.z"), grid[0], grid[1], patterns=pats)
+            deck = ("wave=%.4f, %.4f, %.6f, %d\nsave=0, 0, 1, 1, 1\nvmic=%.3f\nmolbrd=%d\n"
+                    "lines=\n-1  lines.z\n\nmodel=model.krz\nmus=9\nbframe=%d\nbfield=%s\n"
+                    % (grid + (vmic, molbrd, frame, ", ".join("%g" % v for v in bfield))))
+            log = run_ref(wd, deck)
+            assert "polarised" in log, log
+            co = fsio.read_opac(os.path.join(wd, "fs_contop.bin"))
+            sp = fsio.read_spec(os.path.join(wd, "fs_spec.bin"))
+            fl = fsio.read_flux(os.path.join(wd, "fs_flux.bin"))
+        for k in ("rhox", "T", "xne", "xna", "rho"):
+            assert np.array_equal(co[k], state[k]), "EOS state differs from the recovered one: " + k
+        wave = co["wave"]
+        sel = (wave >= region[0] - 1e-9) & (wave <= region[1] + 1e-9)
+        i0, i1 = (int(x) for x in np.nonzero(sel)[0][[0, -1]])
+        out.update({"f%d_bfield" % frame: np.array(bfield), "f%d_spz" % frame: sp["spz"][i0:i1 + 1],
+                    "f%d_spc" % frame: sp["spc"][i0:i1 + 1], "f%d_sfl" % frame: fl["sfl"][i0:i1 + 1]})
+    np.savez_compressed(os.path.join(gold, "pin_magnetic_frames.npz"), i0=i0, i1=i1, xmu=sp["xmu"], **out)
+    print("pin_magnetic_frames: frames", list(MAG_FRAMES), "region pixels", i1 - i0 + 1)
+
+
 def make_mag_linst_pin(gold):
     """Line strengths of the magnetic driver (MagLineopCalc with SAVE flag 1, synth.f90:1098-1455): the
     pin_magnetic deck with BFRAME 1 and the explicit Zeeman patterns, its fs_linst.bin restricted to the
@@ -1355,6 +1401,8 @@ if __name__ == "__main__":
         make_convol_pin(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "reentry":
         make_reentry_pin(os.path.join(REPO, "tests", "golden"))
+    elif len(sys.argv) > 1 and sys.argv[1] == "magframes":
+        make_mag_frames_pin(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "maglinst":
         make_mag_linst_pin(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "linst":

@@ -106,6 +106,26 @@ def test_mag_against_reference_pin(fsg):
     assert np.max(np.abs(sfc[i0:i1 + 1] / d["sfc"] - 1)) < 1e-8
 
 
+@pytest.mark.parametrize("frame", [0, 2])
+def test_mag_frames_against_reference_pin(fsg, frame):
+    """The stellar-frame (BFRAME 0) and per-angle (BFRAME 2) field geometries on the GPU FP64 path against
+    the reference's Stokes IQUV (tests/golden/pin_magnetic_frames.npz); 1e-8 of Ic as for BFRAME 1."""
+    d = H.load_pin("pin_magnetic")
+    f = H.load_pin("pin_magnetic_frames")
+    grid, st, co, lines, z = H.mag_pin_setup(d)
+    C, x, w = mag_ctx(fsg, grid, st, co, nmu=len(f["xmu"]), vmicro=float(d["vmicro"]))
+    assert np.array_equal(x, f["xmu"])
+    bfield = f["f%d_bfield" % frame]
+    C.mag_lineop_calc(fsg.LineList.from_arrays(lines, zeeman=z), frame, bfield, want=False)
+    spz, spc, sfl, sfc = C.mag_radtran(frame, bfield)
+    i0, i1 = int(f["i0"]), int(f["i1"])
+    ref, ic = f["f%d_spz" % frame], f["f%d_spc" % frame]
+    assert np.max(np.abs(spz[i0:i1 + 1, 0] / ref[:, 0] - 1)) < 1e-8
+    for q in (1, 2, 3):
+        assert np.max(np.abs(spz[i0:i1 + 1, q] - ref[:, q]) / ic) < 1e-8
+    assert np.max(np.abs(sfl[i0:i1 + 1] / f["f%d_sfl" % frame] - 1)) < 1e-8
+
+
 def test_mag_linstr_against_reference_pin(fsg):
     """Line strengths of the magnetic driver on the GPU against the reference's fs_linst.bin for the
     pin_magnetic deck (tests/golden/pin_magnetic_linst.npz)."""

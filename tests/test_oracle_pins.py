@@ -122,6 +122,29 @@ def test_oracle_linstr_pins_reference(oracle_mod, name):
     assert np.all(ref["strength"] > 0)
 
 
+@pytest.mark.parametrize("frame", [0, 2])
+def test_oracle_magnetic_frames_pin_reference(oracle_mod, frame):
+    """MagRadTranCalc's other field frames (synth.f90:1948-1980): the stellar-frame field projected at
+    each disk position (BFRAME 0) and per-angle observer-frame angles (BFRAME 2), on the pin_magnetic
+    list, against the reference's Stokes IQUV (tests/golden/pin_magnetic_frames.npz)."""
+    d = H.load_pin("pin_magnetic")
+    f = H.load_pin("pin_magnetic_frames")
+    grid, st, co, lines, z = H.mag_pin_setup(d)
+    S = oracle_mod.State(grid, st, contopac=co, vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]))
+    bfield = f["f%d_bfield" % frame]
+    r = oracle_mod.mag_lineop_calc(S, oracle_mod.Lines(**lines, kind=2, zeeman=z), frame, bfield)
+    spz, spc = oracle_mod.mag_radtran(S, f["xmu"], frame, bfield, np.zeros((S.nwl, S.ntau)), r["maglineopac"])
+    i0, i1 = int(f["i0"]), int(f["i1"])
+    ref, ic = f["f%d_spz" % frame], f["f%d_spc" % frame]
+    assert np.max(np.abs(spz[i0:i1 + 1, 0] / ref[:, 0] - 1)) < 1e-8
+    for q in (1, 2, 3):
+        assert np.max(np.abs(spz[i0:i1 + 1, q] - ref[:, q]) / ic) < 1e-8
+        assert np.max(np.abs(ref[:, q]) / ic) > 1e-5                 # the field polarises every parameter
+    x, w, _ = oracle_mod.mu_quadrature(1, len(f["xmu"]))
+    sfl, _ = oracle_mod.disk_integ(w, spz[i0:i1 + 1, 0], spc[i0:i1 + 1])
+    assert np.max(np.abs(sfl / f["f%d_sfl" % frame] - 1)) < 1e-8
+
+
 def test_oracle_magnetic_linstr_pin_reference(oracle_mod):
     """Line strengths from the magnetic driver (MagLineopCalc, SAVE flag 1) against the reference's
     fs_linst.bin for the pin_magnetic deck (9 angles, BFRAME 1)."""
