@@ -172,8 +172,9 @@ def run_batch(backend, costs, sizes, group=None, device=None):
     """Batch-axis sharding.  costs[i] and sizes[i] (wavelength count) of every synthesis are known on
     every rank; rank r runs batch_partition's share r through backend.synthesize(indices), which returns
     one float64 [2, sizes[i]] tensor (line+continuum flux, continuum flux) per index, on `device`.  The
-    shares are packed, padded to the longest, and gathered to rank 0 (one collective).  Returns (list of
-    [2, sizes[i]] tensors in the original order on rank 0, None on the other ranks; this rank's indices)."""
+    shares are packed, padded to the longest, and gathered to rank 0 (one collective) in a buffer on
+    `device` (a CUDA device under NCCL; the host under gloo).  Returns (list of [2, sizes[i]] tensors in
+    the original order on rank 0, None on the other ranks; this rank's indices)."""
     world = dist.get_world_size(group)
     rank = dist.get_rank(group)
     parts = batch_partition(costs, world)
