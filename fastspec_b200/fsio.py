@@ -151,9 +151,32 @@ def write_linst(path, species, ion, wave, strength, append=False):
 MAXION = 5      # highest ionisation stage the reference's EOS supports (lines above it are dropped)
 
 
-def read_hdf5_lines(path, species, exact=True):
-    """A FastSpec HDF5 line list as the library's SoA records, converted as ReadHDF converts them
-    (ioutils.f90:889-1000 atomic / Zeeman, 790-812 molecular): gf = 10.0**LGGF; atomic Grad =
+def vac2air(lam):
+    """Vac2Air (utils.f90:1007-1017): vacuum to air wavelength [A] above 2000 A, unchanged below."""
+    lam = np.asarray(lam, np.float64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        s = 1e4 / lam
+        s2 = s * s
+        n = 1.0 + 8.34254e-5 + 2.406147e-2 / (130.0 - s2) + 1.5998e-4 / (38.9 - s2)
+        return np.where(lam > 2000.0, lam / n, lam)
+
+
+def _lower_bound(a, x):
+    """LowerBoundReal8 (utils.f90:702-718): first 1-based i with a(i) >= x (n + 1 if none)."""
+    return int(np.searchsorted(a, x, side="left")) + 1
+
+
+def _upper_bound(a, x):
+    """UpperBoundReal8 (utils.f90:721-737): last 1-based i with a(i) <= x (0 if none)."""
+    return int(np.searchsorted(a, x, side="right"))
+
+
+def read_hdf5_lines(path, species, exact=True, wstart=None, wend=None):
+    """A FastSpec HDF5 line list as the library's SoA records, selected and converted as ReadHDF does
+    (ioutils.f90:686-790): wavelengths of a list with WL_VAC = 1 turned to air (Vac2Air); the column
+    must be sorted (ValueError otherwise, where ReadHDF stops); with wstart / wend (the synthesis range,
+    WAVE=) only the lines with wstart <= W <= wend are kept, as the reader's bound search does.  Then
+    the record conversions (ioutils.f90:889-1000 atomic / Zeeman, 790-812 molecular): gf = 10.0**LGGF; atomic Grad =
     10.0**GRAD for 0 < GRAD < 20, Gqst / Gvdw = 10.0**x for x < 0 (a positive GVDW is the packed ABO
     parameter), all in single precision (libm powf when exact, numpy's power otherwise); atomic lines
     above ionisation stage 5 are dropped.  Molecular single-species lists take GRAD as stored and no
@@ -167,6 +190,16 @@ def read_hdf5_lines(path, species, exact=True):
     from . import hdf5
     from .workloads import pow10f
     cols, attrs, _ = hdf5.read_lines(path)
+    w = np.asarray(cols["W"], np.float64)
+    if int(attrs.get("WL_VAC", 0)) == 1:
+        w = vac2air(w)
+    if not np.all(w[:-1] <= w[1:]):
+        raise ValueError("read_hdf5_lines: wavelength array is not sorted in " + str(path))
+    i1 = 1 if wstart is None else _lower_bound(w, wstart)
+    i2 = len(w) if wend is None else _upper_bound(w, wend)
+    sel = slice(i1 - 1, max(i2, i1 - 1))
+    cols = {k: np.asarray(v)[sel] for k, v in cols.items()}
+    cols["W"] = w[sel]
     p10 = pow10f if exact else (lambda v: np.power(np.float32(10.0), np.asarray(v, np.float32)).astype(np.float32))
     f32 = lambda a: np.asarray(a, np.float32)
     table = {(str(n), int(i)): k for k, (n, i) in enumerate(species)}

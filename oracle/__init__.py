@@ -374,6 +374,11 @@ def sphere_init(rhox, height, radius, xmu):
     return out
 
 
+def air2vac(lam):
+    """Air2Vac (utils.f90:1020-1032) of one wavelength [A]."""
+    return float(lib().or_air2vac(float(lam)))
+
+
 HE_NTAB = 37
 
 

@@ -799,6 +799,63 @@ def make_h5_pin(gold):
     print("pin_solar_h5: region pixels", i1 - i0 + 1, "lines", extra.n)
 
 
+def air2vac(lam):
+    """Air2Vac (utils.f90:1020-1032) on an array."""
+    return np.array([oracle.air2vac(float(x)) for x in np.asarray(lam, np.float64)])
+
+
+def make_h5vac_pin(gold):
+    """Vacuum wavelengths and range selection of HDF5 lists (ReadHDF, ioutils.f90:686-790;
+    pin_solar_h5vac.npz): the pin_solar list plus 12 lines above the synthesis range (5045.2-5046.8 A,
+    whose wings would reach the region) and 6 below it, all turned to vacuum (Air2Vac) and written with
+    WL_VAC = 1; the reference converts back (Vac2Air) and keeps only the lines inside WAVE=."""
+    name, atmname, mk, grid, region = pin_specs()[0]
+    teff, logg, ntau, species, ismol, _, _, vmic, molbrd, _, _ = CONFIGS[atmname]
+    model = W.eddington_model(teff, logg, ntau)
+    state = load_state(atmname)
+    extra = merge([mk(), W.atomic_lines(12, 5045.2, 5046.8, W.SEED0 + 45), W.atomic_lines(6, 4998.0, 4999.8, W.SEED0 + 46)])
+    pgf = np.load(os.path.join(DATA, "atm_%s.npz" % atmname))["probe_loggf"]
+    probes = probe_list(species, grid[0], 2.0, ismol=ismol, loggf=pgf)
+    t = extra._txt
+    wvac = air2vac(extra.wl)
+    with tempfile.TemporaryDirectory() as wd:
+        W.write_krz(os.path.join(wd, "model.krz"), model)
+        probes.write_z(os.path.join(wd, "probes.z"), grid[0], grid[1])
+        path = os.path.join(wd, "lines.h5")
+        fsio.write_hdf5_lines(path, extra.species, extra.spc, wvac,
+                              W.f32_of_text(t["elo"], "%.4f"), W.f32_of_text(t["loggf"], "%.3f"),
+                              W.f32_of_text(t["lgrad"], "%.3f"), W.f32_of_text(t["lgqst"], "%.3f"),
+                              W.f32_of_text(t["lgvdw"], "%.3f"), wl_vac=1, provenance="pin_solar list in vacuum")
+        deck = ("wave=%.4f, %.4f, %.6f, %d\nsave=0, 1, 1, 1, 1\nvmic=%.3f\nmolbrd=%d\n"
+                "lines=\n-1  probes.z\n-1  lines.h5\n\nmodel=model.krz\nmus=7\n" % (grid + (vmic, molbrd)))
+        log = run_ref(wd, deck)
+        r = fsio.read_hdf5_lines(path, species, wstart=grid[0], wend=grid[1])
+        lo = fsio.read_opac(os.path.join(wd, "fs_lineop.bin"))
+        co = fsio.read_opac(os.path.join(wd, "fs_contop.bin"))
+        sp = fsio.read_spec(os.path.join(wd, "fs_spec.bin"))
+        fl = fsio.read_flux(os.path.join(wd, "fs_flux.bin"))
+    assert "Lines read: %d" % len(r["wl"]) in log, log
+    for k in ("rhox", "T", "xne", "xna", "rho"):
+        assert np.array_equal(lo[k], state[k]), "EOS state differs from the recovered one: " + k
+    wave = lo["wave"]
+    sel = (wave >= region[0] - 1e-9) & (wave <= region[1] + 1e-9)
+    i0, i1 = (int(x) for x in np.nonzero(sel)[0][[0, -1]])
+    g = dict(wmode=grid[3], wstart=grid[0], wend=grid[1], dstep=grid[2])
+    S = oracle.State(g, state, contopac=co["opac"], vmicro=vmic, molbrd=molbrd)
+    o = oracle.lineop_calc(S, oracle.Lines(**{k: r[k] for k in ("wl", "elo", "gf", "grad", "gqst", "gvdw", "spc",
+                                                               "ismol")}, kind=0), list_type=0)
+    ref = lo["opac"][i0:i1 + 1]
+    m = ref > 0
+    mine = o["lineopac"][i0:i1 + 1]
+    print("  h5vac pin: %d of %d lines read, pattern equal %s, line opacity max rel %.2e"
+          % (len(r["wl"]), extra.n, np.array_equal(mine > 0, m), np.max(np.abs(mine[m] / ref[m] - 1))))
+    np.savez_compressed(
+        os.path.join(gold, "pin_solar_h5vac.npz"), grid=np.array(grid, np.float64), i0=i0, i1=i1, atm=atmname,
+        vmicro=vmic, molbrd=molbrd, contopac=co["opac"][i0:i1 + 1], lineopac=ref, wave=wave[i0:i1 + 1],
+        xmu=sp["xmu"], sfl=fl["sfl"][i0:i1 + 1], sfc=fl["sfc"][i0:i1 + 1], nread=len(r["wl"]),
+        **{"txt_" + k: np.asarray(v) for k, v in t.items()}, line_wvac=wvac, line_spc=extra.spc)
+
+
 def zh5_seeded():
     """The Zeeman list of the .zh5 fixture: pin_magnetic's seeded lines with three Lande factors set to
     the converters' 99 (unknown), which the reader turns into unsplit lines."""
@@ -1401,6 +1458,8 @@ if __name__ == "__main__":
         make_convol_pin(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "reentry":
         make_reentry_pin(os.path.join(REPO, "tests", "golden"))
+    elif len(sys.argv) > 1 and sys.argv[1] == "h5vac":
+        make_h5vac_pin(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "magframes":
         make_mag_frames_pin(os.path.join(REPO, "tests", "golden"))
     elif len(sys.argv) > 1 and sys.argv[1] == "maglinst":

@@ -58,6 +58,8 @@ def test_reader_molecular_list_matches_text_source():
         assert np.array_equal(cols[k][:n], g["feh_" + k.lower()]), k
     r = fsio.read_hdf5_lines(os.path.join(EXAMPLES, "56Fe1H_Exomol_Irw.h5"), [("FeH", 1)], exact=False)
     assert r["kind"] == 1 and np.all(r["spc"] == 0) and np.all(r["ismol"] == 1)
+    assert np.array_equal(r["wl"], fsio.vac2air(cols["W"]))        # WL_VAC = 1: air wavelengths, as ReadHDF
+    assert np.all(r["wl"] < cols["W"])
     assert np.array_equal(r["grad"], cols["GRAD"])               # molecular GRAD is taken as stored
     assert np.allclose(r["gf"], 10.0 ** cols["LGGF"].astype(np.float64), rtol=1e-6)
 
@@ -126,6 +128,55 @@ def test_oracle_hdf5_list_against_reference_pin(oracle_mod, tmp_path):
     x, w, _ = oracle_mod.mu_quadrature(1, len(d["xmu"]))
     sfl, _ = oracle_mod.disk_integ(w, spl[i0:i1 + 1], spc[i0:i1 + 1])
     assert np.max(np.abs(sfl / d["sfl"] - 1)) < 1e-8
+
+
+def test_oracle_vacuum_list_and_range_selection_against_reference_pin(oracle_mod, tmp_path):
+    """A list written in vacuum wavelengths (WL_VAC = 1) with lines beyond both ends of WAVE=: read as
+    ReadHDF reads it (Vac2Air, then only wstart <= W <= wend), the records give the reference's line
+    opacity for the same file (tests/golden/pin_solar_h5vac.npz); the lines above the range would
+    change the region if they were kept."""
+    from fastspec_b200 import fsio, workloads as W
+    d = H.load_pin("pin_solar_h5vac")
+    st, meta = H.load_atm("solar")
+    species = [(s.split()[0], int(s.split()[1])) for s in meta["species"]]
+    p = str(tmp_path / "lines.h5")
+    f = lambda k, fmt: W.f32_of_text(d["txt_" + k], fmt)
+    fsio.write_hdf5_lines(p, species, d["line_spc"], d["line_wvac"], f("elo", "%.4f"), f("loggf", "%.3f"),
+                          f("lgrad", "%.3f"), f("lgqst", "%.3f"), f("lgvdw", "%.3f"), wl_vac=1)
+    grid, st, meta, co = H.pin_setup(d)
+    r = fsio.read_hdf5_lines(p, species, wstart=grid["wstart"], wend=grid["wend"])
+    assert len(r["wl"]) == int(d["nread"]) < len(d["line_wvac"])
+    assert np.all((r["wl"] >= grid["wstart"]) & (r["wl"] <= grid["wend"]))
+    wa = fsio.vac2air(d["line_wvac"])
+    assert np.array_equal(r["wl"], wa[(wa >= grid["wstart"]) & (wa <= grid["wend"])])
+    S = oracle_mod.State(grid, st, contopac=co, vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]))
+    keys = ("wl", "elo", "gf", "grad", "gqst", "gvdw", "spc", "ismol")
+    o = oracle_mod.lineop_calc(S, oracle_mod.Lines(**{k: r[k] for k in keys}, kind=0), list_type=0)
+    i0, i1 = int(d["i0"]), int(d["i1"])
+    lo, ref = o["lineopac"][i0:i1 + 1], d["lineopac"]
+    assert np.array_equal(lo > 0, ref > 0)
+    assert np.max(np.abs(lo[ref > 0] / ref[ref > 0] - 1)) < 1e-8
+    spl, spc = oracle_mod.radtran(S, d["xmu"], o["lineopac"])
+    x, w, _ = oracle_mod.mu_quadrature(1, len(d["xmu"]))
+    sfl, _ = oracle_mod.disk_integ(w, spl[i0:i1 + 1], spc[i0:i1 + 1])
+    assert np.max(np.abs(sfl / d["sfl"] - 1)) < 1e-8
+    full = fsio.read_hdf5_lines(p, species)                       # no range: the outside lines stay
+    o2 = oracle_mod.lineop_calc(S, oracle_mod.Lines(**{k: full[k] for k in keys}, kind=0), list_type=0)
+    m = ref > 0
+    assert np.max(np.abs(o2["lineopac"][i0:i1 + 1][m] / ref[m] - 1)) > 1e-4
+
+
+def test_reader_rejects_unsorted_wavelengths(tmp_path):
+    from fastspec_b200 import fsio, hdf5
+    import pytest
+    p = str(tmp_path / "u.h5")
+    fsio.write_hdf5_lines(p, [("Fe", 1)], [0, 0], [5000.0, 5001.0], [1.0, 1.0], [-1.0, -1.0], [8.0, 8.0],
+                          [-5.0, -5.0], [-7.5, -7.5])
+    cols, attrs, units = hdf5.read_lines(p)
+    cols["W"] = cols["W"][::-1].copy()
+    hdf5.write_lines(p, cols, attrs, units)
+    with pytest.raises(ValueError, match="not sorted"):
+        fsio.read_hdf5_lines(p, [("Fe", 1)])
 
 
 def zh5_pin_lines(tmp_path, pattern):
