@@ -190,6 +190,10 @@ def read_hdf5_lines(path, species, exact=True, wstart=None, wend=None):
     from . import hdf5
     from .workloads import pow10f
     cols, attrs, _ = hdf5.read_lines(path)
+    if int(attrs.get("HFLAG", 0)) == 1:
+        # a dedicated hydrogen list goes to the reference's hydrogen line opacity (synth.f90:136-146),
+        # which stays with the caller
+        raise ValueError("read_hdf5_lines: %s is a hydrogen line list (HFLAG = 1)" % path)
     w = np.asarray(cols["W"], np.float64)
     if int(attrs.get("WL_VAC", 0)) == 1:
         w = vac2air(w)

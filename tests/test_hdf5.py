@@ -166,7 +166,9 @@ def test_oracle_vacuum_list_and_range_selection_against_reference_pin(oracle_mod
     assert np.max(np.abs(o2["lineopac"][i0:i1 + 1][m] / ref[m] - 1)) > 1e-4
 
 
-def test_reader_rejects_unsorted_wavelengths(tmp_path):
+def test_reader_rejects_unsorted_and_hydrogen_lists(tmp_path):
+    """ReadHDF stops on an unsorted wavelength column; a dedicated hydrogen list (HFLAG = 1) belongs to
+    the hydrogen line opacity, which is not part of this library."""
     from fastspec_b200 import fsio, hdf5
     import pytest
     p = str(tmp_path / "u.h5")
@@ -176,6 +178,11 @@ def test_reader_rejects_unsorted_wavelengths(tmp_path):
     cols["W"] = cols["W"][::-1].copy()
     hdf5.write_lines(p, cols, attrs, units)
     with pytest.raises(ValueError, match="not sorted"):
+        fsio.read_hdf5_lines(p, [("Fe", 1)])
+    cols["W"] = cols["W"][::-1].copy()
+    attrs["HFLAG"] = np.int16(1)
+    hdf5.write_lines(p, cols, attrs, units)
+    with pytest.raises(ValueError, match="hydrogen line list"):
         fsio.read_hdf5_lines(p, [("Fe", 1)])
 
 
