@@ -4,6 +4,7 @@ tests/golden/make_bin_golden.py) are read and written back byte for byte."""
 import os
 
 import numpy as np
+import pytest
 
 import helpers as H
 
@@ -125,3 +126,34 @@ def test_spec_grid_orders_angles_and_detects_log_grids():
     u = fsio.spec_grid(dict(xmu=np.array([1.0]), wave=5000.0 + 0.01 * np.arange(4), spl=np.zeros((4, 1)),
                             spc=np.ones((4, 1))))
     assert u["wmode"] == 0 and abs(u["dstep"] - 0.01) < 1e-12
+
+
+REF_BIN = "/root/reference/src/fastspec_Linux_x86_64"
+MAG_EXAMPLE = "/root/reference/examples/magnetic-synthesis/fs_spec.bin"
+
+
+@pytest.mark.skipif(not (os.path.exists(REF_BIN) and os.path.exists(MAG_EXAMPLE)),
+                    reason="the reference program and its examples are not present")
+def test_post_processing_of_the_shipped_magnetic_example(fsg, oracle_mod, tmp_path):
+    """The post-processing mode on the reference's own shipped Stokes intensities (examples/
+    magnetic-synthesis/fs_spec.bin: 7 angles, 39,194 wavelengths): the reference program run here on
+    that file against fsio.spec_grid + mu_quad_type + the oracle's broadened disk integration."""
+    import shutil
+    import subprocess
+    from fastspec_b200 import fsio
+    shutil.copy(MAG_EXAMPLE, str(tmp_path / "fs_spec.bin"))
+    vs, vm, vg = 12.0, 4.0, 80000.0
+    r = subprocess.run([REF_BIN, "fs_spec.bin", "%g" % vs, "%g" % vm, "%g" % vg], cwd=str(tmp_path),
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    ref = fsio.read_flux(str(tmp_path / "fs_flux.bin"))
+    s = fsio.spec_grid(fsio.read_spec(MAG_EXAMPLE))
+    q = fsg.mu_quad_type(s["xmu"])
+    x, w, rr = fsg.mu_quadrature(q, len(s["xmu"]), x=s["xmu"])
+    grid = dict(wmode=s["wmode"], wstart=s["wstart"], wend=s["wend"], dstep=s["dstep"])
+    wave = s["wave"] + s["wstart"]
+    sfl, sfc = oracle_mod.disk_integ_conv(x, w, rr, s["spl"], s["spc"], oracle_mod.grid_dv(grid, wave), vs, vm,
+                                          oracle_mod.gauss_sigma_pix(grid, wave, vg))
+    assert np.array_equal(ref["wave"], wave) and len(wave) > 30000
+    assert np.max(np.abs(sfl / ref["sfl"] - 1)) < 1e-12
+    assert np.max(np.abs(sfc / ref["sfc"] - 1)) < 1e-12
