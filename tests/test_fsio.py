@@ -157,3 +157,35 @@ def test_post_processing_of_the_shipped_magnetic_example(fsg, oracle_mod, tmp_pa
     assert np.array_equal(ref["wave"], wave) and len(wave) > 30000
     assert np.max(np.abs(sfl / ref["sfl"] - 1)) < 1e-12
     assert np.max(np.abs(sfc / ref["sfc"] - 1)) < 1e-12
+
+
+EXAMPLES = "/root/reference/examples"
+
+
+@pytest.mark.skipif(not os.path.isdir(EXAMPLES), reason="the reference's examples are not present")
+def test_shipped_example_outputs_round_trip(tmp_path):
+    """The reference's shipped outputs (examples/*-synthesis: the atomic flux and line strengths of
+    44,380 lines, the molecular flux, the magnetic Stokes intensities) read and written back byte for
+    byte."""
+    from fastspec_b200 import fsio
+    for sub, name in (("atomic-synthesis", "fs_flux.bin"), ("molecular-synthesis", "fs_flux.bin"),
+                      ("atomic-synthesis", "fs_linst.bin"), ("magnetic-synthesis", "fs_spec.bin")):
+        src = os.path.join(EXAMPLES, sub, name)
+        raw = open(src, "rb").read()
+        out = str(tmp_path / (sub + "_" + name))
+        if name == "fs_flux.bin":
+            f = fsio.read_flux(src)
+            fsio.write_flux(out, f["wave"], f["sfl"], f["sfc"])
+        elif name == "fs_spec.bin":
+            r = fsio.read_spec(src)
+            assert r["magnetic"] and len(r["xmu"]) == 7
+            fsio.write_spec(out, r["wave"], r["xmu"], r["spl"], r["spc"], r["spz"])
+        else:
+            r = fsio.read_linst(src)
+            assert len(r["wave"]) > 40000
+            a = 0
+            for k, n in enumerate(r["nrec"]):
+                sl = slice(a, a + n)
+                fsio.write_linst(out, r["species"][sl], r["ion"][sl], r["wave"][sl], r["strength"][sl], append=k > 0)
+                a += n
+        assert open(out, "rb").read() == raw, src
