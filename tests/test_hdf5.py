@@ -265,3 +265,14 @@ def test_oracle_molecular_h5_lists_against_reference_pin(oracle_mod, tmp_path):
     assert rel.max() < 2e-7 and np.median(rel) < 1e-8
     spl, spc = oracle_mod.radtran(S, d["xmu"], lo)
     assert np.max(np.abs(spl[i0:i1 + 1] / d["spl"] - 1)) < 2e-7
+
+
+@pytest.mark.skipif(not os.path.isdir(EXAMPLES), reason="reference example line lists not present")
+def test_reader_refuses_the_shipped_hydrogen_list():
+    """VALD_H1_10-10000.h5 is the reference's dedicated hydrogen list (HFLAG = 1): it feeds the
+    hydrogen line opacity, not this library."""
+    from fastspec_b200 import fsio, hdf5
+    cols, attrs, units = hdf5.read_lines(os.path.join(EXAMPLES, "VALD_H1_10-10000.h5"))
+    assert int(attrs["HFLAG"]) == 1 and np.all(np.char.strip(np.asarray(cols["EL"]).astype("U8")) == "H")
+    with pytest.raises(ValueError, match="hydrogen line list"):
+        fsio.read_hdf5_lines(os.path.join(EXAMPLES, "VALD_H1_10-10000.h5"), [("Fe", 1)])
