@@ -9,6 +9,13 @@ import numpy as np
 import helpers as H
 
 
+def he_entries():
+    """(centre, lower level energy) of the 37 tabulated lines, parsed from the library's data header."""
+    import re
+    src = open(os.path.join(H.REPO, "fastspec_b200", "csrc", "fsg_hestark_tables.h")).read()
+    return [(float(a), float(b)) for a, b in re.findall(r"^\s*\{([0-9.]+), ([0-9.]+), [46],$", src, re.M)]
+
+
 def hot_state():
     d = np.load(os.path.join(H.DATA, "atm_hot.npz"))
     st, meta = H.load_atm("hot")
@@ -131,3 +138,20 @@ def test_line_list_table_match_column(fsg):
     assert M._keep["wl"] is L._keep["wl"]                       # the other columns are shared, not copied
     E = fsg.LineList.from_arrays(dict(a, ihe=np.zeros(len(a["wl"]), np.int32)))
     assert E._with_he_match(0, 3855.0) is E
+
+
+def test_match_idx_random_lines_equal_oracle(fsg, oracle_mod):
+    """HeMatchIdx over 50,000 seeded He I lines scattered around every table entry (within +-1.5 A and
+    +-0.02 eV, so both edges of both windows are crossed): the library equals the oracle line by line."""
+    HE_ENTRIES = he_entries()
+    rng = np.random.default_rng(17)
+    n = 50_000
+    k = rng.integers(0, len(HE_ENTRIES), n)
+    wl = np.array([HE_ENTRIES[i][0] for i in k]) + rng.uniform(-1.5, 1.5, n)
+    elo = (np.array([HE_ENTRIES[i][1] for i in k]) + rng.uniform(-0.02, 0.02, n)).astype(np.float32)
+    spc = np.zeros(n, np.int32)
+    wfirst = 2000.0
+    got = fsg.he_match_idx(wl, elo, spc, 0, wfirst)
+    want = np.array([oracle_mod.he_match_idx((w - wfirst) + wfirst, float(e)) for w, e in zip(wl, elo)])
+    assert np.array_equal(got, want)
+    assert 0.2 < np.mean(got > 0) < 0.8
