@@ -207,7 +207,7 @@ def batched_grid(F, torch, dev, natm, nlines, steps, warmup):
         C.set_contopac(co)
         C.set_mu(x, w)
         ctxs.append(C)
-    B = F.Batch(ctxs, LL, margin=10.0)
+    B = F.Batch(ctxs, LL)                          # each atmosphere reads the lines of its span
     t0 = time.perf_counter()
     tuning = B.tune()
     tune_s = time.perf_counter() - t0
@@ -228,7 +228,7 @@ def batched_grid(F, torch, dev, natm, nlines, steps, warmup):
     t_seq = 0.0
     for C, m in zip(ctxs, members):
         g = m["grid"]
-        a0, a1 = np.searchsorted(wl, g["wstart"] - 10.0), np.searchsorted(wl, g["wend"] + 10.0, side="right")
+        a0, a1 = np.searchsorted(wl, g["wstart"]), np.searchsorted(wl, g["wend"], side="right")
         sub = F.LineList.from_arrays({k: np.ascontiguousarray(v[a0:a1]) for k, v in arr.items()})
         C.lineop_reset()
         r = C.lineop_calc(sub, want_lineopac=False, want_lines=False)
@@ -244,7 +244,7 @@ def batched_grid(F, torch, dev, natm, nlines, steps, warmup):
         C64.set_atmosphere(m["state"])
         C64.set_contopac(conts[k])
         C64.set_mu(x, w)
-        a0, a1 = np.searchsorted(wl, g["wstart"] - 10.0), np.searchsorted(wl, g["wend"] + 10.0, side="right")
+        a0, a1 = np.searchsorted(wl, g["wstart"]), np.searchsorted(wl, g["wend"], side="right")
         sub = F.LineList.from_arrays({kk: np.ascontiguousarray(v[a0:a1]) for kk, v in arr.items()})
         r = C64.lineop_calc(sub, want_lineopac=False, want_lines=False)
         t64 += r["stats"]["ms_total"]

@@ -76,7 +76,8 @@ EXPORTS = [
     "fsg_set_atmosphere", "fsg_set_contopac", "fsg_set_contopac_dev", "fsg_set_hestark", "fsg_hestark_tables",
     "fsg_he_match_idx",
     "fsg_lineop_calc", "fsg_lineop_calc_dev", "fsg_lineop_reset", "fsg_lineop_get", "fsg_lineop_set",
-    "fsg_lineop_device_ptr", "fsg_set_mu", "fsg_radtran", "fsg_radtran_dev", "fsg_mag_lineop_calc",
+    "fsg_lineop_device_ptr", "fsg_set_mu", "fsg_radtran", "fsg_radtran_dev", "fsg_radtran_range_dev",
+    "fsg_mag_lineop_calc",
     "fsg_mag_lineop_reset", "fsg_mag_radtran", "fsg_hvoigt", "fsg_fvoigt", "fsg_voigt_tables",
     "fsg_locprf_pp", "fsg_locprf_pp_noalloc", "fsg_mu_quadrature", "fsg_zeeman_pattern",
     "fsg_central_dev", "fsg_accumulate_dev", "fsg_batch_create", "fsg_batch_tune", "fsg_batch_set_tuning",
@@ -130,6 +131,8 @@ def lib():
     L.fsg_set_geometry.argtypes = [C.c_void_p, C.c_double, _dp]
     L.fsg_radtran.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
     L.fsg_radtran_dev.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.fsg_radtran_range_dev.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p]
     L.fsg_mag_lineop_calc.argtypes = [C.c_void_p, C.POINTER(CLines), C.c_int, _dp, C.c_int, _dp, _ip, _ip,
                                       _ip, _fp, C.POINTER(Stats)]
     L.fsg_mag_lineop_reset.argtypes = [C.c_void_p]
@@ -544,6 +547,12 @@ class Context:
         v = lambda p: C.c_void_p(p) if p else None
         self._ck(self._lib.fsg_radtran_dev(self.h, v(d_spl), v(d_spc), v(d_sfl), v(d_sfc)), "fsg_radtran_dev")
 
+    def radtran_range_dev(self, i0, i1, d_spl, d_spc, d_sfl, d_sfc):
+        """RadTranCalc + flux over wavelengths i0..i1 (1-based, inclusive) into whole-grid device arrays."""
+        v = lambda p: C.c_void_p(p) if p else None
+        self._ck(self._lib.fsg_radtran_range_dev(self.h, int(i0), int(i1), v(d_spl), v(d_spc), v(d_sfl), v(d_sfc)),
+                 "fsg_radtran_range_dev")
+
     def mag_lineop_calc(self, lines, bframe, bfield, want=True, want_linstr=False):
         n = lines.n
         bf = _f64(bfield)
@@ -600,9 +609,11 @@ class Context:
 class Batch:
     """Batched synthesis (fsg_batch_*): many contexts (grid, atmosphere, continuum and mu set, mixed
     precision) and one line list sorted by wavelength.  run() replays one CUDA graph of the whole
-    batch (tuned and captured on the first call); flux(i) reads atmosphere i's flux."""
+    batch (tuned and captured on the first call); flux(i) reads atmosphere i's flux.  Each atmosphere
+    takes the lines with centres in [wstart - margin, wend + margin]; margin = 0 (the default) is the
+    reference's reader rule (ioutils.f90:752-753, 1496-1497)."""
 
-    def __init__(self, contexts, lines, margin=10.0):
+    def __init__(self, contexts, lines, margin=0.0):
         self._lib = lib()
         self.contexts = list(contexts)
         self.lines = lines

@@ -15,8 +15,8 @@ void fsg_launch_xline_init(cudaStream_t, int, const double *, const double *, co
 void fsg_launch_center(cudaStream_t, const AtmView &, const LineView &, const VoigtTables &, int32_t *,
                        int32_t *, int32_t *, unsigned long long *);
 void fsg_launch_params_fast(cudaStream_t, const AtmView &, const LineView &, const int64_t *, int64_t, int64_t,
-                            const int32_t *, const int32_t *, const int32_t *, const VoigtTables &, WingRec *,
-                            CoreRec *, LineHdr *);
+                            int64_t, const int32_t *, const int32_t *, const int32_t *, const VoigtTables &,
+                            WingRec *, CoreRec *, LineHdr *);
 void fsg_launch_params_fp64(cudaStream_t, const AtmView &, const LineView &, int64_t, int64_t, const int32_t *,
                             double3 *);
 void fsg_launch_span(cudaStream_t, int64_t, const int32_t *, const int32_t *, const int32_t *, int *, int *);
@@ -680,14 +680,18 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st, cons
         if (rc) return cuda_fail(ctx, cudaGetLastError(), "select");
         ctx->launches += 3;
         int64_t nc = (int64_t)hist[c];
-        int64_t bcap = std::min(cap, nc);
+        // blocks of at most cap lines (LIMITRAM); block b takes every nblk-th line of the class from
+        // its b-th, so each block is sorted by wavelength and spans the whole grid: every tile of a
+        // launch has work, however small the blocks
+        const int64_t nblk = (nc + cap - 1) / cap;
+        const int64_t bcap = (nc + nblk - 1) / nblk;
         ALLOC(ctx->d_wing, sizeof(WingRec) * (size_t)bcap * nt);
         ALLOC(ctx->d_core, sizeof(CoreRec) * (size_t)bcap * nt);
         ALLOC(ctx->d_hdr, sizeof(LineHdr) * (size_t)bcap);
         ALLOC(ctx->d_span, fsg_tile_span_scratch(bcap));
-        for (int64_t j0 = 0; j0 < nc; j0 += bcap) {
-            int64_t nb = std::min(bcap, nc - j0);
-            fsg_launch_params_fast(s, A, LV, ctx->d_idx.as<int64_t>(), j0, nb, fl, wl_, wr_, ctx->tab,
+        for (int64_t b = 0; b < nblk; b++) {
+            const int64_t nb = (nc - b + nblk - 1) / nblk;
+            fsg_launch_params_fast(s, A, LV, ctx->d_idx.as<int64_t>(), b, nblk, nb, fl, wl_, wr_, ctx->tab,
                                    ctx->d_wing.as<WingRec>(), ctx->d_core.as<CoreRec>(), ctx->d_hdr.as<LineHdr>());
             if (fsg_launch_tile_span(s, c, ctx->nwl, nb, ctx->d_hdr.as<LineHdr>(), ctx->d_tlo.as<int>(),
                                      ctx->d_thi.as<int>(), ctx->d_span.p, ctx->d_span.cap))
@@ -751,8 +755,12 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st, cons
     return FSG_OK;
 }
 
-// plain FP64 path mirroring LineopCalc's PACK / MarkWideLines / Lstart-Lstop / segment loop
-static int accumulate_fp64(fsg_ctx *ctx, const LineView &LV, int64_t nkeep, fsg_stats *st) {
+// plain FP64 path mirroring LineopCalc's PACK / MarkWideLines / Lstart-Lstop / segment loop, over the
+// windows in ctx->d_flags / d_ileft / d_iright.  [i0, i1]: 1-based wavelength range to fill (1..nwl for
+// the whole grid); PACK, the wide-line marking and the segments are those of the whole grid, so every
+// wavelength of the range sums the same lines in the same order as a whole-grid run.  nkeep < 0: count
+// the retained lines here.
+static int accumulate_fp64(fsg_ctx *ctx, const LineView &LV, int64_t nkeep, fsg_stats *st, int i0, int i1) {
     int64_t n = LV.n;
     const int nt = ctx->ntau, nwl = ctx->nwl;
     cudaStream_t s = ctx->stream;
@@ -775,6 +783,10 @@ static int accumulate_fp64(fsg_ctx *ctx, const LineView &LV, int64_t nkeep, fsg_
     if (pack) {
         fsg_select(s, n, pf, pl, pr, -1, ctx->d_counts.as<int>(), ctx->d_offs.as<int64_t>(), ctx->d_idx.as<int64_t>(),
                    ctx->d_total.as<int64_t>());
+        if (nkeep < 0) {
+            CK(cudaMemcpyAsync(&nkeep, ctx->d_total.p, sizeof nkeep, cudaMemcpyDeviceToHost, s), "retained lines");
+            CK(cudaStreamSynchronize(s), "retained lines");
+        }
         nw = nkeep;
         // gather the per-line arrays of the retained lines (host-side gather is avoided: device gather)
         size_t need = 64 * (size_t)std::max<int64_t>(nw, 1);
@@ -786,6 +798,7 @@ static int accumulate_fp64(fsg_ctx *ctx, const LineView &LV, int64_t nkeep, fsg_
     }
     if (nw == 0) { if (st) st->nlines_used = 0; return FSG_OK; }
     // MarkWideLines (synth.f90:709-744)
+    ALLOC(ctx->d_nkeep, sizeof(unsigned long long));
     unsigned long long *d_nw = ctx->d_nkeep.as<unsigned long long>();
     CK(cudaMemsetAsync(d_nw, 0, sizeof(unsigned long long), s), "wide");
     fsg_launch_mark_wide(s, A, nw, W.wl, nstep, pf, pl, pr, d_nw);
@@ -811,7 +824,7 @@ static int accumulate_fp64(fsg_ctx *ctx, const LineView &LV, int64_t nkeep, fsg_
                         ctx->d_total.as<int64_t>());
         ALLOC(ctx->d_pw, sizeof(double3) * nwide * nt);
         fsg_launch_wide_fp64(s, A, W, (int)nwide, ctx->d_widx.as<int64_t>(), pf, pl, pr, ctx->d_pw.as<double3>(),
-                             ctx->tab, 1, nwl, ctx->d_lineopac.as<double>(), ctx->d_evals.as<double>());
+                             ctx->tab, i0, i1, ctx->d_lineopac.as<double>(), ctx->d_evals.as<double>());
         ctx->launches += 5;
     }
     // segment loop (synth.f90:1006-1088): choose segments on the host from Lstart/Lstop
@@ -844,22 +857,25 @@ static int accumulate_fp64(fsg_ctx *ctx, const LineView &LV, int64_t nkeep, fsg_
         }
         int64_t iline2 = std::min<int64_t>(iline1 + nstep - 1, nw);
         int64_t loff = iline1 - 1;
-        if (iline1 != ilineb) {
-            ilineb = iline1;
-            fsg_launch_params_fp64(s, A, W, loff, iline2 - loff, pf, ctx->d_p64.as<double3>());
+        const int ra = std::max(iwl1, i0), rb = std::min(iwl2, i1);    // the segment's part of the range
+        if (ra <= rb) {
+            if (iline1 != ilineb) {
+                ilineb = iline1;
+                fsg_launch_params_fp64(s, A, W, loff, iline2 - loff, pf, ctx->d_p64.as<double3>());
+                ctx->launches += 1;
+                nblocks++;
+            }
+            cudaEvent_t ea = ctx->ev[4], eb = ctx->ev[5];
+            cudaEventRecord(ea, s);
+            fsg_launch_accum_fp64(s, A, W.wl, ra, rb, ctx->d_lstart.as<int>(), ctx->d_lstop.as<int>(), pf, pl, pr,
+                                  loff, ctx->d_p64.as<double3>(), ctx->tab, ctx->d_lineopac.as<double>(),
+                                  ctx->d_evals.as<double>());
+            CK(cudaGetLastError(), "fp64 accumulation");
+            cudaEventRecord(eb, s);
+            CK(cudaEventSynchronize(eb), "fp64 accumulation");
+            { float x = 0; cudaEventElapsedTime(&x, ea, eb); if (st) { st->ms_accum_kernels += x; st->accum_launches++; } }
             ctx->launches += 1;
-            nblocks++;
         }
-        cudaEvent_t ea = ctx->ev[4], eb = ctx->ev[5];
-        cudaEventRecord(ea, s);
-        fsg_launch_accum_fp64(s, A, W.wl, iwl1, iwl2, ctx->d_lstart.as<int>(), ctx->d_lstop.as<int>(), pf, pl, pr,
-                              loff, ctx->d_p64.as<double3>(), ctx->tab, ctx->d_lineopac.as<double>(),
-                              ctx->d_evals.as<double>());
-        CK(cudaGetLastError(), "fp64 accumulation");
-        cudaEventRecord(eb, s);
-        CK(cudaEventSynchronize(eb), "fp64 accumulation");
-        { float x = 0; cudaEventElapsedTime(&x, ea, eb); if (st) { st->ms_accum_kernels += x; st->accum_launches++; } }
-        ctx->launches += 1;
         if (iwl2 == nwl) break;
         iwl1 = iwl2 + 1;
     }
@@ -938,7 +954,7 @@ static int lineop_dev(fsg_ctx *ctx, const fsg_lines *D, fsg_stats *st, const fsg
     if (rc) return rc;
     CK(cudaEventRecord(ctx->ev[1], s), "event");
     if (st) { st->nlines_used = nkeep; st->nweak = D->n - nkeep; }
-    if (ctx->cfg.precision == FSG_PREC_FP64) rc = accumulate_fp64(ctx, LV, nkeep, st);
+    if (ctx->cfg.precision == FSG_PREC_FP64) rc = accumulate_fp64(ctx, LV, nkeep, st, 1, ctx->nwl);
     else rc = accumulate_fast(ctx, LV, st, ctx->d_flags.as<int32_t>(), ctx->d_ileft.as<int32_t>(),
                               ctx->d_iright.as<int32_t>(), 1, ctx->nwl);
     if (rc) return rc;
@@ -982,8 +998,6 @@ int fsg_central_dev(fsg_ctx *ctx, const fsg_lines *d_lines, int32_t *d_flags, in
 int fsg_accumulate_dev(fsg_ctx *ctx, const fsg_lines *d_lines, const int32_t *d_flags, const int32_t *d_ileft,
                        const int32_t *d_iright, int i0, int i1, fsg_stats *st) {
     int rc = check_lines(ctx, d_lines); if (rc) return rc;
-    if (ctx->cfg.precision == FSG_PREC_FP64)
-        return fail(ctx, FSG_E_STATE, "fsg_accumulate_dev: the wavelength-range accumulation is mixed precision only");
     if (i0 < 1 || i1 > ctx->nwl || i0 > i1) return fail(ctx, FSG_E_ARG, "fsg_accumulate_dev: need 1 <= i0 <= i1 <= nwl");
     if (d_lines->n > 0 && (!d_flags || !d_ileft || !d_iright))
         return fail(ctx, FSG_E_ARG, "fsg_accumulate_dev: window arrays missing");
@@ -993,7 +1007,17 @@ int fsg_accumulate_dev(fsg_ctx *ctx, const fsg_lines *d_lines, const int32_t *d_
     if (d_lines->n == 0) return FSG_OK;
     cudaStream_t s = ctx->stream;
     CK(cudaEventRecord(ctx->ev[1], s), "event");
-    rc = accumulate_fast(ctx, make_view(d_lines), st, d_flags, d_ileft, d_iright, i0, i1);
+    if (ctx->cfg.precision == FSG_PREC_FP64) {
+        // the FP64 path marks wide lines in its own copy of the windows
+        const size_t nb = sizeof(int32_t) * (size_t)d_lines->n;
+        ALLOC(ctx->d_flags, nb); ALLOC(ctx->d_ileft, nb); ALLOC(ctx->d_iright, nb);
+        CK(cudaMemcpyAsync(ctx->d_flags.p, d_flags, nb, cudaMemcpyDeviceToDevice, s), "windows");
+        CK(cudaMemcpyAsync(ctx->d_ileft.p, d_ileft, nb, cudaMemcpyDeviceToDevice, s), "windows");
+        CK(cudaMemcpyAsync(ctx->d_iright.p, d_iright, nb, cudaMemcpyDeviceToDevice, s), "windows");
+        rc = accumulate_fp64(ctx, make_view(d_lines), -1, st, i0, i1);
+    } else {
+        rc = accumulate_fast(ctx, make_view(d_lines), st, d_flags, d_ileft, d_iright, i0, i1);
+    }
     if (rc) return rc;
     CK(cudaEventRecord(ctx->ev[2], s), "event");
     CK(cudaStreamSynchronize(s), "accumulate");
@@ -1001,7 +1025,8 @@ int fsg_accumulate_dev(fsg_ctx *ctx, const fsg_lines *d_lines, const int32_t *d_
         float b = 0;
         cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
         st->ms_accum = b; st->ms_total = b;
-        st->line_evals = fsg_count_evals(ctx, d_lines->n, d_flags, d_ileft, d_iright, i0, i1);
+        if (ctx->cfg.precision != FSG_PREC_FP64)
+            st->line_evals = fsg_count_evals(ctx, d_lines->n, d_flags, d_ileft, d_iright, i0, i1);
     }
     return FSG_OK;
 }
@@ -1059,19 +1084,33 @@ int fsg_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, double *lineopac, int3
 }
 
 // ---- RadTranCalc ------------------------------------------------------------------------------------
-static int radtran_dev(fsg_ctx *ctx, double *spl, double *spc, double *sfl, double *sfc) {
+// RadTranCalc + flux over the wavelengths i0..i1 (1-based, inclusive) into arrays laid out over the
+// whole grid.  The solver kernels index wavelengths from the view's base pointers, so the range is a
+// view whose wave / continuum / line-opacity / output bases start at wavelength i0.
+static int radtran_dev(fsg_ctx *ctx, double *spl, double *spc, double *sfl, double *sfc, int i0 = 1,
+                       int i1 = -1) {
     if (!ctx->have_grid || !ctx->have_atm || !ctx->have_cont || ctx->nmu < 1)
         return fail(ctx, FSG_E_STATE, "radtran: set grid, atmosphere, continuum and mu first");
+    if (i1 < 0) i1 = ctx->nwl;
+    if (i0 < 1 || i1 > ctx->nwl || i0 > i1) return fail(ctx, FSG_E_ARG, "radtran: need 1 <= i0 <= i1 <= nwl");
     int rc = ensure_lineopac(ctx); if (rc) return rc;
     AtmView A = fsg_view(ctx);
+    const size_t o = (size_t)(i0 - 1), nt = (size_t)ctx->ntau, nmu = (size_t)ctx->nmu;
+    A.nwl = i1 - i0 + 1;
+    A.wave += o;
+    A.contopac += o * nt;
+    const double *lop = ctx->d_lineopac.as<double>() + o * nt;
+    if (spl) spl += o * nmu;
+    if (spc) spc += o * nmu;
+    if (sfl) sfl += o;
+    if (sfc) sfc += o;
     RayView R;
     rc = rays_prepare(ctx, &R); if (rc) return rc;
     if (R.nmu > 0)
-        rc = fsg_launch_radtran_sph(ctx->stream, A, ctx->d_lineopac.as<double>(), R, ctx->d_wmu.as<double>(), spl, spc,
-                                    sfl, sfc);
+        rc = fsg_launch_radtran_sph(ctx->stream, A, lop, R, ctx->d_wmu.as<double>(), spl, spc, sfl, sfc);
     else
-        rc = fsg_launch_radtran(ctx->stream, A, ctx->d_lineopac.as<double>(), ctx->d_rhox.as<double>(), ctx->nmu,
-                                ctx->d_xmu.as<double>(), ctx->d_wmu.as<double>(), spl, spc, sfl, sfc);
+        rc = fsg_launch_radtran(ctx->stream, A, lop, ctx->d_rhox.as<double>(), ctx->nmu, ctx->d_xmu.as<double>(),
+                                ctx->d_wmu.as<double>(), spl, spc, sfl, sfc);
     ctx->launches += 1;
     if (rc) return cuda_fail(ctx, cudaGetLastError(), "k_radtran");
     return FSG_OK;
@@ -1081,6 +1120,14 @@ int fsg_radtran_dev(fsg_ctx *ctx, double *d_spl, double *d_spc, double *d_sfl, d
     if (!ctx) return FSG_E_ARG;
     cudaSetDevice(ctx->device);
     int rc = radtran_dev(ctx, d_spl, d_spc, d_sfl, d_sfc); if (rc) return rc;
+    CK(cudaStreamSynchronize(ctx->stream), "radtran");
+    return FSG_OK;
+}
+
+int fsg_radtran_range_dev(fsg_ctx *ctx, int i0, int i1, double *d_spl, double *d_spc, double *d_sfl, double *d_sfc) {
+    if (!ctx) return FSG_E_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = radtran_dev(ctx, d_spl, d_spc, d_sfl, d_sfc, i0, i1); if (rc) return rc;
     CK(cudaStreamSynchronize(ctx->stream), "radtran");
     return FSG_OK;
 }
@@ -1907,7 +1954,7 @@ static int batch_prepare(fsg_batch *b, int P) {
         LineView LV = batch_view(b, a);
         fsg_launch_center(s, A, LV, c->tab, a.flags.as<int32_t>(), a.il.as<int32_t>(), a.ir.as<int32_t>(),
                           b->nk.as<unsigned long long>());
-        fsg_launch_params_fast(s, A, LV, b->idx.as<int64_t>(), 0, a.cn, a.flags.as<int32_t>(), a.il.as<int32_t>(),
+        fsg_launch_params_fast(s, A, LV, b->idx.as<int64_t>(), 0, 1, a.cn, a.flags.as<int32_t>(), a.il.as<int32_t>(),
                                a.ir.as<int32_t>(), c->tab, a.wing.as<WingRec>(), a.core.as<CoreRec>(),
                                a.hdr.as<LineHdr>());
         if (fsg_launch_tile_span(s, P == 2 ? 0 : 2, c->nwl, a.cn, a.hdr.as<LineHdr>(), a.wtlo.as<int>(),
@@ -2029,7 +2076,8 @@ int fsg_batch_create(fsg_ctx *const *atms, int natm, const fsg_lines *lines, dou
         fsg_ctx *c = atms[i];
         a.ctx = c;
         b->ntau_max = std::max(b->ntau_max, c->ntau);
-        // candidates: lines with centres in [first wavelength - margin, last wavelength + margin]
+        // candidates: lines with centres in [wstart - margin, wend + margin]; margin 0 is the reference
+        // readers' WAVE= selection (ioutils.f90:752-753, 1496-1497)
         double w0 = c->wstart - margin, w1 = c->wend + margin;
         const double *wl = lines->wl;
         a.c0 = std::lower_bound(wl, wl + lines->n, w0) - wl;

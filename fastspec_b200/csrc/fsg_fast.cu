@@ -66,14 +66,6 @@ __device__ __forceinline__ float rcp_approx(float x) {
     return r;
 }
 
-// a = sqrt(twoA / 2) for the continued fraction: one MUFU operation (relative error ~2^-23) instead of
-// the correctly rounded square root's instruction sequence
-__device__ __forceinline__ float sqrt_approx(float x) {
-    float r;
-    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
-    return r;
-}
-
 // Wing pass.  Every window point outside the line's core range [cl, cr] has s >= 196 at every
 // depth, so there HVoigt * LinCop is the rational wing form alone:
 //   val = c1 (t + 1) / (t^2 + twoA),  t = dl^2 vv2 + c2m1
@@ -347,16 +339,20 @@ int fsg_launch_accum_batch(cudaStream_t st, int P, int ntau_max, const WingJob *
 // one 16-byte load from the cell-major copy of VgtTab.
 #define CORE_D 4
 
-__device__ __forceinline__ float hv_core32(const float4 *__restrict__ vtab4, float av, const CoreRec &c, float twoA) {
-    if (c.ia > 0 && av < 8.0f) {
-        const float fv = av * 125.0f;
+// HVoigt * LinCop where s < 196 (voigt.f90:81-107): the table lerp for a < 8 and v < 8, else the
+// continued fraction.  v = adl * LinVvgt, the table column iv and its fraction tv in FP64 as the
+// reference forms them; the lerp itself in FP32 on the FP32 table.
+__device__ __forceinline__ float hv_core32(const float4 *__restrict__ vtab4, double adl, const CoreRec &c) {
+    const double av = adl * c.vv;
+    if (c.ia > 0 && av < 8.0) {
+        const double fv = av * 125.0;
         const int iv = min((int)fv, FSG_NVV - 1);
-        const float tv = fv - (float)iv;
+        const float tv = (float)(fv - (double)iv);
         const float4 g = __ldg(vtab4 + (c.ia - 1) * FSG_NV1 + iv);
         const float c0 = g.x + tv * (g.y - g.x), c1 = g.z + tv * (g.w - g.z);
         return (c0 + c.ua * (c1 - c0)) * c.cop;
     }
-    return hv_cf32(av, sqrt_approx(0.5f * twoA), c.cop);
+    return hv_cf32((float)av, c.a, c.cop);
 }
 
 // One core-pass job: as WingJob plus the core records; tiles of 32 wavelengths
@@ -390,7 +386,8 @@ __device__ __forceinline__ void core_tile(const CoreJob &J, int tile, const floa
         if (h.cr < tile_first || h.cl > tile_last) continue;          // core range misses the tile
         if (p1 < h.cl || p1 > h.cr) continue;
         const float dl = (wvh - h.wlh) + (wvl - h.wll);
-        const float x = dl * dl, adl = fabsf(dl);
+        const float x = dl * dl;                          // the wing pass's x: the same branch split
+        const double adl = fabs(wd - ((double)h.wlh + (double)h.wll));
         const WingRec *wr = J.wing + (size_t)j * ntau + t0;
         const CoreRec *cr = J.core + (size_t)j * ntau + t0;
 #pragma unroll
@@ -401,7 +398,7 @@ __device__ __forceinline__ void core_tile(const CoreJob &J, int tile, const floa
                 const float t = fmaf(x, w.vv2, w.c2m1);
                 float v;
                 if (t < 195.5f) {
-                    v = hv_core32(vtab4, adl * c.vv, c, w.twoA);
+                    v = hv_core32(vtab4, adl, c);
                 } else {
                     v = fmaf(w.c1, t, w.c1) * rcp_approx(fmaf(t, t, w.twoA));
                 }

@@ -75,10 +75,13 @@ struct XCoef {
 //   H * LinCop = c1 (t + 1) / (t^2 + twoA),  t = dl^2 vv2 + c2m1,
 // with vv2 = LinVvgt^2, c2m1 = a^2 - 1/2, twoA = 2 a^2, c1 = LinCop a / sqrt(pi).
 struct __align__(16) WingRec { float vv2, c2m1, twoA, c1; };
-// Table / continued-fraction region (s < 196): LinVvgt, LinCop and the table row ia (1-based)
-// with its interpolation weight ua as HVoigt derives them from a (voigt.f90:84-92); ia = 0 when
-// a >= 8 (no table).  a itself is recovered as sqrt(twoA / 2) from the wing record.
-struct __align__(16) CoreRec { float vv, cop, ua; int ia; };
+// Table / continued-fraction region (s < 196): LinVvgt in FP64, LinCop, a, and the table row ia
+// (1-based) with its interpolation weight ua as HVoigt derives them from a in FP64
+// (voigt.f90:84-92); ia = 0 when a >= 8 (no table).  v = |dl| LinVvgt and the table column and
+// fraction are formed in FP64 as the reference forms them: on the Gaussian flanks of a line core
+// H falls as exp(-v^2), so an FP32 v (relative error ~1e-7) would move H by 2 v^2 * 1e-7.
+struct __align__(16) CoreRec { double vv; float cop, ua, a; int ia; int pad0, pad1; };
+static_assert(sizeof(CoreRec) == 32, "core record: 32 bytes");
 
 // Line header of a retained line inside a block (fast path).  The centre offset Wlcent is split
 // into FP32 wlh + wll (wlh = fl32(Wlcent), wll = fl32(Wlcent - wlh)).  [cl, cr] is the core range:

@@ -241,16 +241,16 @@ void fsg_launch_center(cudaStream_t s, const AtmView &A, const LineView &L, cons
 // Block refill: per retained line of the block, XlineSetup once then XlineDepth over depths.
 // ================================================================================================
 
-__global__ void k_params_fast(AtmView A, LineView L, const int64_t *__restrict__ idx, int64_t j0,
+// Line j of the block is list line idx[j0 + j * stride].
+__global__ void k_params_fast(AtmView A, LineView L, const int64_t *__restrict__ idx, int64_t j0, int64_t stride,
                               int64_t nb, const int32_t *__restrict__ flags,
                               const int32_t *__restrict__ ileft, const int32_t *__restrict__ iright,
                               const double *__restrict__ anode, const double *__restrict__ aida,
                               WingRec *wing, CoreRec *core, LineHdr *hdr) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= nb) return;
-    int64_t i = idx[j0 + j];
+    int64_t i = idx[j0 + j * stride];
     const int nt = A.ntau;
-    const float an1 = (float)anode[1], ai0 = (float)aida[0];
     int f = flags[i];
     double wlc = L.wl[i] - A.wfirst;
     XCoef XC;
@@ -269,15 +269,14 @@ __global__ void k_params_fast(AtmView A, LineView L, const int64_t *__restrict__
         w.c1 = (float)(cop * av * FSG_SQRTPIINV);
         vv2min = fminf(vv2min, w.vv2);
         CoreRec c;
-        c.vv = (float)vv; c.cop = (float)cop;
-        // table row and weight of a in FP32 (sqrt(a) nodes, voigt.f90:84-92); ia = 0: a >= 8
-        const float af = (float)av;
-        if (!(af < 8.0f)) { c.ia = 0; c.ua = 0.0f; }
-        else if (af < an1) { c.ia = 1; c.ua = af * ai0; }
+        c.vv = vv; c.cop = (float)cop; c.a = (float)av; c.pad0 = c.pad1 = 0;
+        // table row and weight of a in FP64 (sqrt(a) nodes, voigt.f90:84-92); ia = 0: a >= 8
+        if (!(av < 8.0)) { c.ia = 0; c.ua = 0.0f; }
+        else if (av < anode[1]) { c.ia = 1; c.ua = (float)(av * aida[0]); }
         else {
-            int ia = min((int)(sqrtf(af) * 141.42135623730951f) + 1, FSG_NVA);
+            const int ia = min((int)(sqrt(av) * (1.0 / (2.8284271247461903 / 400.0))) + 1, FSG_NVA);
             c.ia = ia;
-            c.ua = (af - (float)anode[ia - 1]) * (float)aida[ia - 1];
+            c.ua = (float)((av - anode[ia - 1]) * aida[ia - 1]);
         }
         wing[(size_t)j * nt + t] = w;
         core[(size_t)j * nt + t] = c;
@@ -310,11 +309,11 @@ __global__ void k_params_fast(AtmView A, LineView L, const int64_t *__restrict__
 }
 
 void fsg_launch_params_fast(cudaStream_t s, const AtmView &A, const LineView &L, const int64_t *idx,
-                            int64_t j0, int64_t nb, const int32_t *flags, const int32_t *ileft,
+                            int64_t j0, int64_t stride, int64_t nb, const int32_t *flags, const int32_t *ileft,
                             const int32_t *iright, const VoigtTables &T, WingRec *wing, CoreRec *core,
                             LineHdr *hdr) {
     if (nb <= 0) return;
-    k_params_fast<<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(A, L, idx, j0, nb, flags, ileft, iright,
+    k_params_fast<<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(A, L, idx, j0, stride, nb, flags, ileft, iright,
                                                                T.anode, T.aida, wing, core, hdr);
 }
 

@@ -55,6 +55,7 @@ extern "C" int fsg_locprf_pp_noalloc(int nprof, int nmu, const double *d_xmu, in
     int rc = work_ptr(dev, &work);
     if (rc != FSG_OK) return rc;
     cudaStream_t s = (cudaStream_t)stream;
+    cudaGetLastError();                 // an earlier call's leftover error is not this launch's
     fsg_launch_locprf(s, nprof, nmu, d_xmu, ntau, d_xki, d_src, d_rhox, d_ploc, work);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return FSG_E_CUDA;

@@ -142,7 +142,7 @@ class GpuBackend:
         return self.C.accumulate_dev(self.full, win[0].data_ptr(), win[1].data_ptr(), win[2].data_ptr(), i0, i1)
 
     def flux(self, i0, i1):
-        self.C.radtran_dev(None, None, self.sfl.data_ptr(), self.sfc.data_ptr())
+        self.C.radtran_range_dev(i0, i1, None, None, self.sfl.data_ptr(), self.sfc.data_ptr())
         return torch.stack([self.sfl[i0 - 1:i1], self.sfc[i0 - 1:i1]])
 
 
@@ -206,7 +206,7 @@ class BatchGpuBackend:
     contexts and the shared line list runs them in one graph replay; the fluxes come back as float64
     tensors on `device`."""
 
-    def __init__(self, F, make_context, lines, device, margin=10.0):
+    def __init__(self, F, make_context, lines, device, margin=0.0):
         self.F, self.make_context, self.lines, self.device, self.margin = F, make_context, lines, device, margin
         self.batch = None
 

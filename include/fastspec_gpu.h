@@ -161,9 +161,10 @@ int fsg_lineop_calc_dev(fsg_ctx *ctx, const fsg_lines *d_lines, fsg_stats *stats
  * list into caller-owned device arrays LinFlag / Ileft / Iright (n each) and returns the retained
  * count; fsg_accumulate_dev accumulates a device list whose windows are given onto the device
  * LineOpac, over wavelength indices i0..i1 (1-based, inclusive) only.  Each wavelength of the range
- * sums the same lines in the same order as a whole-grid fsg_lineop_calc_dev (equal to rounding:
- * the Kahan groups of a tile cut by the range ends, and the blocks of a class, may differ); other
- * wavelengths are left as they are.  Mixed precision only (FSG_E_STATE otherwise). */
+ * sums the same lines in the same order as a whole-grid fsg_lineop_calc_dev (mixed precision: equal
+ * to rounding, as the Kahan groups of a tile cut by the range ends, and the blocks of a class, may
+ * differ; FP64: the same segments and order, so equal bit for bit); other wavelengths are left as
+ * they are. */
 int fsg_central_dev(fsg_ctx *ctx, const fsg_lines *d_lines, int32_t *d_flags, int32_t *d_ileft,
                     int32_t *d_iright, int64_t *nkeep);
 int fsg_accumulate_dev(fsg_ctx *ctx, const fsg_lines *d_lines, const int32_t *d_flags,
@@ -181,6 +182,12 @@ int fsg_set_mu(fsg_ctx *ctx, int nmu, const double *xmu, const double *wmu);
  * spl/spc [nwl][nmu], sfl/sfc [nwl]; any output may be NULL.  Uses the device LineOpac. */
 int fsg_radtran(fsg_ctx *ctx, double *spl, double *spc, double *sfl, double *sfc);
 int fsg_radtran_dev(fsg_ctx *ctx, double *d_spl, double *d_spc, double *d_sfl, double *d_sfc);
+/* The same over the wavelength indices i0..i1 only (1-based, inclusive): the formal solver and flux
+ * of one wavelength shard.  The device outputs keep the whole grid's layout; rows i0..i1 are
+ * written, the others are left as they are.  RadTranCalc's loop over wavelengths is independent per
+ * wavelength (synth.f90:1825-1866), so each row equals the whole-grid call's. */
+int fsg_radtran_range_dev(fsg_ctx *ctx, int i0, int i1, double *d_spl, double *d_spc, double *d_sfl,
+                          double *d_sfc);
 
 /* DiskInteg with broadening (convol.f90:67-300): rotation (vsini [km/s], annulus kernels from the
  * nmu + 1 projected radii of fsg_mu_quadrature), radial-tangential macroturbulence (vmacro
@@ -223,7 +230,8 @@ int fsg_locprf_pp(fsg_ctx *ctx, int nprof, int nmu, const double *xmu, int ntau,
  * caller (xmu [nmu], xki/src [nprof][ntau], rhox [ntau], ploc [nprof][nmu]); the kernel's work
  * arrays sit in a fixed 8 MiB device array of the library, so nprof * ntau * 3 may not exceed
  * 1,048,576 (larger sizes return FSG_E_ARG).  stream is a cudaStream_t (NULL: the default
- * stream); the call returns after the kernel has finished.  The first call on a device looks up
+ * stream); the call waits for the kernel with cudaStreamSynchronize on that stream and returns
+ * after it has finished.  The first call on a device looks up
  * the array's device address with that device current; make that first call before any stream
  * capture.  All calls share the array, so calls that overlap on the GPU race. */
 int fsg_locprf_pp_noalloc(int nprof, int nmu, const double *d_xmu, int ntau, const double *d_xki,
@@ -253,8 +261,13 @@ int fsg_adjoint_dev(fsg_ctx *ctx, const fsg_lines *d_lines, const double *d_gflu
 
 /* ---- batched synthesis ---------------------------------------------------------------------
  * Many atmospheres (each a context with grid, atmosphere, continuum and mu set; mixed precision)
- * and one line list sorted by wavelength: per atmosphere the lines with centres inside its grid
- * +- margin [A] take the central pass and block refill, then one persistent wing-pass launch and
+ * and one line list sorted by wavelength: per atmosphere the lines with centres in
+ * [wstart - margin, wend + margin] [A] take the central pass and block refill.  margin = 0 is the
+ * reference's own rule: a synthesis over [Wstart, Wend] reads the lines whose centres lie in that
+ * range (ReadHDF, ioutils.f90:752-753; ReadAscMag, ioutils.f90:1496-1497), so each atmosphere's
+ * result is the reference's run of its deck on the shared list; margin > 0 adds the lines just
+ * outside, whose windows the reference's WaveIdx clamps to the grid's ends (opacity.f90:594-608).
+ * Then one persistent wing-pass launch and
  * one persistent core-pass launch take (atmosphere, tile) items from device work queues, then the
  * formal solver and flux run per atmosphere.  The sequence has no host synchronisation; the
  * first fsg_batch_run tunes it (unless fsg_batch_set_tuning gave a choice), captures it as a CUDA

@@ -85,6 +85,9 @@ def lib():
         L.or_xline.argtypes = [C.POINTER(_State), C.POINTER(_Lines), C.c_long, _dp, _dp, _dp]
         L.or_lineop_calc.argtypes = [C.POINTER(_State), C.POINTER(_Lines), C.c_int, C.c_long, _dp,
                                      _ip, _ip, _ip, _fp, C.c_int, _dp, _dp, C.POINTER(_Stats)]
+        L.or_lineop_calc_range.argtypes = [C.POINTER(_State), C.POINTER(_Lines), C.c_int, C.c_long, _dp,
+                                           _ip, _ip, _ip, _fp, C.c_int, _dp, _dp, C.POINTER(_Stats),
+                                           C.c_int, C.c_int]
         L.or_mag_lineop_calc.argtypes = [C.POINTER(_State), C.POINTER(_Lines), C.c_int, _dp,
                                          C.c_long, _dp, _ip, _ip, _ip, _fp, C.c_int, _dp, _dp,
                                          C.POINTER(_Stats)]
@@ -283,6 +286,17 @@ class Lines:
         self.n = n
 
 
+def reader_select(arrays, wstart, wend):
+    """The lines a synthesis over [wstart, wend] reads from a list sorted by wavelength: those with
+    wstart <= wl <= wend, as ReadHDF locates them (LowerBoundReal8 / UpperBoundReal8 on the sorted
+    wavelength column, ioutils.f90:752-753) and ReadAscMag packs them (ioutils.f90:1496-1497).
+    arrays: dict of per-line numpy arrays with "wl"; returns the same dict restricted."""
+    wl = arrays["wl"]
+    i1 = int(np.searchsorted(wl, wstart, side="left"))
+    i2 = int(np.searchsorted(wl, wend, side="right"))
+    return {k: np.ascontiguousarray(v[i1:i2]) for k, v in arrays.items()}
+
+
 def xline(state, lines, i):
     n = state.ntau
     cop, vv, av = (np.zeros(n) for _ in range(3))
@@ -292,8 +306,10 @@ def xline(state, lines, i):
 
 
 def lineop_calc(state, lines, list_type=2, nlines_lim=0, lineopac=None, nmu=0, xmu=None, wmu=None,
-                want_linstr=False):
-    """LineopCalc.  Returns dict(lineopac [nwl][ntau], flags, ileft, iright, stats, linstr)."""
+                want_linstr=False, wrange=None):
+    """LineopCalc.  Returns dict(lineopac [nwl][ntau], flags, ileft, iright, stats, linstr).
+    wrange = (i0, i1), 1-based inclusive: windows on the whole grid, accumulation only over those
+    wavelengths (the rows of a whole-grid run; other rows stay zero)."""
     n = lines.n
     lo = np.zeros((state.nwl, state.ntau)) if lineopac is None else lineopac
     flags = np.zeros(max(n, 1), np.int32); il = np.zeros(max(n, 1), np.int32)
@@ -301,10 +317,11 @@ def lineop_calc(state, lines, list_type=2, nlines_lim=0, lineopac=None, nmu=0, x
     ls = np.zeros(max(n, 1), np.float32) if want_linstr else None
     st = _Stats()
     xmu = _f64(xmu); wmu = _f64(wmu)
-    rc = lib().or_lineop_calc(C.byref(state.s), C.byref(lines.L), int(list_type), int(nlines_lim),
-                              _p(lo, C.c_double), _p(flags, C.c_int), _p(il, C.c_int), _p(ir, C.c_int),
-                              _p(ls, C.c_float), int(nmu), _p(xmu, C.c_double), _p(wmu, C.c_double),
-                              C.byref(st))
+    i0, i1 = (1, state.nwl) if wrange is None else (int(wrange[0]), int(wrange[1]))
+    rc = lib().or_lineop_calc_range(C.byref(state.s), C.byref(lines.L), int(list_type), int(nlines_lim),
+                                    _p(lo, C.c_double), _p(flags, C.c_int), _p(il, C.c_int), _p(ir, C.c_int),
+                                    _p(ls, C.c_float), int(nmu), _p(xmu, C.c_double), _p(wmu, C.c_double),
+                                    C.byref(st), i0, i1)
     if rc != 0:
         raise RuntimeError("or_lineop_calc failed: %d" % rc)
     return dict(lineopac=lo, flags=flags[:n], ileft=il[:n], iright=ir[:n], linstr=None if ls is None else ls[:n],

@@ -870,8 +870,19 @@ int or_lineop_calc(const or_state *s, const or_lines *L, int list_type, long nli
                    double *lineopac, int *flags_out, int *ileft_out, int *iright_out,
                    float *linstr_out, int nmu, const double *xmu, const double *wmu,
                    or_stats *st) {
+    return or_lineop_calc_range(s, L, list_type, nlines_lim, lineopac, flags_out, ileft_out, iright_out,
+                                linstr_out, nmu, xmu, wmu, st, 1, s->nwl);
+}
+
+/* LineopCalc with the accumulation restricted to the wavelengths [r0, r1] */
+int or_lineop_calc_range(const or_state *s, const or_lines *L, int list_type, long nlines_lim,
+                         double *lineopac, int *flags_out, int *ileft_out, int *iright_out,
+                         float *linstr_out, int nmu, const double *xmu, const double *wmu,
+                         or_stats *st, int r0, int r1) {
     or_voigt_init();
     int nt = s->ntau, nwl = s->nwl;
+    if (r0 < 1) r0 = 1;
+    if (r1 > nwl) r1 = nwl;
     long N = L->n;
     long nstep = (nlines_lim > 0 && nlines_lim < N) ? nlines_lim : N;
     linework W; W.n = N;
@@ -949,12 +960,13 @@ int or_lineop_calc(const or_state *s, const or_lines *L, int list_type, long nli
             xcoef XC; long i0 = W.orig[il];
             xline_setup(s, L, i0, W.wlcent[il], W.flag[il], &XC);
             for (int t = 0; t < nt; t++) xline_depth(s, t, &XC, &cop[t], &vv[t], &av[t]);
-            wide_evals += (double)nt * (W.iright[il] - W.ileft[il] + 1);
+            const int wa = W.ileft[il] > r0 ? W.ileft[il] : r0, wb = W.iright[il] < r1 ? W.iright[il] : r1;
+            if (wa <= wb) wide_evals += (double)nt * (wb - wa + 1);
             #pragma omp parallel
             {
                 double *lo = (double *)malloc(sizeof(double) * nt);
                 #pragma omp for schedule(dynamic, 1000)
-                for (int iwl = W.ileft[il]; iwl <= W.iright[il]; iwl++) {
+                for (int iwl = wa; iwl <= wb; iwl++) {
                     lineopacity2(s, s->wave[iwl - 1], &W, il, iwl, cop, vv, av, lo);
                     double *dst = lineopac + (size_t)(iwl - 1) * nt;
                     for (int t = 0; t < nt; t++) dst[t] = dst[t] + lo[t];
@@ -989,8 +1001,9 @@ int or_lineop_calc(const or_state *s, const or_lines *L, int list_type, long nli
         #pragma omp parallel reduction(+:evals)
         {
             double *lo = (double *)malloc(sizeof(double) * nt);
+            const int pa = iwl1 > r0 ? iwl1 : r0, pb = iwl2 < r1 ? iwl2 : r1;
             #pragma omp for schedule(dynamic)
-            for (int iwl = iwl1; iwl <= iwl2; iwl++) {
+            for (int iwl = pa; iwl <= pb; iwl++) {
                 double Wl = s->wave[iwl - 1];
                 for (int t = 0; t < nt; t++) lo[t] = 0.0;
                 for (long il = Lstart[iwl - 1]; il <= Lstop[iwl - 1]; il++) {

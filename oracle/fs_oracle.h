@@ -135,6 +135,14 @@ int or_lineop_calc(const or_state *s, const or_lines *L, int list_type, long nli
                    double *lineopac, int *flags_out, int *ileft_out, int *iright_out,
                    float *linstr_out, int nmu, const double *xmu, const double *wmu,
                    or_stats *st);
+/* The same with the accumulation (wide lines and LineOpacity1) restricted to the wavelengths
+ * [i0, i1] (1-based, inclusive) of the grid; windows, rejection and segments are those of the whole
+ * grid.  The reference's accumulation is independent per wavelength (synth.f90:1075-1080), so the
+ * rows [i0, i1] equal the whole-grid call's; the other rows are left untouched. */
+int or_lineop_calc_range(const or_state *s, const or_lines *L, int list_type, long nlines_lim,
+                         double *lineopac, int *flags_out, int *ileft_out, int *iright_out,
+                         float *linstr_out, int nmu, const double *xmu, const double *wmu,
+                         or_stats *st, int i0, int i1);
 
 /* MagLineopCalc (synth.f90:1098-1455); maglineopac [nwl][ntau][6] accumulated. */
 int or_mag_lineop_calc(const or_state *s, const or_lines *L, int bframe, const double *bfield,

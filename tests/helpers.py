@@ -76,3 +76,51 @@ def sphere_pin(part):
         out.update({k: v for k, v in d.items() if k.startswith("z_")})
         out["vmicro"], out["molbrd"] = 1.0, 0
     return out
+
+
+def device_molecular_lines(n, wmin, wmax, seed, device):
+    """A cool-dwarf list of n lines drawn on the device with the distributions of
+    workloads.molecular_lines (wavenumber uniform over [1e8/wmax, 1e8/wmin], four species at 25 %,
+    log gf ~ N(-5, 1.5), E_low ~ Exp(1 eV) capped at 5 eV, log G6/NH ~ U(-8, -7), Grad = Gqst = 0),
+    sorted by wavelength: dict of device tensors.  Seeded torch generator on the device; drawing 1e8
+    lines takes well under a second there, against minutes on the host."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    sig = torch.empty(n, dtype=torch.float64, device=device).uniform_(1e8 / wmax, 1e8 / wmin, generator=g)
+    wl, order = torch.sort(1e8 / sig)
+    del sig
+    out = {"wl": wl.contiguous()}
+    spc = torch.randint(0, 4, (n,), generator=g, device=device, dtype=torch.int32)
+    out["spc"] = spc[order].contiguous()
+    del spc
+    lg = torch.empty(n, dtype=torch.float32, device=device).normal_(-5.0, 1.5, generator=g)
+    out["gf"] = torch.pow(10.0, lg[order]).contiguous()
+    del lg
+    el = torch.empty(n, dtype=torch.float32, device=device).exponential_(1.0, generator=g)
+    out["elo"] = torch.clamp(el[order], max=5.0).contiguous()
+    del el
+    lv = torch.empty(n, dtype=torch.float32, device=device).uniform_(-8.0, -7.0, generator=g)
+    out["gvdw"] = torch.pow(10.0, lv[order]).contiguous()
+    del lv, order
+    out["grad"] = torch.zeros(n, dtype=torch.float32, device=device)
+    out["gqst"] = torch.zeros(n, dtype=torch.float32, device=device)
+    out["ismol"] = torch.ones(n, dtype=torch.int32, device=device)
+    return out
+
+
+def device_view(F, dt, a=0, b=None, kind=2):
+    """fsg_lines view (CLines) of lines [a, b) of a dict of device tensors."""
+    import ctypes as C
+    b = int(dt["wl"].numel()) if b is None else b
+    v = F.CLines()
+    v.n = b - a
+    v.kind = kind
+    ptr = lambda t, ct: C.cast(t.data_ptr() + a * t.element_size(), C.POINTER(ct))
+    v.wl = ptr(dt["wl"], C.c_double)
+    for k in ("elo", "gf", "grad", "gqst", "gvdw"):
+        setattr(v, k, ptr(dt[k], C.c_float))
+    v.spc = ptr(dt["spc"], C.c_int32)
+    if "ismol" in dt:
+        v.ismol = ptr(dt["ismol"], C.c_int32)
+    return v

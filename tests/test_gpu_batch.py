@@ -1,14 +1,14 @@
 """Batched synthesis on the GPU (fsg_batch_*): each atmosphere's flux against the oracle run on the
-same candidate lines (mixed-path flux tolerance 1e-5) and against the single-context path; graph
-replays are deterministic; a given tuning is applied."""
+whole shared list as the reference would read it for that atmosphere's deck (the lines with centres
+in [Wstart, Wend], ioutils.f90:752-753, 1496-1497; mixed-path flux tolerance 1e-5) and against the
+single-context path; with a margin, against the oracle on the lines the margin adds; graph replays
+are deterministic; a given tuning is applied."""
 import numpy as np
 import pytest
 
 import helpers as H
 
 pytestmark = pytest.mark.gpu
-
-MARGIN = 10.0
 
 
 def small_batch(fsg, natm=4, span=3.0, nlines=120_000, seed=5):
@@ -35,21 +35,26 @@ def small_batch(fsg, natm=4, span=3.0, nlines=120_000, seed=5):
     return ctxs, cases, arr
 
 
-def candidates(arr, g):
-    sel = (arr["wl"] >= g["wstart"] - MARGIN) & (arr["wl"] <= g["wend"] + MARGIN)
+def candidates(arr, g, margin=0.0):
+    sel = (arr["wl"] >= g["wstart"] - margin) & (arr["wl"] <= g["wend"] + margin)
     return {k: np.ascontiguousarray(v[sel]) for k, v in arr.items()}
 
 
-def test_batch_flux_vs_oracle_and_single_context(fsg, oracle_mod):
+@pytest.mark.parametrize("margin", [0.0, 2.0])
+def test_batch_flux_vs_oracle_and_single_context(fsg, oracle_mod, margin):
     ctxs, cases, arr = small_batch(fsg)
-    B = fsg.Batch(ctxs, fsg.LineList.from_arrays(arr), margin=MARGIN)
+    B = fsg.Batch(ctxs, fsg.LineList.from_arrays(arr), margin=margin)
     st = B.run()
     assert st["natm"] == len(ctxs) and st["line_evals"] > 0 and st["ms_total"] > 0
     assert st["tuning"]["tile_pix"] in (64, 128)
     x, w, _ = oracle_mod.mu_quadrature(1, 7)
+    ncand = 0
     for i, (g, state, co) in enumerate(cases):
         sfl, sfc = B.flux(i)
-        cand = candidates(arr, g)
+        # margin 0: the oracle reads the whole shared list with the reference's WAVE= selection
+        cand = (oracle_mod.reader_select(arr, g["wstart"], g["wend"]) if margin == 0.0
+                else candidates(arr, g, margin))
+        ncand += len(cand["wl"])
         S = oracle_mod.State(g, state, contopac=co, vmicro=1.0)
         r = oracle_mod.lineop_calc(S, oracle_mod.Lines(**cand, kind=2), list_type=2)
         osfl, osfc = oracle_mod.disk_integ(w, *oracle_mod.radtran(S, x, r["lineopac"]))
@@ -61,12 +66,13 @@ def test_batch_flux_vs_oracle_and_single_context(fsg, oracle_mod):
         C.lineop_calc(fsg.LineList.from_arrays(cand), want_lineopac=False, want_lines=False)
         _, _, csfl, _ = C.radtran()
         assert np.max(np.abs(sfl / csfl - 1)) < 1e-6
+    assert st["nlines_candidate"] == ncand
     B.close()
 
 
 def test_batch_replay_and_given_tuning(fsg):
     ctxs, cases, arr = small_batch(fsg, natm=3, seed=6)
-    B = fsg.Batch(ctxs, fsg.LineList.from_arrays(arr), margin=MARGIN)
+    B = fsg.Batch(ctxs, fsg.LineList.from_arrays(arr))
     B.run()
     f1 = [B.flux(i)[0] for i in range(3)]
     B.run()
@@ -102,7 +108,7 @@ def test_batch_axis_shares(fsg):
     from fastspec_b200 import shard
     ctxs, cases, arr = small_batch(fsg, natm=5, seed=8)
     lines = fsg.LineList.from_arrays(arr)
-    B = fsg.Batch(ctxs, lines, margin=MARGIN)
+    B = fsg.Batch(ctxs, lines)
     B.run()
     whole = [np.stack(B.flux(i)) for i in range(len(ctxs))]
     B.close()

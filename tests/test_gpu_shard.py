@@ -64,17 +64,48 @@ def test_central_slices_and_range_accumulation(fsg):
     assert np.max(np.abs(f[1] / sfc[i0 - 1:i1] - 1)) < 1e-12
 
 
-def test_range_accumulation_rejects_fp64_and_bad_ranges(fsg):
-    grid, st, co, arr = cooldwarf_case(n=50)
-    C = make(fsg, grid, st, co, prec=fsg.PREC_FP64)
-    dt = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in arr.items()}
+def test_range_accumulation_fp64_and_bad_ranges(fsg):
+    """FP64: adjacent ranges rebuild the whole-grid LineOpac bit for bit (same segments, same order
+    per wavelength); ranges outside 1..nwl or empty are refused."""
     from fastspec_b200 import shard
+    grid, st, co, arr = cooldwarf_case(n=3000, seed=24)
+    C = make(fsg, grid, st, co, prec=fsg.PREC_FP64)
+    full = C.lineop_calc(fsg.LineList.from_arrays(arr))
+    dt = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in arr.items()}
     B = shard.GpuBackend(fsg, C, dt)
     win = B.central(0, B.n, B.n)
+    assert np.array_equal(win[1].cpu().numpy(), full["ileft"])
+    C.lineop_reset()
+    nwl = C.nwl
+    for i0, i1 in ((1, nwl // 3), (nwl // 3 + 1, nwl // 2), (nwl // 2 + 1, nwl)):
+        C.accumulate_dev(B.full, win[0].data_ptr(), win[1].data_ptr(), win[2].data_ptr(), i0, i1)
+    assert np.array_equal(C.lineop_get(), full["lineopac"])
     with pytest.raises(fsg.FsgError):
-        C.accumulate_dev(B.full, win[0].data_ptr(), win[1].data_ptr(), win[2].data_ptr(), 1, C.nwl)
-    C2 = make(fsg, grid, st, co)
+        C.accumulate_dev(B.full, win[0].data_ptr(), win[1].data_ptr(), win[2].data_ptr(), 0, nwl)
     with pytest.raises(fsg.FsgError):
-        C2.accumulate_dev(B.full, win[0].data_ptr(), win[1].data_ptr(), win[2].data_ptr(), 0, C2.nwl)
+        C.accumulate_dev(B.full, win[0].data_ptr(), win[1].data_ptr(), win[2].data_ptr(), 5, 4)
+
+
+def test_radtran_range_solves_only_its_rows(fsg):
+    """fsg_radtran_range_dev writes rows i0..i1 of whole-grid outputs, equal to the whole-grid solve,
+    and leaves the other rows as they were."""
+    grid, st, co, arr = cooldwarf_case(n=800, seed=25)
+    C = make(fsg, grid, st, co)
+    C.lineop_calc(fsg.LineList.from_arrays(arr), want_lineopac=False, want_lines=False)
+    spl, spc, sfl, sfc = C.radtran()
+    nwl, nmu = C.nwl, C.nmu
+    i0, i1 = nwl // 4, nwl // 2
+    out = [torch.full((nwl, nmu), -7.0, dtype=torch.float64, device="cuda"),
+           torch.full((nwl, nmu), -7.0, dtype=torch.float64, device="cuda"),
+           torch.full((nwl,), -7.0, dtype=torch.float64, device="cuda"),
+           torch.full((nwl,), -7.0, dtype=torch.float64, device="cuda")]
+    torch.cuda.synchronize()
+    C.radtran_range_dev(i0, i1, *[t.data_ptr() for t in out])
+    got = [t.cpu().numpy() for t in out]
+    for g, ref in zip(got, (spl, spc, sfl, sfc)):
+        assert np.array_equal(g[i0 - 1:i1], ref[i0 - 1:i1])
+        assert np.all(g[:i0 - 1] == -7.0) and np.all(g[i1:] == -7.0)
     with pytest.raises(fsg.FsgError):
-        C2.accumulate_dev(B.full, win[0].data_ptr(), win[1].data_ptr(), win[2].data_ptr(), 5, 4)
+        C.radtran_range_dev(0, 5, None, None, out[2].data_ptr(), None)
+    with pytest.raises(fsg.FsgError):
+        C.radtran_range_dev(10, nwl + 1, None, None, out[2].data_ptr(), None)
