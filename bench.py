@@ -14,10 +14,15 @@ summed over retained lines), plus spectra/s.  `value` times the mixed-precision 
 line list resident in HBM; `e2e` times the public C-ABI call with host (pinned) buffers, the
 host->device copy of the line list and the device->host read of the flux inside each step.
 
+Line blocks are capped at 2 GB (the configuration's "lines streamed in 2 GB blocks", LIMITRAM);
+`limitram_24gb` repeats one step with 24 GB blocks.  `plain_fp64` runs the plain FP64-faithful GPU
+path once on the whole list.
+
 --impl reference: the reference's CPU implementation of the path timed on this host: its own
 OpenMP executable (copied unmodified to baseline/_ref by the build; there is no Fortran compiler to
-build it) on all host threads, on a bounded wavelength sample of the same workload, or, without the
-executable, the FP64 C restatement (oracle/) with OpenMP.
+build it) on all host threads, on the configuration's whole grid with a uniform random subsample of
+the line list per step (RefSampler), or, without the executable, the FP64 C restatement (oracle/)
+with OpenMP.  That arm loads nothing of the CUDA library.
 """
 import argparse
 import json
@@ -36,7 +41,10 @@ sys.path.insert(0, os.path.join(HERE, "tests"))
 METRIC = "Voigt line-evals/s (cool-dwarf 1e8-line synthesis)"
 UNIT = "line-evals/s"
 FLOPS_PER_EVAL = 12          # nominal FP32 work of one wing evaluation (v^2, rational, scale, sum)
-W0, W1, DSTEP, NMU = 5000.0, 25000.0, 1.0, 7
+W0, W1, DSTEP, NMU = 5000.0, 25000.0, 2.99792458e5 / 3e5, 7      # R = 3e5 on the ln-lambda grid
+LIMITRAM_GB = 2.0            # the configuration's 2 GB line blocks
+WORKLOAD = ("cool-dwarf molecular synthesis, 1e8 lines, 72 depths (71 after the model's temperature check), "
+            "R = 3e5 (5000-25000 A), 7 mu, 2 GB line blocks")
 
 
 def parse():
@@ -49,11 +57,13 @@ def parse():
     p.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
-    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--limitram", type=float, default=LIMITRAM_GB, help="line-block memory cap [GB]")
     p.add_argument("--no-plain", action="store_true", help="skip the plain FP64 path comparison")
     p.add_argument("--shard", action="store_true",
                    help="run the wavelength-sharded synthesis even on one GPU (a process group of one)")
-    p.add_argument("--plain-lines", type=float, default=1e6)
+    p.add_argument("--plain-lines", type=float, default=-1,
+                   help="lines of the plain FP64 comparison; default: the whole headline list")
+    p.add_argument("--no-extra", action="store_true", help="skip the 24 GB block-size step")
     p.add_argument("--no-batched", action="store_true", help="skip the batched-grid measurement")
     p.add_argument("--batch-atm", type=int, default=256)
     p.add_argument("--batch-lines", type=float, default=2e6)
@@ -119,64 +129,66 @@ class ClockSampler:
 
 
 # ---- GPU arm -------------------------------------------------------------------------------------
-def device_lines(F, torch, arr, dev):
-    """Device copies of a line list and the fsg_lines view of them (kind 2, molecular SoA)."""
-    dt = {k: torch.from_numpy(np.ascontiguousarray(v)).to(f"cuda:{dev}") for k, v in arr.items()}
-    dl = F.CLines()
-    dl.n = int(dt["wl"].numel())
-    dl.kind = 2
-    dl.wl = F.C.cast(dt["wl"].data_ptr(), F._dp)
-    for k in ("elo", "gf", "grad", "gqst", "gvdw"):
-        setattr(dl, k, F.C.cast(dt[k].data_ptr(), F._fp))
-    dl.spc = F.C.cast(dt["spc"].data_ptr(), F._ip)
-    dl.ismol = F.C.cast(dt["ismol"].data_ptr(), F._ip)
-    return dt, dl
+def device_list(F, torch, nlines, dev, seed):
+    """The headline list drawn on the device (seeded torch generator with the distributions of
+    workloads.molecular_lines, sorted by wavelength; 1e8 lines in about a second instead of minutes on
+    the host) and its fsg_lines view."""
+    import helpers as H
+    dt = H.device_molecular_lines(int(nlines), W0, W1, seed, torch.device("cuda", dev))
+    return dt, H.device_view(F, dt)
 
 
-def plain_vs_mixed(F, torch, st, meta, co, dev, nlines):
-    """The same synthesis through the plain FP64 path and the mixed path on a smaller list with the
-    same distributions over the full grid: line-evals/s of each, and the flux difference."""
-    from fastspec_b200 import workloads as W
-    arr = W.molecular_lines(nlines, W0, W1, W.SEED0 + 7, exact=False).arrays()
+def plain_fp64(F, torch, st, meta, co, dev, dt, nlines, mixed):
+    """The plain FP64-faithful GPU path (LineOpacity1's per-wavelength order and FP64 table lerp, the
+    reference's PACK / wide lines / segments) on the headline list, or on a uniform subsample of
+    nlines of it, one synthesis timed with CUDA events; against the mixed path on the same lines.
+    mixed: (ms per step, flux) of the headline's mixed path on the whole list.  Its blocks hold 24 GB of
+    FP64 records: with 2 GB blocks the lines that reach one wavelength exceed one block and the
+    segmentation stops as the reference's does (synth.f90:1035-1040)."""
+    import helpers as H
+    n_all = int(dt["wl"].numel())
+    if nlines <= 0 or nlines >= n_all:
+        sub, nlines = dt, n_all
+    else:
+        step = n_all // int(nlines)
+        sub = {k: v[::step].contiguous() for k, v in dt.items()}
+        nlines = int(sub["wl"].numel())
+    dl = H.device_view(F, sub)
     x, w, _ = F.mu_quadrature(1, NMU)
-    out = {}
-    flux = {}
+    out, flux = {}, {}
     for name, prec in (("fp64", F.PREC_FP64), ("mixed", F.PREC_MIXED)):
-        C = F.Context(device=dev, precision=prec, vmicro=meta["vmicro"], molbrd=meta["molbrd"], limitram_gb=24.0)
+        if name == "mixed" and sub is dt:
+            out["mixed"] = {"ms": mixed[0]}
+            flux["mixed"] = mixed[1]
+            continue
+        C = F.Context(device=dev, precision=prec, vmicro=meta["vmicro"], molbrd=meta["molbrd"],
+                      limitram_gb=24.0 if prec == F.PREC_FP64 else LIMITRAM_GB)
         C.set_grid(1, W0, W1, DSTEP)
         C.set_atmosphere(st)
         C.set_contopac(co)
         C.set_mu(x, w)
-        dt, dl = device_lines(F, torch, arr, dev)
         sfl = torch.empty(C.nwl, dtype=torch.float64, device=f"cuda:{dev}")
         sfc = torch.empty_like(sfl)
         stream = torch.cuda.ExternalStream(C.stream_ptr(), device=dev)
-
-        def step():
-            C.lineop_reset()
-            s_ = C.lineop_calc_dev(dl)
-            C.radtran_dev(None, None, sfl.data_ptr(), sfc.data_ptr())
-            return s_
-
-        step()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        s_ = step()
+        C.lineop_reset()
+        s_ = C.lineop_calc_dev(dl)
+        C.radtran_dev(None, None, sfl.data_ptr(), sfc.data_ptr())
         e1.record(stream)
         e1.synchronize()
-        ms = e0.elapsed_time(e1)
-        ev = s_["line_evals"] if prec == F.PREC_MIXED else None
-        out[name] = {"ms": ms, "ms_accum": s_["ms_accum"], "stats_evals": s_["line_evals"]}
-        flux[name] = sfl.cpu().numpy() / sfc.cpu().numpy()
-        if ev is not None:
-            out["evals"] = ev
+        out[name] = {"ms": e0.elapsed_time(e1), "ms_center": s_["ms_center"], "ms_accum": s_["ms_accum"],
+                     "line_evals": s_["line_evals"], "segments_or_blocks": s_["nblocks"], "wide": s_["nwide"]}
+        flux[name] = (sfl / sfc).cpu().numpy()
         C.close()
-    ev = out["evals"]
-    return {"sample": "%d lines, same distributions, full grid" % nlines,
-            "fp64_value": ev / (out["fp64"]["ms"] / 1e3), "mixed_value": ev / (out["mixed"]["ms"] / 1e3),
-            "unit": UNIT, "speedup": out["fp64"]["ms"] / out["mixed"]["ms"],
-            "fp64_ms": out["fp64"]["ms"], "mixed_ms": out["mixed"]["ms"],
+        del sfl, sfc
+    ev = out["fp64"]["line_evals"]
+    return {"lines": nlines, "sample": "the whole headline list" if sub is dt else
+            "every %d-th line of the headline list" % (n_all // nlines),
+            "fp64": out["fp64"], "mixed_ms": out["mixed"]["ms"],
+            "fp64_value": ev / (out["fp64"]["ms"] / 1e3), "unit": UNIT,
+            "mixed_over_fp64": out["fp64"]["ms"] / out["mixed"]["ms"],
             "flux_max_rel_diff": float(np.max(np.abs(flux["mixed"] / flux["fp64"] - 1.0)))}
 
 
@@ -284,7 +296,7 @@ def differentiable_fit(F, torch, dev, steps, warmup):
     wave = F.make_grid(0, w0, w1, step) + w0
     lk = np.log(d["cont_opac"])
     co = np.exp(np.stack([np.interp(wave, d["cont_wave"], lk[:, t]) for t in range(lk.shape[1])], axis=1))
-    arr = W.atomic_lines(100_000, w0 - 0.5, w1 + 0.5, W.SEED0 + 4, exact=False).arrays()
+    arr = W.atomic_lines(100_000, w0, w1, W.SEED0 + 4, exact=False).arrays()
     M = AD.FluxModel(F, grid, st, co, arr, species, vmicro=float(d["vmicro"]), device=dev)
     loggf0 = np.log10(arr["gf"].astype(np.float64))
     rng = np.random.default_rng(W.SEED0 + 4)
@@ -403,20 +415,23 @@ def run_gpu(args, rank, world):
     wave = F.make_grid(1, W0, W1, DSTEP)
     co = contopac_for(meta, wave + W0)
     nlines = int(args.lines)
-    L = W.molecular_lines(nlines, W0, W1, W.SEED0 + 1, exact=False)
-    arr = L.arrays()
     x, w, _ = F.mu_quadrature(1, NMU)
     prec = F.PREC_MIXED if args.precision == "mixed" else F.PREC_FP64
-    C = F.Context(device=dev, precision=prec, vmicro=meta["vmicro"], molbrd=meta["molbrd"], limitram_gb=24.0)
-    C.set_grid(1, W0, W1, DSTEP)
-    C.set_atmosphere(st)
-    C.set_contopac(co)
-    C.set_mu(x, w)
+
+    def make_context(limitram):
+        c = F.Context(device=dev, precision=prec, vmicro=meta["vmicro"], molbrd=meta["molbrd"], limitram_gb=limitram)
+        c.set_grid(1, W0, W1, DSTEP)
+        c.set_atmosphere(st)
+        c.set_contopac(co)
+        c.set_mu(x, w)
+        return c
+
+    C = make_context(args.limitram)
     nwl, ntau = C.nwl, C.ntau
     stream = torch.cuda.ExternalStream(C.stream_ptr(), device=dev)
 
-    # resident device copies of the line list (value arm)
-    dt, dl = device_lines(F, torch, arr, dev)
+    # the line list, resident in HBM (value arm)
+    dt, dl = device_list(F, torch, nlines, dev, W.SEED0 + 1)
     spl = torch.empty((nwl, NMU), dtype=torch.float64, device=f"cuda:{dev}")
     spc = torch.empty_like(spl)
     sfl = torch.empty(nwl, dtype=torch.float64, device=f"cuda:{dev}")
@@ -484,10 +499,32 @@ def run_gpu(args, rank, world):
 
     out = dict(ms=ms, evals=evals, stats=stats[-1], launches=launches, clocks=clk.summary(), nwl=nwl,
                ntau=ntau, nlines=nlines)
+    if use_shard:
+        mixed_flux = (sharded["res"]["flux"][0] / sharded["res"]["flux"][1]).cpu().numpy()
+    else:
+        mixed_flux = (sfl / sfc).cpu().numpy()
+
+    # the same step with 24 GB line blocks
+    if not args.no_extra and not use_shard:
+        C24 = make_context(24.0)
+        stream24 = torch.cuda.ExternalStream(C24.stream_ptr(), device=dev)
+        for _ in range(2):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream24)
+            C24.lineop_reset()
+            s24 = C24.lineop_calc_dev(dl)
+            C24.radtran_dev(spl.data_ptr(), spc.data_ptr(), sfl.data_ptr(), sfc.data_ptr())
+            e1.record(stream24)
+            e1.synchronize()
+        out["limitram_24gb"] = {"ms_per_step": e0.elapsed_time(e1), "wing_ms": s24["ms_wing_kernels"],
+                                "core_ms": s24["ms_core_kernels"], "blocks": s24["nblocks"],
+                                "line_evals_per_s": s24["line_evals"] / (e0.elapsed_time(e1) / 1e3)}
+        C24.close()
 
     # e2e arm: host pinned line list through fsg_lineop_calc + fsg_radtran (flux read back)
     if not args.no_e2e:
-        pin = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory() for k, v in arr.items()}
+        pin = {k: v.cpu().pin_memory() for k, v in dt.items()}
         hl = F.CLines()
         hl.n = nlines
         hl.kind = 2
@@ -524,9 +561,10 @@ def run_gpu(args, rank, world):
         h2d = sum(int(v.numel() * v.element_size()) for v in pin.values())
         out.update(ms_e2e=ms_e2e, h2d=h2d, d2h=2 * nwl * 8, flux_check=float(hsfl[nwl // 2].item()))
     C.close()
-    del dt
     if not args.no_plain and rank == 0:
-        out["plain"] = plain_vs_mixed(F, torch, st, meta, co, dev, int(args.plain_lines))
+        out["plain"] = plain_fp64(F, torch, st, meta, co, dev, dt, int(args.plain_lines), (ms / args.steps, mixed_flux))
+    del dt, dl
+    torch.cuda.empty_cache()
     if not args.no_stokes and rank == 0:
         out["stokes"] = stokes_synthesis(F, torch, dev, args.steps, args.warmup)
     if not args.no_fit and rank == 0:
@@ -536,40 +574,19 @@ def run_gpu(args, rank, world):
     return out
 
 
-# ---- CPU: the oracle (FP64 restatement of the reference) on a bounded sample -----------------------
-def cpu_sample(seconds, w0=10000.0, threads=None):
-    import oracle
-    from fastspec_b200 import workloads as W
-    import fastspec_b200 as F
-    oracle.build()
-    st, meta = load_atmosphere()
-    density = 1e8 / (1.0 / W0 - 1.0 / W1)          # lines per unit wavenumber-in-1/A
-    span = 0.5
-    while True:
-        margin = 4.0
-        a, b = w0 - margin, w0 + span + margin
-        n = int(density * (1.0 / a - 1.0 / b))
-        L = W.molecular_lines(n, a, b, 99, exact=False)
-        grid = dict(wmode=1, wstart=w0, wend=w0 + span, dstep=DSTEP)
-        wave = F.make_grid(1, w0, w0 + span, DSTEP) + w0
-        co = contopac_for(meta, wave)
-        S = oracle.State(grid, st, contopac=co, vmicro=meta["vmicro"], molbrd=meta["molbrd"])
-        ar = L.arrays()
-        OL = oracle.Lines(wl=ar["wl"], elo=ar["elo"], gf=ar["gf"], grad=ar["grad"], gqst=ar["gqst"],
-                          gvdw=ar["gvdw"], spc=ar["spc"], ismol=ar["ismol"], kind=2)
-        x, w, _ = oracle.mu_quadrature(1, NMU)
-        t = time.perf_counter()
-        r = oracle.lineop_calc(S, OL, list_type=2)
-        spl, spcc = oracle.radtran(S, x, r["lineopac"])
-        oracle.disk_integ(w, spl, spcc)
-        dt = time.perf_counter() - t
-        ev = r["stats"]["line_evals"] + r["stats"]["wide_evals"]
-        if dt >= seconds or span >= 64:
-            return dict(evals=ev, seconds=dt, span=span, nlines=n, nwl=S.nwl)
-        span *= max(2.0, min(8.0, seconds / max(dt, 1e-3)))
-
-
+# ---- CPU: the reference's own executable (or the oracle port) on a bounded sample -------------------
+# The sample keeps the configuration's whole grid (5000-25000 A at R = 3e5, 482,832 wavelengths) and
+# takes a uniform random subsample of the 1e8-line list (same distributions, its own seed per step).
+# Windows are a property of each line and the atmosphere, so the work per line, the share of lines
+# whose windows span more than 5000 km/s (wide lines, MarkWideLines, synth.f90:709-744) and the
+# per-wavelength accumulation match the full synthesis, scaled by the sample fraction.  The sample
+# fits one line block, the reference's fastest mode: the full list would run in the 100,000-line
+# minimum blocks NlinesMax falls back to (opacity.f90:712-771: the list alone exceeds LIMITRAM),
+# where far more lines are accumulated one by one as wide lines.  The rate is therefore an upper
+# bound on the reference's speed for the whole configuration.
 REF_BIN = os.path.join(HERE, "baseline", "_ref", "fastspec_Linux_x86_64")
+REF_LINES = 50_000            # lines per timed reference sample (1/2000 of the list)
+REF_WARM_LINES = 5_000        # lines per warm-up run
 
 
 def _stage_seconds(text, key):
@@ -577,96 +594,143 @@ def _stage_seconds(text, key):
     import re
     for line in text.splitlines():
         if key in line:
-            m = re.search(r"Time spent: (\d+):(\d+):([\d.]+)", line)
+            m = re.search(r"[Tt]ime spent: (\d+):(\d+):([\d.]+)", line)
             if m:
                 return int(m.group(1)) * 3600 + int(m.group(2)) * 60 + float(m.group(3))
     return None
 
 
-def ref_binary_sample(seconds, threads, w0=10000.0):
-    """The reference executable on the cool-dwarf workload: a span of the R = 3e5 grid at w0 with the
-    molecular lines of the 1e8-line list that fall inside it (the executable reads the lines of its
-    wavelength range), OMP_NUM_THREADS = threads.  The span grows until the line-opacity stage takes
-    `seconds`.  Its line-evals (windows inside the grid, wide lines included) are counted by the oracle
-    on the same list, whose windows equal the executable's."""
-    import tempfile
-    import oracle
-    from fastspec_b200 import workloads as W
-    import fastspec_b200 as F
-    oracle.build()
-    st, meta = load_atmosphere()
-    d = np.load(os.path.join(HERE, "fastspec_b200", "data", "atm_cooldwarf.npz"))
-    model = W.eddington_model(float(d["teff"]), float(d["logg"]), 72)
-    density = 1e8 / (1.0 / W0 - 1.0 / W1)
-    span = 2.0
-    while True:
-        n = int(density * (1.0 / w0 - 1.0 / (w0 + span)))
-        L = W.molecular_lines(n, w0, w0 + span, 99, exact=True)
-        with tempfile.TemporaryDirectory() as wd:
-            W.write_krz(os.path.join(wd, "model.krz"), model)
-            L.write_z(os.path.join(wd, "lines.z"), w0, w0 + span)
-            deck = ("wave=%.4f, %.4f, %.6f, 1\nsave=0, 0, 0, 0, 1\nvmic=%.3f\nmolbrd=%d\nlines=\n-1  lines.z\n\n"
-                    "model=model.krz\nmus=%d\n" % (w0, w0 + span, DSTEP, meta["vmicro"], meta["molbrd"], NMU))
-            with open(os.path.join(wd, "in.dat"), "w") as f:
-                f.write(deck)
-            t0 = time.perf_counter()
-            r = subprocess.run([REF_BIN, "in.dat"], cwd=wd, capture_output=True, text=True,
-                               env=dict(os.environ, OMP_NUM_THREADS=str(threads)))
-            wall = time.perf_counter() - t0
+class RefSampler:
+    """Samples of the cool-dwarf configuration for the CPU baselines.  Loads nothing of the CUDA
+    library: the grid, the windows and the line-eval counts come from the oracle (whose windows equal
+    the executable's), the line lists and the model from the workload generator (numpy)."""
+
+    def __init__(self):
+        import tempfile
+        import oracle
+        from fastspec_b200 import workloads as W
+        oracle.build()
+        self.oracle, self.W = oracle, W
+        self.st, self.meta = load_atmosphere()
+        self.grid = dict(wmode=1, wstart=W0, wend=W1, dstep=DSTEP)
+        self.S = None
+        self.wd = tempfile.mkdtemp(prefix="fsref_")
+        d = np.load(os.path.join(HERE, "fastspec_b200", "data", "atm_cooldwarf.npz"))
+        W.write_krz(os.path.join(self.wd, "model.krz"), W.eddington_model(float(d["teff"]), float(d["logg"]), 72))
+
+    def state(self):
+        if self.S is None:
+            S0 = self.oracle.State(self.grid, self.st)
+            co = contopac_for(self.meta, S0.wave + W0)
+            self.S = self.oracle.State(self.grid, self.st, contopac=co, vmicro=self.meta["vmicro"],
+                                       molbrd=self.meta["molbrd"])
+        return self.S
+
+    def lines(self, n, seed, exact):
+        return self.W.molecular_lines(int(n), W0, W1, seed, exact=exact)
+
+    def evals(self, L):
+        """Line-evals of a list on the whole grid: Ntau x the retained windows (oracle central pass)."""
+        S = self.state()
+        r = self.oracle.lineop_calc(S, self.oracle.Lines(**L.arrays(), kind=2), list_type=2, wrange=(1, 0))
+        keep = (r["flags"] & 1) == 0
+        return float(S.ntau) * float(np.sum(r["iright"][keep].astype(np.int64) - r["ileft"][keep] + 1))
+
+    def run_binary(self, L, threads, wend=W1):
+        """One run of the reference executable on list L over [W0, wend]; its stage times."""
+        L.write_z(os.path.join(self.wd, "lines.z"), W0, W1)
+        deck = ("wave=%.4f, %.4f, %.12f, 1\nsave=0, 0, 0, 0, 1\nvmic=%.3f\nmolbrd=%d\nlines=\n-1  lines.z\n\n"
+                "model=model.krz\nmus=%d\n" % (W0, wend, DSTEP, self.meta["vmicro"], self.meta["molbrd"], NMU))
+        with open(os.path.join(self.wd, "in.dat"), "w") as f:
+            f.write(deck)
+        t0 = time.perf_counter()
+        r = subprocess.run([REF_BIN, "in.dat"], cwd=self.wd, capture_output=True, text=True,
+                           env=dict(os.environ, OMP_NUM_THREADS=str(threads)))
+        wall = time.perf_counter() - t0
         if r.returncode != 0 or "Total time" not in r.stdout:
             raise RuntimeError("reference executable failed: " + (r.stdout + r.stderr)[-500:])
-        tl = _stage_seconds(r.stdout, "Total lines read")
-        if (tl is not None and tl >= seconds) or span >= 64:
-            break
-        span *= max(2.0, min(8.0, seconds / max(tl or 0.05, 0.05)))
-    grid = dict(wmode=1, wstart=w0, wend=w0 + span, dstep=DSTEP)
-    wave = F.make_grid(1, w0, w0 + span, DSTEP) + w0
-    S = oracle.State(grid, st, contopac=contopac_for(meta, wave), vmicro=meta["vmicro"], molbrd=meta["molbrd"])
-    ar = L.arrays()
-    rr = oracle.lineop_calc(S, oracle.Lines(**ar, kind=2), list_type=2)
-    ev = rr["stats"]["line_evals"] + rr["stats"]["wide_evals"]
-    return dict(evals=ev, seconds=tl, wall=wall, span=span, nlines=n, nwl=S.nwl, threads=threads,
-                stdout_tail=" | ".join(x.strip() for x in r.stdout.splitlines()[-6:]))
+        return dict(lines_s=_stage_seconds(r.stdout, "Total lines read"),
+                    rt_s=_stage_seconds(r.stdout, "radiative transfer"),
+                    total_s=_stage_seconds(r.stdout, "Total time spent"), wall_s=wall,
+                    stage_line=next((x.strip() for x in r.stdout.splitlines() if "Total lines read" in x), ""))
+
+    def parse_seconds(self, L, threads):
+        """The list-reading share of the stage time: the same list on a two-wavelength grid, where the
+        reader parses every record and keeps almost none (its WAVE= selection)."""
+        return self.run_binary(L, threads, wend=W0 * np.exp(1.5 * DSTEP / 2.99792458e5))["lines_s"]
+
+    def binary_sample(self, n, seed, threads):
+        L = self.lines(n, seed, exact=True)
+        run = self.run_binary(L, threads)
+        return dict(run, evals=self.evals(L), nlines=L.n, L=L)
+
+    def port_sample(self, n, seed):
+        """The oracle (FP64 C restatement, OpenMP) on the same kind of sample, timed here."""
+        L = self.lines(n, seed, exact=False)
+        S = self.state()
+        t = time.perf_counter()
+        r = self.oracle.lineop_calc(S, self.oracle.Lines(**L.arrays(), kind=2), list_type=2)
+        dt = time.perf_counter() - t
+        return dict(evals=r["stats"]["line_evals"] + r["stats"]["wide_evals"], lines_s=dt, nlines=L.n)
+
+
+def reference_rate(threads, steps, warmup, seed0=20261203 + 500):
+    """The reference's line-evals/s on `steps` samples (each its own subsample): per-step rates from the
+    executable's own line-opacity stage time less the list-reading share, with their spread."""
+    R = RefSampler()
+    cores = threads
+    if os.path.exists(REF_BIN):
+        for k in range(warmup):
+            R.run_binary(R.lines(REF_WARM_LINES, seed0 + 1000 + k, exact=True), threads)
+        rates, rates_incl, samp, ms, parse = [], [], None, 0.0, 0.0
+        for k in range(steps):
+            samp = R.binary_sample(REF_LINES, seed0 + k, threads)
+            if k == 0:
+                parse = R.parse_seconds(samp["L"], threads)
+            lines_s = max(samp["lines_s"] - parse, 0.05)
+            rates.append(samp["evals"] / lines_s)
+            rates_incl.append(samp["evals"] / samp["lines_s"])
+            ms += samp["lines_s"] * 1e3
+        kind = "reference"
+        sample = ("reference executable (OpenMP, %d threads) on the configuration's whole grid (%d wavelengths, "
+                  "R = 3e5) with %d-line uniform subsamples of the 1e8-line list (1/%d, one per step): line-"
+                  "opacity stage time by its own timer (0.1 s resolution, ~%.1f s per sample) less the list-"
+                  "reading share (%.2f s, the same list on a two-wavelength grid); line-evals counted by the "
+                  "oracle; single-block mode, an upper bound on the reference's speed for the full list"
+                  % (threads, R.state().nwl, REF_LINES, int(1e8 // REF_LINES), ms / 1e3 / steps, parse))
+        extra = {"rate_including_list_reading": float(np.mean(rates_incl)), "parse_seconds": parse,
+                 "stage_line": samp["stage_line"], "rt_seconds": samp["rt_s"], "total_seconds": samp["total_s"]}
+    else:
+        cores = os.cpu_count()
+        for k in range(warmup):
+            R.port_sample(REF_WARM_LINES // 5, seed0 + 1000 + k)
+        rates, samp, ms = [], None, 0.0
+        for k in range(steps):
+            samp = R.port_sample(REF_LINES // 10, seed0 + k)
+            rates.append(samp["evals"] / samp["lines_s"])
+            ms += samp["lines_s"] * 1e3
+        kind = "port"
+        sample = ("oracle FP64 C restatement (OpenMP) on the configuration's whole grid with %d-line uniform "
+                  "subsamples of the 1e8-line list (one per step)" % (REF_LINES // 10))
+        extra = {}
+    rates = np.asarray(rates)
+    extra.update(rate_min=float(rates.min()), rate_max=float(rates.max()),
+                 spread=float((rates.max() - rates.min()) / rates.mean()))
+    return dict(value=float(rates.mean()), ms=ms, kind=kind, cores=cores, sample=sample, extra=extra)
 
 
 def run_reference(args):
-    cores = os.cpu_count()
-    cfg = {"workload": "cool-dwarf molecular synthesis, 1e8 lines, 72 depths, R=3e5 (5000-25000 A), 7 mu"}
-    if os.path.exists(REF_BIN):
-        # the reference's own OpenMP executable, its line-opacity stage timed by itself
-        seconds = max(3.0, args.cpu_seconds / max(1, args.steps))
-        for _ in range(args.warmup):
-            ref_binary_sample(1.0, cores)
-        rates, ms, samp = [], 0.0, None
-        for _ in range(args.steps):
-            samp = ref_binary_sample(seconds, cores)
-            rates.append(samp["evals"] / samp["seconds"])
-            ms += samp["seconds"] * 1e3
-        value = float(np.mean(rates))
-        sample = ("reference executable (OpenMP, %d threads): line-opacity stage of %.2f A at 10000 A "
-                  "(%d lines, %d wavelengths), its own stage time (includes reading the .z list); "
-                  "line-evals counted by the oracle on the same list" % (cores, samp["span"], samp["nlines"], samp["nwl"]))
-        kind = "reference"
-        cfg["sample"] = sample
-        cfg["reference_output"] = samp["stdout_tail"]
-    else:
-        for _ in range(args.warmup):
-            cpu_sample(1.0)
-        rates, ms, samp = [], 0.0, None
-        for _ in range(args.steps):
-            samp = cpu_sample(args.cpu_seconds / max(1, args.steps))
-            rates.append(samp["evals"] / samp["seconds"])
-            ms += samp["seconds"] * 1e3
-        value = float(np.mean(rates))
-        sample = "oracle FP64 C restatement (OpenMP) on %.2f A at 10000 A (%d lines, %d pixels)" % (
-            samp["span"], samp["nlines"], samp["nwl"])
-        kind = "port"
-        cfg["sample"] = sample
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": cfg,
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    cfg = {"workload": WORKLOAD}
+    r = reference_rate(os.cpu_count(), args.steps, args.warmup)
+    cfg["sample"] = r["sample"]
+    line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
+                             "sample": r["sample"]},
+            "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_samples": r["extra"]}
     print(json.dumps(line))
 
 
@@ -692,18 +756,9 @@ def main():
     r = run_gpu(args, rank, world)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        if os.path.exists(REF_BIN):
-            s = ref_binary_sample(args.cpu_seconds, os.cpu_count())
-            cpu = {"value": s["evals"] / s["seconds"], "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                   "sample": "reference executable (OpenMP, %d threads), line-opacity stage of %.2f A at 10000 A "
-                             "(%d lines, %d wavelengths): %.1f s by its own timer" % (s["threads"], s["span"],
-                                                                                    s["nlines"], s["nwl"],
-                                                                                    s["seconds"])}
-        else:
-            s = cpu_sample(args.cpu_seconds)
-            cpu = {"value": s["evals"] / s["seconds"], "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                   "sample": "oracle FP64 C restatement (OpenMP) on %.2f A at 10000 A (%d lines, %d pixels), %.1f s"
-                             % (s["span"], s["nlines"], s["nwl"], s["seconds"])}
+        c = reference_rate(os.cpu_count(), 2, 0)
+        cpu = {"value": c["value"], "unit": UNIT, "cores": c["cores"], "kind": c["kind"], "sample": c["sample"],
+               "spread": c["extra"]["spread"]}
     if world > 1 or args.shard:
         import torch.distributed as dist
         dist.barrier()
@@ -734,7 +789,7 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
-        "config": {"workload": "cool-dwarf molecular synthesis, 1e8 lines, 72 depths, R=3e5 (5000-25000 A), 7 mu",
+        "config": {"workload": WORKLOAD, "limitram_gb": args.limitram,
                    "nlines": r["nlines"], "nwl": r["nwl"], "ntau": r["ntau"], "precision": args.precision,
                    "l2": "inputs (3.6 GB lines, 278 MB ContOpac) exceed the 126 MB L2; no flush",
                    "parallelism": ("wavelength shards over %d GPUs (windows all-gathered over NCCL)" % world)
@@ -773,6 +828,8 @@ def main():
         line["cpu_baseline"] = cpu
     if "plain" in r:
         line["plain_fp64"] = r["plain"]
+    if "limitram_24gb" in r:
+        line["limitram_24gb"] = r["limitram_24gb"]
     if "batched" in r:
         line["batched"] = r["batched"]
     if "fit" in r:

@@ -83,6 +83,8 @@ EXPORTS = [
     "fsg_central_dev", "fsg_accumulate_dev", "fsg_batch_create", "fsg_batch_tune", "fsg_batch_set_tuning",
     "fsg_batch_run", "fsg_batch_flux", "fsg_batch_stream", "fsg_batch_last_error", "fsg_batch_destroy",
     "fsg_set_vmicro", "fsg_set_fractionpf", "fsg_adjoint_dev", "fsg_disk_integ_conv", "fsg_disk_integ_conv_dev",
+    "fsg_xline_setup", "fsg_xline_depth", "fsg_lineopacity1", "fsg_lineopacity2", "fsg_mag_lineopacity1",
+    "fsg_analytic_window", "fsg_stokes_prf_pp",
 ]
 
 _lib = None
@@ -157,6 +159,14 @@ def lib():
     L.fsg_batch_last_error.restype = C.c_char_p
     L.fsg_batch_destroy.argtypes = [C.c_void_p]
     L.fsg_batch_destroy.restype = None
+    vp = C.c_void_p
+    L.fsg_xline_setup.argtypes = [vp, C.POINTER(CLines), vp]
+    L.fsg_xline_depth.argtypes = [vp, C.c_int64, vp, vp, vp, vp]
+    L.fsg_lineopacity1.argtypes = [vp, C.POINTER(CLineBlock), C.c_int64, vp, vp, vp, vp, C.c_int64, vp]
+    L.fsg_mag_lineopacity1.argtypes = [vp, C.POINTER(CLineBlock), C.c_int64, vp, vp, vp, vp, C.c_int64, vp]
+    L.fsg_lineopacity2.argtypes = [vp, C.POINTER(CLineBlock), C.c_int64, vp, vp, vp, vp, vp, vp, vp]
+    L.fsg_analytic_window.argtypes = [vp, C.c_int64, vp, vp, vp, vp, vp, vp]
+    L.fsg_stokes_prf_pp.argtypes = [vp, C.c_int64, vp, vp, vp, vp, vp, vp, vp, vp]
     _lib = L
     return L
 
@@ -341,6 +351,51 @@ class LineList:
     def from_arrays(cls, a, kind=2, zeeman=None):
         return cls(a["wl"], a["elo"], a["gf"], a["grad"], a["gqst"], a["gvdw"], a["spc"], kind=kind,
                    ismol=a.get("ismol"), ihe=a.get("ihe"), zeeman=zeeman)
+
+
+# XlineCoef (opacity.f90:43-58) as fsg_xcoef lays it out
+XCOEF_DTYPE = np.dtype([(n, np.float64) for n in ("WaveL", "Hnux", "Elo", "Gf", "Grad", "Xmass", "Cqst", "Qdiv",
+                                                  "Cvdw", "AboPre", "AboVbc", "AboExp")] +
+                       [(n, np.int32) for n in ("IxPF", "MdQst", "MdVdw", "IxHe")])
+
+
+class CLineBlock(C.Structure):
+    _fields_ = [("nlines", C.c_int64), ("nblock", C.c_int64), ("wlcent", _dp), ("flags", _ip), ("ileft", _ip),
+                ("iright", _ip), ("lincop", _dp), ("linvvgt", _dp), ("linavgt", _dp), ("npi", _ip), ("nsi", _ip),
+                ("pi_off", C.POINTER(C.c_int64)), ("si_off", C.POINTER(C.c_int64)), ("splpi", _fp), ("strpi", _fp),
+                ("splsi", _fp), ("strsi", _fp)]
+
+
+class LineBlock:
+    """The reference's line arrays for the kernel-level routines (fsg_lineblock): per line wlcent (centre
+    less Wfirst), flags, ileft, iright; per block line lincop / linvvgt / linavgt [nblock][ntau]; optional
+    Zeeman components (npi, nsi, spl_pi, str_pi, spl_si, str_si) with shifts in [A]."""
+
+    def __init__(self, wlcent, flags, ileft, iright, lincop=None, linvvgt=None, linavgt=None, zeeman=None):
+        k = self._keep = {}
+        b = CLineBlock()
+        k["wlcent"] = _f64(wlcent); b.wlcent = _p(k["wlcent"], C.c_double)
+        for name, arr in (("flags", flags), ("ileft", ileft), ("iright", iright)):
+            k[name] = _i32(arr); setattr(b, name, _p(k[name], C.c_int32))
+        b.nlines = len(k["wlcent"])
+        if lincop is not None:
+            for name, arr in (("lincop", lincop), ("linvvgt", linvvgt), ("linavgt", linavgt)):
+                k[name] = _f64(arr); setattr(b, name, _p(k[name], C.c_double))
+            b.nblock = k["lincop"].shape[0]
+        if zeeman is not None:
+            npi, nsi, spl_pi, str_pi, spl_si, str_si = zeeman
+            k["npi"] = _i32(npi); k["nsi"] = _i32(nsi)
+            k["pi_off"] = np.ascontiguousarray(np.concatenate([[0], np.cumsum(k["npi"])[:-1]]), np.int64)
+            k["si_off"] = np.ascontiguousarray(np.concatenate([[0], np.cumsum(k["nsi"])[:-1]]), np.int64)
+            for name, arr in (("splpi", spl_pi), ("strpi", str_pi), ("splsi", spl_si), ("strsi", str_si)):
+                k[name] = _f32(arr if len(arr) else np.zeros(1, np.float32)); setattr(b, name, _p(k[name], C.c_float))
+            b.npi = _p(k["npi"], C.c_int32); b.nsi = _p(k["nsi"], C.c_int32)
+            b.pi_off = _p(k["pi_off"], C.c_int64); b.si_off = _p(k["si_off"], C.c_int64)
+        self.c = b
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
 
 
 class Context:
@@ -578,6 +633,63 @@ class Context:
                                            _p(spc, C.c_double), _p(sfl, C.c_double), _p(sfc, C.c_double)),
                  "fsg_mag_radtran")
         return spz, spc, sfl, sfc
+
+    # ---- kernel-level routines (the reference's elemental functions, batched on the GPU) -----------
+    def xline_setup(self, lines):
+        """XlineSetup of every line of a LineList: structured array of XCOEF_DTYPE."""
+        xc = np.zeros(max(lines.n, 1), XCOEF_DTYPE)
+        self._ck(self._lib.fsg_xline_setup(self.h, C.byref(lines.c), _ptr(xc)), "fsg_xline_setup")
+        return xc[:lines.n]
+
+    def xline_depth(self, xc):
+        """XlineDepth at every depth: (lincop, linvvgt, linavgt) [n][ntau]."""
+        xc = np.ascontiguousarray(xc, XCOEF_DTYPE)
+        n = len(xc)
+        out = [np.zeros((max(n, 1), self.ntau)) for _ in range(3)]
+        self._ck(self._lib.fsg_xline_depth(self.h, n, _ptr(xc), *[_ptr(o) for o in out]), "fsg_xline_depth")
+        return tuple(o[:n] for o in out)
+
+    def lineopacity1(self, block, wl, l1, l2, iwl, loff=0):
+        """LineOpacity1 at points (wl, l1, l2, iwl arrays; 1-based): [npts][ntau]."""
+        wl = _f64(wl); l1 = _i32(l1); l2 = _i32(l2); iwl = _i32(iwl)
+        out = np.zeros((max(len(wl), 1), self.ntau))
+        self._ck(self._lib.fsg_lineopacity1(self.h, C.byref(block.c), len(wl), _ptr(wl), _ptr(l1), _ptr(l2), _ptr(iwl),
+                                            int(loff), _ptr(out)), "fsg_lineopacity1")
+        return out[:len(wl)]
+
+    def mag_lineopacity1(self, block, wl, l1, l2, iwl, loff=0):
+        """MagLineOpacity1 at points: [npts][ntau][6]."""
+        wl = _f64(wl); l1 = _i32(l1); l2 = _i32(l2); iwl = _i32(iwl)
+        out = np.zeros((max(len(wl), 1), self.ntau, 6))
+        self._ck(self._lib.fsg_mag_lineopacity1(self.h, C.byref(block.c), len(wl), _ptr(wl), _ptr(l1), _ptr(l2),
+                                                _ptr(iwl), int(loff), _ptr(out)), "fsg_mag_lineopacity1")
+        return out[:len(wl)]
+
+    def lineopacity2(self, block, wl, iline, iwl, lincop, linvvgt, linavgt):
+        """LineOpacity2 at points, each with its own parameter rows [npts][ntau]: [npts][ntau]."""
+        wl = _f64(wl); iline = _i32(iline); iwl = _i32(iwl)
+        c, v, a = _f64(lincop), _f64(linvvgt), _f64(linavgt)
+        out = np.zeros((max(len(wl), 1), self.ntau))
+        self._ck(self._lib.fsg_lineopacity2(self.h, C.byref(block.c), len(wl), _ptr(wl), _ptr(iline), _ptr(iwl),
+                                            _ptr(c), _ptr(v), _ptr(a), _ptr(out)), "fsg_lineopacity2")
+        return out[:len(wl)]
+
+    def analytic_window(self, flags, lincop, linvvgt, linavgt, contopac):
+        """AnalyticWindow of n lines (rows [n][ntau]): half-widths [n] in A."""
+        f = _i32(flags); c, v, a, co = _f64(lincop), _f64(linvvgt), _f64(linavgt), _f64(contopac)
+        out = np.zeros(max(len(f), 1))
+        self._ck(self._lib.fsg_analytic_window(self.h, len(f), _ptr(f), _ptr(c), _ptr(v), _ptr(a), _ptr(co),
+                                               _ptr(out)), "fsg_analytic_window")
+        return out[:len(f)]
+
+    def stokes_prf_pp(self, iwl, src, sphi2, cphi2, cphi, s2psi, c2psi):
+        """StokesPrfPP at grid wavelengths iwl (1-based) with sources src [npts][ntau]: [npts][4][nmu]."""
+        iwl = _i32(iwl); src = _f64(src)
+        g = [_f64(x) for x in (sphi2, cphi2, cphi, s2psi, c2psi)]
+        out = np.zeros((max(len(iwl), 1), 4, self.nmu))
+        self._ck(self._lib.fsg_stokes_prf_pp(self.h, len(iwl), _ptr(iwl), _ptr(src), *[_ptr(x) for x in g], _ptr(out)),
+                 "fsg_stokes_prf_pp")
+        return out[:len(iwl)]
 
     def hvoigt(self, a, v):
         a = _f64(a); v = _f64(v); h = np.zeros_like(a)

@@ -10,6 +10,23 @@
 #include <vector>
 
 // ---- kernels defined in fsg_kernels64.cu / fsg_fast.cu / fsg_mag.cu ------------------------------
+void fsg_launch_xline_setup(cudaStream_t, const AtmView &, const LineView &, XCoef *);
+void fsg_launch_xline_depth(cudaStream_t, const AtmView &, int64_t, const XCoef *, double *, double *, double *);
+void fsg_launch_lineopacity1_pts(cudaStream_t, const AtmView &, const BlockView &, int64_t, const double *,
+                                 const int32_t *, const int32_t *, const int32_t *, int64_t, const VoigtTables &,
+                                 double *);
+void fsg_launch_lineopacity2_pts(cudaStream_t, const AtmView &, const BlockView &, int64_t, const double *,
+                                 const int32_t *, const int32_t *, const double *, const double *, const double *,
+                                 const VoigtTables &, double *);
+void fsg_launch_analytic_window(cudaStream_t, const AtmView &, int64_t, const int32_t *, const double *,
+                                const double *, const double *, const double *, double *);
+void fsg_launch_mag_lineopacity1_pts(cudaStream_t, const AtmView &, const BlockView &, const ZView &, int64_t,
+                                     const double *, const int32_t *, const int32_t *, const int32_t *, int64_t,
+                                     const VoigtTables &, double *);
+size_t fsg_stokes_pts_work(int64_t, int, int);
+void fsg_launch_stokes_prf_pts(cudaStream_t, const AtmView &, const double *, const double *, const double *, int,
+                               const double *, const double *, int64_t, const int32_t *, const double *, double *,
+                               double *);
 void fsg_launch_xline_init(cudaStream_t, int, const double *, const double *, const double *, const float *,
                            const float *, const float *, double, double *);
 void fsg_launch_center(cudaStream_t, const AtmView &, const LineView &, const VoigtTables &, int32_t *,
@@ -1549,6 +1566,245 @@ int fsg_mag_radtran(fsg_ctx *ctx, int bframe, const double *bfield, int nbfield,
 }
 
 // ---- elemental entry points --------------------------------------------------------------------------
+// ---- kernel-level entry points (XlineSetup / XlineDepth, LineOpacity1/2, MagLineOpacity1,
+// AnalyticWindow, StokesPrfPP): host arrays staged in per-call device buffers ---------------------
+}  // extern "C"
+namespace {
+struct Stage {                                      // device copies freed when the call returns
+    std::vector<DBuf *> bufs;
+    ~Stage() { for (DBuf *b : bufs) { b->release(); delete b; } }
+    template <class T> T *put(const T *h, size_t n, cudaStream_t s, int *rc) {
+        DBuf *b = new DBuf();
+        bufs.push_back(b);
+        if (b->ensure(sizeof(T) * std::max<size_t>(n, 1)) != FSG_OK) { *rc = FSG_E_NOMEM; return nullptr; }
+        if (h && n && cudaMemcpyAsync(b->p, h, sizeof(T) * n, cudaMemcpyHostToDevice, s) != cudaSuccess)
+            *rc = FSG_E_CUDA;
+        return (T *)b->p;
+    }
+    template <class T> T *out(size_t n, int *rc) { return put<T>(nullptr, n, nullptr, rc); }
+};
+}  // namespace
+extern "C" {
+
+static int block_stage(fsg_ctx *ctx, Stage &S, const fsg_lineblock *b, int mag, BlockView *B, ZView *Z) {
+    int rc = FSG_OK;
+    cudaStream_t s = ctx->stream;
+    const size_t nl = (size_t)b->nlines, nb = (size_t)b->nblock * ctx->ntau;
+    B->wlcent = S.put(b->wlcent, nl, s, &rc);
+    B->flags = S.put(b->flags, nl, s, &rc); B->ileft = S.put(b->ileft, nl, s, &rc);
+    B->iright = S.put(b->iright, nl, s, &rc);
+    B->cop = S.put(b->lincop, nb, s, &rc); B->vv = S.put(b->linvvgt, nb, s, &rc); B->av = S.put(b->linavgt, nb, s, &rc);
+    if (mag) {
+        int64_t np = 0, ns = 0;
+        for (size_t i = 0; i < nl; i++) {
+            np = std::max<int64_t>(np, b->pi_off[i] + b->npi[i]);
+            ns = std::max<int64_t>(ns, b->si_off[i] + b->nsi[i]);
+        }
+        memset(Z, 0, sizeof *Z);
+        Z->npi = S.put(b->npi, nl, s, &rc); Z->nsi = S.put(b->nsi, nl, s, &rc);
+        Z->pi_off = S.put(b->pi_off, nl, s, &rc); Z->si_off = S.put(b->si_off, nl, s, &rc);
+        Z->splpi = S.put(b->splpi, (size_t)np, s, &rc); Z->strpi = S.put(b->strpi, (size_t)np, s, &rc);
+        Z->splsi = S.put(b->splsi, (size_t)ns, s, &rc); Z->strsi = S.put(b->strsi, (size_t)ns, s, &rc);
+    }
+    return rc;
+}
+
+static int check_block(fsg_ctx *ctx, const fsg_lineblock *b, int mag, const char *who) {
+    if (!b || b->nlines < 0 || b->nblock < 0 || (b->nlines > 0 && (!b->wlcent || !b->flags || !b->ileft || !b->iright)) ||
+        (b->nblock > 0 && (!b->lincop || !b->linvvgt || !b->linavgt)))
+        return fail(ctx, FSG_E_ARG, who);
+    if (mag && b->nlines > 0 && (!b->npi || !b->nsi || !b->pi_off || !b->si_off || !b->splpi || !b->strpi ||
+                                 !b->splsi || !b->strsi))
+        return fail(ctx, FSG_E_ARG, who);
+    return FSG_OK;
+}
+
+// line ranges of the points inside the list and the block (LineOpacity1's L1..L2 - Loff)
+static int check_points(fsg_ctx *ctx, const fsg_lineblock *b, int64_t npts, const int32_t *l1, const int32_t *l2,
+                        const int32_t *iwl, int64_t loff, const char *who) {
+    for (int64_t k = 0; k < npts; k++) {
+        if (iwl[k] < 1 || iwl[k] > ctx->nwl) return fail(ctx, FSG_E_ARG, who);
+        if (l1[k] > l2[k]) continue;
+        if (l1[k] < 1 || l2[k] > b->nlines || l1[k] - loff < 1 || l2[k] - loff > b->nblock) return fail(ctx, FSG_E_ARG, who);
+    }
+    return FSG_OK;
+}
+
+int fsg_xline_setup(fsg_ctx *ctx, const fsg_lines *lines, fsg_xcoef *xc) {
+    int rc = check_lines(ctx, lines); if (rc) return rc;
+    if (lines->n > 0 && !xc) return fail(ctx, FSG_E_ARG, "fsg_xline_setup: output missing");
+    if (lines->n == 0) return FSG_OK;
+    cudaSetDevice(ctx->device);
+    fsg_lines D{};
+    rc = upload_lines(ctx, lines, &D); if (rc) return rc;
+    Stage S;
+    XCoef *dx = S.out<XCoef>((size_t)lines->n, &rc);
+    if (rc) return fail(ctx, rc, "fsg_xline_setup: device buffers");
+    fsg_launch_xline_setup(ctx->stream, fsg_view(ctx), make_view(&D), dx);
+    ctx->launches += 1;
+    CK(cudaGetLastError(), "k_xline_setup");
+    CK(cudaMemcpyAsync(xc, dx, sizeof(XCoef) * (size_t)lines->n, cudaMemcpyDeviceToHost, ctx->stream), "xline setup");
+    CK(cudaStreamSynchronize(ctx->stream), "xline setup");
+    return FSG_OK;
+}
+
+int fsg_xline_depth(fsg_ctx *ctx, int64_t n, const fsg_xcoef *xc, double *lincop, double *linvvgt, double *linavgt) {
+    if (!ctx || n < 0 || (n > 0 && (!xc || !lincop || !linvvgt || !linavgt)))
+        return fail(ctx, FSG_E_ARG, "fsg_xline_depth: bad arguments");
+    if (!ctx->have_atm) return fail(ctx, FSG_E_STATE, "fsg_xline_depth: set the atmosphere first");
+    if (n == 0) return FSG_OK;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    Stage S;
+    int rc = FSG_OK;
+    const size_t m = (size_t)n * ctx->ntau;
+    const XCoef *dx = S.put((const XCoef *)xc, (size_t)n, s, &rc);
+    double *c = S.out<double>(m, &rc), *v = S.out<double>(m, &rc), *a = S.out<double>(m, &rc);
+    if (rc) return fail(ctx, rc, "fsg_xline_depth: device buffers");
+    fsg_launch_xline_depth(s, fsg_view(ctx), n, dx, c, v, a);
+    ctx->launches += 1;
+    CK(cudaGetLastError(), "k_xline_depth");
+    CK(cudaMemcpyAsync(lincop, c, sizeof(double) * m, cudaMemcpyDeviceToHost, s), "xline depth");
+    CK(cudaMemcpyAsync(linvvgt, v, sizeof(double) * m, cudaMemcpyDeviceToHost, s), "xline depth");
+    CK(cudaMemcpyAsync(linavgt, a, sizeof(double) * m, cudaMemcpyDeviceToHost, s), "xline depth");
+    CK(cudaStreamSynchronize(s), "xline depth");
+    return FSG_OK;
+}
+
+static int lineop1_common(fsg_ctx *ctx, const fsg_lineblock *blk, int64_t npts, const double *wl, const int32_t *l1,
+                          const int32_t *l2, const int32_t *iwl, int64_t loff, double *out, int mag) {
+    const char *who = mag ? "fsg_mag_lineopacity1: bad arguments" : "fsg_lineopacity1: bad arguments";
+    if (!ctx) return FSG_E_ARG;
+    if (npts < 0 || (npts > 0 && (!wl || !l1 || !l2 || !iwl || !out))) return fail(ctx, FSG_E_ARG, who);
+    if (!ctx->have_grid || !ctx->have_atm) return fail(ctx, FSG_E_STATE, "set grid and atmosphere first");
+    int rc = check_block(ctx, blk, mag, who); if (rc) return rc;
+    rc = check_points(ctx, blk, npts, l1, l2, iwl, loff, who); if (rc) return rc;
+    if (npts == 0) return FSG_OK;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    Stage S;
+    BlockView B; ZView Z;
+    rc = block_stage(ctx, S, blk, mag, &B, &Z);
+    const double *dwl = S.put(wl, (size_t)npts, s, &rc);
+    const int32_t *d1 = S.put(l1, (size_t)npts, s, &rc), *d2 = S.put(l2, (size_t)npts, s, &rc);
+    const int32_t *di = S.put(iwl, (size_t)npts, s, &rc);
+    const size_t m = (size_t)npts * ctx->ntau * (mag ? 6 : 1);
+    double *dout = S.out<double>(m, &rc);
+    if (rc) return fail(ctx, rc, "lineopacity1: device buffers");
+    if (mag) fsg_launch_mag_lineopacity1_pts(s, fsg_view(ctx), B, Z, npts, dwl, d1, d2, di, loff, ctx->tab, dout);
+    else fsg_launch_lineopacity1_pts(s, fsg_view(ctx), B, npts, dwl, d1, d2, di, loff, ctx->tab, dout);
+    ctx->launches += 1;
+    CK(cudaGetLastError(), "lineopacity1");
+    CK(cudaMemcpyAsync(out, dout, sizeof(double) * m, cudaMemcpyDeviceToHost, s), "lineopacity1");
+    CK(cudaStreamSynchronize(s), "lineopacity1");
+    return FSG_OK;
+}
+
+int fsg_lineopacity1(fsg_ctx *ctx, const fsg_lineblock *blk, int64_t npts, const double *wl, const int32_t *l1,
+                     const int32_t *l2, const int32_t *iwl, int64_t loff, double *linop) {
+    return lineop1_common(ctx, blk, npts, wl, l1, l2, iwl, loff, linop, 0);
+}
+
+int fsg_mag_lineopacity1(fsg_ctx *ctx, const fsg_lineblock *blk, int64_t npts, const double *wl, const int32_t *l1,
+                         const int32_t *l2, const int32_t *iwl, int64_t loff, double *maglinop) {
+    return lineop1_common(ctx, blk, npts, wl, l1, l2, iwl, loff, maglinop, 1);
+}
+
+int fsg_lineopacity2(fsg_ctx *ctx, const fsg_lineblock *blk, int64_t npts, const double *wl, const int32_t *iline,
+                     const int32_t *iwl, const double *lincop, const double *linvvgt, const double *linavgt,
+                     double *linop) {
+    if (!ctx) return FSG_E_ARG;
+    const char *who = "fsg_lineopacity2: bad arguments";
+    if (npts < 0 || (npts > 0 && (!wl || !iline || !iwl || !lincop || !linvvgt || !linavgt || !linop)))
+        return fail(ctx, FSG_E_ARG, who);
+    if (!ctx->have_grid || !ctx->have_atm) return fail(ctx, FSG_E_STATE, "set grid and atmosphere first");
+    int rc = check_block(ctx, blk, 0, who); if (rc) return rc;
+    for (int64_t k = 0; k < npts; k++)
+        if (iline[k] < 1 || iline[k] > blk->nlines || iwl[k] < 1 || iwl[k] > ctx->nwl) return fail(ctx, FSG_E_ARG, who);
+    if (npts == 0) return FSG_OK;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    Stage S;
+    fsg_lineblock lb = *blk;
+    lb.nblock = 0;                                  // the points carry their own parameter rows
+    BlockView B; ZView Z;
+    rc = block_stage(ctx, S, &lb, 0, &B, &Z);
+    const size_t m = (size_t)npts * ctx->ntau;
+    const double *dwl = S.put(wl, (size_t)npts, s, &rc);
+    const int32_t *dl = S.put(iline, (size_t)npts, s, &rc), *di = S.put(iwl, (size_t)npts, s, &rc);
+    const double *c = S.put(lincop, m, s, &rc), *v = S.put(linvvgt, m, s, &rc), *a = S.put(linavgt, m, s, &rc);
+    double *dout = S.out<double>(m, &rc);
+    if (rc) return fail(ctx, rc, "fsg_lineopacity2: device buffers");
+    fsg_launch_lineopacity2_pts(s, fsg_view(ctx), B, npts, dwl, dl, di, c, v, a, ctx->tab, dout);
+    ctx->launches += 1;
+    CK(cudaGetLastError(), "k_lineopacity2_pts");
+    CK(cudaMemcpyAsync(linop, dout, sizeof(double) * m, cudaMemcpyDeviceToHost, s), "lineopacity2");
+    CK(cudaStreamSynchronize(s), "lineopacity2");
+    return FSG_OK;
+}
+
+int fsg_analytic_window(fsg_ctx *ctx, int64_t n, const int32_t *flags, const double *lincop, const double *linvvgt,
+                        const double *linavgt, const double *contopac, double *dw) {
+    if (!ctx) return FSG_E_ARG;
+    if (n < 0 || (n > 0 && (!flags || !lincop || !linvvgt || !linavgt || !contopac || !dw)))
+        return fail(ctx, FSG_E_ARG, "fsg_analytic_window: bad arguments");
+    if (!ctx->have_atm) return fail(ctx, FSG_E_STATE, "fsg_analytic_window: set the atmosphere first");
+    if (n == 0) return FSG_OK;
+    cudaSetDevice(ctx->device);
+    cudaStream_t s = ctx->stream;
+    Stage S;
+    int rc = FSG_OK;
+    const size_t m = (size_t)n * ctx->ntau;
+    const int32_t *df = S.put(flags, (size_t)n, s, &rc);
+    const double *c = S.put(lincop, m, s, &rc), *v = S.put(linvvgt, m, s, &rc), *a = S.put(linavgt, m, s, &rc);
+    const double *co = S.put(contopac, m, s, &rc);
+    double *dout = S.out<double>((size_t)n, &rc);
+    if (rc) return fail(ctx, rc, "fsg_analytic_window: device buffers");
+    fsg_launch_analytic_window(s, fsg_view(ctx), n, df, c, v, a, co, dout);
+    ctx->launches += 1;
+    CK(cudaGetLastError(), "k_analytic_window");
+    CK(cudaMemcpyAsync(dw, dout, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, s), "analytic window");
+    CK(cudaStreamSynchronize(s), "analytic window");
+    return FSG_OK;
+}
+
+int fsg_stokes_prf_pp(fsg_ctx *ctx, int64_t npts, const int32_t *iwl, const double *src, const double *sphi2,
+                      const double *cphi2, const double *cphi, const double *s2psi, const double *c2psi, double *stokes) {
+    if (!ctx) return FSG_E_ARG;
+    if (npts < 0 || (npts > 0 && (!iwl || !src || !sphi2 || !cphi2 || !cphi || !s2psi || !c2psi || !stokes)))
+        return fail(ctx, FSG_E_ARG, "fsg_stokes_prf_pp: bad arguments");
+    if (!ctx->have_grid || !ctx->have_atm || !ctx->have_cont || ctx->nmu < 1)
+        return fail(ctx, FSG_E_STATE, "fsg_stokes_prf_pp: set grid, atmosphere, continuum and mu first");
+    if (ctx->d_maglineopac.cap < sizeof(double) * 6 * (size_t)ctx->nwl * ctx->ntau)
+        return fail(ctx, FSG_E_STATE, "fsg_stokes_prf_pp: run fsg_mag_lineop_calc first");
+    for (int64_t k = 0; k < npts; k++)
+        if (iwl[k] < 1 || iwl[k] > ctx->nwl) return fail(ctx, FSG_E_ARG, "fsg_stokes_prf_pp: wavelength index");
+    if (npts == 0) return FSG_OK;
+    cudaSetDevice(ctx->device);
+    int rc = ensure_lineopac(ctx); if (rc) return rc;
+    cudaStream_t s = ctx->stream;
+    Stage S;
+    const int nmu = ctx->nmu;
+    std::vector<double> geo(5 * (size_t)nmu);
+    for (int im = 0; im < nmu; im++) {
+        geo[0 * nmu + im] = sphi2[im]; geo[1 * nmu + im] = cphi2[im]; geo[2 * nmu + im] = cphi[im];
+        geo[3 * nmu + im] = s2psi[im]; geo[4 * nmu + im] = c2psi[im];
+    }
+    const double *dg = S.put(geo.data(), geo.size(), s, &rc);
+    const int32_t *di = S.put(iwl, (size_t)npts, s, &rc);
+    const double *dsrc = S.put(src, (size_t)npts * ctx->ntau, s, &rc);
+    double *work = S.out<double>(fsg_stokes_pts_work(npts, nmu, ctx->ntau) / sizeof(double), &rc);
+    double *dout = S.out<double>((size_t)npts * 4 * nmu, &rc);
+    if (rc) return fail(ctx, rc, "fsg_stokes_prf_pp: device buffers");
+    fsg_launch_stokes_prf_pts(s, fsg_view(ctx), ctx->d_lineopac.as<double>(), ctx->d_maglineopac.as<double>(),
+                              ctx->d_rhox.as<double>(), nmu, ctx->d_xmu.as<double>(), dg, npts, di, dsrc, work, dout);
+    ctx->launches += 1;
+    CK(cudaGetLastError(), "k_stokes_prf_pts");
+    CK(cudaMemcpyAsync(stokes, dout, sizeof(double) * (size_t)npts * 4 * nmu, cudaMemcpyDeviceToHost, s), "stokes");
+    CK(cudaStreamSynchronize(s), "stokes");
+    return FSG_OK;
+}
+
 int fsg_hvoigt(fsg_ctx *ctx, int64_t n, const double *a, const double *v, double *h) {
     if (!ctx || n < 0 || (n > 0 && (!a || !v || !h))) return fail(ctx, FSG_E_ARG, "fsg_hvoigt: bad arguments");
     if (n == 0) return FSG_OK;

@@ -100,6 +100,15 @@ struct ZView {
     const float *rawpi, *rawsi;       // shifts as read (Lande-type units)
 };
 
+// The reference's per-line and block arrays as the elemental routines read them (device pointers):
+// Wlcent, LinFlag, Ileft, Iright per line; LinCop, LinVvgt, LinAvgt [nblock][ntau] per block line.
+struct BlockView {
+    const double *wlcent;
+    const int32_t *flags, *ileft, *iright;
+    const double *cop, *vv, *av;
+};
+static_assert(sizeof(XCoef) == sizeof(fsg_xcoef), "fsg_xcoef mirrors XCoef");
+
 // Rays of a spherical model (SphereInit, solver.f90:45-120), device arrays [nmu][stride], stride =
 // 2 ntau.  Ray im has n[im] points (ntau, or 2 n for a grazing ray that turns below layer n); point k
 // samples layer map[im][k] (0-based) at column mass m[im][k] along the ray.  nmu = 0: plane-parallel.

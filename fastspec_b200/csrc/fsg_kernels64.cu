@@ -855,3 +855,133 @@ void fsg_launch_conv(cudaStream_t s, int nwl, const double *in, int st, const do
                      const double *acc, double w) {
     if (nwl > 0) k_conv<<<(nwl + 255) / 256, 256, 0, s>>>(nwl, in, st, kern, n, out, acc, w);
 }
+
+
+// ================================================================================================
+// The reference's elemental line-opacity routines on their own, batched (kernel-level entry points):
+// XlineSetup / XlineDepth, LineOpacity1 and LineOpacity2 at given points, AnalyticWindow.  The same
+// device functions as the drivers, in the reference's operand order.
+// ================================================================================================
+// XlineSetup of every line with the drivers' input flags (synth.f90:837-845)
+__global__ void k_xline_setup(AtmView A, LineView L, XCoef *xc) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L.n) return;
+    XCoef XC;
+    xline_setup(A, L, i, L.wl[i] - A.wfirst, line_input_flags(L, i, 0), &XC);
+    xc[i] = XC;
+}
+
+// XlineDepth of n lines at every depth: out [n][ntau]
+__global__ void k_xline_depth(AtmView A, int64_t n, const XCoef *__restrict__ xc, double *cop, double *vv,
+                              double *av) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n * A.ntau) return;
+    const int64_t i = g / A.ntau;
+    const int t = (int)(g - i * A.ntau);
+    xline_depth(A, t, xc[i], &cop[g], &vv[g], &av[g]);
+}
+
+// LineOpacity1 (opacity.f90:297-346) at npts points, one warp per point, lanes over depths
+__global__ void k_lineopacity1_pts(AtmView A, BlockView B, int64_t npts, const double *__restrict__ wl,
+                                   const int32_t *__restrict__ l1, const int32_t *__restrict__ l2,
+                                   const int32_t *__restrict__ iwl, int64_t loff, const float *__restrict__ vtab,
+                                   const double *__restrict__ anode, const double *__restrict__ aida, double *out) {
+    const int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (k >= npts) return;
+    const int nt = A.ntau;
+    for (int t = lane; t < nt; t += 32) {
+        double acc = 0.0;
+        for (int64_t il = l1[k]; il <= l2[k]; il++) {
+            const int f = B.flags[il - 1];
+            if ((f & FSG_F_WEAK) || (f & FSG_F_WIDE) || iwl[k] < B.ileft[il - 1] || iwl[k] > B.iright[il - 1]) continue;
+            const int ihe = (f >> 8) & 255;
+            const double dWl0 = wl[k] - B.wlcent[il - 1];
+            double dWl = dWl0;
+            if (ihe > 0) dWl = dWl0 - A.heshf[(ihe - 1) * nt + t];
+            const size_t o = (size_t)(il - loff - 1) * nt + t;
+            const double V = dWl * B.vv[o];
+            const double Vgt = hvoigt64(vtab, anode, aida, B.av[o], V) * B.cop[o];
+            acc = acc + Vgt;
+        }
+        if (A.motype == 1) acc = acc / A.contstd[t];
+        out[(size_t)k * nt + t] = acc;
+    }
+}
+
+// LineOpacity2 (opacity.f90:350-386): point k is line iline[k] at wl[k], grid index iwl[k], with its
+// own parameter rows; one thread per (point, depth)
+__global__ void k_lineopacity2_pts(AtmView A, BlockView B, int64_t npts, const double *__restrict__ wl,
+                                   const int32_t *__restrict__ iline, const int32_t *__restrict__ iwl,
+                                   const double *__restrict__ cop, const double *__restrict__ vv,
+                                   const double *__restrict__ av, const float *__restrict__ vtab,
+                                   const double *__restrict__ anode, const double *__restrict__ aida, double *out) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int nt = A.ntau;
+    if (g >= npts * nt) return;
+    const int64_t k = g / nt;
+    const int t = (int)(g - k * nt);
+    const int64_t il = iline[k] - 1;
+    const int f = B.flags[il];
+    double v = 0.0;
+    if (!(f & FSG_F_WEAK) && iwl[k] >= B.ileft[il] && iwl[k] <= B.iright[il]) {
+        const int ihe = (f >> 8) & 255;
+        const double dWl0 = wl[k] - B.wlcent[il];
+        double dWl = dWl0;
+        if (ihe > 0) dWl = dWl0 - A.heshf[(ihe - 1) * nt + t];
+        const double V = dWl * vv[g];
+        v = hvoigt64(vtab, anode, aida, av[g], V) * cop[g];
+    }
+    if (A.motype == 1) v = v / A.contstd[t];
+    out[g] = v;
+}
+
+// AnalyticWindow (opacity.f90:678-710) of n lines, one thread per line
+__global__ void k_analytic_window(AtmView A, int64_t n, const int32_t *__restrict__ flags,
+                                  const double *__restrict__ cop, const double *__restrict__ vv,
+                                  const double *__restrict__ av, const double *__restrict__ co, double *dw) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int nt = A.ntau;
+    const double iSqrtPi = 0.5641895835477563;
+    const int ihe = (flags[i] >> 8) & 255;
+    double dWwin = 0.0;
+    for (int t = 0; t < nt; t++) {
+        const size_t o = (size_t)i * nt + t;
+        double r = cop[o] / (A.epsopac * co[o]);
+        if (A.motype == 1) r = r / A.contstd[t];
+        if (r <= 1.0) continue;
+        double w = sqrt(log(r) + fmax(0.0, av[o] * (r * iSqrtPi - av[o]))) / vv[o];
+        if (ihe > 0) w = w + fabs(A.heshf[(ihe - 1) * nt + t]);
+        dWwin = fmax(dWwin, w);
+    }
+    dw[i] = dWwin;
+}
+
+void fsg_launch_xline_setup(cudaStream_t s, const AtmView &A, const LineView &L, XCoef *xc) {
+    if (L.n > 0) k_xline_setup<<<(unsigned)((L.n + 127) / 128), 128, 0, s>>>(A, L, xc);
+}
+void fsg_launch_xline_depth(cudaStream_t s, const AtmView &A, int64_t n, const XCoef *xc, double *cop, double *vv,
+                            double *av) {
+    const int64_t m = n * A.ntau;
+    if (m > 0) k_xline_depth<<<(unsigned)((m + 127) / 128), 128, 0, s>>>(A, n, xc, cop, vv, av);
+}
+void fsg_launch_lineopacity1_pts(cudaStream_t s, const AtmView &A, const BlockView &B, int64_t npts, const double *wl,
+                                 const int32_t *l1, const int32_t *l2, const int32_t *iwl, int64_t loff,
+                                 const VoigtTables &T, double *out) {
+    if (npts > 0)
+        k_lineopacity1_pts<<<(unsigned)((npts + 7) / 8), 256, 0, s>>>(A, B, npts, wl, l1, l2, iwl, loff, T.vtab,
+                                                                      T.anode, T.aida, out);
+}
+void fsg_launch_lineopacity2_pts(cudaStream_t s, const AtmView &A, const BlockView &B, int64_t npts, const double *wl,
+                                 const int32_t *iline, const int32_t *iwl, const double *cop, const double *vv,
+                                 const double *av, const VoigtTables &T, double *out) {
+    const int64_t m = npts * A.ntau;
+    if (m > 0)
+        k_lineopacity2_pts<<<(unsigned)((m + 127) / 128), 128, 0, s>>>(A, B, npts, wl, iline, iwl, cop, vv, av,
+                                                                       T.vtab, T.anode, T.aida, out);
+}
+void fsg_launch_analytic_window(cudaStream_t s, const AtmView &A, int64_t n, const int32_t *flags, const double *cop,
+                                const double *vv, const double *av, const double *co, double *dw) {
+    if (n > 0) k_analytic_window<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(A, n, flags, cop, vv, av, co, dw);
+}

@@ -617,3 +617,118 @@ void fsg_launch_mag_wide(cudaStream_t s, const AtmView &A, const double *wl, con
         k_mag_wide<<<(A.nwl + 7) / 8, 256, 0, s>>>(A, wl, Z, zmap, nwide, widx, flags, ileft, iright, pw, T.fvtab,
                                                    T.anode, T.aida, mlo);
 }
+
+
+// ================================================================================================
+// MagLineOpacity1 and StokesPrfPP on their own, batched (kernel-level entry points)
+// ================================================================================================
+// MagLineOpacity1 (opacity.f90:391-464) at npts points; the block's Zeeman components are indexed by
+// line (Z's CSR arrays); one warp per point, lanes over depths; out [npts][ntau][6]
+__global__ void k_mag_lineopacity1_pts(AtmView A, BlockView B, ZView Z, int64_t npts, const double *__restrict__ wl,
+                                       const int32_t *__restrict__ l1, const int32_t *__restrict__ l2,
+                                       const int32_t *__restrict__ iwl, int64_t loff, const float2 *__restrict__ fvtab,
+                                       const double *__restrict__ anode, const double *__restrict__ aida, double *out) {
+    const int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (k >= npts) return;
+    const int nt = A.ntau;
+    for (int t = lane; t < nt; t += 32) {
+        double m[6] = { 0, 0, 0, 0, 0, 0 };
+        for (int64_t il = l1[k]; il <= l2[k]; il++) {
+            const int f = B.flags[il - 1];
+            if ((f & FSG_F_WEAK) || (f & FSG_F_WIDE) || iwl[k] < B.ileft[il - 1] || iwl[k] > B.iright[il - 1]) continue;
+            const size_t o = (size_t)(il - loff - 1) * nt + t;
+            mag_profiles_t(A, t, wl[k], B.wlcent[il - 1], (f >> 8) & 255, Z, il - 1, B.cop[o], B.vv[o], B.av[o],
+                           fvtab, anode, aida, m);
+        }
+        double *dst = out + ((size_t)k * nt + t) * 6;
+        for (int q = 0; q < 6; q++) dst[q] = (A.motype == 1) ? m[q] / A.contstd[t] : m[q];
+    }
+}
+
+// StokesPrfPP (solver.f90:265-394) at the grid wavelengths iwl[k] (1-based) with given source functions
+// src [npts][ntau]: one thread per (point, angle) over per-thread work arrays, as k_stokes_thr;
+// geo [5][nmu] (SPhi2, CPhi2, CPhi, S2Psi, C2Psi); out [npts][4][nmu]
+__global__ void __launch_bounds__(128)
+k_stokes_prf_pts(AtmView A, const double *__restrict__ lineopac, const double *__restrict__ mlo,
+                 const double *__restrict__ rhox, int nmu, const double *__restrict__ xmu,
+                 const double *__restrict__ geo, int64_t npts, const int32_t *__restrict__ iwls,
+                 const double *__restrict__ src, double *work, double *out) {
+    const size_t T = (size_t)gridDim.x * blockDim.x;
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= npts * nmu) return;
+    const int64_t k = g / nmu;
+    const int im = (int)(g - k * nmu);
+    const int iwl = iwls[k] - 1;
+    const int N = A.ntau;
+    double *W = work + g;
+#define F(f, t) W[((size_t)(f) * N + (t)) * T]
+    const double gm[5] = { geo[0 * nmu + im], geo[1 * nmu + im], geo[2 * nmu + im], geo[3 * nmu + im],
+                           geo[4 * nmu + im] };
+    for (int t = 0; t < N; t++) {
+        const size_t o = (size_t)iwl * N + t;
+        double e6[6], s4[4];
+        F(0, t) = stokes_point(mlo + o * 6, lineopac[o], A.contopac[o], src[(size_t)k * N + t], gm, e6, s4);
+        for (int q = 0; q < 6; q++) F(1 + q, t) = e6[q];
+        for (int q = 0; q < 4; q++) F(13 + q, t) = s4[q];
+    }
+    const double Xmu = xmu[im];
+    for (int t = 0; t < N - 1; t++) {
+        if (t == 0) {
+            double Dx1 = (rhox[1] - rhox[0]) / Xmu;
+            double Yp = (F(0, 1) - F(0, 0)) / Dx1;
+            F(21, 0) = Dx1 * (F(0, 1) + 2.0 * F(0, 0) + Dx1 / 2.0 * Yp) / 3.0;
+        } else {
+            const int kk = t + 1;
+            double Dx = (rhox[kk - 1] - rhox[kk - 2]) / Xmu, Dx1 = (rhox[kk] - rhox[kk - 1]) / Xmu;
+            double Der = (F(0, kk - 1) - F(0, kk - 2)) / Dx, Der1 = (F(0, kk) - F(0, kk - 1)) / Dx1, Yp;
+            if (Der * Der1 > 0.0) {
+                double Lambda = (1.0 + Dx1 / (Dx + Dx1)) / 3.0;
+                Yp = (Der / (Lambda * Der1 + (1.0 - Lambda) * Der)) * Der1;
+            } else Yp = 0.0;
+            F(21, kk - 1) = Dx1 * (F(0, kk) + 2.0 * F(0, kk - 1) + Dx1 / 2.0 * Yp) / 3.0;
+        }
+    }
+    for (int row = 0; row < 10; row++) {
+        const int fi = row < 4 ? 13 + row : 1 + (row - 4), fo = row < 4 ? 17 + row : 7 + (row - 4);
+        for (int kk = 0; kk < N; kk++) {
+            double o;
+            if (kk == 0) o = (F(fi, 1) - F(fi, 0)) / F(21, 0);
+            else if (kk == N - 1) o = (F(fi, N - 1) - F(fi, N - 2)) / F(21, N - 2);
+            else {
+                double Dx = F(21, kk - 1), Dx1 = F(21, kk);
+                double InvDx = 1.0 / Dx, InvDx1 = 1.0 / Dx1;
+                double Lambda = (1.0 + Dx1 / (Dx + Dx1)) / 3.0, Lambda1 = 1.0 - Lambda;
+                double Der = (F(fi, kk) - F(fi, kk - 1)) * InvDx, Der1 = (F(fi, kk + 1) - F(fi, kk)) * InvDx1;
+                o = (Der * Der1 > 0.0) ? (Der / (Lambda * Der1 + Lambda1 * Der)) * Der1 : 0.0;
+            }
+            F(fo, kk) = o;
+        }
+    }
+    double XINT2[4] = { F(13, N - 1), 0.0, 0.0, 0.0 };
+    stokes_sweep(N, N, &F(1, 0), &F(7, 0), &F(13, 0), &F(17, 0), &F(21, 0), XINT2, T);
+    for (int q = 0; q < 4; q++) out[((size_t)k * 4 + q) * nmu + im] = XINT2[q];
+#undef F
+}
+
+void fsg_launch_mag_lineopacity1_pts(cudaStream_t s, const AtmView &A, const BlockView &B, const ZView &Z,
+                                     int64_t npts, const double *wl, const int32_t *l1, const int32_t *l2,
+                                     const int32_t *iwl, int64_t loff, const VoigtTables &T, double *out) {
+    if (npts > 0)
+        k_mag_lineopacity1_pts<<<(unsigned)((npts + 7) / 8), 256, 0, s>>>(A, B, Z, npts, wl, l1, l2, iwl, loff,
+                                                                          T.fvtab, T.anode, T.aida, out);
+}
+
+size_t fsg_stokes_pts_work(int64_t npts, int nmu, int ntau) {
+    const int64_t thr = ((npts * nmu + 127) / 128) * 128;
+    return sizeof(double) * (size_t)STK_FIELDS * (size_t)ntau * (size_t)thr;
+}
+
+void fsg_launch_stokes_prf_pts(cudaStream_t s, const AtmView &A, const double *lineopac, const double *mlo,
+                               const double *rhox, int nmu, const double *xmu, const double *geo, int64_t npts,
+                               const int32_t *iwl, const double *src, double *work, double *out) {
+    const int64_t m = npts * nmu;
+    if (m > 0)
+        k_stokes_prf_pts<<<(unsigned)((m + 127) / 128), 128, 0, s>>>(A, lineopac, mlo, rhox, nmu, xmu, geo, npts, iwl,
+                                                                     src, work, out);
+}

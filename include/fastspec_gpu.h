@@ -212,7 +212,62 @@ int fsg_mag_lineop_reset(fsg_ctx *ctx);
 int fsg_mag_radtran(fsg_ctx *ctx, int bframe, const double *bfield, int nbfield, double *spz,
                     double *spc, double *sfl, double *sfc);
 
-/* ---- kernel-level entry points (elemental reference functions, batched on the GPU) ------- */
+/* ---- kernel-level entry points (elemental reference functions, batched on the GPU) -------
+ * Each evaluates many lines or wavelengths in one call with the drivers' own device code (FP64, the
+ * reference's operand order).  Host arrays in the reference's argument meaning; line and wavelength
+ * indices 1-based.  The atmosphere (and, for StokesPrfPP, the continuum, LineOpac, MagLineOpac and
+ * angles) come from the context, as the reference's routines read them from module globals. */
+typedef struct {            /* XlineCoef (opacity.f90:43-58); IxPF: 0-based species column */
+    double  WaveL, Hnux, Elo, Gf, Grad, Xmass, Cqst, Qdiv, Cvdw, AboPre, AboVbc, AboExp;
+    int32_t IxPF, MdQst, MdVdw, IxHe;
+} fsg_xcoef;
+/* The reference's line arrays as LineopCalc / MagLineopCalc hold them: per line (nlines) Wlcent (the
+ * centre less Wfirst [A]), LinFlag, Ileft, Iright; per block line (nblock) LinCop, LinVvgt, LinAvgt
+ * [nblock][ntau] (the reference's (Ntau, NlinesStep) arrays); for the magnetic routine the Zeeman
+ * components by line (npi / nsi counts, pi_off / si_off offsets, shifts scaled to [A] as MagLineopCalc
+ * scales them, synth.f90:1150-1154, and strengths; each sigma list holds its blue half first). */
+typedef struct {
+    int64_t nlines, nblock;
+    const double *wlcent;
+    const int32_t *flags, *ileft, *iright;
+    const double *lincop, *linvvgt, *linavgt;
+    const int32_t *npi, *nsi;
+    const int64_t *pi_off, *si_off;
+    const float *splpi, *strpi, *splsi, *strsi;
+} fsg_lineblock;
+/* XlineSetup (opacity.f90:96-235) of every line of a host list, with the flags the drivers set
+ * before it (molecule and ABO bits from the list, synth.f90:837-845): xc[n]. */
+int fsg_xline_setup(fsg_ctx *ctx, const fsg_lines *lines, fsg_xcoef *xc);
+/* XlineDepth (opacity.f90:239-293) of n lines at every depth: lincop/linvvgt/linavgt [n][ntau]. */
+int fsg_xline_depth(fsg_ctx *ctx, int64_t n, const fsg_xcoef *xc, double *lincop, double *linvvgt,
+                    double *linavgt);
+/* LineOpacity1 (opacity.f90:297-346) at npts points: point k sums lines l1[k]..l2[k] of the block
+ * (weak and wide lines, and lines whose window misses iwl[k], skipped) at Wl = wl[k] (the grid offset
+ * Wave(iwl[k])), block line = line - loff: linop [npts][ntau] (divided by ContOpacStd under Motype 1). */
+int fsg_lineopacity1(fsg_ctx *ctx, const fsg_lineblock *blk, int64_t npts, const double *wl,
+                     const int32_t *l1, const int32_t *l2, const int32_t *iwl, int64_t loff, double *linop);
+/* LineOpacity2 (opacity.f90:350-386): point k is line iline[k] of the block at Wl = wl[k], grid index
+ * iwl[k], with its own rows lincop/linvvgt/linavgt [npts][ntau]: linop [npts][ntau]. */
+int fsg_lineopacity2(fsg_ctx *ctx, const fsg_lineblock *blk, int64_t npts, const double *wl,
+                     const int32_t *iline, const int32_t *iwl, const double *lincop, const double *linvvgt,
+                     const double *linavgt, double *linop);
+/* MagLineOpacity1 (opacity.f90:391-464) as LineOpacity1 over the block's Zeeman components:
+ * maglinop [npts][ntau][6] (pi, blue and red sigma absorption; pi, blue and red dispersion). */
+int fsg_mag_lineopacity1(fsg_ctx *ctx, const fsg_lineblock *blk, int64_t npts, const double *wl,
+                         const int32_t *l1, const int32_t *l2, const int32_t *iwl, int64_t loff,
+                         double *maglinop);
+/* AnalyticWindow (opacity.f90:678-710) of n lines: line k with LinFlag flags[k] (He I entry in bits
+ * 8-15) and rows lincop/linvvgt/linavgt/contopac [n][ntau] (ContOpacL: the continuum at its centre):
+ * the window half-widths dw[n] [A]. */
+int fsg_analytic_window(fsg_ctx *ctx, int64_t n, const int32_t *flags, const double *lincop,
+                        const double *linvvgt, const double *linavgt, const double *contopac, double *dw);
+/* StokesPrfPP (solver.f90:265-394) at npts grid wavelengths iwl[k]: the context's MagLineOpac (after
+ * fsg_mag_lineop_calc), LineOpac, ContOpac, Rhox and angles, the source function src [npts][ntau] and
+ * the field projection per angle sphi2, cphi2, cphi, s2psi, c2psi [nmu]: stokes [npts][4][nmu]
+ * (I, Q, U, V). */
+int fsg_stokes_prf_pp(fsg_ctx *ctx, int64_t npts, const int32_t *iwl, const double *src, const double *sphi2,
+                      const double *cphi2, const double *cphi, const double *s2psi, const double *c2psi,
+                      double *stokes);
 /* HVoigt (voigt.f90:76-110) and FVoigt (voigt.f90:256-299) over host arrays of length n. */
 int fsg_hvoigt(fsg_ctx *ctx, int64_t n, const double *a, const double *v, double *h);
 int fsg_fvoigt(fsg_ctx *ctx, int64_t n, const double *a, const double *v, double *h, double *l);

@@ -51,6 +51,13 @@ class _Lines(C.Structure):
     ]
 
 
+class XCoef(C.Structure):
+    """or_xcoef: XlineCoef (opacity.f90:43-58)."""
+    _fields_ = [(n, C.c_double) for n in ("WaveL", "Hnux", "Elo", "Gf", "Grad", "Xmass", "Cqst", "Qdiv", "Cvdw",
+                                          "AboPre", "AboVbc", "AboExp")] + \
+               [(n, C.c_int) for n in ("IxPF", "MdQst", "MdVdw", "IxHe")]
+
+
 class _Stats(C.Structure):
     _fields_ = [("nlines_in", C.c_long), ("nlines_used", C.c_long), ("nwide", C.c_long),
                 ("nweak", C.c_long), ("nsegments", C.c_long), ("nrefills", C.c_long),
@@ -92,6 +99,18 @@ def lib():
                                          C.c_long, _dp, _ip, _ip, _ip, _fp, C.c_int, _dp, _dp,
                                          C.POINTER(_Stats)]
         L.or_locprf_pp.argtypes = [_dp, _dp, C.c_int, _dp, _dp, _dp, C.c_int]
+        L.or_xline_setup.argtypes = [C.POINTER(_State), C.POINTER(_Lines), C.c_long, C.c_int, C.POINTER(XCoef)]
+        L.or_xline_depth.argtypes = [C.POINTER(_State), C.c_int, C.POINTER(XCoef), _dp, _dp, _dp]
+        L.or_lineopacity1.argtypes = [C.POINTER(_State), _dp, _ip, _ip, _ip, _dp, _dp, _dp, C.c_double, C.c_int,
+                                      C.c_int, C.c_int, C.c_long, _dp]
+        L.or_lineopacity2.argtypes = [C.POINTER(_State), C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_int,
+                                      _dp, _dp, _dp, _dp]
+        L.or_mag_lineopacity1.argtypes = [C.POINTER(_State), _dp, _ip, _ip, _ip, _dp, _dp, _dp, _ip, _ip, _lp, _lp,
+                                          _fp, _fp, _fp, _fp, C.c_double, C.c_int, C.c_int, C.c_int, C.c_long, _dp]
+        L.or_analytic_window.restype = C.c_double
+        L.or_analytic_window.argtypes = [C.POINTER(_State), C.c_int, _dp, _dp, _dp, _dp]
+        L.or_stokes_prf_pp.argtypes = [C.POINTER(_State), _dp, _dp, _dp, _dp, C.c_int, _dp, _dp, _dp, _dp, _dp,
+                                       _dp, _dp]
         L.or_solve4x4.argtypes = [_dp, _dp, _dp]
         L.or_radtran.argtypes = [C.POINTER(_State), C.c_int, _dp, _dp, _dp, _dp]
         L.or_mag_radtran.argtypes = [C.POINTER(_State), C.c_int, _dp, C.c_int, _dp, _dp, _dp, _dp, _dp]
@@ -284,6 +303,81 @@ class Lines:
             L.pi_off = _p(k["pi_off"], C.c_long); L.si_off = _p(k["si_off"], C.c_long)
         self.L = L
         self.n = n
+
+
+# ---- the elemental routines on their own (checks of the library's kernel-level entry points) --------
+def xline_setup(state, lines, i, list_type=2):
+    """XlineSetup of line i (0-based): an XCoef structure."""
+    xc = XCoef()
+    lib().or_xline_setup(C.byref(state.s), C.byref(lines.L), int(i), int(list_type), C.byref(xc))
+    return xc
+
+
+def xline_depth(state, xc):
+    """XlineDepth of one XCoef at every depth: (lincop, linvvgt, linavgt) [ntau]."""
+    n = state.ntau
+    out = [np.zeros(n) for _ in range(3)]
+    for t in range(n):
+        c, v, a = C.c_double(), C.c_double(), C.c_double()
+        lib().or_xline_depth(C.byref(state.s), t, C.byref(xc), C.byref(c), C.byref(v), C.byref(a))
+        out[0][t], out[1][t], out[2][t] = c.value, v.value, a.value
+    return tuple(out)
+
+
+def lineopacity1(state, blk, Wl, l1, l2, iwl, loff=0):
+    """LineOpacity1 over the block dict (wlcent, flags, ileft, iright, lincop, linvvgt, linavgt): [ntau]."""
+    out = np.zeros(state.ntau)
+    b = {k: (_f64(v) if k in ("wlcent", "lincop", "linvvgt", "linavgt") else _i32(v)) for k, v in blk.items()
+         if k in ("wlcent", "flags", "ileft", "iright", "lincop", "linvvgt", "linavgt")}
+    lib().or_lineopacity1(C.byref(state.s), _p(b["wlcent"], C.c_double), _p(b["flags"], C.c_int),
+                          _p(b["ileft"], C.c_int), _p(b["iright"], C.c_int), _p(b["lincop"], C.c_double),
+                          _p(b["linvvgt"], C.c_double), _p(b["linavgt"], C.c_double), float(Wl), int(l1), int(l2),
+                          int(iwl), int(loff), _p(out, C.c_double))
+    return out
+
+
+def lineopacity2(state, Wl, wlcent, flag, ileft, iright, iwl, lincop, linvvgt, linavgt):
+    out = np.zeros(state.ntau)
+    c, v, a = _f64(lincop), _f64(linvvgt), _f64(linavgt)
+    lib().or_lineopacity2(C.byref(state.s), float(Wl), float(wlcent), int(flag), int(ileft), int(iright), int(iwl),
+                          _p(c, C.c_double), _p(v, C.c_double), _p(a, C.c_double), _p(out, C.c_double))
+    return out
+
+
+def mag_lineopacity1(state, blk, zeeman, Wl, l1, l2, iwl, loff=0):
+    """MagLineOpacity1 over the block dict and Zeeman components (npi, nsi, spl_pi, str_pi, spl_si,
+    str_si; shifts in A): [ntau][6]."""
+    out = np.zeros((state.ntau, 6))
+    b = {k: (_f64(v) if k in ("wlcent", "lincop", "linvvgt", "linavgt") else _i32(v)) for k, v in blk.items()
+         if k in ("wlcent", "flags", "ileft", "iright", "lincop", "linvvgt", "linavgt")}
+    npi, nsi = _i32(zeeman[0]), _i32(zeeman[1])
+    poff = np.ascontiguousarray(np.concatenate([[0], np.cumsum(npi)[:-1]]), np.int64)
+    soff = np.ascontiguousarray(np.concatenate([[0], np.cumsum(nsi)[:-1]]), np.int64)
+    z = [_f32(x) if len(x) else np.zeros(1, np.float32) for x in zeeman[2:]]
+    lib().or_mag_lineopacity1(C.byref(state.s), _p(b["wlcent"], C.c_double), _p(b["flags"], C.c_int),
+                              _p(b["ileft"], C.c_int), _p(b["iright"], C.c_int), _p(b["lincop"], C.c_double),
+                              _p(b["linvvgt"], C.c_double), _p(b["linavgt"], C.c_double), _p(npi, C.c_int),
+                              _p(nsi, C.c_int), _p(poff, C.c_long), _p(soff, C.c_long), _p(z[0], C.c_float),
+                              _p(z[1], C.c_float), _p(z[2], C.c_float), _p(z[3], C.c_float), float(Wl), int(l1),
+                              int(l2), int(iwl), int(loff), _p(out, C.c_double))
+    return out
+
+
+def analytic_window(state, flag, lincop, linvvgt, linavgt, contopac):
+    c, v, a, co = _f64(lincop), _f64(linvvgt), _f64(linavgt), _f64(contopac)
+    return lib().or_analytic_window(C.byref(state.s), int(flag), _p(c, C.c_double), _p(v, C.c_double),
+                                    _p(a, C.c_double), _p(co, C.c_double))
+
+
+def stokes_prf_pp(state, m6, lop, cop, src, xmu, sphi2, cphi2, cphi, s2psi, c2psi):
+    """StokesPrfPP: m6 [ntau][6], lop/cop/src [ntau], field per angle: [4][nmu]."""
+    xmu = _f64(xmu)
+    out = np.zeros((4, len(xmu)))
+    arr = [_f64(x) for x in (m6, lop, cop, src)]
+    g = [_f64(x) for x in (sphi2, cphi2, cphi, s2psi, c2psi)]
+    lib().or_stokes_prf_pp(C.byref(state.s), *[_p(x, C.c_double) for x in arr], len(xmu), _p(xmu, C.c_double),
+                           *[_p(x, C.c_double) for x in g], _p(out, C.c_double))
+    return out
 
 
 def reader_select(arrays, wstart, wend):

@@ -1744,3 +1744,110 @@ void or_disk_integ_conv(int nmu, int nwl, const double *xmu, const double *wmu, 
     if (gsig > 0.0) { or_convol_gau(nwl, sfl, gsig); or_convol_gau(nwl, sfc, gsig); }
     free(rk); free(mk); free(mr); free(mt); free(siL); free(siC); free(tL); free(tC);
 }
+
+
+/* ---- the elemental routines on their own ------------------------------------------------------- */
+void or_xline_setup(const or_state *s, const or_lines *L, long i, int list_type, or_xcoef *xc) {
+    xcoef XC;
+    xline_setup(s, L, i, L->wl[i] - s->wfirst, input_flags(L, i, list_type), &XC);
+    xc->WaveL = XC.WaveL; xc->Hnux = XC.Hnux; xc->Elo = XC.Elo; xc->Gf = XC.Gf; xc->Grad = XC.Grad;
+    xc->Xmass = XC.Xmass; xc->Cqst = XC.Cqst; xc->Qdiv = XC.Qdiv; xc->Cvdw = XC.Cvdw;
+    xc->AboPre = XC.AboPre; xc->AboVbc = XC.AboVbc; xc->AboExp = XC.AboExp;
+    xc->IxPF = XC.IxPF; xc->MdQst = XC.MdQst; xc->MdVdw = XC.MdVdw; xc->IxHe = XC.IxHe;
+}
+
+void or_xline_depth(const or_state *s, int t, const or_xcoef *xc, double *lincop, double *linvvgt,
+                    double *linavgt) {
+    xcoef XC;
+    XC.WaveL = xc->WaveL; XC.Hnux = xc->Hnux; XC.Elo = xc->Elo; XC.Gf = xc->Gf; XC.Grad = xc->Grad;
+    XC.Xmass = xc->Xmass; XC.Cqst = xc->Cqst; XC.Qdiv = xc->Qdiv; XC.Cvdw = xc->Cvdw;
+    XC.AboPre = xc->AboPre; XC.AboVbc = xc->AboVbc; XC.AboExp = xc->AboExp;
+    XC.IxPF = xc->IxPF; XC.MdQst = xc->MdQst; XC.MdVdw = xc->MdVdw; XC.IxHe = xc->IxHe;
+    xline_depth(s, t, &XC, lincop, linvvgt, linavgt);
+}
+
+void or_lineopacity1(const or_state *s, const double *wlcent, const int *flags, const int *ileft,
+                     const int *iright, const double *lincop, const double *linvvgt, const double *linavgt,
+                     double Wl, int l1, int l2, int iwl, long loff, double *linop) {
+    int nt = s->ntau;
+    for (int t = 0; t < nt; t++) linop[t] = 0.0;
+    for (long il = l1; il <= l2; il++) {
+        int f = flags[il - 1];
+        if ((f & 1) || (f & 8) || iwl < ileft[il - 1] || iwl > iright[il - 1]) continue;
+        int ihe = (f >> 8) & 255;
+        double dWl0 = Wl - wlcent[il - 1];
+        const double *c = lincop + (il - loff - 1) * nt, *v = linvvgt + (il - loff - 1) * nt,
+                     *a = linavgt + (il - loff - 1) * nt;
+        for (int t = 0; t < nt; t++) {
+            double dWl = dWl0;
+            if (ihe > 0) dWl = dWl0 - s->heshf[(ihe - 1) * nt + t];
+            double V = dWl * v[t];
+            linop[t] = linop[t] + or_hvoigt(a[t], V) * c[t];
+        }
+    }
+    if (s->motype == 1) for (int t = 0; t < nt; t++) linop[t] = linop[t] / s->contopac_std[t];
+}
+
+void or_lineopacity2(const or_state *s, double Wl, double wlcent, int flag, int ileft, int iright, int iwl,
+                     const double *lincop, const double *linvvgt, const double *linavgt, double *linop) {
+    linework W;
+    long orig = 0;
+    W.n = 1; W.wlcent = &wlcent; W.flag = &flag; W.ileft = &ileft; W.iright = &iright; W.orig = &orig;
+    lineopacity2(s, Wl, &W, 0, iwl, lincop, linvvgt, linavgt, linop);
+}
+
+void or_mag_lineopacity1(const or_state *s, const double *wlcent, const int *flags, const int *ileft,
+                         const int *iright, const double *lincop, const double *linvvgt, const double *linavgt,
+                         const int *npi, const int *nsi, const long *pi_off, const long *si_off,
+                         const float *splpi, const float *strpi, const float *splsi, const float *strsi,
+                         double Wl, int l1, int l2, int iwl, long loff, double *M) {
+    int nt = s->ntau;
+    for (int q = 0; q < 6 * nt; q++) M[q] = 0.0;
+    for (long iline = l1; iline <= l2; iline++) {
+        int f = flags[iline - 1];
+        if ((f & 1) || (f & 8) || iwl < ileft[iline - 1] || iwl > iright[iline - 1]) continue;
+        long il = iline - loff - 1;
+        int ihe = (f >> 8) & 255;
+        const long i = iline - 1;
+        for (int t = 0; t < nt; t++) {
+            vline FL = fvline_init(linavgt[il * nt + t]);
+            double Xn = lincop[il * nt + t], sc = linvvgt[il * nt + t];
+            double Vbase = (Wl - wlcent[i]) * sc;
+            if (ihe > 0) Vbase = Vbase - s->heshf[(ihe - 1) * nt + t] * sc;
+            double *m = M + 6 * t, V, Vg, Fv, Str;
+            for (int k = 0; k < npi[i]; k++) {
+                V = Vbase - (double)splpi[pi_off[i] + k] * sc;
+                fvoigt_line(FL, V, &Vg, &Fv);
+                Str = Xn * (double)strpi[pi_off[i] + k];
+                m[0] = m[0] + Str * Vg; m[3] = m[3] + Str * Fv;
+            }
+            int Nsh = nsi[i] / 2;
+            for (int k = 0; k < Nsh; k++) {
+                V = Vbase - (double)splsi[si_off[i] + k] * sc;
+                fvoigt_line(FL, V, &Vg, &Fv);
+                Str = Xn * (double)strsi[si_off[i] + k];
+                m[1] = m[1] + Str * Vg; m[4] = m[4] + Str * Fv;
+            }
+            for (int k = Nsh; k < nsi[i]; k++) {
+                V = Vbase - (double)splsi[si_off[i] + k] * sc;
+                fvoigt_line(FL, V, &Vg, &Fv);
+                Str = Xn * (double)strsi[si_off[i] + k];
+                m[2] = m[2] + Str * Vg; m[5] = m[5] + Str * Fv;
+            }
+        }
+    }
+    if (s->motype == 1)
+        for (int t = 0; t < nt; t++)
+            for (int q = 0; q < 6; q++) M[6 * t + q] = M[6 * t + q] / s->contopac_std[t];
+}
+
+double or_analytic_window(const or_state *s, int flag, const double *lincop, const double *linvvgt,
+                          const double *linavgt, const double *contopac) {
+    return analytic_window(s, flag, lincop, linvvgt, linavgt, contopac);
+}
+
+void or_stokes_prf_pp(const or_state *s, const double *m6, const double *lop, const double *cop,
+                      const double *src, int nmu, const double *xmu, const double *sphi2, const double *cphi2,
+                      const double *cphi, const double *s2psi, const double *c2psi, double *stokes) {
+    stokes_prf_pp(s, m6, lop, cop, src, nmu, xmu, sphi2, cphi2, cphi, s2psi, c2psi, stokes);
+}

@@ -144,6 +144,39 @@ int or_lineop_calc_range(const or_state *s, const or_lines *L, int list_type, lo
                          float *linstr_out, int nmu, const double *xmu, const double *wmu,
                          or_stats *st, int i0, int i1);
 
+/* ---- the elemental routines on their own (checks of the library's kernel-level entry points) ---- */
+typedef struct {           /* XlineCoef (opacity.f90:43-58); IxPF the 0-based species column */
+    double WaveL, Hnux, Elo, Gf, Grad, Xmass, Cqst, Qdiv, Cvdw, AboPre, AboVbc, AboExp;
+    int IxPF, MdQst, MdVdw, IxHe;
+} or_xcoef;
+/* XlineSetup (opacity.f90:96-235) of line i with the drivers' input flags (synth.f90:837-845) */
+void or_xline_setup(const or_state *s, const or_lines *L, long i, int list_type, or_xcoef *xc);
+/* XlineDepth (opacity.f90:239-293) at depth t (0-based) */
+void or_xline_depth(const or_state *s, int t, const or_xcoef *xc, double *lincop, double *linvvgt,
+                    double *linavgt);
+/* LineOpacity1 (opacity.f90:297-346) over explicit block arrays: per line wlcent, flags, ileft,
+ * iright; per block line lincop/linvvgt/linavgt [nblock][ntau]; lines l1..l2 (1-based), offset loff */
+void or_lineopacity1(const or_state *s, const double *wlcent, const int *flags, const int *ileft,
+                     const int *iright, const double *lincop, const double *linvvgt, const double *linavgt,
+                     double Wl, int l1, int l2, int iwl, long loff, double *linop);
+/* LineOpacity2 (opacity.f90:350-386) of one line (its wlcent, flag, ileft, iright) */
+void or_lineopacity2(const or_state *s, double Wl, double wlcent, int flag, int ileft, int iright, int iwl,
+                     const double *lincop, const double *linvvgt, const double *linavgt, double *linop);
+/* MagLineOpacity1 (opacity.f90:391-464) over explicit block arrays and Zeeman components (CSR by
+ * line, shifts in A): maglinop [ntau][6] */
+void or_mag_lineopacity1(const or_state *s, const double *wlcent, const int *flags, const int *ileft,
+                         const int *iright, const double *lincop, const double *linvvgt, const double *linavgt,
+                         const int *npi, const int *nsi, const long *pi_off, const long *si_off,
+                         const float *splpi, const float *strpi, const float *splsi, const float *strsi,
+                         double Wl, int l1, int l2, int iwl, long loff, double *maglinop);
+/* AnalyticWindow (opacity.f90:678-710) */
+double or_analytic_window(const or_state *s, int flag, const double *lincop, const double *linvvgt,
+                          const double *linavgt, const double *contopac);
+/* StokesPrfPP (solver.f90:265-394): m6 [ntau][6], lop/cop/src [ntau], field per angle; stokes [4][nmu] */
+void or_stokes_prf_pp(const or_state *s, const double *m6, const double *lop, const double *cop,
+                      const double *src, int nmu, const double *xmu, const double *sphi2, const double *cphi2,
+                      const double *cphi, const double *s2psi, const double *c2psi, double *stokes);
+
 /* MagLineopCalc (synth.f90:1098-1455); maglineopac [nwl][ntau][6] accumulated. */
 int or_mag_lineop_calc(const or_state *s, const or_lines *L, int bframe, const double *bfield,
                        long nlines_lim, double *maglineopac, int *flags_out, int *ileft_out,
