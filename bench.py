@@ -401,7 +401,44 @@ def stokes_synthesis(F, torch, dev, steps, warmup):
                             "stokes_QUV_max_over_Ic": float(max(np.max(np.abs(a[0][:, q] - b[0][:, q]) / b[1])
                                                                 for q in (1, 2, 3))),
                             "flux_max_rel": float(np.max(np.abs(a[2] / b[2] - 1)))}
+    if os.path.exists(REF_BIN):
+        ref = ref_stokes(L, os.cpu_count())
+        out["reference"] = ref
+        out["mixed_over_reference"] = out["mixed"]["spectra_per_s"] / ref["spectra_per_s"]
     return out
+
+
+def ref_stokes(L, threads):
+    """The reference executable on the same polarised deck (the 5000 Zeeman lines with their explicit
+    splitting patterns, 6000-6100 A at 0.002 A, BFRAME 1, 2 kG at 60/30 deg, 9 angles), all host
+    threads: its own stage times of the magnetic line opacity (list reading included) and of the
+    polarised formal solver."""
+    import tempfile
+    import oracle
+    from fastspec_b200 import workloads as W
+    d = np.load(os.path.join(HERE, "fastspec_b200", "data", "atm_magnetic.npz"))
+    jlo, jup, glo, gup = L.zeeman
+    pats = [oracle.zeeman_pattern(jlo[i], jup[i], glo[i], gup[i]) for i in range(L.n)]
+    with tempfile.TemporaryDirectory() as wd:
+        W.write_krz(os.path.join(wd, "model.krz"), W.eddington_model(float(d["teff"]), float(d["logg"]),
+                                                                     len(d["T"])))
+        L.write_z(os.path.join(wd, "lines.z"), 6000.0, 6100.0, patterns=pats)
+        deck = ("wave=6000.0, 6100.0, 0.002, 0\nsave=0, 0, 0, 0, 1\nvmic=%.3f\nmolbrd=%d\nlines=\n-1  lines.z\n\n"
+                "model=model.krz\nmus=9\nbframe=1\nbfield=2000, 60, 30\n" % (float(d["vmicro"]), int(d["molbrd"])))
+        with open(os.path.join(wd, "in.dat"), "w") as f:
+            f.write(deck)
+        t0 = time.perf_counter()
+        r = subprocess.run([REF_BIN, "in.dat"], cwd=wd, capture_output=True, text=True,
+                           env=dict(os.environ, OMP_NUM_THREADS=str(threads)))
+        wall = time.perf_counter() - t0
+    if r.returncode != 0 or "Total time" not in r.stdout:
+        return {"error": (r.stdout + r.stderr)[-300:]}
+    lines_s = _stage_seconds(r.stdout, "Total lines read")
+    rt_s = _stage_seconds(r.stdout, "radiative transfer")
+    return {"threads": threads, "opacity_s": lines_s, "solver_s": rt_s, "wall_s": wall,
+            "spectra_per_s": 1.0 / max((lines_s or 0.0) + (rt_s or 0.0), 0.1),
+            "timing": "the executable's own stage timers (0.1 s resolution): line opacity (list reading included) "
+                      "+ polarised radiative transfer, per spectrum"}
 
 
 def run_gpu(args, rank, world):

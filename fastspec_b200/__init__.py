@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(_HERE, "libfastspec_b200.so")
 
 PREC_MIXED = 0
 PREC_FP64 = 1
+FAULT_NONE, FAULT_ALLOC_LIMIT, FAULT_COPY_TIMEOUT = 0, 1, 2
 F_WEAK, F_MOL, F_ABO, F_WIDE = 1, 2, 4, 8
 
 _dp = C.POINTER(C.c_double)
@@ -84,7 +85,7 @@ EXPORTS = [
     "fsg_batch_run", "fsg_batch_flux", "fsg_batch_stream", "fsg_batch_last_error", "fsg_batch_destroy",
     "fsg_set_vmicro", "fsg_set_fractionpf", "fsg_adjoint_dev", "fsg_disk_integ_conv", "fsg_disk_integ_conv_dev",
     "fsg_xline_setup", "fsg_xline_depth", "fsg_lineopacity1", "fsg_lineopacity2", "fsg_mag_lineopacity1",
-    "fsg_analytic_window", "fsg_stokes_prf_pp",
+    "fsg_analytic_window", "fsg_stokes_prf_pp", "fsg_adjoint_range_dev", "fsg_set_fault",
 ]
 
 _lib = None
@@ -167,6 +168,8 @@ def lib():
     L.fsg_lineopacity2.argtypes = [vp, C.POINTER(CLineBlock), C.c_int64, vp, vp, vp, vp, vp, vp, vp]
     L.fsg_analytic_window.argtypes = [vp, C.c_int64, vp, vp, vp, vp, vp, vp]
     L.fsg_stokes_prf_pp.argtypes = [vp, C.c_int64, vp, vp, vp, vp, vp, vp, vp, vp]
+    L.fsg_adjoint_range_dev.argtypes = [vp, C.POINTER(CLines), vp, vp, vp, C.c_int, C.c_int, vp, vp, vp, vp]
+    L.fsg_set_fault.argtypes = [vp, C.c_int, C.c_double]
     _lib = L
     return L
 
@@ -572,6 +575,11 @@ class Context:
         spc = getattr(self, "_he_spc", None)
         return lines if spc is None else lines._with_he_match(spc, self.wfirst)
 
+    def set_fault(self, kind, value=0.0):
+        """Failure injection for tests of the error paths: FAULT_ALLOC_LIMIT (bytes), FAULT_COPY_TIMEOUT
+        (wait bound in ms), FAULT_NONE."""
+        self._ck(self._lib.fsg_set_fault(self.h, int(kind), float(value)), "fsg_set_fault")
+
     def set_vmicro(self, vmicro):
         self._ck(self._lib.fsg_set_vmicro(self.h, C.c_double(float(vmicro))), "fsg_set_vmicro")
 
@@ -580,6 +588,13 @@ class Context:
         v = lambda p: C.c_void_p(p) if p else None
         self._ck(self._lib.fsg_adjoint_dev(self.h, C.byref(dlines), v(d_gflux), v(d_gkappa), v(d_glin), v(d_gvmic)),
                  "fsg_adjoint_dev")
+
+    def adjoint_range_dev(self, dlines, d_flags, d_ileft, d_iright, i0, i1, d_gflux, d_glin, d_gvmic, d_gkappa=None):
+        """The adjoint of one wavelength shard [i0, i1] with the whole list's windows (device pointers)."""
+        v = lambda p: C.c_void_p(p) if p else None
+        self._ck(self._lib.fsg_adjoint_range_dev(self.h, C.byref(dlines), v(d_flags), v(d_ileft), v(d_iright), int(i0),
+                                                 int(i1), v(d_gflux), v(d_gkappa), v(d_glin), v(d_gvmic)),
+                 "fsg_adjoint_range_dev")
 
     def lineop_get(self):
         lo = np.zeros((self.nwl, self.ntau))

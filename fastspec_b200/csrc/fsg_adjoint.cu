@@ -161,7 +161,7 @@ __global__ void k_solver_adjoint(AtmView A, const double *__restrict__ lineopac,
 size_t fsg_line_adjoint_work(int, int, int64_t);
 int fsg_launch_line_adjoint(cudaStream_t, const AtmView &, const LineView &, const VoigtTables &, const int32_t *,
                             const int32_t *, const int32_t *, const double *, const float *, const float *,
-                            const float *, double, double *, double *, void *);
+                            const float *, double, double *, double *, void *, int, int);
 
 // solver work (10 x nt x nwl doubles), dL/dkappa in FP32, the wavelength offsets as FP32 hi + lo,
 // then the line pass's workspace
@@ -177,13 +177,13 @@ size_t fsg_adjoint_work(int nwl, int nt, int64_t n) {
 int fsg_launch_adjoint(cudaStream_t s, const AtmView &A, const LineView &L, const VoigtTables &T,
                        const double *lineopac, const double *rhox, int nmu, const double *xmu, const double *wmu,
                        const int32_t *flags, const int32_t *ileft, const int32_t *iright, const double *gflux,
-                       double *gkappa, double *work, double vmic, double *glin, double *gvmic) {
+                       double *gkappa, double *work, double vmic, double *glin, double *gvmic, int i0, int i1) {
     float *gk32 = (float *)(work + 10 * (size_t)A.ntau * A.nwl), *wvh = gk32 + (size_t)A.ntau * A.nwl, *wvl = wvh + A.nwl;
     k_solver_adjoint<<<(A.nwl + 127) / 128, 128, 0, s>>>(A, lineopac, rhox, nmu, xmu, wmu, gflux, gkappa, work, gk32,
                                                           wvh, wvl);
     if (cudaGetLastError() != cudaSuccess) return FSG_E_CUDA;
     if (L.n > 0)
         return fsg_launch_line_adjoint(s, A, L, T, flags, ileft, iright, gkappa, gk32, wvh, wvl, vmic, glin, gvmic,
-                                       (char *)work + solver_part(A.nwl, A.ntau));
+                                       (char *)work + solver_part(A.nwl, A.ntau), i0, i1);
     return FSG_OK;
 }

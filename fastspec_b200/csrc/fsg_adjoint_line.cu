@@ -86,7 +86,7 @@ k_adj_setup(AtmView A, LineView L, const float *__restrict__ vtab, const float2 
             const int32_t *__restrict__ ileft, const int32_t *__restrict__ iright,
             const double *__restrict__ gkappa, double vmic, int ntp, float *__restrict__ prec,
             float4 *__restrict__ crec, float2 *__restrict__ tabi, LineHdr *__restrict__ hdr, double *glin,
-            double *gvmic) {
+            double *gvmic, int i0, int i1) {
     extern __shared__ double sh[];
     const int nt = A.ntau;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -130,7 +130,9 @@ k_adj_setup(AtmView A, LineView L, const float *__restrict__ vtab, const float2 
     }
     for (int t = nt + lane; t < ntp; t += 32) put_pad_rec(pr, t);
     __syncwarp();
+    // the line's window and its part inside the wavelength range [i0, i1] this call reduces over
     const int il = ileft[i], ir = iright[i];
+    const int rl = max(il, i0), rr_ = min(ir, i1);
     double sl = 0.0, sv = 0.0;
     const double isp2 = 2.0 * FSG_SQRTPIINV;
     if (he) {
@@ -139,7 +141,7 @@ k_adj_setup(AtmView A, LineView L, const float *__restrict__ vtab, const float2 
             const double c = cop[t], vvt = vv[t], a = av[t], qt = q[t], off = wlc + shf[t];
             const VLine64 VL = vline64(anode, aida, a);
             double s1 = 0.0, s2 = 0.0;
-            for (int iw = il - 1; iw < ir; iw++) {
+            for (int iw = rl - 1; iw < rr_; iw++) {
                 const double g = gkappa[(size_t)iw * nt + t];
                 const double v = (A.wave[iw] - off) * vvt;
                 double Hf, Lf;
@@ -169,12 +171,12 @@ k_adj_setup(AtmView A, LineView L, const float *__restrict__ vtab, const float2 
     double eb = 0.0;                                      // sum over free edges of dL/dkappa * profile / step
     for (int t = lane; t < nt; t += 32) {
         const VLine64 VL = vline64(anode, aida, av[t]);
-        if (il > 1) {
+        if (il > 1 && il >= i0 && il <= i1) {            // a free edge inside the range
             const int iw = il - 1;
             const double v = (A.wave[iw] - wlc - shf[t]) * vv[t];
             eb += gkappa[(size_t)iw * nt + t] * hvoigt_line64(vtab, VL, v) * cop[t] / (A.wave[iw] - A.wave[iw - 1]);
         }
-        if (ir < A.nwl) {
+        if (ir < A.nwl && ir >= i0 && ir <= i1) {
             const int iw = ir - 1;
             const double v = (A.wave[iw] - wlc - shf[t]) * vv[t];
             eb += gkappa[(size_t)iw * nt + t] * hvoigt_line64(vtab, VL, v) * cop[t] / (A.wave[iw + 1] - A.wave[iw]);
@@ -196,8 +198,8 @@ k_adj_setup(AtmView A, LineView L, const float *__restrict__ vtab, const float2 
         LineHdr h = {};
         h.wlh = (float)wlc;
         h.wll = (float)(wlc - (double)h.wlh);
-        h.ileft = he ? 1 : il;                            // helium lines: done above
-        h.iright = he ? 0 : ir;
+        h.ileft = he ? 1 : rl;                            // helium lines: done above
+        h.iright = he ? 0 : rr_;
         h.cl = 1; h.cr = 0;
         if (hcore >= 0.0 && !he) {
             // 1-based indices of the first wavelength >= wlc - hcore and the last <= wlc + hcore,
@@ -205,7 +207,7 @@ k_adj_setup(AtmView A, LineView L, const float *__restrict__ vtab, const float2 
             const int a = lower_index(A.wave, A.nwl, wlc - hcore) + 1;
             int b = lower_index(A.wave, A.nwl, wlc + hcore);
             if (b < A.nwl && A.wave[b] == wlc + hcore) b++;
-            const int cl = max(a - 1, il), cr = min(b + 1, ir);
+            const int cl = max(a - 1, rl), cr = min(b + 1, rr_);
             if (cl <= cr) { h.cl = cl; h.cr = cr; }
         }
         hdr[i] = h;
@@ -476,7 +478,7 @@ size_t fsg_line_adjoint_work(int nwl, int nt, int64_t n) {
 int fsg_launch_line_adjoint(cudaStream_t s, const AtmView &A, const LineView &L, const VoigtTables &T,
                             const int32_t *flags, const int32_t *ileft, const int32_t *iright, const double *gkappa,
                             const float *gk32, const float *wvh, const float *wvl, double vmic, double *glin,
-                            double *gvmic, void *work) {
+                            double *gvmic, void *work, int i0, int i1) {
     const int nt = A.ntau, nwl = A.nwl, ntp = adj_ntp(nt), kd = adj_kd(nt), nw = ntp / kd;
     const int64_t n = L.n;
     const int ntiles = (nwl + ADJ_TW - 1) / ADJ_TW;
@@ -494,7 +496,7 @@ int fsg_launch_line_adjoint(cudaStream_t s, const AtmView &A, const LineView &L,
     size_t smem = sizeof(double) * 6 * nt * ADJ_SETUP_WARPS;
     k_adj_setup<<<(unsigned)((n + ADJ_SETUP_WARPS - 1) / ADJ_SETUP_WARPS), 32 * ADJ_SETUP_WARPS, smem, s>>>(
         A, L, T.vtab, T.fvtab, T.anode, T.aida, flags, ileft, iright, gkappa, vmic, ntp, prec, crec, tabi, hdr, glin,
-        gvmic);
+        gvmic, i0, i1);
     int rc = fsg_launch_tile_span_tw(s, ADJ_TW, 0, nwl, n, hdr, tlo, thi, span, span_bytes);
     if (rc) return rc;
     AdjTileJob J;

@@ -1,5 +1,6 @@
 // fsg_api.cu -- C-ABI entry points: context, uploads, and the LineopCalc / RadTranCalc drivers.
 #include "fsg_internal.cuh"
+#include "fsg_mbar.cuh"
 
 #include <math.h>
 #include <stdio.h>
@@ -51,16 +52,18 @@ void fsg_launch_fvoigt(cudaStream_t, int64_t, const double *, const double *, do
 void fsg_launch_locprf(cudaStream_t, int, int, const double *, int, const double *, const double *, const double *,
                        double *, double *);
 int fsg_launch_accum_fast(cudaStream_t, int, int, int, const double *, const LineHdr *, const WingRec *,
-                          const int *, const int *, double *, int *);
-void fsg_launch_count_core(cudaStream_t, int64_t, const LineHdr *, unsigned long long *);
+                          const int *, const int *, double *, int *, unsigned, unsigned long long);
 int fsg_launch_core_fast(cudaStream_t, int, int, const double *, const LineHdr *, const WingRec *, const CoreRec *,
-                         const int *, const int *, const float4 *, double *);
+                         const int *, const int *, const float4 *, double *, unsigned long long *, int *, unsigned,
+                         unsigned long long);
 struct WingJob { int ntau, nwl; const double *wave; const LineHdr *hdr; const WingRec *wing;
-                 const int *tile_lo, *tile_hi; double *lineopac; };
+                 const int *tile_lo, *tile_hi; double *lineopac; unsigned extra_tx; unsigned long long wait_ns; };
 struct CoreJob { int ntau, nwl; const double *wave; const LineHdr *hdr; const WingRec *wing; const CoreRec *core;
-                 const int *tile_lo, *tile_hi; double *lineopac; };
+                 const int *tile_lo, *tile_hi; double *lineopac; unsigned long long *nevals; unsigned extra_tx;
+                 unsigned long long wait_ns; };
 int fsg_launch_accum_batch(cudaStream_t, int, int, const WingJob *, const int *, int, int, unsigned *, int *);
-int fsg_launch_core_batch(cudaStream_t, int, const CoreJob *, const int *, int, int, const float4 *, unsigned *);
+int fsg_launch_core_batch(cudaStream_t, int, const CoreJob *, const int *, int, int, const float4 *, unsigned *,
+                          int *);
 int fsg_class_pix(int);
 int fsg_fast_tiles(int);
 size_t fsg_tile_span_scratch(int64_t);
@@ -75,7 +78,7 @@ void fsg_launch_conv(cudaStream_t, int, const double *, int, const double *, int
 size_t fsg_adjoint_work(int, int, int64_t);
 int fsg_launch_adjoint(cudaStream_t, const AtmView &, const LineView &, const VoigtTables &, const double *,
                        const double *, int, const double *, const double *, const int32_t *, const int32_t *,
-                       const int32_t *, const double *, double *, double *, double, double *, double *);
+                       const int32_t *, const double *, double *, double *, double, double *, double *, int, int);
 size_t fsg_linstr_work(int64_t, int, int);
 void fsg_launch_linstr(cudaStream_t, const AtmView &, const LineView &, const VoigtTables &, const int32_t *, int64_t,
                        int64_t, int, const double *, const double *, const double *, const RayView &, double *, float *);
@@ -96,7 +99,8 @@ void fsg_launch_gather_lines(cudaStream_t, const LineView &, const int64_t *, in
 int fsg_select_wide(cudaStream_t, int64_t, const int32_t *, int *, int64_t *, int64_t *, int64_t *);
 void fsg_launch_scatter_flags(cudaStream_t, int64_t, const int64_t *, const int32_t *, int32_t *);
 double fsg_count_evals(fsg_ctx *, int64_t, const int32_t *, const int32_t *, const int32_t *, int, int);
-static double count_windows(fsg_ctx *, int64_t, const int32_t *, const int32_t *, const int32_t *, int, int);
+static double count_windows(fsg_ctx *, int64_t, const int32_t *, const int32_t *, const int32_t *, int, int,
+                            const int32_t *npi = nullptr, const int32_t *nsi = nullptr);
 void fsg_launch_range_clip(cudaStream_t, int64_t, const int32_t *, const int32_t *, const int32_t *, int, int,
                            int32_t *, int32_t *, int32_t *);
 int fsg_launch_stokes(cudaStream_t, const AtmView &, const double *, const double *, const double *, int,
@@ -140,6 +144,11 @@ struct DBuf {
 struct fsg_ctx {
     fsg_config cfg;
     int device = 0;
+    // failure injection (fsg_set_fault): allocation cap [bytes, 0 = none]; extra bytes every staged chunk
+    // expects and the bound of the staging waits
+    size_t fault_alloc = 0;
+    unsigned fault_extra_tx = 0;
+    unsigned long long fault_wait_ns = WAIT_NS;
     cudaStream_t stream = nullptr;
     std::string err;
     VoigtTables tab{};
@@ -191,7 +200,10 @@ static int cuda_fail(fsg_ctx *c, cudaError_t e, const char *what) {
     return FSG_E_CUDA;
 }
 #define CK(call, what) do { cudaError_t _e = (call); if (_e != cudaSuccess) return cuda_fail(ctx, _e, what); } while (0)
-#define ALLOC(buf, bytes) do { if ((buf).ensure(bytes) != FSG_OK) return fail(ctx, FSG_E_NOMEM, "device allocation failed: " #buf); } while (0)
+#define ALLOC(buf, bytes) do { \
+        if (ctx->fault_alloc && (size_t)(bytes) > ctx->fault_alloc && (buf).cap < (size_t)(bytes)) \
+            return fail(ctx, FSG_E_NOMEM, "device allocation refused (fault injection): " #buf); \
+        if ((buf).ensure(bytes) != FSG_OK) return fail(ctx, FSG_E_NOMEM, "device allocation failed: " #buf); } while (0)
 
 AtmView fsg_view(const fsg_ctx *ctx) {
     AtmView A;
@@ -713,12 +725,12 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st, cons
             if (fsg_launch_tile_span(s, c, ctx->nwl, nb, ctx->d_hdr.as<LineHdr>(), ctx->d_tlo.as<int>(),
                                      ctx->d_thi.as<int>(), ctx->d_span.p, ctx->d_span.cap))
                 return cuda_fail(ctx, cudaGetLastError(), "tile span");
-            fsg_launch_count_core(s, nb, ctx->d_hdr.as<LineHdr>(), ctx->d_ncore.as<unsigned long long>());
             cudaEvent_t ea = kevent(), em = kevent(), eb = kevent();
             cudaEventRecord(ea, s);
             int rc2 = fsg_launch_accum_fast(s, c, nt, ctx->nwl, ctx->d_wave.as<double>(), ctx->d_hdr.as<LineHdr>(),
                                             ctx->d_wing.as<WingRec>(), ctx->d_tlo.as<int>(), ctx->d_thi.as<int>(),
-                                            ctx->d_lineopac.as<double>(), ctx->d_err.as<int>());
+                                            ctx->d_lineopac.as<double>(), ctx->d_err.as<int>(), ctx->fault_extra_tx,
+                                            ctx->fault_wait_ns);
             if (rc2) return cuda_fail(ctx, cudaGetLastError(), "k_accum_fast");
             cudaEventRecord(em, s);
             // core ranges of the same lines, 32-wavelength tiles
@@ -727,7 +739,9 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st, cons
                 return cuda_fail(ctx, cudaGetLastError(), "core tile span");
             rc2 = fsg_launch_core_fast(s, nt, ctx->nwl, ctx->d_wave.as<double>(), ctx->d_hdr.as<LineHdr>(),
                                        ctx->d_wing.as<WingRec>(), ctx->d_core.as<CoreRec>(), ctx->d_tlo.as<int>(),
-                                       ctx->d_thi.as<int>(), ctx->tab.vtab4, ctx->d_lineopac.as<double>());
+                                       ctx->d_thi.as<int>(), ctx->tab.vtab4, ctx->d_lineopac.as<double>(),
+                                       ctx->d_ncore.as<unsigned long long>(), ctx->d_err.as<int>(),
+                                       ctx->fault_extra_tx, ctx->fault_wait_ns);
             if (rc2) return cuda_fail(ctx, cudaGetLastError(), "k_core_fast");
             cudaEventRecord(eb, s);
             kt.push_back({ ea, em });
@@ -767,7 +781,7 @@ static int accumulate_fast(fsg_ctx *ctx, const LineView &LV, fsg_stats *st, cons
     if (st) {
         st->nblocks = nblocks; st->accum_launches = (int64_t)kt.size(); st->ms_accum_kernels = msw + msc;
         st->ms_wing_kernels = msw; st->ms_core_kernels = msc;
-        st->core_evals = (double)ncore * nt;
+        st->core_evals = (double)ncore;
     }
     return FSG_OK;
 }
@@ -1298,7 +1312,7 @@ int fsg_mag_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, int bframe, const 
             st->ms_center = a; st->ms_accum = b; st->ms_total = a + b;
             st->nblocks = nblocks;
             st->line_evals = count_windows(ctx, n, ctx->d_flags.as<int32_t>(), ctx->d_ileft.as<int32_t>(),
-                                           ctx->d_iright.as<int32_t>(), 1, nwl) * nt;
+                                           ctx->d_iright.as<int32_t>(), 1, nwl, Z.npi, Z.nsi) * nt;
         }
         return FSG_OK;
     }
@@ -1427,7 +1441,10 @@ int fsg_mag_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, int bframe, const 
         cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]);
         cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]);
         st->ms_center = a; st->ms_accum = b; st->ms_total = a + b;
-        st->nwide = (int64_t)nwide; st->nblocks = nblocks; st->line_evals = ev;
+        st->nwide = (int64_t)nwide; st->nblocks = nblocks;
+        (void)ev;                                          // the kernels' own count leaves components out
+        st->line_evals = count_windows(ctx, n, ctx->d_flags.as<int32_t>(), ctx->d_ileft.as<int32_t>(),
+                                       ctx->d_iright.as<int32_t>(), 1, nwl, Z.npi, Z.nsi) * nt;
     }
     return FSG_OK;
 }
@@ -2130,20 +2147,62 @@ int fsg_set_fractionpf(fsg_ctx *ctx, const float *fractionpf) {
     return FSG_OK;
 }
 
+int fsg_set_fault(fsg_ctx *ctx, int kind, double value) {
+    if (!ctx) return FSG_E_ARG;
+    switch (kind) {
+        case FSG_FAULT_NONE:
+            ctx->fault_alloc = 0; ctx->fault_extra_tx = 0; ctx->fault_wait_ns = WAIT_NS;
+            return FSG_OK;
+        case FSG_FAULT_ALLOC_LIMIT:
+            if (!(value >= 1.0)) return fail(ctx, FSG_E_ARG, "fsg_set_fault: allocation cap >= 1 byte");
+            ctx->fault_alloc = (size_t)value;
+            return FSG_OK;
+        case FSG_FAULT_COPY_TIMEOUT:
+            if (!(value >= 0.01 && value <= 1000.0)) return fail(ctx, FSG_E_ARG, "fsg_set_fault: wait bound 0.01-1000 ms");
+            ctx->fault_extra_tx = 16;
+            ctx->fault_wait_ns = (unsigned long long)(value * 1e6);
+            return FSG_OK;
+        default:
+            return fail(ctx, FSG_E_ARG, "fsg_set_fault: unknown kind");
+    }
+}
+
 int fsg_set_vmicro(fsg_ctx *ctx, double vmicro) {
     if (!ctx || !(vmicro >= 0.0)) return fail(ctx, FSG_E_ARG, "fsg_set_vmicro: vmicro >= 0");
     ctx->cfg.vmicro = vmicro;
     return FSG_OK;
 }
 
+static int adjoint_common(fsg_ctx *ctx, const fsg_lines *d_lines, const int32_t *fl, const int32_t *il,
+                          const int32_t *ir, int i0, int i1, const double *d_gflux, double *d_gkappa, double *d_glin,
+                          double *d_gvmic);
+
 int fsg_adjoint_dev(fsg_ctx *ctx, const fsg_lines *d_lines, const double *d_gflux, double *d_gkappa, double *d_glin,
                     double *d_gvmic) {
     int rc = check_lines(ctx, d_lines); if (rc) return rc;
+    if (ctx->d_flags.cap < sizeof(int32_t) * (size_t)d_lines->n)
+        return fail(ctx, FSG_E_STATE, "fsg_adjoint_dev: run fsg_lineop_calc(_dev) on this list first");
+    return adjoint_common(ctx, d_lines, ctx->d_flags.as<int32_t>(), ctx->d_ileft.as<int32_t>(),
+                          ctx->d_iright.as<int32_t>(), 1, ctx->nwl, d_gflux, d_gkappa, d_glin, d_gvmic);
+}
+
+int fsg_adjoint_range_dev(fsg_ctx *ctx, const fsg_lines *d_lines, const int32_t *d_flags, const int32_t *d_ileft,
+                          const int32_t *d_iright, int i0, int i1, const double *d_gflux, double *d_gkappa,
+                          double *d_glin, double *d_gvmic) {
+    int rc = check_lines(ctx, d_lines); if (rc) return rc;
+    if (i0 < 1 || i1 > ctx->nwl || i0 > i1) return fail(ctx, FSG_E_ARG, "fsg_adjoint_range_dev: need 1 <= i0 <= i1 <= nwl");
+    if (d_lines->n > 0 && (!d_flags || !d_ileft || !d_iright))
+        return fail(ctx, FSG_E_ARG, "fsg_adjoint_range_dev: window arrays missing");
+    return adjoint_common(ctx, d_lines, d_flags, d_ileft, d_iright, i0, i1, d_gflux, d_gkappa, d_glin, d_gvmic);
+}
+
+static int adjoint_common(fsg_ctx *ctx, const fsg_lines *d_lines, const int32_t *fl, const int32_t *il,
+                          const int32_t *ir, int i0, int i1, const double *d_gflux, double *d_gkappa, double *d_glin,
+                          double *d_gvmic) {
+    int rc;
     if (ctx->nmu < 1) return fail(ctx, FSG_E_STATE, "fsg_adjoint_dev: set mu first");
     if (ctx->radius > 0.0) return fail(ctx, FSG_E_STATE, "fsg_adjoint_dev: plane-parallel models only");
     if (!d_gflux || !d_glin || !d_gvmic) return fail(ctx, FSG_E_ARG, "fsg_adjoint_dev: null argument");
-    if (ctx->d_flags.cap < sizeof(int32_t) * (size_t)d_lines->n)
-        return fail(ctx, FSG_E_STATE, "fsg_adjoint_dev: run fsg_lineop_calc(_dev) on this list first");
     cudaSetDevice(ctx->device);
     rc = ensure_lineopac(ctx); if (rc) return rc;
     const size_t ng = sizeof(double) * (size_t)ctx->nwl * ctx->ntau;
@@ -2151,8 +2210,8 @@ int fsg_adjoint_dev(fsg_ctx *ctx, const fsg_lines *d_lines, const double *d_gflu
     ALLOC(ctx->d_adjwork, fsg_adjoint_work(ctx->nwl, ctx->ntau, d_lines->n));
     rc = fsg_launch_adjoint(ctx->stream, fsg_view(ctx), make_view(d_lines), ctx->tab, ctx->d_lineopac.as<double>(),
                             ctx->d_rhox.as<double>(), ctx->nmu, ctx->d_xmu.as<double>(), ctx->d_wmu.as<double>(),
-                            ctx->d_flags.as<int32_t>(), ctx->d_ileft.as<int32_t>(), ctx->d_iright.as<int32_t>(),
-                            d_gflux, d_gkappa, ctx->d_adjwork.as<double>(), ctx->cfg.vmicro, d_glin, d_gvmic);
+                            fl, il, ir, d_gflux, d_gkappa, ctx->d_adjwork.as<double>(), ctx->cfg.vmicro, d_glin,
+                            d_gvmic, i0, i1);
     ctx->launches += 2;
     if (rc) return cuda_fail(ctx, cudaGetLastError(), "adjoint");
     CK(cudaStreamSynchronize(ctx->stream), "adjoint");
@@ -2232,9 +2291,10 @@ static int batch_jobs(fsg_batch *b, int P) {
         fsg_ctx *c = a.ctx;
         if (a.cn == 0) continue;
         jw.push_back(WingJob{ c->ntau, c->nwl, c->d_wave.as<double>(), a.hdr.as<LineHdr>(), a.wing.as<WingRec>(),
-                              a.wtlo.as<int>(), a.wthi.as<int>(), c->d_lineopac.as<double>() });
+                              a.wtlo.as<int>(), a.wthi.as<int>(), c->d_lineopac.as<double>(), 0u, WAIT_NS });
         jc.push_back(CoreJob{ c->ntau, c->nwl, c->d_wave.as<double>(), a.hdr.as<LineHdr>(), a.wing.as<WingRec>(),
-                              a.core.as<CoreRec>(), a.ctlo.as<int>(), a.cthi.as<int>(), c->d_lineopac.as<double>() });
+                              a.core.as<CoreRec>(), a.ctlo.as<int>(), a.cthi.as<int>(), c->d_lineopac.as<double>(),
+                              nullptr, 0u, WAIT_NS });
         tw.push_back(tw.back() + (c->nwl + 32 * P - 1) / (32 * P));
         tc.push_back(tc.back() + (c->nwl + 31) / 32);
     }
@@ -2271,7 +2331,7 @@ static int batch_accumulate_solve(fsg_batch *b, const fsg_batch_tuning &t, cudaE
             return cuda_fail(ctx, cudaGetLastError(), "k_accum_batch");
         if (ev) cudaEventRecord(ev[1], s);
         if (fsg_launch_core_batch(s, b->ntau_max, b->jobs_c.as<CoreJob>(), b->tile0_c.as<int>(), njobs, t.core_ctas,
-                                  b->atm[0].ctx->tab.vtab4, b->queue.as<unsigned>() + 1))
+                                  b->atm[0].ctx->tab.vtab4, b->queue.as<unsigned>() + 1, b->err.as<int>()))
             return cuda_fail(ctx, cudaGetLastError(), "k_core_batch");
         if (ev) cudaEventRecord(ev[2], s);
     }
@@ -2522,13 +2582,14 @@ void fsg_batch_destroy(fsg_batch *b) {
 }  // extern "C"
 
 // ---- eval counting for the stats (sum over retained lines of Ntau x window) -------------------------
+// npi / nsi (may be null): Zeeman component counts; each window wavelength then counts once per component
 __global__ void k_count_evals(int64_t n, const int32_t *flags, const int32_t *il, const int32_t *ir, int i0, int i1,
-                              unsigned long long *acc) {
+                              const int32_t *npi, const int32_t *nsi, unsigned long long *acc) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long v = 0;
     if (i < n && !(flags[i] & FSG_F_WEAK)) {
         int a = max(il[i], i0), b = min(ir[i], i1);
-        if (a <= b) v = (unsigned long long)(b - a + 1);
+        if (a <= b) v = (unsigned long long)(b - a + 1) * (npi ? (unsigned long long)(npi[i] + nsi[i]) : 1ull);
     }
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     if ((threadIdx.x & 31) == 0 && v) atomicAdd(acc, v);
@@ -2539,14 +2600,14 @@ double fsg_count_evals(fsg_ctx *ctx, int64_t n, const int32_t *fl, const int32_t
     return count_windows(ctx, n, fl, il, ir, i0, i1) * ctx->ntau;
 }
 
-// retained-window wavelengths (inside [i0, i1]) of n lines
+// retained-window wavelengths (inside [i0, i1]) of n lines, times their Zeeman components when given
 static double count_windows(fsg_ctx *ctx, int64_t n, const int32_t *fl, const int32_t *il, const int32_t *ir, int i0,
-                            int i1) {
+                            int i1, const int32_t *npi, const int32_t *nsi) {
     if (ctx->d_nkeep.ensure(sizeof(unsigned long long)) != FSG_OK) return 0.0;
     ctx->launches += 1;
     unsigned long long *d = ctx->d_nkeep.as<unsigned long long>();
     cudaMemsetAsync(d, 0, sizeof(unsigned long long), ctx->stream);
-    k_count_evals<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(n, fl, il, ir, i0, i1, d);
+    k_count_evals<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(n, fl, il, ir, i0, i1, npi, nsi, d);
     unsigned long long h = 0;
     cudaMemcpyAsync(&h, d, sizeof h, cudaMemcpyDeviceToHost, ctx->stream);
     cudaStreamSynchronize(ctx->stream);

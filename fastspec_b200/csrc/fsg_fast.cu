@@ -15,10 +15,10 @@
 // tile's candidate range stays close to the lines that touch it; narrow classes use 64-wavelength
 // tiles, wide ones 128.
 //
-// Core pass (k_core_fast): over the core ranges, 32-wavelength tiles, the table lerp (|v| < 8,
-// a < 8), the two-term continued fraction (voigt.f90:103-107) or the wing form, point by point,
-// exactly as HVoigt branches.  No atomics; one read-modify-write of the FP64 LineOpac per tile and
-// launch; deterministic order.
+// Core pass (k_core_fast): over the core ranges, 32-wavelength tiles, the points where s < 196: the
+// table lerp (|v| < 8, a < 8) or the two-term continued fraction (voigt.f90:103-107), exactly as
+// HVoigt branches.  No atomics; one read-modify-write of the FP64 LineOpac per tile and launch;
+// deterministic order.
 #include "fsg_internal.cuh"
 #include "fsg_mbar.cuh"
 
@@ -47,15 +47,15 @@ __device__ __forceinline__ float hv_cf32(float av, float a, float cop) {
 // Candidate lines staged per TMA bulk copy (double-buffered)
 #define CH 32
 // cp.async.bulk moves multiples of 16 bytes between 16-byte aligned addresses
-static_assert(sizeof(WingRec) % 16 == 0 && sizeof(LineHdr) % 16 == 0, "bulk-copied records: multiples of 16 bytes");
+static_assert(sizeof(WingRec) % 16 == 0 && sizeof(LineHdr) % 16 == 0 && sizeof(CoreRec) % 16 == 0, "bulk-copied records: multiples of 16 bytes");
 
 // Issue the bulk copies of chunk c (lines lo + c*CH ...) into buffer b; one thread calls this.
 __device__ __forceinline__ void stage_chunk(int c, int lo, int hi, int ntau, const LineHdr *hdr, const WingRec *wing,
-                                            LineHdr *shdr, WingRec *swing, uint64_t *bar) {
+                                            LineHdr *shdr, WingRec *swing, uint64_t *bar, unsigned extra_tx) {
     int j0 = lo + c * CH;
     int n = min(CH, hi - j0 + 1);
     unsigned brec = (unsigned)(n * ntau * (int)sizeof(WingRec)), bhdr = (unsigned)(n * (int)sizeof(LineHdr));
-    mbar_expect_tx(bar, brec + bhdr);
+    mbar_expect_tx(bar, brec + bhdr + extra_tx);
     tma_bulk_g2s(swing, wing + (size_t)j0 * ntau, brec, bar);
     tma_bulk_g2s(shdr, hdr + j0, bhdr, bar);
 }
@@ -66,13 +66,19 @@ __device__ __forceinline__ float rcp_approx(float x) {
     return r;
 }
 
-// Wing pass.  Every window point outside the line's core range [cl, cr] has s >= 196 at every
-// depth, so there HVoigt * LinCop is the rational wing form alone:
+// Wing pass.  Every window point where fl32(t) >= 195.5 (s >= 196) takes HVoigt's rational wing
+// form:
 //   val = c1 (t + 1) / (t^2 + twoA),  t = dl^2 vv2 + c2m1
-// (three FMAs, one reciprocal, one FMA into the partial sum).  Lines whose window covers the
-// whole tile outside their core range (the common case for wide windows) skip the mask; for the others
-// the masked points get an x for which the term is exactly 0, so one body serves both.
+// (three FMAs, one reciprocal, one FMA into the partial sum).  Outside the line's core range [cl, cr]
+// that is every depth.  Lines whose window covers the whole tile outside their core range (the common
+// case for wide windows) skip the mask; for the others the points outside the window get an x for
+// which the term is exactly 0.  On tiles that meet the core range, each point whose t is below 195.5
+// (table or continued fraction, the core pass's share) has its t replaced by 1e19, whose term is
+// exactly 0 too: the two passes split the points by the same FP32 test, so each point is evaluated
+// once.
 // One wing-pass job: the line records and tiles of one LineOpac (one atmosphere and grid).
+// extra_tx / wait_ns: 0 and WAIT_NS in use; a test of the error path (fsg_set_fault) makes every
+// chunk expect extra_tx bytes more than its copies deliver and bounds the waits by wait_ns.
 struct WingJob {
     int ntau, nwl;
     const double *wave;
@@ -80,6 +86,8 @@ struct WingJob {
     const WingRec *wing;
     const int *tile_lo, *tile_hi;
     double *lineopac;
+    unsigned extra_tx;
+    unsigned long long wait_ns;
 };
 
 // shared memory of the wing pass for at most ntau_max depths:
@@ -115,7 +123,7 @@ __device__ __forceinline__ bool wing_tile(const WingJob &J, int tile, unsigned c
     if (threadIdx.x == 0) {
         for (int c = 0; c < 2 && c < nchunks; c++) {
             const int b = (kk + c) & 1;
-            stage_chunk(c, lo, hi, ntau, hdr, wing, shdr + b * CH, swing + b * CH * ntau_max, &bars[b]);
+            stage_chunk(c, lo, hi, ntau, hdr, wing, shdr + b * CH, swing + b * CH * ntau_max, &bars[b], J.extra_tx);
         }
     }
     // wavelength offsets as FP32 hi + lo: dl = (wvh - wlh) + (wvl - wll) keeps dl to FP32 relative
@@ -143,7 +151,7 @@ __device__ __forceinline__ bool wing_tile(const WingJob &J, int tile, unsigned c
     for (int c = 0; c < nchunks; c++) {
         const unsigned g = kk + c;
         const int b = g & 1;
-        const bool ok = mbar_wait(&bars[b], (g >> 1) & 1);
+        const bool ok = mbar_wait(&bars[b], (g >> 1) & 1, J.wait_ns);
         if (__syncthreads_or(!ok)) { failed = c; break; }
         const LineHdr *ch = shdr + b * CH;
         const WingRec *cw = swing + b * CH * ntau_max;
@@ -161,28 +169,41 @@ __device__ __forceinline__ bool wing_tile(const WingJob &J, int tile, unsigned c
                 WingRec w[D];
 #pragma unroll
                 for (int d = 0; d < D; d++) w[d] = cw[q * ntau + t0 + min(d, nd - 1)];
-                const bool full = h.ileft <= tile_first && h.iright >= tile_last &&
-                                  (h.cr < tile_first || h.cl > tile_last);
+                const bool core_hit = h.cl <= h.cr && h.cr >= tile_first && h.cl <= tile_last;
+                const bool full = h.ileft <= tile_first && h.iright >= tile_last && !core_hit;
                 if (!full) {
-                    // points outside the window or inside the core range take the header's offset x,
-                    // for which the wing term is exactly 0: one body serves every tile
+                    // points outside the window take the header's offset x, for which the wing term is
+                    // exactly 0
                     const float xm = __int_as_float(h.pad0);
 #pragma unroll
                     for (int k = 0; k < P; k++) {
                         const int p1 = pix[k] + 1;
-                        const bool in = p1 >= h.ileft && p1 <= h.iright && (p1 < h.cl || p1 > h.cr);
+                        const bool in = p1 >= h.ileft && p1 <= h.iright;
                         x[k] = in ? x[k] : xm;
                     }
                 }
+                if (!core_hit) {
 #pragma unroll
-                for (int d = 0; d < D; d++)
+                    for (int d = 0; d < D; d++)
 #pragma unroll
-                    for (int k = 0; k < P; k++) {
-                        float t = fmaf(x[k], w[d].vv2, w[d].c2m1);
-                        float den = fmaf(t, t, w[d].twoA);
-                        float num = fmaf(w[d].c1, t, w[d].c1);
-                        part[d][k] = fmaf(num, rcp_approx(den), part[d][k]);
-                    }
+                        for (int k = 0; k < P; k++) {
+                            float t = fmaf(x[k], w[d].vv2, w[d].c2m1);
+                            float den = fmaf(t, t, w[d].twoA);
+                            float num = fmaf(w[d].c1, t, w[d].c1);
+                            part[d][k] = fmaf(num, rcp_approx(den), part[d][k]);
+                        }
+                } else {
+#pragma unroll
+                    for (int d = 0; d < D; d++)
+#pragma unroll
+                        for (int k = 0; k < P; k++) {
+                            float t = fmaf(x[k], w[d].vv2, w[d].c2m1);
+                            t = t < 195.5f ? 1.0e19f : t;        // the core pass's point
+                            float den = fmaf(t, t, w[d].twoA);
+                            float num = fmaf(w[d].c1, t, w[d].c1);
+                            part[d][k] = fmaf(num, rcp_approx(den), part[d][k]);
+                        }
+                }
                 if (++nfold == FOLD) {
                     nfold = 0;
 #pragma unroll
@@ -200,7 +221,8 @@ __device__ __forceinline__ bool wing_tile(const WingJob &J, int tile, unsigned c
         }
         __syncthreads();                                   // every warp is done with buffer b
         if (threadIdx.x == 0 && c + 2 < nchunks)
-            stage_chunk(c + 2, lo, hi, ntau, hdr, wing, shdr + b * CH, swing + b * CH * ntau_max, &bars[b]);
+            stage_chunk(c + 2, lo, hi, ntau, hdr, wing, shdr + b * CH, swing + b * CH * ntau_max, &bars[b],
+                        J.extra_tx);
     }
     if (failed >= 0) {
         // a copy never completed: report, then wait (bounded) for the copies still in flight,
@@ -209,7 +231,7 @@ __device__ __forceinline__ bool wing_tile(const WingJob &J, int tile, unsigned c
             atomicExch(err, FSG_E_TIMEOUT);
             for (int c = failed; c < nchunks && c < failed + 2; c++) {
                 const unsigned g = kk + c;
-                mbar_wait(&bars[g & 1], (g >> 1) & 1);
+                mbar_wait(&bars[g & 1], (g >> 1) & 1, J.wait_ns);
             }
         }
         __syncthreads();
@@ -300,7 +322,8 @@ size_t fsg_wing_smem(int P, int ntau_max) {
     } while (0)
 
 int fsg_launch_accum_fast(cudaStream_t st, int cls, int ntau, int nwl, const double *wave, const LineHdr *hdr,
-                          const WingRec *wing, const int *tile_lo, const int *tile_hi, double *lineopac, int *err) {
+                          const WingRec *wing, const int *tile_lo, const int *tile_hi, double *lineopac, int *err,
+                          unsigned extra_tx, unsigned long long wait_ns) {
     const int P = fsg_class_pix(cls);
     const int TW = 32 * P;
     const int ntiles = (nwl + TW - 1) / TW;
@@ -308,7 +331,7 @@ int fsg_launch_accum_fast(cudaStream_t st, int cls, int ntau, int nwl, const dou
     const int nwarps = (ntau + D - 1) / D;
     const size_t smem = fsg_wing_smem(P, ntau);
     if (smem > 200 * 1024) return FSG_E_ARG;
-    WingJob J{ ntau, nwl, wave, hdr, wing, tile_lo, tile_hi, lineopac };
+    WingJob J{ ntau, nwl, wave, hdr, wing, tile_lo, tile_hi, lineopac, extra_tx, wait_ns };
 #define LAUNCH(DD, PP) do { \
         cudaFuncSetAttribute(k_accum_fast<DD, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
         k_accum_fast<DD, PP><<<ntiles, 32 * nwarps, smem, st>>>(J, err); } while (0)
@@ -332,30 +355,19 @@ int fsg_launch_accum_batch(cudaStream_t st, int P, int ntau_max, const WingJob *
     return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
 }
 
-// Core pass.  Over each line's core range [cl, cr] the full HVoigt branch structure runs point by
-// point: the table lerp or the continued fraction where fl32(t) < 195.5 (s < 196), the wing form
-// elsewhere.  A CTA owns 32 wavelengths x all depths, warp w depths [w*CORE_D, w*CORE_D + CORE_D),
-// lane l wavelength tile0 + l; Kahan sums in registers.  The four table entries of a lerp come in
-// one 16-byte load from the cell-major copy of VgtTab.
-#define CORE_D 4
+// Core pass.  Over each line's core range [cl, cr], the points where fl32(t) < 195.5 (s < 196): the
+// table lerp or the continued fraction, as HVoigt branches (voigt.f90:81-107); the wing pass takes the
+// others (the same FP32 test splits the points, so each is evaluated once).  A CTA owns 32 wavelengths
+// x all depths: warp w depths [w*D, w*D + D), lane l wavelength tile0 + l, Kahan sums in
+// registers.  Headers, wing records and core records of the tile's candidate lines arrive in shared
+// memory CHC lines at a time by double-buffered bulk copies completing on mbarriers (waits bounded;
+// on expiry the kernel reports FSG_E_TIMEOUT and drains its copies), so the loop over lines reads
+// shared memory; per line a thread forms its depths' branch predicates first and issues their table
+// gathers (one 16-byte load of the cell-major VgtTab copy each) together.  D = 4 depths per warp up to
+// 72 depths, 8 beyond (18 warps at most).
 
-// HVoigt * LinCop where s < 196 (voigt.f90:81-107): the table lerp for a < 8 and v < 8, else the
-// continued fraction.  v = adl * LinVvgt, the table column iv and its fraction tv in FP64 as the
-// reference forms them; the lerp itself in FP32 on the FP32 table.
-__device__ __forceinline__ float hv_core32(const float4 *__restrict__ vtab4, double adl, const CoreRec &c) {
-    const double av = adl * c.vv;
-    if (c.ia > 0 && av < 8.0) {
-        const double fv = av * 125.0;
-        const int iv = min((int)fv, FSG_NVV - 1);
-        const float tv = (float)(fv - (double)iv);
-        const float4 g = __ldg(vtab4 + (c.ia - 1) * FSG_NV1 + iv);
-        const float c0 = g.x + tv * (g.y - g.x), c1 = g.z + tv * (g.w - g.z);
-        return (c0 + c.ua * (c1 - c0)) * c.cop;
-    }
-    return hv_cf32((float)av, c.a, c.cop);
-}
-
-// One core-pass job: as WingJob plus the core records; tiles of 32 wavelengths
+// One core-pass job: as WingJob plus the core records; tiles of 32 wavelengths.  nevals (may be null)
+// counts the evaluations.
 struct CoreJob {
     int ntau, nwl;
     const double *wave;
@@ -364,66 +376,183 @@ struct CoreJob {
     const CoreRec *core;
     const int *tile_lo, *tile_hi;
     double *lineopac;
+    unsigned long long *nevals;
+    unsigned extra_tx;
+    unsigned long long wait_ns;
 };
 
-__device__ __forceinline__ void core_tile(const CoreJob &J, int tile, const float4 *__restrict__ vtab4) {
+// shared memory of the core pass for at most ntau_max depths and chc lines per chunk:
+// wing records [2][chc][ntau_max] | core records [2][chc][ntau_max] | headers [2][chc] | mbarriers [2]
+__host__ __device__ inline size_t core_smem(int ntau_max, int chc) {
+    return (sizeof(WingRec) + sizeof(CoreRec)) * 2 * (size_t)chc * ntau_max + sizeof(LineHdr) * 2 * (size_t)chc +
+           2 * sizeof(uint64_t);
+}
+
+__device__ __forceinline__ void core_stage(int c, int lo, int hi, int ntau, int chc, const CoreJob &J,
+                                           WingRec *sw, CoreRec *sc, LineHdr *sh, uint64_t *bar) {
+    const int j0 = lo + c * chc;
+    const int n = min(chc, hi - j0 + 1);
+    const unsigned bw = (unsigned)(n * ntau * (int)sizeof(WingRec)), bc = (unsigned)(n * ntau * (int)sizeof(CoreRec));
+    const unsigned bh = (unsigned)(n * (int)sizeof(LineHdr));
+    mbar_expect_tx(bar, bw + bc + bh + J.extra_tx);
+    tma_bulk_g2s(sw, J.wing + (size_t)j0 * ntau, bw, bar);
+    tma_bulk_g2s(sc, J.core + (size_t)j0 * ntau, bc, bar);
+    tma_bulk_g2s(sh, J.hdr + j0, bh, bar);
+}
+
+// One tile of one job, called by every thread of the CTA with the mbarriers initialised; kk counts
+// the chunks the CTA has consumed (their buffer and phase parity) across tiles.  Returns false after a
+// copy did not complete within its bound (error in *err).
+template <int D>
+__device__ bool core_tile(const CoreJob &J, int tile, const float4 *__restrict__ vtab4, unsigned char *smem_raw,
+                          int ntau_max, int chc, unsigned &kk, int *err) {
     const int ntau = J.ntau, nwl = J.nwl;
     const int lo = J.tile_lo[tile], hi = J.tile_hi[tile];
-    if (lo > hi) return;
+    if (lo > hi) return true;
+    WingRec *sw = (WingRec *)smem_raw;
+    CoreRec *sc = (CoreRec *)(sw + 2 * (size_t)chc * ntau_max);
+    LineHdr *sh = (LineHdr *)(sc + 2 * (size_t)chc * ntau_max);
+    uint64_t *bars = (uint64_t *)(sh + 2 * chc);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int t0 = warp * CORE_D;
-    const int nd = min(CORE_D, ntau - t0);
-    if (nd <= 0) return;                                 // no barrier below: warps may leave early
+    const int t0 = warp * D;
+    const int nd = max(0, min(D, ntau - t0));      // warps past the last depth only wait with the others
     const int p = tile * 32 + lane, p1 = p + 1;
     const int tile_first = tile * 32 + 1, tile_last = min(tile * 32 + 32, nwl);
+    const int nchunks = (hi - lo + chc) / chc;
+    if (threadIdx.x == 0)
+        for (int c = 0; c < 2 && c < nchunks; c++) {
+            const int b = (kk + c) & 1;
+            core_stage(c, lo, hi, ntau, chc, J, sw + (size_t)b * chc * ntau_max, sc + (size_t)b * chc * ntau_max,
+                       sh + b * chc, &bars[b]);
+        }
     const double wd = J.wave[min(p, nwl - 1)];
     const float wvh = (float)wd, wvl = (float)(wd - (double)wvh);
-    float sum[CORE_D], cmp[CORE_D];
+    float sum[D], cmp[D];
 #pragma unroll
-    for (int d = 0; d < CORE_D; d++) { sum[d] = 0.0f; cmp[d] = 0.0f; }
-    for (int j = lo; j <= hi; j++) {
-        const LineHdr h = J.hdr[j];
-        if (h.cr < tile_first || h.cl > tile_last) continue;          // core range misses the tile
-        if (p1 < h.cl || p1 > h.cr) continue;
-        const float dl = (wvh - h.wlh) + (wvl - h.wll);
-        const float x = dl * dl;                          // the wing pass's x: the same branch split
-        const double adl = fabs(wd - ((double)h.wlh + (double)h.wll));
-        const WingRec *wr = J.wing + (size_t)j * ntau + t0;
-        const CoreRec *cr = J.core + (size_t)j * ntau + t0;
+    for (int d = 0; d < D; d++) { sum[d] = 0.0f; cmp[d] = 0.0f; }
+    unsigned cnt = 0;
+    int failed = -1;
+    for (int c = 0; c < nchunks; c++) {
+        const unsigned g = kk + c;
+        const int b = g & 1;
+        const bool ok = mbar_wait(&bars[b], (g >> 1) & 1, J.wait_ns);
+        if (__syncthreads_or(!ok)) { failed = c; break; }
+        const LineHdr *ch = sh + b * chc;
+        const WingRec *cw = sw + (size_t)b * chc * ntau_max;
+        const CoreRec *cc = sc + (size_t)b * chc * ntau_max;
+        const int n = min(chc, hi - (lo + c * chc) + 1);
+        if (nd > 0) {
+            for (int q = 0; q < n; q++) {
+                const LineHdr h = ch[q];
+                if (h.cr < tile_first || h.cl > tile_last) continue;          // core range misses the tile
+                const bool in = p1 >= h.cl && p1 <= h.cr;
+                if (!__any_sync(0xffffffffu, in)) continue;
+                const float dl = (wvh - h.wlh) + (wvl - h.wll);
+                const float x = dl * dl;                  // the wing pass's x: the same branch split
+                const double adl = fabs(wd - ((double)h.wlh + (double)h.wll));
 #pragma unroll
-        for (int d = 0; d < CORE_D; d++) {
-            if (d < nd) {
-                const WingRec w = wr[d];
-                const CoreRec c = cr[d];                  // loaded with w: a broadcast, off the branch's path
-                const float t = fmaf(x, w.vv2, w.c2m1);
-                float v;
-                if (t < 195.5f) {
-                    v = hv_core32(vtab4, adl, c);
-                } else {
-                    v = fmaf(w.c1, t, w.c1) * rcp_approx(fmaf(t, t, w.twoA));
+                for (int g0 = 0; g0 < D; g0 += 4) {               // depths in groups of four
+                    bool core[4], tab[4];
+                    float tv[4];
+                    int cell[4];
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        const int d = g0 + e;
+                        const int td = t0 + min(d, nd - 1);
+                        const WingRec w = cw[q * ntau + td];
+                        const CoreRec cr = cc[q * ntau + td];
+                        const float t = fmaf(x, w.vv2, w.c2m1);
+                        core[e] = in && d < nd && t < 195.5f;
+                        const double av = adl * cr.vv;
+                        tab[e] = core[e] && cr.ia > 0 && av < 8.0;
+                        const double fv = av * 125.0;
+                        const int iv = tab[e] ? min((int)fv, FSG_NVV - 1) : 0;
+                        tv[e] = tab[e] ? (float)(fv - (double)iv) : (float)av;   // CF: |v| in FP32
+                        cell[e] = tab[e] ? (cr.ia - 1) * FSG_NV1 + iv : 0;
+                    }
+                    float4 gv[4];
+#pragma unroll
+                    for (int e = 0; e < 4; e++)
+                        if (tab[e]) gv[e] = __ldg(vtab4 + cell[e]);
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        if (!core[e]) continue;
+                        const int d = g0 + e;
+                        const CoreRec &cr = cc[q * ntau + t0 + d];
+                        float v;
+                        if (tab[e]) {
+                            const float4 gg = gv[e];
+                            const float c0 = gg.x + tv[e] * (gg.y - gg.x), c1 = gg.z + tv[e] * (gg.w - gg.z);
+                            v = (c0 + cr.ua * (c1 - c0)) * cr.cop;
+                        } else {
+                            v = hv_cf32(tv[e], cr.a, cr.cop);
+                        }
+                        KAHAN(sum[d], cmp[d], v);
+                        cnt++;
+                    }
                 }
-                KAHAN(sum[d], cmp[d], v);
             }
         }
+        __syncthreads();                                   // every warp is done with buffer b
+        if (threadIdx.x == 0 && c + 2 < nchunks)
+            core_stage(c + 2, lo, hi, ntau, chc, J, sw + (size_t)b * chc * ntau_max, sc + (size_t)b * chc * ntau_max,
+                       sh + b * chc, &bars[b]);
     }
-    if (p >= nwl) return;
+    if (failed >= 0) {
+        if (threadIdx.x == 0) {
+            atomicExch(err, FSG_E_TIMEOUT);
+            for (int c = failed; c < nchunks && c < failed + 2; c++) {
+                const unsigned g = kk + c;
+                mbar_wait(&bars[g & 1], (g >> 1) & 1, J.wait_ns);
+            }
+        }
+        __syncthreads();
+        return false;
+    }
+    kk += nchunks;
+    if (J.nevals) {
+        unsigned long long v = cnt;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0 && v) atomicAdd(J.nevals, v);
+    }
+    if (nd <= 0 || p >= nwl) return true;
     double *dst = J.lineopac + (size_t)p * ntau + t0;
 #pragma unroll
-    for (int d = 0; d < CORE_D; d++)
+    for (int d = 0; d < D; d++)
         if (d < nd) dst[d] = dst[d] + ((double)sum[d] - (double)cmp[d]);
+    return true;
 }
 
-__global__ void __launch_bounds__(1024)
-k_core_fast(CoreJob J, const float4 *__restrict__ vtab4) {
-    core_tile(J, blockIdx.x, vtab4);
+__device__ __forceinline__ void core_bars_init(unsigned char *smem_raw, int ntau_max, int chc) {
+    uint64_t *bars = (uint64_t *)(smem_raw + core_smem(ntau_max, chc) - 2 * sizeof(uint64_t));
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
 }
 
-// persistent form: each warp takes (job, tile) items from the queue and does its depths of them;
-// a CTA of nwarps warps covers nwarps * CORE_D depths, so every item is taken by whole CTAs
-__global__ void __launch_bounds__(1024)
-k_core_batch(const CoreJob *__restrict__ jobs, const int *__restrict__ tile0, int njobs,
-             const float4 *__restrict__ vtab4, unsigned *queue) {
+template <int D>
+__global__ void __launch_bounds__(32 * 18, D == 4 ? 2 : 1)
+k_core_fast(CoreJob J, const float4 *__restrict__ vtab4, int chc, int *__restrict__ err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    if (J.tile_lo[blockIdx.x] > J.tile_hi[blockIdx.x]) return;
+    core_bars_init(smem_raw, J.ntau, chc);
+    unsigned kk = 0;
+    core_tile<D>(J, blockIdx.x, vtab4, smem_raw, J.ntau, chc, kk, err);
+}
+
+// persistent form: CTAs take (job, tile) items from the queue; a CTA of nwarps warps covers
+// nwarps * D depths, so every item is taken by whole CTAs
+template <int D>
+__global__ void __launch_bounds__(32 * 18, D == 4 ? 2 : 1)
+k_core_batch(const CoreJob *__restrict__ jobs, const int *__restrict__ tile0, int njobs, int ntau_max, int chc,
+             const float4 *__restrict__ vtab4, unsigned *queue, int *__restrict__ err) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ int s_item;
+    core_bars_init(smem_raw, ntau_max, chc);
+    unsigned kk = 0;
     const int total = tile0[njobs];
     for (;;) {
         if (threadIdx.x == 0) s_item = (int)atomicAdd(queue, 1u);
@@ -433,24 +562,51 @@ k_core_batch(const CoreJob *__restrict__ jobs, const int *__restrict__ tile0, in
         if (item >= total) break;
         int a = 0, b = njobs - 1;
         while (a < b) { int m = (a + b + 1) >> 1; if (tile0[m] <= item) a = m; else b = m - 1; }
-        core_tile(jobs[a], item - tile0[a], vtab4);
+        if (!core_tile<D>(jobs[a], item - tile0[a], vtab4, smem_raw, ntau_max, chc, kk, err)) break;
     }
 }
 
+// lines per staged chunk: about 48 KB of records per buffer (two CTAs per SM), 4 to 16 lines
+static int core_chunk(int ntau_max) {
+    const int per_line = ntau_max * (int)(sizeof(WingRec) + sizeof(CoreRec)) + (int)sizeof(LineHdr);
+    return std::max(4, std::min(16, (48 * 1024) / per_line));
+}
+
+static int core_depths(int ntau_max) { return ntau_max <= 72 ? 4 : 8; }
+
 int fsg_launch_core_fast(cudaStream_t st, int ntau, int nwl, const double *wave, const LineHdr *hdr,
                          const WingRec *wing, const CoreRec *core, const int *tile_lo, const int *tile_hi,
-                         const float4 *vtab4, double *lineopac) {
+                         const float4 *vtab4, double *lineopac, unsigned long long *nevals, int *err,
+                         unsigned extra_tx, unsigned long long wait_ns) {
     const int ntiles = (nwl + 31) / 32;
-    const int nwarps = (ntau + CORE_D - 1) / CORE_D;     // ntau <= 128: at most 32 warps
-    CoreJob J{ ntau, nwl, wave, hdr, wing, core, tile_lo, tile_hi, lineopac };
-    k_core_fast<<<ntiles, 32 * nwarps, 0, st>>>(J, vtab4);
+    const int D = core_depths(ntau), nwarps = (ntau + D - 1) / D;
+    if (nwarps > 18) return FSG_E_ARG;
+    const int chc = core_chunk(ntau);
+    const size_t smem = core_smem(ntau, chc);
+    CoreJob J{ ntau, nwl, wave, hdr, wing, core, tile_lo, tile_hi, lineopac, nevals, extra_tx, wait_ns };
+    if (D == 4) {
+        cudaFuncSetAttribute(k_core_fast<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_core_fast<4><<<ntiles, 32 * nwarps, smem, st>>>(J, vtab4, chc, err);
+    } else {
+        cudaFuncSetAttribute(k_core_fast<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_core_fast<8><<<ntiles, 32 * nwarps, smem, st>>>(J, vtab4, chc, err);
+    }
     return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
 }
 
 int fsg_launch_core_batch(cudaStream_t st, int ntau_max, const CoreJob *jobs, const int *tile0, int njobs,
-                          int ctas, const float4 *vtab4, unsigned *queue) {
-    const int nwarps = (ntau_max + CORE_D - 1) / CORE_D;
-    k_core_batch<<<ctas, 32 * nwarps, 0, st>>>(jobs, tile0, njobs, vtab4, queue);
+                          int ctas, const float4 *vtab4, unsigned *queue, int *err) {
+    const int D = core_depths(ntau_max), nwarps = (ntau_max + D - 1) / D;
+    if (nwarps > 18) return FSG_E_ARG;
+    const int chc = core_chunk(ntau_max);
+    const size_t smem = core_smem(ntau_max, chc);
+    if (D == 4) {
+        cudaFuncSetAttribute(k_core_batch<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_core_batch<4><<<ctas, 32 * nwarps, smem, st>>>(jobs, tile0, njobs, ntau_max, chc, vtab4, queue, err);
+    } else {
+        cudaFuncSetAttribute(k_core_batch<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_core_batch<8><<<ctas, 32 * nwarps, smem, st>>>(jobs, tile0, njobs, ntau_max, chc, vtab4, queue, err);
+    }
     return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
 }
 
@@ -532,19 +688,6 @@ int fsg_launch_tile_span_tw(cudaStream_t s, int tw, int use_core, int nwl, int64
     if (cub::DeviceScan::InclusiveScan(tmp, tb, revl, V, cub::Min(), (int)nb, s) != cudaSuccess) return FSG_E_CUDA;
     k_tile_search<<<(ntiles + 255) / 256, 256, 0, s>>>((int)nb, ntiles, tw, nwl, R, V, lo, hi);
     return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
-}
-
-// wavelengths inside the core ranges of a block's lines (the core pass's evaluations / ntau)
-__global__ void k_count_core(int64_t nb, const LineHdr *hdr, unsigned long long *acc) {
-    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    unsigned long long v = 0;
-    if (j < nb) { LineHdr h = hdr[j]; if (h.cl <= h.cr) v = (unsigned long long)(h.cr - h.cl + 1); }
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0 && v) atomicAdd(acc, v);
-}
-
-void fsg_launch_count_core(cudaStream_t s, int64_t nb, const LineHdr *hdr, unsigned long long *acc) {
-    if (nb > 0) k_count_core<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>(nb, hdr, acc);
 }
 
 // Restriction to the wavelength range [i0, i1]: lines whose window misses it are marked weak for the

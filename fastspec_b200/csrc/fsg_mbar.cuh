@@ -24,8 +24,9 @@ __device__ __forceinline__ void tma_bulk_g2s(void *dst, const void *src, unsigne
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                  :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
 }
-// bounded wait for the phase with the given parity; false when the bound was reached
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+// bounded wait for the phase with the given parity; false when the bound (bound_ns of %globaltimer, or
+// WAIT_POLLS polls) was reached
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity, unsigned long long bound_ns = WAIT_NS) {
     const unsigned a = smem_u32(bar);
     uint64_t start = 0;
     for (unsigned it = 0; it < WAIT_POLLS; it++) {
@@ -36,7 +37,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
         if ((it & 255u) == 0) {
             uint64_t now = global_ns();
             if (it == 0) start = now;
-            else if (now - start > WAIT_NS) return false;
+            else if (now - start > bound_ns) return false;
         }
     }
     return false;

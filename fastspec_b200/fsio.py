@@ -18,13 +18,27 @@ SpL -> [nwl][nmu], SpZ -> [nwl][4][nmu].
 import numpy as np
 
 
+class FsioError(ValueError):
+    """A file that is truncated or does not have the layout of the output it should hold."""
+
+
+def _take(f, path, dtype, count, what):
+    """Exactly count values of dtype from f, or FsioError naming the file and the field."""
+    if count < 0:
+        raise FsioError("%s: negative %s count %d (not a FastSpec output file?)" % (path, what, count))
+    a = np.fromfile(f, dtype, count)
+    if a.size != count:
+        raise FsioError("%s: truncated: %s needs %d values, the file holds %d" % (path, what, count, a.size))
+    return a
+
+
 def read_opac(path):
     """fs_lineop.bin / fs_contop.bin -> dict(wave, opac [nwl][ntau], rhox, T, xne, xna, rho)."""
     with open(path, "rb") as f:
-        nwl, ntau = (int(x) for x in np.fromfile(f, "<i4", 2))
-        wave = np.fromfile(f, "<f8", nwl)
-        opac = np.fromfile(f, "<f8", nwl * ntau).reshape(nwl, ntau)
-        atm = np.fromfile(f, "<f8", 5 * ntau).reshape(5, ntau)
+        nwl, ntau = (int(x) for x in _take(f, path, "<i4", 2, "header"))
+        wave = _take(f, path, "<f8", nwl, "wavelengths")
+        opac = _take(f, path, "<f8", nwl * ntau, "opacities").reshape(nwl, ntau)
+        atm = _take(f, path, "<f8", 5 * ntau, "atmosphere").reshape(5, ntau)
     return dict(wave=wave, opac=opac, rhox=atm[0], T=atm[1], xne=atm[2], xna=atm[3], rho=atm[4])
 
 
@@ -42,11 +56,13 @@ def write_opac(path, wave, opac, rhox, T, xne, xna, rho):
 def read_spec(path):
     """fs_spec.bin -> dict(wave, xmu, spl [nwl][nmu], spc [nwl][nmu], magnetic, spz [nwl][4][nmu])."""
     with open(path, "rb") as f:
-        nwl, nmu = (int(x) for x in np.fromfile(f, "<i4", 2))
-        xmu = np.fromfile(f, "<f8", nmu)
-        wave = np.fromfile(f, "<f8", nwl)
+        nwl, nmu = (int(x) for x in _take(f, path, "<i4", 2, "header"))
+        xmu = _take(f, path, "<f8", nmu, "angles")
+        wave = _take(f, path, "<f8", nwl, "wavelengths")
         rest = np.fromfile(f, "<f8")
-    narr = rest.size // (nwl * nmu)
+    narr = rest.size // max(nwl * nmu, 1)
+    if narr not in (2, 5) or rest.size != narr * nwl * nmu:
+        raise FsioError("%s: truncated: %d intensity values, not 2 or 5 arrays of %d x %d" % (path, rest.size, nwl, nmu))
     sp = rest.reshape(narr, nwl, nmu)
     out = dict(wave=wave, xmu=xmu, spl=sp[0], spc=sp[1], magnetic=(narr == 5))
     if narr == 5:
@@ -102,10 +118,10 @@ def spec_grid(spec):
 
 def read_flux(path):
     with open(path, "rb") as f:
-        nwl = int(np.fromfile(f, "<i4", 1)[0])
-        wave = np.fromfile(f, "<f8", nwl)
-        sfl = np.fromfile(f, "<f8", nwl)
-        sfc = np.fromfile(f, "<f8", nwl)
+        nwl = int(_take(f, path, "<i4", 1, "header")[0])
+        wave = _take(f, path, "<f8", nwl, "wavelengths")
+        sfl = _take(f, path, "<f8", nwl, "line flux")
+        sfc = _take(f, path, "<f8", nwl, "continuum flux")
     return dict(wave=wave, sfl=sfl, sfc=sfc)
 
 
@@ -127,10 +143,10 @@ def read_linst(path):
                 break
             n = int(n[0])
             nrec.append(n)
-            species.append(np.char.strip(np.fromfile(f, "S8", n).astype("U8")))
-            ion.append(np.fromfile(f, "<i4", n))
-            wave.append(np.fromfile(f, "<f8", n))
-            strength.append(np.fromfile(f, "<f4", n))
+            species.append(np.char.strip(_take(f, path, "S8", n, "species").astype("U8")))
+            ion.append(_take(f, path, "<i4", n, "ions"))
+            wave.append(_take(f, path, "<f8", n, "wavelengths"))
+            strength.append(_take(f, path, "<f4", n, "line strengths"))
     cat = lambda x, d: np.concatenate(x) if x else np.zeros(0, d)
     return dict(species=cat(species, "U8"), ion=cat(ion, "<i4"), wave=cat(wave, "<f8"),
                 strength=cat(strength, "<f4"), nrec=np.array(nrec, np.int64))

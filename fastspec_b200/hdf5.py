@@ -293,7 +293,17 @@ class _Reader:
 
 def read_lines(path):
     """(columns, attributes, units) of the /Lines group of a FastSpec HDF5 line list: numpy arrays by
-    column name (EL decoded to str), the group attributes, and each column's UNIT attribute."""
+    column name (EL decoded to str), the group attributes, and each column's UNIT attribute.  A file
+    cut short, or with damaged structures, raises HDF5Error."""
+    try:
+        return _read_lines(path)
+    except HDF5Error:
+        raise
+    except (struct.error, IndexError, zlib.error, ValueError, KeyError) as e:
+        raise HDF5Error("%s: truncated or damaged HDF5 file (%s: %s)" % (path, type(e).__name__, e)) from None
+
+
+def _read_lines(path):
     r = _Reader(path)
     top = r.group(r.root["header"])
     if "Lines" not in top:

@@ -14,6 +14,16 @@ and RadTranCalc, synth.f90:1825-1866, are independent per wavelength once the wi
    formal solver and the flux quadrature there;
 5. the flux slices are gathered to every rank.
 
+The gradient of a loss of the flux splits the same way (`adjoint`): rank r runs the adjoint over its
+range with the gathered windows (fsg_adjoint_range_dev: each line's sums over the part of its window
+inside the range), and one all-reduce sums the per-line dL/d ln gf and vmicro shares over the ranks.
+The adjoint is linear in dL/dflux and the ranges cover each window point once, so the sum is the
+whole-grid gradient.
+
+Between steps, `check_peers` is a heartbeat through the process group's store: every rank posts the
+step number and waits, with a bound, for the others'; a rank that has left is reported (PeerLost)
+before any collective of the next step is started, so no collective waits on it.
+
 The arithmetic of each wavelength is the one of a single-GPU run; only which GPU does it changes.
 The work is done by a backend: `GpuBackend` drives the CUDA library through its device entry
 points (fsg_central_dev, fsg_accumulate_dev, fsg_radtran_dev).
@@ -29,6 +39,35 @@ import ctypes as C
 import numpy as np
 import torch
 import torch.distributed as dist
+
+
+class PeerLost(RuntimeError):
+    """Ranks of the group that did not reach a step (they left or hang)."""
+
+    def __init__(self, step, ranks):
+        super().__init__("ranks %s did not reach step %d" % (list(ranks), step))
+        self.step, self.ranks = step, list(ranks)
+
+
+def check_peers(step, timeout_s=10.0, group=None):
+    """Heartbeat before `step`: post this rank's arrival in the process group's store and wait at most
+    timeout_s for every other rank's; raises PeerLost naming the ranks that did not arrive."""
+    import datetime
+    store = dist.distributed_c10d._get_default_store()
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    store.set("fsg_step%d_rank%d" % (step, rank), "1")
+    missing = []
+    deadline = datetime.timedelta(seconds=float(timeout_s))
+    for r in range(world):
+        if r == rank:
+            continue
+        try:
+            store.wait(["fsg_step%d_rank%d" % (step, r)], deadline)
+        except Exception:
+            missing.append(r)
+            deadline = datetime.timedelta(seconds=0.1)    # the bound is spent: poll the rest
+    if missing:
+        raise PeerLost(step, missing)
 
 
 def line_slice(n, world, rank):
@@ -98,6 +137,22 @@ def run(backend, group=None):
     return dict(flux=flux, ranges=ranges, range=(i0, i1), stats=stats, windows=win)
 
 
+def adjoint(backend, res, gflux, group=None):
+    """The wavelength-sharded gradient after `run`: gflux = dL/d(line flux) on the whole grid (each rank
+    needs only its range's entries).  Returns (dL/d ln gf per line [n], dL/dvmicro per line [n]) summed
+    over the ranks, on every rank."""
+    i0, i1 = res["range"]
+    n = backend.n
+    if i0 <= i1:
+        glin, gvm = backend.adjoint(res["windows"], i0, i1, gflux)
+    else:
+        glin = torch.zeros(n, dtype=torch.float64, device=res["windows"].device)
+        gvm = torch.zeros_like(glin)
+    buf = torch.cat([glin, gvm])
+    dist.all_reduce(buf, group=group)
+    return buf[:n], buf[n:]
+
+
 class GpuBackend:
     """The CUDA library as the backend of `run`: a Context with grid, atmosphere, continuum and mu
     set, and the device copy of the whole line list (dict of torch tensors wl, elo, gf, grad, gqst,
@@ -144,6 +199,18 @@ class GpuBackend:
     def flux(self, i0, i1):
         self.C.radtran_range_dev(i0, i1, None, None, self.sfl.data_ptr(), self.sfc.data_ptr())
         return torch.stack([self.sfl[i0 - 1:i1], self.sfc[i0 - 1:i1]])
+
+    def adjoint(self, win, i0, i1, gflux):
+        """This rank's share of the gradient: fsg_adjoint_range_dev over [i0, i1] with the whole list's
+        windows; gflux: dL/d(line flux) [nwl] (float64, this device)."""
+        win = win.contiguous()
+        g = gflux.to(self.dev, torch.float64).contiguous()
+        glin = torch.empty(self.n, dtype=torch.float64, device=self.dev)
+        gvm = torch.empty_like(glin)
+        torch.cuda.current_stream(self.dev).synchronize()
+        self.C.adjoint_range_dev(self.full, win[0].data_ptr(), win[1].data_ptr(), win[2].data_ptr(), i0, i1,
+                                 g.data_ptr(), glin.data_ptr(), gvm.data_ptr())
+        return glin, gvm
 
 
 # ---- batch axis ------------------------------------------------------------------------------

@@ -75,12 +75,14 @@ typedef struct {
 
 typedef struct {
     int64_t nlines_in, nlines_used, nwide, nweak, nblocks;
-    double  line_evals;     /* profile evaluations inside windows (x components if magnetic) */
+    double  line_evals;     /* profile evaluations inside windows: Ntau x the retained lines' window
+                               wavelengths (x each line's Zeeman components if magnetic), in both
+                               precisions */
     double  ms_center, ms_params, ms_accum, ms_total;   /* device time per stage [ms] */
     int64_t accum_launches; /* launches of the accumulation kernel */
     double  ms_accum_kernels;   /* summed device time of those launches [ms] */
     double  ms_wing_kernels, ms_core_kernels;   /* mixed path: the wing and core passes of it [ms] */
-    double  core_evals;     /* mixed path: evaluations inside the lines' core ranges (core pass) */
+    double  core_evals;     /* mixed path: the core pass's evaluations (table and continued fraction, s < 196) */
 } fsg_stats;
 
 /* ---- context ------------------------------------------------------------------------- */
@@ -313,6 +315,25 @@ int fsg_set_vmicro(fsg_ctx *ctx, double vmicro);
 int fsg_set_fractionpf(fsg_ctx *ctx, const float *fractionpf);
 int fsg_adjoint_dev(fsg_ctx *ctx, const fsg_lines *d_lines, const double *d_gflux, double *d_gkappa,
                     double *d_glin, double *d_gvmic);
+/* The same for one wavelength shard: the windows of the whole list are given (the sharded forward's
+ * gathered LinFlag / Ileft / Iright), and each line's sums run over the part of its window inside
+ * wavelengths i0..i1 (1-based, inclusive), window-edge terms only where the window's own edge lies
+ * in the range.  The adjoint is linear in dL/dSfL and the ranges of a partition cover each window
+ * point once, so the sum over ranks of glin and gvmic is the whole-grid gradient (one all-reduce);
+ * LineOpac outside the range is not read. */
+int fsg_adjoint_range_dev(fsg_ctx *ctx, const fsg_lines *d_lines, const int32_t *d_flags,
+                          const int32_t *d_ileft, const int32_t *d_iright, int i0, int i1,
+                          const double *d_gflux, double *d_gkappa, double *d_glin, double *d_gvmic);
+
+/* ---- failure injection, for tests of the error paths (no counterpart in the reference) -------
+ * FSG_FAULT_ALLOC_LIMIT: the context's device allocations larger than value bytes fail as on an
+ * exhausted device (FSG_E_NOMEM with the buffer's name; the context stays usable).
+ * FSG_FAULT_COPY_TIMEOUT: every chunk of line records the accumulation kernels stage expects 16 bytes
+ * more than its bulk copies deliver, so its mbarrier phase never completes and the bounded wait gives
+ * up after value milliseconds (0.01-1000); the copies themselves complete, the kernel drains and
+ * returns, and the call reports FSG_E_TIMEOUT.  FSG_FAULT_NONE restores normal operation. */
+enum { FSG_FAULT_NONE = 0, FSG_FAULT_ALLOC_LIMIT = 1, FSG_FAULT_COPY_TIMEOUT = 2 };
+int fsg_set_fault(fsg_ctx *ctx, int kind, double value);
 
 /* ---- batched synthesis ---------------------------------------------------------------------
  * Many atmospheres (each a context with grid, atmosphere, continuum and mu set; mixed precision)

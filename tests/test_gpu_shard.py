@@ -109,3 +109,37 @@ def test_radtran_range_solves_only_its_rows(fsg):
         C.radtran_range_dev(0, 5, None, None, out[2].data_ptr(), None)
     with pytest.raises(fsg.FsgError):
         C.radtran_range_dev(10, nwl + 1, None, None, out[2].data_ptr(), None)
+
+
+def test_range_adjoints_sum_to_the_whole_gradient(fsg):
+    """fsg_adjoint_range_dev over a partition of the grid into three ranges, summed, equals the
+    whole-grid fsg_adjoint_dev (dL/d ln gf and the vmicro shares of every line); the ranges' own
+    LineOpac is the only opacity the sharded forward gives each rank."""
+    from fastspec_b200 import shard
+    grid, st, co, arr = cooldwarf_case(n=1500, seed=26)
+    C = make(fsg, grid, st, co)
+    dt = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in arr.items()}
+    B = shard.GpuBackend(fsg, C, dt)
+    n, nwl = B.n, C.nwl
+    win = B.central(0, n, n)
+    g = torch.from_numpy(np.random.default_rng(8).normal(0, 1, nwl)).cuda()
+    glin = torch.empty(n, dtype=torch.float64, device="cuda")
+    gvm = torch.empty_like(glin)
+    torch.cuda.synchronize()
+    C.lineop_reset()
+    C.lineop_calc_dev(B.full)                      # the whole-grid adjoint reads the context's own windows
+    C.radtran_dev(None, None, B.sfl.data_ptr(), B.sfc.data_ptr())
+    C.adjoint_dev(B.full, g.data_ptr(), glin.data_ptr(), gvm.data_ptr())
+    ref_lin, ref_vm = glin.cpu().numpy(), gvm.cpu().numpy()
+    sum_lin, sum_vm = np.zeros(n), np.zeros(n)
+    ranges = shard.balanced_ranges(shard.pixel_cost(win, nwl), 3)
+    for i0, i1 in ranges:
+        C.lineop_reset()
+        C.accumulate_dev(B.full, win[0].data_ptr(), win[1].data_ptr(), win[2].data_ptr(), i0, i1)
+        gl, gv = B.adjoint(win, i0, i1, g)
+        sum_lin += gl.cpu().numpy()
+        sum_vm += gv.cpu().numpy()
+    scale = np.max(np.abs(ref_lin))
+    assert np.max(np.abs(sum_lin - ref_lin)) <= 1e-6 * scale
+    assert np.max(np.abs(sum_vm - ref_vm)) <= 1e-6 * np.max(np.abs(ref_vm))
+    assert np.count_nonzero(ref_lin) > n // 2
