@@ -7,7 +7,9 @@ recipe copies that executable, unmodified, to baseline/_ref/ so that `bench.py -
 runs the reference's own stock build on the host cores of the machine it runs on.  The executable
 is only run (decks in, fs_*.bin out), never inspected.
 
-    python oracle/install_reference.py [reference tree, default /root/reference]
+    python oracle/install_reference.py [reference tree]
+The tree: the argument, else $FASTSPEC_REFERENCE, else the read-only mount the build machine keeps it
+at (MOUNT); when none exists nothing is installed.
 """
 import os
 import shutil
@@ -16,9 +18,11 @@ import sys
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DEST = os.path.join(REPO, "baseline", "_ref")
 NAME = "fastspec_Linux_x86_64"
+MOUNT = "/root/reference"
 
 
-def install(ref_tree="/root/reference"):
+def install(ref_tree=None):
+    ref_tree = ref_tree or os.environ.get("FASTSPEC_REFERENCE") or MOUNT
     src = os.path.join(ref_tree, "src", NAME)
     if not os.path.exists(src):
         return None

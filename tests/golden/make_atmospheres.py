@@ -26,7 +26,8 @@ Also writes parity fixtures (tests/golden/pin_*.npz): line lists run through the
 with the reference's line opacity, windows and spectra, for the oracle/GPU parity tests.
 Test infrastructure: the oracle serves as the inversion model here.
 
-Needs the reference at /root/reference (this container only); the outputs are committed.
+Needs the reference tree named by $FASTSPEC_REFERENCE (its prebuilt executable is run); the outputs are
+committed.
 """
 import os
 import subprocess
@@ -43,7 +44,7 @@ sys.path.insert(0, REPO)
 import oracle  # noqa: E402  (fixture generation: the oracle is the inversion model)
 from fastspec_b200 import fsio, workloads as W  # noqa: E402
 
-BIN = "/root/reference/src/fastspec_Linux_x86_64"
+BIN = os.path.join(os.environ.get("FASTSPEC_REFERENCE", ""), "src", "fastspec_Linux_x86_64")
 
 AMASS = {"H": 1.00794, "He": 4.002602, "C": 12.0107, "N": 14.0067, "O": 15.9994,
          "Ca": 40.078, "Ti": 47.867, "Cr": 51.9961, "Fe": 55.845, "Ni": 58.6934}

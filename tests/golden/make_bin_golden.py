@@ -19,7 +19,7 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
 from fastspec_b200 import workloads as W  # noqa: E402
 
-BIN = "/root/reference/src/fastspec_Linux_x86_64"
+BIN = os.path.join(os.environ.get("FASTSPEC_REFERENCE", ""), "src", "fastspec_Linux_x86_64")
 OUT = os.path.join(HERE, "fs_outputs.npz")
 # post-processing runs (Vsini, Vmacro, Vgau) on the two intensity files: a resolving power, a FWHM
 CONV = {"conv_a": (15.0, 3.0, 60000.0), "conv_b": (5.0, 0.0, 2.5)}

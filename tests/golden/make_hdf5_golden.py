@@ -13,7 +13,7 @@ import os
 
 import numpy as np
 
-LINES = "/root/reference/examples/lines"
+LINES = os.path.join(os.environ.get("FASTSPEC_REFERENCE", ""), "examples", "lines")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "hdf5_examples.npz")
 N = 300
 

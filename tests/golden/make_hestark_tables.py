@@ -9,16 +9,18 @@ PARAMETER arrays WlcHe, EloHe, Tt90/Tt84, We90 ... Sp84) and writes them in this
 layout: one record per tabulated line holding its centre, lower level energy, knot count and, per
 perturber, the width and shift at every knot.
 
-Run here, where the reference tree exists:  python make_hestark_tables.py [path/to/hestark.f90]
-The header is committed; the library and the oracle include it.
+    python tests/golden/make_hestark_tables.py [path/to/hestark.f90]
+(default: src/hestark.f90 of the reference tree named by $FASTSPEC_REFERENCE).  The header is
+committed beside the library's sources; the library and the oracle include it.
 """
 import os
 import re
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = "/root/reference/src/hestark.f90"
-OUT = os.path.join(HERE, "fsg_hestark_tables.h")
+REPO = os.path.dirname(os.path.dirname(HERE))
+SRC = os.path.join(os.environ.get("FASTSPEC_REFERENCE", ""), "src", "hestark.f90")
+OUT = os.path.join(REPO, "fastspec_b200", "csrc", "fsg_hestark_tables.h")
 
 
 def parameter_array(text, name):

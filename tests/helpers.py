@@ -6,6 +6,15 @@ import numpy as np
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DATA = os.path.join(REPO, "fastspec_b200", "data")
 GOLD = os.path.join(REPO, "tests", "golden")
+# the reference tree, for the CPU tests that run its executable or read its shipped examples (they skip
+# without it): FASTSPEC_REFERENCE, else the mount the install recipe looks at
+def _reference_tree():
+    from oracle.install_reference import MOUNT
+    tree = os.environ.get("FASTSPEC_REFERENCE") or MOUNT
+    return tree if os.path.isdir(tree) else ""
+
+
+REFERENCE = _reference_tree()
 
 STATE_KEYS = ("rhox", "T", "xne", "xna", "rho", "fractionpf", "xamass", "potion", "ion", "frac_h1", "frac_he1")
 

@@ -128,8 +128,8 @@ def test_spec_grid_orders_angles_and_detects_log_grids():
     assert u["wmode"] == 0 and abs(u["dstep"] - 0.01) < 1e-12
 
 
-REF_BIN = "/root/reference/src/fastspec_Linux_x86_64"
-MAG_EXAMPLE = "/root/reference/examples/magnetic-synthesis/fs_spec.bin"
+REF_BIN = os.path.join(H.REFERENCE, "src", "fastspec_Linux_x86_64")
+MAG_EXAMPLE = os.path.join(H.REFERENCE, "examples", "magnetic-synthesis", "fs_spec.bin")
 
 
 @pytest.mark.skipif(not (os.path.exists(REF_BIN) and os.path.exists(MAG_EXAMPLE)),
@@ -159,7 +159,7 @@ def test_post_processing_of_the_shipped_magnetic_example(fsg, oracle_mod, tmp_pa
     assert np.max(np.abs(sfc / ref["sfc"] - 1)) < 1e-12
 
 
-EXAMPLES = "/root/reference/examples"
+EXAMPLES = os.path.join(H.REFERENCE, "examples")
 
 
 @pytest.mark.skipif(not os.path.isdir(EXAMPLES), reason="the reference's examples are not present")

@@ -16,7 +16,7 @@ import pytest
 
 import helpers as H
 
-EXAMPLES = "/root/reference/examples/lines"
+EXAMPLES = os.path.join(H.REFERENCE, "examples", "lines")
 
 
 def _golden():
