@@ -598,15 +598,18 @@ def run_gpu(args, rank, world):
         h2d = sum(int(v.numel() * v.element_size()) for v in pin.values())
         out.update(ms_e2e=ms_e2e, h2d=h2d, d2h=2 * nwl * 8, flux_check=float(hsfl[nwl // 2].item()))
     C.close()
-    if not args.no_plain and rank == 0:
+    # the side measurements are single-GPU ones: a multi-GPU run leaves them to its N = 1 line, so
+    # that no rank waits at the closing barrier for minutes of rank 0's extra work
+    side = world == 1
+    if not args.no_plain and side:
         out["plain"] = plain_fp64(F, torch, st, meta, co, dev, dt, int(args.plain_lines), (ms / args.steps, mixed_flux))
     del dt, dl
     torch.cuda.empty_cache()
-    if not args.no_stokes and rank == 0:
+    if not args.no_stokes and side:
         out["stokes"] = stokes_synthesis(F, torch, dev, args.steps, args.warmup)
-    if not args.no_fit and rank == 0:
+    if not args.no_fit and side:
         out["fit"] = differentiable_fit(F, torch, dev, args.steps, args.warmup)
-    if not args.no_batched and rank == 0:
+    if not args.no_batched and side:
         out["batched"] = batched_grid(F, torch, dev, args.batch_atm, args.batch_lines, args.steps, args.warmup)
     return out
 

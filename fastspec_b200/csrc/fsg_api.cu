@@ -610,10 +610,10 @@ static int upload_lines(fsg_ctx *ctx, const fsg_lines *L, fsg_lines *D) {
     return FSG_OK;
 }
 
-static int check_lines(fsg_ctx *ctx, const fsg_lines *L) {
+static int check_lines(fsg_ctx *ctx, const fsg_lines *L, bool need_cont = true) {
     if (!ctx) return FSG_E_ARG;
-    if (!ctx->have_grid || !ctx->have_atm || !ctx->have_cont)
-        return fail(ctx, FSG_E_STATE, "lineop: set grid, atmosphere and continuum opacity first");
+    if (!ctx->have_grid || !ctx->have_atm) return fail(ctx, FSG_E_STATE, "lineop: set grid and atmosphere first");
+    if (need_cont && !ctx->have_cont) return fail(ctx, FSG_E_STATE, "lineop: set continuum opacity first");
     if (!L || L->n < 0 || (L->n > 0 && (!L->wl || !L->elo || !L->gf || !L->grad || !L->gqst || !L->gvdw || !L->spc)))
         return fail(ctx, FSG_E_ARG, "lineop: bad line list");
     if (L->kind < 0 || L->kind > 2) return fail(ctx, FSG_E_ARG, "lineop: kind must be 0, 1 or 2");
@@ -1648,7 +1648,7 @@ static int check_points(fsg_ctx *ctx, const fsg_lineblock *b, int64_t npts, cons
 }
 
 int fsg_xline_setup(fsg_ctx *ctx, const fsg_lines *lines, fsg_xcoef *xc) {
-    int rc = check_lines(ctx, lines); if (rc) return rc;
+    int rc = check_lines(ctx, lines, false); if (rc) return rc;      // XlineSetup reads no continuum
     if (lines->n > 0 && !xc) return fail(ctx, FSG_E_ARG, "fsg_xline_setup: output missing");
     if (lines->n == 0) return FSG_OK;
     cudaSetDevice(ctx->device);

@@ -238,7 +238,8 @@ typedef struct {
     const float *splpi, *strpi, *splsi, *strsi;
 } fsg_lineblock;
 /* XlineSetup (opacity.f90:96-235) of every line of a host list, with the flags the drivers set
- * before it (molecule and ABO bits from the list, synth.f90:837-845): xc[n]. */
+ * before it (molecule and ABO bits from the list, synth.f90:837-845): xc[n]. Needs the grid and the
+ * atmosphere, not the continuum. */
 int fsg_xline_setup(fsg_ctx *ctx, const fsg_lines *lines, fsg_xcoef *xc);
 /* XlineDepth (opacity.f90:239-293) of n lines at every depth: lincop/linvvgt/linavgt [n][ntau]. */
 int fsg_xline_depth(fsg_ctx *ctx, int64_t n, const fsg_xcoef *xc, double *lincop, double *linvvgt,

@@ -1769,6 +1769,7 @@ void or_xline_depth(const or_state *s, int t, const or_xcoef *xc, double *lincop
 void or_lineopacity1(const or_state *s, const double *wlcent, const int *flags, const int *ileft,
                      const int *iright, const double *lincop, const double *linvvgt, const double *linavgt,
                      double Wl, int l1, int l2, int iwl, long loff, double *linop) {
+    or_voigt_init();                       /* VgtTab and its damping nodes, built once */
     int nt = s->ntau;
     for (int t = 0; t < nt; t++) linop[t] = 0.0;
     for (long il = l1; il <= l2; il++) {
@@ -1790,6 +1791,7 @@ void or_lineopacity1(const or_state *s, const double *wlcent, const int *flags, 
 
 void or_lineopacity2(const or_state *s, double Wl, double wlcent, int flag, int ileft, int iright, int iwl,
                      const double *lincop, const double *linvvgt, const double *linavgt, double *linop) {
+    or_voigt_init();
     linework W;
     long orig = 0;
     W.n = 1; W.wlcent = &wlcent; W.flag = &flag; W.ileft = &ileft; W.iright = &iright; W.orig = &orig;
@@ -1801,6 +1803,7 @@ void or_mag_lineopacity1(const or_state *s, const double *wlcent, const int *fla
                          const int *npi, const int *nsi, const long *pi_off, const long *si_off,
                          const float *splpi, const float *strpi, const float *splsi, const float *strsi,
                          double Wl, int l1, int l2, int iwl, long loff, double *M) {
+    or_fvoigt_init();                      /* FvTab and its damping nodes, built once */
     int nt = s->ntau;
     for (int q = 0; q < 6 * nt; q++) M[q] = 0.0;
     for (long iline = l1; iline <= l2; iline++) {
@@ -1843,6 +1846,7 @@ void or_mag_lineopacity1(const or_state *s, const double *wlcent, const int *fla
 
 double or_analytic_window(const or_state *s, int flag, const double *lincop, const double *linvvgt,
                           const double *linavgt, const double *contopac) {
+    or_voigt_init();
     return analytic_window(s, flag, lincop, linvvgt, linavgt, contopac);
 }
 

@@ -205,9 +205,11 @@ def test_stokes_prf_pp(fsg, oracle_mod):
     C.set_mu(x, w)
     g = C.mag_lineop_calc(fsg.LineList.from_arrays(L.arrays(), zeeman=z), 1, np.array([2000.0, 60.0, 30.0]))
     mlo = g["maglineopac"]
-    lo = C.lineop_get()
-    S = oracle_mod.State(grid, st, contopac=co, vmicro=1.0)
     rng = np.random.default_rng(11)
+    # a LineOpac of the non-Zeeman lines (StokesPrfPP adds it to the pi and sigma absorption)
+    lo = co * rng.uniform(0.0, 3.0, co.shape)
+    C.lineop_set(lo)
+    S = oracle_mod.State(grid, st, contopac=co, vmicro=1.0)
     npts = 64
     iwl = rng.integers(1, S.nwl + 1, npts).astype(np.int32)
     src = 1e14 * (1.0 + rng.uniform(0, 1, (npts, S.ntau))) * np.linspace(1, 4, S.ntau)
