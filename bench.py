@@ -69,6 +69,7 @@ def parse():
     p.add_argument("--batch-lines", type=float, default=2e6)
     p.add_argument("--no-fit", action="store_true", help="skip the differentiable-fit measurement")
     p.add_argument("--no-stokes", action="store_true", help="skip the polarised (Stokes) synthesis measurement")
+    p.add_argument("--no-c0", action="store_true", help="skip the plain scalar synthesis (20,000 lines) measurement")
     return p.parse_args()
 
 
@@ -348,6 +349,87 @@ def differentiable_fit(F, torch, dev, steps, warmup):
     return out
 
 
+def scalar_c0(F, torch, dev, steps, warmup):
+    """The plain scalar configuration: 20,000 atomic lines over 5000-5200 A at 0.005 A (40,001
+    wavelengths), the solar-like atmosphere (56 depths), 7 angles: LineopCalc + RadTranCalc + flux
+    through the C-ABI with the list and the spectra in host memory, FP64 and mixed; and the reference
+    executable on the same deck with all host threads."""
+    from fastspec_b200 import workloads as W
+    d = np.load(os.path.join(HERE, "fastspec_b200", "data", "atm_solar.npz"))
+    st = {k: d[k] for k in ("rhox", "T", "xne", "xna", "rho", "fractionpf", "xamass", "potion", "ion", "frac_h1",
+                            "frac_he1")}
+    w0, w1, step = 5000.0, 5200.0, 0.005
+    wave = F.make_grid(0, w0, w1, step) + w0
+    lk = np.log(d["cont_opac"])
+    co = np.exp(np.stack([np.interp(wave, d["cont_wave"], lk[:, t]) for t in range(lk.shape[1])], axis=1))
+    L = W.atomic_lines(20000, w0, w1, W.SEED0 + 0, exact=True)
+    LL = F.LineList.from_arrays(L.arrays())
+    x, w, _ = F.mu_quadrature(1, NMU)
+    out = {"config": "20,000 atomic lines 5000-5200 A at 0.005 A (40,001 wavelengths), solar-like 56 depths, 7 mu",
+           "timing": "wall clock per synthesis (LineopCalc + RadTranCalc + flux, host list in, host spectra out)"}
+    flux = {}
+    for name, prec in (("fp64", F.PREC_FP64), ("mixed", F.PREC_MIXED)):
+        C = F.Context(device=dev, precision=prec, vmicro=float(d["vmicro"]), molbrd=int(d["molbrd"]))
+        C.set_grid(0, w0, w1, step)
+        C.set_atmosphere(st)
+        C.set_contopac(co)
+        C.set_mu(x, w)
+
+        def one():
+            C.lineop_reset()
+            r = C.lineop_calc(LL, want_lineopac=False, want_lines=False)
+            return r["stats"], C.radtran()
+
+        for _ in range(warmup):
+            one()
+        torch.cuda.synchronize()
+        n = max(steps, 10)
+        t0 = time.perf_counter()
+        for _ in range(n):
+            stt, sp = one()
+        ms = (time.perf_counter() - t0) * 1e3 / n
+        flux[name] = sp[2] / sp[3]
+        out[name] = {"spectra_per_s": 1e3 / ms, "ms_per_spectrum": ms, "ms_lineop": stt["ms_total"],
+                     "line_evals": stt["line_evals"], "line_evals_per_s": stt["line_evals"] / (stt["ms_total"] / 1e3)}
+        out["nwl"] = C.nwl
+        C.close()
+    out["mixed_vs_fp64_flux_max_rel"] = float(np.max(np.abs(flux["mixed"] / flux["fp64"] - 1)))
+    if os.path.exists(REF_BIN):
+        ref = ref_c0(L, d, os.cpu_count())
+        out["reference"] = ref
+        if "spectra_per_s" in ref:
+            out["mixed_over_reference"] = out["mixed"]["spectra_per_s"] / ref["spectra_per_s"]
+            out["fp64_over_reference"] = out["fp64"]["spectra_per_s"] / ref["spectra_per_s"]
+    return out
+
+
+def ref_c0(L, d, threads):
+    """The reference executable on the plain scalar deck (the same 20,000 lines as a .z list, the
+    solar-like Eddington-grey model it derives the atmosphere state from): its own stage times of the
+    line opacity (list reading included) and of the formal solver, and the wall clock of the whole run."""
+    import tempfile
+    from fastspec_b200 import workloads as W
+    with tempfile.TemporaryDirectory() as wd:
+        W.write_krz(os.path.join(wd, "model.krz"), W.eddington_model(float(d["teff"]), float(d["logg"]), len(d["T"])))
+        L.write_z(os.path.join(wd, "lines.z"), 5000.0, 5200.0)
+        deck = ("wave=5000.0, 5200.0, 0.005, 0\nsave=0, 0, 0, 0, 1\nvmic=%.3f\nmolbrd=%d\nlines=\n-1  lines.z\n\n"
+                "model=model.krz\nmus=%d\n" % (float(d["vmicro"]), int(d["molbrd"]), NMU))
+        with open(os.path.join(wd, "in.dat"), "w") as f:
+            f.write(deck)
+        t0 = time.perf_counter()
+        r = subprocess.run([REF_BIN, "in.dat"], cwd=wd, capture_output=True, text=True,
+                           env=dict(os.environ, OMP_NUM_THREADS=str(threads)))
+        wall = time.perf_counter() - t0
+    if r.returncode != 0 or "Total time" not in r.stdout:
+        return {"threads": threads, "error": (r.stdout + r.stderr)[-300:]}
+    lines_s = _stage_seconds(r.stdout, "Total lines read")
+    rt_s = _stage_seconds(r.stdout, "radiative transfer")
+    return {"threads": threads, "opacity_s": lines_s, "solver_s": rt_s, "wall_s": wall,
+            "spectra_per_s": 1.0 / max((lines_s or 0.0) + (rt_s or 0.0), 0.1),
+            "timing": "the executable's own stage timers (0.1 s resolution, a floor of 0.1 s on their sum): line "
+                      "opacity (list reading included) + formal solver, per spectrum; wall_s: the whole program"}
+
+
 def stokes_synthesis(F, torch, dev, steps, warmup):
     """The polarised configuration: 5000 Zeeman lines over 6000-6100 A at 0.002 A (50,001
     wavelengths), the Teff = 5000 K, log g = 4.5 atmosphere (56 depths), BFRAME 1 with |B| = 2 kG at
@@ -605,6 +687,8 @@ def run_gpu(args, rank, world):
         out["plain"] = plain_fp64(F, torch, st, meta, co, dev, dt, int(args.plain_lines), (ms / args.steps, mixed_flux))
     del dt, dl
     torch.cuda.empty_cache()
+    if not args.no_c0 and side:
+        out["c0"] = scalar_c0(F, torch, dev, args.steps, args.warmup)
     if not args.no_stokes and side:
         out["stokes"] = stokes_synthesis(F, torch, dev, args.steps, args.warmup)
     if not args.no_fit and side:
@@ -876,6 +960,8 @@ def main():
         line["differentiable_fit"] = r["fit"]
     if "stokes" in r:
         line["stokes"] = r["stokes"]
+    if "c0" in r:
+        line["plain_scalar_c0"] = r["c0"]
     print(json.dumps(line))
 
 

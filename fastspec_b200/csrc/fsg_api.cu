@@ -66,6 +66,12 @@ int fsg_launch_core_batch(cudaStream_t, int, const CoreJob *, const int *, int, 
                           int *);
 int fsg_class_pix(int);
 int fsg_fast_tiles(int);
+int fsg_bclass_count(int);
+int fsg_launch_bclass_order(cudaStream_t, int64_t, const int32_t *, const int32_t *, const int32_t *, int, int *,
+                            int64_t *, int64_t *, int64_t *);
+size_t fsg_bspan_scratch(int64_t);
+int fsg_launch_btile_span(cudaStream_t, int, int64_t, const LineHdr *, const int64_t *, int, int, int, int, int, int,
+                          int *, int *, void *, size_t);
 size_t fsg_tile_span_scratch(int64_t);
 int fsg_launch_tile_span_tw(cudaStream_t, int, int, int, int64_t, const LineHdr *, int *, int *, void *, size_t);
 void fsg_launch_mag_params_fast(cudaStream_t, const AtmView &, const LineView &, const int64_t *, int64_t, int64_t,
@@ -2220,19 +2226,21 @@ static int adjoint_common(fsg_ctx *ctx, const fsg_lines *d_lines, const int32_t 
 
 // ================================================================================================
 // Batched synthesis: many atmospheres (each an fsg_ctx with grid, atmosphere, continuum and mu
-// set), one shared line list.  Per atmosphere: central pass and block refill of the lines in its
-// span (plus a margin), tile ranges; then ONE persistent wing-pass launch and ONE persistent
-// core-pass launch take (atmosphere, tile) items from device work queues; then the formal solver
+// set), one shared line list.  Per atmosphere: central pass of the lines in its span (plus a
+// margin), their records in window-width-class order (block refill), tile ranges per class; then
+// two persistent wing-pass launches (narrow classes, wide classes) and one persistent core-pass
+// launch take (atmosphere and class, tile) items from device work queues; then the formal solver
 // and flux of each atmosphere.  The whole sequence has no host synchronisation and is captured
-// once as a CUDA graph; later runs replay it.  The tile width and the CTA counts of the persistent
-// launches are chosen by timing the candidates on the first run (fsg_batch_tune).
+// once as a CUDA graph; later runs replay it.  The wide classes' tile width and the CTA counts of
+// the persistent launches are chosen by timing the candidates on the first run (fsg_batch_tune).
 // ================================================================================================
 static thread_local std::string g_batch_err;        // failure of the last fsg_batch_create on this thread
 
 struct BAtm {
     fsg_ctx *ctx = nullptr;
     int64_t c0 = 0, cn = 0;                    // candidate lines [c0, c0 + cn) of the shared list
-    DBuf flags, il, ir, wing, core, hdr, wtlo, wthi, ctlo, cthi, span, sfl, sfc;
+    int ncls = 1;                              // window-width classes of its record order
+    DBuf flags, il, ir, wing, core, hdr, wtlo, wthi, ctlo, cthi, span, sfl, sfc, order, ccnt, coff, ctot;
 };
 
 struct fsg_batch {
@@ -2240,7 +2248,12 @@ struct fsg_batch {
     std::vector<BAtm> atm;
     fsg_lines dlines{};
     int ntau_max = 0;
-    DBuf idx, jobs_w, jobs_c, tile0_w, tile0_c, queue, err, nk, evals;
+    // atmospheres grouped by depth count: each group's launches are shaped for its deepest member;
+    // per group, the offsets of its jobs (narrow-class wing, wide-class wing, core) in the job arrays and
+    // of its queue prefix sums (each starting at 0) in the tile0 arrays
+    struct Group { int ntau_max, jn0, njn, jw0, njw, jc0, njc, tn0, tw0, tc0; };
+    std::vector<Group> groups;
+    DBuf jobs_wn, jobs_ww, jobs_c, tile0_wn, tile0_ww, tile0_c, queue, err, nk, evals;
     fsg_batch_tuning tune{};
     int tuned = 0;
     cudaGraph_t graph = nullptr;
@@ -2258,7 +2271,14 @@ static LineView batch_view(const fsg_batch *b, const BAtm &a) {
     return make_view(&D);
 }
 
-// the per-atmosphere stages up to the tile ranges (wing tiles of P wavelengths per lane)
+// Wing tiles: 64 wavelengths for the two narrowest window classes (windows up to 512), 32 * P for
+// the others; core tiles: 32 wavelengths.  Tile arrays hold ncls rows of tstride entries.
+static const int BATCH_NARROW = 1;             // classes 0 .. BATCH_NARROW take the narrow tiles
+static int batch_wing_stride(const fsg_ctx *c) { return (c->nwl + 63) / 64; }
+static int batch_core_stride(const fsg_ctx *c) { return (c->nwl + 31) / 32; }
+
+// the per-atmosphere stages up to the tile ranges: central pass, class order, records in that order,
+// tile ranges per class (wide-class wing tiles of P wavelengths per lane)
 static int batch_prepare(fsg_batch *b, int P) {
     fsg_ctx *ctx = b->own;
     cudaStream_t s = ctx->stream;
@@ -2269,45 +2289,81 @@ static int batch_prepare(fsg_batch *b, int P) {
         LineView LV = batch_view(b, a);
         fsg_launch_center(s, A, LV, c->tab, a.flags.as<int32_t>(), a.il.as<int32_t>(), a.ir.as<int32_t>(),
                           b->nk.as<unsigned long long>());
-        fsg_launch_params_fast(s, A, LV, b->idx.as<int64_t>(), 0, 1, a.cn, a.flags.as<int32_t>(), a.il.as<int32_t>(),
+        if (fsg_launch_bclass_order(s, a.cn, a.flags.as<int32_t>(), a.il.as<int32_t>(), a.ir.as<int32_t>(), a.ncls,
+                                    a.ccnt.as<int>(), a.coff.as<int64_t>(), a.ctot.as<int64_t>(), a.order.as<int64_t>()))
+            return cuda_fail(ctx, cudaGetLastError(), "batch class order");
+        fsg_launch_params_fast(s, A, LV, a.order.as<int64_t>(), 0, 1, a.cn, a.flags.as<int32_t>(), a.il.as<int32_t>(),
                                a.ir.as<int32_t>(), c->tab, a.wing.as<WingRec>(), a.core.as<CoreRec>(),
                                a.hdr.as<LineHdr>());
-        if (fsg_launch_tile_span(s, P == 2 ? 0 : 2, c->nwl, a.cn, a.hdr.as<LineHdr>(), a.wtlo.as<int>(),
-                                 a.wthi.as<int>(), a.span.p, a.span.cap) ||
-            fsg_launch_tile_span(s, -1, c->nwl, a.cn, a.hdr.as<LineHdr>(), a.ctlo.as<int>(), a.cthi.as<int>(),
-                                 a.span.p, a.span.cap))
+        if (fsg_launch_btile_span(s, 0, a.cn, a.hdr.as<LineHdr>(), a.coff.as<int64_t>(), a.ncls, BATCH_NARROW, 64,
+                                  32 * P, c->nwl, batch_wing_stride(c), a.wtlo.as<int>(), a.wthi.as<int>(), a.span.p,
+                                  a.span.cap) ||
+            fsg_launch_btile_span(s, 1, a.cn, a.hdr.as<LineHdr>(), a.coff.as<int64_t>(), a.ncls, a.ncls, 32, 32,
+                                  c->nwl, batch_core_stride(c), a.ctlo.as<int>(), a.cthi.as<int>(), a.span.p,
+                                  a.span.cap))
             return cuda_fail(ctx, cudaGetLastError(), "batch tile ranges");
     }
     CK(cudaGetLastError(), "batch prepare");
     return FSG_OK;
 }
 
-// job tables and queue prefix sums for wing tiles of P wavelengths per lane (host, then uploaded)
+// Job tables and queue prefix sums (host, then uploaded).  Atmospheres are grouped by depth count
+// (buckets of 8 depths), so a persistent launch is shaped for its own group's deepest member and few
+// warps idle.  Per group: one job per (atmosphere, class), the wing jobs of the narrow classes
+// (64-wavelength tiles) and of the wide ones (32 P) in two launches, the core jobs in a third; jobs run
+// widest class first, so the longest tiles start early and the queue ends on short ones.
 static int batch_jobs(fsg_batch *b, int P) {
     fsg_ctx *ctx = b->own;
-    std::vector<WingJob> jw; std::vector<CoreJob> jc;
-    std::vector<int> tw(1, 0), tc(1, 0);
-    for (auto &a : b->atm) {
-        fsg_ctx *c = a.ctx;
-        if (a.cn == 0) continue;
-        jw.push_back(WingJob{ c->ntau, c->nwl, c->d_wave.as<double>(), a.hdr.as<LineHdr>(), a.wing.as<WingRec>(),
-                              a.wtlo.as<int>(), a.wthi.as<int>(), c->d_lineopac.as<double>(), 0u, WAIT_NS });
-        jc.push_back(CoreJob{ c->ntau, c->nwl, c->d_wave.as<double>(), a.hdr.as<LineHdr>(), a.wing.as<WingRec>(),
-                              a.core.as<CoreRec>(), a.ctlo.as<int>(), a.cthi.as<int>(), c->d_lineopac.as<double>(),
-                              nullptr, 0u, WAIT_NS });
-        tw.push_back(tw.back() + (c->nwl + 32 * P - 1) / (32 * P));
-        tc.push_back(tc.back() + (c->nwl + 31) / 32);
+    std::vector<WingJob> jn, jw; std::vector<CoreJob> jc;
+    std::vector<int> tn, tw, tc;
+    b->groups.clear();
+    for (int bucket = 0; bucket * 8 < 128; bucket++) {
+        fsg_batch::Group g{ 0, (int)jn.size(), 0, (int)jw.size(), 0, (int)jc.size(), 0, (int)tn.size(),
+                            (int)tw.size(), (int)tc.size() };
+        int cmax = 0;
+        for (auto &a : b->atm)
+            if (a.cn && (a.ctx->ntau - 1) / 8 == bucket) {
+                cmax = std::max(cmax, a.ncls);
+                g.ntau_max = std::max(g.ntau_max, a.ctx->ntau);
+            }
+        if (!g.ntau_max) continue;
+        tn.push_back(0); tw.push_back(0); tc.push_back(0);
+        for (int cls = cmax - 1; cls >= 0; cls--)
+            for (auto &a : b->atm) {
+                fsg_ctx *c = a.ctx;
+                if (a.cn == 0 || (c->ntau - 1) / 8 != bucket || cls >= a.ncls) continue;
+                const int ws = batch_wing_stride(c), cs = batch_core_stride(c);
+                const WingJob J{ c->ntau, c->nwl, c->d_wave.as<double>(), a.hdr.as<LineHdr>(), a.wing.as<WingRec>(),
+                                 a.wtlo.as<int>() + (size_t)cls * ws, a.wthi.as<int>() + (size_t)cls * ws,
+                                 c->d_lineopac.as<double>(), 0u, WAIT_NS };
+                if (cls <= BATCH_NARROW) { jn.push_back(J); tn.push_back(tn.back() + (c->nwl + 63) / 64); }
+                else { jw.push_back(J); tw.push_back(tw.back() + (c->nwl + 32 * P - 1) / (32 * P)); }
+                jc.push_back(CoreJob{ c->ntau, c->nwl, c->d_wave.as<double>(), a.hdr.as<LineHdr>(),
+                                      a.wing.as<WingRec>(), a.core.as<CoreRec>(), a.ctlo.as<int>() + (size_t)cls * cs,
+                                      a.cthi.as<int>() + (size_t)cls * cs, c->d_lineopac.as<double>(), nullptr, 0u,
+                                      WAIT_NS });
+                tc.push_back(tc.back() + (c->nwl + 31) / 32);
+            }
+        g.njn = (int)jn.size() - g.jn0; g.njw = (int)jw.size() - g.jw0; g.njc = (int)jc.size() - g.jc0;
+        b->groups.push_back(g);
     }
-    ALLOC(b->jobs_w, sizeof(WingJob) * std::max<size_t>(jw.size(), 1));
+    ALLOC(b->jobs_wn, sizeof(WingJob) * std::max<size_t>(jn.size(), 1));
+    ALLOC(b->jobs_ww, sizeof(WingJob) * std::max<size_t>(jw.size(), 1));
     ALLOC(b->jobs_c, sizeof(CoreJob) * std::max<size_t>(jc.size(), 1));
-    ALLOC(b->tile0_w, sizeof(int) * tw.size()); ALLOC(b->tile0_c, sizeof(int) * tc.size());
+    ALLOC(b->tile0_wn, sizeof(int) * std::max<size_t>(tn.size(), 1));
+    ALLOC(b->tile0_ww, sizeof(int) * std::max<size_t>(tw.size(), 1));
+    ALLOC(b->tile0_c, sizeof(int) * std::max<size_t>(tc.size(), 1));
+    ALLOC(b->queue, 3 * sizeof(unsigned) * std::max<size_t>(b->groups.size(), 1));
     cudaStream_t s = ctx->stream;
-    if (!jw.empty()) {
-        CK(cudaMemcpyAsync(b->jobs_w.p, jw.data(), sizeof(WingJob) * jw.size(), cudaMemcpyHostToDevice, s), "jobs");
-        CK(cudaMemcpyAsync(b->jobs_c.p, jc.data(), sizeof(CoreJob) * jc.size(), cudaMemcpyHostToDevice, s), "jobs");
-    }
-    CK(cudaMemcpyAsync(b->tile0_w.p, tw.data(), sizeof(int) * tw.size(), cudaMemcpyHostToDevice, s), "jobs");
-    CK(cudaMemcpyAsync(b->tile0_c.p, tc.data(), sizeof(int) * tc.size(), cudaMemcpyHostToDevice, s), "jobs");
+    auto up = [&](DBuf &d, const void *h, size_t nb) {
+        return nb ? cudaMemcpyAsync(d.p, h, nb, cudaMemcpyHostToDevice, s) : cudaSuccess;
+    };
+    CK(up(b->jobs_wn, jn.data(), sizeof(WingJob) * jn.size()), "jobs");
+    CK(up(b->jobs_ww, jw.data(), sizeof(WingJob) * jw.size()), "jobs");
+    CK(up(b->jobs_c, jc.data(), sizeof(CoreJob) * jc.size()), "jobs");
+    CK(up(b->tile0_wn, tn.data(), sizeof(int) * tn.size()), "jobs");
+    CK(up(b->tile0_ww, tw.data(), sizeof(int) * tw.size()), "jobs");
+    CK(up(b->tile0_c, tc.data(), sizeof(int) * tc.size()), "jobs");
     CK(cudaStreamSynchronize(s), "jobs");
     return FSG_OK;
 }
@@ -2317,24 +2373,36 @@ static int batch_jobs(fsg_batch *b, int P) {
 static int batch_accumulate_solve(fsg_batch *b, const fsg_batch_tuning &t, cudaEvent_t *ev) {
     fsg_ctx *ctx = b->own;
     cudaStream_t s = ctx->stream;
-    int njobs = 0;
     for (auto &a : b->atm) {
         fsg_ctx *c = a.ctx;
         CK(cudaMemsetAsync(c->d_lineopac.p, 0, sizeof(double) * (size_t)c->nwl * c->ntau, s), "batch reset");
-        if (a.cn) njobs++;
     }
-    CK(cudaMemsetAsync(b->queue.p, 0, 2 * sizeof(unsigned), s), "queue reset");
-    if (njobs) {
-        if (ev) cudaEventRecord(ev[0], s);
-        if (fsg_launch_accum_batch(s, t.tile_pix / 32, b->ntau_max, b->jobs_w.as<WingJob>(), b->tile0_w.as<int>(),
-                                   njobs, t.wing_ctas, b->queue.as<unsigned>(), b->err.as<int>()))
-            return cuda_fail(ctx, cudaGetLastError(), "k_accum_batch");
-        if (ev) cudaEventRecord(ev[1], s);
-        if (fsg_launch_core_batch(s, b->ntau_max, b->jobs_c.as<CoreJob>(), b->tile0_c.as<int>(), njobs, t.core_ctas,
-                                  b->atm[0].ctx->tab.vtab4, b->queue.as<unsigned>() + 1, b->err.as<int>()))
+    const size_t ng = b->groups.size();
+    CK(cudaMemsetAsync(b->queue.p, 0, 3 * sizeof(unsigned) * std::max<size_t>(ng, 1), s), "queue reset");
+    unsigned *q = b->queue.as<unsigned>();
+    // every group's wing launches (narrow classes, then wide classes: both read-modify-write LineOpac),
+    // then every group's core launch
+    if (ev) cudaEventRecord(ev[0], s);
+    for (size_t gi = 0; gi < ng; gi++) {
+        const fsg_batch::Group &g = b->groups[gi];
+        if (g.njn && fsg_launch_accum_batch(s, 2, g.ntau_max, b->jobs_wn.as<WingJob>() + g.jn0,
+                                            b->tile0_wn.as<int>() + g.tn0, g.njn, t.wing_ctas, q + 3 * gi,
+                                            b->err.as<int>()))
+            return cuda_fail(ctx, cudaGetLastError(), "k_accum_batch (narrow classes)");
+        if (g.njw && fsg_launch_accum_batch(s, t.tile_pix / 32, g.ntau_max, b->jobs_ww.as<WingJob>() + g.jw0,
+                                            b->tile0_ww.as<int>() + g.tw0, g.njw, t.wing_ctas, q + 3 * gi + 1,
+                                            b->err.as<int>()))
+            return cuda_fail(ctx, cudaGetLastError(), "k_accum_batch (wide classes)");
+    }
+    if (ev) cudaEventRecord(ev[1], s);
+    for (size_t gi = 0; gi < ng; gi++) {
+        const fsg_batch::Group &g = b->groups[gi];
+        if (g.njc && fsg_launch_core_batch(s, g.ntau_max, b->jobs_c.as<CoreJob>() + g.jc0, b->tile0_c.as<int>() + g.tc0,
+                                           g.njc, t.core_ctas, b->atm[0].ctx->tab.vtab4, q + 3 * gi + 2,
+                                           b->err.as<int>()))
             return cuda_fail(ctx, cudaGetLastError(), "k_core_batch");
-        if (ev) cudaEventRecord(ev[2], s);
     }
+    if (ev) cudaEventRecord(ev[2], s);
     for (auto &a : b->atm) {
         fsg_ctx *c = a.ctx;
         if (fsg_launch_radtran(s, fsg_view(c), c->d_lineopac.as<double>(), c->d_rhox.as<double>(), c->nmu,
@@ -2385,7 +2453,6 @@ int fsg_batch_create(fsg_ctx *const *atms, int natm, const fsg_lines *lines, dou
     }
     cudaSetDevice(ctx->device);
     if (lines->n > 0) { rc = upload_lines(ctx, lines, &b->dlines); if (rc) return bail(rc, nullptr); }
-    int64_t cmax = 0;
     b->atm.resize(natm);
     for (int i = 0; i < natm; i++) {
         BAtm &a = b->atm[i];
@@ -2398,25 +2465,23 @@ int fsg_batch_create(fsg_ctx *const *atms, int natm, const fsg_lines *lines, dou
         const double *wl = lines->wl;
         a.c0 = std::lower_bound(wl, wl + lines->n, w0) - wl;
         a.cn = (std::upper_bound(wl, wl + lines->n, w1) - wl) - a.c0;
-        cmax = std::max(cmax, a.cn);
         int rca = ensure_lineopac(c); if (rca) return bail(rca, c->err.c_str());
-        size_t nt = c->ntau, cn = std::max<int64_t>(a.cn, 1);
+        if (a.cn > 2000000000LL) return bail(FSG_E_ARG, "fsg_batch_create: more than 2e9 lines in one span");
+        a.ncls = fsg_bclass_count(c->nwl);
+        const size_t nt = c->ntau, cn = std::max<int64_t>(a.cn, 1), ncl = a.ncls;
+        const size_t nsb = (cn + 1023) / 1024 * (ncl + 1);          // class counts per CTA of the order
+        const size_t ws = batch_wing_stride(c) * ncl, cs = batch_core_stride(c) * ncl;
         if (a.flags.ensure(4 * cn) || a.il.ensure(4 * cn) || a.ir.ensure(4 * cn) ||
             a.wing.ensure(sizeof(WingRec) * cn * nt) || a.core.ensure(sizeof(CoreRec) * cn * nt) ||
-            a.hdr.ensure(sizeof(LineHdr) * cn) || a.wtlo.ensure(4 * (size_t)fsg_fast_tiles(c->nwl)) ||
-            a.wthi.ensure(4 * (size_t)fsg_fast_tiles(c->nwl)) || a.ctlo.ensure(4 * (size_t)fsg_fast_tiles(c->nwl)) ||
-            a.cthi.ensure(4 * (size_t)fsg_fast_tiles(c->nwl)) || a.span.ensure(fsg_tile_span_scratch(cn)) ||
+            a.hdr.ensure(sizeof(LineHdr) * cn) || a.wtlo.ensure(4 * ws) || a.wthi.ensure(4 * ws) ||
+            a.ctlo.ensure(4 * cs) || a.cthi.ensure(4 * cs) || a.span.ensure(fsg_bspan_scratch(cn)) ||
+            a.order.ensure(8 * cn) || a.ccnt.ensure(4 * nsb) || a.coff.ensure(8 * nsb) || a.ctot.ensure(8) ||
             a.sfl.ensure(8 * (size_t)c->nwl) || a.sfc.ensure(8 * (size_t)c->nwl))
             return bail(FSG_E_NOMEM, "fsg_batch_create: device allocation failed");
     }
-    std::vector<int64_t> iota(std::max<int64_t>(cmax, 1));
-    for (int64_t i = 0; i < (int64_t)iota.size(); i++) iota[i] = i;
-    if (b->idx.ensure(sizeof(int64_t) * iota.size()) || b->queue.ensure(2 * sizeof(unsigned)) ||
-        b->err.ensure(sizeof(int)) || b->nk.ensure(sizeof(unsigned long long)))
+    if (b->err.ensure(sizeof(int)) || b->nk.ensure(sizeof(unsigned long long)))
         return bail(FSG_E_NOMEM, "fsg_batch_create: device allocation failed");
-    if (cudaMemcpy(b->idx.p, iota.data(), sizeof(int64_t) * iota.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemset(b->err.p, 0, sizeof(int)) != cudaSuccess)
-        return bail(FSG_E_CUDA, "fsg_batch_create: upload failed");
+    if (cudaMemset(b->err.p, 0, sizeof(int)) != cudaSuccess) return bail(FSG_E_CUDA, "fsg_batch_create: upload failed");
     for (int i = 0; i < 6; i++) cudaEventCreate(&b->ev[i]);
     b->tune.tile_pix = 128;
     b->tune.wing_ctas = 148;
@@ -2567,10 +2632,11 @@ void fsg_batch_destroy(fsg_batch *b) {
     if (b->graph) cudaGraphDestroy(b->graph);
     for (auto &a : b->atm) {
         DBuf *bufs[] = { &a.flags, &a.il, &a.ir, &a.wing, &a.core, &a.hdr, &a.wtlo, &a.wthi, &a.ctlo, &a.cthi,
-                         &a.span, &a.sfl, &a.sfc };
+                         &a.span, &a.sfl, &a.sfc, &a.order, &a.ccnt, &a.coff, &a.ctot };
         for (DBuf *d : bufs) d->release();
     }
-    DBuf *bufs[] = { &b->idx, &b->jobs_w, &b->jobs_c, &b->tile0_w, &b->tile0_c, &b->queue, &b->err, &b->nk,
+    DBuf *bufs[] = { &b->jobs_wn, &b->jobs_ww, &b->jobs_c, &b->tile0_wn, &b->tile0_ww, &b->tile0_c, &b->queue,
+                     &b->err, &b->nk,
                      &b->evals };
     for (DBuf *d : bufs) d->release();
     for (int i = 0; i < 6; i++) if (b->ev[i]) cudaEventDestroy(b->ev[i]);

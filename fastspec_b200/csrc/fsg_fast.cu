@@ -23,6 +23,7 @@
 #include "fsg_mbar.cuh"
 
 #include <cub/device/device_scan.cuh>
+#include <cuda/functional>
 #include <algorithm>
 
 #define CLASS_W0 128      // class c: windows of at most CLASS_W0 * 2^(c+1) wavelengths
@@ -658,8 +659,8 @@ int fsg_fast_tiles(int nwl) { return (nwl + 31) / 32; }
 // scratch bytes of fsg_launch_tile_span for nb lines
 size_t fsg_tile_span_scratch(int64_t nb) {
     size_t t1 = 0, t2 = 0;
-    cub::DeviceScan::InclusiveScan(nullptr, t1, (const int *)nullptr, (int *)nullptr, cub::Max(), (int)nb);
-    cub::DeviceScan::InclusiveScan(nullptr, t2, (const int *)nullptr, (int *)nullptr, cub::Min(), (int)nb);
+    cub::DeviceScan::InclusiveScan(nullptr, t1, (const int *)nullptr, (int *)nullptr, cuda::maximum<>{}, (int)nb);
+    cub::DeviceScan::InclusiveScan(nullptr, t2, (const int *)nullptr, (int *)nullptr, cuda::minimum<>{}, (int)nb);
     return 4 * sizeof(int) * (size_t)nb + std::max(t1, t2) + 256;
 }
 
@@ -684,8 +685,8 @@ int fsg_launch_tile_span_tw(cudaStream_t s, int tw, int use_core, int nwl, int64
     void *tmp = (void *)(((uintptr_t)(V + nb) + 255) & ~(uintptr_t)255);
     size_t tb = scratch_bytes - ((char *)tmp - (char *)scratch);
     k_span_extract<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>((int)nb, use_core, hdr, right, revl);
-    if (cub::DeviceScan::InclusiveScan(tmp, tb, right, R, cub::Max(), (int)nb, s) != cudaSuccess) return FSG_E_CUDA;
-    if (cub::DeviceScan::InclusiveScan(tmp, tb, revl, V, cub::Min(), (int)nb, s) != cudaSuccess) return FSG_E_CUDA;
+    if (cub::DeviceScan::InclusiveScan(tmp, tb, right, R, cuda::maximum<>{}, (int)nb, s) != cudaSuccess) return FSG_E_CUDA;
+    if (cub::DeviceScan::InclusiveScan(tmp, tb, revl, V, cuda::minimum<>{}, (int)nb, s) != cudaSuccess) return FSG_E_CUDA;
     k_tile_search<<<(ntiles + 255) / 256, 256, 0, s>>>((int)nb, ntiles, tw, nwl, R, V, lo, hi);
     return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
 }
@@ -818,6 +819,141 @@ void fsg_launch_class_hist(cudaStream_t s, int64_t n, const int32_t *flags, cons
 int fsg_select_wide(cudaStream_t s, int64_t n, const int32_t *flags, int *counts, int64_t *offs, int64_t *out,
                     int64_t *d_total) {
     return fsg_select(s, n, flags, flags, flags, -2, counts, offs, out, d_total);
+}
+
+// ---- batched lists: records in window-width-class order --------------------------------------
+// An atmosphere of a batch keeps its candidate lines in one record array, grouped by window-width
+// class (retained lines of class 0, 1, ..., ncls - 1, then the rejected ones), in list (wavelength)
+// order inside each class.  A tile's candidate range is then searched inside one class, so it spans
+// lines of like width only: the prefix-max / suffix-min spans of a single list with a few very wide
+// windows would stage every line between such a window's centre and the tile.
+#define BCLS_MAX 24
+
+// class of a line for the record order: ncls for rejected lines (and empty windows)
+__device__ __forceinline__ int bclass_of(int f, int il, int ir, int ncls) {
+    if ((f & FSG_F_WEAK) || il > ir) return ncls;
+    return min(width_class(il, ir), ncls - 1);
+}
+
+// lines per class and CTA of SCAN_BS lines: counts[c * nblk + blk], c = 0 .. ncls
+__global__ void k_bclass_count(int64_t n, const int32_t *__restrict__ flags, const int32_t *__restrict__ il,
+                               const int32_t *__restrict__ ir, int ncls, int *counts) {
+    __shared__ int h[BCLS_MAX + 1];
+    for (int c = threadIdx.x; c <= ncls; c += blockDim.x) h[c] = 0;
+    __syncthreads();
+    const int64_t i = (int64_t)blockIdx.x * SCAN_BS + threadIdx.x;
+    if (i < n) atomicAdd(&h[bclass_of(flags[i], il[i], ir[i], ncls)], 1);
+    __syncthreads();
+    for (int c = threadIdx.x; c <= ncls; c += blockDim.x) counts[c * gridDim.x + blockIdx.x] = h[c];
+}
+
+// order[offs[c * nblk + blk] + rank of line i among the CTA's class-c lines] = i (stable)
+__global__ void k_bclass_scatter(int64_t n, const int32_t *__restrict__ flags, const int32_t *__restrict__ il,
+                                 const int32_t *__restrict__ ir, int ncls, const int64_t *__restrict__ offs,
+                                 int64_t *order) {
+    __shared__ int wc[SCAN_BS / 32][BCLS_MAX + 1];       // per warp and class: count, then prefix over warps
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int k = threadIdx.x; k < (SCAN_BS / 32) * (BCLS_MAX + 1); k += blockDim.x) (&wc[0][0])[k] = 0;
+    __syncthreads();
+    const int64_t i = (int64_t)blockIdx.x * SCAN_BS + threadIdx.x;
+    const int c = i < n ? bclass_of(flags[i], il[i], ir[i], ncls) : -1;
+    const unsigned same = __match_any_sync(0xffffffffu, c);
+    const int rank = __popc(same & ((1u << lane) - 1u));
+    if (c >= 0 && rank == 0) wc[w][c] = __popc(same);  // the class's lowest lane in the warp
+    __syncthreads();
+    if (threadIdx.x <= ncls) {
+        int acc = 0;
+        for (int q = 0; q < SCAN_BS / 32; q++) { const int t = wc[q][threadIdx.x]; wc[q][threadIdx.x] = acc; acc += t; }
+    }
+    __syncthreads();
+    if (c >= 0) order[offs[c * gridDim.x + blockIdx.x] + wc[w][c] + rank] = i;
+}
+
+// Class order of n lines (ncls <= BCLS_MAX classes + the rejected): order[n] and the class offsets,
+// class c starting at record offs[c * nblk] (nblk = ceil(n / SCAN_BS)); counts and offs hold
+// (ncls + 1) * nblk entries.
+int fsg_launch_bclass_order(cudaStream_t s, int64_t n, const int32_t *flags, const int32_t *il, const int32_t *ir,
+                            int ncls, int *counts, int64_t *offs, int64_t *total, int64_t *order) {
+    if (n <= 0 || ncls < 1 || ncls > BCLS_MAX) return n <= 0 ? FSG_OK : FSG_E_ARG;
+    const int nblk = (int)((n + SCAN_BS - 1) / SCAN_BS);
+    k_bclass_count<<<nblk, SCAN_BS, 0, s>>>(n, flags, il, ir, ncls, counts);
+    k_scan_counts<<<1, 1024, 0, s>>>((ncls + 1) * nblk, counts, offs, total);
+    k_bclass_scatter<<<nblk, SCAN_BS, 0, s>>>(n, flags, il, ir, ncls, offs, order);
+    return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
+}
+
+// classes of an atmosphere's order: every window fits the grid, so the widest class is that of nwl
+int fsg_bclass_count(int nwl) {
+    int c = 0;
+    while ((CLASS_W0 << (c + 1)) < nwl && c < 30) c++;
+    return std::min(c + 1, BCLS_MAX);
+}
+
+// Segmented spans: key = class << 32 | value, so one prefix max (of right + 1) and one suffix min
+// (of left) over the whole record array stay inside each class, and both key arrays are sorted.
+__global__ void k_bspan_extract(int nb, int use_core, const LineHdr *__restrict__ hdr,
+                                const int64_t *__restrict__ offs, int nblk, int ncls, unsigned long long *right,
+                                unsigned long long *rev_left) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nb) return;
+    int seg = 0;
+    while (seg < ncls && offs[(seg + 1) * nblk] <= j) seg++;
+    int l, r;
+    span_of(hdr[j], use_core, &l, &r);
+    if (seg == ncls) { l = 0x7fffffff; r = -1; }
+    right[j] = ((unsigned long long)seg << 32) | (unsigned)(r + 1);
+    rev_left[nb - 1 - j] = ((unsigned long long)seg << 32) | (unsigned)l;
+}
+
+// Tile t of class c (blockIdx.y): tiles of tw_n wavelengths for classes <= cnarrow, tw_w for the
+// others; lo/hi at c * tstride + t are record indices of class c (lo > hi: no line touches it).
+__global__ void k_btile_search(int nb, int cnarrow, int tw_n, int tw_w, int nwl, int tstride,
+                               const unsigned long long *__restrict__ R, const unsigned long long *__restrict__ V,
+                               int *lo, int *hi) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x, c = blockIdx.y;
+    const int tw = c <= cnarrow ? tw_n : tw_w;
+    if (t >= (nwl + tw - 1) / tw) return;
+    const int f = t * tw + 1, l = min(t * tw + tw, nwl);
+    const unsigned long long kf = ((unsigned long long)c << 32) | (unsigned)(f + 1);
+    const unsigned long long kl = ((unsigned long long)c << 32) | (unsigned)l;
+    int a = 0, b = nb;                                   // first j with R_j >= kf
+    while (a < b) { const int m = (a + b) >> 1; if (R[m] >= kf) b = m; else a = m + 1; }
+    const int jlo = a;
+    a = 0; b = nb;                                       // first j with S_j > kl, S_j = V[nb - 1 - j]
+    while (a < b) { const int m = (a + b) >> 1; if (V[nb - 1 - m] > kl) b = m; else a = m + 1; }
+    lo[c * tstride + t] = jlo;
+    hi[c * tstride + t] = a - 1;
+}
+
+size_t fsg_bspan_scratch(int64_t nb) {
+    size_t t1 = 0, t2 = 0;
+    typedef unsigned long long u64;
+    cub::DeviceScan::InclusiveScan(nullptr, t1, (const u64 *)nullptr, (u64 *)nullptr, cuda::maximum<>{}, (int)nb);
+    cub::DeviceScan::InclusiveScan(nullptr, t2, (const u64 *)nullptr, (u64 *)nullptr, cuda::minimum<>{}, (int)nb);
+    return 4 * sizeof(u64) * (size_t)nb + std::max(t1, t2) + 256;
+}
+
+// tile ranges of every class of a class-ordered record array (offs from fsg_launch_bclass_order)
+int fsg_launch_btile_span(cudaStream_t s, int use_core, int64_t nb, const LineHdr *hdr, const int64_t *offs,
+                          int ncls, int cnarrow, int tw_n, int tw_w, int nwl, int tstride, int *lo, int *hi,
+                          void *scratch, size_t scratch_bytes) {
+    typedef unsigned long long u64;
+    if (nb <= 0) {
+        for (int c = 0; c < ncls; c++) k_tile_reset<<<(tstride + 255) / 256, 256, 0, s>>>(tstride, lo + c * tstride,
+                                                                                          hi + c * tstride);
+        return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
+    }
+    const int nblk = (int)((nb + SCAN_BS - 1) / SCAN_BS);
+    u64 *right = (u64 *)scratch, *revl = right + nb, *R = revl + nb, *V = R + nb;
+    void *tmp = (void *)(((uintptr_t)(V + nb) + 255) & ~(uintptr_t)255);
+    size_t tb = scratch_bytes - ((char *)tmp - (char *)scratch);
+    k_bspan_extract<<<(unsigned)((nb + 255) / 256), 256, 0, s>>>((int)nb, use_core, hdr, offs, nblk, ncls, right, revl);
+    if (cub::DeviceScan::InclusiveScan(tmp, tb, right, R, cuda::maximum<>{}, (int)nb, s) != cudaSuccess) return FSG_E_CUDA;
+    if (cub::DeviceScan::InclusiveScan(tmp, tb, revl, V, cuda::minimum<>{}, (int)nb, s) != cudaSuccess) return FSG_E_CUDA;
+    const int tmax = (nwl + std::min(tw_n, tw_w) - 1) / std::min(tw_n, tw_w);
+    k_btile_search<<<dim3((tmax + 255) / 256, ncls), 256, 0, s>>>((int)nb, cnarrow, tw_n, tw_w, nwl, tstride, R, V,
+                                                                  lo, hi);
+    return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
 }
 
 // Gather the retained lines' SoA fields and per-line outputs into packed arrays (PACK,

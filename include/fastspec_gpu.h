@@ -344,15 +344,17 @@ int fsg_set_fault(fsg_ctx *ctx, int kind, double value);
  * range (ReadHDF, ioutils.f90:752-753; ReadAscMag, ioutils.f90:1496-1497), so each atmosphere's
  * result is the reference's run of its deck on the shared list; margin > 0 adds the lines just
  * outside, whose windows the reference's WaveIdx clamps to the grid's ends (opacity.f90:594-608).
- * Then one persistent wing-pass launch and
- * one persistent core-pass launch take (atmosphere, tile) items from device work queues, then the
- * formal solver and flux run per atmosphere.  The sequence has no host synchronisation; the
+ * Each atmosphere's records are grouped by window-width class; atmospheres are grouped by depth
+ * count (buckets of 8).  Per group, persistent wing-pass launches (narrow classes, wide classes) and
+ * a persistent core-pass launch take (atmosphere and class, tile) items from device work queues;
+ * then the formal solver and flux run per atmosphere.  The sequence has no host synchronisation; the
  * first fsg_batch_run tunes it (unless fsg_batch_set_tuning gave a choice), captures it as a CUDA
  * graph and replays it; later runs replay.  No counterpart in the reference, which synthesises
  * one atmosphere per run (fastspec.f90:192-449). */
 typedef struct fsg_batch fsg_batch;
 typedef struct {
-    int32_t tile_pix;       /* wing-pass tile width: 64 or 128 wavelengths */
+    int32_t tile_pix;       /* wing-pass tile width of the wide classes (windows over 512
+                             * wavelengths): 64 or 128; the narrower ones take 64 */
     int32_t wing_ctas, core_ctas;   /* CTAs of the persistent wing / core launches */
     double  ms_wing, ms_core;       /* their times in the tuning run [ms] */
 } fsg_batch_tuning;
