@@ -269,6 +269,7 @@ def batched_grid(F, torch, dev, natm, nlines, steps, warmup):
            "spectra_per_s": natm / (ms / 1e3), "line_evals_per_s": st["line_evals"] / (ms / 1e3),
            "ms_per_batch": ms, "line_evals": st["line_evals"], "candidate_lines": st["nlines_candidate"],
            "tuning": tuning, "tuning_s": tune_s, "graph": True,
+           "replay_stages_ms": {k: st[k] for k in ("ms_prepare", "ms_wing", "ms_core", "ms_solve")},
            "sequential_line_ms": t_seq,
            "plain_fp64_sample": {"atmospheres": len(samp), "spectra_per_s": fp64_sps,
                                  "ms_line_per_atmosphere": t64 / len(samp)},

@@ -2259,7 +2259,9 @@ struct fsg_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     double line_evals = 0.0;
-    cudaEvent_t ev[6] = { nullptr, nullptr, nullptr, nullptr, nullptr, nullptr };
+    // ev[0..2]: around the wing and core launches; ev[3], ev[4]: around a replay; ev[5..7]: the
+    // replay's stage boundaries (before the central pass, after the core launches, after the solver)
+    cudaEvent_t ev[8] = {};
 };
 
 static LineView batch_view(const fsg_batch *b, const BAtm &a) {
@@ -2368,8 +2370,11 @@ static int batch_jobs(fsg_batch *b, int P) {
     return FSG_OK;
 }
 
-// accumulation (zeroed LineOpac, the two persistent launches), then solver and flux per atmosphere;
-// ev: optional events around the wing and core launches
+// an event record that a stream capture keeps as an event-record node of the graph (timed replays)
+static void batch_mark(cudaEvent_t e, cudaStream_t s) { cudaEventRecordWithFlags(e, s, cudaEventRecordExternal); }
+
+// accumulation (zeroed LineOpac, the persistent launches), then solver and flux per atmosphere;
+// ev: optional events around the wing and core launches (ev[0..2]) and after the solver (ev[7])
 static int batch_accumulate_solve(fsg_batch *b, const fsg_batch_tuning &t, cudaEvent_t *ev) {
     fsg_ctx *ctx = b->own;
     cudaStream_t s = ctx->stream;
@@ -2382,7 +2387,7 @@ static int batch_accumulate_solve(fsg_batch *b, const fsg_batch_tuning &t, cudaE
     unsigned *q = b->queue.as<unsigned>();
     // every group's wing launches (narrow classes, then wide classes: both read-modify-write LineOpac),
     // then every group's core launch
-    if (ev) cudaEventRecord(ev[0], s);
+    if (ev) batch_mark(ev[0], s);
     for (size_t gi = 0; gi < ng; gi++) {
         const fsg_batch::Group &g = b->groups[gi];
         if (g.njn && fsg_launch_accum_batch(s, 2, g.ntau_max, b->jobs_wn.as<WingJob>() + g.jn0,
@@ -2394,7 +2399,7 @@ static int batch_accumulate_solve(fsg_batch *b, const fsg_batch_tuning &t, cudaE
                                             b->err.as<int>()))
             return cuda_fail(ctx, cudaGetLastError(), "k_accum_batch (wide classes)");
     }
-    if (ev) cudaEventRecord(ev[1], s);
+    if (ev) batch_mark(ev[1], s);
     for (size_t gi = 0; gi < ng; gi++) {
         const fsg_batch::Group &g = b->groups[gi];
         if (g.njc && fsg_launch_core_batch(s, g.ntau_max, b->jobs_c.as<CoreJob>() + g.jc0, b->tile0_c.as<int>() + g.tc0,
@@ -2402,7 +2407,7 @@ static int batch_accumulate_solve(fsg_batch *b, const fsg_batch_tuning &t, cudaE
                                            b->err.as<int>()))
             return cuda_fail(ctx, cudaGetLastError(), "k_core_batch");
     }
-    if (ev) cudaEventRecord(ev[2], s);
+    if (ev) batch_mark(ev[2], s);
     for (auto &a : b->atm) {
         fsg_ctx *c = a.ctx;
         if (fsg_launch_radtran(s, fsg_view(c), c->d_lineopac.as<double>(), c->d_rhox.as<double>(), c->nmu,
@@ -2410,6 +2415,7 @@ static int batch_accumulate_solve(fsg_batch *b, const fsg_batch_tuning &t, cudaE
                                a.sfc.as<double>()))
             return cuda_fail(ctx, cudaGetLastError(), "k_radtran (batch)");
     }
+    if (ev && ev[7]) batch_mark(ev[7], s);
     CK(cudaGetLastError(), "batch");
     return FSG_OK;
 }
@@ -2482,7 +2488,7 @@ int fsg_batch_create(fsg_ctx *const *atms, int natm, const fsg_lines *lines, dou
     if (b->err.ensure(sizeof(int)) || b->nk.ensure(sizeof(unsigned long long)))
         return bail(FSG_E_NOMEM, "fsg_batch_create: device allocation failed");
     if (cudaMemset(b->err.p, 0, sizeof(int)) != cudaSuccess) return bail(FSG_E_CUDA, "fsg_batch_create: upload failed");
-    for (int i = 0; i < 6; i++) cudaEventCreate(&b->ev[i]);
+    for (int i = 0; i < 8; i++) cudaEventCreate(&b->ev[i]);
     b->tune.tile_pix = 128;
     b->tune.wing_ctas = 148;
     b->tune.core_ctas = 4 * 148;
@@ -2581,8 +2587,9 @@ int fsg_batch_run(fsg_batch *b, fsg_batch_stats *st) {
         CK(cudaStreamSynchronize(s), "batch");
         batch_count(b);
         CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "graph capture");
+        batch_mark(b->ev[5], s);                        // event-record nodes: the replay's stage times
         rc = batch_prepare(b, P);
-        if (!rc) rc = batch_accumulate_solve(b, b->tune, nullptr);
+        if (!rc) rc = batch_accumulate_solve(b, b->tune, b->ev);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(s, &g);
         if (rc) { if (g) cudaGraphDestroy(g); return rc; }
@@ -2602,6 +2609,12 @@ int fsg_batch_run(fsg_batch *b, fsg_batch_stats *st) {
         float ms = 0;
         cudaEventElapsedTime(&ms, b->ev[3], b->ev[4]);
         st->ms_total = ms;
+        float m0 = 0, m1 = 0, m2 = 0, m3 = 0;
+        cudaEventElapsedTime(&m0, b->ev[5], b->ev[0]);
+        cudaEventElapsedTime(&m1, b->ev[0], b->ev[1]);
+        cudaEventElapsedTime(&m2, b->ev[1], b->ev[2]);
+        cudaEventElapsedTime(&m3, b->ev[2], b->ev[7]);
+        st->ms_prepare = m0; st->ms_wing = m1; st->ms_core = m2; st->ms_solve = m3;
         st->line_evals = b->line_evals;
         for (auto &a : b->atm) st->nlines_candidate += a.cn;
         st->natm = (int)b->atm.size();
@@ -2639,7 +2652,7 @@ void fsg_batch_destroy(fsg_batch *b) {
                      &b->err, &b->nk,
                      &b->evals };
     for (DBuf *d : bufs) d->release();
-    for (int i = 0; i < 6; i++) if (b->ev[i]) cudaEventDestroy(b->ev[i]);
+    for (int i = 0; i < 8; i++) if (b->ev[i]) cudaEventDestroy(b->ev[i]);
     fsg_destroy(b->own);
     cudaGetLastError();
     delete b;

@@ -93,6 +93,8 @@ struct WingJob {
 
 // shared memory of the wing pass for at most ntau_max depths:
 // wing records [2][CH][ntau_max] | headers [2][CH] | mbarriers [2] | Kahan pairs [D * P][blockDim.x]
+// (a warp reads up to D - 1 <= 7 records past its line's last depth: at most 112 bytes past the
+// second record buffer, inside the 2 KB of headers that follow it)
 __host__ __device__ inline size_t wing_smem_recs(int ntau_max) {
     return sizeof(WingRec) * 2 * CH * (size_t)ntau_max + sizeof(LineHdr) * 2 * CH;
 }
@@ -167,9 +169,12 @@ __device__ __forceinline__ bool wing_tile(const WingJob &J, int tile, unsigned c
                     float dl = (wvh[k] - h.wlh) + (wvl[k] - h.wll);
                     x[k] = dl * dl;
                 }
+                // depths past the job's last (last warp only) read the next records of the buffer, or
+                // the headers after it: their partials are never stored
+                const WingRec *wq = cw + q * ntau + t0;
                 WingRec w[D];
 #pragma unroll
-                for (int d = 0; d < D; d++) w[d] = cw[q * ntau + t0 + min(d, nd - 1)];
+                for (int d = 0; d < D; d++) w[d] = wq[d];
                 const bool core_hit = h.cl <= h.cr && h.cr >= tile_first && h.cl <= tile_last;
                 const bool full = h.ileft <= tile_first && h.iright >= tile_last && !core_hit;
                 if (!full) {

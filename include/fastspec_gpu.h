@@ -364,6 +364,9 @@ typedef struct {
     double  line_evals;             /* profile evaluations inside windows (sum) */
     double  ms_total;               /* device time of one graph replay [ms] */
     fsg_batch_tuning tuning;
+    double  ms_prepare, ms_wing, ms_core, ms_solve;   /* its stages: central pass, class order, records
+                                                       * and tile ranges; wing launches; core launches;
+                                                       * formal solver and flux [ms] */
 } fsg_batch_stats;
 /* On failure *out stays NULL and fsg_batch_last_error(NULL) gives the reason. */
 int  fsg_batch_create(fsg_ctx *const *atms, int natm, const fsg_lines *lines, double margin, fsg_batch **out);
