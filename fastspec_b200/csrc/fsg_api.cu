@@ -2370,8 +2370,14 @@ static int batch_jobs(fsg_batch *b, int P) {
     return FSG_OK;
 }
 
-// an event record that a stream capture keeps as an event-record node of the graph (timed replays)
-static void batch_mark(cudaEvent_t e, cudaStream_t s) { cudaEventRecordWithFlags(e, s, cudaEventRecordExternal); }
+// an event record; inside a stream capture it becomes an event-record node of the graph (timed
+// replays), which only the external flag gives, and that flag is refused outside a capture
+static void batch_mark(cudaEvent_t e, cudaStream_t s) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &cs);
+    if (cs == cudaStreamCaptureStatusActive) cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+    else cudaEventRecord(e, s);
+}
 
 // accumulation (zeroed LineOpac, the persistent launches), then solver and flux per atmosphere;
 // ev: optional events around the wing and core launches (ev[0..2]) and after the solver (ev[7])
