@@ -2228,9 +2228,9 @@ static int adjoint_common(fsg_ctx *ctx, const fsg_lines *d_lines, const int32_t 
 // Batched synthesis: many atmospheres (each an fsg_ctx with grid, atmosphere, continuum and mu
 // set), one shared line list.  Per atmosphere: central pass of the lines in its span (plus a
 // margin), their records in window-width-class order (block refill), tile ranges per class; then
-// two persistent wing-pass launches (narrow classes, wide classes) and one persistent core-pass
-// launch take (atmosphere and class, tile) items from device work queues; then the formal solver
-// and flux of each atmosphere.  The whole sequence has no host synchronisation and is captured
+// per group of atmospheres of like depth count and per class, a persistent wing-pass launch and a
+// persistent core-pass launch take (atmosphere, tile) items from device work queues; then the formal
+// solver and flux of each atmosphere.  The whole sequence has no host synchronisation and is captured
 // once as a CUDA graph; later runs replay it.  The wide classes' tile width and the CTA counts of
 // the persistent launches are chosen by timing the candidates on the first run (fsg_batch_tune).
 // ================================================================================================
@@ -2248,12 +2248,12 @@ struct fsg_batch {
     std::vector<BAtm> atm;
     fsg_lines dlines{};
     int ntau_max = 0;
-    // atmospheres grouped by depth count: each group's launches are shaped for its deepest member;
-    // per group, the offsets of its jobs (narrow-class wing, wide-class wing, core) in the job arrays and
-    // of its queue prefix sums (each starting at 0) in the tile0 arrays
-    struct Group { int ntau_max, jn0, njn, jw0, njw, jc0, njc, tn0, tw0, tc0; };
-    std::vector<Group> groups;
-    DBuf jobs_wn, jobs_ww, jobs_c, tile0_wn, tile0_ww, tile0_c, queue, err, nk, evals;
+    // one persistent launch per (depth group, window class) and pass: its jobs (one per atmosphere,
+    // so no two CTAs of a launch update the same LineOpac) at j0 in the pass's job array, its queue
+    // prefix sums (starting at 0) at t0 in the pass's tile0 array; P wavelengths per lane (wing)
+    struct Launch { int ntau_max, P, j0, nj, t0; };
+    std::vector<Launch> lw, lc;
+    DBuf jobs_w, jobs_c, tile0_w, tile0_c, queue, err, nk, evals;
     fsg_batch_tuning tune{};
     int tuned = 0;
     cudaGraph_t graph = nullptr;
@@ -2311,60 +2311,56 @@ static int batch_prepare(fsg_batch *b, int P) {
 
 // Job tables and queue prefix sums (host, then uploaded).  Atmospheres are grouped by depth count
 // (buckets of 8 depths), so a persistent launch is shaped for its own group's deepest member and few
-// warps idle.  Per group: one job per (atmosphere, class), the wing jobs of the narrow classes
-// (64-wavelength tiles) and of the wide ones (32 P) in two launches, the core jobs in a third; jobs run
-// widest class first, so the longest tiles start early and the queue ends on short ones.
+// warps idle.  Per group and window class (widest first) one wing launch (64-wavelength tiles for
+// the narrow classes, 32 P for the others) and one core launch, each with one job per atmosphere: the
+// classes of an atmosphere add into the same LineOpac tiles, so they go to successive launches.
 static int batch_jobs(fsg_batch *b, int P) {
     fsg_ctx *ctx = b->own;
-    std::vector<WingJob> jn, jw; std::vector<CoreJob> jc;
-    std::vector<int> tn, tw, tc;
-    b->groups.clear();
+    std::vector<WingJob> jw; std::vector<CoreJob> jc;
+    std::vector<int> tw, tc;
+    b->lw.clear(); b->lc.clear();
     for (int bucket = 0; bucket * 8 < 128; bucket++) {
-        fsg_batch::Group g{ 0, (int)jn.size(), 0, (int)jw.size(), 0, (int)jc.size(), 0, (int)tn.size(),
-                            (int)tw.size(), (int)tc.size() };
-        int cmax = 0;
+        int cmax = 0, ntmax = 0;
         for (auto &a : b->atm)
             if (a.cn && (a.ctx->ntau - 1) / 8 == bucket) {
                 cmax = std::max(cmax, a.ncls);
-                g.ntau_max = std::max(g.ntau_max, a.ctx->ntau);
+                ntmax = std::max(ntmax, a.ctx->ntau);
             }
-        if (!g.ntau_max) continue;
-        tn.push_back(0); tw.push_back(0); tc.push_back(0);
-        for (int cls = cmax - 1; cls >= 0; cls--)
+        for (int cls = cmax - 1; cls >= 0; cls--) {
+            const int Pc = cls <= BATCH_NARROW ? 2 : P;
+            fsg_batch::Launch w{ ntmax, Pc, (int)jw.size(), 0, (int)tw.size() };
+            fsg_batch::Launch k{ ntmax, 1, (int)jc.size(), 0, (int)tc.size() };
+            tw.push_back(0); tc.push_back(0);
             for (auto &a : b->atm) {
                 fsg_ctx *c = a.ctx;
                 if (a.cn == 0 || (c->ntau - 1) / 8 != bucket || cls >= a.ncls) continue;
                 const int ws = batch_wing_stride(c), cs = batch_core_stride(c);
-                const WingJob J{ c->ntau, c->nwl, c->d_wave.as<double>(), a.hdr.as<LineHdr>(), a.wing.as<WingRec>(),
-                                 a.wtlo.as<int>() + (size_t)cls * ws, a.wthi.as<int>() + (size_t)cls * ws,
-                                 c->d_lineopac.as<double>(), 0u, WAIT_NS };
-                if (cls <= BATCH_NARROW) { jn.push_back(J); tn.push_back(tn.back() + (c->nwl + 63) / 64); }
-                else { jw.push_back(J); tw.push_back(tw.back() + (c->nwl + 32 * P - 1) / (32 * P)); }
+                jw.push_back(WingJob{ c->ntau, c->nwl, c->d_wave.as<double>(), a.hdr.as<LineHdr>(), a.wing.as<WingRec>(),
+                                      a.wtlo.as<int>() + (size_t)cls * ws, a.wthi.as<int>() + (size_t)cls * ws,
+                                      c->d_lineopac.as<double>(), 0u, WAIT_NS });
+                tw.push_back(tw.back() + (c->nwl + 32 * Pc - 1) / (32 * Pc));
                 jc.push_back(CoreJob{ c->ntau, c->nwl, c->d_wave.as<double>(), a.hdr.as<LineHdr>(),
                                       a.wing.as<WingRec>(), a.core.as<CoreRec>(), a.ctlo.as<int>() + (size_t)cls * cs,
                                       a.cthi.as<int>() + (size_t)cls * cs, c->d_lineopac.as<double>(), nullptr, 0u,
                                       WAIT_NS });
                 tc.push_back(tc.back() + (c->nwl + 31) / 32);
             }
-        g.njn = (int)jn.size() - g.jn0; g.njw = (int)jw.size() - g.jw0; g.njc = (int)jc.size() - g.jc0;
-        b->groups.push_back(g);
+            w.nj = (int)jw.size() - w.j0; k.nj = (int)jc.size() - k.j0;
+            if (w.nj) { b->lw.push_back(w); b->lc.push_back(k); }
+        }
     }
-    ALLOC(b->jobs_wn, sizeof(WingJob) * std::max<size_t>(jn.size(), 1));
-    ALLOC(b->jobs_ww, sizeof(WingJob) * std::max<size_t>(jw.size(), 1));
+    ALLOC(b->jobs_w, sizeof(WingJob) * std::max<size_t>(jw.size(), 1));
     ALLOC(b->jobs_c, sizeof(CoreJob) * std::max<size_t>(jc.size(), 1));
-    ALLOC(b->tile0_wn, sizeof(int) * std::max<size_t>(tn.size(), 1));
-    ALLOC(b->tile0_ww, sizeof(int) * std::max<size_t>(tw.size(), 1));
+    ALLOC(b->tile0_w, sizeof(int) * std::max<size_t>(tw.size(), 1));
     ALLOC(b->tile0_c, sizeof(int) * std::max<size_t>(tc.size(), 1));
-    ALLOC(b->queue, 3 * sizeof(unsigned) * std::max<size_t>(b->groups.size(), 1));
+    ALLOC(b->queue, 2 * sizeof(unsigned) * std::max<size_t>(b->lw.size(), 1));
     cudaStream_t s = ctx->stream;
     auto up = [&](DBuf &d, const void *h, size_t nb) {
         return nb ? cudaMemcpyAsync(d.p, h, nb, cudaMemcpyHostToDevice, s) : cudaSuccess;
     };
-    CK(up(b->jobs_wn, jn.data(), sizeof(WingJob) * jn.size()), "jobs");
-    CK(up(b->jobs_ww, jw.data(), sizeof(WingJob) * jw.size()), "jobs");
+    CK(up(b->jobs_w, jw.data(), sizeof(WingJob) * jw.size()), "jobs");
     CK(up(b->jobs_c, jc.data(), sizeof(CoreJob) * jc.size()), "jobs");
-    CK(up(b->tile0_wn, tn.data(), sizeof(int) * tn.size()), "jobs");
-    CK(up(b->tile0_ww, tw.data(), sizeof(int) * tw.size()), "jobs");
+    CK(up(b->tile0_w, tw.data(), sizeof(int) * tw.size()), "jobs");
     CK(up(b->tile0_c, tc.data(), sizeof(int) * tc.size()), "jobs");
     CK(cudaStreamSynchronize(s), "jobs");
     return FSG_OK;
@@ -2388,29 +2384,22 @@ static int batch_accumulate_solve(fsg_batch *b, const fsg_batch_tuning &t, cudaE
         fsg_ctx *c = a.ctx;
         CK(cudaMemsetAsync(c->d_lineopac.p, 0, sizeof(double) * (size_t)c->nwl * c->ntau, s), "batch reset");
     }
-    const size_t ng = b->groups.size();
-    CK(cudaMemsetAsync(b->queue.p, 0, 3 * sizeof(unsigned) * std::max<size_t>(ng, 1), s), "queue reset");
+    const size_t nl = b->lw.size();
+    CK(cudaMemsetAsync(b->queue.p, 0, 2 * sizeof(unsigned) * std::max<size_t>(nl, 1), s), "queue reset");
     unsigned *q = b->queue.as<unsigned>();
-    // every group's wing launches (narrow classes, then wide classes: both read-modify-write LineOpac),
-    // then every group's core launch
+    // the wing launches (each read-modify-writes its atmospheres' LineOpac tiles), then the core ones
     if (ev) batch_mark(ev[0], s);
-    for (size_t gi = 0; gi < ng; gi++) {
-        const fsg_batch::Group &g = b->groups[gi];
-        if (g.njn && fsg_launch_accum_batch(s, 2, g.ntau_max, b->jobs_wn.as<WingJob>() + g.jn0,
-                                            b->tile0_wn.as<int>() + g.tn0, g.njn, t.wing_ctas, q + 3 * gi,
-                                            b->err.as<int>()))
-            return cuda_fail(ctx, cudaGetLastError(), "k_accum_batch (narrow classes)");
-        if (g.njw && fsg_launch_accum_batch(s, t.tile_pix / 32, g.ntau_max, b->jobs_ww.as<WingJob>() + g.jw0,
-                                            b->tile0_ww.as<int>() + g.tw0, g.njw, t.wing_ctas, q + 3 * gi + 1,
-                                            b->err.as<int>()))
-            return cuda_fail(ctx, cudaGetLastError(), "k_accum_batch (wide classes)");
+    for (size_t i = 0; i < nl; i++) {
+        const fsg_batch::Launch &L = b->lw[i];
+        if (fsg_launch_accum_batch(s, L.P, L.ntau_max, b->jobs_w.as<WingJob>() + L.j0, b->tile0_w.as<int>() + L.t0,
+                                   L.nj, t.wing_ctas, q + 2 * i, b->err.as<int>()))
+            return cuda_fail(ctx, cudaGetLastError(), "k_accum_batch");
     }
     if (ev) batch_mark(ev[1], s);
-    for (size_t gi = 0; gi < ng; gi++) {
-        const fsg_batch::Group &g = b->groups[gi];
-        if (g.njc && fsg_launch_core_batch(s, g.ntau_max, b->jobs_c.as<CoreJob>() + g.jc0, b->tile0_c.as<int>() + g.tc0,
-                                           g.njc, t.core_ctas, b->atm[0].ctx->tab.vtab4, q + 3 * gi + 2,
-                                           b->err.as<int>()))
+    for (size_t i = 0; i < nl; i++) {
+        const fsg_batch::Launch &L = b->lc[i];
+        if (fsg_launch_core_batch(s, L.ntau_max, b->jobs_c.as<CoreJob>() + L.j0, b->tile0_c.as<int>() + L.t0, L.nj,
+                                  t.core_ctas, b->atm[0].ctx->tab.vtab4, q + 2 * i + 1, b->err.as<int>()))
             return cuda_fail(ctx, cudaGetLastError(), "k_core_batch");
     }
     if (ev) batch_mark(ev[2], s);
@@ -2654,8 +2643,7 @@ void fsg_batch_destroy(fsg_batch *b) {
                          &a.span, &a.sfl, &a.sfc, &a.order, &a.ccnt, &a.coff, &a.ctot };
         for (DBuf *d : bufs) d->release();
     }
-    DBuf *bufs[] = { &b->jobs_wn, &b->jobs_ww, &b->jobs_c, &b->tile0_wn, &b->tile0_ww, &b->tile0_c, &b->queue,
-                     &b->err, &b->nk,
+    DBuf *bufs[] = { &b->jobs_w, &b->jobs_c, &b->tile0_w, &b->tile0_c, &b->queue, &b->err, &b->nk,
                      &b->evals };
     for (DBuf *d : bufs) d->release();
     for (int i = 0; i < 8; i++) if (b->ev[i]) cudaEventDestroy(b->ev[i]);
