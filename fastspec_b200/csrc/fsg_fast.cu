@@ -61,12 +61,6 @@ __device__ __forceinline__ void stage_chunk(int c, int lo, int hi, int ntau, con
     tma_bulk_g2s(shdr, hdr + j0, bhdr, bar);
 }
 
-// The line's window covers tiles [first, last] whole and its core range misses them: every point
-// takes the wing form, with no mask.
-__device__ __forceinline__ bool wing_only(const LineHdr &h, int first, int last) {
-    return h.ileft <= first && h.iright >= last && !(h.cl <= h.cr && h.cr >= first && h.cl <= last);
-}
-
 __device__ __forceinline__ float rcp_approx(float x) {
     float r;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
@@ -169,49 +163,6 @@ __device__ __forceinline__ bool wing_tile(const WingJob &J, int tile, unsigned c
             for (int q = 0; q < n; q++) {
                 const LineHdr h = ch[q];
                 if (h.iright < tile_first || h.ileft > tile_last) continue;   // window misses the tile
-                if (q + 1 < n && wing_only(h, tile_first, tile_last) && wing_only(ch[q + 1], tile_first, tile_last)) {
-                    // two lines whose windows cover the tile outside their core ranges: one reciprocal
-                    // per pair of terms, 1 / den1 = den2 / (den1 den2) and 1 / den2 = den1 / (den1 den2)
-                    const LineHdr h2 = ch[q + 1];
-                    float x1[P], x2[P];
-#pragma unroll
-                    for (int k = 0; k < P; k++) {
-                        const float d1 = (wvh[k] - h.wlh) + (wvl[k] - h.wll);
-                        const float d2 = (wvh[k] - h2.wlh) + (wvl[k] - h2.wll);
-                        x1[k] = d1 * d1;
-                        x2[k] = d2 * d2;
-                    }
-                    const WingRec *wq1 = cw + q * ntau + t0, *wq2 = wq1 + ntau;
-#pragma unroll
-                    for (int d = 0; d < D; d++) {
-                        const WingRec u = wq1[d], v = wq2[d];
-#pragma unroll
-                        for (int k = 0; k < P; k++) {
-                            const float t1 = fmaf(x1[k], u.vv2, u.c2m1), t2 = fmaf(x2[k], v.vv2, v.c2m1);
-                            const float den1 = fmaf(t1, t1, u.twoA), den2 = fmaf(t2, t2, v.twoA);
-                            const float num1 = fmaf(u.c1, t1, u.c1), num2 = fmaf(v.c1, t2, v.c1);
-                            const float r = rcp_approx(den1 * den2);
-                            part[d][k] = fmaf(num1, den2 * r, part[d][k]);
-                            part[d][k] = fmaf(num2, den1 * r, part[d][k]);
-                        }
-                    }
-                    q++;
-                    nfold += 2;
-                    if (nfold >= FOLD) {
-                        nfold = 0;
-#pragma unroll
-                        for (int d = 0; d < D; d++)
-#pragma unroll
-                            for (int k = 0; k < P; k++) {
-                                float2 &qq = ksum[(d * P + k) * nth + threadIdx.x];
-                                float2 sc = qq;
-                                KAHAN(sc.x, sc.y, part[d][k]);
-                                qq = sc;
-                                part[d][k] = 0.0f;
-                            }
-                    }
-                    continue;
-                }
                 float x[P];
 #pragma unroll
                 for (int k = 0; k < P; k++) {
@@ -259,7 +210,7 @@ __device__ __forceinline__ bool wing_tile(const WingJob &J, int tile, unsigned c
                             part[d][k] = fmaf(num, rcp_approx(den), part[d][k]);
                         }
                 }
-                if (++nfold >= FOLD) {
+                if (++nfold == FOLD) {
                     nfold = 0;
 #pragma unroll
                     for (int d = 0; d < D; d++)
