@@ -270,6 +270,7 @@ def batched_grid(F, torch, dev, natm, nlines, steps, warmup):
            "ms_per_batch": ms, "line_evals": st["line_evals"], "candidate_lines": st["nlines_candidate"],
            "tuning": tuning, "tuning_s": tune_s, "graph": True,
            "replay_stages_ms": {k: st[k] for k in ("ms_prepare", "ms_wing", "ms_core", "ms_solve")},
+           "core_evals": st["core_evals"],
            "sequential_line_ms": t_seq,
            "plain_fp64_sample": {"atmospheres": len(samp), "spectra_per_s": fp64_sps,
                                  "ms_line_per_atmosphere": t64 / len(samp)},

@@ -64,7 +64,8 @@ class BatchTuning(C.Structure):
 class BatchStats(C.Structure):
     _fields_ = [("natm", C.c_int32), ("nlines_candidate", C.c_int64), ("line_evals", C.c_double),
                 ("ms_total", C.c_double), ("tuning", BatchTuning), ("ms_prepare", C.c_double),
-                ("ms_wing", C.c_double), ("ms_core", C.c_double), ("ms_solve", C.c_double)]
+                ("ms_wing", C.c_double), ("ms_core", C.c_double), ("ms_solve", C.c_double),
+                ("core_evals", C.c_double)]
 
     def asdict(self):
         d = {f: getattr(self, f) for f, _ in self._fields_ if f != "tuning"}

@@ -56,11 +56,6 @@ int fsg_launch_accum_fast(cudaStream_t, int, int, int, const double *, const Lin
 int fsg_launch_core_fast(cudaStream_t, int, int, const double *, const LineHdr *, const WingRec *, const CoreRec *,
                          const int *, const int *, const float4 *, double *, unsigned long long *, int *, unsigned,
                          unsigned long long);
-struct WingJob { int ntau, nwl; const double *wave; const LineHdr *hdr; const WingRec *wing;
-                 const int *tile_lo, *tile_hi; double *lineopac; unsigned extra_tx; unsigned long long wait_ns; };
-struct CoreJob { int ntau, nwl; const double *wave; const LineHdr *hdr; const WingRec *wing; const CoreRec *core;
-                 const int *tile_lo, *tile_hi; double *lineopac; unsigned long long *nevals; unsigned extra_tx;
-                 unsigned long long wait_ns; };
 int fsg_launch_accum_batch(cudaStream_t, int, int, const WingJob *, const int *, int, int, unsigned *, int *);
 int fsg_launch_core_batch(cudaStream_t, int, const CoreJob *, const int *, int, int, const float4 *, unsigned *,
                           int *);
@@ -2248,9 +2243,9 @@ struct fsg_batch {
     std::vector<BAtm> atm;
     fsg_lines dlines{};
     int ntau_max = 0;
-    // one persistent launch per (depth group, window class) and pass: its jobs (one per atmosphere,
-    // so no two CTAs of a launch update the same LineOpac) at j0 in the pass's job array, its queue
-    // prefix sums (starting at 0) at t0 in the pass's tile0 array; P wavelengths per lane (wing)
+    // persistent launches (wing: lw, core: lc): a launch's jobs (one per atmosphere, so no two CTAs of
+    // it update the same LineOpac tile) at j0 in its pass's job array, its queue prefix sums (starting
+    // at 0) at t0 in the pass's tile0 array; P wavelengths per lane (wing)
     struct Launch { int ntau_max, P, j0, nj, t0; };
     std::vector<Launch> lw, lc;
     DBuf jobs_w, jobs_c, tile0_w, tile0_c, queue, err, nk, evals;
@@ -2311,49 +2306,55 @@ static int batch_prepare(fsg_batch *b, int P) {
 
 // Job tables and queue prefix sums (host, then uploaded).  Atmospheres are grouped by depth count
 // (buckets of 8 depths), so a persistent launch is shaped for its own group's deepest member and few
-// warps idle.  Per group and window class (widest first) one wing launch (64-wavelength tiles for
-// the narrow classes, 32 P for the others) and one core launch, each with one job per atmosphere: the
-// classes of an atmosphere add into the same LineOpac tiles, so they go to successive launches.
+// warps idle.  Per group three launches, each with one job per atmosphere (so no two CTAs of a launch
+// update the same LineOpac tile): the wing pass over the narrow classes (64-wavelength tiles), the
+// wing pass over the wide ones (32 P), the core pass over all; a job's tile takes its classes' lines
+// in turn into one sum.
 static int batch_jobs(fsg_batch *b, int P) {
     fsg_ctx *ctx = b->own;
     std::vector<WingJob> jw; std::vector<CoreJob> jc;
     std::vector<int> tw, tc;
     b->lw.clear(); b->lc.clear();
     for (int bucket = 0; bucket * 8 < 128; bucket++) {
-        int cmax = 0, ntmax = 0;
+        int ntmax = 0;
         for (auto &a : b->atm)
-            if (a.cn && (a.ctx->ntau - 1) / 8 == bucket) {
-                cmax = std::max(cmax, a.ncls);
-                ntmax = std::max(ntmax, a.ctx->ntau);
-            }
-        for (int cls = cmax - 1; cls >= 0; cls--) {
-            const int Pc = cls <= BATCH_NARROW ? 2 : P;
-            fsg_batch::Launch w{ ntmax, Pc, (int)jw.size(), 0, (int)tw.size() };
-            fsg_batch::Launch k{ ntmax, 1, (int)jc.size(), 0, (int)tc.size() };
-            tw.push_back(0); tc.push_back(0);
+            if (a.cn && (a.ctx->ntau - 1) / 8 == bucket) ntmax = std::max(ntmax, a.ctx->ntau);
+        if (!ntmax) continue;
+        for (int kind = 0; kind < 3; kind++) {             // narrow wing, wide wing, core
+            const int Pk = kind == 0 ? 2 : P;
+            std::vector<int> &t0 = kind < 2 ? tw : tc;
+            fsg_batch::Launch L{ ntmax, Pk, (int)(kind < 2 ? jw.size() : jc.size()), 0, (int)t0.size() };
+            t0.push_back(0);
             for (auto &a : b->atm) {
                 fsg_ctx *c = a.ctx;
-                if (a.cn == 0 || (c->ntau - 1) / 8 != bucket || cls >= a.ncls) continue;
+                if (a.cn == 0 || (c->ntau - 1) / 8 != bucket) continue;
+                const int c0 = kind == 1 ? BATCH_NARROW + 1 : 0;
+                const int nseg = kind == 0 ? std::min(a.ncls, BATCH_NARROW + 1) : kind == 1 ? a.ncls - c0 : a.ncls;
+                if (nseg <= 0) continue;
                 const int ws = batch_wing_stride(c), cs = batch_core_stride(c);
-                jw.push_back(WingJob{ c->ntau, c->nwl, c->d_wave.as<double>(), a.hdr.as<LineHdr>(), a.wing.as<WingRec>(),
-                                      a.wtlo.as<int>() + (size_t)cls * ws, a.wthi.as<int>() + (size_t)cls * ws,
-                                      c->d_lineopac.as<double>(), 0u, WAIT_NS });
-                tw.push_back(tw.back() + (c->nwl + 32 * Pc - 1) / (32 * Pc));
-                jc.push_back(CoreJob{ c->ntau, c->nwl, c->d_wave.as<double>(), a.hdr.as<LineHdr>(),
-                                      a.wing.as<WingRec>(), a.core.as<CoreRec>(), a.ctlo.as<int>() + (size_t)cls * cs,
-                                      a.cthi.as<int>() + (size_t)cls * cs, c->d_lineopac.as<double>(), nullptr, 0u,
-                                      WAIT_NS });
-                tc.push_back(tc.back() + (c->nwl + 31) / 32);
+                if (kind < 2) {
+                    jw.push_back(WingJob{ c->ntau, c->nwl, c->d_wave.as<double>(), a.hdr.as<LineHdr>(),
+                                          a.wing.as<WingRec>(), a.wtlo.as<int>() + (size_t)c0 * ws,
+                                          a.wthi.as<int>() + (size_t)c0 * ws, c->d_lineopac.as<double>(), 0u, WAIT_NS,
+                                          nseg, ws });
+                    t0.push_back(t0.back() + (c->nwl + 32 * Pk - 1) / (32 * Pk));
+                } else {
+                    jc.push_back(CoreJob{ c->ntau, c->nwl, c->d_wave.as<double>(), a.hdr.as<LineHdr>(),
+                                          a.wing.as<WingRec>(), a.core.as<CoreRec>(), a.ctlo.as<int>(), a.cthi.as<int>(),
+                                          c->d_lineopac.as<double>(), b->evals.as<unsigned long long>(), 0u, WAIT_NS,
+                                          nseg, cs });
+                    t0.push_back(t0.back() + (c->nwl + 31) / 32);
+                }
+                L.nj++;
             }
-            w.nj = (int)jw.size() - w.j0; k.nj = (int)jc.size() - k.j0;
-            if (w.nj) { b->lw.push_back(w); b->lc.push_back(k); }
+            if (L.nj) (kind < 2 ? b->lw : b->lc).push_back(L);
         }
     }
     ALLOC(b->jobs_w, sizeof(WingJob) * std::max<size_t>(jw.size(), 1));
     ALLOC(b->jobs_c, sizeof(CoreJob) * std::max<size_t>(jc.size(), 1));
     ALLOC(b->tile0_w, sizeof(int) * std::max<size_t>(tw.size(), 1));
     ALLOC(b->tile0_c, sizeof(int) * std::max<size_t>(tc.size(), 1));
-    ALLOC(b->queue, 2 * sizeof(unsigned) * std::max<size_t>(b->lw.size(), 1));
+    ALLOC(b->queue, sizeof(unsigned) * std::max<size_t>(b->lw.size() + b->lc.size(), 1));
     cudaStream_t s = ctx->stream;
     auto up = [&](DBuf &d, const void *h, size_t nb) {
         return nb ? cudaMemcpyAsync(d.p, h, nb, cudaMemcpyHostToDevice, s) : cudaSuccess;
@@ -2384,22 +2385,23 @@ static int batch_accumulate_solve(fsg_batch *b, const fsg_batch_tuning &t, cudaE
         fsg_ctx *c = a.ctx;
         CK(cudaMemsetAsync(c->d_lineopac.p, 0, sizeof(double) * (size_t)c->nwl * c->ntau, s), "batch reset");
     }
-    const size_t nl = b->lw.size();
-    CK(cudaMemsetAsync(b->queue.p, 0, 2 * sizeof(unsigned) * std::max<size_t>(nl, 1), s), "queue reset");
+    const size_t nw = b->lw.size(), nc = b->lc.size();
+    CK(cudaMemsetAsync(b->queue.p, 0, sizeof(unsigned) * std::max<size_t>(nw + nc, 1), s), "queue reset");
+    CK(cudaMemsetAsync(b->evals.p, 0, sizeof(unsigned long long), s), "count reset");
     unsigned *q = b->queue.as<unsigned>();
     // the wing launches (each read-modify-writes its atmospheres' LineOpac tiles), then the core ones
     if (ev) batch_mark(ev[0], s);
-    for (size_t i = 0; i < nl; i++) {
+    for (size_t i = 0; i < nw; i++) {
         const fsg_batch::Launch &L = b->lw[i];
         if (fsg_launch_accum_batch(s, L.P, L.ntau_max, b->jobs_w.as<WingJob>() + L.j0, b->tile0_w.as<int>() + L.t0,
-                                   L.nj, t.wing_ctas, q + 2 * i, b->err.as<int>()))
+                                   L.nj, t.wing_ctas, q + i, b->err.as<int>()))
             return cuda_fail(ctx, cudaGetLastError(), "k_accum_batch");
     }
     if (ev) batch_mark(ev[1], s);
-    for (size_t i = 0; i < nl; i++) {
+    for (size_t i = 0; i < nc; i++) {
         const fsg_batch::Launch &L = b->lc[i];
         if (fsg_launch_core_batch(s, L.ntau_max, b->jobs_c.as<CoreJob>() + L.j0, b->tile0_c.as<int>() + L.t0, L.nj,
-                                  t.core_ctas, b->atm[0].ctx->tab.vtab4, q + 2 * i + 1, b->err.as<int>()))
+                                  t.core_ctas, b->atm[0].ctx->tab.vtab4, q + nw + i, b->err.as<int>()))
             return cuda_fail(ctx, cudaGetLastError(), "k_core_batch");
     }
     if (ev) batch_mark(ev[2], s);
@@ -2480,7 +2482,8 @@ int fsg_batch_create(fsg_ctx *const *atms, int natm, const fsg_lines *lines, dou
             a.sfl.ensure(8 * (size_t)c->nwl) || a.sfc.ensure(8 * (size_t)c->nwl))
             return bail(FSG_E_NOMEM, "fsg_batch_create: device allocation failed");
     }
-    if (b->err.ensure(sizeof(int)) || b->nk.ensure(sizeof(unsigned long long)))
+    if (b->err.ensure(sizeof(int)) || b->nk.ensure(sizeof(unsigned long long)) ||
+        b->evals.ensure(sizeof(unsigned long long)))
         return bail(FSG_E_NOMEM, "fsg_batch_create: device allocation failed");
     if (cudaMemset(b->err.p, 0, sizeof(int)) != cudaSuccess) return bail(FSG_E_CUDA, "fsg_batch_create: upload failed");
     for (int i = 0; i < 8; i++) cudaEventCreate(&b->ev[i]);
@@ -2610,6 +2613,9 @@ int fsg_batch_run(fsg_batch *b, fsg_batch_stats *st) {
         cudaEventElapsedTime(&m2, b->ev[1], b->ev[2]);
         cudaEventElapsedTime(&m3, b->ev[2], b->ev[7]);
         st->ms_prepare = m0; st->ms_wing = m1; st->ms_core = m2; st->ms_solve = m3;
+        unsigned long long nc = 0;
+        CK(cudaMemcpy(&nc, b->evals.p, sizeof nc, cudaMemcpyDeviceToHost), "core count read");
+        st->core_evals = (double)nc;
         st->line_evals = b->line_evals;
         for (auto &a : b->atm) st->nlines_candidate += a.cn;
         st->natm = (int)b->atm.size();

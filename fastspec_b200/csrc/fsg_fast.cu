@@ -77,19 +77,6 @@ __device__ __forceinline__ float rcp_approx(float x) {
 // (table or continued fraction, the core pass's share) has its t replaced by 1e19, whose term is
 // exactly 0 too: the two passes split the points by the same FP32 test, so each point is evaluated
 // once.
-// One wing-pass job: the line records and tiles of one LineOpac (one atmosphere and grid).
-// extra_tx / wait_ns: 0 and WAIT_NS in use; a test of the error path (fsg_set_fault) makes every
-// chunk expect extra_tx bytes more than its copies deliver and bounds the waits by wait_ns.
-struct WingJob {
-    int ntau, nwl;
-    const double *wave;
-    const LineHdr *hdr;
-    const WingRec *wing;
-    const int *tile_lo, *tile_hi;
-    double *lineopac;
-    unsigned extra_tx;
-    unsigned long long wait_ns;
-};
 
 // shared memory of the wing pass for at most ntau_max depths:
 // wing records [2][CH][ntau_max] | headers [2][CH] | mbarriers [2] | Kahan pairs [D * P][blockDim.x]
@@ -114,21 +101,15 @@ __device__ __forceinline__ bool wing_tile(const WingJob &J, int tile, unsigned c
     uint64_t *bars = (uint64_t *)(shdr + 2 * CH);
     float2 *ksum = (float2 *)(bars + 2);                 // [D * P][blockDim.x]
     constexpr int TW = 32 * P;
-    const int lo = J.tile_lo[tile], hi = J.tile_hi[tile];
-    if (lo > hi) return true;
+    bool any = false;                                   // some segment has lines touching the tile
+    for (int sg = 0; sg < J.nseg; sg++)
+        any = any || J.tile_lo[sg * J.seg_stride + tile] <= J.tile_hi[sg * J.seg_stride + tile];
+    if (!any) return true;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int t0 = warp * D;
     const int nd = max(0, min(D, ntau - t0));            // warps past the last depth only help staging
     const int p0 = tile * TW;
     const int nth = blockDim.x;
-    const int nchunks = (hi - lo + CH) / CH;
-    // chunk c of this tile is the CTA's chunk g = kk + c: buffer g & 1, phase parity (g >> 1) & 1
-    if (threadIdx.x == 0) {
-        for (int c = 0; c < 2 && c < nchunks; c++) {
-            const int b = (kk + c) & 1;
-            stage_chunk(c, lo, hi, ntau, hdr, wing, shdr + b * CH, swing + b * CH * ntau_max, &bars[b], J.extra_tx);
-        }
-    }
     // wavelength offsets as FP32 hi + lo: dl = (wvh - wlh) + (wvl - wll) keeps dl to FP32 relative
     // accuracy next to the line centre
     float wvh[P], wvl[P];
@@ -150,100 +131,113 @@ __device__ __forceinline__ bool wing_tile(const WingJob &J, int tile, unsigned c
         }
     int nfold = 0;
     const int tile_first = p0 + 1, tile_last = min(p0 + TW, nwl);
-    int failed = -1;                                     // chunk whose copy did not complete
-    for (int c = 0; c < nchunks; c++) {
-        const unsigned g = kk + c;
-        const int b = g & 1;
-        const bool ok = mbar_wait(&bars[b], (g >> 1) & 1, J.wait_ns);
-        if (__syncthreads_or(!ok)) { failed = c; break; }
-        const LineHdr *ch = shdr + b * CH;
-        const WingRec *cw = swing + b * CH * ntau_max;
-        const int n = min(CH, hi - (lo + c * CH) + 1);
-        if (nd > 0) {
-            for (int q = 0; q < n; q++) {
-                const LineHdr h = ch[q];
-                if (h.iright < tile_first || h.ileft > tile_last) continue;   // window misses the tile
-                float x[P];
-#pragma unroll
-                for (int k = 0; k < P; k++) {
-                    float dl = (wvh[k] - h.wlh) + (wvl[k] - h.wll);
-                    x[k] = dl * dl;
-                }
-                // depths past the job's last (last warp only) read the next records of the buffer, or
-                // the headers after it: their partials are never stored
-                const WingRec *wq = cw + q * ntau + t0;
-                WingRec w[D];
-#pragma unroll
-                for (int d = 0; d < D; d++) w[d] = wq[d];
-                const bool core_hit = h.cl <= h.cr && h.cr >= tile_first && h.cl <= tile_last;
-                const bool full = h.ileft <= tile_first && h.iright >= tile_last && !core_hit;
-                if (!full) {
-                    // points outside the window take the header's offset x, for which the wing term is
-                    // exactly 0
-                    const float xm = __int_as_float(h.pad0);
+    for (int sg = 0; sg < J.nseg; sg++) {               // the job's segments of lines, in turn
+        const int lo = J.tile_lo[sg * J.seg_stride + tile], hi = J.tile_hi[sg * J.seg_stride + tile];
+        if (lo > hi) continue;
+        const int nchunks = (hi - lo + CH) / CH;
+        // chunk c of this tile is the CTA's chunk g = kk + c: buffer g & 1, phase parity (g >> 1) & 1
+        if (threadIdx.x == 0) {
+            for (int c = 0; c < 2 && c < nchunks; c++) {
+                const int b = (kk + c) & 1;
+                stage_chunk(c, lo, hi, ntau, hdr, wing, shdr + b * CH, swing + b * CH * ntau_max, &bars[b],
+                            J.extra_tx);
+            }
+        }
+        int failed = -1;                                     // chunk whose copy did not complete
+        for (int c = 0; c < nchunks; c++) {
+            const unsigned g = kk + c;
+            const int b = g & 1;
+            const bool ok = mbar_wait(&bars[b], (g >> 1) & 1, J.wait_ns);
+            if (__syncthreads_or(!ok)) { failed = c; break; }
+            const LineHdr *ch = shdr + b * CH;
+            const WingRec *cw = swing + b * CH * ntau_max;
+            const int n = min(CH, hi - (lo + c * CH) + 1);
+            if (nd > 0) {
+                for (int q = 0; q < n; q++) {
+                    const LineHdr h = ch[q];
+                    if (h.iright < tile_first || h.ileft > tile_last) continue;   // window misses the tile
+                    float x[P];
 #pragma unroll
                     for (int k = 0; k < P; k++) {
-                        const int p1 = pix[k] + 1;
-                        const bool in = p1 >= h.ileft && p1 <= h.iright;
-                        x[k] = in ? x[k] : xm;
+                        float dl = (wvh[k] - h.wlh) + (wvl[k] - h.wll);
+                        x[k] = dl * dl;
+                    }
+                    // depths past the job's last (last warp only) read the next records of the buffer, or
+                    // the headers after it: their partials are never stored
+                    const WingRec *wq = cw + q * ntau + t0;
+                    WingRec w[D];
+#pragma unroll
+                    for (int d = 0; d < D; d++) w[d] = wq[d];
+                    const bool core_hit = h.cl <= h.cr && h.cr >= tile_first && h.cl <= tile_last;
+                    const bool full = h.ileft <= tile_first && h.iright >= tile_last && !core_hit;
+                    if (!full) {
+                        // points outside the window take the header's offset x, for which the wing term is
+                        // exactly 0
+                        const float xm = __int_as_float(h.pad0);
+#pragma unroll
+                        for (int k = 0; k < P; k++) {
+                            const int p1 = pix[k] + 1;
+                            const bool in = p1 >= h.ileft && p1 <= h.iright;
+                            x[k] = in ? x[k] : xm;
+                        }
+                    }
+                    if (!core_hit) {
+#pragma unroll
+                        for (int d = 0; d < D; d++)
+#pragma unroll
+                            for (int k = 0; k < P; k++) {
+                                float t = fmaf(x[k], w[d].vv2, w[d].c2m1);
+                                float den = fmaf(t, t, w[d].twoA);
+                                float num = fmaf(w[d].c1, t, w[d].c1);
+                                part[d][k] = fmaf(num, rcp_approx(den), part[d][k]);
+                            }
+                    } else {
+#pragma unroll
+                        for (int d = 0; d < D; d++)
+#pragma unroll
+                            for (int k = 0; k < P; k++) {
+                                float t = fmaf(x[k], w[d].vv2, w[d].c2m1);
+                                t = t < 195.5f ? 1.0e19f : t;        // the core pass's point
+                                float den = fmaf(t, t, w[d].twoA);
+                                float num = fmaf(w[d].c1, t, w[d].c1);
+                                part[d][k] = fmaf(num, rcp_approx(den), part[d][k]);
+                            }
+                    }
+                    if (++nfold == FOLD) {
+                        nfold = 0;
+#pragma unroll
+                        for (int d = 0; d < D; d++)
+#pragma unroll
+                            for (int k = 0; k < P; k++) {
+                                float2 &qq = ksum[(d * P + k) * nth + threadIdx.x];
+                                float2 sc = qq;
+                                KAHAN(sc.x, sc.y, part[d][k]);
+                                qq = sc;
+                                part[d][k] = 0.0f;
+                            }
                     }
                 }
-                if (!core_hit) {
-#pragma unroll
-                    for (int d = 0; d < D; d++)
-#pragma unroll
-                        for (int k = 0; k < P; k++) {
-                            float t = fmaf(x[k], w[d].vv2, w[d].c2m1);
-                            float den = fmaf(t, t, w[d].twoA);
-                            float num = fmaf(w[d].c1, t, w[d].c1);
-                            part[d][k] = fmaf(num, rcp_approx(den), part[d][k]);
-                        }
-                } else {
-#pragma unroll
-                    for (int d = 0; d < D; d++)
-#pragma unroll
-                        for (int k = 0; k < P; k++) {
-                            float t = fmaf(x[k], w[d].vv2, w[d].c2m1);
-                            t = t < 195.5f ? 1.0e19f : t;        // the core pass's point
-                            float den = fmaf(t, t, w[d].twoA);
-                            float num = fmaf(w[d].c1, t, w[d].c1);
-                            part[d][k] = fmaf(num, rcp_approx(den), part[d][k]);
-                        }
-                }
-                if (++nfold == FOLD) {
-                    nfold = 0;
-#pragma unroll
-                    for (int d = 0; d < D; d++)
-#pragma unroll
-                        for (int k = 0; k < P; k++) {
-                            float2 &qq = ksum[(d * P + k) * nth + threadIdx.x];
-                            float2 sc = qq;
-                            KAHAN(sc.x, sc.y, part[d][k]);
-                            qq = sc;
-                            part[d][k] = 0.0f;
-                        }
+            }
+            __syncthreads();                                   // every warp is done with buffer b
+            if (threadIdx.x == 0 && c + 2 < nchunks)
+                stage_chunk(c + 2, lo, hi, ntau, hdr, wing, shdr + b * CH, swing + b * CH * ntau_max, &bars[b],
+                            J.extra_tx);
+        }
+        if (failed >= 0) {
+            // a copy never completed: report, then wait (bounded) for the copies still in flight,
+            // chunks failed and failed + 1, before the CTA's shared memory is released
+            if (threadIdx.x == 0) {
+                atomicExch(err, FSG_E_TIMEOUT);
+                for (int c = failed; c < nchunks && c < failed + 2; c++) {
+                    const unsigned g = kk + c;
+                    mbar_wait(&bars[g & 1], (g >> 1) & 1, J.wait_ns);
                 }
             }
+            __syncthreads();
+            return false;
         }
-        __syncthreads();                                   // every warp is done with buffer b
-        if (threadIdx.x == 0 && c + 2 < nchunks)
-            stage_chunk(c + 2, lo, hi, ntau, hdr, wing, shdr + b * CH, swing + b * CH * ntau_max, &bars[b],
-                        J.extra_tx);
+        kk += nchunks;
     }
-    if (failed >= 0) {
-        // a copy never completed: report, then wait (bounded) for the copies still in flight,
-        // chunks failed and failed + 1, before the CTA's shared memory is released
-        if (threadIdx.x == 0) {
-            atomicExch(err, FSG_E_TIMEOUT);
-            for (int c = failed; c < nchunks && c < failed + 2; c++) {
-                const unsigned g = kk + c;
-                mbar_wait(&bars[g & 1], (g >> 1) & 1, J.wait_ns);
-            }
-        }
-        __syncthreads();
-        return false;
-    }
-    kk += nchunks;
     if (nd <= 0) return true;
 #pragma unroll
     for (int k = 0; k < P; k++) {
@@ -337,7 +331,7 @@ int fsg_launch_accum_fast(cudaStream_t st, int cls, int ntau, int nwl, const dou
     const int nwarps = (ntau + D - 1) / D;
     const size_t smem = fsg_wing_smem(P, ntau);
     if (smem > 200 * 1024) return FSG_E_ARG;
-    WingJob J{ ntau, nwl, wave, hdr, wing, tile_lo, tile_hi, lineopac, extra_tx, wait_ns };
+    WingJob J{ ntau, nwl, wave, hdr, wing, tile_lo, tile_hi, lineopac, extra_tx, wait_ns, 1, 0 };
 #define LAUNCH(DD, PP) do { \
         cudaFuncSetAttribute(k_accum_fast<DD, PP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
         k_accum_fast<DD, PP><<<ntiles, 32 * nwarps, smem, st>>>(J, err); } while (0)
@@ -372,20 +366,6 @@ int fsg_launch_accum_batch(cudaStream_t st, int P, int ntau_max, const WingJob *
 // gathers (one 16-byte load of the cell-major VgtTab copy each) together.  D = 4 depths per warp up to
 // 72 depths, 8 beyond (18 warps at most).
 
-// One core-pass job: as WingJob plus the core records; tiles of 32 wavelengths.  nevals (may be null)
-// counts the evaluations.
-struct CoreJob {
-    int ntau, nwl;
-    const double *wave;
-    const LineHdr *hdr;
-    const WingRec *wing;
-    const CoreRec *core;
-    const int *tile_lo, *tile_hi;
-    double *lineopac;
-    unsigned long long *nevals;
-    unsigned extra_tx;
-    unsigned long long wait_ns;
-};
 
 // shared memory of the core pass for at most ntau_max depths and chc lines per chunk:
 // wing records [2][chc][ntau_max] | core records [2][chc][ntau_max] | headers [2][chc] | mbarriers [2]
@@ -413,8 +393,10 @@ template <int D>
 __device__ bool core_tile(const CoreJob &J, int tile, const float4 *__restrict__ vtab4, unsigned char *smem_raw,
                           int ntau_max, int chc, unsigned &kk, int *err) {
     const int ntau = J.ntau, nwl = J.nwl;
-    const int lo = J.tile_lo[tile], hi = J.tile_hi[tile];
-    if (lo > hi) return true;
+    bool any = false;                              // some segment has core ranges touching the tile
+    for (int sg = 0; sg < J.nseg; sg++)
+        any = any || J.tile_lo[sg * J.seg_stride + tile] <= J.tile_hi[sg * J.seg_stride + tile];
+    if (!any) return true;
     WingRec *sw = (WingRec *)smem_raw;
     CoreRec *sc = (CoreRec *)(sw + 2 * (size_t)chc * ntau_max);
     LineHdr *sh = (LineHdr *)(sc + 2 * (size_t)chc * ntau_max);
@@ -424,98 +406,102 @@ __device__ bool core_tile(const CoreJob &J, int tile, const float4 *__restrict__
     const int nd = max(0, min(D, ntau - t0));      // warps past the last depth only wait with the others
     const int p = tile * 32 + lane, p1 = p + 1;
     const int tile_first = tile * 32 + 1, tile_last = min(tile * 32 + 32, nwl);
-    const int nchunks = (hi - lo + chc) / chc;
-    if (threadIdx.x == 0)
-        for (int c = 0; c < 2 && c < nchunks; c++) {
-            const int b = (kk + c) & 1;
-            core_stage(c, lo, hi, ntau, chc, J, sw + (size_t)b * chc * ntau_max, sc + (size_t)b * chc * ntau_max,
-                       sh + b * chc, &bars[b]);
-        }
     const double wd = J.wave[min(p, nwl - 1)];
     const float wvh = (float)wd, wvl = (float)(wd - (double)wvh);
     float sum[D], cmp[D];
 #pragma unroll
     for (int d = 0; d < D; d++) { sum[d] = 0.0f; cmp[d] = 0.0f; }
     unsigned cnt = 0;
-    int failed = -1;
-    for (int c = 0; c < nchunks; c++) {
-        const unsigned g = kk + c;
-        const int b = g & 1;
-        const bool ok = mbar_wait(&bars[b], (g >> 1) & 1, J.wait_ns);
-        if (__syncthreads_or(!ok)) { failed = c; break; }
-        const LineHdr *ch = sh + b * chc;
-        const WingRec *cw = sw + (size_t)b * chc * ntau_max;
-        const CoreRec *cc = sc + (size_t)b * chc * ntau_max;
-        const int n = min(chc, hi - (lo + c * chc) + 1);
-        if (nd > 0) {
-            for (int q = 0; q < n; q++) {
-                const LineHdr h = ch[q];
-                if (h.cr < tile_first || h.cl > tile_last) continue;          // core range misses the tile
-                const bool in = p1 >= h.cl && p1 <= h.cr;
-                if (!__any_sync(0xffffffffu, in)) continue;
-                const float dl = (wvh - h.wlh) + (wvl - h.wll);
-                const float x = dl * dl;                  // the wing pass's x: the same branch split
-                const double adl = fabs(wd - ((double)h.wlh + (double)h.wll));
+    for (int sg = 0; sg < J.nseg; sg++) {         // the job's segments of lines, in turn
+        const int lo = J.tile_lo[sg * J.seg_stride + tile], hi = J.tile_hi[sg * J.seg_stride + tile];
+        if (lo > hi) continue;
+        const int nchunks = (hi - lo + chc) / chc;
+        if (threadIdx.x == 0)
+            for (int c = 0; c < 2 && c < nchunks; c++) {
+                const int b = (kk + c) & 1;
+                core_stage(c, lo, hi, ntau, chc, J, sw + (size_t)b * chc * ntau_max, sc + (size_t)b * chc * ntau_max,
+                           sh + b * chc, &bars[b]);
+            }
+        int failed = -1;
+        for (int c = 0; c < nchunks; c++) {
+            const unsigned g = kk + c;
+            const int b = g & 1;
+            const bool ok = mbar_wait(&bars[b], (g >> 1) & 1, J.wait_ns);
+            if (__syncthreads_or(!ok)) { failed = c; break; }
+            const LineHdr *ch = sh + b * chc;
+            const WingRec *cw = sw + (size_t)b * chc * ntau_max;
+            const CoreRec *cc = sc + (size_t)b * chc * ntau_max;
+            const int n = min(chc, hi - (lo + c * chc) + 1);
+            if (nd > 0) {
+                for (int q = 0; q < n; q++) {
+                    const LineHdr h = ch[q];
+                    if (h.cr < tile_first || h.cl > tile_last) continue;          // core range misses the tile
+                    const bool in = p1 >= h.cl && p1 <= h.cr;
+                    if (!__any_sync(0xffffffffu, in)) continue;
+                    const float dl = (wvh - h.wlh) + (wvl - h.wll);
+                    const float x = dl * dl;                  // the wing pass's x: the same branch split
+                    const double adl = fabs(wd - ((double)h.wlh + (double)h.wll));
 #pragma unroll
-                for (int g0 = 0; g0 < D; g0 += 4) {               // depths in groups of four
-                    bool core[4], tab[4];
-                    float tv[4];
-                    int cell[4];
+                    for (int g0 = 0; g0 < D; g0 += 4) {               // depths in groups of four
+                        bool core[4], tab[4];
+                        float tv[4];
+                        int cell[4];
 #pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        const int d = g0 + e;
-                        const int td = t0 + min(d, nd - 1);
-                        const WingRec w = cw[q * ntau + td];
-                        const CoreRec cr = cc[q * ntau + td];
-                        const float t = fmaf(x, w.vv2, w.c2m1);
-                        core[e] = in && d < nd && t < 195.5f;
-                        const double av = adl * cr.vv;
-                        tab[e] = core[e] && cr.ia > 0 && av < 8.0;
-                        const double fv = av * 125.0;
-                        const int iv = tab[e] ? min((int)fv, FSG_NVV - 1) : 0;
-                        tv[e] = tab[e] ? (float)(fv - (double)iv) : (float)av;   // CF: |v| in FP32
-                        cell[e] = tab[e] ? (cr.ia - 1) * FSG_NV1 + iv : 0;
-                    }
-                    float4 gv[4];
-#pragma unroll
-                    for (int e = 0; e < 4; e++)
-                        if (tab[e]) gv[e] = __ldg(vtab4 + cell[e]);
-#pragma unroll
-                    for (int e = 0; e < 4; e++) {
-                        if (!core[e]) continue;
-                        const int d = g0 + e;
-                        const CoreRec &cr = cc[q * ntau + t0 + d];
-                        float v;
-                        if (tab[e]) {
-                            const float4 gg = gv[e];
-                            const float c0 = gg.x + tv[e] * (gg.y - gg.x), c1 = gg.z + tv[e] * (gg.w - gg.z);
-                            v = (c0 + cr.ua * (c1 - c0)) * cr.cop;
-                        } else {
-                            v = hv_cf32(tv[e], cr.a, cr.cop);
+                        for (int e = 0; e < 4; e++) {
+                            const int d = g0 + e;
+                            const int td = t0 + min(d, nd - 1);
+                            const WingRec w = cw[q * ntau + td];
+                            const CoreRec cr = cc[q * ntau + td];
+                            const float t = fmaf(x, w.vv2, w.c2m1);
+                            core[e] = in && d < nd && t < 195.5f;
+                            const double av = adl * cr.vv;
+                            tab[e] = core[e] && cr.ia > 0 && av < 8.0;
+                            const double fv = av * 125.0;
+                            const int iv = tab[e] ? min((int)fv, FSG_NVV - 1) : 0;
+                            tv[e] = tab[e] ? (float)(fv - (double)iv) : (float)av;   // CF: |v| in FP32
+                            cell[e] = tab[e] ? (cr.ia - 1) * FSG_NV1 + iv : 0;
                         }
-                        KAHAN(sum[d], cmp[d], v);
-                        cnt++;
+                        float4 gv[4];
+#pragma unroll
+                        for (int e = 0; e < 4; e++)
+                            if (tab[e]) gv[e] = __ldg(vtab4 + cell[e]);
+#pragma unroll
+                        for (int e = 0; e < 4; e++) {
+                            if (!core[e]) continue;
+                            const int d = g0 + e;
+                            const CoreRec &cr = cc[q * ntau + t0 + d];
+                            float v;
+                            if (tab[e]) {
+                                const float4 gg = gv[e];
+                                const float c0 = gg.x + tv[e] * (gg.y - gg.x), c1 = gg.z + tv[e] * (gg.w - gg.z);
+                                v = (c0 + cr.ua * (c1 - c0)) * cr.cop;
+                            } else {
+                                v = hv_cf32(tv[e], cr.a, cr.cop);
+                            }
+                            KAHAN(sum[d], cmp[d], v);
+                            cnt++;
+                        }
                     }
                 }
             }
+            __syncthreads();                                   // every warp is done with buffer b
+            if (threadIdx.x == 0 && c + 2 < nchunks)
+                core_stage(c + 2, lo, hi, ntau, chc, J, sw + (size_t)b * chc * ntau_max,
+                           sc + (size_t)b * chc * ntau_max, sh + b * chc, &bars[b]);
         }
-        __syncthreads();                                   // every warp is done with buffer b
-        if (threadIdx.x == 0 && c + 2 < nchunks)
-            core_stage(c + 2, lo, hi, ntau, chc, J, sw + (size_t)b * chc * ntau_max, sc + (size_t)b * chc * ntau_max,
-                       sh + b * chc, &bars[b]);
-    }
-    if (failed >= 0) {
-        if (threadIdx.x == 0) {
-            atomicExch(err, FSG_E_TIMEOUT);
-            for (int c = failed; c < nchunks && c < failed + 2; c++) {
-                const unsigned g = kk + c;
-                mbar_wait(&bars[g & 1], (g >> 1) & 1, J.wait_ns);
+        if (failed >= 0) {
+            if (threadIdx.x == 0) {
+                atomicExch(err, FSG_E_TIMEOUT);
+                for (int c = failed; c < nchunks && c < failed + 2; c++) {
+                    const unsigned g = kk + c;
+                    mbar_wait(&bars[g & 1], (g >> 1) & 1, J.wait_ns);
+                }
             }
+            __syncthreads();
+            return false;
         }
-        __syncthreads();
-        return false;
+        kk += nchunks;
     }
-    kk += nchunks;
     if (J.nevals) {
         unsigned long long v = cnt;
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -589,7 +575,7 @@ int fsg_launch_core_fast(cudaStream_t st, int ntau, int nwl, const double *wave,
     if (nwarps > 18) return FSG_E_ARG;
     const int chc = core_chunk(ntau);
     const size_t smem = core_smem(ntau, chc);
-    CoreJob J{ ntau, nwl, wave, hdr, wing, core, tile_lo, tile_hi, lineopac, nevals, extra_tx, wait_ns };
+    CoreJob J{ ntau, nwl, wave, hdr, wing, core, tile_lo, tile_hi, lineopac, nevals, extra_tx, wait_ns, 1, 0 };
     if (D == 4) {
         cudaFuncSetAttribute(k_core_fast<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k_core_fast<4><<<ntiles, 32 * nwarps, smem, st>>>(J, vtab4, chc, err);

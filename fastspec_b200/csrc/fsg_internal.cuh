@@ -109,6 +109,39 @@ struct BlockView {
 };
 static_assert(sizeof(XCoef) == sizeof(fsg_xcoef), "fsg_xcoef mirrors XCoef");
 
+// One wing-pass job: the line records and tiles of one LineOpac (one atmosphere and grid).  Its
+// tile ranges come in nseg segments (window-width classes of one record array), segment s at
+// tile_lo / tile_hi + s * seg_stride; a tile takes the segments' lines in turn into one sum.
+// extra_tx / wait_ns: 0 and WAIT_NS in use; a test of the error path (fsg_set_fault) makes every
+// chunk expect extra_tx bytes more than its copies deliver and bounds the waits by wait_ns.
+struct WingJob {
+    int ntau, nwl;
+    const double *wave;
+    const LineHdr *hdr;
+    const WingRec *wing;
+    const int *tile_lo, *tile_hi;
+    double *lineopac;
+    unsigned extra_tx;
+    unsigned long long wait_ns;
+    int nseg, seg_stride;
+};
+
+// One core-pass job: as WingJob plus the core records; tiles of 32 wavelengths.  nevals (may be
+// null) counts the evaluations.
+struct CoreJob {
+    int ntau, nwl;
+    const double *wave;
+    const LineHdr *hdr;
+    const WingRec *wing;
+    const CoreRec *core;
+    const int *tile_lo, *tile_hi;
+    double *lineopac;
+    unsigned long long *nevals;
+    unsigned extra_tx;
+    unsigned long long wait_ns;
+    int nseg, seg_stride;
+};
+
 // Rays of a spherical model (SphereInit, solver.f90:45-120), device arrays [nmu][stride], stride =
 // 2 ntau.  Ray im has n[im] points (ntau, or 2 n for a grazing ray that turns below layer n); point k
 // samples layer map[im][k] (0-based) at column mass m[im][k] along the ray.  nmu = 0: plane-parallel.
