@@ -69,8 +69,8 @@ int fsg_launch_btile_span(cudaStream_t, int, int64_t, const LineHdr *, const int
                           int *, int *, void *, size_t);
 size_t fsg_tile_span_scratch(int64_t);
 int fsg_launch_tile_span_tw(cudaStream_t, int, int, int, int64_t, const LineHdr *, int *, int *, void *, size_t);
-void fsg_launch_mag_params_fast(cudaStream_t, const AtmView &, const LineView &, const int64_t *, int64_t, int64_t,
-                                const int32_t *, const int32_t *, const int32_t *, const VoigtTables &, void *,
+void fsg_launch_mag_params_fast(cudaStream_t, const AtmView &, const LineView &, const ZView &, const int64_t *, int64_t,
+                                int64_t, const int32_t *, const int32_t *, const int32_t *, const VoigtTables &, void *,
                                 LineHdr *, int64_t *);
 size_t fsg_mag_rec_bytes();
 int fsg_launch_mag_fast(cudaStream_t, const AtmView &, const LineHdr *, const void *, const int64_t *, const ZView &,
@@ -1288,7 +1288,7 @@ int fsg_mag_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, int bframe, const 
         int64_t nblocks = 0;
         for (int64_t j0 = 0; j0 < nkeep; j0 += bcap) {
             const int64_t nb = std::min(bcap, nkeep - j0);
-            fsg_launch_mag_params_fast(s, A, LV, ctx->d_idx.as<int64_t>(), j0, nb, pf, pl, pr, ctx->tab, ctx->d_wing.p,
+            fsg_launch_mag_params_fast(s, A, LV, Z, ctx->d_idx.as<int64_t>(), j0, nb, pf, pl, pr, ctx->tab, ctx->d_wing.p,
                                        ctx->d_hdr.as<LineHdr>(), ctx->d_zmap.as<int64_t>());
             if (fsg_launch_tile_span_tw(s, 32, 0, nwl, nb, ctx->d_hdr.as<LineHdr>(), ctx->d_tlo.as<int>(),
                                         ctx->d_thi.as<int>(), ctx->d_span.p, ctx->d_span.cap) ||

@@ -15,8 +15,12 @@
 
 struct __align__(16) MagRec { float vv, cop, a, ua; int ia, pad0, pad1, pad2; };
 
-__global__ void k_mag_params_fast(AtmView A, LineView L, const int64_t *__restrict__ idx, int64_t j0, int64_t nb,
-                                  const int32_t *__restrict__ flags, const int32_t *__restrict__ ileft,
+// Records of a block's lines, and per line its header with the core range [cl, cr]: every wavelength
+// of the window where some depth and Zeeman component may have s = v^2 + a^2 < 196 (half-width
+// max_t sqrt(196.05 - a^2) / LinVvgt, + the largest |component shift| and |He I shift|, + one
+// wavelength); outside it every point takes FVoigt's rational wing pair.
+__global__ void k_mag_params_fast(AtmView A, LineView L, ZView Z, const int64_t *__restrict__ idx, int64_t j0,
+                                  int64_t nb, const int32_t *__restrict__ flags, const int32_t *__restrict__ ileft,
                                   const int32_t *__restrict__ iright, const double *__restrict__ anode,
                                   const double *__restrict__ aida, MagRec *rec, LineHdr *hdr, int64_t *zidx) {
     int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -28,9 +32,14 @@ __global__ void k_mag_params_fast(AtmView A, LineView L, const int64_t *__restri
     XCoef XC;
     xline_setup(A, L, i, wlc, f, &XC);
     const float an1 = (float)anode[1], ai0 = (float)aida[0];
+    const int ihe = (f >> 8) & 255;
+    double hcore = -1.0, shmax = 0.0;
     for (int t = 0; t < nt; t++) {
         double cop, vv, av;
         xline_depth(A, t, XC, &cop, &vv, &av);
+        const double q = 196.05 - av * av;
+        if (q > 0.0) hcore = fmax(hcore, sqrt(q) / vv * (1.0 + 1e-5));
+        if (ihe > 0) shmax = fmax(shmax, fabs(A.heshf[(size_t)(ihe - 1) * nt + t]));
         if (A.motype == 1) cop = cop / A.contstd[t];
         MagRec r;
         r.vv = (float)vv; r.cop = (float)cop; r.a = (float)av;
@@ -49,7 +58,18 @@ __global__ void k_mag_params_fast(AtmView A, LineView L, const int64_t *__restri
     h.wll = (float)(wlc - (double)h.wlh);
     h.ileft = ileft[i]; h.iright = iright[i];
     h.cl = 1; h.cr = 0;
-    h.pad0 = (f >> 8) & 255;                          // He I table index (0: none)
+    if (hcore >= 0.0) {
+        double zmax = 0.0;
+        for (int k = 0; k < Z.npi[i]; k++) zmax = fmax(zmax, fabs((double)Z.splpi[Z.pi_off[i] + k]));
+        for (int k = 0; k < Z.nsi[i]; k++) zmax = fmax(zmax, fabs((double)Z.splsi[Z.si_off[i] + k]));
+        const double half = hcore + zmax + shmax;
+        int a = lower_index(A.wave, A.nwl, wlc - half) + 1;
+        int b = lower_index(A.wave, A.nwl, wlc + half);
+        if (b < A.nwl && A.wave[b] == wlc + half) b++;
+        const int cl = max(a - 1, h.ileft), cr = min(b + 1, h.iright);
+        if (cl <= cr) { h.cl = cl; h.cr = cr; }
+    }
+    h.pad0 = ihe;                                     // He I table index (0: none)
     h.pad1 = 0;
     hdr[j] = h;
     zidx[j] = i;
@@ -133,6 +153,43 @@ k_mag_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *__
         for (int d = 0; d < MAG_D; d++)
 #pragma unroll
             for (int q = 0; q < 6; q++) s[d][q] = 0.0f;
+        if (h.cl > h.cr || h.cr < tile_first || h.cl > tile_last) {
+            // the tile lies outside the line's core range: every point takes the wing pair, here as
+            // H = a/sqrt(pi) (u + a^2 + 1/2) / D and L = v/sqrt(pi) (u + a^2 - 1/2) / D with u = v^2 and
+            // D = s^2 - v^2 + a^2 + 1/4 = u (u + 2a^2 - 1) + (a^2 + 1/2)^2 (voigt.f90:280-289)
+            float b1[MAG_D], b0[MAG_D], ah[MAG_D], am[MAG_D];
+#pragma unroll
+            for (int d = 0; d < MAG_D; d++) {
+                const float a2 = r[d].a * r[d].a;
+                b1[d] = 2.0f * a2 - 1.0f; ah[d] = a2 + 0.5f; am[d] = a2 - 0.5f; b0[d] = ah[d] * ah[d];
+            }
+            auto comps = [&](const float *sp_, const float *st_, int k0, int k1, int qh) {
+                for (int k = k0; k < k1; k++) {
+                    const float sp = sp_[k], st = st_[k];
+#pragma unroll
+                    for (int d = 0; d < MAG_D; d++) {
+                        const float v = fmaf(-sp, r[d].vv, vb[d]);
+                        const float u = v * v;
+                        const float rr = rcp_approx_m(fmaf(u, u + b1[d], b0[d]));
+                        s[d][qh] = fmaf(st, (u + ah[d]) * rr, s[d][qh]);
+                        s[d][qh + 3] = fmaf(st, (u + am[d]) * rr * v, s[d][qh + 3]);
+                    }
+                }
+            };
+            comps(spi, rpi, 0, np, 0);
+            comps(ssi, rsi, 0, nsh, 1);
+            comps(ssi, rsi, nsh, ns, 2);
+#pragma unroll
+            for (int d = 0; d < MAG_D; d++) {
+                const float ch = 0.56418958354775628f * r[d].a * r[d].cop, cv = 0.56418958354775628f * r[d].cop;
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    acc[d][q] += (double)(s[d][q] * ch);
+                    acc[d][q + 3] += (double)(s[d][q + 3] * cv);
+                }
+            }
+            continue;
+        }
         for (int k = 0; k < np; k++) {
             const float sp = spi[k], st = rpi[k];
 #pragma unroll
@@ -168,11 +225,11 @@ k_mag_fast(int ntau, int nwl, const double *__restrict__ wave, const LineHdr *__
     }
 }
 
-void fsg_launch_mag_params_fast(cudaStream_t s, const AtmView &A, const LineView &L, const int64_t *idx, int64_t j0,
-                                int64_t nb, const int32_t *flags, const int32_t *il, const int32_t *ir,
+void fsg_launch_mag_params_fast(cudaStream_t s, const AtmView &A, const LineView &L, const ZView &Z, const int64_t *idx,
+                                int64_t j0, int64_t nb, const int32_t *flags, const int32_t *il, const int32_t *ir,
                                 const VoigtTables &T, void *rec, LineHdr *hdr, int64_t *zidx) {
     if (nb > 0)
-        k_mag_params_fast<<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(A, L, idx, j0, nb, flags, il, ir, T.anode,
+        k_mag_params_fast<<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(A, L, Z, idx, j0, nb, flags, il, ir, T.anode,
                                                                        T.aida, (MagRec *)rec, hdr, zidx);
 }
 
