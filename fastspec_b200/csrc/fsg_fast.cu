@@ -15,11 +15,10 @@
 // tile's candidate range stays close to the lines that touch it; narrow classes use 64-wavelength
 // tiles, wide ones 128.
 //
-// Core pass (k_core_fast): over the core ranges, 32-wavelength tiles, the points of HVoigt's table
-// region (s < 196, a < 8, |v| < 8): the table lerp.  The wing pass takes every other point, the
-// rational wing form where s >= 196 and the two-term continued fraction (voigt.f90:103-107) for the
-// rest of s < 196, as HVoigt branches.  No atomics; one read-modify-write of the FP64 LineOpac per
-// tile and launch; deterministic order.
+// Core pass (k_core_fast): over the core ranges, 32-wavelength tiles, the points where s < 196: the
+// table lerp (|v| < 8, a < 8) or the two-term continued fraction (voigt.f90:103-107), exactly as
+// HVoigt branches.  No atomics; one read-modify-write of the FP64 LineOpac per tile and launch;
+// deterministic order.
 #include "fsg_internal.cuh"
 #include "fsg_mbar.cuh"
 
@@ -28,6 +27,15 @@
 #include <algorithm>
 
 #define CLASS_W0 128      // class c: windows of at most CLASS_W0 * 2^(c+1) wavelengths
+
+// HVoigt * LinCop in FP32 outside the table (a >= 8 or |v| >= 8, s < 196): the two-term continued
+// fraction of voigt.f90:103-107 at |v| = av
+__device__ __forceinline__ float hv_cf32(float av, float a, float cop) {
+    float a2 = a * a, v2 = av * av;
+    float p = v2 - a2 - 1.5f, q = 2.0f * av * a;
+    float dr = av * p - a * q, di = av * q + a * p;
+    return 0.56418958354775628f * __fdividef((p + 0.5f) * di - q * dr, dr * dr + di * di) * cop;
+}
 
 // Kahan-compensated accumulation of one value
 #define KAHAN(S, CC, V) do { float _y = (V) - (CC); float _t = (S) + _y; (CC) = (_t - (S)) - _y; (S) = _t; } while (0)
@@ -65,10 +73,10 @@ __device__ __forceinline__ float rcp_approx(float x) {
 // (three FMAs, one reciprocal, one FMA into the partial sum).  Outside the line's core range [cl, cr]
 // that is every depth.  Lines whose window covers the whole tile outside their core range (the common
 // case for wide windows) skip the mask; for the others the points outside the window get an x for
-// which the term is exactly 0.  On tiles that meet the core range, a point whose t is below 195.5
-// takes the continued fraction, or adds 0 when it lies in the table region (twoA < 128 and
-// fl32(dl^2 vv2) < 64), which is the core pass's: the two passes split the points by the same FP32
-// tests, so each point is evaluated once.
+// which the term is exactly 0.  On tiles that meet the core range, each point whose t is below 195.5
+// (table or continued fraction, the core pass's share) has its t replaced by 1e19, whose term is
+// exactly 0 too: the two passes split the points by the same FP32 test, so each point is evaluated
+// once.
 
 // shared memory of the wing pass for at most ntau_max depths:
 // wing records [2][CH][ntau_max] | headers [2][CH] | mbarriers [2] | Kahan pairs [D * P][blockDim.x]
@@ -184,25 +192,14 @@ __device__ __forceinline__ bool wing_tile(const WingJob &J, int tile, unsigned c
                                 part[d][k] = fmaf(num, rcp_approx(den), part[d][k]);
                             }
                     } else {
-                        // a tile that meets the core range: the wing form where s >= 196, 0 in the table
-                        // region (a < 8, |v| < 8: the core pass's point), and HVoigt's two-term continued
-                        // fraction for the rest of s < 196, written in u = v^2 (voigt.f90:103-107):
-                        // p = u - a^2 - 3/2, dr = |v| (p - 2a^2), di = a (2u + p), q = 2 a |v|,
-                        // LinCop H = c1 [(p + 1/2)(2u + p) - 2u (p - 2a^2)] / [u (p - 2a^2)^2 + a^2 (2u + p)^2]
 #pragma unroll
                         for (int d = 0; d < D; d++)
 #pragma unroll
                             for (int k = 0; k < P; k++) {
-                                const float t = fmaf(x[k], w[d].vv2, w[d].c2m1);
-                                const float u = __fmul_rn(x[k], w[d].vv2);
-                                const bool wing = t >= 195.5f;
-                                const bool tab = !wing && w[d].twoA < 128.0f && u < 64.0f;
-                                const float pp = u - w[d].c2m1 - 2.0f, pm = pp - w[d].twoA;
-                                const float q2 = fmaf(2.0f, u, pp);
-                                const float ncf = fmaf(pp + 0.5f, q2, -2.0f * u * pm);
-                                const float dcf = fmaf(u * pm, pm, 0.5f * w[d].twoA * q2 * q2);
-                                const float num = wing ? fmaf(w[d].c1, t, w[d].c1) : (tab ? 0.0f : w[d].c1 * ncf);
-                                const float den = wing ? fmaf(t, t, w[d].twoA) : (tab ? 1.0f : dcf);
+                                float t = fmaf(x[k], w[d].vv2, w[d].c2m1);
+                                t = t < 195.5f ? 1.0e19f : t;        // the core pass's point
+                                float den = fmaf(t, t, w[d].twoA);
+                                float num = fmaf(w[d].c1, t, w[d].c1);
                                 part[d][k] = fmaf(num, rcp_approx(den), part[d][k]);
                             }
                     }
@@ -458,12 +455,10 @@ __device__ bool core_tile(const CoreJob &J, int tile, const float4 *__restrict__
                             const float t = fmaf(x, w.vv2, w.c2m1);
                             core[e] = in && d < nd && t < 195.5f;
                             const double av = adl * cr.vv;
-                            // the table region, by the wing pass's own FP32 test (twoA < 128 implies a < 8,
-                            // so ia > 0); the continued-fraction points are the wing pass's
-                            tab[e] = core[e] && w.twoA < 128.0f && __fmul_rn(x, w.vv2) < 64.0f;
+                            tab[e] = core[e] && cr.ia > 0 && av < 8.0;
                             const double fv = av * 125.0;
                             const int iv = tab[e] ? min((int)fv, FSG_NVV - 1) : 0;
-                            tv[e] = tab[e] ? (float)(fv - (double)iv) : 0.0f;
+                            tv[e] = tab[e] ? (float)(fv - (double)iv) : (float)av;   // CF: |v| in FP32
                             cell[e] = tab[e] ? (cr.ia - 1) * FSG_NV1 + iv : 0;
                         }
                         float4 gv[4];
@@ -472,12 +467,17 @@ __device__ bool core_tile(const CoreJob &J, int tile, const float4 *__restrict__
                             if (tab[e]) gv[e] = __ldg(vtab4 + cell[e]);
 #pragma unroll
                         for (int e = 0; e < 4; e++) {
-                            if (!tab[e]) continue;
+                            if (!core[e]) continue;
                             const int d = g0 + e;
                             const CoreRec &cr = cc[q * ntau + t0 + d];
-                            const float4 gg = gv[e];
-                            const float c0 = gg.x + tv[e] * (gg.y - gg.x), c1 = gg.z + tv[e] * (gg.w - gg.z);
-                            const float v = (c0 + cr.ua * (c1 - c0)) * cr.cop;
+                            float v;
+                            if (tab[e]) {
+                                const float4 gg = gv[e];
+                                const float c0 = gg.x + tv[e] * (gg.y - gg.x), c1 = gg.z + tv[e] * (gg.w - gg.z);
+                                v = (c0 + cr.ua * (c1 - c0)) * cr.cop;
+                            } else {
+                                v = hv_cf32(tv[e], cr.a, cr.cop);
+                            }
                             KAHAN(sum[d], cmp[d], v);
                             cnt++;
                         }

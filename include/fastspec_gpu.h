@@ -82,8 +82,7 @@ typedef struct {
     int64_t accum_launches; /* launches of the accumulation kernel */
     double  ms_accum_kernels;   /* summed device time of those launches [ms] */
     double  ms_wing_kernels, ms_core_kernels;   /* mixed path: the wing and core passes of it [ms] */
-    double  core_evals;     /* mixed path: the core pass's evaluations (HVoigt's table region: s < 196,
-                               a < 8, |v| < 8) */
+    double  core_evals;     /* mixed path: the core pass's evaluations (table and continued fraction, s < 196) */
 } fsg_stats;
 
 /* ---- context ------------------------------------------------------------------------- */
@@ -368,7 +367,7 @@ typedef struct {
     double  ms_prepare, ms_wing, ms_core, ms_solve;   /* its stages: central pass, class order, records
                                                        * and tile ranges; wing launches; core launches;
                                                        * formal solver and flux [ms] */
-    double  core_evals;     /* the core pass's evaluations (HVoigt's table region) */
+    double  core_evals;     /* the core pass's evaluations (table and continued fraction, s < 196) */
 } fsg_batch_stats;
 /* On failure *out stays NULL and fsg_batch_last_error(NULL) gives the reason. */
 int  fsg_batch_create(fsg_ctx *const *atms, int natm, const fsg_lines *lines, double margin, fsg_batch **out);
