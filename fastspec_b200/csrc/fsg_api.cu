@@ -2257,6 +2257,11 @@ struct fsg_batch {
     // ev[0..2]: around the wing and core launches; ev[3], ev[4]: around a replay; ev[5..7]: the
     // replay's stage boundaries (before the central pass, after the core launches, after the solver)
     cudaEvent_t ev[8] = {};
+    // per-atmosphere stages run round-robin on these streams, forked from and joined to the batch's
+    // stream (inside a capture they become parallel branches of the graph)
+    static const int NAUX = 8;
+    cudaStream_t aux[NAUX] = {};
+    cudaEvent_t fork = nullptr, join[NAUX] = {};
 };
 
 static LineView batch_view(const fsg_batch *b, const BAtm &a) {
@@ -2274,13 +2279,27 @@ static const int BATCH_NARROW = 1;             // classes 0 .. BATCH_NARROW take
 static int batch_wing_stride(const fsg_ctx *c) { return (c->nwl + 63) / 64; }
 static int batch_core_stride(const fsg_ctx *c) { return (c->nwl + 31) / 32; }
 
+static void batch_fork(fsg_batch *b, cudaStream_t s) {
+    cudaEventRecord(b->fork, s);
+    for (int k = 0; k < fsg_batch::NAUX; k++) cudaStreamWaitEvent(b->aux[k], b->fork, 0);
+}
+static void batch_join(fsg_batch *b, cudaStream_t s) {
+    for (int k = 0; k < fsg_batch::NAUX; k++) {
+        cudaEventRecord(b->join[k], b->aux[k]);
+        cudaStreamWaitEvent(s, b->join[k], 0);
+    }
+}
+
 // the per-atmosphere stages up to the tile ranges: central pass, class order, records in that order,
-// tile ranges per class (wide-class wing tiles of P wavelengths per lane)
+// tile ranges per class (wide-class wing tiles of P wavelengths per lane); atmospheres in parallel on
+// the auxiliary streams
 static int batch_prepare(fsg_batch *b, int P) {
     fsg_ctx *ctx = b->own;
-    cudaStream_t s = ctx->stream;
+    batch_fork(b, ctx->stream);
+    int k = 0;
     for (auto &a : b->atm) {
         if (a.cn == 0) continue;
+        const cudaStream_t s = b->aux[k++ % fsg_batch::NAUX];
         fsg_ctx *c = a.ctx;
         AtmView A = fsg_view(c);
         LineView LV = batch_view(b, a);
@@ -2300,6 +2319,7 @@ static int batch_prepare(fsg_batch *b, int P) {
                                   a.span.cap))
             return cuda_fail(ctx, cudaGetLastError(), "batch tile ranges");
     }
+    batch_join(b, ctx->stream);
     CK(cudaGetLastError(), "batch prepare");
     return FSG_OK;
 }
@@ -2405,13 +2425,16 @@ static int batch_accumulate_solve(fsg_batch *b, const fsg_batch_tuning &t, cudaE
             return cuda_fail(ctx, cudaGetLastError(), "k_core_batch");
     }
     if (ev) batch_mark(ev[2], s);
+    batch_fork(b, s);
+    int k = 0;
     for (auto &a : b->atm) {
         fsg_ctx *c = a.ctx;
-        if (fsg_launch_radtran(s, fsg_view(c), c->d_lineopac.as<double>(), c->d_rhox.as<double>(), c->nmu,
-                               c->d_xmu.as<double>(), c->d_wmu.as<double>(), nullptr, nullptr, a.sfl.as<double>(),
-                               a.sfc.as<double>()))
+        if (fsg_launch_radtran(b->aux[k++ % fsg_batch::NAUX], fsg_view(c), c->d_lineopac.as<double>(),
+                               c->d_rhox.as<double>(), c->nmu, c->d_xmu.as<double>(), c->d_wmu.as<double>(), nullptr,
+                               nullptr, a.sfl.as<double>(), a.sfc.as<double>()))
             return cuda_fail(ctx, cudaGetLastError(), "k_radtran (batch)");
     }
+    batch_join(b, s);
     if (ev && ev[7]) batch_mark(ev[7], s);
     CK(cudaGetLastError(), "batch");
     return FSG_OK;
@@ -2487,6 +2510,12 @@ int fsg_batch_create(fsg_ctx *const *atms, int natm, const fsg_lines *lines, dou
         return bail(FSG_E_NOMEM, "fsg_batch_create: device allocation failed");
     if (cudaMemset(b->err.p, 0, sizeof(int)) != cudaSuccess) return bail(FSG_E_CUDA, "fsg_batch_create: upload failed");
     for (int i = 0; i < 8; i++) cudaEventCreate(&b->ev[i]);
+    if (cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess)
+        return bail(FSG_E_CUDA, "fsg_batch_create: event creation failed");
+    for (int k = 0; k < fsg_batch::NAUX; k++)
+        if (cudaStreamCreateWithFlags(&b->aux[k], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&b->join[k], cudaEventDisableTiming) != cudaSuccess)
+            return bail(FSG_E_CUDA, "fsg_batch_create: stream creation failed");
     b->tune.tile_pix = 128;
     b->tune.wing_ctas = 148;
     b->tune.core_ctas = 4 * 148;
@@ -2653,6 +2682,11 @@ void fsg_batch_destroy(fsg_batch *b) {
                      &b->evals };
     for (DBuf *d : bufs) d->release();
     for (int i = 0; i < 8; i++) if (b->ev[i]) cudaEventDestroy(b->ev[i]);
+    for (int k = 0; k < fsg_batch::NAUX; k++) {
+        if (b->aux[k]) { cudaStreamSynchronize(b->aux[k]); cudaStreamDestroy(b->aux[k]); }
+        if (b->join[k]) cudaEventDestroy(b->join[k]);
+    }
+    if (b->fork) cudaEventDestroy(b->fork);
     fsg_destroy(b->own);
     cudaGetLastError();
     delete b;
