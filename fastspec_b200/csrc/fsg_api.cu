@@ -8,7 +8,55 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
+#include <mutex>
+#include <string>
 #include <vector>
+
+#include <nvtx3/nvToolsExt.h>
+
+// ---- tracing and metrics of the C-ABI drivers -----------------------------------------------------
+// The reference reports each stage of a synthesis (lines read and used, time of the line opacity, then
+// of the radiative transfer: fastspec.f90:393-425, timed by MDtime, utils.f90:63-91).  Here every driver
+// call is an NVTX range (visible to Nsight Systems and to ncu's NVTX filters), and when the environment
+// names a file in FSG_METRICS_JSONL each call appends one JSON line to it: the call, its status, its host
+// wall time and the stage figures it produced.
+namespace {
+struct CallTrace {
+    std::chrono::steady_clock::time_point t0;
+    explicit CallTrace(const char *name) : t0(std::chrono::steady_clock::now()) { nvtxRangePushA(name); }
+    ~CallTrace() { nvtxRangePop(); }
+    double ms() const {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+std::mutex g_metrics_mu;
+bool metrics_on() {
+    const char *p = getenv("FSG_METRICS_JSONL");
+    return p && *p;
+}
+void metrics_emit(const char *call, int rc, double wall_ms, const std::string &fields) {
+    const char *path = getenv("FSG_METRICS_JSONL");
+    if (!path || !*path) return;
+    std::lock_guard<std::mutex> lock(g_metrics_mu);
+    FILE *f = fopen(path, "a");
+    if (!f) return;
+    fprintf(f, "{\"call\": \"%s\", \"rc\": %d, \"wall_ms\": %.6f%s%s}\n", call, rc, wall_ms,
+            fields.empty() ? "" : ", ", fields.c_str());
+    fclose(f);
+}
+std::string stats_fields(const fsg_stats &t) {
+    char b[640];
+    snprintf(b, sizeof b,
+             "\"nlines_in\": %lld, \"nlines_used\": %lld, \"nwide\": %lld, \"nweak\": %lld, \"nblocks\": %lld, "
+             "\"line_evals\": %.17g, \"ms_center\": %.6f, \"ms_params\": %.6f, \"ms_accum\": %.6f, "
+             "\"ms_total\": %.6f, \"ms_wing_kernels\": %.6f, \"ms_core_kernels\": %.6f, \"core_evals\": %.17g",
+             (long long)t.nlines_in, (long long)t.nlines_used, (long long)t.nwide, (long long)t.nweak,
+             (long long)t.nblocks, t.line_evals, t.ms_center, t.ms_params, t.ms_accum, t.ms_total,
+             t.ms_wing_kernels, t.ms_core_kernels, t.core_evals);
+    return b;
+}
+}  // namespace
 
 // ---- kernels defined in fsg_kernels64.cu / fsg_fast.cu / fsg_mag.cu ------------------------------
 void fsg_launch_xline_setup(cudaStream_t, const AtmView &, const LineView &, XCoef *);
@@ -1063,7 +1111,7 @@ int fsg_accumulate_dev(fsg_ctx *ctx, const fsg_lines *d_lines, const int32_t *d_
     return FSG_OK;
 }
 
-int fsg_lineop_calc_dev(fsg_ctx *ctx, const fsg_lines *d_lines, fsg_stats *st) {
+static int lineop_calc_dev_body(fsg_ctx *ctx, const fsg_lines *d_lines, fsg_stats *st) {
     int rc = check_lines(ctx, d_lines); if (rc) return rc;
     cudaSetDevice(ctx->device);
     return lineop_dev(ctx, d_lines, st);
@@ -1093,8 +1141,8 @@ static int linstr_calc(fsg_ctx *ctx, const fsg_lines *D, float *linstr) {
     return FSG_OK;
 }
 
-int fsg_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, double *lineopac, int32_t *flags, int32_t *ileft,
-                    int32_t *iright, float *linstr, fsg_stats *st) {
+static int lineop_calc_body(fsg_ctx *ctx, const fsg_lines *lines, double *lineopac, int32_t *flags,
+                            int32_t *ileft, int32_t *iright, float *linstr, fsg_stats *st) {
     int rc = check_lines(ctx, lines); if (rc) return rc;
     if (linstr && ctx->nmu < 1) return fail(ctx, FSG_E_STATE, "fsg_lineop_calc: line strengths need fsg_set_mu first");
     cudaSetDevice(ctx->device);
@@ -1148,7 +1196,7 @@ static int radtran_dev(fsg_ctx *ctx, double *spl, double *spc, double *sfl, doub
     return FSG_OK;
 }
 
-int fsg_radtran_dev(fsg_ctx *ctx, double *d_spl, double *d_spc, double *d_sfl, double *d_sfc) {
+static int radtran_dev_body(fsg_ctx *ctx, double *d_spl, double *d_spc, double *d_sfl, double *d_sfc) {
     if (!ctx) return FSG_E_ARG;
     cudaSetDevice(ctx->device);
     int rc = radtran_dev(ctx, d_spl, d_spc, d_sfl, d_sfc); if (rc) return rc;
@@ -1156,7 +1204,8 @@ int fsg_radtran_dev(fsg_ctx *ctx, double *d_spl, double *d_spc, double *d_sfl, d
     return FSG_OK;
 }
 
-int fsg_radtran_range_dev(fsg_ctx *ctx, int i0, int i1, double *d_spl, double *d_spc, double *d_sfl, double *d_sfc) {
+static int radtran_range_dev_body(fsg_ctx *ctx, int i0, int i1, double *d_spl, double *d_spc, double *d_sfl,
+                                  double *d_sfc) {
     if (!ctx) return FSG_E_ARG;
     cudaSetDevice(ctx->device);
     int rc = radtran_dev(ctx, d_spl, d_spc, d_sfl, d_sfc, i0, i1); if (rc) return rc;
@@ -1164,7 +1213,7 @@ int fsg_radtran_range_dev(fsg_ctx *ctx, int i0, int i1, double *d_spl, double *d
     return FSG_OK;
 }
 
-int fsg_radtran(fsg_ctx *ctx, double *spl, double *spc, double *sfl, double *sfc) {
+static int radtran_body(fsg_ctx *ctx, double *spl, double *spc, double *sfl, double *sfc) {
     if (!ctx) return FSG_E_ARG;
     cudaSetDevice(ctx->device);
     size_t nsp = sizeof(double) * (size_t)ctx->nwl * ctx->nmu, nf = sizeof(double) * ctx->nwl;
@@ -1202,9 +1251,9 @@ int fsg_mag_lineop_reset(fsg_ctx *ctx) {
     return FSG_OK;
 }
 
-int fsg_mag_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, int bframe, const double *bfield, int nbfield,
-                        double *maglineopac, int32_t *flags, int32_t *ileft, int32_t *iright, float *linstr,
-                        fsg_stats *st) {
+static int mag_lineop_calc_body(fsg_ctx *ctx, const fsg_lines *lines, int bframe, const double *bfield,
+                                int nbfield, double *maglineopac, int32_t *flags, int32_t *ileft, int32_t *iright,
+                                float *linstr, fsg_stats *st) {
     int rc = check_lines(ctx, lines); if (rc) return rc;
     if (linstr && ctx->nmu < 1) return fail(ctx, FSG_E_STATE, "fsg_mag_lineop_calc: line strengths need fsg_set_mu first");
     if (lines->kind != 2) return fail(ctx, FSG_E_ARG, "fsg_mag_lineop_calc: magnetic lists have kind 2");
@@ -1507,8 +1556,8 @@ static int mag_radtran_sph(fsg_ctx *ctx, const RayView &R, int bframe, const dou
 }
 
 
-int fsg_mag_radtran(fsg_ctx *ctx, int bframe, const double *bfield, int nbfield, double *spz, double *spc,
-                    double *sfl, double *sfc) {
+static int mag_radtran_body(fsg_ctx *ctx, int bframe, const double *bfield, int nbfield, double *spz,
+                            double *spc, double *sfl, double *sfc) {
     if (!ctx) return FSG_E_ARG;
     if (!ctx->have_grid || !ctx->have_atm || !ctx->have_cont || ctx->nmu < 1)
         return fail(ctx, FSG_E_STATE, "mag_radtran: set grid, atmosphere, continuum and mu first");
@@ -2600,7 +2649,7 @@ int fsg_batch_set_tuning(fsg_batch *b, const fsg_batch_tuning *t) {
     return FSG_OK;
 }
 
-int fsg_batch_run(fsg_batch *b, fsg_batch_stats *st) {
+static int batch_run_body(fsg_batch *b, fsg_batch_stats *st) {
     if (!b) return FSG_E_ARG;
     fsg_ctx *ctx = b->own;
     cudaSetDevice(ctx->device);
@@ -2690,6 +2739,96 @@ void fsg_batch_destroy(fsg_batch *b) {
     fsg_destroy(b->own);
     cudaGetLastError();
     delete b;
+}
+
+// ---- the drivers' public entries: an NVTX range each, and a metrics line when FSG_METRICS_JSONL is set ----
+static std::string grid_fields(const fsg_ctx *ctx) {
+    char b[160];
+    snprintf(b, sizeof b, "\"nwl\": %d, \"ntau\": %d, \"nmu\": %d", ctx ? ctx->nwl : 0, ctx ? ctx->ntau : 0,
+             ctx ? ctx->nmu : 0);
+    return b;
+}
+
+int fsg_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, double *lineopac, int32_t *flags, int32_t *ileft,
+                    int32_t *iright, float *linstr, fsg_stats *st) {
+    CallTrace tr("fsg_lineop_calc");
+    fsg_stats local{};
+    fsg_stats *s = st ? st : (metrics_on() ? &local : nullptr);
+    const int rc = lineop_calc_body(ctx, lines, lineopac, flags, ileft, iright, linstr, s);
+    if (metrics_on()) metrics_emit("fsg_lineop_calc", rc, tr.ms(), rc || !s ? std::string() : stats_fields(*s));
+    return rc;
+}
+
+int fsg_lineop_calc_dev(fsg_ctx *ctx, const fsg_lines *d_lines, fsg_stats *st) {
+    CallTrace tr("fsg_lineop_calc_dev");
+    fsg_stats local{};
+    fsg_stats *s = st ? st : (metrics_on() ? &local : nullptr);
+    const int rc = lineop_calc_dev_body(ctx, d_lines, s);
+    if (metrics_on()) metrics_emit("fsg_lineop_calc_dev", rc, tr.ms(), rc || !s ? std::string() : stats_fields(*s));
+    return rc;
+}
+
+int fsg_mag_lineop_calc(fsg_ctx *ctx, const fsg_lines *lines, int bframe, const double *bfield, int nbfield,
+                        double *maglineopac, int32_t *flags, int32_t *ileft, int32_t *iright, float *linstr,
+                        fsg_stats *st) {
+    CallTrace tr("fsg_mag_lineop_calc");
+    fsg_stats local{};
+    fsg_stats *s = st ? st : (metrics_on() ? &local : nullptr);
+    const int rc = mag_lineop_calc_body(ctx, lines, bframe, bfield, nbfield, maglineopac, flags, ileft, iright,
+                                        linstr, s);
+    if (metrics_on()) metrics_emit("fsg_mag_lineop_calc", rc, tr.ms(), rc || !s ? std::string() : stats_fields(*s));
+    return rc;
+}
+
+int fsg_radtran(fsg_ctx *ctx, double *spl, double *spc, double *sfl, double *sfc) {
+    CallTrace tr("fsg_radtran");
+    const int rc = radtran_body(ctx, spl, spc, sfl, sfc);
+    if (metrics_on()) metrics_emit("fsg_radtran", rc, tr.ms(), grid_fields(ctx));
+    return rc;
+}
+
+int fsg_radtran_dev(fsg_ctx *ctx, double *d_spl, double *d_spc, double *d_sfl, double *d_sfc) {
+    CallTrace tr("fsg_radtran_dev");
+    const int rc = radtran_dev_body(ctx, d_spl, d_spc, d_sfl, d_sfc);
+    if (metrics_on()) metrics_emit("fsg_radtran_dev", rc, tr.ms(), grid_fields(ctx));
+    return rc;
+}
+
+int fsg_radtran_range_dev(fsg_ctx *ctx, int i0, int i1, double *d_spl, double *d_spc, double *d_sfl, double *d_sfc) {
+    CallTrace tr("fsg_radtran_range_dev");
+    const int rc = radtran_range_dev_body(ctx, i0, i1, d_spl, d_spc, d_sfl, d_sfc);
+    if (metrics_on()) {
+        char b[64];
+        snprintf(b, sizeof b, ", \"i0\": %d, \"i1\": %d", i0, i1);
+        metrics_emit("fsg_radtran_range_dev", rc, tr.ms(), grid_fields(ctx) + b);
+    }
+    return rc;
+}
+
+int fsg_mag_radtran(fsg_ctx *ctx, int bframe, const double *bfield, int nbfield, double *spz, double *spc,
+                    double *sfl, double *sfc) {
+    CallTrace tr("fsg_mag_radtran");
+    const int rc = mag_radtran_body(ctx, bframe, bfield, nbfield, spz, spc, sfl, sfc);
+    if (metrics_on()) metrics_emit("fsg_mag_radtran", rc, tr.ms(), grid_fields(ctx));
+    return rc;
+}
+
+int fsg_batch_run(fsg_batch *b, fsg_batch_stats *st) {
+    CallTrace tr("fsg_batch_run");
+    fsg_batch_stats local{};
+    fsg_batch_stats *s = st ? st : (metrics_on() ? &local : nullptr);
+    const int rc = batch_run_body(b, s);
+    if (metrics_on()) {
+        char f[512] = "";
+        if (!rc && s)
+            snprintf(f, sizeof f,
+                     "\"natm\": %d, \"nlines_candidate\": %lld, \"line_evals\": %.17g, \"ms_total\": %.6f, "
+                     "\"ms_prepare\": %.6f, \"ms_wing\": %.6f, \"ms_core\": %.6f, \"ms_solve\": %.6f, \"core_evals\": %.17g",
+                     s->natm, (long long)s->nlines_candidate, s->line_evals, s->ms_total, s->ms_prepare, s->ms_wing,
+                     s->ms_core, s->ms_solve, s->core_evals);
+        metrics_emit("fsg_batch_run", rc, tr.ms(), f);
+    }
+    return rc;
 }
 
 }  // extern "C"

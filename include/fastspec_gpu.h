@@ -85,6 +85,14 @@ typedef struct {
     double  core_evals;     /* mixed path: the core pass's evaluations (table and continued fraction, s < 196) */
 } fsg_stats;
 
+/* Tracing and metrics.  Every driver call (fsg_lineop_calc(_dev), fsg_mag_lineop_calc, fsg_radtran(_dev),
+ * fsg_radtran_range_dev, fsg_mag_radtran, fsg_batch_run) is an NVTX range named after the entry point.
+ * When the environment variable FSG_METRICS_JSONL names a file, each such call appends one JSON line to
+ * it: the call, its status, its host wall time [ms] and the stage figures it produced (fsg_stats /
+ * fsg_batch_stats fields, or the grid sizes for the solvers) -- the counterpart of the reference's
+ * per-stage reports (lines read and used, time of the line opacity and of the radiative transfer,
+ * fastspec.f90:393-425). */
+
 /* ---- context ------------------------------------------------------------------------- */
 int         fsg_create(const fsg_config *cfg, fsg_ctx **out);
 void        fsg_destroy(fsg_ctx *ctx);
