@@ -2478,10 +2478,16 @@ static int batch_accumulate_solve(fsg_batch *b, const fsg_batch_tuning &t, cudaE
     int k = 0;
     for (auto &a : b->atm) {
         fsg_ctx *c = a.ctx;
-        if (fsg_launch_radtran(b->aux[k++ % fsg_batch::NAUX], fsg_view(c), c->d_lineopac.as<double>(),
-                               c->d_rhox.as<double>(), c->nmu, c->d_xmu.as<double>(), c->d_wmu.as<double>(), nullptr,
-                               nullptr, a.sfl.as<double>(), a.sfc.as<double>()))
-            return cuda_fail(ctx, cudaGetLastError(), "k_radtran (batch)");
+        const cudaStream_t as = b->aux[k++ % fsg_batch::NAUX];
+        RayView R;
+        if (rays_prepare(c, &R)) return fail(ctx, FSG_E_STATE, c->err.c_str());   // built at create
+        const int rr = R.nmu > 0
+            ? fsg_launch_radtran_sph(as, fsg_view(c), c->d_lineopac.as<double>(), R, c->d_wmu.as<double>(), nullptr,
+                                     nullptr, a.sfl.as<double>(), a.sfc.as<double>())
+            : fsg_launch_radtran(as, fsg_view(c), c->d_lineopac.as<double>(), c->d_rhox.as<double>(), c->nmu,
+                                 c->d_xmu.as<double>(), c->d_wmu.as<double>(), nullptr, nullptr, a.sfl.as<double>(),
+                                 a.sfc.as<double>());
+        if (rr) return cuda_fail(ctx, cudaGetLastError(), "k_radtran (batch)");
     }
     batch_join(b, s);
     if (ev && ev[7]) batch_mark(ev[7], s);
@@ -2509,7 +2515,10 @@ int fsg_batch_create(fsg_ctx *const *atms, int natm, const fsg_lines *lines, dou
         if (!c->have_grid || !c->have_atm || !c->have_cont || c->nmu < 1)
             return bail(FSG_E_STATE, "fsg_batch_create: set grid, atmosphere, continuum and mu of every context");
         if (c->ntau > 128) return bail(FSG_E_ARG, "fsg_batch_create: ntau <= 128");
-        if (c->radius > 0.0) return bail(FSG_E_ARG, "fsg_batch_create: plane-parallel models only");
+        if (c->radius > 0.0) {                         // spherical: the rays (SphereInit) built now, once
+            RayView R;
+            if (rays_prepare(c, &R)) return bail(FSG_E_ARG, c->err.c_str());
+        }
     }
     rc = check_lines(atms[0], lines); if (rc) return bail(rc, atms[0]->err.c_str());
     bool has_he = false;

@@ -353,9 +353,12 @@ int fsg_set_fault(fsg_ctx *ctx, int kind, double value);
  * result is the reference's run of its deck on the shared list; margin > 0 adds the lines just
  * outside, whose windows the reference's WaveIdx clamps to the grid's ends (opacity.f90:594-608).
  * Each atmosphere's records are grouped by window-width class; atmospheres are grouped by depth
- * count (buckets of 8).  Per group and class, a persistent wing-pass launch and a persistent
- * core-pass launch take (atmosphere, tile) items from device work queues; then the formal solver
- * and flux run per atmosphere.  The sequence has no host synchronisation; the
+ * count (buckets of 8).  Per group, persistent launches (wing pass over the narrow classes, wing pass
+ * over the wide ones, core pass) take (atmosphere, tile) items from device work queues, each tile
+ * adding its classes in turn; then the formal solver and flux run per atmosphere, plane-parallel or
+ * spherical as each context's geometry says (the rays of a spherical one are built by
+ * fsg_batch_create, so the contexts' geometry and angles must not change after it).  The sequence
+ * has no host synchronisation; the
  * first fsg_batch_run tunes it (unless fsg_batch_set_tuning gave a choice), captures it as a CUDA
  * graph and replays it; later runs replay.  No counterpart in the reference, which synthesises
  * one atmosphere per run (fastspec.f90:192-449). */

@@ -88,6 +88,31 @@ def test_batch_replay_and_given_tuning(fsg):
     B.close()
 
 
+def test_batch_spherical_member(fsg):
+    """An atmosphere given a spherical geometry inside a batch is solved along its rays (LocPrfSph,
+    solver.f90:182-261) in the batch's graph: its flux equals the single-context spherical synthesis of
+    the same lines, and the plane-parallel members are unchanged."""
+    ctxs, cases, arr = small_batch(fsg, natm=3, seed=9)
+    g1, st1, _ = cases[1]
+    rhox, rho = np.asarray(st1["rhox"], float), np.asarray(st1["rho"], float)
+    h = np.zeros(len(rhox))                                  # hydrostatic heights, decreasing inward
+    for k in range(1, len(rhox)):
+        h[k] = h[k - 1] - (rhox[k] - rhox[k - 1]) / (0.5 * (rho[k] + rho[k - 1]))
+    h -= h[-1]
+    ctxs[1].set_geometry(3.0e11, h)
+    B = fsg.Batch(ctxs, fsg.LineList.from_arrays(arr))
+    B.run()
+    for i, (g, state, co) in enumerate(cases):
+        sfl, sfc = B.flux(i)
+        C = ctxs[i]
+        C.lineop_reset()
+        C.lineop_calc(fsg.LineList.from_arrays(candidates(arr, g)), want_lineopac=False, want_lines=False)
+        _, _, csfl, csfc = C.radtran()
+        assert np.max(np.abs(sfl / csfl - 1)) < 1e-6, i
+        assert np.max(np.abs(sfc / csfc - 1)) < 1e-12, i
+    B.close()
+
+
 def test_batch_rejects_bad_inputs(fsg):
     ctxs, cases, arr = small_batch(fsg, natm=2, seed=7, nlines=2000)
     bad = {k: v[::-1].copy() for k, v in arr.items()}                  # not sorted
