@@ -388,15 +388,16 @@ __device__ __forceinline__ double stokes_point(const double *m, double lop, doub
     return PI;
 }
 
-// StokesPrfPP, one thread per (wavelength, angle) from the first wavelength iwl0 on: each thread builds
-// its propagation data, TauStep and CentDer over depth into its own global work arrays (STK_FIELDS x
-// ntau doubles, element stride = the launch's thread count T, so that the threads of a warp touch
-// consecutive addresses) and runs the sequential 4x4 sweep itself; every lane of every warp sweeps.
-// The reference's operations, in its order.
+// StokesPrfPP, one thread per (wavelength, angle) from the first wavelength iwl0 on, in two launches
+// over per-thread global work arrays (STK_FIELDS x ntau doubles, element stride = the launch's thread
+// count T, so that the threads of a warp touch consecutive addresses).  k_stokes_prep builds the
+// propagation data, TauStep and CentDer over depth; it needs few registers, so many warps hide the
+// latency of its array traffic.  k_stokes_thr runs the sequential 4x4 sweep (about 200 registers);
+// every lane of every warp sweeps.  The reference's operations, in its order.
 __global__ void __launch_bounds__(128)
-k_stokes_thr(AtmView A, const double *__restrict__ lineopac, const double *__restrict__ mlo,
-             const double *__restrict__ rhox, int nmu, const double *__restrict__ xmu,
-             const double *__restrict__ geo, int iwl0, int nwl_chunk, double *work, double *spz) {
+k_stokes_prep(AtmView A, const double *__restrict__ lineopac, const double *__restrict__ mlo,
+              const double *__restrict__ rhox, int nmu, const double *__restrict__ xmu,
+              const double *__restrict__ geo, int iwl0, int nwl_chunk, double *work) {
     const size_t T = (size_t)gridDim.x * blockDim.x;
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= nwl_chunk * nmu) return;
@@ -452,6 +453,18 @@ k_stokes_thr(AtmView A, const double *__restrict__ lineopac, const double *__res
             F(fo, k) = out;
         }
     }
+#undef F
+}
+
+__global__ void __launch_bounds__(128)
+k_stokes_thr(AtmView A, int nmu, int iwl0, int nwl_chunk, const double *work, double *spz) {
+    const size_t T = (size_t)gridDim.x * blockDim.x;
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= nwl_chunk * nmu) return;
+    const int iwl = iwl0 + g / nmu, im = g - (g / nmu) * nmu;
+    const int N = A.ntau;
+    const double *W = work + g;
+#define F(f, t) W[((size_t)(f) * N + (t)) * T]
     double XINT2[4] = { F(13, N - 1), 0.0, 0.0, 0.0 };
     stokes_sweep(N, N, &F(1, 0), &F(7, 0), &F(13, 0), &F(17, 0), &F(21, 0), XINT2, T);
     for (int q = 0; q < 4; q++) spz[((size_t)iwl * 4 + q) * nmu + im] = XINT2[q];
@@ -568,7 +581,8 @@ int fsg_launch_stokes(cudaStream_t s, const AtmView &A, const double *lineopac, 
     for (int w0 = 0; w0 < A.nwl; w0 += nwl_chunk) {
         const int nw = std::min(nwl_chunk, A.nwl - w0);
         const int nb = (nwl_chunk * nmu + 127) / 128;      // the grid of a full chunk: fixed element stride
-        k_stokes_thr<<<nb, 128, 0, s>>>(A, lineopac, mlo, rhox, nmu, xmu, geo, w0, nw, work, spz);
+        k_stokes_prep<<<nb, 128, 0, s>>>(A, lineopac, mlo, rhox, nmu, xmu, geo, w0, nw, work);
+        k_stokes_thr<<<nb, 128, 0, s>>>(A, nmu, w0, nw, work, spz);
     }
     if (sfl) k_stokes_flux<<<(A.nwl + 127) / 128, 128, 0, s>>>(A.nwl, nmu, spz, wmu, sfl);
     return cudaGetLastError() == cudaSuccess ? FSG_OK : FSG_E_CUDA;
