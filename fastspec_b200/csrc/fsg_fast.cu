@@ -45,8 +45,9 @@ __device__ __forceinline__ float hv_cf32(float av, float a, float cop) {
 // memory.  The partials carry at most FOLD terms, so their rounding stays at the FP32 unit
 // roundoff of a few terms; the Kahan pairs carry the long sums.
 #define FOLD 32
-// Candidate lines staged per TMA bulk copy (double-buffered)
+// Candidate lines staged per TMA bulk copy, and the wing pass's staging buffers (copies in flight)
 #define CH 32
+#define WNB 2
 // cp.async.bulk moves multiples of 16 bytes between 16-byte aligned addresses
 static_assert(sizeof(WingRec) % 16 == 0 && sizeof(LineHdr) % 16 == 0 && sizeof(CoreRec) % 16 == 0, "bulk-copied records: multiples of 16 bytes");
 
@@ -79,11 +80,11 @@ __device__ __forceinline__ float rcp_approx(float x) {
 // once.
 
 // shared memory of the wing pass for at most ntau_max depths:
-// wing records [2][CH][ntau_max] | headers [2][CH] | mbarriers [2] | Kahan pairs [D * P][blockDim.x]
+// wing records [WNB][CH][ntau_max] | headers [WNB][CH] | mbarriers [WNB] | Kahan pairs [D * P][blockDim.x]
 // (a warp reads up to D - 1 <= 7 records past its line's last depth: at most 112 bytes past the
-// second record buffer, inside the 2 KB of headers that follow it)
+// last record buffer, inside the headers that follow it)
 __host__ __device__ inline size_t wing_smem_recs(int ntau_max) {
-    return sizeof(WingRec) * 2 * CH * (size_t)ntau_max + sizeof(LineHdr) * 2 * CH;
+    return sizeof(WingRec) * WNB * CH * (size_t)ntau_max + sizeof(LineHdr) * WNB * CH;
 }
 
 // One tile of one job.  Called by every thread of the CTA with the mbarriers initialised; kk counts
@@ -97,9 +98,9 @@ __device__ __forceinline__ bool wing_tile(const WingJob &J, int tile, unsigned c
     const LineHdr *__restrict__ hdr = J.hdr;
     const WingRec *__restrict__ wing = J.wing;
     WingRec *swing = (WingRec *)smem_raw;
-    LineHdr *shdr = (LineHdr *)(swing + 2 * CH * ntau_max);
-    uint64_t *bars = (uint64_t *)(shdr + 2 * CH);
-    float2 *ksum = (float2 *)(bars + 2);                 // [D * P][blockDim.x]
+    LineHdr *shdr = (LineHdr *)(swing + WNB * CH * ntau_max);
+    uint64_t *bars = (uint64_t *)(shdr + WNB * CH);
+    float2 *ksum = (float2 *)(bars + WNB);               // [D * P][blockDim.x]
     constexpr int TW = 32 * P;
     bool any = false;                                   // some segment has lines touching the tile
     for (int sg = 0; sg < J.nseg; sg++)
@@ -135,10 +136,10 @@ __device__ __forceinline__ bool wing_tile(const WingJob &J, int tile, unsigned c
         const int lo = J.tile_lo[sg * J.seg_stride + tile], hi = J.tile_hi[sg * J.seg_stride + tile];
         if (lo > hi) continue;
         const int nchunks = (hi - lo + CH) / CH;
-        // chunk c of this tile is the CTA's chunk g = kk + c: buffer g & 1, phase parity (g >> 1) & 1
+        // chunk c of this tile is the CTA's chunk g = kk + c: buffer g % WNB, phase parity (g / WNB) & 1
         if (threadIdx.x == 0) {
-            for (int c = 0; c < 2 && c < nchunks; c++) {
-                const int b = (kk + c) & 1;
+            for (int c = 0; c < WNB && c < nchunks; c++) {
+                const int b = (kk + c) % WNB;
                 stage_chunk(c, lo, hi, ntau, hdr, wing, shdr + b * CH, swing + b * CH * ntau_max, &bars[b],
                             J.extra_tx);
             }
@@ -146,8 +147,8 @@ __device__ __forceinline__ bool wing_tile(const WingJob &J, int tile, unsigned c
         int failed = -1;                                     // chunk whose copy did not complete
         for (int c = 0; c < nchunks; c++) {
             const unsigned g = kk + c;
-            const int b = g & 1;
-            const bool ok = mbar_wait(&bars[b], (g >> 1) & 1, J.wait_ns);
+            const int b = g % WNB;
+            const bool ok = mbar_wait(&bars[b], (g / WNB) & 1, J.wait_ns);
             if (__syncthreads_or(!ok)) { failed = c; break; }
             const LineHdr *ch = shdr + b * CH;
             const WingRec *cw = swing + b * CH * ntau_max;
@@ -219,18 +220,18 @@ __device__ __forceinline__ bool wing_tile(const WingJob &J, int tile, unsigned c
                 }
             }
             __syncthreads();                                   // every warp is done with buffer b
-            if (threadIdx.x == 0 && c + 2 < nchunks)
-                stage_chunk(c + 2, lo, hi, ntau, hdr, wing, shdr + b * CH, swing + b * CH * ntau_max, &bars[b],
+            if (threadIdx.x == 0 && c + WNB < nchunks)
+                stage_chunk(c + WNB, lo, hi, ntau, hdr, wing, shdr + b * CH, swing + b * CH * ntau_max, &bars[b],
                             J.extra_tx);
         }
         if (failed >= 0) {
             // a copy never completed: report, then wait (bounded) for the copies still in flight,
-            // chunks failed and failed + 1, before the CTA's shared memory is released
+            // chunks failed .. failed + WNB - 1, before the CTA's shared memory is released
             if (threadIdx.x == 0) {
                 atomicExch(err, FSG_E_TIMEOUT);
-                for (int c = failed; c < nchunks && c < failed + 2; c++) {
+                for (int c = failed; c < nchunks && c < failed + WNB; c++) {
                     const unsigned g = kk + c;
-                    mbar_wait(&bars[g & 1], (g >> 1) & 1, J.wait_ns);
+                    mbar_wait(&bars[g % WNB], (g / WNB) & 1, J.wait_ns);
                 }
             }
             __syncthreads();
@@ -256,8 +257,7 @@ __device__ __forceinline__ bool wing_tile(const WingJob &J, int tile, unsigned c
 __device__ __forceinline__ void wing_bars_init(unsigned char *smem_raw, int ntau_max) {
     uint64_t *bars = (uint64_t *)(smem_raw + wing_smem_recs(ntau_max));
     if (threadIdx.x == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
+        for (int b = 0; b < WNB; b++) mbar_init(&bars[b], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -312,7 +312,7 @@ static int wing_depths(int P, int ntau) {
 
 size_t fsg_wing_smem(int P, int ntau_max) {
     const int D = wing_depths(P, ntau_max), nwarps = (ntau_max + D - 1) / D;
-    return wing_smem_recs(ntau_max) + 2 * sizeof(uint64_t) + sizeof(float2) * (size_t)D * P * 32 * nwarps;
+    return wing_smem_recs(ntau_max) + WNB * sizeof(uint64_t) + sizeof(float2) * (size_t)D * P * 32 * nwarps;
 }
 
 #define WING_DISPATCH(P, D, LAUNCH) do { \
