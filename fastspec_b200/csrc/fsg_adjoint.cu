@@ -158,32 +158,165 @@ __global__ void k_solver_adjoint(AtmView A, const double *__restrict__ lineopac,
     wvl[w] = (float)(wv - (double)wvh[w]);
 }
 
+// Spherical models: the same chain along each ray of LocPrfSph (solver.f90:182-261, the forward is
+// delo_ray): per ray the TauStep steps on the ray's column mass, CentDer of the source, the Bezier
+// terms and the sweep (grazing rays start from zero at the far side), run backwards from dL/dI_ray =
+// Wmu dL/dSfL; a ray point's derivative goes to the layer it samples.  One thread per wavelength; work:
+// per wavelength X, Y, GX by layer (3 nt) and D, R, U, YS, GD, GR, GU by ray point (7 x 2 nt).
+#define SPH_WORK 17
+__global__ void k_solver_adjoint_sph(AtmView A, const double *__restrict__ lineopac, RayView RV,
+                                     const double *__restrict__ wmu, const double *__restrict__ gflux,
+                                     double *__restrict__ gkappa, double *work, float *__restrict__ gk32,
+                                     float *__restrict__ wvh, float *__restrict__ wvl) {
+    const int w = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nwl = A.nwl, nt = A.ntau, M = 2 * nt;
+    if (w >= nwl) return;
+    const double PlkC1 = FSG_HC * FSG_VC * 1e13 / FSG_KBOLT;
+    // layer arrays at 0, nt, 2 nt; ray-point arrays at 3 nt + k M
+    auto L = [&](int k, int t) -> double & { return work[((size_t)k * nt + t) * nwl + w]; };
+    auto P = [&](int k, int j) -> double & { return work[((size_t)3 * nt + (size_t)k * M + j) * nwl + w]; };
+    enum { X, Y, GX };
+    enum { D, R, U, YS, GD, GR, GU };
+    const double wl = A.wave[w] + A.wfirst;
+    const double C1 = PlkC1 / wl, C2 = exp(50.7649141 - 5.0 * log(wl));
+    for (int t = 0; t < nt; t++) {
+        size_t g = (size_t)w * nt + t;
+        L(X, t) = A.contopac[g] + lineopac[g];
+        L(Y, t) = C2 / (exp(C1 / A.xi[XI_T * nt + t]) - 1.0);
+        L(GX, t) = 0.0;
+    }
+    const double gF = gflux[w];
+    for (int im = 0; im < RV.nmu; im++) {
+        const int N = RV.n[im];
+        const int *mp = RV.map + (size_t)im * RV.stride;
+        const double *m = RV.m + (size_t)im * RV.stride;
+        auto x = [&](int j) { return L(X, mp[j]); };
+        auto y = [&](int j) { return L(Y, mp[j]); };
+        // forward: TauStep on the ray, CentDer of the source, Bezier terms, the sweep (storing Y_j)
+        for (int j = 0; j <= N - 2; j++) {
+            double d;
+            if (j == 0) {
+                const double Dx1 = m[1] - m[0], Yp = (x(1) - x(0)) / Dx1;
+                d = Dx1 * (x(1) + 2.0 * x(0) + Dx1 / 2.0 * Yp) / 3.0;
+            } else {
+                const double Dx = m[j] - m[j - 1], Dx1 = m[j + 1] - m[j];
+                const double Der = (x(j) - x(j - 1)) / Dx, Der1 = (x(j + 1) - x(j)) / Dx1;
+                double Yp = 0.0;
+                if (Der * Der1 > 0.0) {
+                    const double Lambda = (1.0 + Dx1 / (Dx + Dx1)) / 3.0;
+                    Yp = (Der / (Lambda * Der1 + (1.0 - Lambda) * Der)) * Der1;
+                }
+                d = Dx1 * (x(j + 1) + 2.0 * x(j) + Dx1 / 2.0 * Yp) / 3.0;
+            }
+            P(D, j) = d;
+            P(GD, j) = 0.0; P(GU, j) = 0.0;
+        }
+        for (int j = 0; j < N; j++) P(GR, j) = 0.0;
+        P(R, 0) = (y(1) - y(0)) / P(D, 0);
+        P(R, N - 1) = (y(N - 1) - y(N - 2)) / P(D, N - 2);
+        for (int j = 1; j <= N - 2; j++) P(R, j) = centder3(P(D, j - 1), P(D, j), y(j - 1), y(j), y(j + 1));
+        for (int j = 0; j <= N - 2; j++)
+            P(U, j) = 0.5 * (y(j) + 0.5 * P(D, j) * P(R, j) + y(j + 1) - 0.5 * P(D, j) * P(R, j + 1));
+        double Yv = RV.graz[im] ? 0.0 : y(N - 1);
+        P(YS, N - 1) = Yv;
+        for (int j = N - 2; j >= 0; j--) {
+            double E, Al, Be, Ga;
+            delo_coef(P(D, j), E, Al, Be, Ga);
+            Yv = Yv * E + Al * y(j) + Be * y(j + 1) + Ga * P(U, j);
+            P(YS, j) = Yv;
+        }
+        // backward from dL/dI = Wmu dL/dSfL
+        double gY = wmu[im] * gF;
+        for (int j = 0; j <= N - 2; j++) {
+            double E, Al, Be, Ga, dE, dAl, dBe, dGa;
+            delo_coef_d(P(D, j), E, Al, Be, Ga, dE, dAl, dBe, dGa);
+            P(GD, j) += gY * (P(YS, j + 1) * dE + y(j) * dAl + y(j + 1) * dBe + P(U, j) * dGa);
+            P(GU, j) += gY * Ga;
+            gY = gY * E;
+        }
+        for (int j = 0; j <= N - 2; j++) {                 // U_j -> D_j, R_j, R_j+1
+            const double gu = P(GU, j);
+            P(GD, j) += gu * 0.25 * (P(R, j) - P(R, j + 1));
+            P(GR, j) += gu * 0.25 * P(D, j);
+            P(GR, j + 1) -= gu * 0.25 * P(D, j);
+        }
+        P(GD, 0) -= P(GR, 0) * P(R, 0) / P(D, 0);          // CentDer -> D
+        P(GD, N - 2) -= P(GR, N - 1) * P(R, N - 1) / P(D, N - 2);
+        for (int j = 1; j <= N - 2; j++) {
+            const double Dx = P(D, j - 1), Dx1 = P(D, j);
+            const double Der = (y(j) - y(j - 1)) / Dx, Der1 = (y(j + 1) - y(j)) / Dx1;
+            if (!(Der * Der1 > 0.0)) continue;
+            double Lambda = (1.0 + Dx1 / (Dx + Dx1)) / 3.0, Yp, dDer, dDer1, dLam;
+            hmean_d(Der, Der1, Lambda, Yp, dDer, dDer1, dLam);
+            const double sm = Dx + Dx1, g = P(GR, j);
+            P(GD, j - 1) += g * (dDer * (-Der / Dx) + dLam * (-Dx1 / (3.0 * sm * sm)));
+            P(GD, j) += g * (dDer1 * (-Der1 / Dx1) + dLam * (Dx / (3.0 * sm * sm)));
+        }
+        {                                                  // TauStep -> the opacity of each ray point's layer
+            const double Dx1 = m[1] - m[0];
+            L(GX, mp[0]) += P(GD, 0) * 0.5 * Dx1;
+            L(GX, mp[1]) += P(GD, 0) * 0.5 * Dx1;
+        }
+        for (int j = 1; j <= N - 2; j++) {
+            const double Dx = m[j] - m[j - 1], Dx1 = m[j + 1] - m[j];
+            const double Der = (x(j) - x(j - 1)) / Dx, Der1 = (x(j + 1) - x(j)) / Dx1;
+            const double g = P(GD, j);
+            L(GX, mp[j + 1]) += g * Dx1 / 3.0;
+            L(GX, mp[j]) += g * 2.0 * Dx1 / 3.0;
+            if (Der * Der1 > 0.0) {
+                double Lambda = (1.0 + Dx1 / (Dx + Dx1)) / 3.0, Yp, dDer, dDer1, dLam;
+                hmean_d(Der, Der1, Lambda, Yp, dDer, dDer1, dLam);
+                const double c = g * Dx1 * Dx1 / 6.0;
+                L(GX, mp[j + 1]) += c * dDer1 / Dx1;
+                L(GX, mp[j]) += c * (dDer / Dx - dDer1 / Dx1);
+                L(GX, mp[j - 1]) += c * (-dDer / Dx);
+            }
+        }
+    }
+    for (int t = 0; t < nt; t++) {
+        gkappa[(size_t)w * nt + t] = L(GX, t);
+        gk32[(size_t)t * nwl + w] = (float)L(GX, t);
+    }
+    const double wv = A.wave[w];
+    wvh[w] = (float)wv;
+    wvl[w] = (float)(wv - (double)wvh[w]);
+}
+
 size_t fsg_line_adjoint_work(int, int, int64_t);
 int fsg_launch_line_adjoint(cudaStream_t, const AtmView &, const LineView &, const VoigtTables &, const int32_t *,
                             const int32_t *, const int32_t *, const double *, const float *, const float *,
                             const float *, double, double *, double *, void *, int, int);
 
-// solver work (10 x nt x nwl doubles), dL/dkappa in FP32, the wavelength offsets as FP32 hi + lo,
-// then the line pass's workspace
-static size_t solver_part(int nwl, int nt) {
-    return (sizeof(double) * 10 * (size_t)nt * nwl + sizeof(float) * ((size_t)nt * nwl + 2 * (size_t)nwl) + 255) &
-           ~(size_t)255;
+// solver work (10 x nt x nwl doubles; SPH_WORK x nt x nwl for spherical models), dL/dkappa in FP32,
+// the wavelength offsets as FP32 hi + lo, then the line pass's workspace
+static size_t solver_doubles(int nwl, int nt, int sph) { return (size_t)(sph ? SPH_WORK : 10) * nt * nwl; }
+static size_t solver_part(int nwl, int nt, int sph) {
+    return (sizeof(double) * solver_doubles(nwl, nt, sph) + sizeof(float) * ((size_t)nt * nwl + 2 * (size_t)nwl) +
+            255) & ~(size_t)255;
 }
 
-size_t fsg_adjoint_work(int nwl, int nt, int64_t n) {
-    return solver_part(nwl, nt) + fsg_line_adjoint_work(nwl, nt, n) + 256;
+size_t fsg_adjoint_work(int nwl, int nt, int64_t n, int sph) {
+    return solver_part(nwl, nt, sph) + fsg_line_adjoint_work(nwl, nt, n) + 256;
 }
 
+// rays: the spherical model's rays (nmu = 0: plane-parallel)
 int fsg_launch_adjoint(cudaStream_t s, const AtmView &A, const LineView &L, const VoigtTables &T,
                        const double *lineopac, const double *rhox, int nmu, const double *xmu, const double *wmu,
-                       const int32_t *flags, const int32_t *ileft, const int32_t *iright, const double *gflux,
-                       double *gkappa, double *work, double vmic, double *glin, double *gvmic, int i0, int i1) {
-    float *gk32 = (float *)(work + 10 * (size_t)A.ntau * A.nwl), *wvh = gk32 + (size_t)A.ntau * A.nwl, *wvl = wvh + A.nwl;
-    k_solver_adjoint<<<(A.nwl + 127) / 128, 128, 0, s>>>(A, lineopac, rhox, nmu, xmu, wmu, gflux, gkappa, work, gk32,
-                                                          wvh, wvl);
+                       const RayView &rays, const int32_t *flags, const int32_t *ileft, const int32_t *iright,
+                       const double *gflux, double *gkappa, double *work, double vmic, double *glin, double *gvmic,
+                       int i0, int i1) {
+    const int sph = rays.nmu > 0;
+    float *gk32 = (float *)(work + solver_doubles(A.nwl, A.ntau, sph)), *wvh = gk32 + (size_t)A.ntau * A.nwl;
+    float *wvl = wvh + A.nwl;
+    if (sph)
+        k_solver_adjoint_sph<<<(A.nwl + 127) / 128, 128, 0, s>>>(A, lineopac, rays, wmu, gflux, gkappa, work, gk32,
+                                                                  wvh, wvl);
+    else
+        k_solver_adjoint<<<(A.nwl + 127) / 128, 128, 0, s>>>(A, lineopac, rhox, nmu, xmu, wmu, gflux, gkappa, work,
+                                                              gk32, wvh, wvl);
     if (cudaGetLastError() != cudaSuccess) return FSG_E_CUDA;
     if (L.n > 0)
         return fsg_launch_line_adjoint(s, A, L, T, flags, ileft, iright, gkappa, gk32, wvh, wvl, vmic, glin, gvmic,
-                                       (char *)work + solver_part(A.nwl, A.ntau), i0, i1);
+                                       (char *)work + solver_part(A.nwl, A.ntau, sph), i0, i1);
     return FSG_OK;
 }

@@ -124,10 +124,11 @@ size_t fsg_mag_rec_bytes();
 int fsg_launch_mag_fast(cudaStream_t, const AtmView &, const LineHdr *, const void *, const int64_t *, const ZView &,
                         const int *, const int *, const VoigtTables &, double *);
 void fsg_launch_conv(cudaStream_t, int, const double *, int, const double *, int, double *, const double *, double);
-size_t fsg_adjoint_work(int, int, int64_t);
+size_t fsg_adjoint_work(int, int, int64_t, int);
 int fsg_launch_adjoint(cudaStream_t, const AtmView &, const LineView &, const VoigtTables &, const double *,
-                       const double *, int, const double *, const double *, const int32_t *, const int32_t *,
-                       const int32_t *, const double *, double *, double *, double, double *, double *, int, int);
+                       const double *, int, const double *, const double *, const RayView &, const int32_t *,
+                       const int32_t *, const int32_t *, const double *, double *, double *, double, double *,
+                       double *, int, int);
 size_t fsg_linstr_work(int64_t, int, int);
 void fsg_launch_linstr(cudaStream_t, const AtmView &, const LineView &, const VoigtTables &, const int32_t *, int64_t,
                        int64_t, int, const double *, const double *, const double *, const RayView &, double *, float *);
@@ -2251,16 +2252,17 @@ static int adjoint_common(fsg_ctx *ctx, const fsg_lines *d_lines, const int32_t 
                           double *d_gvmic) {
     int rc;
     if (ctx->nmu < 1) return fail(ctx, FSG_E_STATE, "fsg_adjoint_dev: set mu first");
-    if (ctx->radius > 0.0) return fail(ctx, FSG_E_STATE, "fsg_adjoint_dev: plane-parallel models only");
     if (!d_gflux || !d_glin || !d_gvmic) return fail(ctx, FSG_E_ARG, "fsg_adjoint_dev: null argument");
     cudaSetDevice(ctx->device);
     rc = ensure_lineopac(ctx); if (rc) return rc;
     const size_t ng = sizeof(double) * (size_t)ctx->nwl * ctx->ntau;
     if (!d_gkappa) { ALLOC(ctx->d_gkappa, ng); d_gkappa = ctx->d_gkappa.as<double>(); }
-    ALLOC(ctx->d_adjwork, fsg_adjoint_work(ctx->nwl, ctx->ntau, d_lines->n));
+    RayView rays;                                      // spherical models: the rays of LocPrfSph
+    rc = rays_prepare(ctx, &rays); if (rc) return rc;
+    ALLOC(ctx->d_adjwork, fsg_adjoint_work(ctx->nwl, ctx->ntau, d_lines->n, rays.nmu > 0));
     rc = fsg_launch_adjoint(ctx->stream, fsg_view(ctx), make_view(d_lines), ctx->tab, ctx->d_lineopac.as<double>(),
                             ctx->d_rhox.as<double>(), ctx->nmu, ctx->d_xmu.as<double>(), ctx->d_wmu.as<double>(),
-                            fl, il, ir, d_gflux, d_gkappa, ctx->d_adjwork.as<double>(), ctx->cfg.vmicro, d_glin,
+                            rays, fl, il, ir, d_gflux, d_gkappa, ctx->d_adjwork.as<double>(), ctx->cfg.vmicro, d_glin,
                             d_gvmic, i0, i1);
     ctx->launches += 2;
     if (rc) return cuda_fail(ctx, cudaGetLastError(), "adjoint");

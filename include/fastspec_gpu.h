@@ -126,8 +126,8 @@ int fsg_set_atmosphere(fsg_ctx *ctx, int ntau, const double *rhox, const double 
  * (height may then be NULL).  fsg_set_atmosphere resets the model to plane-parallel, as reading a new
  * model does, so call this after it.  The rays (one per angle of fsg_set_mu) are built on the host at
  * the next RadTranCalc / LinStrCalc / MagRadTranCalc call, which then solve along them (LocPrfSph,
- * StokesPrfSph; errors: an angle mu <= 0, a ray tangent in the top layer).  The adjoint and the batched
- * path take plane-parallel models only.  Replaces Radius/Atmos%Height (shared.f90:520-527). */
+ * StokesPrfSph; errors: an angle mu <= 0, a ray tangent in the top layer); the batched path and the
+ * adjoint solve along them too.  Replaces Radius/Atmos%Height (shared.f90:520-527). */
 int fsg_set_geometry(fsg_ctx *ctx, double radius, const double *height);
 /* Continuum opacity ContOpac [nwl][ntau] (ContopCalc output, synth.f90:642-674), ContOpacStd
  * [ntau] (may be NULL when motype == 0) and the model type (Motype). */
@@ -313,7 +313,8 @@ int fsg_zeeman_pattern(float jlo, float jup, float glo, float gup, int32_t *npi,
  * fsg_set_vmicro changes the microturbulence of later calls [km/s]; fsg_set_fractionpf replaces the
  * FractionPF of fsg_set_atmosphere ([ntau][nspc]) and keeps the rest of the atmosphere.
  * fsg_adjoint_dev: given d_gflux = dL/dSfL [nwl] (device) for the flux of the last fsg_radtran(_dev)
- * of this context, computes with one backward sweep of the DELO-Bezier solver per wavelength
+ * of this context, computes with one backward sweep of the DELO-Bezier solver per wavelength (per ray
+ * of a spherical model, each ray point's derivative returned to the layer it samples)
  * d_gkappa = dL/dLineOpac [nwl][ntau] (may be NULL: kept inside the context), and per line of the
  * device list d_lines -- which must be the list of the last fsg_lineop_calc(_dev), whose windows it
  * uses -- d_glin[l] = sum dL/dLineOpac * H * LinCop (= dL/d ln gf_l and, summed over an element's

@@ -94,6 +94,39 @@ def test_gradients_vs_finite_differences(fsg):
     M.close()
 
 
+def test_spherical_gradients_vs_finite_differences(fsg):
+    """The same atmosphere as a spherical model (the radius and layer heights of the reference's
+    spherical pin; the seven quadrature rays of LocPrfSph, solver.f90:182-261): the adjoint runs each
+    ray's sweep backwards and returns a ray point's derivative to the layer it samples.  Gradients
+    against central finite differences of the FP64 spherical forward, and different from the
+    plane-parallel model's."""
+    from fastspec_b200 import adjoint as AD
+    d = H.sphere_pin("s")
+    M, arr = model(fsg, fsg.PREC_FP64)
+    loggf0 = np.log10(arr["gf"].astype(np.float64))
+    fobs = target(M, loggf0)
+    gl_pp, ga_pp, _ = grads(M, loggf0, fobs)
+    M.C.set_geometry(float(d["radius"]), d["height"])
+    gl, ga, gv = grads(M, loggf0, fobs)
+    ne = len(AD.ELEMENTS)
+    h = 1e-4
+    for el in ELS:
+        e = AD.ELEMENTS.index(el)
+        dd = np.zeros(ne); dd[e] = h
+        fd = (chi2_at(M, fobs, loggf0, dd, 1.0) - chi2_at(M, fobs, loggf0, -dd, 1.0)) / (2 * h)
+        assert abs(ga[e] - fd) <= 1e-3 * abs(fd) + 1e-3, (el, ga[e], fd)
+    for i in np.argsort(-np.abs(gl))[:4]:
+        lp = loggf0.copy(); lp[i] += h
+        lm = loggf0.copy(); lm[i] -= h
+        fd = (chi2_at(M, fobs, lp, np.zeros(ne), 1.0) - chi2_at(M, fobs, lm, np.zeros(ne), 1.0)) / (2 * h)
+        assert abs(gl[i] - fd) <= 1e-3 * abs(fd), (i, gl[i], fd)
+    hv = 0.02
+    fd = (chi2_at(M, fobs, loggf0, np.zeros(ne), 1.0 + hv) - chi2_at(M, fobs, loggf0, np.zeros(ne), 1.0 - hv)) / (2 * hv)
+    assert abs(gv - fd) <= 2e-3 * abs(fd), (gv, fd)
+    assert np.max(np.abs(gl - gl_pp)) > 1e-3 * np.max(np.abs(gl_pp))
+    M.close()
+
+
 def test_mixed_forward_gradients_match_fp64(fsg):
     M64, arr = model(fsg, fsg.PREC_FP64)
     loggf0 = np.log10(arr["gf"].astype(np.float64))
