@@ -558,10 +558,11 @@ k_core_batch(const CoreJob *__restrict__ jobs, const int *__restrict__ tile0, in
     }
 }
 
-// lines per staged chunk: about 48 KB of records per buffer (two CTAs per SM), 4 to 16 lines
+// lines per staged chunk: about 24 KB of records per buffer, 4 to 16 lines (with 48 KB the two CTAs
+// per SM left less of the SM's L1 to the table gathers: the core pass took 4 % longer)
 static int core_chunk(int ntau_max) {
     const int per_line = ntau_max * (int)(sizeof(WingRec) + sizeof(CoreRec)) + (int)sizeof(LineHdr);
-    return std::max(4, std::min(16, (48 * 1024) / per_line));
+    return std::max(4, std::min(16, (24 * 1024) / per_line));
 }
 
 static int core_depths(int ntau_max) { return ntau_max <= 72 ? 4 : 8; }
