@@ -558,11 +558,12 @@ k_core_batch(const CoreJob *__restrict__ jobs, const int *__restrict__ tile0, in
     }
 }
 
-// lines per staged chunk: about 24 KB of records per buffer, 4 to 16 lines (with 48 KB the two CTAs
-// per SM left less of the SM's L1 to the table gathers: the core pass took 4 % longer)
+// lines per staged chunk: about 32 KB of records per buffer, 4 to 16 lines.  The buffers share the
+// SM's L1 with the table gathers: per 1e8-line step the core pass took 1.82 / 1.71 / 1.75 / 1.85 s
+// with 48 / 32 / 24 / 16 KB.
 static int core_chunk(int ntau_max) {
     const int per_line = ntau_max * (int)(sizeof(WingRec) + sizeof(CoreRec)) + (int)sizeof(LineHdr);
-    return std::max(4, std::min(16, (24 * 1024) / per_line));
+    return std::max(4, std::min(16, (32 * 1024) / per_line));
 }
 
 static int core_depths(int ntau_max) { return ntau_max <= 72 ? 4 : 8; }
