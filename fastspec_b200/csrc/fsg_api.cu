@@ -2358,7 +2358,11 @@ static int batch_prepare(fsg_batch *b, int P) {
                           b->nk.as<unsigned long long>());
         if (fsg_launch_bclass_order(s, a.cn, a.flags.as<int32_t>(), a.il.as<int32_t>(), a.ir.as<int32_t>(), a.ncls,
                                     a.ccnt.as<int>(), a.coff.as<int64_t>(), a.ctot.as<int64_t>(), a.order.as<int64_t>()))
-            return cuda_fail(ctx, cudaGetLastError(), "batch class order");
+        {
+            const cudaError_t e = cudaGetLastError();
+            batch_join(b, ctx->stream);                // the forked streams rejoin on every path
+            return cuda_fail(ctx, e, "batch class order");
+        }
         fsg_launch_params_fast(s, A, LV, a.order.as<int64_t>(), 0, 1, a.cn, a.flags.as<int32_t>(), a.il.as<int32_t>(),
                                a.ir.as<int32_t>(), c->tab, a.wing.as<WingRec>(), a.core.as<CoreRec>(),
                                a.hdr.as<LineHdr>());
@@ -2368,7 +2372,11 @@ static int batch_prepare(fsg_batch *b, int P) {
             fsg_launch_btile_span(s, 1, a.cn, a.hdr.as<LineHdr>(), a.coff.as<int64_t>(), a.ncls, a.ncls, 32, 32,
                                   c->nwl, batch_core_stride(c), a.ctlo.as<int>(), a.cthi.as<int>(), a.span.p,
                                   a.span.cap))
-            return cuda_fail(ctx, cudaGetLastError(), "batch tile ranges");
+        {
+            const cudaError_t e = cudaGetLastError();
+            batch_join(b, ctx->stream);
+            return cuda_fail(ctx, e, "batch tile ranges");
+        }
     }
     batch_join(b, ctx->stream);
     CK(cudaGetLastError(), "batch prepare");
@@ -2482,14 +2490,21 @@ static int batch_accumulate_solve(fsg_batch *b, const fsg_batch_tuning &t, cudaE
         fsg_ctx *c = a.ctx;
         const cudaStream_t as = b->aux[k++ % fsg_batch::NAUX];
         RayView R;
-        if (rays_prepare(c, &R)) return fail(ctx, FSG_E_STATE, c->err.c_str());   // built at create
+        if (rays_prepare(c, &R)) {                     // built at create: no host work here
+            batch_join(b, s);
+            return fail(ctx, FSG_E_STATE, c->err.c_str());
+        }
         const int rr = R.nmu > 0
             ? fsg_launch_radtran_sph(as, fsg_view(c), c->d_lineopac.as<double>(), R, c->d_wmu.as<double>(), nullptr,
                                      nullptr, a.sfl.as<double>(), a.sfc.as<double>())
             : fsg_launch_radtran(as, fsg_view(c), c->d_lineopac.as<double>(), c->d_rhox.as<double>(), c->nmu,
                                  c->d_xmu.as<double>(), c->d_wmu.as<double>(), nullptr, nullptr, a.sfl.as<double>(),
                                  a.sfc.as<double>());
-        if (rr) return cuda_fail(ctx, cudaGetLastError(), "k_radtran (batch)");
+        if (rr) {
+            const cudaError_t e = cudaGetLastError();
+            batch_join(b, s);
+            return cuda_fail(ctx, e, "k_radtran (batch)");
+        }
     }
     batch_join(b, s);
     if (ev && ev[7]) batch_mark(ev[7], s);
