@@ -241,50 +241,98 @@ void fsg_launch_center(cudaStream_t s, const AtmView &A, const LineView &L, cons
 // Block refill: per retained line of the block, XlineSetup once then XlineDepth over depths.
 // ================================================================================================
 
-// Line j of the block is list line idx[j0 + j * stride].
-__global__ void k_params_fast(AtmView A, LineView L, const int64_t *__restrict__ idx, int64_t j0, int64_t stride,
-                              int64_t nb, const int32_t *__restrict__ flags,
-                              const int32_t *__restrict__ ileft, const int32_t *__restrict__ iright,
-                              const double *__restrict__ anode, const double *__restrict__ aida,
-                              WingRec *wing, CoreRec *core, LineHdr *hdr) {
-    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= nb) return;
-    int64_t i = idx[j0 + j * stride];
+// Line j of the block is list line idx[j0 + j * stride].  One warp per group of 32 lines: lane k
+// runs XlineSetup for line k of the group into shared memory, then the warp walks the group's
+// (line, depth) pairs in record order, one pair per lane, so that each store of wing and core
+// records covers consecutive records of the arrays.  The per-line maximum core half-width and the
+// minimum vv2 are reduced over each line's run of lanes with shuffles (a run is a line's depths in
+// one step) and merged into shared memory by the run's first lane; lane k then writes the header of
+// line k.  Both reductions are exact (max / min), so the records and headers do not depend on the
+// order in which depths are taken.
+#define PF_WARPS 4
+__global__ void __launch_bounds__(PF_WARPS * 32)
+k_params_fast(AtmView A, LineView L, const int64_t *__restrict__ idx, int64_t j0, int64_t stride,
+              int64_t nb, const int32_t *__restrict__ flags,
+              const int32_t *__restrict__ ileft, const int32_t *__restrict__ iright,
+              const double *__restrict__ anode, const double *__restrict__ aida,
+              WingRec *wing, CoreRec *core, LineHdr *hdr) {
+    __shared__ XCoef xs[PF_WARPS][32];
+    __shared__ unsigned long long hcs[PF_WARPS][32];   // bits of hcore + 1 (0: no depth has a core)
+    __shared__ unsigned vms[PF_WARPS][32];             // bits of the smallest vv2 (non-negative floats)
+    const int wp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t jb = ((int64_t)blockIdx.x * PF_WARPS + wp) * 32;
+    if (jb >= nb) return;                               // whole warps only: no block barrier below
+    const int ng = (nb - jb < 32) ? (int)(nb - jb) : 32;
     const int nt = A.ntau;
-    int f = flags[i];
-    double wlc = L.wl[i] - A.wfirst;
-    XCoef XC;
-    xline_setup(A, L, i, wlc, f, &XC);
-    double hcore = -1.0;        // largest |dl| of any depth's core region (s < 196)
-    float vv2min = 3.0e38f;     // smallest FP32 vv2 over depths (the wing pass's mask offset)
-    for (int t = 0; t < nt; t++) {
-        double cop, vv, av;
-        xline_depth(A, t, XC, &cop, &vv, &av);
-        if (A.motype == 1) cop = cop / A.contstd[t];     // LineOpacity1 divides the sum by ContOpacStd
-        double a2 = av * av;
-        WingRec w;
-        w.vv2 = (float)(vv * vv);
-        w.c2m1 = (float)(a2 - 0.5);
-        w.twoA = (float)(2.0 * a2);
-        w.c1 = (float)(cop * av * FSG_SQRTPIINV);
-        vv2min = fminf(vv2min, w.vv2);
-        CoreRec c;
-        c.vv = vv; c.cop = (float)cop; c.a = (float)av; c.pad0 = c.pad1 = 0;
-        // table row and weight of a in FP64 (sqrt(a) nodes, voigt.f90:84-92); ia = 0: a >= 8
-        if (!(av < 8.0)) { c.ia = 0; c.ua = 0.0f; }
-        else if (av < anode[1]) { c.ia = 1; c.ua = (float)(av * aida[0]); }
-        else {
-            const int ia = min((int)(sqrt(av) * (1.0 / (2.8284271247461903 / 400.0))) + 1, FSG_NVA);
-            c.ia = ia;
-            c.ua = (float)((av - anode[ia - 1]) * aida[ia - 1]);
-        }
-        wing[(size_t)j * nt + t] = w;
-        core[(size_t)j * nt + t] = c;
-        // the accumulation evaluates the core form where fl32(dl^2 vv2 + c2m1) < 195.5; a margin of
-        // 0.05 in s and 1e-5 in dl covers the FP32 rounding of the records and of dl^2
-        double q = 196.05 - a2;
-        if (q > 0.0) hcore = fmax(hcore, sqrt(q) / vv * (1.0 + 1e-5));
+    int64_t i = 0; int f = 0; double wlc = 0.0;
+    if (lane < ng) {
+        i = idx[j0 + (jb + lane) * stride];
+        f = flags[i];
+        wlc = L.wl[i] - A.wfirst;
+        xline_setup(A, L, i, wlc, f, &xs[wp][lane]);
     }
+    hcs[wp][lane] = 0ull;
+    vms[wp][lane] = __float_as_uint(3.0e38f);
+    __syncwarp();
+    const int tot = ng * nt;
+    WingRec *wg = wing + (size_t)jb * nt;
+    CoreRec *cg = core + (size_t)jb * nt;
+    // pair p = lane + step: line ln = p / nt, depth t = p % nt, advanced by 32 per step
+    int ln = lane / nt, t = lane - (lane / nt) * nt;
+    for (int p0 = 0; p0 < tot; p0 += 32) {
+        const int p = p0 + lane;
+        const bool on = p < tot;
+        double hc = -1.0;          // this pair's core half-width (s < 196), -1 when none
+        float vv2 = 3.0e38f;
+        if (on) {
+            const XCoef &XC = xs[wp][ln];
+            double cop, vv, av;
+            xline_depth(A, t, XC, &cop, &vv, &av);
+            if (A.motype == 1) cop = cop / A.contstd[t];     // LineOpacity1 divides the sum by ContOpacStd
+            double a2 = av * av;
+            WingRec w;
+            w.vv2 = (float)(vv * vv);
+            w.c2m1 = (float)(a2 - 0.5);
+            w.twoA = (float)(2.0 * a2);
+            w.c1 = (float)(cop * av * FSG_SQRTPIINV);
+            vv2 = w.vv2;
+            CoreRec c;
+            c.vv = vv; c.cop = (float)cop; c.a = (float)av; c.pad0 = c.pad1 = 0;
+            // table row and weight of a in FP64 (sqrt(a) nodes, voigt.f90:84-92); ia = 0: a >= 8
+            if (!(av < 8.0)) { c.ia = 0; c.ua = 0.0f; }
+            else if (av < anode[1]) { c.ia = 1; c.ua = (float)(av * aida[0]); }
+            else {
+                const int ia = min((int)(sqrt(av) * (1.0 / (2.8284271247461903 / 400.0))) + 1, FSG_NVA);
+                c.ia = ia;
+                c.ua = (float)((av - anode[ia - 1]) * aida[ia - 1]);
+            }
+            wg[p] = w;
+            cg[p] = c;
+            // the accumulation evaluates the core form where fl32(dl^2 vv2 + c2m1) < 195.5; a margin
+            // of 0.05 in s and 1e-5 in dl covers the FP32 rounding of the records and of dl^2
+            double q = 196.05 - a2;
+            if (q > 0.0) hc = sqrt(q) / vv * (1.0 + 1e-5);
+        }
+        // segmented reduction over the run of lanes that share this lane's line (lanes past the
+        // last pair form their own run at the end); the run's first lane ends with the run's value
+        #pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            double oh = __shfl_down_sync(0xffffffffu, hc, off);
+            float ov = __shfl_down_sync(0xffffffffu, vv2, off);
+            if (lane + off < 32 && t + off < nt) { hc = fmax(hc, oh); vv2 = fminf(vv2, ov); }
+        }
+        if (on && (lane == 0 || t == 0)) {
+            if (hc >= 0.0) atomicMax(&hcs[wp][ln], (unsigned long long)__double_as_longlong(hc) + 1ull);
+            atomicMin(&vms[wp][ln], __float_as_uint(vv2));
+        }
+        t += 32;
+        while (t >= nt) { t -= nt; ln++; }
+    }
+    __syncwarp();
+    if (lane >= ng) return;
+    const unsigned long long hb = hcs[wp][lane];
+    const double hcore = hb ? __longlong_as_double((long long)(hb - 1ull)) : -1.0;
+    const float vv2min = __uint_as_float(vms[wp][lane]);
     LineHdr h;
     h.wlh = (float)wlc;
     h.wll = (float)(wlc - (double)h.wlh);
@@ -305,7 +353,7 @@ __global__ void k_params_fast(AtmView A, LineView L, const int64_t *__restrict__
     // c1 (t + 1) stays finite; the point then adds exactly 0
     h.pad0 = __float_as_int(1.0e19f / vv2min);
     h.pad1 = 0;
-    hdr[j] = h;
+    hdr[jb + lane] = h;
 }
 
 void fsg_launch_params_fast(cudaStream_t s, const AtmView &A, const LineView &L, const int64_t *idx,
@@ -313,8 +361,9 @@ void fsg_launch_params_fast(cudaStream_t s, const AtmView &A, const LineView &L,
                             const int32_t *iright, const VoigtTables &T, WingRec *wing, CoreRec *core,
                             LineHdr *hdr) {
     if (nb <= 0) return;
-    k_params_fast<<<(unsigned)((nb + 127) / 128), 128, 0, s>>>(A, L, idx, j0, stride, nb, flags, ileft, iright,
-                                                               T.anode, T.aida, wing, core, hdr);
+    const int64_t per = PF_WARPS * 32;
+    k_params_fast<<<(unsigned)((nb + per - 1) / per), PF_WARPS * 32, 0, s>>>(A, L, idx, j0, stride, nb, flags, ileft,
+                                                                            iright, T.anode, T.aida, wing, core, hdr);
 }
 
 // FP64 parameters for the plain path: p64[j][t] = (LinCop, LinVvgt, LinAvgt)
