@@ -297,9 +297,8 @@ int fsg_locprf_pp(fsg_ctx *ctx, int nprof, int nmu, const double *xmu, int ntau,
  * arrays sit in a fixed 8 MiB device array of the library, so nprof * ntau * 3 may not exceed
  * 1,048,576 (larger sizes return FSG_E_ARG).  stream is a cudaStream_t (NULL: the default
  * stream); the call waits for the kernel with cudaStreamSynchronize on that stream and returns
- * after it has finished.  The first call on a device looks up
- * the array's device address with that device current; make that first call before any stream
- * capture.  All calls share the array, so calls that overlap on the GPU race. */
+ * after it has finished.  The first call on a device looks up the array's device address with
+ * that device current.  All calls share the array, so calls that overlap on the GPU race. */
 int fsg_locprf_pp_noalloc(int nprof, int nmu, const double *d_xmu, int ntau, const double *d_xki,
                           const double *d_src, const double *d_rhox, double *d_ploc, void *stream);
 /* MuQuadrature (utils.f90:1273-1330): x (in/out when setnodes == 0), w, r [n+1]. */
