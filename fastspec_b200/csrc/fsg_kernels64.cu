@@ -177,7 +177,9 @@ __device__ __forceinline__ double center_shift(const AtmView &A, int ihe, int t)
     return (ihe > 0) ? A.heshf[(ihe - 1) * A.ntau + t] : 0.0;
 }
 
-__global__ void k_center(AtmView A, LineView L, const float *__restrict__ vtab,
+// Eight 128-thread CTAs per SM (64 registers, a few spilled): the sweep is bound by the FP64 pipe,
+// and the extra resident warps hide more of its latency (177 -> 150 ms on the 1e8-line list).
+__global__ void __launch_bounds__(128, 8) k_center(AtmView A, LineView L, const float *__restrict__ vtab,
                          const double *__restrict__ anode, const double *__restrict__ aida,
                          int32_t *flags, int32_t *ileft, int32_t *iright, unsigned long long *nkeep) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
